@@ -1,0 +1,259 @@
+"""Seeded synthetic RGB-D sequences with an analytic scene SDF.
+
+The reference is exercised on TUM RGB-D sequences (640x480 uint16 depth at
+5000 units/m, fx=fy=525, cx=319.5, cy=239.5; reference
+src/onlinefusionviewer_main.cpp:234-237, README.md:60-70).  No dataset is
+available offline, so this module ray-casts depth and colour frames of the
+same shape from an analytic scene in FP64:
+
+* a room (an axis-aligned box seen from the inside) holding seeded random
+  axis-aligned boxes and spheres, each with one uint8 RGB albedo;
+* per-pixel depth z along the optical axis, plus Gaussian noise with
+  sigma = noise_k * z^2 metres and a fraction of random zero "holes";
+* depth stored as round(z * 5000) in uint16 (0 where z >= 13.1 m), colour as
+  BGR uint8, the reference's channel order (update_functions.cpp:1262-1290
+  reads red from byte 2).
+
+Poses are camera-to-world [R|t] with the OpenCV camera frame (x right, y
+down, z forward), the convention of the reference's CameraInfo.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+DEPTH_UNITS_PER_M = 5000.0
+
+
+@dataclasses.dataclass
+class Scene:
+    room: np.ndarray          # (3,) room extent in metres, room = [0, room]^3
+    box_lo: np.ndarray        # (B, 3)
+    box_hi: np.ndarray        # (B, 3)
+    box_rgb: np.ndarray       # (B, 3) uint8 (R, G, B)
+    sph_c: np.ndarray         # (S, 3)
+    sph_r: np.ndarray         # (S,)
+    sph_rgb: np.ndarray       # (S, 3) uint8
+    wall_rgb: np.ndarray      # (6, 3) uint8: -x, +x, -y, +y, -z, +z walls
+
+    def sdf(self, p: np.ndarray) -> np.ndarray:
+        """Signed distance of points p (N,3) to the scene surfaces, positive in
+        free space: min over the room walls (seen from inside) and the solids."""
+        p = np.asarray(p, dtype=np.float64)
+        d = np.min(np.concatenate([p, self.room[None, :] - p], axis=1), axis=1)
+        for lo, hi in zip(self.box_lo, self.box_hi):
+            c = 0.5 * (lo + hi)
+            h = 0.5 * (hi - lo)
+            q = np.abs(p - c) - h
+            outside = np.linalg.norm(np.maximum(q, 0.0), axis=1)
+            inside = np.minimum(np.max(q, axis=1), 0.0)
+            d = np.minimum(d, outside + inside)
+        for c, r in zip(self.sph_c, self.sph_r):
+            d = np.minimum(d, np.linalg.norm(p - c, axis=1) - r)
+        return d
+
+
+def make_scene(seed: int, room=(4.0, 4.0, 3.0), n_prims: int = 20, size=(0.1, 0.8),
+               keep_clear=None) -> Scene:
+    """Room plus n_prims seeded boxes/spheres (p = 1/2 each), sizes U(size)."""
+    rng = np.random.default_rng(seed)
+    room = np.asarray(room, dtype=np.float64)
+    box_lo, box_hi, box_rgb, sph_c, sph_r, sph_rgb = [], [], [], [], [], []
+    tries = 0
+    while len(box_lo) + len(sph_c) < n_prims and tries < 100 * max(n_prims, 1):
+        tries += 1
+        c = rng.uniform(0.0, 1.0, 3) * room
+        rgb = rng.integers(0, 256, 3).astype(np.uint8)
+        is_box = rng.uniform() < 0.5
+        if is_box:
+            ext = rng.uniform(size[0], size[1], 3)
+            radius = float(np.linalg.norm(ext) / 2)
+        else:
+            radius = float(rng.uniform(size[0], size[1]) / 2)
+        if keep_clear is not None and not keep_clear(c, radius + 0.15):
+            continue
+        if is_box:
+            box_lo.append(c - ext / 2)
+            box_hi.append(c + ext / 2)
+            box_rgb.append(rgb)
+        else:
+            sph_c.append(c)
+            sph_r.append(radius)
+            sph_rgb.append(rgb)
+    wall_rgb = rng.integers(40, 256, (6, 3)).astype(np.uint8)
+    z3 = np.zeros((0, 3))
+    return Scene(room=room,
+                 box_lo=np.array(box_lo) if box_lo else z3, box_hi=np.array(box_hi) if box_hi else z3,
+                 box_rgb=np.array(box_rgb, dtype=np.uint8).reshape(-1, 3),
+                 sph_c=np.array(sph_c) if sph_c else z3, sph_r=np.array(sph_r, dtype=np.float64),
+                 sph_rgb=np.array(sph_rgb, dtype=np.uint8).reshape(-1, 3), wall_rgb=wall_rgb)
+
+
+def look_at(pos, target, up=(0.0, 0.0, 1.0)) -> np.ndarray:
+    """Camera-to-world rotation (columns = camera x right, y down, z forward)."""
+    pos = np.asarray(pos, dtype=np.float64)
+    z = np.asarray(target, dtype=np.float64) - pos
+    z /= np.linalg.norm(z)
+    x = np.cross(z, np.asarray(up, dtype=np.float64))
+    x /= np.linalg.norm(x)
+    y = np.cross(z, x)
+    return np.stack([x, y, z], axis=1)
+
+
+def circle_trajectory(n_frames: int, centre=(2.0, 2.0), radius=1.5, height=1.2, target=(2.0, 2.0, 1.5)):
+    """Pose k at angle 2*pi*k/n on a horizontal circle, looking at target."""
+    poses = []
+    for k in range(n_frames):
+        a = 2.0 * math.pi * k / n_frames
+        pos = np.array([centre[0] + radius * math.cos(a), centre[1] + radius * math.sin(a), height])
+        poses.append((look_at(pos, target), pos))
+    return poses
+
+
+def random_walk_trajectory(n_frames: int, seed: int, room=(8.0, 8.0, 3.0), step=0.02, yaw_jitter_deg=2.0,
+                           height=1.2, margin=0.8):
+    """Seeded random walk at fixed height, bouncing off a margin to the walls."""
+    rng = np.random.default_rng(seed + 7919)
+    pos = np.array([room[0] / 2, room[1] / 2, height])
+    yaw = rng.uniform(0, 2 * math.pi)
+    poses = []
+    for _ in range(n_frames):
+        yaw += math.radians(rng.normal(0.0, yaw_jitter_deg))
+        d = np.array([math.cos(yaw), math.sin(yaw), 0.0])
+        nxt = pos + step * d
+        if not (margin < nxt[0] < room[0] - margin and margin < nxt[1] < room[1] - margin):
+            yaw += math.pi
+            d = -d
+            nxt = pos + step * d
+        pos = nxt
+        target = pos + d + np.array([0.0, 0.0, 0.1])
+        poses.append((look_at(pos, target), pos.copy()))
+    return poses
+
+
+def _hit_box(o, d, lo, hi):
+    with np.errstate(divide='ignore', invalid='ignore'):
+        inv = 1.0 / d
+        t1 = (lo[None, :] - o[None, :]) * inv
+        t2 = (hi[None, :] - o[None, :]) * inv
+    tn = np.nanmax(np.minimum(t1, t2), axis=1)
+    tf = np.nanmin(np.maximum(t1, t2), axis=1)
+    hit = (tn <= tf) & (tn > 1e-9)
+    return np.where(hit, tn, np.inf)
+
+
+def _hit_sphere(o, d, c, r):
+    oc = o - c
+    a = np.einsum('ij,ij->i', d, d)
+    b = d @ oc
+    cc = float(oc @ oc) - r * r
+    disc = b * b - a * cc
+    ok = disc >= 0
+    sq = np.sqrt(np.where(ok, disc, 0.0))
+    t = (-b - sq) / a
+    return np.where(ok & (t > 1e-9), t, np.inf)
+
+
+def render(scene: Scene, R: np.ndarray, t: np.ndarray, width: int, height: int, fx: float, fy: float,
+           cx: float, cy: float, rng: np.random.Generator | None = None, noise_k: float = 0.0012,
+           hole_frac: float = 0.02):
+    """Ray-cast one frame.  Returns (depth uint16 [H,W], bgr uint8 [H,W,3], z_true float64 [H,W])."""
+    xs = (np.arange(width, dtype=np.float64) - cx) / fx
+    ys = (np.arange(height, dtype=np.float64) - cy) / fy
+    dcam = np.stack(np.broadcast_arrays(xs[None, :], ys[:, None], np.ones((height, width))), axis=-1).reshape(-1, 3)
+    d = dcam @ R.T          # ray direction in world, parametrised so that t == camera z
+    o = np.asarray(t, dtype=np.float64)
+    # room from the inside: exit distance
+    with np.errstate(divide='ignore', invalid='ignore'):
+        inv = 1.0 / d
+        ta = (0.0 - o[None, :]) * inv
+        tb = (scene.room[None, :] - o[None, :]) * inv
+    texit = np.where(np.isfinite(ta), np.maximum(ta, tb), np.inf)
+    axis = np.argmin(texit, axis=1)
+    tbest = texit[np.arange(len(axis)), axis]
+    side = (d[np.arange(len(axis)), axis] > 0).astype(np.int64)
+    colour = scene.wall_rgb[2 * axis + side].astype(np.uint8)
+    for lo, hi, rgb in zip(scene.box_lo, scene.box_hi, scene.box_rgb):
+        th = _hit_box(o, d, lo, hi)
+        closer = th < tbest
+        tbest = np.where(closer, th, tbest)
+        colour[closer] = rgb
+    for c, r, rgb in zip(scene.sph_c, scene.sph_r, scene.sph_rgb):
+        th = _hit_sphere(o, d, c, r)
+        closer = th < tbest
+        tbest = np.where(closer, th, tbest)
+        colour[closer] = rgb
+    z_true = tbest.reshape(height, width)
+    z = z_true.copy()
+    if rng is not None:
+        if noise_k > 0:
+            z = z + rng.normal(0.0, 1.0, z.shape) * noise_k * z * z
+        if hole_frac > 0:
+            z[rng.uniform(size=z.shape) < hole_frac] = 0.0
+    z = np.where(np.isfinite(z) & (z > 0), z, 0.0)
+    depth = np.round(z * DEPTH_UNITS_PER_M)
+    depth[(z >= 13.1) | (depth > 65535)] = 0
+    depth = depth.astype(np.uint16)
+    bgr = colour[:, ::-1].reshape(height, width, 3).copy()
+    return depth, bgr, z_true
+
+
+@dataclasses.dataclass
+class Sequence:
+    scene: Scene
+    K: np.ndarray             # fx, fy, cx, cy (float64)
+    width: int
+    height: int
+    poses: list               # [(R (3,3), t (3,)), ...]
+    seed: int
+    noise_k: float = 0.0012
+    hole_frac: float = 0.02
+
+    def frame(self, k: int):
+        rng = np.random.default_rng((self.seed, k))
+        R, t = self.poses[k]
+        fx, fy, cx, cy = self.K
+        depth, bgr, _ = render(self.scene, R, t, self.width, self.height, fx, fy, cx, cy, rng,
+                               self.noise_k, self.hole_frac)
+        return depth, bgr, R, t
+
+    def __len__(self):
+        return len(self.poses)
+
+
+def room_circle_sequence(seed: int = 0, n_frames: int = 100, width: int = 640, height: int = 480,
+                         n_prims: int = 20, room=(4.0, 4.0, 3.0)) -> Sequence:
+    """The plain-method workload: a 4x4x3 m room with 20 seeded primitives,
+    frames on a circle of radius 1.5 m at 1.2 m height around the room centre
+    looking at (2, 2, 1.5).  Intrinsics scale with the resolution from the
+    640x480 values fx=fy=525, cx=319.5, cy=239.5."""
+    s = width / 640.0
+    K = np.array([525.0 * s, 525.0 * s, (width - 1) / 2.0, (height - 1) / 2.0])
+    centre = (room[0] / 2, room[1] / 2)
+
+    def clear(c, rad):
+        dxy = math.hypot(c[0] - centre[0], c[1] - centre[1])
+        return abs(dxy - 1.5) > rad or abs(c[2] - 1.2) > rad
+
+    scene = make_scene(seed, room=room, n_prims=n_prims, keep_clear=clear)
+    poses = circle_trajectory(n_frames, centre=centre, radius=1.5, height=1.2,
+                              target=(centre[0], centre[1], 1.5))
+    return Sequence(scene=scene, K=K, width=width, height=height, poses=poses, seed=seed)
+
+
+def room_walk_sequence(seed: int = 0, n_frames: int = 1000, width: int = 640, height: int = 480,
+                       n_prims: int = 80, room=(8.0, 8.0, 3.0)) -> Sequence:
+    """The larger workload: an 8x8x3 m room with 80 primitives and a seeded
+    random walk (2 cm steps, 2 degree yaw jitter) at 1.2 m height."""
+    s = width / 640.0
+    K = np.array([525.0 * s, 525.0 * s, (width - 1) / 2.0, (height - 1) / 2.0])
+    poses = random_walk_trajectory(n_frames, seed, room=room)
+    cams = np.array([p[1] for p in poses])
+
+    def clear(c, rad):
+        return np.min(np.linalg.norm(cams - c[None, :], axis=1)) > rad + 0.3
+
+    scene = make_scene(seed, room=room, n_prims=n_prims, keep_clear=clear)
+    return Sequence(scene=scene, K=K, width=width, height=height, poses=poses, seed=seed)

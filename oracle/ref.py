@@ -1,0 +1,164 @@
+"""ctypes view of oracle/_ref/libffref.so: the reference's own FusionMipMapCPU
+compiled from its sources (see oracle/Makefile).
+
+ORACLE INFRASTRUCTURE ONLY.  Imported by tests/, the smoke check and the CPU
+baseline leg of bench.py, never by fastfusion_b200/.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_ref", "libffref.so")
+_libs = {}
+
+BRANCHINIT = 0xFFFFFFFE
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    key = 0
+    if key not in _libs:
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ll, i32 = ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int
+        L.ref_create.restype = vp
+        L.ref_create.argtypes = [ctypes.c_float, ctypes.c_float, i32, ll]
+        L.ref_destroy.argtypes = [vp]
+        L.ref_quiet.argtypes = [i32]
+        L.ref_set_incremental_meshing.argtypes = [vp, i32]
+        L.ref_add_map.restype = i32
+        L.ref_add_map.argtypes = [vp, vp, vp, i32, i32, vp, vp, vp, ctypes.c_float, ctypes.c_float]
+        L.ref_update_meshes.restype = i32
+        L.ref_update_meshes.argtypes = [vp]
+        L.ref_mesh_counts.argtypes = [vp, ctypes.POINTER(ll), ctypes.POINTER(ll)]
+        L.ref_mesh_copy.argtypes = [vp, vp, vp, vp]
+        L.ref_state.argtypes = [vp, vp, vp]
+        L.ref_leaves.argtypes = [vp, ll, vp, vp, vp]
+        L.ref_queue.argtypes = [vp, vp]
+        L.ref_tree.argtypes = [vp, vp]
+        L.ref_bricks.argtypes = [vp, ll, vp, vp, vp]
+        L.ref_cells.restype = ll
+        L.ref_cells.argtypes = [vp, vp]
+        L.ref_queue_all_cells.argtypes = [vp]
+        L.ref_cell_mesh.restype = ll
+        L.ref_cell_mesh.argtypes = [vp, ll, vp, vp, vp, ctypes.POINTER(ll)]
+        L.ref_mc_offset_table.argtypes = [vp]
+        _libs[key] = L
+    return _libs[key]
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class RefFusion:
+    """The reference FusionMipMapCPU (single-threaded meshing)."""
+
+    def __init__(self, scale=0.005, threshold=0.01, color=True, pool_bytes=0, quiet=True):
+        self.L = L = lib()
+        if quiet:
+            L.ref_quiet(1)
+        self.h = L.ref_create(scale, threshold, 1 if color else 0, int(pool_bytes))
+
+    def close(self):
+        if self.h:
+            self.L.ref_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_map(self, depth, bgr, K, R, t, scaling=1.0 / 5000.0, maxcam=4.0) -> int:
+        depth = np.ascontiguousarray(depth, dtype=np.uint16)
+        bgr = np.ascontiguousarray(bgr, dtype=np.uint8)
+        K = np.ascontiguousarray(K, dtype=np.float64)
+        R = np.ascontiguousarray(R, dtype=np.float64)
+        t = np.ascontiguousarray(t, dtype=np.float64)
+        h, w = depth.shape
+        return self.L.ref_add_map(self.h, _p(depth), _p(bgr), w, h, _p(K), _p(R), _p(t),
+                                 ctypes.c_float(scaling), ctypes.c_float(maxcam))
+
+    def update_meshes(self) -> bool:
+        return bool(self.L.ref_update_meshes(self.h))
+
+    def mesh(self):
+        nv, nf = ctypes.c_longlong(), ctypes.c_longlong()
+        self.L.ref_mesh_counts(self.h, ctypes.byref(nv), ctypes.byref(nf))
+        xyz = np.zeros((nv.value, 3), np.float32)
+        rgb = np.zeros((nv.value, 3), np.uint8)
+        faces = np.zeros((nf.value, 3), np.uint32)
+        self.L.ref_mesh_copy(self.h, _p(xyz), _p(rgb), _p(faces))
+        return xyz, rgb, faces
+
+    def state(self) -> dict:
+        ints = np.zeros(16, np.int64)
+        off = np.zeros(3, np.float32)
+        self.L.ref_state(self.h, _p(ints), _p(off))
+        keys = ["n", "leaves_used", "branches_used", "queued", "leaves_total", "branches_total",
+                "cells", "frames", "bandwidth", "incremental"]
+        d = {k: int(v) for k, v in zip(keys, ints)}
+        d["offset"] = off
+        return d
+
+    def leaves(self, n=None):
+        if n is None:
+            n = self.state()["leaves_used"]
+        pos = np.zeros((n, 3), np.uint16)
+        scl = np.zeros(n, np.uint16)
+        par = np.zeros(n, np.uint32)
+        self.L.ref_leaves(self.h, n, _p(pos), _p(scl), _p(par))
+        return pos, scl, par
+
+    def queue(self):
+        n = self.state()["queued"]
+        q = np.zeros(n, np.uint32)
+        self.L.ref_queue(self.h, _p(q))
+        return q
+
+    def tree(self):
+        n = self.state()["branches_used"]
+        tr = np.zeros(n, np.uint32)
+        self.L.ref_tree(self.h, _p(tr))
+        return tr
+
+    def bricks(self, n=None):
+        if n is None:
+            n = min(self.state()["leaves_used"], self.state()["leaves_total"])
+        d = np.zeros((n, 512), np.float32)
+        w = np.zeros((n, 512), np.float32)
+        c = np.zeros((n, 512, 3), np.uint16)
+        self.L.ref_bricks(self.h, n, _p(d), _p(w), _p(c))
+        return d, w, c
+
+    def cells(self):
+        n = self.L.ref_cells(self.h, None)
+        out = np.zeros((n, 14), np.int32)
+        self.L.ref_cells(self.h, _p(out))
+        return out
+
+    def queue_all_cells(self):
+        self.L.ref_queue_all_cells(self.h)
+
+    def cell_mesh(self, i):
+        nf = ctypes.c_longlong()
+        nv = self.L.ref_cell_mesh(self.h, i, None, None, None, ctypes.byref(nf))
+        xyz = np.zeros((nv, 3), np.float32)
+        rgb = np.zeros((nv, 3), np.uint8)
+        faces = np.zeros((nf.value, 3), np.uint32)
+        self.L.ref_cell_mesh(self.h, i, _p(xyz), _p(rgb), _p(faces), ctypes.byref(nf))
+        return xyz, rgb, faces
+
+
+def mc_offset_table() -> np.ndarray:
+    out = np.zeros((256, 16), np.int32)
+    lib().ref_mc_offset_table(_p(out))
+    return out

@@ -1,0 +1,252 @@
+/*
+ * C entry points over the reference's own FusionMipMapCPU, compiled from the
+ * unmodified reference sources (src/fusion/*.cpp) into oracle/_ref/libffref.so.
+ *
+ * ORACLE INFRASTRUCTURE ONLY.  Only tests/, the smoke check and bench.py's CPU
+ * baseline leg load this library, as the checker and as the timed reference
+ * CPU path.  Nothing in fastfusion_b200/ links or calls it.
+ *
+ * The harness reads the fusion object's internal arrays (leaf table, queue,
+ * brick pool, mesh cells) so the GPU path can be compared with it field by
+ * field; it therefore compiles the reference header with protected members
+ * opened up.  The object layout is unchanged by that.
+ */
+/* Standard headers first, so opening access below touches only the
+ * reference's own classes. */
+#include <opencv2/opencv.hpp>
+#include <boost/thread.hpp>
+#include <fstream>
+#include <sstream>
+#include <iostream>
+#include <thread>
+#include <tuple>
+#define protected public
+#define private public
+#include <fusion/geometryfusion_mipmap_cpu.hpp>
+#undef protected
+#undef private
+
+#include <auxiliary/memory.hpp>
+#include <fcntl.h>
+#include <unistd.h>
+
+#include <cstdint>
+#include <cstdio>
+
+/* The reference sizes its brick pool from half the physical memory, capped at
+ * 2e9 bytes (geometryfusion_mipmap_cpu.cpp:497-507).  The oracle build links
+ * these definitions in place of src/auxiliary/memory.cpp so a test can ask for
+ * a small pool (and so force pool overflow) without touching the reference. */
+static long long g_total_system_memory = 4000000000LL;
+long long getTotalSystemMemory() { return g_total_system_memory; }
+long long getAvailableSystemMemory() { return g_total_system_memory; }
+ProcessMemoryStats getProcessMemory() {
+  ProcessMemoryStats s = {0, 0, 0, 0, 0, 0, 0, 4096};
+  return s;
+}
+
+extern "C" {
+
+/* Redirect the reference's (very chatty) stderr to /dev/null, or back. */
+static int g_saved_stderr = -1;
+void ref_quiet(int quiet) {
+  fflush(stderr);
+  if (quiet && g_saved_stderr < 0) {
+    g_saved_stderr = dup(2);
+    int fd = open("/dev/null", O_WRONLY);
+    dup2(fd, 2);
+    close(fd);
+  } else if (!quiet && g_saved_stderr >= 0) {
+    dup2(g_saved_stderr, 2);
+    close(g_saved_stderr);
+    g_saved_stderr = -1;
+  }
+}
+
+/* pool_bytes: the memory budget handed to the reference's sizing rule
+ * (0 keeps the default: the 2e9-byte cap). */
+void *ref_create(float scale, float threshold, int color, long long pool_bytes) {
+  g_total_system_memory = pool_bytes > 0 ? 2 * pool_bytes : 4000000000LL;
+  FusionMipMapCPU *f = new FusionMipMapCPU(0, 0, 0, scale, threshold, 0, color != 0);
+  f->setThreadMeshing(false);
+  return f;
+}
+
+void ref_destroy(void *h) { delete (FusionMipMapCPU *)h; }
+
+void ref_set_incremental_meshing(void *h, int on) { ((FusionMipMapCPU *)h)->setIncrementalMeshing(on != 0); }
+
+int ref_add_map(void *h, const uint16_t *depth, const uint8_t *bgr, int w, int hgt, const double *K4,
+                const double *R9, const double *t3, float scaling, float maxcam) {
+  FusionMipMapCPU *f = (FusionMipMapCPU *)h;
+  cv::Mat d(hgt, w, CV_16UC1, (void *)depth);
+  cv::Mat c(hgt, w, CV_8UC3, (void *)bgr);
+  CameraInfo cam;
+  cv::Mat K = cv::Mat::eye(3, 3, CV_64FC1);
+  K.at<double>(0, 0) = K4[0];
+  K.at<double>(1, 1) = K4[1];
+  K.at<double>(0, 2) = K4[2];
+  K.at<double>(1, 2) = K4[3];
+  cam.setIntrinsic(K);
+  cv::Mat E = cv::Mat::eye(4, 4, CV_64FC1);
+  for (int r = 0; r < 3; r++) {
+    for (int k = 0; k < 3; k++) E.at<double>(r, k) = R9[r * 3 + k];
+    E.at<double>(r, 3) = t3[r];
+  }
+  cam.setExtrinsic(E);
+  return f->addMap(d, cam, c, scaling, maxcam);
+}
+
+int ref_update_meshes(void *h) { return ((FusionMipMapCPU *)h)->updateMeshes() ? 1 : 0; }
+
+/* Mesh of the last finished update: counts, then copies. */
+void ref_mesh_counts(void *h, long long *nv, long long *nf) {
+  FusionMipMapCPU *f = (FusionMipMapCPU *)h;
+  *nv = (long long)f->_meshCurrent->vertices.size();
+  *nf = (long long)f->_meshCurrent->faces.size() / 3;
+}
+
+void ref_mesh_copy(void *h, float *xyz, uint8_t *rgb, uint32_t *faces) {
+  FusionMipMapCPU *f = (FusionMipMapCPU *)h;
+  const MeshInterleaved &m = *f->_meshCurrent;
+  for (size_t i = 0; i < m.vertices.size(); i++) {
+    xyz[3 * i + 0] = m.vertices[i].x;
+    xyz[3 * i + 1] = m.vertices[i].y;
+    xyz[3 * i + 2] = m.vertices[i].z;
+  }
+  for (size_t i = 0; i < m.colors.size(); i++) {
+    rgb[3 * i + 0] = m.colors[i].r;
+    rgb[3 * i + 1] = m.colors[i].g;
+    rgb[3 * i + 2] = m.colors[i].b;
+  }
+  for (size_t i = 0; i < m.faces.size(); i++) faces[i] = m.faces[i];
+}
+
+/* Scalar state: n, offset, counters. */
+void ref_state(void *h, long long *ints, float *offset) {
+  FusionMipMapCPU *f = (FusionMipMapCPU *)h;
+  ints[0] = f->_n;
+  ints[1] = f->_nLeavesUsed;
+  ints[2] = f->_nBranchesUsed;
+  ints[3] = f->_nLeavesQueuedSurface;
+  ints[4] = f->_nLeavesTotal;
+  ints[5] = f->_nBranchesTotal;
+  ints[6] = (long long)f->_meshCells.size();
+  ints[7] = f->_framesAdded;
+  ints[8] = f->_bandwidth;
+  ints[9] = f->_performIncrementalMeshing ? 1 : 0;
+  offset[0] = f->_offset.x;
+  offset[1] = f->_offset.y;
+  offset[2] = f->_offset.z;
+}
+
+/* Leaf table for leaves [0, n): position (3 x uint16), scale, parent leaf. */
+void ref_leaves(void *h, long long n, uint16_t *pos, uint16_t *scl, uint32_t *parent) {
+  FusionMipMapCPU *f = (FusionMipMapCPU *)h;
+  for (long long i = 0; i < n; i++) {
+    pos[3 * i + 0] = f->_leafPos[i].x;
+    pos[3 * i + 1] = f->_leafPos[i].y;
+    pos[3 * i + 2] = f->_leafPos[i].z;
+    scl[i] = f->_leafScale[i];
+    parent[i] = (size_t)i < f->_leafParent.size() ? f->_leafParent[i] : 0xFFFFFFFFu;
+  }
+}
+
+/* The queue of leaves touched by the last addMap, in the reference's order. */
+void ref_queue(void *h, uint32_t *q) {
+  FusionMipMapCPU *f = (FusionMipMapCPU *)h;
+  for (volumetype i = 0; i < f->_nLeavesQueuedSurface; i++) q[i] = f->_leafNumberSurface[i];
+}
+
+/* The raw octree array (first nBranchesUsed entries). */
+void ref_tree(void *h, uint32_t *tree) {
+  FusionMipMapCPU *f = (FusionMipMapCPU *)h;
+  for (volumetype i = 0; i < f->_nBranchesUsed; i++) tree[i] = f->_tree[i];
+}
+
+/* Brick contents of leaves [0, n): 512 SDF, 512 weights, 512x3 colour each. */
+void ref_bricks(void *h, long long n, float *dist, float *wgt, uint16_t *col) {
+  FusionMipMapCPU *f = (FusionMipMapCPU *)h;
+  for (long long i = 0; i < n * 512; i++) {
+    dist[i] = f->_distance[i];
+    wgt[i] = f->_weights[i];
+    if (f->_color) {
+      col[3 * i + 0] = f->_color[i].x;
+      col[3 * i + 1] = f->_color[i].y;
+      col[3 * i + 2] = f->_color[i].z;
+    }
+  }
+}
+
+/* Mesh cells: 14 int32 each: type, ox, oy, oz, size, has_mesh, lastLeaf[8]. */
+long long ref_cells(void *h, int32_t *out) {
+  FusionMipMapCPU *f = (FusionMipMapCPU *)h;
+  long long n = (long long)f->_meshCells.size();
+  if (!out) return n;
+  for (long long i = 0; i < n; i++) {
+    const MeshCell &c = f->_meshCells[i];
+    int32_t *o = out + 14 * i;
+    o[0] = c.type;
+    o[1] = c.ox;
+    o[2] = c.oy;
+    o[3] = c.oz;
+    o[4] = c.size;
+    o[5] = c.meshinterleaved ? (int32_t)c.meshinterleaved->vertices.size() : -1;
+    for (int k = 0; k < 8; k++) o[6 + k] = (int32_t)c.lastLeaf[k];
+  }
+  return n;
+}
+
+/* Queue every mesh cell whose leaves are all allocated, so that the next
+ * updateMeshes() re-meshes the whole map from the current voxel data. */
+void ref_queue_all_cells(void *h) {
+  FusionMipMapCPU *f = (FusionMipMapCPU *)h;
+  f->_meshCellIsQueuedNext->resize(f->_meshCells.size(), false);
+  for (size_t j = 0; j < f->_meshCells.size(); j++) {
+    if ((*f->_meshCellIsQueuedNext)[j]) continue;
+    const MeshCell &c = f->_meshCells[j];
+    int need = c.type == 0 ? 1 : c.type <= 3 ? 2 : c.type <= 6 ? 4 : 8;
+    if (c.type > 7) continue;
+    bool ok = true;
+    for (int k = 0; k < need; k++) ok = ok && c.lastLeaf[k] < BRANCHINIT;
+    if (!ok) continue;
+    f->_meshCellQueueNext.push_back(j);
+    (*f->_meshCellIsQueuedNext)[j] = true;
+  }
+}
+
+/* Mesh of one cell as last meshed: counts, then copies (vertex order as the
+ * reference's per-cell mesh). */
+long long ref_cell_mesh(void *h, long long cell, float *xyz, uint8_t *rgb, uint32_t *faces, long long *nf) {
+  FusionMipMapCPU *f = (FusionMipMapCPU *)h;
+  const MeshCell &c = f->_meshCells[cell];
+  if (!c.meshinterleaved) {
+    if (nf) *nf = 0;
+    return 0;
+  }
+  const MeshInterleaved &m = *c.meshinterleaved;
+  if (nf) *nf = (long long)m.faces.size() / 3;
+  if (xyz) {
+    for (size_t i = 0; i < m.vertices.size(); i++) {
+      xyz[3 * i + 0] = m.vertices[i].x;
+      xyz[3 * i + 1] = m.vertices[i].y;
+      xyz[3 * i + 2] = m.vertices[i].z;
+      rgb[3 * i + 0] = m.colors[i].r;
+      rgb[3 * i + 1] = m.colors[i].g;
+      rgb[3 * i + 2] = m.colors[i].b;
+    }
+    for (size_t i = 0; i < m.faces.size(); i++) faces[i] = m.faces[i];
+  }
+  return (long long)m.vertices.size();
+}
+
+/* The marching-cubes triangle table as the reference holds it: per case, up to
+ * 5 triangles of (edge-slot offsets), -1 terminated.  Used only to generate a
+ * golden fixture that pins the product's own table. */
+void ref_mc_offset_table(int32_t *out /* 256 x 16 */) {
+  MarchingCubesIndexed mc(8, 8);
+  for (int i = 0; i < 256; i++)
+    for (int j = 0; j < 16; j++) out[16 * i + j] = mc.offsetTable[i][j];
+}
+
+}  // extern "C"
