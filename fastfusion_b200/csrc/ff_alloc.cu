@@ -1,0 +1,503 @@
+// Brick allocation: per-pixel projection, row/column de-duplication and the
+// parallel octree insert that replaces the reference's sequential traversal
+// (transformLoopSimPrecalculatedNeg_subtree, traversal_wrapper_functions.cpp:576-694,
+//  queryPointDepthSingle_func_subtree / addLeaf, traversal_functions.cpp:185-211, 308-395).
+//
+// The reference walks pixels in raster order; three of its outcomes depend on
+// that order and are reproduced exactly here:
+//   * which pixels are processed (the de-duplication recurrence) -- computed
+//     by an exact tiled fixed-point solve of the recurrence;
+//   * leaf indices -- assigned in order of the first pixel that created each
+//     leaf (sort of pending leaves by first pixel);
+//   * parent leaves -- the finest ancestor leaf that existed when the leaf was
+//     created, i.e. the finest ancestor with a smaller index.
+// Branch indices are assigned in arrival order; they are internal.
+#include <cub/cub.cuh>
+
+#include "ff_kernels.h"
+
+namespace ffb {
+
+__device__ __forceinline__ uint32_t ld_volatile(const uint32_t *p) { return *(volatile const uint32_t *)p; }
+
+// ---------------------------------------------------------------- bbox ----
+
+// computeBoundingboxIntCPU(ushort), geometryfusion_mipmap_cpu.cpp:1270-1303,
+// round-to-nearest float arithmetic in the reference's operation order.
+__global__ void k_first_bbox(const uint16_t *depth, int W, int H, CamF p, float scaling, float maxcam, int bw,
+                             Counters *cnt) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int mn[3] = {1000000, 1000000, 1000000}, mx[3] = {-1000000, -1000000, -1000000};
+  if (i < W * H) {
+    int x = i % W, y = i / W;
+    float pz = __fmul_rn((float)depth[i], scaling);
+    if (pz > 0.0f && pz < maxcam) {
+      float px = __fmul_rn(__fdiv_rn(__fsub_rn((float)x, p.cx), p.fx), pz);
+      float py = __fmul_rn(__fdiv_rn(__fsub_rn((float)y, p.cy), p.fy), pz);
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        float s = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(p.r[3 * r], px), __fmul_rn(p.r[3 * r + 1], py)),
+                                      __fmul_rn(p.r[3 * r + 2], pz)),
+                            p.t[r]);
+        int v = __float2int_rz(s);
+        mn[r] = v - bw;
+        mx[r] = v + bw;
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    int a = mn[r], b = mx[r];
+    for (int o = 16; o > 0; o >>= 1) {
+      a = min(a, __shfl_xor_sync(0xffffffffu, a, o));
+      b = max(b, __shfl_xor_sync(0xffffffffu, b, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(&cnt->box_min[r], a);
+      atomicMax(&cnt->box_max[r], b);
+    }
+  }
+}
+
+void launch_first_bbox(const uint16_t *depth, int W, int H, const CamF &p, float scaling, float maxcam, int bw,
+                       Counters *cnt, cudaStream_t s) {
+  int n = W * H;
+  k_first_bbox<<<(n + 255) / 256, 256, 0, s>>>(depth, W, H, p, scaling, maxcam, bw, cnt);
+}
+
+// ------------------------------------------------------------- project ----
+
+// Per pixel: v = (int)(((qx[x] + qy[y]) * depth) * scaling + t), the
+// reference's key arithmetic (traversal_wrapper_functions.cpp:613-630,
+// addMap's qxp/qyp, geometryfusion_mipmap_cpu.cpp:1807-1822), in
+// round-to-nearest with no fused multiply-add.  w = target brick edge in
+// voxels, floor(max(depth,1)*8) (leafScaleFunc, inline_functions.hpp:128-145),
+// or -1 for invalid depth.
+__global__ void k_project(const uint16_t *depth, int W, int H, const float *pxp, const float *pyp, CamF p,
+                          float scaling, float maxcam, int4 *vox) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= W * H) return;
+  int x = i % W, y = i / W;
+  float d = (float)depth[i];
+  float px = pxp[x], py = pyp[y];
+  int v[3];
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    float qx = __fmul_rn(p.r[3 * r + 0], px);
+    float qy = __fadd_rn(__fmul_rn(p.r[3 * r + 1], py), p.r[3 * r + 2]);
+    float s = __fadd_rn(__fmul_rn(__fmul_rn(__fadd_rn(qx, qy), d), scaling), p.t[r]);
+    v[r] = __float2int_rz(s);
+  }
+  float ds = __fmul_rn(d, scaling);
+  int target = -1;
+  if (ds > 0.0f && ds < maxcam) {
+    float f = ds < 1.0f ? 1.0f : ds;
+    target = (int)(uint16_t)floorf(__fmul_rn(f, 8.0f));
+  }
+  vox[i] = make_int4(v[0], v[1], v[2], target);
+}
+
+void launch_project(const uint16_t *depth, int W, int H, const float *pxp, const float *pyp, const CamF &p,
+                    float scaling, float maxcam, int4 *vox, cudaStream_t s) {
+  int n = W * H;
+  k_project<<<(n + 255) / 256, 256, 0, s>>>(depth, W, H, pxp, pyp, p, scaling, maxcam, vox);
+}
+
+// ------------------------------------------------------------- dedupe -----
+//
+// The reference processes pixel (x,y) iff its depth is valid and its brick
+// key k = v & -8 differs from s(x,y-1) and from s(x-1,y), where
+// s = k if processed and -1 otherwise (traversal_wrapper_functions.cpp:636-639,
+// 688-690).  This is a recurrence over the two predecessors only, so it has a
+// unique solution.  Each warp solves one 32x32 tile exactly, given the state
+// of the column to its left and the row above it: rows top to bottom, and
+// within a row the left-to-right dependency p(x) = a(x) && !(p(x-1) && k(x)==k(x-1))
+// as an inclusive warp scan over the composition of maps {0,1}->{0,1}.
+// Tiles exchange boundary states and repeat until no boundary changes; a
+// chain of dependencies crosses at most tilesX+tilesY tiles, which bounds the
+// number of rounds.
+
+struct TileSt {
+  int kx, ky, kz, p;
+};
+
+__device__ __forceinline__ uint32_t compose(uint32_t g, uint32_t f) {
+  // maps encoded as (bit0 = f(0), bit1 = f(1)); returns g o f
+  uint32_t h0 = (g >> (f & 1u)) & 1u;
+  uint32_t h1 = (g >> ((f >> 1) & 1u)) & 1u;
+  return h0 | (h1 << 1);
+}
+
+__device__ void grid_barrier(uint32_t *bar, uint32_t nblocks, Counters *cnt) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile uint32_t *gen = bar + 1;
+    uint32_t g = *gen;
+    __threadfence();
+    if (atomicAdd(bar, 1u) == nblocks - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      int spins = 0;
+      while (*gen == g) {
+        if (++spins > SPIN_LIMIT) {
+          atomicOr(&cnt->error, ERR_SPIN_TIMEOUT);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+__global__ void k_dedupe(const int4 *__restrict__ vox, int W, int H, int tilesX, int tilesY, int4 *bnd,
+                         uint8_t *processed, Counters *cnt, uint32_t *bar) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int ntiles = tilesX * tilesY;
+  // boundary buffers: [2][ntiles][32] right-column states and [2][ntiles][32] bottom-row states
+  int4 *right[2] = {bnd, bnd + (size_t)ntiles * 32};
+  int4 *bottom[2] = {bnd + (size_t)2 * ntiles * 32, bnd + (size_t)3 * ntiles * 32};
+  const int max_rounds = tilesX + tilesY + 1;
+  int round = 0;
+  for (; round < max_rounds; round++) {
+    const int in = round & 1, out = in ^ 1;
+    int changed = 0;
+    for (int tile = warp; tile < ntiles; tile += nwarps) {
+      const int tx = tile % tilesX, ty = tile / tilesX;
+      const int x = tx * 32 + lane;
+      int4 above = make_int4(0, 0, 0, 0);
+      if (ty > 0) above = bottom[in][(size_t)(tile - tilesX) * 32 + lane];
+      int4 prev_bottom = bottom[in][(size_t)tile * 32 + lane];
+      int ak = above.x, bk = above.y, ck = above.z, ap = above.w;
+      for (int r = 0; r < 32; r++) {
+        const int y = ty * 32 + r;
+        if (y >= H) break;
+        int4 v = make_int4(0, 0, 0, -1);
+        if (x < W) v = vox[(size_t)y * W + x];
+        const int valid = v.w >= 0;
+        const int k0 = v.x & -8, k1 = v.y & -8, k2 = v.z & -8;
+        const int a = valid && !(ap && k0 == ak && k1 == bk && k2 == ck);
+        int4 left = make_int4(0, 0, 0, 0);
+        if (lane == 0 && tx > 0) left = right[in][(size_t)(tile - 1) * 32 + r];
+        const int p0 = __shfl_up_sync(0xffffffffu, k0, 1);
+        const int p1 = __shfl_up_sync(0xffffffffu, k1, 1);
+        const int p2 = __shfl_up_sync(0xffffffffu, k2, 1);
+        uint32_t T;
+        if (lane == 0) {
+          const int e = left.w && left.x == k0 && left.y == k1 && left.z == k2;
+          const uint32_t c = (a && !e) ? 1u : 0u;
+          T = c | (c << 1);
+        } else {
+          const int e = (p0 == k0 && p1 == k1 && p2 == k2);
+          T = !a ? 0u : (e ? 1u /* NOT: f(0)=1,f(1)=0 */ : 3u);
+        }
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          uint32_t other = __shfl_up_sync(0xffffffffu, T, o);
+          if (lane >= o) T = compose(T, other);
+        }
+        const int p = T & 1u;
+        ak = k0;
+        bk = k1;
+        ck = k2;
+        ap = p;
+        if (x < W) processed[(size_t)y * W + x] = (uint8_t)p;
+        if (lane == 31) {
+          int4 nv = make_int4(k0, k1, k2, p);
+          int4 ov = right[in][(size_t)tile * 32 + r];
+          if (ov.x != nv.x || ov.y != nv.y || ov.z != nv.z || ov.w != nv.w) changed = 1;
+          right[out][(size_t)tile * 32 + r] = nv;
+        }
+      }
+      int4 nb = make_int4(ak, bk, ck, ap);
+      if (nb.x != prev_bottom.x || nb.y != prev_bottom.y || nb.z != prev_bottom.z || nb.w != prev_bottom.w)
+        changed = 1;
+      bottom[out][(size_t)tile * 32 + lane] = nb;
+    }
+    changed = __any_sync(0xffffffffu, changed);
+    if (changed && lane == 0) atomicAdd(&cnt->dedupe_changed, 1u);
+    grid_barrier(bar, gridDim.x, cnt);
+    const uint32_t any = *(volatile uint32_t *)&cnt->dedupe_changed;
+    grid_barrier(bar, gridDim.x, cnt);
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt->dedupe_changed = 0;
+    grid_barrier(bar, gridDim.x, cnt);
+    if (!any) break;
+    if (*(volatile uint32_t *)&cnt->error & ERR_SPIN_TIMEOUT) break;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    cnt->dedupe_iters = round + 1;
+    if (round >= max_rounds) atomicOr(&cnt->error, ERR_DEDUPE_NOT_CONVERGED);
+  }
+}
+
+cudaError_t launch_dedupe(const int4 *vox, int W, int H, int4 *bnd, uint8_t *processed, Counters *cnt,
+                          uint32_t *barrier, int device, cudaStream_t s) {
+  int tilesX = (W + 31) / 32, tilesY = (H + 31) / 32;
+  int ntiles = tilesX * tilesY;
+  const int threads = 256;
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dedupe, threads, 0);
+  if (e != cudaSuccess) return e;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  int want = (ntiles + threads / 32 - 1) / (threads / 32);
+  int maxb = per_sm * sms;
+  int blocks = want < maxb ? want : maxb;
+  if (blocks < 1) blocks = 1;
+  void *args[] = {(void *)&vox, (void *)&W, (void *)&H, (void *)&tilesX, (void *)&tilesY, (void *)&bnd,
+                  (void *)&processed, (void *)&cnt, (void *)&barrier};
+  return cudaLaunchCooperativeKernel((const void *)k_dedupe, dim3(blocks), dim3(threads), args, 0, s);
+}
+
+// -------------------------------------------------------------- insert ----
+
+__device__ __forceinline__ void queue_leaf(uint32_t leaf, uint32_t frame, uint32_t *stamp, uint32_t *queue,
+                                           Counters *cnt) {
+  if (atomicExch(&stamp[leaf], frame) != frame) {
+    uint32_t q = atomicAdd(&cnt->queued, 1u);
+    queue[q] = leaf;
+  }
+}
+
+// Wait until another thread finished allocating tree[ptr]; bounded.
+__device__ __forceinline__ uint32_t wait_unlocked(uint32_t *tree, uint32_t ptr, uint32_t cur, Counters *cnt,
+                                                  bool *ok) {
+  int spins = 0;
+  while (cur == LOCKED) {
+    if (++spins > SPIN_LIMIT) {
+      atomicOr(&cnt->error, ERR_SPIN_TIMEOUT);
+      *ok = false;
+      return cur;
+    }
+    __nanosleep(20);
+    cur = ld_volatile(tree + ptr);
+  }
+  return cur;
+}
+
+// One processed pixel: bounding-box growth, then (inside the volume) the
+// descent of queryPointDepthSingle_func_subtree: queue the existing coarser
+// leaves on the path, allocate missing branches, claim the final leaf.
+__global__ void k_insert(const int4 *__restrict__ vox, const uint8_t *__restrict__ processed, int npix, uint32_t n,
+                         int bw, uint32_t *tree, uint32_t leaves_max, uint32_t branches_max, uint32_t frame,
+                         uint32_t *stamp, uint32_t *queue, PendingLeaf *pend, uint32_t pend_cap, Counters *cnt) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool act = i < npix && processed[i];
+  unsigned m = __ballot_sync(0xffffffffu, act);
+  if (!act) return;
+  if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&cnt->processed, __popc(m));
+  int4 v = vox[i];
+  int vv[3] = {v.x, v.y, v.z};
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    int lo = vv[r] - bw, hi = vv[r] + bw;
+    if (lo < 0) atomicMin(&cnt->box_min[r], lo);
+    if (hi >= (int)n) atomicMax(&cnt->box_max[r], hi);
+  }
+  if (!(v.x >= 0 && (uint16_t)v.x < n && v.y >= 0 && (uint16_t)v.y < n && v.z >= 0 && (uint16_t)v.z < n)) return;
+  const uint32_t x = (uint16_t)v.x, y = (uint16_t)v.y, z = (uint16_t)v.z;
+  const uint32_t target = (uint32_t)v.w;
+  uint32_t ox = 0, oy = 0, oz = 0;
+  uint32_t half = (uint16_t)(n >> 1);
+  uint32_t branch = 0;
+  bool ok = true;
+  while ((half >> 1) >= target) {
+    uint32_t co = (x >= ox + half) * 1u + (y >= oy + half) * 2u + (z >= oz + half) * 4u;
+    uint32_t ptr = branch + co + 8;
+    uint32_t leaf = ld_volatile(tree + ptr - 8);
+    if (leaf < leaves_max) queue_leaf(leaf, frame, stamp, queue, cnt);
+    uint32_t child = ld_volatile(tree + ptr);
+    if (child == BRANCHINIT) {
+      uint32_t old = atomicCAS(tree + ptr, BRANCHINIT, LOCKED);
+      if (old == BRANCHINIT) {
+        uint32_t nb = atomicAdd(&cnt->branches_used, 16u);
+        if (nb + 16 > branches_max) {
+          atomicOr(&cnt->error, ERR_BRANCH_OVERFLOW);
+          atomicExch(tree + ptr, BRANCHINIT);
+          return;
+        }
+        __threadfence();
+        atomicExch(tree + ptr, nb);
+        child = nb;
+      } else {
+        child = old;
+      }
+    }
+    child = wait_unlocked(tree, ptr, child, cnt, &ok);
+    if (!ok || child == BRANCHINIT) return;
+    ox += half * ((co & 1) != 0);
+    oy += half * ((co & 2) != 0);
+    oz += half * ((co & 4) != 0);
+    branch = child;
+    half >>= 1;
+  }
+  uint32_t co = (x >= ox + half) * 1u + (y >= oy + half) * 2u + (z >= oz + half) * 4u;
+  uint32_t ptr = branch + co;
+  uint32_t cur = ld_volatile(tree + ptr);
+  if (cur == BRANCHINIT) {
+    uint32_t old = atomicCAS(tree + ptr, BRANCHINIT, LOCKED);
+    if (old == BRANCHINIT) {
+      uint32_t rec = atomicAdd(&cnt->pending, 1u);
+      if (rec >= pend_cap) {
+        atomicOr(&cnt->error, ERR_PENDING_OVERFLOW);
+        atomicExch(tree + ptr, BRANCHINIT);
+        return;
+      }
+      PendingLeaf pl;
+      pl.slot = ptr;
+      pl.first_pixel = (uint32_t)i;
+      pl.pos = make_ushort4((uint16_t)(ox + half * ((co & 1) != 0)), (uint16_t)(oy + half * ((co & 2) != 0)),
+                            (uint16_t)(oz + half * ((co & 4) != 0)), (uint16_t)(half / BL));
+      pend[rec] = pl;
+      __threadfence();
+      atomicExch(tree + ptr, PENDING + rec);
+      return;
+    }
+    cur = old;
+  }
+  cur = wait_unlocked(tree, ptr, cur, cnt, &ok);
+  if (!ok) return;
+  if (cur >= PENDING && cur < PENDING + pend_cap) {
+    atomicMin(&pend[cur - PENDING].first_pixel, (uint32_t)i);
+  } else if (cur < leaves_max) {
+    queue_leaf(cur, frame, stamp, queue, cnt);
+  }
+}
+
+void launch_insert(const int4 *vox, const uint8_t *processed, int W, int H, uint32_t n, int bw, uint32_t *tree,
+                   uint32_t leaves_max, uint32_t branches_max, uint32_t frame, uint32_t *stamp, uint32_t *queue,
+                   PendingLeaf *pend, uint32_t pend_cap, Counters *cnt, cudaStream_t s) {
+  int npix = W * H;
+  k_insert<<<(npix + 255) / 256, 256, 0, s>>>(vox, processed, npix, n, bw, tree, leaves_max, branches_max, frame,
+                                              stamp, queue, pend, pend_cap, cnt);
+}
+
+// ------------------------------------------------- pending leaf order -----
+
+__global__ void k_pending_keys(const PendingLeaf *pend, int npend, uint32_t *keys, uint32_t *vals) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npend) return;
+  keys[i] = pend[i].first_pixel;
+  vals[i] = (uint32_t)i;
+}
+
+size_t pending_sort_bytes(int n) {
+  size_t bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, (uint32_t *)nullptr, (uint32_t *)nullptr, (uint32_t *)nullptr,
+                                  (uint32_t *)nullptr, n);
+  return bytes;
+}
+
+cudaError_t sort_pending(const PendingLeaf *pend, int npend, uint32_t *keys_in, uint32_t *vals_in, uint32_t *keys_out,
+                         uint32_t *vals_out, void *tmp, size_t tmp_bytes, int end_bit, cudaStream_t s) {
+  if (npend <= 0) return cudaSuccess;
+  k_pending_keys<<<(npend + 255) / 256, 256, 0, s>>>(pend, npend, keys_in, vals_in);
+  return cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys_in, keys_out, vals_in, vals_out, npend, 0, end_bit,
+                                         s);
+}
+
+// Leaf index = leaves_before + rank of first pixel; indices past the pool are
+// stored in the tree but get no leaf record, like addLeaf's overflow
+// (traversal_functions.cpp:201-210).
+__global__ void k_finalize(const PendingLeaf *pend, const uint32_t *order, int npend, uint32_t leaves_before,
+                           uint32_t leaves_max, uint32_t *tree, ushort4 *leaf, uint32_t frame, uint32_t *stamp,
+                           uint32_t *queue, Counters *cnt) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= npend) return;
+  const PendingLeaf p = pend[order[j]];
+  const uint32_t idx = leaves_before + (uint32_t)j;
+  tree[p.slot] = idx;
+  if (idx < leaves_max) {
+    leaf[idx] = p.pos;
+    queue_leaf(idx, frame, stamp, queue, cnt);
+  }
+}
+
+void launch_finalize(const PendingLeaf *pend, const uint32_t *order, int npend, uint32_t leaves_before,
+                     uint32_t leaves_max, uint32_t *tree, ushort4 *leaf, uint32_t frame, uint32_t *stamp,
+                     uint32_t *queue, Counters *cnt, cudaStream_t s) {
+  if (npend <= 0) return;
+  k_finalize<<<(npend + 255) / 256, 256, 0, s>>>(pend, order, npend, leaves_before, leaves_max, tree, leaf, frame,
+                                                 stamp, queue, cnt);
+}
+
+// parent = finest ancestor leaf that existed when this leaf was created: the
+// reference records the last leaf met on the descent (`pl`,
+// traversal_functions.cpp:327-333, 376-379); leaves of this frame exist in
+// index order, so that is the finest ancestor with a smaller index.
+__global__ void k_parents(int npend, uint32_t leaves_before, uint32_t leaves_max, const uint32_t *tree, uint32_t n,
+                          const ushort4 *leaf, uint32_t *parent) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= npend) return;
+  const uint32_t idx = leaves_before + (uint32_t)j;
+  if (idx >= leaves_max) return;
+  const ushort4 p = leaf[idx];
+  const uint32_t edge = (uint32_t)p.w * BL;
+  uint32_t ox = 0, oy = 0, oz = 0, half = n >> 1, branch = 0, pl = BRANCHINIT;
+  while (half > edge) {
+    uint32_t co = (p.x >= ox + half) * 1u + (p.y >= oy + half) * 2u + (p.z >= oz + half) * 4u;
+    uint32_t l = tree[branch + co];
+    if (l < leaves_max && l < idx) pl = l;
+    branch = tree[branch + co + 8];
+    if (branch >= PENDING) break;  // no child branch (cannot happen for a placed leaf)
+    ox += half * ((co & 1) != 0);
+    oy += half * ((co & 2) != 0);
+    oz += half * ((co & 4) != 0);
+    half >>= 1;
+  }
+  parent[idx] = pl;
+}
+
+void launch_parents(int npend, uint32_t leaves_before, uint32_t leaves_max, const uint32_t *tree, uint32_t n,
+                    const ushort4 *leaf, uint32_t *parent, cudaStream_t s) {
+  if (npend <= 0) return;
+  k_parents<<<(npend + 255) / 256, 256, 0, s>>>(npend, leaves_before, leaves_max, tree, n, leaf, parent);
+}
+
+// ---------------------------------------------------------------- grow ----
+
+__global__ void k_shift_branches(uint32_t *tree, uint32_t used, uint32_t shift) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= used) return;
+  if ((i & 15) >= 8 && tree[i] != BRANCHINIT) tree[i] += shift;
+}
+
+void launch_shift_branches(uint32_t *tree, uint32_t used, uint32_t shift, cudaStream_t s) {
+  if (!used) return;
+  k_shift_branches<<<(used + 255) / 256, 256, 0, s>>>(tree, used, shift);
+}
+
+__global__ void k_shift_leaves(ushort4 *leaf, uint32_t n, ushort3 add) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  ushort4 p = leaf[i];
+  p.x = (uint16_t)(p.x + add.x);
+  p.y = (uint16_t)(p.y + add.y);
+  p.z = (uint16_t)(p.z + add.z);
+  leaf[i] = p;
+}
+
+void launch_shift_leaves(ushort4 *leaf, uint32_t n, ushort3 add, cudaStream_t s) {
+  if (!n) return;
+  k_shift_leaves<<<(n + 255) / 256, 256, 0, s>>>(leaf, n, add);
+}
+
+__global__ void k_fill(uint32_t *p, size_t n, uint32_t v) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (; i < n; i += stride) p[i] = v;
+}
+
+void launch_fill(uint32_t *p, size_t n, uint32_t v, cudaStream_t s) {
+  if (!n) return;
+  size_t blocks = (n + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  k_fill<<<(unsigned)blocks, 256, 0, s>>>(p, n, v);
+}
+
+}  // namespace ffb

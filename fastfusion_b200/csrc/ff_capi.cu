@@ -1,0 +1,713 @@
+// C ABI of the B200 fusion path (include/fastfusion_b200.h): host-side
+// orchestration of one map (the reference's FusionMipMapCPU).
+//
+// Per frame (ff_add_map_u16): camera parameters in FP64 rounded once to FP32
+// like the reference's camPamsFloat; on the first frame the integer bounding
+// box sizes the volume; then project -> de-duplicate -> insert on the device,
+// one read-back of the counters, leaf-index assignment, grow() when the
+// frame's points left the volume, and the voxel update of every queued brick.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/fastfusion_b200.h"
+#include "ff_kernels.h"
+#include "ff_mesh.h"
+
+using namespace ffb;
+
+struct ff_handle {
+  ff_config cfg;
+  std::string err;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+
+  // map state on the device
+  uint32_t *d_tree = nullptr;
+  ushort4 *d_leaf = nullptr;
+  uint32_t *d_parent = nullptr;
+  float *d_sdf = nullptr, *d_wgt = nullptr;
+  __half *d_sdf16 = nullptr, *d_wgt16 = nullptr;
+  uint16_t *d_col = nullptr;
+  uint32_t *d_stamp = nullptr;
+  uint32_t *d_queue = nullptr;
+  Counters *d_cnt = nullptr;
+  Counters *h_cnt = nullptr;  // pinned
+  uint32_t *d_barrier = nullptr;
+
+  // per-image scratch
+  int img_w = 0, img_h = 0, cap_pix = 0;
+  uint16_t *d_depth = nullptr;
+  uint8_t *d_bgr = nullptr;
+  float *d_pxp = nullptr, *d_pyp = nullptr;
+  int4 *d_vox = nullptr;
+  uint8_t *d_proc = nullptr;
+  int4 *d_bnd = nullptr;
+  size_t bnd_elems = 0;
+  PendingLeaf *d_pend = nullptr;
+  uint32_t *d_keys = nullptr;  // 4 x cap_pix
+  void *d_sort_tmp = nullptr;
+  size_t sort_tmp_bytes = 0;
+
+  // host mirror of the scalar state
+  uint32_t n = 0;
+  float offset[3] = {0, 0, 0};
+  uint32_t leaves_used = 0, branches_used = 16;
+  uint32_t frames = 0, queued = 0, grows = 0, processed = 0, new_leaves = 0;
+  bool meshing_ok = true;
+  uint16_t bandwidth = 0;
+
+  MeshState mesh;
+};
+
+static thread_local std::string g_create_error;
+
+#define CK(call)                                                                      \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess) {                                                          \
+      h->err = std::string(#call) + ": " + cudaGetErrorString(e_);                    \
+      return FF_ERR_CUDA;                                                             \
+    }                                                                                 \
+  } while (0)
+
+static ff_status set_err(ff_handle *h, ff_status s, const std::string &m) {
+  if (h) h->err = m;
+  return s;
+}
+
+// ----------------------------------------------------------- camera math --
+
+// p: world -> voxel grid (reference geometryfusion_mipmap_cpu.cpp:1617-1625)
+static CamF cam_world_to_grid(const ff_handle *h, const double *K, const double *R, const double *t) {
+  CamF p;
+  for (int i = 0; i < 9; i++) p.r[i] = (float)(R[i] / (double)h->cfg.scale);
+  for (int i = 0; i < 3; i++) p.t[i] = (float)((t[i] - (double)h->offset[i]) / (double)h->cfg.scale);
+  p.fx = (float)K[0];
+  p.fy = (float)K[1];
+  p.cx = (float)K[2];
+  p.cy = (float)K[3];
+  return p;
+}
+
+// pInv: voxel grid (offset folded in) -> camera, from the extrinsic inverse
+// [R^T | -R^T t] (geometryfusion_mipmap_cpu.cpp:1771-1793, camerautils.cpp:153-161);
+// FP64 throughout, one rounding to FP32 per parameter.
+static CamF cam_grid_to_camera(const ff_handle *h, const double *K, const double *R, const double *t) {
+  CamF q;
+  double r2[9], t2[3];
+  for (int r = 0; r < 3; r++) {
+    for (int c = 0; c < 3; c++) r2[r * 3 + c] = R[c * 3 + r];
+    double s = R[0 * 3 + r] * t[0] + R[1 * 3 + r] * t[1];
+    s = s + R[2 * 3 + r] * t[2];
+    t2[r] = -s;
+  }
+  for (int i = 0; i < 9; i++) q.r[i] = (float)r2[i];
+  for (int r = 0; r < 3; r++) {
+    double v = r2[r * 3 + 0] * (double)h->offset[0] + r2[r * 3 + 1] * (double)h->offset[1];
+    v = v + r2[r * 3 + 2] * (double)h->offset[2];
+    v = v + t2[r];
+    q.t[r] = (float)v;
+  }
+  q.fx = (float)K[0];
+  q.fy = (float)K[1];
+  q.cx = (float)K[2];
+  q.cy = (float)K[3];
+  return q;
+}
+
+// setInitialVolume (geometryfusion_mipmap_cpu.cpp:1186-1233)
+static bool set_initial_volume(ff_handle *h, const int *mn, const int *mx) {
+  if (mn[0] >= mx[0] || mn[1] >= mx[1] || mn[2] >= mx[2]) return false;
+  uint16_t hi[3];
+  for (int r = 0; r < 3; r++) hi[r] = (uint16_t)(mx[r] - mn[r]);
+  uint16_t high = std::max(std::max(hi[0], hi[1]), hi[2]);
+  uint16_t n;
+  for (n = 2 * BL; n <= high; n = (uint16_t)(n * 2)) {
+  }
+  h->n = n;
+  for (int r = 0; r < 3; r++) h->offset[r] = (float)(mn[r] - ((int)n - (int)hi[r]) / 2) * h->cfg.scale;
+  return true;
+}
+
+static uint16_t highest_pow2(uint16_t in) {
+  uint16_t r = 1;
+  while (r * 2 <= in) r = (uint16_t)(r * 2);
+  return r;
+}
+
+// grow() (geometryfusion_mipmap_cpu.cpp:3071-3319): add levels above the
+// root so that the frame's bounding box fits; the old tree becomes a child.
+static ff_status grow(ff_handle *h, const int *box_min, const int *box_max) {
+  int n = h->n;
+  uint16_t pl_[3], mi_[3];
+  for (int r = 0; r < 3; r++) {
+    pl_[r] = (uint16_t)((box_max[r] >= n) * ((box_max[r] - n) / n + 1));
+    mi_[r] = (uint16_t)((box_min[r] < 0) * ((-box_min[r]) / n + 1));
+  }
+  for (int r = 0; r < 3; r++) {
+    uint16_t cut = pl_[r] & mi_[r];
+    if (cut) {
+      if (mi_[r] > pl_[r])
+        mi_[r] = (uint16_t)(2 * highest_pow2(mi_[r]) + (mi_[r] & (uint16_t)~cut));
+      else
+        pl_[r] = (uint16_t)(2 * highest_pow2(pl_[r]) + (pl_[r] & (uint16_t)~cut));
+    }
+  }
+  uint16_t levels = highest_pow2(mi_[0]);
+  for (int r = 0; r < 3; r++) {
+    levels = std::max(levels, highest_pow2(pl_[r]));
+    levels = std::max(levels, highest_pow2(mi_[r]));
+  }
+  uint32_t shift = (uint32_t)levels * 16;
+  if (shift > h->cfg.branches_max - h->branches_used) return FF_OK;  // the reference's split() is a stub
+  cudaStream_t s = h->stream;
+  launch_shift_branches(h->d_tree, h->branches_used, shift, s);
+  // move the tree up by `shift` entries (through the free tail of the array)
+  uint32_t used = h->branches_used;
+  if (used + shift + used <= h->cfg.branches_max) {
+    CK(cudaMemcpyAsync(h->d_tree + used + shift, h->d_tree, sizeof(uint32_t) * used, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(h->d_tree + shift, h->d_tree + used + shift, sizeof(uint32_t) * used,
+                       cudaMemcpyDeviceToDevice, s));
+    launch_fill(h->d_tree + used + shift, used, BRANCHINIT, s);
+  } else {
+    uint32_t *tmp = nullptr;
+    CK(cudaMallocAsync((void **)&tmp, sizeof(uint32_t) * used, s));
+    CK(cudaMemcpyAsync(tmp, h->d_tree, sizeof(uint32_t) * used, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(h->d_tree + shift, tmp, sizeof(uint32_t) * used, cudaMemcpyDeviceToDevice, s));
+    CK(cudaFreeAsync(tmp, s));
+  }
+  launch_fill(h->d_tree, shift, BRANCHINIT, s);
+  h->branches_used += shift;
+  uint16_t add[3] = {0, 0, 0};
+  std::vector<std::pair<uint32_t, uint32_t>> links;
+  uint32_t index = (uint32_t)(levels - 1) * 16;
+  for (uint16_t level = 0; level < levels; level++) {
+    unsigned dec = 1u << level;
+    uint32_t co = 0;
+    for (int r = 0; r < 3; r++) {
+      if ((mi_[r] & dec) || (!(pl_[r] & dec) && (pl_[r] > mi_[r]))) {
+        add[r] = (uint16_t)(add[r] + h->n);
+        co += 1u << r;
+      }
+    }
+    links.push_back({index + co + 8, index + 16});
+    h->n = (uint16_t)(h->n * 2);
+    index -= 16;
+  }
+  for (auto &l : links) CK(cudaMemcpyAsync(h->d_tree + l.first, &l.second, 4, cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));  // `links` lives on this stack frame
+  for (int r = 0; r < 3; r++) h->offset[r] -= (float)add[r] * h->cfg.scale;
+  uint32_t nl = std::min(h->leaves_used, h->cfg.leaves_max);
+  launch_shift_leaves(h->d_leaf, nl, make_ushort3(add[0], add[1], add[2]), s);
+  h->grows++;
+  return FF_OK;
+}
+
+// ------------------------------------------------------------- buffers ----
+
+template <typename T>
+static cudaError_t alloc(T **p, size_t count) {
+  return cudaMalloc((void **)p, sizeof(T) * std::max<size_t>(count, 1));
+}
+
+static ff_status ensure_image(ff_handle *h, int W, int H) {
+  int npix = W * H;
+  if (npix > h->cap_pix) {
+    cudaFree(h->d_depth);
+    cudaFree(h->d_bgr);
+    cudaFree(h->d_vox);
+    cudaFree(h->d_proc);
+    cudaFree(h->d_pend);
+    cudaFree(h->d_keys);
+    cudaFree(h->d_sort_tmp);
+    h->d_depth = nullptr;
+    CK(alloc(&h->d_depth, npix));
+    CK(alloc(&h->d_bgr, (size_t)npix * 3));
+    CK(alloc(&h->d_vox, npix));
+    CK(alloc(&h->d_proc, npix));
+    CK(alloc(&h->d_pend, npix));
+    CK(alloc(&h->d_keys, (size_t)npix * 4));
+    h->sort_tmp_bytes = pending_sort_bytes(npix);
+    CK(cudaMalloc(&h->d_sort_tmp, std::max<size_t>(h->sort_tmp_bytes, 16)));
+    h->cap_pix = npix;
+  }
+  size_t tiles = (size_t)((W + 31) / 32) * ((H + 31) / 32);
+  if (tiles * 32 * 4 > h->bnd_elems) {
+    cudaFree(h->d_bnd);
+    h->bnd_elems = tiles * 32 * 4;
+    CK(alloc(&h->d_bnd, h->bnd_elems));
+  }
+  return FF_OK;
+}
+
+// ------------------------------------------------------------------ API ---
+
+extern "C" {
+
+const char *ff_version(void) { return "fastfusion_b200 0.1 (sm_100a)"; }
+
+const char *ff_last_error(const ff_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+ff_status ff_create(const ff_config *cfg, ff_handle **out) {
+  if (!cfg || !out) {
+    g_create_error = "ff_create: NULL argument";
+    return FF_ERR_BAD_ARG;
+  }
+  *out = nullptr;
+  if (!(cfg->scale > 0.0f) || !(cfg->threshold > 0.0f)) {
+    g_create_error = "ff_create: scale and threshold must be > 0";
+    return FF_ERR_BAD_ARG;
+  }
+  if (cfg->storage != FF_STORAGE_FP32 && cfg->storage != FF_STORAGE_FP16) {
+    g_create_error = "ff_create: unknown storage";
+    return FF_ERR_BAD_ARG;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+    cudaGetLastError();
+    g_create_error = "ff_create: no CUDA device";
+    return FF_ERR_NO_DEVICE;
+  }
+  if (cfg->device < 0 || cfg->device >= ndev) {
+    g_create_error = "ff_create: bad device ordinal";
+    return FF_ERR_BAD_ARG;
+  }
+  ff_handle *h = new ff_handle();
+  h->cfg = *cfg;
+  if (cudaSetDevice(cfg->device) != cudaSuccess) {
+    g_create_error = "ff_create: cudaSetDevice failed";
+    delete h;
+    return FF_ERR_CUDA;
+  }
+  size_t brick_bytes = 512 * (cfg->storage == FF_STORAGE_FP16 ? 4 : 8) + 512 * 6;
+  if (h->cfg.leaves_max == 0) {
+    uint64_t pool = cfg->pool_bytes ? cfg->pool_bytes : 2000000000ull;
+    h->cfg.leaves_max = (uint32_t)std::min<uint64_t>(pool / (brick_bytes + 24), 0x3FFFFFFFull);
+  }
+  if (h->cfg.branches_max == 0)
+    h->cfg.branches_max = (uint32_t)std::min<uint64_t>((uint64_t)h->cfg.leaves_max * 4 + (1u << 20), 0xBFFFFFF0ull);
+  h->cfg.branches_max &= ~15u;
+  // _bandwidth(_distanceThreshold / _scale * BANDWIDTHFACTOR)
+  h->bandwidth = (uint16_t)(double)(cfg->threshold / cfg->scale * 1.0);
+  ff_status st = FF_OK;
+  auto fail = [&](ff_status s, const char *m) {
+    g_create_error = std::string("ff_create: ") + m + ": " + cudaGetErrorString(cudaGetLastError());
+    st = s;
+  };
+  do {
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { fail(FF_ERR_CUDA, "stream"); break; }
+    h->own_stream = true;
+    size_t L = h->cfg.leaves_max;
+    if (alloc(&h->d_tree, h->cfg.branches_max) != cudaSuccess) { fail(FF_ERR_OOM_POOL, "tree"); break; }
+    if (alloc(&h->d_leaf, L) != cudaSuccess || alloc(&h->d_parent, L) != cudaSuccess ||
+        alloc(&h->d_stamp, L) != cudaSuccess || alloc(&h->d_queue, L) != cudaSuccess) {
+      fail(FF_ERR_OOM_POOL, "leaf table");
+      break;
+    }
+    if (cfg->storage == FF_STORAGE_FP16) {
+      if (alloc(&h->d_sdf16, L * 512) != cudaSuccess || alloc(&h->d_wgt16, L * 512) != cudaSuccess) {
+        fail(FF_ERR_OOM_POOL, "brick pool");
+        break;
+      }
+    } else {
+      if (alloc(&h->d_sdf, L * 512) != cudaSuccess || alloc(&h->d_wgt, L * 512) != cudaSuccess) {
+        fail(FF_ERR_OOM_POOL, "brick pool");
+        break;
+      }
+    }
+    if (alloc(&h->d_col, L * 1536) != cudaSuccess) { fail(FF_ERR_OOM_POOL, "colour pool"); break; }
+    if (alloc(&h->d_cnt, 1) != cudaSuccess || alloc(&h->d_barrier, 4) != cudaSuccess) { fail(FF_ERR_CUDA, "counters"); break; }
+    if (cudaMallocHost((void **)&h->h_cnt, sizeof(Counters)) != cudaSuccess) { fail(FF_ERR_CUDA, "pinned"); break; }
+    launch_fill(h->d_tree, h->cfg.branches_max, BRANCHINIT, h->stream);
+    cudaMemsetAsync(h->d_stamp, 0, sizeof(uint32_t) * L, h->stream);
+    cudaMemsetAsync(h->d_parent, 0xFF, sizeof(uint32_t) * L, h->stream);
+    cudaMemsetAsync(h->d_leaf, 0, sizeof(ushort4) * L, h->stream);
+    if (h->d_sdf) {
+      cudaMemsetAsync(h->d_sdf, 0, sizeof(float) * L * 512, h->stream);
+      cudaMemsetAsync(h->d_wgt, 0, sizeof(float) * L * 512, h->stream);
+    } else {
+      cudaMemsetAsync(h->d_sdf16, 0, sizeof(__half) * L * 512, h->stream);
+      cudaMemsetAsync(h->d_wgt16, 0, sizeof(__half) * L * 512, h->stream);
+    }
+    cudaMemsetAsync(h->d_col, 0, sizeof(uint16_t) * L * 1536, h->stream);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) { fail(FF_ERR_CUDA, "init"); break; }
+  } while (0);
+  if (st != FF_OK) {
+    ff_destroy(h);
+    return st;
+  }
+  *out = h;
+  return FF_OK;
+}
+
+ff_status ff_destroy(ff_handle *h) {
+  if (!h) return FF_ERR_BAD_ARG;
+  cudaSetDevice(h->cfg.device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  mesh_free(h->mesh);
+  void *ptrs[] = {h->d_tree, h->d_leaf, h->d_parent, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
+                  h->d_stamp, h->d_queue, h->d_cnt, h->d_barrier, h->d_depth, h->d_bgr, h->d_pxp, h->d_pyp,
+                  h->d_vox, h->d_proc, h->d_bnd, h->d_pend, h->d_keys, h->d_sort_tmp};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (h->h_cnt) cudaFreeHost(h->h_cnt);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return FF_OK;
+}
+
+ff_status ff_set_stream(ff_handle *h, void *cuda_stream) {
+  if (!h) return FF_ERR_BAD_ARG;
+  cudaSetDevice(h->cfg.device);
+  cudaStreamSynchronize(h->stream);
+  if (h->own_stream) cudaStreamDestroy(h->stream);
+  if (cuda_stream) {
+    h->stream = (cudaStream_t)cuda_stream;
+    h->own_stream = false;
+  } else {
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+  }
+  return FF_OK;
+}
+
+// The frame, with depth/bgr already on the device (h->d_depth/h->d_bgr or caller memory).
+static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uint8_t *d_bgr, int W, int H,
+                                const double *K, const double *R, const double *t, float scaling, float maxcam,
+                                int32_t *queued) {
+  cudaStream_t s = h->stream;
+  CamF p = cam_world_to_grid(h, K, R, t);
+  Counters &hc = *h->h_cnt;
+
+  if (!h->n) {
+    // first frame: integer bounding box of the valid points (computeBoundingboxIntCPU)
+    memset(&hc, 0, sizeof(Counters));
+    for (int r = 0; r < 3; r++) {
+      hc.box_min[r] = 1000000;
+      hc.box_max[r] = -1000000;
+    }
+    CK(cudaMemcpyAsync(h->d_cnt, &hc, sizeof(Counters), cudaMemcpyHostToDevice, s));
+    launch_first_bbox(d_depth, W, H, p, scaling, maxcam, h->bandwidth, h->d_cnt, s);
+    CK(cudaMemcpyAsync(&hc, h->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    set_initial_volume(h, hc.box_min, hc.box_max);
+    p = cam_world_to_grid(h, K, R, t);
+  }
+  if (h->img_w != W || h->img_h != H) {
+    // _pxp/_pyp, recomputed on a size change only (geometryfusion_mipmap_cpu.cpp:1745-1764)
+    std::vector<float> px(W), py(H);
+    for (int x = 0; x < W; x++) px[x] = ((float)x - p.cx) / p.fx;
+    for (int y = 0; y < H; y++) py[y] = ((float)y - p.cy) / p.fy;
+    cudaFree(h->d_pxp);
+    cudaFree(h->d_pyp);
+    h->d_pxp = h->d_pyp = nullptr;
+    CK(alloc(&h->d_pxp, W));
+    CK(alloc(&h->d_pyp, H));
+    CK(cudaMemcpyAsync(h->d_pxp, px.data(), sizeof(float) * W, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->d_pyp, py.data(), sizeof(float) * H, cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    h->img_w = W;
+    h->img_h = H;
+  }
+  const uint32_t frame = h->frames + 1;
+  memset(&hc, 0, sizeof(Counters));
+  hc.branches_used = h->branches_used;
+  for (int r = 0; r < 3; r++) {
+    hc.box_min[r] = 0;
+    hc.box_max[r] = (int)h->n - 1;
+  }
+  CK(cudaMemcpyAsync(h->d_cnt, &hc, sizeof(Counters), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(h->d_barrier, 0, 16, s));
+  CK(cudaMemsetAsync(h->d_bnd, 0, sizeof(int4) * h->bnd_elems, s));
+  // voxel -> camera parameters are taken before any grow() of this frame,
+  // as in the reference (pInv is built before the traversal)
+  CamF q = cam_grid_to_camera(h, K, R, t);
+
+  launch_project(d_depth, W, H, h->d_pxp, h->d_pyp, p, scaling, maxcam, h->d_vox, s);
+  CK(launch_dedupe(h->d_vox, W, H, h->d_bnd, h->d_proc, h->d_cnt, h->d_barrier, h->cfg.device, s));
+  launch_insert(h->d_vox, h->d_proc, W, H, h->n, h->bandwidth, h->d_tree, h->cfg.leaves_max, h->cfg.branches_max,
+                frame, h->d_stamp, h->d_queue, h->d_pend, (uint32_t)(W * H), h->d_cnt, s);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(&hc, h->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (hc.error & (ERR_SPIN_TIMEOUT | ERR_DEDUPE_NOT_CONVERGED))
+    return set_err(h, FF_ERR_TIMEOUT, "a bounded device-side wait gave up during allocation");
+  if (hc.error & ERR_PENDING_OVERFLOW) return set_err(h, FF_ERR_STATE, "pending-leaf buffer overflow");
+  if (hc.error & ERR_BRANCH_OVERFLOW) h->meshing_ok = false;
+  h->branches_used = std::min(hc.branches_used, h->cfg.branches_max);
+  h->processed = hc.processed;
+  const uint32_t npend = hc.pending;
+  const uint32_t leaves_before = h->leaves_used;
+  const uint32_t existing_queued = hc.queued;
+  if (npend) {
+    uint32_t *k_in = h->d_keys, *v_in = h->d_keys + h->cap_pix, *k_out = h->d_keys + 2 * h->cap_pix,
+             *v_out = h->d_keys + 3 * h->cap_pix;
+    int end_bit = 1;
+    while ((1u << end_bit) < (uint32_t)(W * H)) end_bit++;
+    CK(sort_pending(h->d_pend, (int)npend, k_in, v_in, k_out, v_out, h->d_sort_tmp, h->sort_tmp_bytes, end_bit, s));
+    launch_finalize(h->d_pend, v_out, (int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->d_leaf, frame,
+                    h->d_stamp, h->d_queue, h->d_cnt, s);
+    launch_parents((int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->n, h->d_leaf, h->d_parent, s);
+    h->leaves_used += npend;
+  }
+  uint32_t new_queued = 0;
+  if (leaves_before < h->cfg.leaves_max) new_queued = std::min(npend, h->cfg.leaves_max - leaves_before);
+  h->new_leaves = npend;
+  const uint32_t nq = existing_queued + new_queued;
+  if (h->leaves_used < h->cfg.leaves_max && h->branches_used < h->cfg.branches_max &&
+      (hc.box_min[0] < 0 || hc.box_min[1] < 0 || hc.box_min[2] < 0 || hc.box_max[0] >= (int)h->n ||
+       hc.box_max[1] >= (int)h->n || hc.box_max[2] >= (int)h->n)) {
+    ff_status st = grow(h, hc.box_min, hc.box_max);
+    if (st != FF_OK) return st;
+  }
+  launch_fuse(h->d_queue, (int)nq, h->d_leaf, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
+              h->cfg.storage, h->cfg.leaves_max, d_depth, d_bgr, W, H, q, h->cfg.scale, h->cfg.threshold, scaling,
+              maxcam, s);
+  CK(cudaGetLastError());
+  if (h->leaves_used > h->cfg.leaves_max) h->meshing_ok = false;
+  h->queued = nq;
+  h->frames++;
+  mesh_note_frame(h->mesh);
+  if (queued) *queued = (int32_t)nq;
+  return FF_OK;
+}
+
+ff_status ff_add_map_u16(ff_handle *h, const uint16_t *depth, int width, int height, size_t depth_pitch,
+                         const uint8_t *bgr, size_t bgr_pitch, const double K[4], const double R[9],
+                         const double t[3], float scaling, float maxcam, int32_t *queued) {
+  if (!h) return FF_ERR_BAD_ARG;
+  if (!depth || !bgr || !K || !R || !t || width <= 0 || height <= 0)
+    return set_err(h, FF_ERR_BAD_ARG, "ff_add_map_u16: NULL pointer or empty image");
+  CK(cudaSetDevice(h->cfg.device));
+  ff_status st = ensure_image(h, width, height);
+  if (st != FF_OK) return st;
+  if (!depth_pitch) depth_pitch = sizeof(uint16_t) * width;
+  if (!bgr_pitch) bgr_pitch = 3 * (size_t)width;
+  CK(cudaMemcpy2DAsync(h->d_depth, sizeof(uint16_t) * width, depth, depth_pitch, sizeof(uint16_t) * width, height,
+                       cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpy2DAsync(h->d_bgr, 3 * (size_t)width, bgr, bgr_pitch, 3 * (size_t)width, height,
+                       cudaMemcpyHostToDevice, h->stream));
+  return add_map_device(h, h->d_depth, h->d_bgr, width, height, K, R, t, scaling, maxcam, queued);
+}
+
+ff_status ff_add_map_u16_device(ff_handle *h, const uint16_t *d_depth, const uint8_t *d_bgr, int width, int height,
+                                const double K[4], const double R[9], const double t[3], float scaling,
+                                float maxcam, int32_t *queued) {
+  if (!h) return FF_ERR_BAD_ARG;
+  if (!d_depth || !d_bgr || !K || !R || !t || width <= 0 || height <= 0)
+    return set_err(h, FF_ERR_BAD_ARG, "ff_add_map_u16_device: NULL pointer or empty image");
+  CK(cudaSetDevice(h->cfg.device));
+  ff_status st = ensure_image(h, width, height);
+  if (st != FF_OK) return st;
+  return add_map_device(h, d_depth, d_bgr, width, height, K, R, t, scaling, maxcam, queued);
+}
+
+ff_status ff_get_stats(ff_handle *h, ff_stats *o) {
+  if (!h || !o) return FF_ERR_BAD_ARG;
+  memset(o, 0, sizeof(*o));
+  o->n = h->n;
+  for (int r = 0; r < 3; r++) o->offset[r] = h->offset[r];
+  o->leaves_used = h->leaves_used;
+  o->leaves_max = h->cfg.leaves_max;
+  o->branches_used = h->branches_used;
+  o->branches_max = h->cfg.branches_max;
+  o->queued = h->queued;
+  o->frames = h->frames;
+  o->meshing_ok = h->meshing_ok ? 1 : 0;
+  o->grows = h->grows;
+  o->mesh_vertices = h->mesh.n_vertices;
+  o->mesh_faces = h->mesh.n_faces;
+  o->mesh_cells = h->mesh.n_cells;
+  o->mesh_cells_dirty = h->mesh.n_dirty;
+  o->processed_pixels = h->processed;
+  o->new_leaves = h->new_leaves;
+  return FF_OK;
+}
+
+ff_status ff_get_leaves(ff_handle *h, uint16_t *pos, uint16_t *scale, uint32_t *parent) {
+  if (!h || !pos || !scale || !parent) return FF_ERR_BAD_ARG;
+  CK(cudaSetDevice(h->cfg.device));
+  uint32_t n = std::min(h->leaves_used, h->cfg.leaves_max);
+  std::vector<ushort4> tmp(n);
+  if (n) {
+    CK(cudaMemcpyAsync(tmp.data(), h->d_leaf, sizeof(ushort4) * n, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(parent, h->d_parent, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, h->stream));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  for (uint32_t i = 0; i < n; i++) {
+    pos[3 * i] = tmp[i].x;
+    pos[3 * i + 1] = tmp[i].y;
+    pos[3 * i + 2] = tmp[i].z;
+    scale[i] = tmp[i].w;
+  }
+  return FF_OK;
+}
+
+ff_status ff_get_queue(ff_handle *h, uint32_t *leaves) {
+  if (!h || !leaves) return FF_ERR_BAD_ARG;
+  CK(cudaSetDevice(h->cfg.device));
+  if (h->queued) CK(cudaMemcpyAsync(leaves, h->d_queue, sizeof(uint32_t) * h->queued, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return FF_OK;
+}
+
+ff_status ff_get_tree(ff_handle *h, uint32_t *tree) {
+  if (!h || !tree) return FF_ERR_BAD_ARG;
+  CK(cudaSetDevice(h->cfg.device));
+  CK(cudaMemcpyAsync(tree, h->d_tree, sizeof(uint32_t) * h->branches_used, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return FF_OK;
+}
+
+ff_status ff_get_bricks(ff_handle *h, uint32_t first, uint32_t count, float *sdf, float *weight, uint16_t *rgb) {
+  if (!h || !sdf || !weight || !rgb) return FF_ERR_BAD_ARG;
+  if ((uint64_t)first + count > h->cfg.leaves_max) return set_err(h, FF_ERR_BAD_ARG, "ff_get_bricks: range");
+  CK(cudaSetDevice(h->cfg.device));
+  size_t nv = (size_t)count * 512;
+  if (h->cfg.storage == FF_STORAGE_FP16) {
+    std::vector<__half> a(nv), b(nv);
+    CK(cudaMemcpyAsync(a.data(), h->d_sdf16 + (size_t)first * 512, 2 * nv, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(b.data(), h->d_wgt16 + (size_t)first * 512, 2 * nv, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (size_t i = 0; i < nv; i++) {
+      sdf[i] = __half2float(a[i]);
+      weight[i] = __half2float(b[i]);
+    }
+  } else {
+    CK(cudaMemcpyAsync(sdf, h->d_sdf + (size_t)first * 512, 4 * nv, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(weight, h->d_wgt + (size_t)first * 512, 4 * nv, cudaMemcpyDeviceToHost, h->stream));
+  }
+  std::vector<uint16_t> planes(nv * 3);
+  CK(cudaMemcpyAsync(planes.data(), h->d_col + (size_t)first * 1536, 2 * nv * 3, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (size_t b = 0; b < count; b++)
+    for (int c = 0; c < 3; c++)
+      for (int v = 0; v < 512; v++) rgb[(b * 512 + v) * 3 + c] = planes[b * 1536 + c * 512 + v];
+  return FF_OK;
+}
+
+ff_status ff_set_bricks(ff_handle *h, uint32_t first, uint32_t count, const float *sdf, const float *weight,
+                        const uint16_t *rgb) {
+  if (!h || !sdf || !weight || !rgb) return FF_ERR_BAD_ARG;
+  if ((uint64_t)first + count > h->cfg.leaves_max) return set_err(h, FF_ERR_BAD_ARG, "ff_set_bricks: range");
+  CK(cudaSetDevice(h->cfg.device));
+  size_t nv = (size_t)count * 512;
+  if (h->cfg.storage == FF_STORAGE_FP16) {
+    std::vector<__half> a(nv), b(nv);
+    for (size_t i = 0; i < nv; i++) {
+      a[i] = __float2half_rn(sdf[i]);
+      b[i] = __float2half_rn(weight[i]);
+    }
+    CK(cudaMemcpyAsync(h->d_sdf16 + (size_t)first * 512, a.data(), 2 * nv, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_wgt16 + (size_t)first * 512, b.data(), 2 * nv, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  } else {
+    CK(cudaMemcpyAsync(h->d_sdf + (size_t)first * 512, sdf, 4 * nv, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_wgt + (size_t)first * 512, weight, 4 * nv, cudaMemcpyHostToDevice, h->stream));
+  }
+  std::vector<uint16_t> planes(nv * 3);
+  for (size_t b = 0; b < count; b++)
+    for (int c = 0; c < 3; c++)
+      for (int v = 0; v < 512; v++) planes[b * 1536 + c * 512 + v] = rgb[(b * 512 + v) * 3 + c];
+  CK(cudaMemcpyAsync(h->d_col + (size_t)first * 1536, planes.data(), 2 * nv * 3, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  mesh_invalidate(h->mesh);
+  return FF_OK;
+}
+
+ff_status ff_set_state(ff_handle *h, uint32_t n, const float offset[3], const uint32_t *tree, uint32_t branches_used,
+                       const uint16_t *pos, const uint16_t *scale, const uint32_t *parent, uint32_t leaves_used,
+                       const float *sdf, const float *weight, const uint16_t *rgb) {
+  if (!h || !offset || !tree || !pos || !scale || !parent) return FF_ERR_BAD_ARG;
+  if (branches_used > h->cfg.branches_max || leaves_used > h->cfg.leaves_max || (branches_used & 15))
+    return set_err(h, FF_ERR_BAD_ARG, "ff_set_state: state larger than this map's capacity");
+  CK(cudaSetDevice(h->cfg.device));
+  launch_fill(h->d_tree, h->cfg.branches_max, BRANCHINIT, h->stream);
+  CK(cudaMemcpyAsync(h->d_tree, tree, sizeof(uint32_t) * branches_used, cudaMemcpyHostToDevice, h->stream));
+  std::vector<ushort4> lp(leaves_used);
+  for (uint32_t i = 0; i < leaves_used; i++) lp[i] = make_ushort4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], scale[i]);
+  if (leaves_used) {
+    CK(cudaMemcpyAsync(h->d_leaf, lp.data(), sizeof(ushort4) * leaves_used, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_parent, parent, sizeof(uint32_t) * leaves_used, cudaMemcpyHostToDevice, h->stream));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  h->n = n;
+  for (int r = 0; r < 3; r++) h->offset[r] = offset[r];
+  h->branches_used = branches_used;
+  h->leaves_used = leaves_used;
+  if (sdf && weight && rgb && leaves_used) {
+    ff_status st = ff_set_bricks(h, 0, leaves_used, sdf, weight, rgb);
+    if (st != FF_OK) return st;
+  }
+  mesh_invalidate(h->mesh);
+  return FF_OK;
+}
+
+// ------------------------------------------------------------- meshing ----
+
+ff_status ff_update_meshes(ff_handle *h, int *updated) {
+  if (!h) return FF_ERR_BAD_ARG;
+  CK(cudaSetDevice(h->cfg.device));
+  if (!h->meshing_ok || !h->n) {
+    if (updated) *updated = 1;
+    return FF_OK;
+  }
+  MeshInputs in;
+  in.tree = h->d_tree;
+  in.branches_used = h->branches_used;
+  in.leaf = h->d_leaf;
+  in.parent = h->d_parent;
+  in.sdf = h->d_sdf;
+  in.wgt = h->d_wgt;
+  in.sdf16 = h->d_sdf16;
+  in.wgt16 = h->d_wgt16;
+  in.col = h->d_col;
+  in.storage = h->cfg.storage;
+  in.leaves_used = std::min(h->leaves_used, h->cfg.leaves_max);
+  in.leaves_max = h->cfg.leaves_max;
+  in.stamp = h->d_stamp;
+  in.frame = h->frames;
+  in.n = h->n;
+  for (int r = 0; r < 3; r++) in.offset[r] = h->offset[r];
+  in.scale = h->cfg.scale;
+  in.cnt = h->d_cnt;
+  in.h_cnt = h->h_cnt;
+  std::string err;
+  int rc = mesh_update(h->mesh, in, h->stream, err);
+  if (rc != 0) return set_err(h, (ff_status)rc, err);
+  if (updated) *updated = 1;
+  return FF_OK;
+}
+
+ff_status ff_get_mesh_counts(ff_handle *h, uint64_t *nv, uint64_t *nf) {
+  if (!h || !nv || !nf) return FF_ERR_BAD_ARG;
+  *nv = h->mesh.n_vertices;
+  *nf = h->mesh.n_faces;
+  return FF_OK;
+}
+
+ff_status ff_get_mesh(ff_handle *h, float *xyz, uint8_t *rgb, uint32_t *faces) {
+  if (!h) return FF_ERR_BAD_ARG;
+  if ((h->mesh.n_vertices && (!xyz || !rgb)) || (h->mesh.n_faces && !faces))
+    return set_err(h, FF_ERR_BAD_ARG, "ff_get_mesh: NULL output buffer");
+  CK(cudaSetDevice(h->cfg.device));
+  std::string err;
+  int rc = mesh_copy_out(h->mesh, xyz, rgb, faces, h->stream, err);
+  if (rc != 0) return set_err(h, (ff_status)rc, err);
+  return FF_OK;
+}
+
+ff_status ff_get_mesh_device(ff_handle *h, const float **xyz, const uint8_t **rgb, const uint32_t **faces) {
+  if (!h || !xyz || !rgb || !faces) return FF_ERR_BAD_ARG;
+  *xyz = h->mesh.d_xyz;
+  *rgb = h->mesh.d_rgb;
+  *faces = h->mesh.d_faces;
+  return FF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,64 @@
+// Shared device-side definitions of the B200 fusion path.
+//
+// Data layout in HBM (one map):
+//   tree      uint32[branches_max]  16 entries per branch: [0..7] leaf index of
+//                                   each octant, [8..15] child branch -- the
+//                                   reference's _tree (traversal_functions.cpp:308-395)
+//   leaf_pos  ushort4[leaves_max]   x, y, z (voxels), scale (voxel spacing)
+//   leaf_par  uint32[leaves_max]    parent leaf (_leafParent)
+//   sdf, wgt  float[leaves_max][512]   (or __half with FP16 storage)
+//   col       uint16[leaves_max][3][512]  R, G, B planes per brick (x256)
+// Voxel v of a brick is (z*8 + y)*8 + x, the reference's order.
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ffb {
+
+constexpr uint32_t BRANCHINIT = 0xFFFFFFFEu;  // reference definitions.h:128
+constexpr uint32_t LOCKED = 0xFFFFFFFDu;      // slot being allocated (device-internal)
+constexpr uint32_t PENDING = 0xC0000000u;     // slot holds a leaf created this frame: PENDING + record
+constexpr int BL = 8;                         // BRICKLENGTH
+constexpr float DIST_W_EPS = 0.005f;          // DISTANCEWEIGHTEPSILON
+constexpr float WEIGHT_FACTOR = 3.0f;
+constexpr float COLOR_MUL = 256.0f;
+constexpr int SPIN_LIMIT = 1 << 22;           // bound of every device-side wait
+
+// error bits written by kernels into Counters::error
+enum : uint32_t {
+  ERR_BRANCH_OVERFLOW = 1u,
+  ERR_SPIN_TIMEOUT = 2u,
+  ERR_PENDING_OVERFLOW = 4u,
+  ERR_CELL_OVERFLOW = 8u,
+  ERR_MESH_OVERFLOW = 16u,
+  ERR_DEDUPE_NOT_CONVERGED = 32u,
+};
+
+// Per-map counters kept in device memory; read back once per frame.
+struct Counters {
+  uint32_t branches_used;
+  uint32_t pending;        // new leaves claimed this frame
+  uint32_t queued;         // bricks queued this frame (existing + new)
+  uint32_t processed;      // pixels that passed de-duplication
+  int32_t box_min[3];
+  int32_t box_max[3];
+  uint32_t error;
+  uint32_t dedupe_changed;
+  uint32_t dedupe_iters;
+  uint32_t n_cells;
+  uint32_t n_work;
+  uint32_t n_work_next;
+  uint64_t mesh_v;
+  uint64_t mesh_f;
+  uint32_t pad[4];
+};
+
+// Float camera parameters (the reference's camPamsFloat, definitions.h:71-88).
+struct CamF {
+  float r[9];
+  float t[3];
+  float fx, fy, cx, cy;
+};
+
+}  // namespace ffb

@@ -1,0 +1,53 @@
+// Incremental marching cubes over the dual cells of the brick octree
+// (internal interface of the library).
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "ff_common.cuh"
+
+namespace ffb {
+
+struct MeshInputs {
+  const uint32_t *tree;
+  uint32_t branches_used;
+  const ushort4 *leaf;
+  const uint32_t *parent;
+  const float *sdf, *wgt;
+  const __half *sdf16, *wgt16;
+  const uint16_t *col;
+  int storage;
+  uint32_t leaves_used, leaves_max;
+  const uint32_t *stamp;  // frame of the last update of each brick
+  uint32_t frame;
+  uint32_t n;
+  float offset[3];
+  float scale;
+  Counters *cnt;
+  Counters *h_cnt;
+};
+
+struct MeshState {
+  // output of the last update
+  float *d_xyz = nullptr;
+  uint8_t *d_rgb = nullptr;
+  uint32_t *d_faces = nullptr;
+  uint64_t n_vertices = 0, n_faces = 0;
+  uint64_t cap_vertices = 0, cap_faces = 0;
+  uint64_t n_cells = 0, n_dirty = 0;
+  uint32_t last_frame = 0;
+  bool valid = false;
+  void *impl = nullptr;  // buffers private to ff_mesh.cu
+};
+
+// returns 0 or an ff_status value
+int mesh_update(MeshState &m, const MeshInputs &in, cudaStream_t s, std::string &err);
+int mesh_copy_out(MeshState &m, float *xyz, uint8_t *rgb, uint32_t *faces, cudaStream_t s, std::string &err);
+void mesh_free(MeshState &m);
+void mesh_invalidate(MeshState &m);
+void mesh_note_frame(MeshState &m);
+
+}  // namespace ffb

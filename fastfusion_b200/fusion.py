@@ -1,0 +1,276 @@
+"""Python host API of the B200 fusion path, mirroring the reference's C++
+interface (tum-vision/fastfusion src/fusion/geometryfusion_mipmap_cpu.hpp):
+
+    fusion = FusionMipMapCPU(0, 0, 0, scale, distanceThreshold, 0, True)
+    n = fusion.addMap(depth_u16, CameraInfo(K, R, t), bgr_u8, 1/5000., maxcam)
+    fusion.updateMeshes()
+    mesh = fusion.getMeshInterleavedMarchingCubes()
+
+Every call goes through the C ABI of libfastfusion_b200.so
+(include/fastfusion_b200.h); there is no CPU fallback.  Loading fails loudly
+when the library or a CUDA device is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libfastfusion_b200.so")
+
+FF_OK = 0
+_STATUS = {0: "FF_OK", 1: "FF_ERR_BAD_ARG", 2: "FF_ERR_CUDA", 3: "FF_ERR_OOM_POOL", 4: "FF_ERR_OOM_MESH",
+           5: "FF_ERR_TIMEOUT", 6: "FF_ERR_STATE", 7: "FF_ERR_NO_DEVICE"}
+STORAGE = {"fp32": 0, "fp16": 1}
+BRANCHINIT = 0xFFFFFFFE
+
+
+class FFError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{_STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class ff_config(ctypes.Structure):
+    _fields_ = [("scale", ctypes.c_float), ("threshold", ctypes.c_float), ("color", ctypes.c_int),
+                ("leaves_max", ctypes.c_uint32), ("branches_max", ctypes.c_uint32),
+                ("pool_bytes", ctypes.c_uint64), ("device", ctypes.c_int), ("storage", ctypes.c_int)]
+
+
+class ff_stats(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint32), ("offset", ctypes.c_float * 3), ("leaves_used", ctypes.c_uint32),
+                ("leaves_max", ctypes.c_uint32), ("branches_used", ctypes.c_uint32),
+                ("branches_max", ctypes.c_uint32), ("queued", ctypes.c_uint32), ("frames", ctypes.c_uint32),
+                ("meshing_ok", ctypes.c_uint32), ("grows", ctypes.c_uint32), ("mesh_vertices", ctypes.c_uint64),
+                ("mesh_faces", ctypes.c_uint64), ("mesh_cells", ctypes.c_uint64),
+                ("mesh_cells_dirty", ctypes.c_uint64), ("processed_pixels", ctypes.c_uint32),
+                ("new_leaves", ctypes.c_uint32)]
+
+
+# Every entry point of include/fastfusion_b200.h with its ctypes signature.
+_vp, _i32, _u32, _u64, _f32, _sz = (ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint64,
+                                    ctypes.c_float, ctypes.c_size_t)
+SIGNATURES = {
+    "ff_create": (_i32, [ctypes.POINTER(ff_config), ctypes.POINTER(_vp)]),
+    "ff_destroy": (_i32, [_vp]),
+    "ff_set_stream": (_i32, [_vp, _vp]),
+    "ff_add_map_u16": (_i32, [_vp, _vp, _i32, _i32, _sz, _vp, _sz, _vp, _vp, _vp, _f32, _f32, _vp]),
+    "ff_add_map_u16_device": (_i32, [_vp, _vp, _vp, _i32, _i32, _vp, _vp, _vp, _f32, _f32, _vp]),
+    "ff_update_meshes": (_i32, [_vp, _vp]),
+    "ff_get_mesh_counts": (_i32, [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
+    "ff_get_mesh": (_i32, [_vp, _vp, _vp, _vp]),
+    "ff_get_mesh_device": (_i32, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
+    "ff_get_stats": (_i32, [_vp, ctypes.POINTER(ff_stats)]),
+    "ff_get_leaves": (_i32, [_vp, _vp, _vp, _vp]),
+    "ff_get_queue": (_i32, [_vp, _vp]),
+    "ff_get_bricks": (_i32, [_vp, _u32, _u32, _vp, _vp, _vp]),
+    "ff_set_bricks": (_i32, [_vp, _u32, _u32, _vp, _vp, _vp]),
+    "ff_get_tree": (_i32, [_vp, _vp]),
+    "ff_set_state": (_i32, [_vp, _u32, _vp, _vp, _u32, _vp, _vp, _vp, _u32, _vp, _vp, _vp]),
+    "ff_last_error": (ctypes.c_char_p, [_vp]),
+    "ff_version": (ctypes.c_char_p, []),
+}
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libfastfusion_b200.so (raises if it is missing: no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise FFError(7, f"{path} is missing; build it with `python -m fastfusion_b200.build`")
+        L = ctypes.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class CameraInfo:
+    """Pinhole intrinsics plus camera-to-world pose, the reference's CameraInfo
+    (src/camerautils/camerautils.hpp:22-56) reduced to what addMap reads."""
+
+    def __init__(self, K, R, t):
+        K = np.asarray(K, dtype=np.float64)
+        if K.shape == (3, 3):
+            K = np.array([K[0, 0], K[1, 1], K[0, 2], K[1, 2]])
+        self.K = np.ascontiguousarray(K, dtype=np.float64).reshape(4)
+        self.R = np.ascontiguousarray(R, dtype=np.float64).reshape(3, 3)
+        self.t = np.ascontiguousarray(t, dtype=np.float64).reshape(3)
+
+    def getIntrinsic(self):
+        fx, fy, cx, cy = self.K
+        return np.array([[fx, 0, cx], [0, fy, cy], [0, 0, 1.0]])
+
+    def getRotation(self):
+        return self.R.copy()
+
+    def getTranslation(self):
+        return self.t.reshape(3, 1).copy()
+
+
+@dataclasses.dataclass
+class MeshInterleaved:
+    """The reference's MeshInterleaved (mesh_interleaved.hpp:35-69): vertices
+    in world metres, one colour per vertex, triangles as vertex indices."""
+    vertices: np.ndarray  # (nv, 3) float32
+    colors: np.ndarray    # (nv, 3) uint8 (r, g, b)
+    faces: np.ndarray     # (nf, 3) uint32
+
+
+class FusionMipMapCPU:
+    """Drop-in for the reference's FusionMipMapCPU on one B200."""
+
+    def __init__(self, offsetX: float = 0.0, offsetY: float = 0.0, offsetZ: float = 0.0, scale: float = 0.005,
+                 distanceThreshold: float = 0.01, n: int = 0, color: bool = True, *, leaves_max: int = 0,
+                 branches_max: int = 0, pool_bytes: int = 0, device: int = 0, storage: str = "fp32"):
+        # The reference ignores the offset and n arguments (its constructor
+        # passes 0,0,0 and n=0 to the base class, geometryfusion_mipmap_cpu.cpp:420-424).
+        self._L = load_library()
+        cfg = ff_config(scale=scale, threshold=distanceThreshold, color=1 if color else 0,
+                        leaves_max=leaves_max, branches_max=branches_max, pool_bytes=pool_bytes,
+                        device=device, storage=STORAGE[storage])
+        h = ctypes.c_void_p()
+        st = self._L.ff_create(ctypes.byref(cfg), ctypes.byref(h))
+        if st != FF_OK:
+            raise FFError(st, self._L.ff_last_error(None).decode())
+        self._h = h
+        self.storage = storage
+
+    # -- lifetime --------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.ff_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int):
+        if st != FF_OK:
+            raise FFError(st, self._L.ff_last_error(self._h).decode())
+
+    # -- the reference's API ----------------------------------------------
+    def addMap(self, depth: np.ndarray, caminfo: CameraInfo, rgb: np.ndarray, scaling: float = 1.0 / 5000.0,
+               maxcamdistance: float = 10.0) -> int:
+        depth = np.ascontiguousarray(depth, dtype=np.uint16)
+        rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
+        if depth.ndim != 2 or rgb.shape != depth.shape + (3,):
+            raise FFError(1, "addMap: depth must be HxW uint16 and rgb HxWx3 uint8")
+        q = ctypes.c_int32()
+        h, w = depth.shape
+        self._check(self._L.ff_add_map_u16(self._h, _p(depth), w, h, 0, _p(rgb), 0, _p(caminfo.K),
+                                           _p(caminfo.R), _p(caminfo.t), ctypes.c_float(scaling),
+                                           ctypes.c_float(maxcamdistance), ctypes.byref(q)))
+        return q.value
+
+    def addMapDevice(self, d_depth: int, d_bgr: int, width: int, height: int, caminfo: CameraInfo,
+                     scaling: float = 1.0 / 5000.0, maxcamdistance: float = 10.0) -> int:
+        """addMap with depth/bgr already in device memory (raw device pointers)."""
+        q = ctypes.c_int32()
+        self._check(self._L.ff_add_map_u16_device(self._h, ctypes.c_void_p(d_depth), ctypes.c_void_p(d_bgr), width,
+                                                  height, _p(caminfo.K), _p(caminfo.R), _p(caminfo.t),
+                                                  ctypes.c_float(scaling), ctypes.c_float(maxcamdistance),
+                                                  ctypes.byref(q)))
+        return q.value
+
+    def updateMeshes(self) -> bool:
+        u = ctypes.c_int()
+        self._check(self._L.ff_update_meshes(self._h, ctypes.byref(u)))
+        return bool(u.value)
+
+    def getMeshInterleavedMarchingCubes(self) -> MeshInterleaved:
+        nv, nf = ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(self._L.ff_get_mesh_counts(self._h, ctypes.byref(nv), ctypes.byref(nf)))
+        xyz = np.zeros((nv.value, 3), np.float32)
+        rgb = np.zeros((nv.value, 3), np.uint8)
+        faces = np.zeros((nf.value, 3), np.uint32)
+        self._check(self._L.ff_get_mesh(self._h, _p(xyz), _p(rgb), _p(faces)))
+        return MeshInterleaved(xyz, rgb, faces)
+
+    def setThreadMeshing(self, threadMeshing: bool):
+        """Meshing runs on the GPU stream; there is no mesher thread."""
+
+    def setIncrementalMeshing(self, incrementalMeshing: bool):
+        """Meshing is always incremental (dirty cells only)."""
+
+    def setDepthChecks(self, depthchecks: int):
+        """A no-op in the reference too (its code is commented out)."""
+
+    def set_stream(self, stream_ptr: int | None):
+        self._check(self._L.ff_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)))
+
+    # -- inspection ---------------------------------------------------------
+    def stats(self) -> dict:
+        s = ff_stats()
+        self._check(self._L.ff_get_stats(self._h, ctypes.byref(s)))
+        d = {f: getattr(s, f) for f, _ in ff_stats._fields_}
+        d["offset"] = np.array(list(s.offset), np.float32)
+        return d
+
+    def leaves(self):
+        st = self.stats()
+        n = min(st["leaves_used"], st["leaves_max"])
+        pos = np.zeros((n, 3), np.uint16)
+        scl = np.zeros(n, np.uint16)
+        par = np.zeros(n, np.uint32)
+        self._check(self._L.ff_get_leaves(self._h, _p(pos), _p(scl), _p(par)))
+        return pos, scl, par
+
+    def queue(self) -> np.ndarray:
+        q = np.zeros(self.stats()["queued"], np.uint32)
+        self._check(self._L.ff_get_queue(self._h, _p(q)))
+        return q
+
+    def tree(self) -> np.ndarray:
+        t = np.zeros(self.stats()["branches_used"], np.uint32)
+        self._check(self._L.ff_get_tree(self._h, _p(t)))
+        return t
+
+    def bricks(self, first: int = 0, count: int | None = None):
+        st = self.stats()
+        if count is None:
+            count = min(st["leaves_used"], st["leaves_max"]) - first
+        d = np.zeros((count, 512), np.float32)
+        w = np.zeros((count, 512), np.float32)
+        c = np.zeros((count, 512, 3), np.uint16)
+        self._check(self._L.ff_get_bricks(self._h, first, count, _p(d), _p(w), _p(c)))
+        return d, w, c
+
+    def set_bricks(self, first: int, d, w, c):
+        d = np.ascontiguousarray(d, np.float32)
+        w = np.ascontiguousarray(w, np.float32)
+        c = np.ascontiguousarray(c, np.uint16)
+        self._check(self._L.ff_set_bricks(self._h, first, d.shape[0], _p(d), _p(w), _p(c)))
+
+    def set_state(self, n: int, offset, tree, pos, scale, parent, sdf=None, weight=None, rgb=None):
+        """Snapshot restore of the whole map."""
+        offset = np.ascontiguousarray(offset, np.float32)
+        tree = np.ascontiguousarray(tree, np.uint32)
+        pos = np.ascontiguousarray(pos, np.uint16)
+        scale = np.ascontiguousarray(scale, np.uint16)
+        parent = np.ascontiguousarray(parent, np.uint32)
+        args = [None, None, None]
+        if sdf is not None:
+            args = [np.ascontiguousarray(sdf, np.float32), np.ascontiguousarray(weight, np.float32),
+                    np.ascontiguousarray(rgb, np.uint16)]
+        ptrs = [_p(a) if a is not None else None for a in args]
+        self._check(self._L.ff_set_state(self._h, n, _p(offset), _p(tree), tree.shape[0], _p(pos), _p(scale),
+                                         _p(parent), pos.shape[0], *ptrs))
+
+
+def version() -> str:
+    return load_library().ff_version().decode()

@@ -1,0 +1,150 @@
+/*
+ * fastfusion_b200 -- C ABI of the B200 depth-fusion + incremental-meshing path.
+ *
+ * One handle is one map: the reference's FusionMipMapCPU object
+ * (tum-vision/fastfusion src/fusion/geometryfusion_mipmap_cpu.hpp:111-534).
+ * Every entry point returns ff_status; ff_last_error() describes the last
+ * failure on a handle.  A handle is used by one host thread at a time; its
+ * device work is ordered on one CUDA stream (ff_set_stream).
+ *
+ * Plain pointers and sizes only: no CUDA, C++ or torch types in signatures.
+ */
+#ifndef FASTFUSION_B200_H
+#define FASTFUSION_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ff_status {
+  FF_OK = 0,
+  FF_ERR_BAD_ARG = 1,   /* NULL handle/pointer, bad size, bad config */
+  FF_ERR_CUDA = 2,      /* a CUDA runtime call failed (message in ff_last_error) */
+  FF_ERR_OOM_POOL = 3,  /* device memory for the brick pool could not be had */
+  FF_ERR_OOM_MESH = 4,  /* mesh output larger than the mesh buffers allow */
+  FF_ERR_TIMEOUT = 5,   /* a bounded device-side wait gave up */
+  FF_ERR_STATE = 6,     /* call not valid in the current state */
+  FF_ERR_NO_DEVICE = 7  /* no CUDA device / library built without one */
+} ff_status;
+
+/* Voxel storage of the brick pool. */
+enum { FF_STORAGE_FP32 = 0, FF_STORAGE_FP16 = 1 };
+
+typedef struct ff_config {
+  float scale;             /* voxel edge in metres (FusionMipMapCPU ctor `scale`) */
+  float threshold;         /* truncation distance in metres (ctor `distanceThreshold`) */
+  int color;               /* fuse colour (ctor `color`); must be 1 like the reference's AVX update */
+  uint32_t leaves_max;     /* brick pool capacity in 8^3 bricks; 0 = derive from pool_bytes */
+  uint32_t branches_max;   /* octree capacity in uint32 entries (16 per branch); 0 = 4 x leaves_max x 16 / 8 */
+  uint64_t pool_bytes;     /* used when leaves_max == 0 */
+  int device;              /* CUDA device ordinal */
+  int storage;             /* FF_STORAGE_FP32 (reference layout) or FF_STORAGE_FP16 */
+} ff_config;
+
+typedef struct ff_handle ff_handle;
+
+/* Counters of the map; field names follow the reference's members. */
+typedef struct ff_stats {
+  uint32_t n;                  /* _n: side of the octree volume in voxels */
+  float offset[3];             /* _offset: world position of voxel (0,0,0), metres */
+  uint32_t leaves_used;        /* _nLeavesUsed (may exceed leaves_max after overflow) */
+  uint32_t leaves_max;         /* _nLeavesTotal */
+  uint32_t branches_used;      /* _nBranchesUsed (entries) */
+  uint32_t branches_max;       /* _nBranchesTotal */
+  uint32_t queued;             /* _nLeavesQueuedSurface of the last frame */
+  uint32_t frames;             /* _framesAdded */
+  uint32_t meshing_ok;         /* _performIncrementalMeshing */
+  uint32_t grows;              /* number of grow() events */
+  uint64_t mesh_vertices;      /* size of the current mesh */
+  uint64_t mesh_faces;
+  uint64_t mesh_cells;         /* mesh cells of the last update */
+  uint64_t mesh_cells_dirty;   /* cells re-meshed by the last update */
+  uint32_t processed_pixels;   /* pixels that passed the row/column de-duplication */
+  uint32_t new_leaves;         /* leaves allocated by the last frame */
+} ff_stats;
+
+/* Create a map.  Replaces `new FusionMipMapCPU(0,0,0,scale,threshold,0,color)`
+ * (geometryfusion_mipmap_cpu.cpp:420-640). */
+ff_status ff_create(const ff_config *cfg, ff_handle **out);
+
+/* Destroy a map and free its device memory (~FusionMipMapCPU). */
+ff_status ff_destroy(ff_handle *h);
+
+/* Order this map's device work on the given cudaStream_t (NULL = the
+ * library's own stream). */
+ff_status ff_set_stream(ff_handle *h, void *cuda_stream);
+
+/* Fuse one frame.  Replaces FusionMipMapCPU::addMap(const cv::Mat &depth
+ * CV_16UC1, CameraInfo, const cv::Mat &rgb CV_8UC3 BGR, float scaling, float
+ * maxcamdistance) (geometryfusion_mipmap_cpu.hpp:122-123, .cpp:1603-2034).
+ * depth/bgr are HOST buffers, borrowed for the call; pitches in bytes
+ * (0 = tightly packed).  K = {fx, fy, cx, cy}; R (row-major) and t are the
+ * camera-to-world pose (CameraInfo rotation/translation).  *queued (may be
+ * NULL) receives addMap's return value, the number of bricks updated. */
+ff_status ff_add_map_u16(ff_handle *h, const uint16_t *depth, int width, int height, size_t depth_pitch,
+                         const uint8_t *bgr, size_t bgr_pitch, const double K[4], const double R[9],
+                         const double t[3], float scaling, float maxcam, int32_t *queued);
+
+/* Same as ff_add_map_u16 with depth/bgr already in device memory (tightly
+ * packed).  No host<->device copy of the images. */
+ff_status ff_add_map_u16_device(ff_handle *h, const uint16_t *d_depth, const uint8_t *d_bgr, int width, int height,
+                                const double K[4], const double R[9], const double t[3], float scaling,
+                                float maxcam, int32_t *queued);
+
+/* Re-mesh the cells touched since the last update and rebuild the
+ * interleaved mesh.  Replaces FusionMipMapCPU::updateMeshes()
+ * (geometryfusion_mipmap_cpu.cpp:2884-2954) with threaded meshing off;
+ * *updated = 1 like its `true` return. */
+ff_status ff_update_meshes(ff_handle *h, int *updated);
+
+/* Size of the mesh of the last update (MeshInterleaved vertices/faces). */
+ff_status ff_get_mesh_counts(ff_handle *h, uint64_t *n_vertices, uint64_t *n_faces);
+
+/* Copy the mesh of the last update to HOST buffers: xyz float[3*nv] (world
+ * metres), rgb uint8[3*nv], faces uint32[3*nf].  Replaces
+ * getMeshInterleavedMarchingCubes() (geometryfusion_mipmap_cpu.cpp:3359-3374). */
+ff_status ff_get_mesh(ff_handle *h, float *xyz, uint8_t *rgb, uint32_t *faces);
+
+/* Device pointers to the same mesh, valid until the next ff_update_meshes. */
+ff_status ff_get_mesh_device(ff_handle *h, const float **xyz, const uint8_t **rgb, const uint32_t **faces);
+
+ff_status ff_get_stats(ff_handle *h, ff_stats *out);
+
+/* Leaf table of leaves [0, min(leaves_used, leaves_max)): position (3 x
+ * uint16 voxels), scale (voxel spacing of the brick) and parent leaf
+ * (0xFFFFFFFE if none) -- the reference's _leafPos/_leafScale/_leafParent. */
+ff_status ff_get_leaves(ff_handle *h, uint16_t *pos, uint16_t *scale, uint32_t *parent);
+
+/* Bricks updated by the last frame (leaf indices, unordered). */
+ff_status ff_get_queue(ff_handle *h, uint32_t *leaves);
+
+/* Brick contents of leaves [first, first+count) as the reference stores
+ * them: SDF float[512], weight float[512], colour uint16[512][3] (R,G,B x256)
+ * per brick, voxel index (z*8+y)*8+x. */
+ff_status ff_get_bricks(ff_handle *h, uint32_t first, uint32_t count, float *sdf, float *weight, uint16_t *rgb);
+ff_status ff_set_bricks(ff_handle *h, uint32_t first, uint32_t count, const float *sdf, const float *weight,
+                        const uint16_t *rgb);
+
+/* The octree array (branches_used entries): 16 per branch, [0..7] leaf index
+ * per octant, [8..15] child branch -- the reference's _tree layout. */
+ff_status ff_get_tree(ff_handle *h, uint32_t *tree);
+
+/* Replace the whole map state (snapshot restore): octree, leaf table, bricks,
+ * volume side n and offset.  Used to resume and to mesh a given voxel state. */
+ff_status ff_set_state(ff_handle *h, uint32_t n, const float offset[3], const uint32_t *tree, uint32_t branches_used,
+                       const uint16_t *pos, const uint16_t *scale, const uint32_t *parent, uint32_t leaves_used,
+                       const float *sdf, const float *weight, const uint16_t *rgb);
+
+/* Message of the last failure on this handle (or of ff_create when h is NULL). */
+const char *ff_last_error(const ff_handle *h);
+
+/* Library build/version string. */
+const char *ff_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
