@@ -6,6 +6,7 @@
  */
 #define _GNU_SOURCE
 #include "ff_port.h"
+#include "ff_port_internal.h"
 
 #include <fenv.h>
 #include <xmmintrin.h>
@@ -46,6 +47,10 @@ struct ffp_map {
   int grows;
   int branch_overflow;
   int rz_exact;
+  /* mesh of the last ffp_update_meshes */
+  ffp_cell *cells;
+  int64_t ncells;
+  ffp_mesh_result mesh;
 };
 
 /* ---------------------------------------------------------------- helpers */
@@ -109,6 +114,11 @@ void ffp_destroy(ffp_map *m) {
   free(m->col);
   free(m->pxp);
   free(m->pyp);
+  free(m->cells);
+  free(m->mesh.xyz);
+  free(m->mesh.rgb);
+  free(m->mesh.faces);
+  free(m->mesh.cell_v);
   free(m);
 }
 
@@ -527,4 +537,81 @@ void ffp_set_bricks(ffp_map *m, int64_t n, const float *dist, const float *wgt, 
   memcpy(m->dist, dist, sizeof(float) * 512 * n);
   memcpy(m->wgt, wgt, sizeof(float) * 512 * n);
   memcpy(m->col, col, sizeof(uint16_t) * 512 * 3 * n);
+}
+
+/* -------------------------------------------------------------- meshing */
+
+/* updateMeshes() with every cell re-meshed from the current voxel data; the
+ * cells come in ascending (type, quirk, size, origin) order. */
+int64_t ffp_update_meshes(ffp_map *m) {
+  free(m->cells);
+  free(m->mesh.xyz);
+  free(m->mesh.rgb);
+  free(m->mesh.faces);
+  free(m->mesh.cell_v);
+  memset(&m->mesh, 0, sizeof(m->mesh));
+  m->cells = NULL;
+  m->ncells = 0;
+  if (!m->n || !m->meshing_ok) return 0;
+  m->ncells = ffp_enumerate_cells(m->tree, m->n, m->leaves_total, &m->cells);
+  ffp_mesh_src src;
+  src.pos = m->leaf_pos;
+  src.scale_of = m->leaf_scale;
+  src.parent = m->leaf_parent;
+  src.dist = m->dist;
+  src.wgt = m->wgt;
+  src.col = m->col;
+  src.leaves_used = m->leaves_used < m->leaves_total ? m->leaves_used : m->leaves_total;
+  for (int r = 0; r < 3; r++) src.offset[r] = m->offset[r];
+  src.scale = m->scale;
+  ffp_mesh_cells(&src, m->cells, m->ncells, &m->mesh);
+  return m->ncells;
+}
+
+void ffp_mesh_counts(const ffp_map *m, int64_t *ncells, int64_t *nv, int64_t *nf) {
+  *ncells = m->ncells;
+  *nv = m->mesh.nv;
+  *nf = m->mesh.nf;
+}
+
+/* cells: 14 int32 each (type, quirk, ox, oy, oz, size, L0..L7); ranges: 4 int64 each */
+void ffp_mesh_copy(const ffp_map *m, int32_t *cells, int64_t *ranges, float *xyz, uint8_t *rgb, uint32_t *faces) {
+  for (int64_t i = 0; i < m->ncells; i++) {
+    const ffp_cell *e = &m->cells[i];
+    int32_t *o = cells + 14 * i;
+    o[0] = e->type;
+    o[1] = e->quirk;
+    o[2] = e->o[0];
+    o[3] = e->o[1];
+    o[4] = e->o[2];
+    o[5] = e->size;
+    for (int k = 0; k < 8; k++) o[6 + k] = (int32_t)e->L[k];
+  }
+  if (m->ncells) memcpy(ranges, m->mesh.cell_v, sizeof(int64_t) * 4 * m->ncells);
+  if (m->mesh.nv) {
+    memcpy(xyz, m->mesh.xyz, sizeof(float) * 3 * m->mesh.nv);
+    memcpy(rgb, m->mesh.rgb, 3 * m->mesh.nv);
+  }
+  if (m->mesh.nf) memcpy(faces, m->mesh.faces, sizeof(uint32_t) * 3 * m->mesh.nf);
+}
+
+/* Replace the whole state (octree, leaf table, bricks) -- e.g. with the
+ * compiled reference's, so that meshing can be compared on identical input. */
+int ffp_set_state(ffp_map *m, uint32_t n, const float *offset, const uint32_t *tree, uint32_t branches_used,
+                  const uint16_t *pos, const uint16_t *scale, const uint32_t *parent, uint32_t leaves_used,
+                  const float *dist, const float *wgt, const uint16_t *col) {
+  if (branches_used > m->branches_total || leaves_used > m->leaves_total) return -1;
+  for (uint32_t i = 0; i < m->branches_total; i++) m->tree[i] = i < branches_used ? tree[i] : BRANCHINIT;
+  m->branches_used = branches_used;
+  memcpy(m->leaf_pos, pos, sizeof(uint16_t) * 3 * leaves_used);
+  memcpy(m->leaf_scale, scale, sizeof(uint16_t) * leaves_used);
+  memcpy(m->leaf_parent, parent, sizeof(uint32_t) * leaves_used);
+  memcpy(m->dist, dist, sizeof(float) * 512 * (size_t)leaves_used);
+  memcpy(m->wgt, wgt, sizeof(float) * 512 * (size_t)leaves_used);
+  memcpy(m->col, col, sizeof(uint16_t) * 3 * 512 * (size_t)leaves_used);
+  m->leaves_used = leaves_used;
+  m->n = (uint16_t)n;
+  for (int r = 0; r < 3; r++) m->offset[r] = offset[r];
+  m->meshing_ok = 1;
+  return 0;
 }

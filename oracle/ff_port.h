@@ -57,6 +57,17 @@ void ffp_bricks(const ffp_map *m, int64_t n, float *dist, float *wgt, uint16_t *
 /* Replace brick contents (used to start the update from a given state). */
 void ffp_set_bricks(ffp_map *m, int64_t n, const float *dist, const float *wgt, const uint16_t *col);
 
+/* Meshing (ff_port_mesh.c): every cell re-meshed from the current voxels.
+ * Returns the number of cells; cells are sorted by (type, quirk, size, origin). */
+int64_t ffp_update_meshes(ffp_map *m);
+void ffp_mesh_counts(const ffp_map *m, int64_t *ncells, int64_t *nv, int64_t *nf);
+/* cells: 14 int32 each (type, quirk, ox, oy, oz, size, L0..L7);
+ * ranges: per cell first vertex, vertex count, first face, face count. */
+void ffp_mesh_copy(const ffp_map *m, int32_t *cells, int64_t *ranges, float *xyz, uint8_t *rgb, uint32_t *faces);
+int ffp_set_state(ffp_map *m, uint32_t n, const float *offset, const uint32_t *tree, uint32_t branches_used,
+                  const uint16_t *pos, const uint16_t *scale, const uint32_t *parent, uint32_t leaves_used,
+                  const float *dist, const float *wgt, const uint16_t *col);
+
 #ifdef __cplusplus
 }
 #endif

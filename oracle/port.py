@@ -42,6 +42,12 @@ def lib():
         L.ffp_tree.argtypes = [vp, vp]
         L.ffp_bricks.argtypes = [vp, i64, vp, vp, vp]
         L.ffp_set_bricks.argtypes = [vp, i64, vp, vp, vp]
+        L.ffp_update_meshes.restype = i64
+        L.ffp_update_meshes.argtypes = [vp]
+        L.ffp_mesh_counts.argtypes = [vp, vp, vp, vp]
+        L.ffp_mesh_copy.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.ffp_set_state.restype = i32
+        L.ffp_set_state.argtypes = [vp, u32, vp, vp, u32, vp, vp, vp, u32, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -125,3 +131,35 @@ class PortFusion:
         w = np.ascontiguousarray(w, np.float32)
         c = np.ascontiguousarray(c, np.uint16)
         lib().ffp_set_bricks(self.h, d.shape[0], _p(d), _p(w), _p(c))
+
+    # -- meshing ---------------------------------------------------------
+    def update_meshes(self) -> int:
+        """Re-mesh every cell; returns the number of cells."""
+        return lib().ffp_update_meshes(self.h)
+
+    def mesh(self):
+        """(cells int32[n,14], ranges int64[n,4], xyz, rgb, faces) of the last update."""
+        c = np.zeros(3, np.int64)
+        lib().ffp_mesh_counts(self.h, _p(c[0:1]), _p(c[1:2]), _p(c[2:3]))
+        nc, nv, nf = (int(x) for x in c)
+        cells = np.zeros((nc, 14), np.int32)
+        ranges = np.zeros((nc, 4), np.int64)
+        xyz = np.zeros((nv, 3), np.float32)
+        rgb = np.zeros((nv, 3), np.uint8)
+        faces = np.zeros((nf, 3), np.uint32)
+        lib().ffp_mesh_copy(self.h, _p(cells), _p(ranges), _p(xyz), _p(rgb), _p(faces))
+        return cells, ranges, xyz, rgb, faces
+
+    def set_state(self, n, offset, tree, pos, scale, parent, dist, wgt, col):
+        offset = np.ascontiguousarray(offset, np.float32)
+        tree = np.ascontiguousarray(tree, np.uint32)
+        pos = np.ascontiguousarray(pos, np.uint16)
+        scale = np.ascontiguousarray(scale, np.uint16)
+        parent = np.ascontiguousarray(parent, np.uint32)
+        dist = np.ascontiguousarray(dist, np.float32)
+        wgt = np.ascontiguousarray(wgt, np.float32)
+        col = np.ascontiguousarray(col, np.uint16)
+        r = lib().ffp_set_state(self.h, int(n), _p(offset), _p(tree), tree.shape[0], _p(pos), _p(scale), _p(parent),
+                                pos.shape[0], _p(dist), _p(wgt), _p(col))
+        if r != 0:
+            raise ValueError("state larger than this map's capacity")

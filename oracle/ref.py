@@ -25,6 +25,11 @@ def available() -> bool:
 def lib():
     key = 0
     if key not in _libs:
+        # The reference is C++ and formats numbers through libstdc++'s locale
+        # machinery.  When numpy has already pulled libstdc++ in as a private
+        # dependency of its bundled BLAS, a library loaded afterwards crashes
+        # in that machinery; making libstdc++ global first avoids it.
+        ctypes.CDLL("libstdc++.so.6", mode=ctypes.RTLD_GLOBAL)
         L = ctypes.CDLL(LIB_PATH)
         vp, ll, i32 = ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int
         L.ref_create.restype = vp
@@ -49,6 +54,7 @@ def lib():
         L.ref_cell_mesh.restype = ll
         L.ref_cell_mesh.argtypes = [vp, ll, vp, vp, vp, ctypes.POINTER(ll)]
         L.ref_mc_offset_table.argtypes = [vp]
+        L.ref_mc_tables.argtypes = [vp, vp]
         _libs[key] = L
     return _libs[key]
 
@@ -162,3 +168,11 @@ def mc_offset_table() -> np.ndarray:
     out = np.zeros((256, 16), np.int32)
     lib().ref_mc_offset_table(_p(out))
     return out
+
+
+def mc_tables():
+    """(edge mask per case, triangle edge list per case) of the reference."""
+    em = np.zeros(256, np.int32)
+    tri = np.zeros((256, 16), np.int32)
+    lib().ref_mc_tables(_p(em), _p(tri))
+    return em, tri

@@ -21,10 +21,8 @@
 #include <thread>
 #include <tuple>
 #define protected public
-#define private public
 #include <fusion/geometryfusion_mipmap_cpu.hpp>
 #undef protected
-#undef private
 
 #include <auxiliary/memory.hpp>
 #include <fcntl.h>
@@ -247,6 +245,15 @@ void ref_mc_offset_table(int32_t *out /* 256 x 16 */) {
   MarchingCubesIndexed mc(8, 8);
   for (int i = 0; i < 256; i++)
     for (int j = 0; j < 16; j++) out[16 * i + j] = mc.offsetTable[i][j];
+}
+
+/* The non-indexed tables: edge mask and triangle list (edge numbers) per case. */
+void ref_mc_tables(int32_t *edge_mask /* 256 */, int32_t *tri /* 256 x 16 */) {
+  MarchingCubesIndexed mc(8, 8);
+  for (int i = 0; i < 256; i++) {
+    edge_mask[i] = mc.edgeTable[i];
+    for (int j = 0; j < 16; j++) tri[16 * i + j] = mc.triTable[i][j];
+  }
 }
 
 }  // extern "C"

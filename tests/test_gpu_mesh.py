@@ -1,0 +1,96 @@
+"""GPU marching cubes against the oracle.
+
+The oracle's meshing (oracle/ff_port_mesh.c) is pinned cell by cell against
+the compiled reference (tests/test_oracle.py).  Both sort cells by (type,
+quirk, size, origin), so the GPU mesh must equal the oracle's array for array:
+vertex bits, colours and face indices.
+"""
+import numpy as np
+import pytest
+
+from tests.helpers import MAXCAM, SCALING, circle_frames
+
+pytestmark = pytest.mark.gpu
+
+
+def _cam(K, R, t):
+    from fastfusion_b200.fusion import CameraInfo
+    return CameraInfo(K, R, t)
+
+
+def _gpu(**kw):
+    from fastfusion_b200.fusion import FusionMipMapCPU
+    return FusionMipMapCPU(0, 0, 0, 0.005, 0.01, 0, True, leaves_max=kw.get("leaves_max", 271420),
+                           branches_max=kw.get("branches_max", 4793488), storage=kw.get("storage", "fp32"))
+
+
+def _assert_same_mesh(gmesh, pmesh):
+    cells, ranges, xyz, rgb, faces = pmesh
+    assert gmesh.vertices.shape == xyz.shape, (gmesh.vertices.shape, xyz.shape)
+    assert gmesh.faces.shape == faces.shape
+    assert np.array_equal(gmesh.vertices.view(np.uint32), xyz.view(np.uint32)), "vertex bits differ"
+    assert np.array_equal(gmesh.colors, rgb), "colours differ"
+    assert np.array_equal(gmesh.faces, faces), "faces differ"
+
+
+@pytest.mark.parametrize("wh,nframes", [((160, 120), 8), ((640, 480), 4)])
+def test_mesh_after_fusion_matches_oracle(lib_built, port_lib, wh, nframes):
+    K, frames = circle_frames(0, nframes, *wh)
+    g = _gpu()
+    p = port_lib.PortFusion(leaves_total=271420, branches_total=4793488)
+    for depth, bgr, R, t in frames:
+        g.addMap(depth, _cam(K, R, t), bgr, SCALING, MAXCAM)
+        p.add_map(depth, bgr, K, R, t, SCALING, MAXCAM)
+    g.updateMeshes()
+    ncells = p.update_meshes()
+    assert g.stats()["mesh_cells"] == ncells
+    _assert_same_mesh(g.getMeshInterleavedMarchingCubes(), p.mesh())
+
+
+def test_incremental_equals_full_remesh(lib_built, port_lib):
+    """Meshing every third frame (dirty cells only) ends with the same mesh as
+    one full meshing at the end, and as the oracle."""
+    K, frames = circle_frames(2, 12, 160, 120)
+    a, b = _gpu(), _gpu()
+    p = port_lib.PortFusion(leaves_total=271420, branches_total=4793488)
+    dirty = []
+    for k, (depth, bgr, R, t) in enumerate(frames):
+        for m in (a, b):
+            m.addMap(depth, _cam(K, R, t), bgr, SCALING, MAXCAM)
+        p.add_map(depth, bgr, K, R, t, SCALING, MAXCAM)
+        if k % 3 == 2:
+            a.updateMeshes()
+            dirty.append((a.stats()["mesh_cells_dirty"], a.stats()["mesh_cells"]))
+    a.updateMeshes()
+    b.updateMeshes()
+    p.update_meshes()
+    ma, mb = a.getMeshInterleavedMarchingCubes(), b.getMeshInterleavedMarchingCubes()
+    assert np.array_equal(ma.vertices.view(np.uint32), mb.vertices.view(np.uint32))
+    assert np.array_equal(ma.faces, mb.faces)
+    assert np.array_equal(ma.colors, mb.colors)
+    _assert_same_mesh(ma, p.mesh())
+    # later updates re-mesh only part of the map
+    assert any(d < n for d, n in dirty[1:]), dirty
+
+
+def test_mesh_of_reference_state(lib_built, port_lib):
+    """Mesh the compiled reference's own voxel state (imported as a snapshot):
+    GPU == oracle on identical input."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("oracle/_ref/libffref.so not built")
+    K, frames = circle_frames(1, 5, 160, 120)
+    r = ref.RefFusion()
+    for depth, bgr, R, t in frames:
+        r.add_map(depth, bgr, K, R, t, SCALING, MAXCAM)
+    st = r.state()
+    pos, scl, par = r.leaves()
+    d, w, c = r.bricks()
+    tree = r.tree()
+    g = _gpu()
+    g.set_state(st["n"], st["offset"], tree, pos, scl, par, d, w, c)
+    p = port_lib.PortFusion(leaves_total=271420, branches_total=4793488)
+    p.set_state(st["n"], st["offset"], tree, pos, scl, par, d, w, c)
+    g.updateMeshes()
+    p.update_meshes()
+    _assert_same_mesh(g.getMeshInterleavedMarchingCubes(), p.mesh())
