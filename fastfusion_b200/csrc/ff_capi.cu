@@ -38,6 +38,7 @@ struct ff_handle {
   Counters *d_cnt = nullptr;
   Counters *h_cnt = nullptr;  // pinned
   uint32_t *d_barrier = nullptr;
+  uint32_t *d_rcp_tab = nullptr;  // FF_RCP_HOST: the host CPU's RCPPS per mantissa
 
   // per-image scratch
   int img_w = 0, img_h = 0, cap_pix = 0;
@@ -263,6 +264,10 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
     g_create_error = "ff_create: scale and threshold must be > 0";
     return FF_ERR_BAD_ARG;
   }
+  if (cfg->rcp_mode != FF_RCP_HOST && cfg->rcp_mode != FF_RCP_EXACT) {
+    g_create_error = "ff_create: unknown rcp_mode";
+    return FF_ERR_BAD_ARG;
+  }
   if (cfg->storage != FF_STORAGE_FP32 && cfg->storage != FF_STORAGE_FP16) {
     g_create_error = "ff_create: unknown storage";
     return FF_ERR_BAD_ARG;
@@ -323,6 +328,19 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
     if (alloc(&h->d_col, L * 1536) != cudaSuccess) { fail(FF_ERR_OOM_POOL, "colour pool"); break; }
     if (alloc(&h->d_cnt, 1) != cudaSuccess || alloc(&h->d_barrier, 4) != cudaSuccess) { fail(FF_ERR_CUDA, "counters"); break; }
     if (cudaMallocHost((void **)&h->h_cnt, sizeof(Counters)) != cudaSuccess) { fail(FF_ERR_CUDA, "pinned"); break; }
+    if (cfg->rcp_mode == FF_RCP_HOST) {
+      std::vector<uint32_t> tab;
+      if (!build_rcp_table(tab)) {
+        g_create_error = "ff_create: FF_RCP_HOST needs an x86-64 host whose RCPPS follows the mantissa-table rules";
+        st = FF_ERR_BAD_ARG;
+        break;
+      }
+      if (alloc(&h->d_rcp_tab, tab.size()) != cudaSuccess) { fail(FF_ERR_OOM_POOL, "rcp table"); break; }
+      if (cudaMemcpy(h->d_rcp_tab, tab.data(), 4 * tab.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        fail(FF_ERR_CUDA, "rcp table upload");
+        break;
+      }
+    }
     launch_fill(h->d_tree, h->cfg.branches_max, BRANCHINIT, h->stream);
     cudaMemsetAsync(h->d_stamp, 0, sizeof(uint32_t) * L, h->stream);
     cudaMemsetAsync(h->d_parent, 0xFF, sizeof(uint32_t) * L, h->stream);
@@ -352,7 +370,7 @@ ff_status ff_destroy(ff_handle *h) {
   mesh_free(h->mesh);
   void *ptrs[] = {h->d_tree, h->d_leaf, h->d_parent, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
                   h->d_stamp, h->d_queue, h->d_cnt, h->d_barrier, h->d_depth, h->d_bgr, h->d_pxp, h->d_pyp,
-                  h->d_vox, h->d_proc, h->d_bnd, h->d_pend, h->d_keys, h->d_sort_tmp};
+                  h->d_vox, h->d_proc, h->d_bnd, h->d_pend, h->d_keys, h->d_sort_tmp, h->d_rcp_tab};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->h_cnt) cudaFreeHost(h->h_cnt);
@@ -467,7 +485,7 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
   }
   launch_fuse(h->d_queue, (int)nq, h->d_leaf, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
               h->cfg.storage, h->cfg.leaves_max, d_depth, d_bgr, W, H, q, h->cfg.scale, h->cfg.threshold, scaling,
-              maxcam, s);
+              maxcam, h->d_rcp_tab, s);
   CK(cudaGetLastError());
   if (h->leaves_used > h->cfg.leaves_max) h->meshing_ok = false;
   h->queued = nq;
@@ -698,6 +716,15 @@ ff_status ff_get_mesh(ff_handle *h, float *xyz, uint8_t *rgb, uint32_t *faces) {
   CK(cudaSetDevice(h->cfg.device));
   std::string err;
   int rc = mesh_copy_out(h->mesh, xyz, rgb, faces, h->stream, err);
+  if (rc != 0) return set_err(h, (ff_status)rc, err);
+  return FF_OK;
+}
+
+ff_status ff_get_mesh_cells(ff_handle *h, int32_t *cells, int64_t *ranges) {
+  if (!h || (h->mesh.n_cells && (!cells || !ranges))) return FF_ERR_BAD_ARG;
+  CK(cudaSetDevice(h->cfg.device));
+  std::string err;
+  int rc = mesh_copy_cells(h->mesh, cells, ranges, h->stream, err);
   if (rc != 0) return set_err(h, (ff_status)rc, err);
   return FF_OK;
 }

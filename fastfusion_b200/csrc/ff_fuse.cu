@@ -5,12 +5,22 @@
 // round-toward-zero (the reference sets MXCSR=RZ, :1678-1679) with the
 // reference's operation order, voxel positions accumulated the way the
 // reference's loops accumulate them (z steps, then y steps, then x * step),
-// and exact RZ reciprocals (__frcp_rz) in place of _mm256_rcp_ps.
+// and the reference's three reciprocals either exactly as the host CPU's
+// RCPPS computes them (FF_RCP_HOST: table of the instruction's mantissa map,
+// bit-identical to the reference binary on that host) or as exact RZ
+// reciprocals (FF_RCP_EXACT: __frcp_rz, host-independent).
 // Every voxel of every queued brick is read and written, like the reference.
 //
 // One CTA per brick, one thread per voxel: the 512 SDF and weight words of a
 // brick and its three 512-entry colour planes are contiguous, so each load and
 // store is a fully coalesced 2 KB / 1 KB segment.
+#include <string.h>
+
+#include <vector>
+#if defined(__x86_64__) || defined(_M_X64)
+#include <xmmintrin.h>
+#endif
+
 #include "ff_kernels.h"
 
 namespace ffb {
@@ -22,14 +32,37 @@ __device__ __forceinline__ int cvt_x86_rz(float f) {
   return __float2int_rz(f);
 }
 
-template <bool FP16>
+// Reciprocal as the host CPU's RCPPS computes it: the result mantissa is a
+// function of the input mantissa alone (tab, measured from the instruction
+// for x in [1,2)), the exponent is negated; zero and denormal inputs give
+// infinity, infinity gives zero, results below the normal range are flushed
+// to zero, NaN stays NaN -- the behaviour checked when the table is built.
+__device__ __forceinline__ float rcp_host(float x, const uint32_t *__restrict__ tab) {
+  const uint32_t u = __float_as_uint(x);
+  const uint32_t sgn = u & 0x80000000u;
+  const int e = (int)((u >> 23) & 255u);
+  const uint32_t m = u & 0x7fffffu;
+  if (e == 255) return m ? __uint_as_float(u | 0x400000u) : __uint_as_float(sgn);
+  if (e == 0) return __uint_as_float(sgn | 0x7f800000u);
+  const uint32_t t = __ldg(tab + m);
+  const int te = (int)((t >> 23) & 255u) - (e - 127);
+  if (te <= 0) return __uint_as_float(sgn);
+  return __uint_as_float(sgn | (t & 0x7fffffu) | ((uint32_t)te << 23));
+}
+
+template <bool RCP_HOST>
+__device__ __forceinline__ float rcp_upd(float x, const uint32_t *tab) {
+  return RCP_HOST ? rcp_host(x, tab) : __frcp_rz(x);
+}
+
+template <bool FP16, bool RCP_HOST>
 __global__ void __launch_bounds__(512) k_fuse(const uint32_t *__restrict__ queue, const ushort4 *__restrict__ leaf,
                                               float *__restrict__ sdf, float *__restrict__ wgt,
                                               __half *__restrict__ sdf16, __half *__restrict__ wgt16,
                                               uint16_t *__restrict__ col, uint32_t leaves_max,
                                               const uint16_t *__restrict__ depth, const uint8_t *__restrict__ bgr,
                                               int W, int H, CamF q, float scale, float thr, float scaling,
-                                              float maxcam) {
+                                              float maxcam, const uint32_t *__restrict__ rtab) {
   const uint32_t brick = queue[blockIdx.x];
   const int v = threadIdx.x;
   const int x = v & 7, y = (v >> 3) & 7, z = v >> 6;
@@ -64,7 +97,7 @@ __global__ void __launch_bounds__(512) k_fuse(const uint32_t *__restrict__ queue
   const float px = __fadd_rz(pzx, kx), py = __fadd_rz(pzy, ky), pz = __fadd_rz(pzz, kz);
 
   const float len = __fsqrt_rz(__fadd_rz(__fadd_rz(__fmul_rz(px, px), __fmul_rz(py, py)), __fmul_rz(pz, pz)));
-  const float rc = __frcp_rz(pz);
+  const float rc = rcp_upd<RCP_HOST>(pz, rtab);
   const int imx = cvt_x86_rz(__fadd_rz(q.cx, __fmul_rz(q.fx, __fmul_rz(px, rc))));
   const int imy = cvt_x86_rz(__fadd_rz(q.cy, __fmul_rz(q.fy, __fmul_rz(py, rc))));
   const int cyi = max(min(imy, H - 1), 0);
@@ -77,7 +110,7 @@ __global__ void __launch_bounds__(512) k_fuse(const uint32_t *__restrict__ queue
   const float thrW = __fmul_rz(__fmul_rz(WEIGHT_FACTOR, thr), ls);
   const float front = dInc < DIST_W_EPS ? 1.0f : 0.0f;
   const float back = (dInc >= DIST_W_EPS && dInc < thrW) ? 1.0f : 0.0f;
-  const float fall = __fmul_rz(__fsub_rz(thrW, dInc), __frcp_rz(__fsub_rz(thrW, DIST_W_EPS)));
+  const float fall = __fmul_rz(__fsub_rz(thrW, dInc), rcp_upd<RCP_HOST>(__fsub_rz(thrW, DIST_W_EPS), rtab));
   const float wInc = mask ? __fadd_rz(front, __fmul_rz(fall, back)) : 0.0f;
 
   const size_t vi = (size_t)brick * 512 + v;
@@ -90,7 +123,7 @@ __global__ void __launch_bounds__(512) k_fuse(const uint32_t *__restrict__ queue
     dAcc = sdf[vi];
   }
   const float wNew = __fadd_rz(wAcc, wInc);
-  const float factor = __frcp_rz(__fadd_rz(wNew, wNew <= 0.0f ? 1.0f : 0.0f));
+  const float factor = rcp_upd<RCP_HOST>(__fadd_rz(wNew, wNew <= 0.0f ? 1.0f : 0.0f), rtab);
   float tr = dInc < thrD ? dInc : thrD;
   const float lo = -thrD;
   tr = tr > lo ? tr : lo;
@@ -119,14 +152,54 @@ __global__ void __launch_bounds__(512) k_fuse(const uint32_t *__restrict__ queue
 void launch_fuse(const uint32_t *queue, int nq, const ushort4 *leaf, float *sdf, float *wgt, __half *sdf16,
                  __half *wgt16, uint16_t *col, int storage, uint32_t leaves_max, const uint16_t *depth,
                  const uint8_t *bgr, int W, int H, const CamF &q, float scale, float thr, float scaling,
-                 float maxcam, cudaStream_t s) {
+                 float maxcam, const uint32_t *rcp_tab, cudaStream_t s) {
   if (nq <= 0) return;
-  if (storage == 1)
-    k_fuse<true><<<nq, 512, 0, s>>>(queue, leaf, sdf, wgt, sdf16, wgt16, col, leaves_max, depth, bgr, W, H, q,
-                                    scale, thr, scaling, maxcam);
-  else
-    k_fuse<false><<<nq, 512, 0, s>>>(queue, leaf, sdf, wgt, sdf16, wgt16, col, leaves_max, depth, bgr, W, H, q,
-                                     scale, thr, scaling, maxcam);
+#define FF_FUSE(F16, RH)                                                                                         \
+  k_fuse<F16, RH><<<nq, 512, 0, s>>>(queue, leaf, sdf, wgt, sdf16, wgt16, col, leaves_max, depth, bgr, W, H, q, \
+                                     scale, thr, scaling, maxcam, rcp_tab)
+  const bool rh = rcp_tab != nullptr;
+  if (storage == 1) {
+    if (rh) FF_FUSE(true, true); else FF_FUSE(true, false);
+  } else {
+    if (rh) FF_FUSE(false, true); else FF_FUSE(false, false);
+  }
+#undef FF_FUSE
+}
+
+// Measure the host CPU's RCPPS for every mantissa of [1,2) and check the
+// exponent/sign/special-value rules that rcp_host() relies on.
+bool build_rcp_table(std::vector<uint32_t> &tab) {
+#if defined(__x86_64__) || defined(_M_X64)
+  tab.resize(1u << 23);
+  for (uint32_t m = 0; m < (1u << 23); m += 4) {
+    float x[4];
+    for (int k = 0; k < 4; k++) {
+      uint32_t u = (127u << 23) | (m + k);
+      memcpy(&x[k], &u, 4);
+    }
+    __m128 r = _mm_rcp_ps(_mm_loadu_ps(x));
+    _mm_storeu_ps(reinterpret_cast<float *>(&tab[m]), r);
+  }
+  auto bits = [](float f) { uint32_t u; memcpy(&u, &f, 4); return u; };
+  auto rcp1 = [](float f) { return _mm_cvtss_f32(_mm_rcp_ss(_mm_set_ss(f))); };
+  for (int e = 1; e < 255; e += 7) {
+    for (uint32_t m = 0; m < (1u << 23); m += 65537) {
+      uint32_t u = ((uint32_t)e << 23) | m;
+      float x;
+      memcpy(&x, &u, 4);
+      uint32_t t = tab[m];
+      int te = (int)((t >> 23) & 255u) - (e - 127);
+      uint32_t pred = te <= 0 ? 0u : ((t & 0x7fffffu) | ((uint32_t)te << 23));
+      if (bits(rcp1(x)) != pred || bits(rcp1(-x)) != (pred | 0x80000000u)) return false;
+    }
+  }
+  if (bits(rcp1(0.0f)) != 0x7f800000u || bits(rcp1(1e-40f)) != 0x7f800000u) return false;
+  if (bits(rcp1(__builtin_inff())) != 0u) return false;
+  return true;
+#else
+  (void)tab;
+  return false;
+#endif
 }
 
 }  // namespace ffb

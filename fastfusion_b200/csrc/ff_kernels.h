@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "ff_common.cuh"
 
 namespace ffb {
@@ -55,6 +57,10 @@ void launch_fill(uint32_t *p, size_t n, uint32_t v, cudaStream_t s);
 void launch_fuse(const uint32_t *queue, int nq, const ushort4 *leaf, float *sdf, float *wgt, __half *sdf16,
                  __half *wgt16, uint16_t *col, int storage, uint32_t leaves_max, const uint16_t *depth,
                  const uint8_t *bgr, int W, int H, const CamF &q, float scale, float thr, float scaling,
-                 float maxcam, cudaStream_t s);
+                 float maxcam, const uint32_t *rcp_tab, cudaStream_t s);
+
+// Table of the host CPU's RCPPS over the mantissas of [1,2); false when the
+// host is not x86-64 or the instruction does not follow the expected rules.
+bool build_rcp_table(std::vector<uint32_t> &tab);
 
 }  // namespace ffb

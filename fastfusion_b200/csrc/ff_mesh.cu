@@ -1272,6 +1272,45 @@ int mesh_copy_out(MeshState &M, float *xyz, uint8_t *rgb, uint32_t *faces, cudaS
   return 0;
 }
 
+__global__ void k_export_cells(const Cell *cells, const CellOut *out, const uint64_t *vbase, const uint64_t *fbase,
+                               uint32_t n, int32_t *rows, int64_t *ranges) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Cell c = cells[i];
+  int32_t *r = rows + 14 * (size_t)i;
+  r[0] = c.type;
+  r[1] = c.quirk;
+  r[2] = c.o[0];
+  r[3] = c.o[1];
+  r[4] = c.o[2];
+  r[5] = c.size;
+  for (int k = 0; k < 8; k++) r[6 + k] = (int32_t)c.L[k];
+  int64_t *g = ranges + 4 * (size_t)i;
+  g[0] = (int64_t)vbase[i];
+  g[1] = out[i].nv;
+  g[2] = (int64_t)fbase[i];
+  g[3] = out[i].nf;
+}
+
+int mesh_copy_cells(MeshState &M, int32_t *rows, int64_t *ranges, cudaStream_t s, std::string &err) {
+  if (!M.impl || !M.valid || !M.n_cells) return 0;
+  MeshImpl &I = impl(M);
+  const uint32_t n = (uint32_t)M.n_cells;
+  int32_t *d_rows = nullptr;
+  int64_t *d_ranges = nullptr;
+  MCK(cudaMallocAsync((void **)&d_rows, sizeof(int32_t) * 14 * n, s));
+  MCK(cudaMallocAsync((void **)&d_ranges, sizeof(int64_t) * 4 * n, s));
+  // after an update the current cells, counts and bases are the "old" set
+  k_export_cells<<<(n + 255) / 256, 256, 0, s>>>(I.old_cells, I.old_out, I.old_vbase, I.old_fbase, n, d_rows,
+                                                 d_ranges);
+  MCK(cudaMemcpyAsync(rows, d_rows, sizeof(int32_t) * 14 * n, cudaMemcpyDeviceToHost, s));
+  MCK(cudaMemcpyAsync(ranges, d_ranges, sizeof(int64_t) * 4 * n, cudaMemcpyDeviceToHost, s));
+  MCK(cudaFreeAsync(d_rows, s));
+  MCK(cudaFreeAsync(d_ranges, s));
+  MCK(cudaStreamSynchronize(s));
+  return 0;
+}
+
 void mesh_free(MeshState &M) {
   if (M.impl) {
     MeshImpl &I = impl(M);

@@ -46,6 +46,9 @@ struct MeshState {
 // returns 0 or an ff_status value
 int mesh_update(MeshState &m, const MeshInputs &in, cudaStream_t s, std::string &err);
 int mesh_copy_out(MeshState &m, float *xyz, uint8_t *rgb, uint32_t *faces, cudaStream_t s, std::string &err);
+// cells of the last update: 14 int32 each (type, quirk, ox, oy, oz, size, L0..L7) and per cell
+// (first vertex, vertex count, first face, face count)
+int mesh_copy_cells(MeshState &m, int32_t *rows, int64_t *ranges, cudaStream_t s, std::string &err);
 void mesh_free(MeshState &m);
 void mesh_invalidate(MeshState &m);
 void mesh_note_frame(MeshState &m);

@@ -25,6 +25,7 @@ FF_OK = 0
 _STATUS = {0: "FF_OK", 1: "FF_ERR_BAD_ARG", 2: "FF_ERR_CUDA", 3: "FF_ERR_OOM_POOL", 4: "FF_ERR_OOM_MESH",
            5: "FF_ERR_TIMEOUT", 6: "FF_ERR_STATE", 7: "FF_ERR_NO_DEVICE"}
 STORAGE = {"fp32": 0, "fp16": 1}
+RCP = {"host": 0, "exact": 1}
 BRANCHINIT = 0xFFFFFFFE
 
 
@@ -37,7 +38,8 @@ class FFError(RuntimeError):
 class ff_config(ctypes.Structure):
     _fields_ = [("scale", ctypes.c_float), ("threshold", ctypes.c_float), ("color", ctypes.c_int),
                 ("leaves_max", ctypes.c_uint32), ("branches_max", ctypes.c_uint32),
-                ("pool_bytes", ctypes.c_uint64), ("device", ctypes.c_int), ("storage", ctypes.c_int)]
+                ("pool_bytes", ctypes.c_uint64), ("device", ctypes.c_int), ("storage", ctypes.c_int),
+                ("rcp_mode", ctypes.c_int)]
 
 
 class ff_stats(ctypes.Structure):
@@ -63,6 +65,7 @@ SIGNATURES = {
     "ff_get_mesh_counts": (_i32, [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
     "ff_get_mesh": (_i32, [_vp, _vp, _vp, _vp]),
     "ff_get_mesh_device": (_i32, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
+    "ff_get_mesh_cells": (_i32, [_vp, _vp, _vp]),
     "ff_get_stats": (_i32, [_vp, ctypes.POINTER(ff_stats)]),
     "ff_get_leaves": (_i32, [_vp, _vp, _vp, _vp]),
     "ff_get_queue": (_i32, [_vp, _vp]),
@@ -133,13 +136,14 @@ class FusionMipMapCPU:
 
     def __init__(self, offsetX: float = 0.0, offsetY: float = 0.0, offsetZ: float = 0.0, scale: float = 0.005,
                  distanceThreshold: float = 0.01, n: int = 0, color: bool = True, *, leaves_max: int = 0,
-                 branches_max: int = 0, pool_bytes: int = 0, device: int = 0, storage: str = "fp32"):
+                 branches_max: int = 0, pool_bytes: int = 0, device: int = 0, storage: str = "fp32",
+                 rcp: str = "host"):
         # The reference ignores the offset and n arguments (its constructor
         # passes 0,0,0 and n=0 to the base class, geometryfusion_mipmap_cpu.cpp:420-424).
         self._L = load_library()
         cfg = ff_config(scale=scale, threshold=distanceThreshold, color=1 if color else 0,
                         leaves_max=leaves_max, branches_max=branches_max, pool_bytes=pool_bytes,
-                        device=device, storage=STORAGE[storage])
+                        device=device, storage=STORAGE[storage], rcp_mode=RCP[rcp])
         h = ctypes.c_void_p()
         st = self._L.ff_create(ctypes.byref(cfg), ctypes.byref(h))
         if st != FF_OK:
@@ -200,6 +204,14 @@ class FusionMipMapCPU:
         faces = np.zeros((nf.value, 3), np.uint32)
         self._check(self._L.ff_get_mesh(self._h, _p(xyz), _p(rgb), _p(faces)))
         return MeshInterleaved(xyz, rgb, faces)
+
+    def mesh_cells(self):
+        """(cells int32[n,14], ranges int64[n,4]) of the last updateMeshes."""
+        n = self.stats()["mesh_cells"]
+        cells = np.zeros((n, 14), np.int32)
+        ranges = np.zeros((n, 4), np.int64)
+        self._check(self._L.ff_get_mesh_cells(self._h, _p(cells), _p(ranges)))
+        return cells, ranges
 
     def setThreadMeshing(self, threadMeshing: bool):
         """Meshing runs on the GPU stream; there is no mesher thread."""

@@ -33,6 +33,16 @@ typedef enum ff_status {
 /* Voxel storage of the brick pool. */
 enum { FF_STORAGE_FP32 = 0, FF_STORAGE_FP16 = 1 };
 
+/* Reciprocal of the voxel update.  The reference runs its update with the
+ * approximate x86 RCPPS instruction (update_functions.cpp:1246,1373,1386),
+ * whose result bits depend on the CPU model.
+ *   FF_RCP_HOST:  reproduce the RCPPS of the CPU this library runs on (a
+ *                 2^23-entry table measured from the instruction at
+ *                 ff_create, 32 MB of device memory); results are bit-identical
+ *                 to the reference binary on the same host.  x86-64 only.
+ *   FF_RCP_EXACT: exact round-toward-zero reciprocal; host-independent. */
+enum { FF_RCP_HOST = 0, FF_RCP_EXACT = 1 };
+
 typedef struct ff_config {
   float scale;             /* voxel edge in metres (FusionMipMapCPU ctor `scale`) */
   float threshold;         /* truncation distance in metres (ctor `distanceThreshold`) */
@@ -42,6 +52,7 @@ typedef struct ff_config {
   uint64_t pool_bytes;     /* used when leaves_max == 0 */
   int device;              /* CUDA device ordinal */
   int storage;             /* FF_STORAGE_FP32 (reference layout) or FF_STORAGE_FP16 */
+  int rcp_mode;            /* FF_RCP_HOST (default, reference bits) or FF_RCP_EXACT */
 } ff_config;
 
 typedef struct ff_handle ff_handle;
@@ -107,6 +118,14 @@ ff_status ff_get_mesh_counts(ff_handle *h, uint64_t *n_vertices, uint64_t *n_fac
  * metres), rgb uint8[3*nv], faces uint32[3*nf].  Replaces
  * getMeshInterleavedMarchingCubes() (geometryfusion_mipmap_cpu.cpp:3359-3374). */
 ff_status ff_get_mesh(ff_handle *h, float *xyz, uint8_t *rgb, uint32_t *faces);
+
+/* The mesh cells of the last update (ff_stats.mesh_cells of them), in mesh
+ * order: 14 int32 each -- type (0 interior, 1-3 wall x/y/z, 4-6 edge x/y/z,
+ * 7 corner), quirk flag, origin x/y/z, size (voxels), the leaf of each side
+ * (8 entries, 0xFFFFFFFE past the cell's side count) -- the reference's
+ * MeshCell (treeandbrick_incremental.hpp:71-93); and 4 int64 each: first
+ * vertex, vertex count, first face, face count of the cell's part of the mesh. */
+ff_status ff_get_mesh_cells(ff_handle *h, int32_t *cells, int64_t *ranges);
 
 /* Device pointers to the same mesh, valid until the next ff_update_meshes. */
 ff_status ff_get_mesh_device(ff_handle *h, const float **xyz, const uint8_t **rgb, const uint32_t **faces);

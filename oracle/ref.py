@@ -48,6 +48,7 @@ def lib():
         L.ref_queue.argtypes = [vp, vp]
         L.ref_tree.argtypes = [vp, vp]
         L.ref_bricks.argtypes = [vp, ll, vp, vp, vp]
+        L.ref_set_bricks.argtypes = [vp, ll, vp, vp, vp]
         L.ref_cells.restype = ll
         L.ref_cells.argtypes = [vp, vp]
         L.ref_queue_all_cells.argtypes = [vp]
@@ -144,6 +145,12 @@ class RefFusion:
         c = np.zeros((n, 512, 3), np.uint16)
         self.L.ref_bricks(self.h, n, _p(d), _p(w), _p(c))
         return d, w, c
+
+    def set_bricks(self, d, w, c):
+        d = np.ascontiguousarray(d, np.float32)
+        w = np.ascontiguousarray(w, np.float32)
+        c = np.ascontiguousarray(c, np.uint16)
+        self.L.ref_set_bricks(self.h, d.shape[0], _p(d), _p(w), _p(c))
 
     def cells(self):
         n = self.L.ref_cells(self.h, None)

@@ -176,6 +176,21 @@ void ref_bricks(void *h, long long n, float *dist, float *wgt, uint16_t *col) {
   }
 }
 
+/* Overwrite the brick contents of leaves [0, n) (same layout as ref_bricks),
+ * e.g. with a machine-independent voxel state, before re-meshing. */
+void ref_set_bricks(void *h, long long n, const float *dist, const float *wgt, const uint16_t *col) {
+  FusionMipMapCPU *f = (FusionMipMapCPU *)h;
+  for (long long i = 0; i < n * 512; i++) {
+    f->_distance[i] = dist[i];
+    f->_weights[i] = wgt[i];
+    if (f->_color) {
+      f->_color[i].x = col[3 * i + 0];
+      f->_color[i].y = col[3 * i + 1];
+      f->_color[i].z = col[3 * i + 2];
+    }
+  }
+}
+
 /* Mesh cells: 14 int32 each: type, ox, oy, oz, size, has_mesh, lastLeaf[8]. */
 long long ref_cells(void *h, int32_t *out) {
   FusionMipMapCPU *f = (FusionMipMapCPU *)h;

@@ -1,11 +1,12 @@
 """GPU parity of brick allocation and voxel fusion against the oracle.
 
 The oracle (oracle/ff_port.c) restates the reference's addMap with
-round-toward-zero arithmetic and exact reciprocals; its traversal is pinned
-bit-exact against the compiled reference (tests/test_oracle.py).  Here the
-CUDA path must reproduce it exactly: leaf table (positions, scales, parents,
-in index order), the set of updated bricks, and every SDF, weight and colour
-bit.
+round-toward-zero arithmetic; with the host CPU's RCPPS (update mode 2) it
+is pinned bit-exact against the compiled reference (tests/test_oracle.py),
+with exact reciprocals (mode 1) it is the host-independent target.  The CUDA
+path must reproduce either exactly (rcp="host" / rcp="exact"): leaf table
+(positions, scales, parents, in index order), the set of updated bricks, and
+every SDF, weight and colour bit.
 """
 import numpy as np
 import pytest
@@ -15,11 +16,12 @@ from tests.helpers import MAXCAM, SCALING, circle_frames, queue_set
 pytestmark = pytest.mark.gpu
 
 
-def _pair(port_lib, leaves_max=271420, branches_max=4793488, storage="fp32"):
+def _pair(port_lib, leaves_max=271420, branches_max=4793488, storage="fp32", rcp="exact"):
     from fastfusion_b200.fusion import FusionMipMapCPU
     g = FusionMipMapCPU(0, 0, 0, 0.005, 0.01, 0, True, leaves_max=leaves_max, branches_max=branches_max,
-                        storage=storage)
-    p = port_lib.PortFusion(leaves_total=leaves_max, branches_total=branches_max, update_mode=1)
+                        storage=storage, rcp=rcp)
+    p = port_lib.PortFusion(leaves_total=leaves_max, branches_total=branches_max,
+                            update_mode=1 if rcp == "exact" else 2)
     return g, p
 
 
@@ -46,10 +48,11 @@ def _compare_frame(g, p, check_bricks=True):
         assert np.array_equal(cg, cp), "colour differs"
 
 
+@pytest.mark.parametrize("rcp", ["exact", "host"])
 @pytest.mark.parametrize("wh", [(160, 120), (640, 480)])
-def test_alloc_fuse_bit_exact(lib_built, port_lib, wh):
+def test_alloc_fuse_bit_exact(lib_built, port_lib, wh, rcp):
     K, frames = circle_frames(0, 6 if wh[0] == 640 else 12, wh[0], wh[1])
-    g, p = _pair(port_lib)
+    g, p = _pair(port_lib, rcp=rcp)
     for depth, bgr, R, t in frames:
         qg = g.addMap(depth, _cam(K, R, t), bgr, SCALING, MAXCAM)
         qp = p.add_map(depth, bgr, K, R, t, SCALING, MAXCAM)
@@ -111,3 +114,26 @@ def test_empty_frame(lib_built, port_lib):
     assert g.stats()["n"] == p.state()["n"] == 0
     assert g.addMap(depth, _cam(K, R, t), bgr, SCALING, MAXCAM) == p.add_map(depth, bgr, K, R, t, SCALING, MAXCAM)
     _compare_frame(g, p)
+
+
+def test_bit_exact_with_reference_binary(lib_built):
+    """rcp="host": the GPU reproduces the compiled reference itself, run on
+    this host's CPU -- leaf table, updated bricks, every voxel bit."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("oracle/_ref/libffref.so not built")
+    from fastfusion_b200.fusion import FusionMipMapCPU
+    K, frames = circle_frames(0, 5, 640, 480)
+    r = ref.RefFusion()
+    st = r.state()
+    g = FusionMipMapCPU(0, 0, 0, 0.005, 0.01, 0, True, leaves_max=st["leaves_total"],
+                        branches_max=st["branches_total"], rcp="host")
+    for depth, bgr, R, t in frames:
+        assert g.addMap(depth, _cam(K, R, t), bgr, SCALING, MAXCAM) == r.add_map(depth, bgr, K, R, t, SCALING, MAXCAM)
+        for a, b in zip(g.leaves(), r.leaves()):
+            assert np.array_equal(a, b)
+        assert queue_set(g.queue()) == queue_set(r.queue())
+    (dg, wg, cg), (dr, wr, cr) = g.bricks(), r.bricks()
+    assert np.array_equal(dg.view(np.uint32), dr.view(np.uint32))
+    assert np.array_equal(wg.view(np.uint32), wr.view(np.uint32))
+    assert np.array_equal(cg, cr)

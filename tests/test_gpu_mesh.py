@@ -21,7 +21,8 @@ def _cam(K, R, t):
 def _gpu(**kw):
     from fastfusion_b200.fusion import FusionMipMapCPU
     return FusionMipMapCPU(0, 0, 0, 0.005, 0.01, 0, True, leaves_max=kw.get("leaves_max", 271420),
-                           branches_max=kw.get("branches_max", 4793488), storage=kw.get("storage", "fp32"))
+                           branches_max=kw.get("branches_max", 4793488), storage=kw.get("storage", "fp32"),
+                           rcp=kw.get("rcp", "exact"))
 
 
 def _assert_same_mesh(gmesh, pmesh):
@@ -94,3 +95,44 @@ def test_mesh_of_reference_state(lib_built, port_lib):
     g.updateMeshes()
     p.update_meshes()
     _assert_same_mesh(g.getMeshInterleavedMarchingCubes(), p.mesh())
+
+
+def test_mesh_matches_reference_binary_cells(lib_built):
+    """rcp="host" end to end against the compiled reference: fuse the same
+    frames, then every cell the reference and the GPU both have must carry the
+    same mesh (vertex bits, colours, local faces)."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("oracle/_ref/libffref.so not built")
+    need = {0: 1, 1: 2, 2: 2, 3: 2, 4: 4, 5: 4, 6: 4, 7: 8}
+    K, frames = circle_frames(0, 4, 320, 240)
+    r = ref.RefFusion()
+    g = _gpu(rcp="host")
+    for depth, bgr, R, t in frames:
+        r.add_map(depth, bgr, K, R, t, SCALING, MAXCAM)
+        g.addMap(depth, _cam(K, R, t), bgr, SCALING, MAXCAM)
+    r.queue_all_cells()
+    r.update_meshes()
+    g.updateMeshes()
+    mesh = g.getMeshInterleavedMarchingCubes()
+    cells, ranges = g.mesh_cells()
+    refmap = {}
+    for i, row in enumerate(r.cells()):
+        t = int(row[0])
+        L = tuple(int(x) & 0xFFFFFFFF for x in row[6:6 + need[t]])
+        if all(x < ref.BRANCHINIT for x in L):
+            refmap[(t, int(row[1]), int(row[2]), int(row[3]), int(row[4]), L)] = i
+    common = same = 0
+    for i, row in enumerate(cells):
+        t = int(row[0])
+        key = (t, int(row[2]), int(row[3]), int(row[4]), int(row[5]), tuple(int(x) & 0xFFFFFFFF for x in row[6:6 + need[t]]))
+        if key not in refmap:
+            continue
+        common += 1
+        rx, rc, rf = r.cell_mesh(refmap[key])
+        v0, nv, f0, nf = (int(x) for x in ranges[i])
+        same += (rx.shape[0] == nv and rf.shape[0] == nf
+                 and np.array_equal(rx.view(np.uint32), mesh.vertices[v0:v0 + nv].view(np.uint32))
+                 and np.array_equal(rc, mesh.colors[v0:v0 + nv]) and np.array_equal(rf, mesh.faces[f0:f0 + nf] - v0))
+    assert common >= 0.97 * len(refmap)
+    assert same == common
