@@ -9,10 +9,9 @@
 // size of the smallest slot it touches; each side refers to the finest leaf
 // at or above its slot.  Here they are generated from the octree by a
 // level-synchronous cell/face/edge/vertex traversal (one kernel per octree
-// level, work queues in HBM), keeping one bookkeeping quirk of the reference
-// (corners at the midpoints of split x-edges are shifted by one cell along x
-// and have their x-pairs of leaves swapped), then sorted by (type, quirk,
-// size, origin) so that the output order is deterministic.
+// level, work queues in HBM) -- the reference's cell set, cell for cell --
+// then sorted by (type, size, origin, leaves) so that the output order is
+// deterministic.
 //
 // Meshing.  A warp per interior/wall/edge cell gathers the cell's lattice of
 // samples (falling back along the parent-leaf chain where the weight is zero),
@@ -85,7 +84,6 @@ struct EdgeItem {
 };
 struct VertItem {
   Slot s[8];
-  int xedge;
 };
 
 struct GenQueues {
@@ -159,27 +157,24 @@ __device__ __forceinline__ void push(T *q, uint32_t *count, uint32_t cap, const 
   q[i] = v;
 }
 
-__device__ void vert_item(const GenCtx &g, const GenQueues &Q, const Slot *S8, int xedge, int nb) {
+__device__ void vert_item(const GenCtx &g, const GenQueues &Q, const Slot *S8, int nb) {
   bool any = false;
   for (int j = 0; j < 8; j++) any |= is_sub(g, S8[j]);
   if (any) {
     VertItem v;
     for (int j = 0; j < 8; j++) v.s[j] = ch(g, S8[j], 7 - j);
-    v.xedge = 0;
     push(Q.vertq[nb], Q.count + nb * 4 + 3, Q.cap_vert, v, Q.error);
     return;
   }
-  int size = S8[0].size;
-  for (int j = 1; j < 8; j++) size = min(size, (int)S8[j].size);
-  int o[3] = {(int)S8[1].o[0] - size, (int)S8[2].o[1] - size, (int)S8[4].o[2] - size};
+  // the vertex is a corner of the smallest slot around it
+  int size = S8[0].size, small = 0;
+  for (int j = 1; j < 8; j++)
+    if (S8[j].size < size) size = S8[j].size, small = j;
+  int o[3];
+  for (int r = 0; r < 3; r++) o[r] = (int)S8[small].o[r] + (((small >> r) & 1) ? 0 : size) - size;
   uint32_t L[8];
-  if (xedge) {
-    o[0] += size;
-    for (int j = 0; j < 8; j++) L[j] = S8[j ^ 1].la;
-  } else {
-    for (int j = 0; j < 8; j++) L[j] = S8[j].la;
-  }
-  emit_cell(Q, 7, xedge, o, size, L, 8);
+  for (int j = 0; j < 8; j++) L[j] = S8[j].la;
+  emit_cell(Q, 7, 0, o, size, L, 8);
 }
 
 __device__ void edge_item(const GenCtx &g, const GenQueues &Q, const Slot *S4, int e, int nb) {
@@ -188,13 +183,14 @@ __device__ void edge_item(const GenCtx &g, const GenQueues &Q, const Slot *S4, i
   int p, q;
   others(e, p, q);
   if (!any) {
+    // the edge line runs along a side of the smallest slot
     int size = S4[0].size, small = 0;
     for (int j = 1; j < 4; j++)
       if (S4[j].size < size) size = S4[j].size, small = j;
     int o[3];
     o[e] = S4[small].o[e];
-    o[p] = (int)S4[1].o[p] - size;
-    o[q] = (int)S4[2].o[q] - size;
+    o[p] = (int)S4[small].o[p] + ((small & 1) ? 0 : size) - size;
+    o[q] = (int)S4[small].o[q] + ((small & 2) ? 0 : size) - size;
     uint32_t L[4] = {S4[0].la, S4[1].la, S4[2].la, S4[3].la};
     emit_cell(Q, 4 + e, 0, o, size, L, 4);
     return;
@@ -210,21 +206,13 @@ __device__ void edge_item(const GenCtx &g, const GenQueues &Q, const Slot *S4, i
   }
   Slot S8[8];
   for (int j = 0; j < 8; j++) {
+    // across the edge line: the half of the slot next to the line; along the
+    // edge: the half on the vertex's own side of the midpoint
     int pj = (j >> p) & 1, qj = (j >> q) & 1, ej = (j >> e) & 1;
-    int k = (pj ? 0 : (1 << p)) | (qj ? 0 : (1 << q)) | (ej ? 0 : (1 << e));
+    int k = (pj ? 0 : (1 << p)) | (qj ? 0 : (1 << q)) | (ej ? (1 << e) : 0);
     S8[j] = ch(g, S4[pj | (qj << 1)], k);
   }
-  // the midpoint vertex is expanded at this level, as the recursion does
-  bool any8 = false;
-  for (int j = 0; j < 8; j++) any8 |= is_sub(g, S8[j]);
-  if (any8) {
-    VertItem v;
-    for (int j = 0; j < 8; j++) v.s[j] = ch(g, S8[j], 7 - j);
-    v.xedge = 0;
-    push(Q.vertq[nb], Q.count + nb * 4 + 3, Q.cap_vert, v, Q.error);
-  } else {
-    vert_item(g, Q, S8, e == 0, nb);
-  }
+  vert_item(g, Q, S8, nb);
 }
 
 __device__ void face_item(const GenCtx &g, const GenQueues &Q, const Slot &A, const Slot &B, int ax, int nb) {
@@ -272,7 +260,7 @@ __device__ void face_item(const GenCtx &g, const GenQueues &Q, const Slot &A, co
     int k = j & ~bit;
     S8[j] = ((j >> ax) & 1) ? ch(g, B, k) : ch(g, A, k | bit);
   }
-  vert_item(g, Q, S8, 0, nb);
+  vert_item(g, Q, S8, nb);
 }
 
 // one subdivided slot: its children, their 12 faces, 6 edges and centre
@@ -301,7 +289,7 @@ __device__ void cell_item(const GenCtx &g, const GenQueues &Q, const Slot *C, in
     Slot S4[4] = {C[z], C[z | 1], C[z | 2], C[z | 3]};
     edge_item(g, Q, S4, 2, nb);
   }
-  vert_item(g, Q, C, 0, nb);
+  vert_item(g, Q, C, nb);
 }
 
 // Items of level `cur` expand into level `cur ^ 1` (or emit cells).
@@ -338,7 +326,7 @@ __global__ void k_gen_level(GenCtx g, GenQueues Q, int cur, int root, uint32_t n
       edge_item(g, Q, e.s, e.axis, nb);
     } else {
       const VertItem v = Q.vertq[cur][i - nc - nf - ne];
-      vert_item(g, Q, v.s, v.xedge, nb);
+      vert_item(g, Q, v.s, nb);
     }
   }
 }
@@ -926,10 +914,7 @@ __global__ void k_mark_dirty(const Cell *cells, uint32_t n, const Cell *old_cell
       break;
     }
   }
-  // a quirk corner samples voxels outside its own leaves (the reference's
-  // shifted bookkeeping puts a sample beyond its brick), so it is re-meshed
-  // every time
-  bool d = found < 0 || c.quirk;
+  bool d = found < 0;
   const int nl = c.type == 0 ? 1 : (c.type <= 3 ? 2 : (c.type <= 6 ? 4 : 8));
   for (int k = 0; k < nl && !d; k++) {
     int guard = 0;

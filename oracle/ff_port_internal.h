@@ -6,7 +6,7 @@
 
 typedef struct {
   int type;  /* 0 interior, 1-3 wall x/y/z, 4-6 edge x/y/z, 7 corner */
-  int quirk; /* corner of a split x-edge with the reference's x-mirrored bookkeeping */
+  int quirk; /* always 0; kept so that rows keep their layout */
   int o[3];
   int size;
   uint32_t L[8]; /* lastLeaf of each side */

@@ -11,10 +11,8 @@
  * edge, one corner cell per eight slots around a vertex, each as large as
  * the smallest slot it touches.  A cell side refers to the finest leaf at or
  * above its slot (lastLeaf).  This file enumerates those cells directly from
- * the octree with the recursive cell/face/edge/vertex traversal, and carries
- * one bookkeeping quirk of the reference: a corner cell created at the
- * midpoint of a split x-edge has its x origin one cell size too far and its
- * x-pairs of leaves swapped.
+ * the octree with the recursive cell/face/edge/vertex traversal; the result is
+ * the reference's cell set, cell for cell.
  *
  * Per-cell meshing restates addBrickInterior_indexed_incremental_optimized,
  * addBrickWallX/Y/Z_, addBrickEdgeX/Y/Z_ and addBrickMiddle_indexed_incremental
@@ -153,7 +151,7 @@ static slot_t child_of(const enum_ctx *c, const slot_t *s, int co) {
 
 static slot_t ch(const enum_ctx *c, const slot_t *s, int co) { return is_sub(c, s) ? child_of(c, s, co) : *s; }
 
-static void emit(enum_ctx *c, int type, int quirk, const int *o, int size, const uint32_t *L, int nl) {
+static void emit(enum_ctx *c, int type, const int *o, int size, const uint32_t *L, int nl) {
   for (int k = 0; k < nl; k++)
     if (L[k] >= BRANCHINIT) return; /* never meshed: some side has no leaf */
   if (c->n == c->cap) {
@@ -162,33 +160,30 @@ static void emit(enum_ctx *c, int type, int quirk, const int *o, int size, const
   }
   ffp_cell *e = &c->cells[c->n++];
   e->type = type;
-  e->quirk = quirk;
+  e->quirk = 0;
   for (int r = 0; r < 3; r++) e->o[r] = o[r];
   e->size = size;
   for (int k = 0; k < 8; k++) e->L[k] = k < nl ? L[k] : BRANCHINIT;
 }
 
-static void vert_proc(enum_ctx *c, const slot_t *S8, int from_xedge) {
+static void vert_proc(enum_ctx *c, const slot_t *S8) {
   int any = 0;
   for (int j = 0; j < 8; j++) any |= is_sub(c, &S8[j]);
   if (any) {
     slot_t T[8];
     for (int j = 0; j < 8; j++) T[j] = ch(c, &S8[j], 7 - j);
-    vert_proc(c, T, 0);
+    vert_proc(c, T);
     return;
   }
-  int size = S8[0].size;
+  /* the vertex is a corner of the smallest slot around it */
+  int size = S8[0].size, small = 0;
   for (int j = 1; j < 8; j++)
-    if (S8[j].size < size) size = S8[j].size;
-  int o[3] = {S8[1].o[0] - size, S8[2].o[1] - size, S8[4].o[2] - size};
+    if (S8[j].size < size) size = S8[j].size, small = j;
+  int o[3];
+  for (int r = 0; r < 3; r++) o[r] = S8[small].o[r] + (((small >> r) & 1) ? 0 : size) - size;
   uint32_t L[8];
-  if (from_xedge) {
-    o[0] += size;
-    for (int j = 0; j < 8; j++) L[j] = S8[j ^ 1].la;
-  } else {
-    for (int j = 0; j < 8; j++) L[j] = S8[j].la;
-  }
-  emit(c, 7, from_xedge, o, size, L, 8);
+  for (int j = 0; j < 8; j++) L[j] = S8[j].la;
+  emit(c, 7, o, size, L, 8);
 }
 
 /* the two axes other than e, ascending */
@@ -207,12 +202,13 @@ static void edge_proc(enum_ctx *c, const slot_t *S4, int e) {
     int size = S4[0].size, small = 0;
     for (int j = 1; j < 4; j++)
       if (S4[j].size < size) size = S4[j].size, small = j;
+    /* the edge line runs along a side of the smallest slot */
     int o[3];
     o[e] = S4[small].o[e];
-    o[p] = S4[1].o[p] - size;
-    o[q] = S4[2].o[q] - size;
+    o[p] = S4[small].o[p] + ((small & 1) ? 0 : size) - size;
+    o[q] = S4[small].o[q] + ((small & 2) ? 0 : size) - size;
     uint32_t L[4] = {S4[0].la, S4[1].la, S4[2].la, S4[3].la};
-    emit(c, 4 + e, 0, o, size, L, 4);
+    emit(c, 4 + e, o, size, L, 4);
     return;
   }
   for (int half = 0; half < 2; half++) {
@@ -226,10 +222,12 @@ static void edge_proc(enum_ctx *c, const slot_t *S4, int e) {
   slot_t S8[8];
   for (int j = 0; j < 8; j++) {
     int pj = (j >> p) & 1, qj = (j >> q) & 1, ej = (j >> e) & 1;
-    int k = (pj ? 0 : (1 << p)) | (qj ? 0 : (1 << q)) | (ej ? 0 : (1 << e));
+    /* across the edge line: the half of the slot next to the line; along
+     * the edge: the half on the vertex's own side of the midpoint */
+    int k = (pj ? 0 : (1 << p)) | (qj ? 0 : (1 << q)) | (ej ? (1 << e) : 0);
     S8[j] = ch(c, &S4[pj | (qj << 1)], k);
   }
-  vert_proc(c, S8, e == 0);
+  vert_proc(c, S8);
 }
 
 static void face_proc(enum_ctx *c, const slot_t *A, const slot_t *B, int ax) {
@@ -239,7 +237,7 @@ static void face_proc(enum_ctx *c, const slot_t *A, const slot_t *B, int ax) {
     int o[3] = {small->o[0], small->o[1], small->o[2]};
     o[ax] = B->o[ax] - size;
     uint32_t L[2] = {A->la, B->la};
-    emit(c, 1 + ax, 0, o, size, L, 2);
+    emit(c, 1 + ax, o, size, L, 2);
     return;
   }
   int bit = 1 << ax, u, v;
@@ -272,7 +270,7 @@ static void face_proc(enum_ctx *c, const slot_t *A, const slot_t *B, int ax) {
     int k = j & ~bit;
     S8[j] = ((j >> ax) & 1) ? ch(c, B, k) : ch(c, A, k | bit);
   }
-  vert_proc(c, S8, 0);
+  vert_proc(c, S8);
 }
 
 static void cell_children(enum_ctx *c, const slot_t *C) {
@@ -286,7 +284,7 @@ static void cell_children(enum_ctx *c, const slot_t *C) {
       cell_children(c, T);
     } else {
       uint32_t L[1] = {C[j].la};
-      emit(c, 0, 0, C[j].o, C[j].size, L, 1);
+      emit(c, 0, C[j].o, C[j].size, L, 1);
     }
   }
   for (int i = 0; i < 4; i++) face_proc(c, &C[FX[i][0]], &C[FX[i][1]], 0);
@@ -304,7 +302,7 @@ static void cell_children(enum_ctx *c, const slot_t *C) {
     slot_t S4[4] = {C[z], C[z | 1], C[z | 2], C[z | 3]};
     edge_proc(c, S4, 2);
   }
-  vert_proc(c, C, 0);
+  vert_proc(c, C);
 }
 
 static uint64_t cell_key(const ffp_cell *e) {

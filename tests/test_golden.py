@@ -3,9 +3,8 @@
 
 * traversal: per frame, the volume, offset, number of leaves and the set of
   updated bricks, and the final leaf table -- exactly;
-* meshing: for every mesh cell the oracle and the reference both have, the
-  cell's mesh (vertex bits, colours, faces) -- exactly, from the same voxel
-  state;
+* meshing: the set of mesh cells, and every cell's mesh (vertex bits,
+  colours, faces) -- exactly, from the same voxel state;
 * the marching-cubes triangle table of the product equals the reference's.
 """
 import hashlib
@@ -76,14 +75,11 @@ def test_mesh_cells_match_reference(fix, port_run):
     for row, dg in zip(fix["cells"], fix["cell_digest"]):
         t = int(row[0])
         refc[(t, int(row[1]), int(row[2]), int(row[3]), int(row[4]), tuple(int(x) for x in row[5:5 + NEED[t]]))] = dg
-    common = set(mine) & set(refc)
-    # the reference's incremental bookkeeping places a few edge/corner cells
-    # differently (history-dependent); everything else is the same cell set
-    assert len(common) >= 0.97 * len(refc)
-    bad = [k for k in common if mine[k] != refc[k]]
-    assert not bad, f"{len(bad)} of {len(common)} common cells mesh differently, e.g. {bad[:3]}"
-    only = (set(mine) ^ set(refc))
-    assert all(k[0] in (4, 5, 6, 7) for k in only)
+    # the same cells (type, origin, size, side leaves) ...
+    assert set(mine) == set(refc)
+    # ... each with the same mesh
+    bad = [k for k in refc if mine[k] != refc[k]]
+    assert not bad, "%d of %d cells mesh differently, e.g. %s" % (len(bad), len(refc), bad[:3])
 
 
 def _product_table():

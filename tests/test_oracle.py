@@ -82,5 +82,5 @@ def test_meshing_cells_match_reference_live(port_lib):
         v0, nv, f0, nf = ranges[i]
         n_same += (rx.shape[0] == nv and rf.shape[0] == nf and np.array_equal(rx.view(np.uint32), xyz[v0:v0 + nv].view(np.uint32))
                    and np.array_equal(rc, rgb[v0:v0 + nv]) and np.array_equal(rf, faces[f0:f0 + nf] - v0))
-    assert n_common >= 0.97 * len(refmap)
+    assert n_common == len(refmap) == len(cells)
     assert n_same == n_common
