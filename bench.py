@@ -1,0 +1,524 @@
+"""Throughput of the fusion + incremental-meshing path on B200.
+
+Workload (one map per GPU): 640x480 uint16 depth + BGR8 frames of a seeded
+8x8x3 m room with 80 boxes/spheres, rendered along a seeded random walk
+(2 cm steps, 2 degree yaw jitter, 1.2 m height; fx=fy=525).  Fusion at 5 mm
+voxels, 10 mm truncation, 4 m maximum camera distance, 8^3 bricks, FP32
+storage; incremental meshing every 10 frames.  One step = 10 addMap calls
+plus one updateMeshes.  The default run (3 warm-up + 97 timed steps) covers
+the 1000-frame walk.
+
+Reported (one JSON line from rank 0):
+  value      frames/s over all ranks, depth/BGR already in HBM (ff_add_map_u16_device)
+  e2e        the same through the host API (ff_add_map_u16 from pinned host
+             memory, ff_update_meshes, and the whole mesh copied back to the host
+             every step)
+  roofline   the dominant stage's algorithmic bytes / CUDA-event time vs the
+             measured HBM copy bandwidth
+  cpu_baseline  the reference's FusionMipMapCPU (compiled from its sources) on
+             one host core over a bounded prefix of the same frames
+
+`--impl reference` times the reference's CPU implementation instead: one map
+per host core (all cores the box gives this process, bounded by host memory),
+each running the same frames, aggregated frames/s.
+
+Multi-GPU (`torchrun --nproc-per-node N bench.py --gpus N`): every rank fuses
+its own independent map (walk seed = rank); no data-path collective; weak
+scaling; the timed region is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+FRAMES_PER_STEP = 10
+WIDTH, HEIGHT = 640, 480
+SCALING = 1.0 / 5000.0
+MAXCAM = 4.0
+VOXEL = 0.005
+THRESHOLD = 0.01
+METRIC = "depth frames/s fused+meshed (640x480, 5 mm)"
+UNIT = "frames/s"
+FALLBACK_HBM_GBS = 6650.0
+L2_FLUSH_BYTES = 256 << 20
+CPU_SAMPLE_SECONDS = 20.0
+
+# stage -> kernels it times (for the roofline record)
+STAGE_KERNELS = {
+    "project": "k_project",
+    "dedupe": "k_dedupe",
+    "insert": "k_insert",
+    "finalize": "k_pending_keys+radix sort+k_finalize+k_parents",
+    "fuse": "k_fuse",
+    "mesh_cells": "k_gen_level+k_cell_keys+radix sort+k_gather_cells",
+    "mesh_count": "k_mesh_lattice<count>+k_mesh_corner<count>",
+    "mesh_emit": "k_mesh_lattice<emit>+k_mesh_corner<emit>+k_copy_clean",
+}
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=97)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--storage", choices=["fp32", "fp16"], default="fp32")
+    ap.add_argument("--rcp", choices=["host", "exact"], default="host")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workers", type=int, default=0, help="reference arm: maps in parallel (0 = all cores)")
+    a = ap.parse_args(argv)
+    if a.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    if a.steps < 1:
+        ap.error("--steps must be at least 1")
+    return a
+
+
+def n_frames_needed(a) -> int:
+    return (a.warmup + a.steps) * FRAMES_PER_STEP
+
+
+def make_sequence(seed: int, n_frames: int):
+    from fastfusion_b200.scene import room_walk_sequence
+    # the scene keeps its primitives clear of the whole trajectory, so the
+    # trajectory length is fixed at 1000 frames unless more are needed
+    return room_walk_sequence(seed, n_frames=max(1000, n_frames), width=WIDTH, height=HEIGHT)
+
+
+def render_frames(seq, n_frames: int, device):
+    """All frames as device tensors: depth int16 [F,H,W] (uint16 bits), bgr uint8 [F,H,W,3]."""
+    import torch
+    from fastfusion_b200.scene import render_torch
+    depth = torch.empty((n_frames, HEIGHT, WIDTH), dtype=torch.int16, device=device)
+    bgr = torch.empty((n_frames, HEIGHT, WIDTH, 3), dtype=torch.uint8, device=device)
+    for k in range(n_frames):
+        R, t = seq.poses[k]
+        d, c = render_torch(seq.scene, R, t, WIDTH, HEIGHT, seq.K, seq.seed, k, device=device)
+        depth[k].copy_(d)
+        bgr[k].copy_(c)
+    return depth, bgr
+
+
+def workload_config(a, n_frames: int) -> dict:
+    return {
+        "workload": f"walk{n_frames}: 8x8x3 m room, 80 primitives, {n_frames} frames 640x480 along a seeded "
+                    f"random walk, voxel 5 mm, threshold 10 mm, maxcam 4 m, 8^3 bricks, updateMeshes every "
+                    f"{FRAMES_PER_STEP} frames",
+        "frames": n_frames,
+        "frames_per_step": FRAMES_PER_STEP,
+        "width": WIDTH,
+        "height": HEIGHT,
+        "voxel_m": VOXEL,
+        "threshold_m": THRESHOLD,
+        "maxcam_m": MAXCAM,
+        "storage": a.storage,
+        "rcp": a.rcp,
+        "seed": a.seed,
+        "l2": "flushed between timed steps (256 MB write)",
+    }
+
+
+# -- clocks ---------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi samples of the SM clock and throttle reasons (every 200 ms)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: str):
+        self.path = tempfile.mktemp(prefix="ffclk_", suffix=".csv")
+        self.f = open(self.path, "w")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", gpu_index, f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict | None:
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+            self.p.wait()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def measured_hbm_peak():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            v = float(json.load(f)["hbm_gbs"])
+        return v, "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def read_traffic_table() -> dict:
+    """Per-brick / per-sample DRAM traffic from the committed ncu summaries
+    (lines `traffic <stage> <bytes per unit> <unit>`)."""
+    out = {}
+    p = os.path.join(HERE, "profiles", "traffic.txt")
+    if not os.path.exists(p):
+        return out
+    with open(p) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) >= 4 and parts[0] == "traffic":
+                out[parts[1]] = (float(parts[2]), parts[3])
+    return out
+
+
+# -- the B200 arm ------------------------------------------------------------------
+def run_b200(a):
+    import torch
+    import torch.distributed as dist
+    from fastfusion_b200 import fusion as ff
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != a.gpus:
+        raise SystemExit(f"--gpus {a.gpus} but WORLD_SIZE={world}")
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    nf = n_frames_needed(a)
+    seq = make_sequence(a.seed + rank, nf)
+    depth, bgr = render_frames(seq, nf, dev)
+    cams = [ff.CameraInfo(seq.K, *seq.poses[k]) for k in range(nf)]
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize(dev)
+
+    def new_map():
+        m = ff.FusionMipMapCPU(0, 0, 0, VOXEL, THRESHOLD, 0, True, device=local, storage=a.storage, rcp=a.rcp)
+        m.set_stream(stream.cuda_stream)
+        return m
+
+    def device_step(m, s):
+        for k in range(s * FRAMES_PER_STEP, (s + 1) * FRAMES_PER_STEP):
+            m.addMapDevice(depth[k].data_ptr(), bgr[k].data_ptr(), WIDTH, HEIGHT, cams[k], SCALING, MAXCAM)
+        m.updateMeshes()
+
+    def timed(step_fn, m, on_timed_start=None):
+        """W untimed steps, then K steps timed one by one with CUDA events
+        (L2 flushed before each); returns (device ms summed, wall s)."""
+        for s in range(a.warmup):
+            step_fn(m, s)
+        if on_timed_start:
+            on_timed_start(m)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+        torch.cuda.synchronize(dev)
+        barrier()
+        torch.cuda.synchronize(dev)
+        w0 = time.perf_counter()
+        for i in range(a.steps):
+            flush.fill_(i)
+            ev[i][0].record(stream)
+            step_fn(m, a.warmup + i)
+            ev[i][1].record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        torch.cuda.synchronize(dev)
+        wall = time.perf_counter() - w0
+        return sum(e0.elapsed_time(e1) for e0, e1 in ev), wall
+
+    gpu_index = os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[local] if \
+        os.environ.get("CUDA_VISIBLE_DEVICES") else str(local)
+    clk = ClockSampler(gpu_index) if rank == 0 else None
+
+    # 1. device-resident throughput
+    m = new_map()
+    launches = {}
+
+    def mark(mm):
+        launches["own0"], launches["lib0"] = ff.kernel_launches()
+
+    dev_ms, dev_wall = timed(device_step, m, mark)
+    own1, lib1 = ff.kernel_launches()
+    gpu_launches, lib_calls = own1 - launches["own0"], lib1 - launches["lib0"]
+    st = m.stats()
+    m.close()
+    del m
+
+    # 2. per-stage profile of the same steps (separate map; events per stage)
+    m = new_map()
+    prof_ms, _ = timed(device_step, m, lambda mm: mm.profile(True))
+    stages = m.profile_read()
+    m.close()
+    del m
+
+    # 3. end to end through the host API
+    e2e = None
+    rms = None
+    if not a.no_e2e:
+        h_depth = depth.cpu().pin_memory()
+        h_bgr = bgr.cpu().pin_memory()
+        hd = h_depth.numpy().view(np.uint16)
+        hb = h_bgr.numpy()
+        d2h = []
+        last_mesh = {}
+
+        def host_step(mm, s):
+            for k in range(s * FRAMES_PER_STEP, (s + 1) * FRAMES_PER_STEP):
+                mm.addMap(hd[k], cams[k], hb[k], SCALING, MAXCAM)
+            mm.updateMeshes()
+            mesh = mm.getMeshInterleavedMarchingCubes()
+            d2h.append(mesh.vertices.nbytes + mesh.colors.nbytes + mesh.faces.nbytes)
+            last_mesh["m"] = mesh
+
+        m = new_map()
+        e2e_ms, _ = timed(host_step, m, lambda mm: d2h.clear())
+        m.close()
+        del m
+        e2e_ms = max_over_ranks(e2e_ms)
+        e2e = {"value": sum_over_ranks(a.steps * FRAMES_PER_STEP) / (e2e_ms / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": FRAMES_PER_STEP * (WIDTH * HEIGHT * 2 + WIDTH * HEIGHT * 3),
+               "d2h_bytes_per_step": int(np.mean(d2h)) if d2h else 0,
+               "ms_per_step": e2e_ms / a.steps}
+        if rank == 0 and "m" in last_mesh and len(last_mesh["m"].vertices):
+            v = last_mesh["m"].vertices
+            rng = np.random.default_rng(0)
+            sel = rng.choice(len(v), size=min(len(v), 300000), replace=False)
+            rms = float(np.sqrt(np.mean(seq.scene.sdf(v[sel].astype(np.float64)) ** 2)))
+    clocks = clk.stop() if clk else None
+
+    dev_ms_max = max_over_ranks(dev_ms)
+    frames_all = sum_over_ranks(a.steps * FRAMES_PER_STEP)
+    value = frames_all / (dev_ms_max / 1e3)
+
+    # roofline of the dominant stage
+    peak, peak_kind = measured_hbm_peak()
+    dom = max(stages, key=lambda k: stages[k][0])
+    ms_d, bytes_d, n_d = stages[dom]
+    achieved = bytes_d / (ms_d / 1e3) / 1e9 if ms_d > 0 else 0.0
+    traffic = None
+    tt = read_traffic_table()
+    if dom in tt and n_d:
+        per_unit, unit = tt[dom]
+        unit_bytes = {"brick": 14336.0 if a.storage == "fp32" else 10240.0}.get(unit)
+        if unit_bytes:
+            traffic = per_unit * (bytes_d / unit_bytes) / n_d
+    roofline = {"bound": "hbm", "kernel": STAGE_KERNELS[dom], "stage": dom, "achieved": round(achieved, 1),
+                "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "peak_source": f"{peak_kind} (copy bandwidth)",
+                "algorithmic_bytes_per_launch": bytes_d / n_d if n_d else 0, "launches": n_d,
+                "avg_launch_us": 1e3 * ms_d / n_d if n_d else 0, "traffic": traffic}
+    stage_rec = {k: {"ms": round(v[0], 3), "share": round(v[0] / prof_ms, 4) if prof_ms else 0,
+                     "GB/s": round(v[1] / (v[0] / 1e3) / 1e9, 1) if v[0] > 0 else 0, "launches": v[2]}
+                 for k, v in stages.items()}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(depth, bgr, seq, a)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(dev_ms_max / a.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if a.storage == "fp32" else "f16-storage/f32",
+            "data": "synthetic: seeded room scene rendered to depth+BGR on the GPU (the TUM RGB-D sequences "
+                    "the reference documents are not available offline)",
+            "config": dict(workload_config(a, n_frames_needed(a)), parallelism=f"independent maps x{world}"),
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": gpu_launches,
+            "library_calls": lib_calls, "clocks": clocks, "stages": stage_rec,
+            "wall_s_timed": round(dev_wall, 3), "surface_rms_m": rms,
+            "map": {"leaves": st["leaves_used"], "leaves_max": st["leaves_max"], "n": st["n"],
+                    "mesh_vertices": st["mesh_vertices"], "mesh_faces": st["mesh_faces"],
+                    "mesh_cells": st["mesh_cells"], "grows": st["grows"], "meshing_ok": st["meshing_ok"]},
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# -- CPU baseline (oracle side: the reference compiled from its sources) --------------
+def _cpu_impl():
+    from oracle import ref
+    if ref.available():
+        return "reference", ref
+    return "port", None
+
+
+def cpu_baseline(depth, bgr, seq, a) -> dict:
+    """The reference on one core over a bounded prefix of the same steps."""
+    kind, ref = _cpu_impl()
+    steps_max = a.warmup + a.steps
+    hd = depth.cpu().numpy().view(np.uint16)
+    hb = bgr.cpu().numpy()
+    if kind == "reference":
+        m = ref.RefFusion(VOXEL, THRESHOLD, True)
+        add = lambda k: m.add_map(hd[k], hb[k], seq.K, *seq.poses[k], SCALING, MAXCAM)
+        upd = m.update_meshes
+    else:
+        from oracle.port import PortFusion
+        m = PortFusion(update_mode=2)
+        add = lambda k: m.add_map(hd[k], hb[k], seq.K, *seq.poses[k], SCALING, MAXCAM)
+        upd = m.update_meshes
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < steps_max and time.perf_counter() - t0 < CPU_SAMPLE_SECONDS:
+        for k in range(steps * FRAMES_PER_STEP, (steps + 1) * FRAMES_PER_STEP):
+            add(k)
+        upd()
+        steps += 1
+    el = time.perf_counter() - t0
+    if kind == "reference":
+        m.close()
+    return {"value": round(steps * FRAMES_PER_STEP / el, 3), "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"first {steps} steps ({steps * FRAMES_PER_STEP} frames + {steps} updateMeshes) of the "
+                      f"same walk on one host core, {el:.1f} s"}
+
+
+# -- the reference arm ------------------------------------------------------------
+def _ref_worker(args):
+    (idx, dpath, bpath, K, poses, warmup, steps, barrier, q) = args
+    import numpy as np  # noqa: F811
+    from oracle import ref as refmod
+    hd = np.load(dpath, mmap_mode="r")
+    hb = np.load(bpath, mmap_mode="r")
+    if refmod.available():
+        m = refmod.RefFusion(VOXEL, THRESHOLD, True)
+        add = lambda k: m.add_map(np.asarray(hd[k]), np.asarray(hb[k]), K, *poses[k], SCALING, MAXCAM)
+    else:
+        from oracle.port import PortFusion
+        m = PortFusion(update_mode=2)
+        add = lambda k: m.add_map(np.asarray(hd[k]), np.asarray(hb[k]), K, *poses[k], SCALING, MAXCAM)
+    for s in range(warmup):
+        for k in range(s * FRAMES_PER_STEP, (s + 1) * FRAMES_PER_STEP):
+            add(k)
+        m.update_meshes()
+    barrier.wait()
+    t0 = time.perf_counter()
+    for s in range(warmup, warmup + steps):
+        for k in range(s * FRAMES_PER_STEP, (s + 1) * FRAMES_PER_STEP):
+            add(k)
+        m.update_meshes()
+    q.put((idx, time.perf_counter() - t0))
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    import torch
+    kind, _ = _cpu_impl()
+    nf = n_frames_needed(a)
+    seq = make_sequence(a.seed, nf)
+    device = "cuda" if torch.cuda.is_available() else "cpu"
+    depth, bgr = render_frames(seq, nf, device)
+    tmp = tempfile.mkdtemp(prefix="ffref_")
+    dpath, bpath = os.path.join(tmp, "depth.npy"), os.path.join(tmp, "bgr.npy")
+    np.save(dpath, depth.cpu().numpy().view(np.uint16))
+    np.save(bpath, bgr.cpu().numpy())
+    del depth, bgr
+    cores = len(os.sched_getaffinity(0))
+    try:
+        import psutil
+        mem_maps = int(psutil.virtual_memory().available // (3 << 30))
+    except ImportError:
+        mem_maps = cores
+    workers = a.workers or max(1, min(cores, mem_maps))
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(workers)
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_ref_worker, args=((i, dpath, bpath, seq.K, seq.poses[:nf], a.warmup, a.steps,
+                                                    barrier, q),)) for i in range(workers)]
+    for p in procs:
+        p.start()
+    times = [q.get() for _ in procs]
+    for p in procs:
+        p.join()
+    for f in (dpath, bpath):
+        os.unlink(f)
+    os.rmdir(tmp)
+    wall = max(t for _, t in times)
+    value = workers * a.steps * FRAMES_PER_STEP / wall
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(1e3 * wall / a.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: same frames as the B200 arm",
+        "config": dict(workload_config(a, nf), parallelism=f"{workers} independent maps on {workers} host cores"),
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": workers, "kind": kind,
+                         "sample": f"{workers} maps in parallel, each {a.steps} timed steps after {a.warmup} "
+                                   f"warm-up steps of the walk"},
+        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main(argv=None):
+    a = parse_args(argv)
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_b200(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -62,6 +62,7 @@ __global__ void k_first_bbox(const uint16_t *depth, int W, int H, CamF p, float 
 void launch_first_bbox(const uint16_t *depth, int W, int H, const CamF &p, float scaling, float maxcam, int bw,
                        Counters *cnt, cudaStream_t s) {
   int n = W * H;
+  note_launch();
   k_first_bbox<<<(n + 255) / 256, 256, 0, s>>>(depth, W, H, p, scaling, maxcam, bw, cnt);
 }
 
@@ -100,6 +101,7 @@ __global__ void k_project(const uint16_t *depth, int W, int H, const float *pxp,
 void launch_project(const uint16_t *depth, int W, int H, const float *pxp, const float *pyp, const CamF &p,
                     float scaling, float maxcam, int4 *vox, cudaStream_t s) {
   int n = W * H;
+  note_launch();
   k_project<<<(n + 255) / 256, 256, 0, s>>>(depth, W, H, pxp, pyp, p, scaling, maxcam, vox);
 }
 
@@ -251,6 +253,7 @@ cudaError_t launch_dedupe(const int4 *vox, int W, int H, int4 *bnd, uint8_t *pro
   if (blocks < 1) blocks = 1;
   void *args[] = {(void *)&vox, (void *)&W, (void *)&H, (void *)&tilesX, (void *)&tilesY, (void *)&bnd,
                   (void *)&processed, (void *)&cnt, (void *)&barrier};
+  note_launch();
   return cudaLaunchCooperativeKernel((const void *)k_dedupe, dim3(blocks), dim3(threads), args, 0, s);
 }
 
@@ -373,6 +376,7 @@ void launch_insert(const int4 *vox, const uint8_t *processed, int W, int H, uint
                    uint32_t leaves_max, uint32_t branches_max, uint32_t frame, uint32_t *stamp, uint32_t *queue,
                    PendingLeaf *pend, uint32_t pend_cap, Counters *cnt, cudaStream_t s) {
   int npix = W * H;
+  note_launch();
   k_insert<<<(npix + 255) / 256, 256, 0, s>>>(vox, processed, npix, n, bw, tree, leaves_max, branches_max, frame,
                                               stamp, queue, pend, pend_cap, cnt);
 }
@@ -396,7 +400,9 @@ size_t pending_sort_bytes(int n) {
 cudaError_t sort_pending(const PendingLeaf *pend, int npend, uint32_t *keys_in, uint32_t *vals_in, uint32_t *keys_out,
                          uint32_t *vals_out, void *tmp, size_t tmp_bytes, int end_bit, cudaStream_t s) {
   if (npend <= 0) return cudaSuccess;
+  note_launch();
   k_pending_keys<<<(npend + 255) / 256, 256, 0, s>>>(pend, npend, keys_in, vals_in);
+  note_lib_call();
   return cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys_in, keys_out, vals_in, vals_out, npend, 0, end_bit,
                                          s);
 }
@@ -422,6 +428,7 @@ void launch_finalize(const PendingLeaf *pend, const uint32_t *order, int npend, 
                      uint32_t leaves_max, uint32_t *tree, ushort4 *leaf, uint32_t frame, uint32_t *stamp,
                      uint32_t *queue, Counters *cnt, cudaStream_t s) {
   if (npend <= 0) return;
+  note_launch();
   k_finalize<<<(npend + 255) / 256, 256, 0, s>>>(pend, order, npend, leaves_before, leaves_max, tree, leaf, frame,
                                                  stamp, queue, cnt);
 }
@@ -456,6 +463,7 @@ __global__ void k_parents(int npend, uint32_t leaves_before, uint32_t leaves_max
 void launch_parents(int npend, uint32_t leaves_before, uint32_t leaves_max, const uint32_t *tree, uint32_t n,
                     const ushort4 *leaf, uint32_t *parent, cudaStream_t s) {
   if (npend <= 0) return;
+  note_launch();
   k_parents<<<(npend + 255) / 256, 256, 0, s>>>(npend, leaves_before, leaves_max, tree, n, leaf, parent);
 }
 
@@ -469,6 +477,7 @@ __global__ void k_shift_branches(uint32_t *tree, uint32_t used, uint32_t shift) 
 
 void launch_shift_branches(uint32_t *tree, uint32_t used, uint32_t shift, cudaStream_t s) {
   if (!used) return;
+  note_launch();
   k_shift_branches<<<(used + 255) / 256, 256, 0, s>>>(tree, used, shift);
 }
 
@@ -484,6 +493,7 @@ __global__ void k_shift_leaves(ushort4 *leaf, uint32_t n, ushort3 add) {
 
 void launch_shift_leaves(ushort4 *leaf, uint32_t n, ushort3 add, cudaStream_t s) {
   if (!n) return;
+  note_launch();
   k_shift_leaves<<<(n + 255) / 256, 256, 0, s>>>(leaf, n, add);
 }
 
@@ -497,6 +507,7 @@ void launch_fill(uint32_t *p, size_t n, uint32_t v, cudaStream_t s) {
   if (!n) return;
   size_t blocks = (n + 255) / 256;
   if (blocks > 148 * 32) blocks = 148 * 32;
+  note_launch();
   k_fill<<<(unsigned)blocks, 256, 0, s>>>(p, n, v);
 }
 

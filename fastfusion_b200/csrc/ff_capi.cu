@@ -17,6 +17,11 @@
 #include "../../include/fastfusion_b200.h"
 #include "ff_kernels.h"
 #include "ff_mesh.h"
+#include "ff_prof.h"
+
+namespace ffb {
+std::atomic<unsigned long long> g_own_launches{0}, g_lib_calls{0};
+}
 
 using namespace ffb;
 
@@ -63,6 +68,7 @@ struct ff_handle {
   uint16_t bandwidth = 0;
 
   MeshState mesh;
+  Prof prof;
 };
 
 static thread_local std::string g_create_error;
@@ -368,6 +374,7 @@ ff_status ff_destroy(ff_handle *h) {
   cudaSetDevice(h->cfg.device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   mesh_free(h->mesh);
+  h->prof.destroy();
   void *ptrs[] = {h->d_tree, h->d_leaf, h->d_parent, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
                   h->d_stamp, h->d_queue, h->d_cnt, h->d_barrier, h->d_depth, h->d_bgr, h->d_pxp, h->d_pyp,
                   h->d_vox, h->d_proc, h->d_bnd, h->d_pend, h->d_keys, h->d_sort_tmp, h->d_rcp_tab};
@@ -446,10 +453,17 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
   // as in the reference (pInv is built before the traversal)
   CamF q = cam_grid_to_camera(h, K, R, t);
 
+  const double npix = (double)W * H;
+  int pi = h->prof.begin(ST_PROJECT, s);
   launch_project(d_depth, W, H, h->d_pxp, h->d_pyp, p, scaling, maxcam, h->d_vox, s);
+  h->prof.end(pi, npix * (2 + 16), s);  // depth in, voxel key out
+  pi = h->prof.begin(ST_DEDUPE, s);
   CK(launch_dedupe(h->d_vox, W, H, h->d_bnd, h->d_proc, h->d_cnt, h->d_barrier, h->cfg.device, s));
+  h->prof.end(pi, npix * (16 + 1), s);  // keys in, processed flags out
+  pi = h->prof.begin(ST_INSERT, s);
   launch_insert(h->d_vox, h->d_proc, W, H, h->n, h->bandwidth, h->d_tree, h->cfg.leaves_max, h->cfg.branches_max,
                 frame, h->d_stamp, h->d_queue, h->d_pend, (uint32_t)(W * H), h->d_cnt, s);
+  h->prof.end(pi, npix * (16 + 1), s);  // keys and flags in (tree walks counted below)
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(&hc, h->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -463,6 +477,7 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
   const uint32_t leaves_before = h->leaves_used;
   const uint32_t existing_queued = hc.queued;
   if (npend) {
+    pi = h->prof.begin(ST_FINALIZE, s);
     uint32_t *k_in = h->d_keys, *v_in = h->d_keys + h->cap_pix, *k_out = h->d_keys + 2 * h->cap_pix,
              *v_out = h->d_keys + 3 * h->cap_pix;
     int end_bit = 1;
@@ -471,6 +486,7 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
     launch_finalize(h->d_pend, v_out, (int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->d_leaf, frame,
                     h->d_stamp, h->d_queue, h->d_cnt, s);
     launch_parents((int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->n, h->d_leaf, h->d_parent, s);
+    h->prof.end(pi, (double)npend * (sizeof(PendingLeaf) + 8 + 4), s);
     h->leaves_used += npend;
   }
   uint32_t new_queued = 0;
@@ -483,9 +499,14 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
     ff_status st = grow(h, hc.box_min, hc.box_max);
     if (st != FF_OK) return st;
   }
+  // fuse: every voxel of every queued brick read and written: SDF, weight
+  // (4+4 B, or 2+2 B in FP16) and three 16-bit colour channels
+  const double brick_bytes = 512.0 * 2 * ((h->cfg.storage == FF_STORAGE_FP16 ? 4 : 8) + 6);
+  pi = h->prof.begin(ST_FUSE, s);
   launch_fuse(h->d_queue, (int)nq, h->d_leaf, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
               h->cfg.storage, h->cfg.leaves_max, d_depth, d_bgr, W, H, q, h->cfg.scale, h->cfg.threshold, scaling,
               maxcam, h->d_rcp_tab, s);
+  h->prof.end(pi, (double)nq * brick_bytes, s);
   CK(cudaGetLastError());
   if (h->leaves_used > h->cfg.leaves_max) h->meshing_ok = false;
   h->queued = nq;
@@ -695,10 +716,38 @@ ff_status ff_update_meshes(ff_handle *h, int *updated) {
   in.scale = h->cfg.scale;
   in.cnt = h->d_cnt;
   in.h_cnt = h->h_cnt;
+  in.prof = &h->prof;
   std::string err;
   int rc = mesh_update(h->mesh, in, h->stream, err);
   if (rc != 0) return set_err(h, (ff_status)rc, err);
   if (updated) *updated = 1;
+  return FF_OK;
+}
+
+ff_status ff_kernel_launches(uint64_t *own, uint64_t *library) {
+  if (!own || !library) return FF_ERR_BAD_ARG;
+  *own = g_own_launches.load();
+  *library = g_lib_calls.load();
+  return FF_OK;
+}
+
+ff_status ff_profile(ff_handle *h, int enable) {
+  if (!h) return FF_ERR_BAD_ARG;
+  CK(cudaSetDevice(h->cfg.device));
+  h->prof.reset();
+  h->prof.on = enable != 0;
+  return FF_OK;
+}
+
+ff_status ff_profile_read(ff_handle *h, double *ms, double *bytes, uint64_t *launches) {
+  if (!h || !ms || !bytes || !launches) return FF_ERR_BAD_ARG;
+  CK(cudaSetDevice(h->cfg.device));
+  h->prof.flush();
+  for (int i = 0; i < FF_PROFILE_STAGES; i++) {
+    ms[i] = h->prof.ms[i];
+    bytes[i] = h->prof.bytes[i];
+    launches[i] = h->prof.launches[i];
+  }
   return FF_OK;
 }
 

@@ -14,7 +14,15 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 namespace ffb {
+
+// Process-wide counts of this library's own kernel launches and of the CUB
+// (library) calls it makes, for launch accounting by callers.
+extern std::atomic<unsigned long long> g_own_launches, g_lib_calls;
+inline void note_launch(unsigned n = 1) { g_own_launches.fetch_add(n, std::memory_order_relaxed); }
+inline void note_lib_call() { g_lib_calls.fetch_add(1, std::memory_order_relaxed); }
 
 constexpr uint32_t BRANCHINIT = 0xFFFFFFFEu;  // reference definitions.h:128
 constexpr uint32_t LOCKED = 0xFFFFFFFDu;      // slot being allocated (device-internal)

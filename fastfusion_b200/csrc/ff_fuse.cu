@@ -158,6 +158,7 @@ void launch_fuse(const uint32_t *queue, int nq, const ushort4 *leaf, float *sdf,
   k_fuse<F16, RH><<<nq, 512, 0, s>>>(queue, leaf, sdf, wgt, sdf16, wgt16, col, leaves_max, depth, bgr, W, H, q, \
                                      scale, thr, scaling, maxcam, rcp_tab)
   const bool rh = rcp_tab != nullptr;
+  note_launch();
   if (storage == 1) {
     if (rh) FF_FUSE(true, true); else FF_FUSE(true, false);
   } else {

@@ -368,6 +368,7 @@ struct VoxSrc {
   uint32_t leaves_used;
   float offset[3];
   float scale;
+  unsigned long long *samples;  // count pass: voxel samples read (profiling)
 };
 
 __device__ __forceinline__ size_t vox_index(const VoxSrc &m, uint32_t leaf, uint16_t lx, uint16_t ly, uint16_t lz) {
@@ -690,6 +691,7 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
     for (int k = lane; k < 512 * 3; k += 32) W.edge_set[k] = 0;
     fit = __all_sync(0xffffffffu, fit);
     __syncwarp();
+    if (!EMIT && lane == 0) atomicAdd(m.samples, (unsigned long long)nsamp);
     if (!fit) {
       if (!EMIT && lane == 0) out[cid] = CellOut{0u, 0u};
       continue;
@@ -809,6 +811,7 @@ __global__ void k_mesh_corner(VoxSrc m, const Cell *__restrict__ cells, uint32_t
     if (!EMIT) out[cid] = CellOut{0u, 0u};
     return;
   }
+  if (!EMIT) atomicAdd(m.samples, 8ull);
   float d[8], w[8];
   uint16_t col[8][3];
   for (int k = 0; k < 8; k++) {
@@ -1079,6 +1082,7 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
     for (uint32_t h = in.n; h > 8; h >>= 1) levels++;
     int cur = 0;
     for (int lv = 0; lv < levels; lv++) {
+      note_launch(2);
       k_clear_counts<<<1, 32, 0, s>>>(I.d_count, cur ^ 1);
       k_gen_level<<<148 * 8, 128, 0, s>>>(g, Q, cur, lv == 0 ? 1 : 0, in.n);
       cur ^= 1;
@@ -1111,6 +1115,7 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
   MCK(grow_buf(I.vals_sorted, I.cap_vals2, ncells));
   MCK(grow_buf(I.cells, I.cap_cells, ncells));
   if (ncells) {
+    note_launch(2);
     k_cell_keys<<<(ncells + 255) / 256, 256, 0, s>>>(I.raw, ncells, I.keys, I.vals);
     size_t bytes = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, bytes, I.keys, I.keys_sorted, I.vals, I.vals_sorted, (int)ncells, 0, 57,
@@ -1120,6 +1125,7 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
       MCK(cudaMalloc(&I.sort_tmp, bytes));
       I.sort_tmp_bytes = bytes;
     }
+    note_lib_call();
     MCK(cub::DeviceRadixSort::SortPairs(I.sort_tmp, I.sort_tmp_bytes, I.keys, I.keys_sorted, I.vals, I.vals_sorted,
                                         (int)ncells, 0, 57, s));
     k_gather_cells<<<(ncells + 255) / 256, 256, 0, s>>>(I.raw, I.vals_sorted, ncells, I.cells);
@@ -1130,8 +1136,12 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
 int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string &err) {
   MeshImpl &I = impl(M);
   uint32_t ncells = 0;
+  Prof &P = *in.prof;
+  int pi = P.begin(ST_MESH_CELLS, s);
   int rc = generate_cells(I, in, s, ncells, err);
   if (rc) return rc;
+  // cells written by generation, then read and written by the key sort
+  P.end(pi, (double)ncells * sizeof(Cell) * 3, s);
   VoxSrc vs;
   vs.leaf = in.leaf;
   vs.parent = in.parent;
@@ -1144,6 +1154,9 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   vs.leaves_used = in.leaves_used;
   for (int r = 0; r < 3; r++) vs.offset[r] = in.offset[r];
   vs.scale = in.scale;
+  // d_count words 12-13 hold the sample counter (8-byte aligned)
+  vs.samples = reinterpret_cast<unsigned long long *>(I.d_count + 12);
+  MCK(cudaMemsetAsync(I.d_count + 12, 0, 2 * sizeof(uint32_t), s));
 
   MCK(grow_buf(I.out, I.cap_out, ncells));
   MCK(grow_buf(I.dirty, I.cap_dirty, ncells));
@@ -1157,6 +1170,7 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   MCK(cudaMemsetAsync(I.d_count + 10, 0, sizeof(uint32_t), s));
   if (ncells) {
     if (incremental) {
+      note_launch(2);
       k_mark_dirty<<<(ncells + 255) / 256, 256, 0, s>>>(I.cells, ncells, I.old_cells, I.n_old, I.old_keys, in.stamp,
                                                         in.parent, in.leaves_used, I.since, I.dirty, I.old_index,
                                                         I.d_count + 10);
@@ -1176,13 +1190,17 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
     attr_set = true;
   }
   const uint8_t *dmask = I.dirty;
+  pi = P.begin(ST_MESH_COUNT, s);
   const int lat_blocks = std::max(1, std::min<int>(148 * 8, (int)((first_corner + MESH_WARPS - 1) / MESH_WARPS)));
+  note_launch((first_corner ? 1 : 0) + (ncells > first_corner ? 1 : 0) + (ncells ? 1 : 0));
   if (first_corner)
     k_mesh_lattice<false><<<lat_blocks, 32 * MESH_WARPS, smem, s>>>(vs, I.cells, 0, first_corner, dmask, I.out,
                                                                     nullptr, nullptr, nullptr, nullptr, nullptr);
   if (ncells > first_corner)
     k_mesh_corner<false><<<(ncells - first_corner + 127) / 128, 128, 0, s>>>(
         vs, I.cells, first_corner, ncells - first_corner, dmask, I.out, nullptr, nullptr, nullptr, nullptr, nullptr);
+  const int pi_count = pi;
+  P.end(pi_count, 0.0, s);
   MCK(cudaGetLastError());
   // exclusive scans of vertex and face counts -> per-cell bases
   if (ncells) k_counts_to_arrays<<<(ncells + 255) / 256, 256, 0, s>>>(I.out, ncells, I.nv, I.nf);
@@ -1195,14 +1213,21 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
     MCK(cudaMalloc(&I.scan_tmp, bytes));
     I.scan_tmp_bytes = bytes;
   }
+  note_lib_call();
+  note_lib_call();
   MCK(cub::DeviceScan::ExclusiveSum(I.scan_tmp, I.scan_tmp_bytes, I.nv, I.vbase, (int)ncells + 1, s));
   MCK(cub::DeviceScan::ExclusiveSum(I.scan_tmp, I.scan_tmp_bytes, I.nf, I.fbase, (int)ncells + 1, s));
   uint64_t tot[2];
+  unsigned long long nsamples = 0;
   uint32_t ndirty = ncells;
   MCK(cudaMemcpyAsync(&tot[0], I.vbase + ncells, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
   MCK(cudaMemcpyAsync(&tot[1], I.fbase + ncells, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
   if (incremental) MCK(cudaMemcpyAsync(&ndirty, I.d_count + 10, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  MCK(cudaMemcpyAsync(&nsamples, I.d_count + 12, sizeof(nsamples), cudaMemcpyDeviceToHost, s));
   MCK(cudaStreamSynchronize(s));
+  // count pass: SDF, weight and colour of every sample of the dirty cells
+  const double sample_bytes = vs.fp16 ? 10.0 : 14.0;
+  P.set_bytes(pi_count, (double)nsamples * sample_bytes);
   // the previous output becomes the copy source; the new output is written fresh
   std::swap(I.old_xyz, M.d_xyz);
   std::swap(I.cap_oxyz, I.cap_xyz);
@@ -1213,6 +1238,8 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   MCK(grow_buf(M.d_xyz, I.cap_xyz, 3 * tot[0] + 3));
   MCK(grow_buf(M.d_rgb, I.cap_rgb, 3 * tot[0] + 3));
   MCK(grow_buf(M.d_faces, I.cap_faces, 3 * tot[1] + 3));
+  pi = P.begin(ST_MESH_EMIT, s);
+  note_launch((first_corner ? 1 : 0) + (ncells > first_corner ? 1 : 0) + (incremental && ncells ? 1 : 0));
   if (first_corner)
     k_mesh_lattice<true><<<lat_blocks, 32 * MESH_WARPS, smem, s>>>(vs, I.cells, 0, first_corner, dmask, I.out,
                                                                    I.vbase, I.fbase, M.d_xyz, M.d_rgb, M.d_faces);
@@ -1224,6 +1251,9 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
     k_copy_clean<<<148 * 8, 256, 0, s>>>(I.dirty, I.old_index, ncells, I.out, I.vbase, I.fbase, I.old_vbase,
                                          I.old_fbase, I.old_xyz, I.old_rgb, I.old_faces, M.d_xyz, M.d_rgb,
                                          M.d_faces);
+  // emit pass: the samples again and the whole mesh written (xyz 12 B + rgb
+  // 3 B per vertex, 12 B per face)
+  P.end(pi, (double)nsamples * sample_bytes + (double)tot[0] * 15 + (double)tot[1] * 12, s);
   MCK(cudaGetLastError());
   // keep this update's cells, counts and bases for the next one
   std::swap(I.cells, I.old_cells);
@@ -1286,6 +1316,7 @@ int mesh_copy_cells(MeshState &M, int32_t *rows, int64_t *ranges, cudaStream_t s
   MCK(cudaMallocAsync((void **)&d_rows, sizeof(int32_t) * 14 * n, s));
   MCK(cudaMallocAsync((void **)&d_ranges, sizeof(int64_t) * 4 * n, s));
   // after an update the current cells, counts and bases are the "old" set
+  note_launch();
   k_export_cells<<<(n + 255) / 256, 256, 0, s>>>(I.old_cells, I.old_out, I.old_vbase, I.old_fbase, n, d_rows,
                                                  d_ranges);
   MCK(cudaMemcpyAsync(rows, d_rows, sizeof(int32_t) * 14 * n, cudaMemcpyDeviceToHost, s));

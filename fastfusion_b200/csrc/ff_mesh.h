@@ -8,6 +8,7 @@
 #include <string>
 
 #include "ff_common.cuh"
+#include "ff_prof.h"
 
 namespace ffb {
 
@@ -28,6 +29,7 @@ struct MeshInputs {
   float scale;
   Counters *cnt;
   Counters *h_cnt;
+  Prof *prof;
 };
 
 struct MeshState {

@@ -73,6 +73,9 @@ SIGNATURES = {
     "ff_set_bricks": (_i32, [_vp, _u32, _u32, _vp, _vp, _vp]),
     "ff_get_tree": (_i32, [_vp, _vp]),
     "ff_set_state": (_i32, [_vp, _u32, _vp, _vp, _u32, _vp, _vp, _vp, _u32, _vp, _vp, _vp]),
+    "ff_profile": (_i32, [_vp, _i32]),
+    "ff_kernel_launches": (_i32, [ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
+    "ff_profile_read": (_i32, [_vp, _vp, _vp, _vp]),
     "ff_last_error": (ctypes.c_char_p, [_vp]),
     "ff_version": (ctypes.c_char_p, []),
 }
@@ -225,6 +228,22 @@ class FusionMipMapCPU:
     def set_stream(self, stream_ptr: int | None):
         self._check(self._L.ff_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)))
 
+    # -- profiling ----------------------------------------------------------
+    PROFILE_STAGES = ("project", "dedupe", "insert", "finalize", "fuse", "mesh_cells", "mesh_count", "mesh_emit")
+
+    def profile(self, enable: bool = True):
+        """Reset the per-stage CUDA-event profile and switch it on or off."""
+        self._check(self._L.ff_profile(self._h, 1 if enable else 0))
+
+    def profile_read(self) -> dict:
+        """{stage: (milliseconds, algorithmic bytes, launches)} summed since profile()."""
+        k = len(self.PROFILE_STAGES)
+        ms = np.zeros(k, np.float64)
+        by = np.zeros(k, np.float64)
+        n = np.zeros(k, np.uint64)
+        self._check(self._L.ff_profile_read(self._h, _p(ms), _p(by), _p(n)))
+        return {name: (float(ms[i]), float(by[i]), int(n[i])) for i, name in enumerate(self.PROFILE_STAGES)}
+
     # -- inspection ---------------------------------------------------------
     def stats(self) -> dict:
         s = ff_stats()
@@ -286,3 +305,13 @@ class FusionMipMapCPU:
 
 def version() -> str:
     return load_library().ff_version().decode()
+
+
+def kernel_launches() -> tuple[int, int]:
+    """(own kernel launches, CUB calls) of this process since the library loaded."""
+    L = load_library()
+    own, lib = ctypes.c_uint64(), ctypes.c_uint64()
+    r = L.ff_kernel_launches(ctypes.byref(own), ctypes.byref(lib))
+    if r:
+        raise FFError(r, "ff_kernel_launches failed")
+    return own.value, lib.value

@@ -257,3 +257,72 @@ def room_walk_sequence(seed: int = 0, n_frames: int = 1000, width: int = 640, he
 
     scene = make_scene(seed, room=room, n_prims=n_prims, keep_clear=clear)
     return Sequence(scene=scene, K=K, width=width, height=height, poses=poses, seed=seed)
+
+
+def render_torch(scene: Scene, R, t, width: int, height: int, K, seed: int, frame: int, device="cuda",
+                 noise_k: float = 0.0012, hole_frac: float = 0.02):
+    """render() on a torch device in FP64 (same geometry and colour rules;
+    noise and holes from a torch generator seeded by (seed, frame)).
+    Returns (depth uint16 [H,W], bgr uint8 [H,W,3]) as device tensors."""
+    import torch
+    dev = torch.device(device)
+    f64 = torch.float64
+    fx, fy, cx, cy = (float(v) for v in K)
+    xs = (torch.arange(width, dtype=f64, device=dev) - cx) / fx
+    ys = (torch.arange(height, dtype=f64, device=dev) - cy) / fy
+    dcam = torch.stack(torch.broadcast_tensors(xs[None, :], ys[:, None], torch.ones(height, width, dtype=f64,
+                                                                                   device=dev)), -1).reshape(-1, 3)
+    Rt = torch.as_tensor(np.asarray(R), dtype=f64, device=dev)
+    o = torch.as_tensor(np.asarray(t), dtype=f64, device=dev)
+    d = dcam @ Rt.T
+    room = torch.as_tensor(scene.room, dtype=f64, device=dev)
+    inv = 1.0 / d
+    ta = (0.0 - o[None, :]) * inv
+    tb = (room[None, :] - o[None, :]) * inv
+    texit = torch.where(torch.isfinite(ta), torch.maximum(ta, tb), torch.full_like(ta, float("inf")))
+    tbest, axis = torch.min(texit, dim=1)
+    side = (d.gather(1, axis[:, None])[:, 0] > 0).long()
+    wall = torch.as_tensor(scene.wall_rgb, dtype=torch.uint8, device=dev)
+    colour = wall[2 * axis + side]
+    if len(scene.box_lo):
+        lo = torch.as_tensor(scene.box_lo, dtype=f64, device=dev)
+        hi = torch.as_tensor(scene.box_hi, dtype=f64, device=dev)
+        rgb = torch.as_tensor(scene.box_rgb, dtype=torch.uint8, device=dev)
+        t1 = (lo[None] - o[None, None]) * inv[:, None]
+        t2 = (hi[None] - o[None, None]) * inv[:, None]
+        tn = torch.nan_to_num(torch.minimum(t1, t2), nan=-float("inf")).amax(-1)
+        tf = torch.nan_to_num(torch.maximum(t1, t2), nan=float("inf")).amin(-1)
+        th = torch.where((tn <= tf) & (tn > 1e-9), tn, torch.full_like(tn, float("inf")))
+        tmin, idx = th.min(1)
+        closer = tmin < tbest
+        tbest = torch.where(closer, tmin, tbest)
+        colour = torch.where(closer[:, None], rgb[idx], colour)
+    if len(scene.sph_c):
+        c = torch.as_tensor(scene.sph_c, dtype=f64, device=dev)
+        r = torch.as_tensor(scene.sph_r, dtype=f64, device=dev)
+        rgb = torch.as_tensor(scene.sph_rgb, dtype=torch.uint8, device=dev)
+        oc = o[None] - c
+        a = (d * d).sum(1)[:, None]
+        b = d @ oc.T
+        cc = (oc * oc).sum(1)[None] - r[None] ** 2
+        disc = b * b - a * cc
+        ok = disc >= 0
+        th = (-b - torch.sqrt(torch.clamp(disc, min=0.0))) / a
+        th = torch.where(ok & (th > 1e-9), th, torch.full_like(th, float("inf")))
+        tmin, idx = th.min(1)
+        closer = tmin < tbest
+        tbest = torch.where(closer, tmin, tbest)
+        colour = torch.where(closer[:, None], rgb[idx], colour)
+    z = tbest.reshape(height, width)
+    g = torch.Generator(device=dev)
+    g.manual_seed(int(seed) * 1000003 + int(frame))
+    if noise_k > 0:
+        z = z + torch.randn(z.shape, generator=g, dtype=f64, device=dev) * noise_k * z * z
+    if hole_frac > 0:
+        z = torch.where(torch.rand(z.shape, generator=g, dtype=f64, device=dev) < hole_frac, torch.zeros_like(z), z)
+    z = torch.where(torch.isfinite(z) & (z > 0), z, torch.zeros_like(z))
+    depth = torch.round(z * DEPTH_UNITS_PER_M)
+    depth = torch.where((z >= 13.1) | (depth > 65535), torch.zeros_like(depth), depth)
+    depth = depth.to(torch.int32).to(torch.int16)  # bit pattern of the uint16 value
+    bgr = colour.flip(-1).reshape(height, width, 3).contiguous()
+    return depth, bgr

@@ -157,6 +157,22 @@ ff_status ff_set_state(ff_handle *h, uint32_t n, const float offset[3], const ui
                        const uint16_t *pos, const uint16_t *scale, const uint32_t *parent, uint32_t leaves_used,
                        const float *sdf, const float *weight, const uint16_t *rgb);
 
+/* Device-time profile per stage, measured with CUDA events on the map's
+ * stream.  ff_profile(h, 1) resets and starts recording; ff_profile_read
+ * returns, per stage, the summed milliseconds, the algorithmic bytes (bytes
+ * the stage must move at minimum: e.g. 14,336 B per fused FP32 brick) and the
+ * number of launches.  Stages, in order: project, dedupe, insert, finalize
+ * (leaf indices and parents), fuse, mesh_cells (cell generation and sort),
+ * mesh_count, mesh_emit. */
+#define FF_PROFILE_STAGES 8
+ff_status ff_profile(ff_handle *h, int enable);
+ff_status ff_profile_read(ff_handle *h, double *ms, double *bytes, uint64_t *launches);
+
+/* Process-wide counts, since the library was loaded, of this library's own
+ * kernel launches and of its calls into CUB (sort and scan, each of which
+ * launches a few library kernels). */
+ff_status ff_kernel_launches(uint64_t *own, uint64_t *library);
+
 /* Message of the last failure on this handle (or of ff_create when h is NULL). */
 const char *ff_last_error(const ff_handle *h);
 

@@ -1,0 +1,43 @@
+"""Per-stage profile and launch accounting of the C ABI (ff_profile,
+ff_profile_read, ff_kernel_launches) on a short fusion + meshing run."""
+import numpy as np
+import pytest
+
+from tests.helpers import MAXCAM, SCALING, circle_frames
+
+pytestmark = pytest.mark.gpu
+
+
+def test_profile_counts_match_the_work(lib_built):
+    from fastfusion_b200 import fusion as ff
+    K, frames = circle_frames(0, 6, 160, 120)
+    m = ff.FusionMipMapCPU(0, 0, 0, 0.005, 0.01, 0, True, leaves_max=271420, branches_max=4793488, rcp="exact")
+    m.profile(True)
+    own0, lib0 = ff.kernel_launches()
+    queued = 0
+    for depth, bgr, R, t in frames:
+        queued += m.addMap(depth, ff.CameraInfo(K, R, t), bgr, SCALING, MAXCAM)
+    m.updateMeshes()
+    own1, lib1 = ff.kernel_launches()
+    prof = m.profile_read()
+    assert set(prof) == set(ff.FusionMipMapCPU.PROFILE_STAGES)
+    # one launch of each per-frame stage per frame; the fuse bytes are the
+    # 14,336 B of every queued FP32 brick
+    for stage in ("project", "dedupe", "insert", "fuse"):
+        assert prof[stage][2] == len(frames), (stage, prof[stage])
+        assert prof[stage][0] > 0.0
+    assert prof["fuse"][1] == pytest.approx(14336.0 * queued)
+    for stage in ("mesh_cells", "mesh_count", "mesh_emit"):
+        assert prof[stage][2] == 1
+    assert prof["mesh_count"][1] > 0
+    st = m.stats()
+    assert prof["mesh_emit"][1] >= st["mesh_vertices"] * 15 + st["mesh_faces"] * 12
+    # own kernels: at least project, dedupe, insert, fuse per frame plus the mesher's
+    assert own1 - own0 >= 4 * len(frames) + 4
+    assert lib1 - lib0 >= 3  # cell sort and the two scans
+    # switching off: nothing more is recorded
+    m.profile(False)
+    depth, bgr, R, t = frames[0]
+    m.addMap(depth, ff.CameraInfo(K, R, t), bgr, SCALING, MAXCAM)
+    assert all(v[2] == 0 for v in m.profile_read().values())
+    m.close()
