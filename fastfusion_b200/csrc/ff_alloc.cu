@@ -155,85 +155,149 @@ __device__ void grid_barrier(uint32_t *bar, uint32_t nblocks, Counters *cnt) {
   __syncthreads();
 }
 
-__global__ void k_dedupe(const int4 *__restrict__ vox, int W, int H, int tilesX, int tilesY, int4 *bnd,
-                         uint8_t *processed, Counters *cnt, uint32_t *bar) {
+constexpr int DD_WARPS = 4;      // tiles (warps) per block
+constexpr int DD_TILES_MAX = 4;  // tiles per warp; the first one is kept in shared memory
+
+// One tile of one warp, one round: rows top to bottom from the row state
+// above and the column state to the left (read from the previous round's
+// boundary buffers; all-unprocessed in round 0).  Returns the tile's
+// processed bits (bit r of lane l = pixel (l, r) of the tile).
+__device__ __forceinline__ uint32_t dedupe_tile(const int4 *__restrict__ vox, const int4 *tile_s, int W, int H,
+                                                int tilesX, int tile, int round, int4 *const right[2],
+                                                int4 *const bottom[2], int &changed) {
+  const int lane = threadIdx.x & 31;
+  const int in = round & 1, out = in ^ 1;
+  const int tx = tile % tilesX, ty = tile / tilesX;
+  const int x = tx * 32 + lane;
+  int4 above = make_int4(0, 0, 0, 0);
+  if (round > 0 && ty > 0) above = bottom[in][(size_t)(tile - tilesX) * 32 + lane];
+  int4 prev_bottom = make_int4(0, 0, 0, 0);
+  if (round > 0) prev_bottom = bottom[in][(size_t)tile * 32 + lane];
+  int ak = above.x, bk = above.y, ck = above.z, ap = above.w;
+  uint32_t bits = 0;
+  for (int r = 0; r < 32; r++) {
+    const int y = ty * 32 + r;
+    if (y >= H) break;
+    int k0, k1, k2, valid;
+    if (tile_s) {
+      const int4 t = tile_s[r * 32 + lane];
+      k0 = t.x, k1 = t.y, k2 = t.z, valid = t.w;
+    } else {
+      int4 v = make_int4(0, 0, 0, -1);
+      if (x < W) v = vox[(size_t)y * W + x];
+      k0 = v.x & -8, k1 = v.y & -8, k2 = v.z & -8, valid = v.w >= 0;
+    }
+    const int a = valid && !(ap && k0 == ak && k1 == bk && k2 == ck);
+    int4 left = make_int4(0, 0, 0, 0);
+    if (lane == 0 && tx > 0 && round > 0) left = right[in][(size_t)(tile - 1) * 32 + r];
+    const int p0 = __shfl_up_sync(0xffffffffu, k0, 1);
+    const int p1 = __shfl_up_sync(0xffffffffu, k1, 1);
+    const int p2 = __shfl_up_sync(0xffffffffu, k2, 1);
+    uint32_t T;
+    if (lane == 0) {
+      const int e = left.w && left.x == k0 && left.y == k1 && left.z == k2;
+      const uint32_t c = (a && !e) ? 1u : 0u;
+      T = c | (c << 1);
+    } else {
+      const int e = (p0 == k0 && p1 == k1 && p2 == k2);
+      T = !a ? 0u : (e ? 1u /* NOT: f(0)=1,f(1)=0 */ : 3u);
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t other = __shfl_up_sync(0xffffffffu, T, o);
+      if (lane >= o) T = compose(T, other);
+    }
+    const int p = T & 1u;
+    ak = k0;
+    bk = k1;
+    ck = k2;
+    ap = p;
+    bits |= (uint32_t)p << r;
+    if (lane == 31) {
+      const int4 nv = make_int4(k0, k1, k2, p);
+      if (round == 0) {
+        changed = 1;
+      } else {
+        const int4 ov = right[in][(size_t)tile * 32 + r];
+        if (ov.x != nv.x || ov.y != nv.y || ov.z != nv.z || ov.w != nv.w) changed = 1;
+      }
+      right[out][(size_t)tile * 32 + r] = nv;
+    }
+  }
+  const int4 nb = make_int4(ak, bk, ck, ap);
+  if (round == 0 || nb.x != prev_bottom.x || nb.y != prev_bottom.y || nb.z != prev_bottom.z ||
+      nb.w != prev_bottom.w)
+    changed = 1;
+  bottom[out][(size_t)tile * 32 + lane] = nb;
+  return bits;
+}
+
+// bar: [0] arrivals, [1] generation, [4..6] per-round change counters (rotating)
+__global__ void __launch_bounds__(32 * DD_WARPS) k_dedupe(const int4 *__restrict__ vox, int W, int H, int tilesX,
+                                                          int tilesY, int4 *bnd, uint8_t *processed, Counters *cnt,
+                                                          uint32_t *bar) {
+  extern __shared__ int4 dd_tiles[];
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const int ntiles = tilesX * tilesY;
   // boundary buffers: [2][ntiles][32] right-column states and [2][ntiles][32] bottom-row states
-  int4 *right[2] = {bnd, bnd + (size_t)ntiles * 32};
-  int4 *bottom[2] = {bnd + (size_t)2 * ntiles * 32, bnd + (size_t)3 * ntiles * 32};
+  int4 *const right[2] = {bnd, bnd + (size_t)ntiles * 32};
+  int4 *const bottom[2] = {bnd + (size_t)2 * ntiles * 32, bnd + (size_t)3 * ntiles * 32};
+  // the warp's first tile: brick keys and validity, read once for all rounds
+  int4 *tile_s = dd_tiles + (size_t)(threadIdx.x >> 5) * 32 * 32;
+  if (warp < ntiles) {
+    const int tx = warp % tilesX, ty = warp / tilesX;
+    const int x = tx * 32 + lane;
+    for (int r = 0; r < 32; r++) {
+      const int y = ty * 32 + r;
+      int4 v = make_int4(0, 0, 0, -1);
+      if (x < W && y < H) v = vox[(size_t)y * W + x];
+      tile_s[r * 32 + lane] = make_int4(v.x & -8, v.y & -8, v.z & -8, v.w >= 0 ? 1 : 0);
+    }
+  }
+  __syncwarp();
+  uint32_t bits[DD_TILES_MAX];
   const int max_rounds = tilesX + tilesY + 1;
+  volatile uint32_t *chg = bar + 4;
   int round = 0;
+  bool converged = false;
   for (; round < max_rounds; round++) {
-    const int in = round & 1, out = in ^ 1;
     int changed = 0;
-    for (int tile = warp; tile < ntiles; tile += nwarps) {
-      const int tx = tile % tilesX, ty = tile / tilesX;
-      const int x = tx * 32 + lane;
-      int4 above = make_int4(0, 0, 0, 0);
-      if (ty > 0) above = bottom[in][(size_t)(tile - tilesX) * 32 + lane];
-      int4 prev_bottom = bottom[in][(size_t)tile * 32 + lane];
-      int ak = above.x, bk = above.y, ck = above.z, ap = above.w;
-      for (int r = 0; r < 32; r++) {
-        const int y = ty * 32 + r;
-        if (y >= H) break;
-        int4 v = make_int4(0, 0, 0, -1);
-        if (x < W) v = vox[(size_t)y * W + x];
-        const int valid = v.w >= 0;
-        const int k0 = v.x & -8, k1 = v.y & -8, k2 = v.z & -8;
-        const int a = valid && !(ap && k0 == ak && k1 == bk && k2 == ck);
-        int4 left = make_int4(0, 0, 0, 0);
-        if (lane == 0 && tx > 0) left = right[in][(size_t)(tile - 1) * 32 + r];
-        const int p0 = __shfl_up_sync(0xffffffffu, k0, 1);
-        const int p1 = __shfl_up_sync(0xffffffffu, k1, 1);
-        const int p2 = __shfl_up_sync(0xffffffffu, k2, 1);
-        uint32_t T;
-        if (lane == 0) {
-          const int e = left.w && left.x == k0 && left.y == k1 && left.z == k2;
-          const uint32_t c = (a && !e) ? 1u : 0u;
-          T = c | (c << 1);
-        } else {
-          const int e = (p0 == k0 && p1 == k1 && p2 == k2);
-          T = !a ? 0u : (e ? 1u /* NOT: f(0)=1,f(1)=0 */ : 3u);
-        }
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          uint32_t other = __shfl_up_sync(0xffffffffu, T, o);
-          if (lane >= o) T = compose(T, other);
-        }
-        const int p = T & 1u;
-        ak = k0;
-        bk = k1;
-        ck = k2;
-        ap = p;
-        if (x < W) processed[(size_t)y * W + x] = (uint8_t)p;
-        if (lane == 31) {
-          int4 nv = make_int4(k0, k1, k2, p);
-          int4 ov = right[in][(size_t)tile * 32 + r];
-          if (ov.x != nv.x || ov.y != nv.y || ov.z != nv.z || ov.w != nv.w) changed = 1;
-          right[out][(size_t)tile * 32 + r] = nv;
-        }
-      }
-      int4 nb = make_int4(ak, bk, ck, ap);
-      if (nb.x != prev_bottom.x || nb.y != prev_bottom.y || nb.z != prev_bottom.z || nb.w != prev_bottom.w)
-        changed = 1;
-      bottom[out][(size_t)tile * 32 + lane] = nb;
+    for (int ti = 0; ti < DD_TILES_MAX; ti++) {
+      const int tile = warp + ti * nwarps;
+      if (tile < ntiles)
+        bits[ti] = dedupe_tile(vox, ti == 0 ? tile_s : nullptr, W, H, tilesX, tile, round, right, bottom, changed);
     }
     changed = __any_sync(0xffffffffu, changed);
-    if (changed && lane == 0) atomicAdd(&cnt->dedupe_changed, 1u);
+    if (changed && lane == 0) atomicAdd((uint32_t *)&chg[round % 3], 1u);
+    // counter (round + 1) % 3 was last read before the previous barrier
+    if (blockIdx.x == 0 && threadIdx.x == 0) chg[(round + 1) % 3] = 0;
     grid_barrier(bar, gridDim.x, cnt);
-    const uint32_t any = *(volatile uint32_t *)&cnt->dedupe_changed;
-    grid_barrier(bar, gridDim.x, cnt);
-    if (blockIdx.x == 0 && threadIdx.x == 0) cnt->dedupe_changed = 0;
-    grid_barrier(bar, gridDim.x, cnt);
-    if (!any) break;
+    const uint32_t any = chg[round % 3];
+    if (!any) {
+      converged = true;
+      break;
+    }
     if (*(volatile uint32_t *)&cnt->error & ERR_SPIN_TIMEOUT) break;
+  }
+#pragma unroll
+  for (int ti = 0; ti < DD_TILES_MAX; ti++) {
+    const int tile = warp + ti * nwarps;
+    if (tile >= ntiles) continue;
+    const int tx = tile % tilesX, ty = tile / tilesX;
+    const int x = tx * 32 + lane;
+    if (x >= W) continue;
+    for (int r = 0; r < 32; r++) {
+      const int y = ty * 32 + r;
+      if (y >= H) break;
+      processed[(size_t)y * W + x] = (uint8_t)((bits[ti] >> r) & 1u);
+    }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     cnt->dedupe_iters = round + 1;
-    if (round >= max_rounds) atomicOr(&cnt->error, ERR_DEDUPE_NOT_CONVERGED);
+    if (!converged) atomicOr(&cnt->error, ERR_DEDUPE_NOT_CONVERGED);
   }
 }
 
@@ -241,20 +305,29 @@ cudaError_t launch_dedupe(const int4 *vox, int W, int H, int4 *bnd, uint8_t *pro
                           uint32_t *barrier, int device, cudaStream_t s) {
   int tilesX = (W + 31) / 32, tilesY = (H + 31) / 32;
   int ntiles = tilesX * tilesY;
-  const int threads = 256;
+  const int threads = 32 * DD_WARPS;
+  const size_t smem = sizeof(int4) * 32 * 32 * DD_WARPS;
+  static std::atomic<unsigned long long> attr_devices{0};
+  const unsigned long long bit = 1ull << (device & 63);
+  if (!(attr_devices.load() & bit)) {
+    cudaError_t e = cudaFuncSetAttribute(k_dedupe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_devices.fetch_or(bit);
+  }
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dedupe, threads, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dedupe, threads, smem);
   if (e != cudaSuccess) return e;
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  int want = (ntiles + threads / 32 - 1) / (threads / 32);
+  int want = (ntiles + DD_WARPS - 1) / DD_WARPS;
   int maxb = per_sm * sms;
   int blocks = want < maxb ? want : maxb;
   if (blocks < 1) blocks = 1;
+  if ((size_t)blocks * DD_WARPS * DD_TILES_MAX < (size_t)ntiles) return cudaErrorInvalidConfiguration;
   void *args[] = {(void *)&vox, (void *)&W, (void *)&H, (void *)&tilesX, (void *)&tilesY, (void *)&bnd,
                   (void *)&processed, (void *)&cnt, (void *)&barrier};
   note_launch();
-  return cudaLaunchCooperativeKernel((const void *)k_dedupe, dim3(blocks), dim3(threads), args, 0, s);
+  return cudaLaunchCooperativeKernel((const void *)k_dedupe, dim3(blocks), dim3(threads), args, smem, s);
 }
 
 // -------------------------------------------------------------- insert ----

@@ -332,7 +332,7 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
       }
     }
     if (alloc(&h->d_col, L * 1536) != cudaSuccess) { fail(FF_ERR_OOM_POOL, "colour pool"); break; }
-    if (alloc(&h->d_cnt, 1) != cudaSuccess || alloc(&h->d_barrier, 4) != cudaSuccess) { fail(FF_ERR_CUDA, "counters"); break; }
+    if (alloc(&h->d_cnt, 1) != cudaSuccess || alloc(&h->d_barrier, 8) != cudaSuccess) { fail(FF_ERR_CUDA, "counters"); break; }
     if (cudaMallocHost((void **)&h->h_cnt, sizeof(Counters)) != cudaSuccess) { fail(FF_ERR_CUDA, "pinned"); break; }
     if (cfg->rcp_mode == FF_RCP_HOST) {
       std::vector<uint32_t> tab;
@@ -447,8 +447,7 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
     hc.box_max[r] = (int)h->n - 1;
   }
   CK(cudaMemcpyAsync(h->d_cnt, &hc, sizeof(Counters), cudaMemcpyHostToDevice, s));
-  CK(cudaMemsetAsync(h->d_barrier, 0, 16, s));
-  CK(cudaMemsetAsync(h->d_bnd, 0, sizeof(int4) * h->bnd_elems, s));
+  CK(cudaMemsetAsync(h->d_barrier, 0, 8 * sizeof(uint32_t), s));
   // voxel -> camera parameters are taken before any grow() of this frame,
   // as in the reference (pInv is built before the traversal)
   CamF q = cam_grid_to_camera(h, K, R, t);
@@ -766,6 +765,26 @@ ff_status ff_get_mesh(ff_handle *h, float *xyz, uint8_t *rgb, uint32_t *faces) {
   std::string err;
   int rc = mesh_copy_out(h->mesh, xyz, rgb, faces, h->stream, err);
   if (rc != 0) return set_err(h, (ff_status)rc, err);
+  return FF_OK;
+}
+
+ff_status ff_alloc_host(size_t bytes, void **out) {
+  if (!out) return FF_ERR_BAD_ARG;
+  *out = nullptr;
+  if (!bytes) return FF_OK;
+  if (cudaHostAlloc(out, bytes, cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    *out = nullptr;
+    return FF_ERR_CUDA;
+  }
+  return FF_OK;
+}
+
+ff_status ff_free_host(void *p) {
+  if (p && cudaFreeHost(p) != cudaSuccess) {
+    cudaGetLastError();
+    return FF_ERR_CUDA;
+  }
   return FF_OK;
 }
 

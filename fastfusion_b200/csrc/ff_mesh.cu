@@ -91,7 +91,7 @@ struct GenQueues {
   FaceItem *faceq[2];
   EdgeItem *edgeq[2];
   VertItem *vertq[2];
-  uint32_t *count;  // [2][4]: cell, face, edge, vert counts of the two buffers
+  uint32_t *lvl;  // [level][4]: cell, face, edge, vert item counts of each level
   uint32_t cap_cell, cap_face, cap_edge, cap_vert;
   Cell *cells;
   uint32_t *n_cells;
@@ -99,6 +99,11 @@ struct GenQueues {
   uint32_t *error;
   uint32_t *n_corners;
 };
+
+// counter words of the generation (see MeshImpl::d_count)
+constexpr int LEVEL_COUNTS = 32;
+constexpr int MAX_GEN_LEVELS = 48;
+constexpr int COUNT_WORDS = LEVEL_COUNTS + 4 * (MAX_GEN_LEVELS + 1) + 28;
 
 struct GenCtx {
   const uint32_t *tree;
@@ -128,15 +133,28 @@ __device__ __forceinline__ void others(int e, int &p, int &q) {
   q = e == 2 ? 1 : 2;
 }
 
+// Slot in a per-launch queue: one atomic per group of lanes that push to the
+// same counter at the same time (lanes that are active together share it).
+__device__ __forceinline__ uint32_t claim(uint32_t *ctr) {
+  const unsigned mask = __activemask();
+  const unsigned peers = __match_any_sync(mask, (unsigned long long)(uintptr_t)ctr);
+  const int leader = __ffs(peers) - 1;
+  const unsigned lane = threadIdx.x & 31;
+  uint32_t base = 0;
+  if ((int)lane == leader) base = atomicAdd(ctr, (uint32_t)__popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  return base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+}
+
 __device__ void emit_cell(const GenQueues &Q, int type, int quirk, const int *o, int size, const uint32_t *L, int nl) {
   for (int k = 0; k < nl; k++)
     if (L[k] >= BRANCHINIT) return;  // a side without a leaf is never meshed
-  uint32_t i = atomicAdd(Q.n_cells, 1u);
+  const uint32_t i = claim(Q.n_cells);
   if (i >= Q.cap_cells) {
     atomicOr(Q.error, ERR_CELL_OVERFLOW);
     return;
   }
-  if (type == 7) atomicAdd(Q.n_corners, 1u);
+  if (type == 7) claim(Q.n_corners);
   Cell c;
   c.type = (uint8_t)type;
   c.quirk = (uint8_t)quirk;
@@ -149,7 +167,7 @@ __device__ void emit_cell(const GenQueues &Q, int type, int quirk, const int *o,
 
 template <typename T>
 __device__ __forceinline__ void push(T *q, uint32_t *count, uint32_t cap, const T &v, uint32_t *error) {
-  uint32_t i = atomicAdd(count, 1u);
+  const uint32_t i = claim(count);
   if (i >= cap) {
     atomicOr(error, ERR_CELL_OVERFLOW);
     return;
@@ -157,13 +175,47 @@ __device__ __forceinline__ void push(T *q, uint32_t *count, uint32_t cap, const 
   q[i] = v;
 }
 
-__device__ void vert_item(const GenCtx &g, const GenQueues &Q, const Slot *S8, int nb) {
+// Every item is a pure function of its slots, so an item found while
+// expanding another is queued for the next launch rather than expanded by the
+// same thread: each thread does a bounded amount of work (a few independent
+// tree reads, a few pushes) and the levels run wide.
+struct Out {
+  Slot *cellq;
+  FaceItem *faceq;
+  EdgeItem *edgeq;
+  VertItem *vertq;
+  uint32_t *count;  // the next level's 4 counters
+};
+
+__device__ __forceinline__ void push_cell(const GenQueues &Q, const Out &O, const Slot &s) {
+  push(O.cellq, O.count + 0, Q.cap_cell, s, Q.error);
+}
+__device__ __forceinline__ void push_face(const GenQueues &Q, const Out &O, const Slot &a, const Slot &b, int ax) {
+  FaceItem f;
+  f.a = a;
+  f.b = b;
+  f.axis = ax;
+  push(O.faceq, O.count + 1, Q.cap_face, f, Q.error);
+}
+__device__ __forceinline__ void push_edge(const GenQueues &Q, const Out &O, const Slot *S4, int e) {
+  EdgeItem it;
+  it.axis = e;
+  for (int j = 0; j < 4; j++) it.s[j] = S4[j];
+  push(O.edgeq, O.count + 2, Q.cap_edge, it, Q.error);
+}
+__device__ __forceinline__ void push_vert(const GenQueues &Q, const Out &O, const Slot *S8) {
+  VertItem v;
+  for (int j = 0; j < 8; j++) v.s[j] = S8[j];
+  push(O.vertq, O.count + 3, Q.cap_vert, v, Q.error);
+}
+
+__device__ void vert_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot *S8) {
   bool any = false;
   for (int j = 0; j < 8; j++) any |= is_sub(g, S8[j]);
   if (any) {
-    VertItem v;
-    for (int j = 0; j < 8; j++) v.s[j] = ch(g, S8[j], 7 - j);
-    push(Q.vertq[nb], Q.count + nb * 4 + 3, Q.cap_vert, v, Q.error);
+    Slot C[8];
+    for (int j = 0; j < 8; j++) C[j] = ch(g, S8[j], 7 - j);
+    push_vert(Q, O, C);
     return;
   }
   // the vertex is a corner of the smallest slot around it
@@ -177,7 +229,7 @@ __device__ void vert_item(const GenCtx &g, const GenQueues &Q, const Slot *S8, i
   emit_cell(Q, 7, 0, o, size, L, 8);
 }
 
-__device__ void edge_item(const GenCtx &g, const GenQueues &Q, const Slot *S4, int e, int nb) {
+__device__ void edge_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot *S4, int e) {
   bool any = false;
   for (int j = 0; j < 4; j++) any |= is_sub(g, S4[j]);
   int p, q;
@@ -196,13 +248,12 @@ __device__ void edge_item(const GenCtx &g, const GenQueues &Q, const Slot *S4, i
     return;
   }
   for (int half = 0; half < 2; half++) {
-    EdgeItem it;
-    it.axis = e;
+    Slot H[4];
     for (int j = 0; j < 4; j++) {
       int k = ((j & 1) ? 0 : (1 << p)) | (((j >> 1) & 1) ? 0 : (1 << q)) | (half ? (1 << e) : 0);
-      it.s[j] = ch(g, S4[j], k);
+      H[j] = ch(g, S4[j], k);
     }
-    push(Q.edgeq[nb], Q.count + nb * 4 + 2, Q.cap_edge, it, Q.error);
+    push_edge(Q, O, H, e);
   }
   Slot S8[8];
   for (int j = 0; j < 8; j++) {
@@ -212,10 +263,10 @@ __device__ void edge_item(const GenCtx &g, const GenQueues &Q, const Slot *S4, i
     int k = (pj ? 0 : (1 << p)) | (qj ? 0 : (1 << q)) | (ej ? (1 << e) : 0);
     S8[j] = ch(g, S4[pj | (qj << 1)], k);
   }
-  vert_item(g, Q, S8, nb);
+  push_vert(Q, O, S8);
 }
 
-__device__ void face_item(const GenCtx &g, const GenQueues &Q, const Slot &A, const Slot &B, int ax, int nb) {
+__device__ void face_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot &A, const Slot &B, int ax) {
   if (!is_sub(g, A) && !is_sub(g, B)) {
     int size = min((int)A.size, (int)B.size);
     const Slot &small = A.size <= B.size ? A : B;
@@ -228,13 +279,17 @@ __device__ void face_item(const GenCtx &g, const GenQueues &Q, const Slot &A, co
   const int bit = 1 << ax;
   int u, v;
   others(ax, u, v);
+  // the two sides' halves next to the face: A's children on its +ax side, B's
+  // on its -ax side (a slot that is not subdivided stands for all of them)
+  Slot a[8], b[8];
+  for (int k = 0; k < 8; k++) {
+    if (k & bit) continue;
+    a[k] = ch(g, A, k | bit);
+    b[k] = ch(g, B, k);
+  }
   for (int qd = 0; qd < 4; qd++) {
     int k = ((qd & 1) ? (1 << u) : 0) | ((qd & 2) ? (1 << v) : 0);
-    FaceItem f;
-    f.a = ch(g, A, k | bit);
-    f.b = ch(g, B, k);
-    f.axis = ax;
-    push(Q.faceq[nb], Q.count + nb * 4 + 1, Q.cap_face, f, Q.error);
+    push_face(Q, O, a[k], b[k], ax);
   }
   for (int t = 0; t < 2; t++) {
     const int e = t == 0 ? u : v;
@@ -248,26 +303,24 @@ __device__ void face_item(const GenCtx &g, const GenQueues &Q, const Slot &A, co
         side[p] = j & 1;
         side[q] = (j >> 1) & 1;
         int k = (half ? (1 << e) : 0) | (side[other] ? (1 << other) : 0);
-        S4[j] = side[ax] ? ch(g, B, k) : ch(g, A, k | bit);
+        S4[j] = side[ax] ? b[k] : a[k];
       }
-      // an edge is handled at the level where it is created, like a
-      // recursive edge call: emit or expand now
-      edge_item(g, Q, S4, e, nb);
+      push_edge(Q, O, S4, e);
     }
   }
   Slot S8[8];
   for (int j = 0; j < 8; j++) {
     int k = j & ~bit;
-    S8[j] = ((j >> ax) & 1) ? ch(g, B, k) : ch(g, A, k | bit);
+    S8[j] = ((j >> ax) & 1) ? b[k] : a[k];
   }
-  vert_item(g, Q, S8, nb);
+  push_vert(Q, O, S8);
 }
 
 // one subdivided slot: its children, their 12 faces, 6 edges and centre
-__device__ void cell_item(const GenCtx &g, const GenQueues &Q, const Slot *C, int nb) {
+__device__ void cell_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot *C) {
   for (int j = 0; j < 8; j++) {
     if (is_sub(g, C[j])) {
-      push(Q.cellq[nb], Q.count + nb * 4 + 0, Q.cap_cell, C[j], Q.error);
+      push_cell(Q, O, C[j]);
     } else {
       int o[3] = {C[j].o[0], C[j].o[1], C[j].o[2]};
       uint32_t L[1] = {C[j].la};
@@ -276,26 +329,29 @@ __device__ void cell_item(const GenCtx &g, const GenQueues &Q, const Slot *C, in
   }
   const int F[3][4][2] = {{{0, 1}, {2, 3}, {4, 5}, {6, 7}}, {{0, 2}, {1, 3}, {4, 6}, {5, 7}}, {{0, 4}, {1, 5}, {2, 6}, {3, 7}}};
   for (int ax = 0; ax < 3; ax++)
-    for (int i = 0; i < 4; i++) face_item(g, Q, C[F[ax][i][0]], C[F[ax][i][1]], ax, nb);
+    for (int i = 0; i < 4; i++) push_face(Q, O, C[F[ax][i][0]], C[F[ax][i][1]], ax);
   for (int x = 0; x < 2; x++) {
     Slot S4[4] = {C[x], C[x | 2], C[x | 4], C[x | 6]};
-    edge_item(g, Q, S4, 0, nb);
+    push_edge(Q, O, S4, 0);
   }
   for (int y = 0; y < 4; y += 2) {
     Slot S4[4] = {C[y], C[y | 1], C[y | 4], C[y | 5]};
-    edge_item(g, Q, S4, 1, nb);
+    push_edge(Q, O, S4, 1);
   }
   for (int z = 0; z < 8; z += 4) {
     Slot S4[4] = {C[z], C[z | 1], C[z | 2], C[z | 3]};
-    edge_item(g, Q, S4, 2, nb);
+    push_edge(Q, O, S4, 2);
   }
-  vert_item(g, Q, C, nb);
+  push_vert(Q, O, C);
 }
 
-// Items of level `cur` expand into level `cur ^ 1` (or emit cells).
-__global__ void k_gen_level(GenCtx g, GenQueues Q, int cur, int root, uint32_t n) {
-  const int nb = cur ^ 1;
-  const uint32_t *cnt = Q.count + cur * 4;
+// Items of level `lv` (queue buffer lv & 1, counters lvl + 4 lv) expand into
+// level lv + 1 or emit cells.  Level 0 is the root: the volume's 8 octants.
+__global__ void __launch_bounds__(128) k_gen_level(GenCtx g, GenQueues Q, int lv, uint32_t n) {
+  const int cur = lv & 1, nb = cur ^ 1;
+  const bool root = lv == 0;
+  const uint32_t *cnt = Q.lvl + 4 * lv;
+  Out O{Q.cellq[nb], Q.faceq[nb], Q.edgeq[nb], Q.vertq[nb], Q.lvl + 4 * (lv + 1)};
   const uint32_t nc = root ? 1u : min(cnt[0], Q.cap_cell), nf = root ? 0u : min(cnt[1], Q.cap_face);
   const uint32_t ne = root ? 0u : min(cnt[2], Q.cap_edge), nv = root ? 0u : min(cnt[3], Q.cap_vert);
   const uint32_t total = nc + nf + ne + nv;
@@ -317,22 +373,18 @@ __global__ void k_gen_level(GenCtx g, GenQueues Q, int cur, int root, uint32_t n
         const Slot s = Q.cellq[cur][i];
         for (int co = 0; co < 8; co++) C[co] = child_of(g, s, co);
       }
-      cell_item(g, Q, C, nb);
+      cell_item(g, Q, O, C);
     } else if (i < nc + nf) {
       const FaceItem f = Q.faceq[cur][i - nc];
-      face_item(g, Q, f.a, f.b, f.axis, nb);
+      face_item(g, Q, O, f.a, f.b, f.axis);
     } else if (i < nc + nf + ne) {
       const EdgeItem e = Q.edgeq[cur][i - nc - nf];
-      edge_item(g, Q, e.s, e.axis, nb);
+      edge_item(g, Q, O, e.s, e.axis);
     } else {
       const VertItem v = Q.vertq[cur][i - nc - nf - ne];
-      vert_item(g, Q, v.s, nb);
+      vert_item(g, Q, O, v.s);
     }
   }
-}
-
-__global__ void k_clear_counts(uint32_t *count, int which) {
-  if (threadIdx.x < 4) count[which * 4 + threadIdx.x] = 0;
 }
 
 __device__ __forceinline__ uint64_t cell_key(const Cell &c) {
@@ -996,7 +1048,9 @@ struct MeshImpl {
   VertItem *vertq[2] = {nullptr, nullptr};
   size_t cap_cellq[2] = {0, 0}, cap_faceq[2] = {0, 0}, cap_edgeq[2] = {0, 0}, cap_vertq[2] = {0, 0};
   uint32_t n_corners = 0;
-  uint32_t *d_count = nullptr;  // 8 queue counts, then n_cells, error, n_dirty
+  // words 8 n_cells, 9 error, 10 n_dirty, 11 n_corners, 12-13 samples;
+  // from LEVEL_COUNTS: 4 item counters per generation level
+  uint32_t *d_count = nullptr;
   uint32_t *h_count = nullptr;
   // cells: unsorted, sorted (current), previous
   Cell *raw = nullptr, *cells = nullptr, *old_cells = nullptr;
@@ -1056,10 +1110,10 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
     }
     MCK(grow_buf(I.raw, I.cap_raw, want_q * 8));
     if (!I.d_count) {
-      MCK(cudaMalloc((void **)&I.d_count, 16 * sizeof(uint32_t)));
-      MCK(cudaMallocHost((void **)&I.h_count, 16 * sizeof(uint32_t)));
+      MCK(cudaMalloc((void **)&I.d_count, COUNT_WORDS * sizeof(uint32_t)));
+      MCK(cudaMallocHost((void **)&I.h_count, COUNT_WORDS * sizeof(uint32_t)));
     }
-    MCK(cudaMemsetAsync(I.d_count, 0, 16 * sizeof(uint32_t), s));
+    MCK(cudaMemsetAsync(I.d_count, 0, COUNT_WORDS * sizeof(uint32_t), s));
     GenQueues Q;
     for (int b = 0; b < 2; b++) {
       Q.cellq[b] = I.cellq[b];
@@ -1067,7 +1121,7 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
       Q.edgeq[b] = I.edgeq[b];
       Q.vertq[b] = I.vertq[b];
     }
-    Q.count = I.d_count;
+    Q.lvl = I.d_count + LEVEL_COUNTS;
     Q.cap_cell = (uint32_t)std::min(I.cap_cellq[0], I.cap_cellq[1]);
     Q.cap_face = (uint32_t)std::min(I.cap_faceq[0], I.cap_faceq[1]);
     Q.cap_edge = (uint32_t)std::min(I.cap_edgeq[0], I.cap_edgeq[1]);
@@ -1078,26 +1132,32 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
     Q.error = I.d_count + 9;
     Q.n_corners = I.d_count + 11;
     GenCtx g{in.tree, in.leaves_max};
-    int levels = 2;
-    for (uint32_t h = in.n; h > 8; h >>= 1) levels++;
-    int cur = 0;
-    for (int lv = 0; lv < levels; lv++) {
-      note_launch(2);
-      k_clear_counts<<<1, 32, 0, s>>>(I.d_count, cur ^ 1);
-      k_gen_level<<<148 * 8, 128, 0, s>>>(g, Q, cur, lv == 0 ? 1 : 0, in.n);
-      cur ^= 1;
+    // a chain cell -> face -> edge -> vertex adds up to three levels below
+    // the octree's depth; more levels run if items are left
+    int depth = 1;
+    for (uint32_t h = in.n; h > 8; h >>= 1) depth++;
+    int lv = 0, batch = depth + 4;
+    bool leftover = true, overflow = false;
+    while (leftover && lv < MAX_GEN_LEVELS) {
+      const int end = std::min(lv + batch, MAX_GEN_LEVELS);
+      note_launch((unsigned)(end - lv));
+      for (; lv < end; lv++) k_gen_level<<<148 * 8, 128, 0, s>>>(g, Q, lv, in.n);
+      MCK(cudaGetLastError());
+      MCK(cudaMemcpyAsync(I.h_count, I.d_count, COUNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      MCK(cudaStreamSynchronize(s));
+      const uint32_t *c = I.h_count + LEVEL_COUNTS + 4 * lv;
+      leftover = c[0] || c[1] || c[2] || c[3];
+      overflow = (I.h_count[9] & ERR_CELL_OVERFLOW) != 0;
+      if (overflow) break;
+      batch = 4;
     }
-    MCK(cudaGetLastError());
-    MCK(cudaMemcpyAsync(I.h_count, I.d_count, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    MCK(cudaStreamSynchronize(s));
     const uint32_t *hc = I.h_count;
-    bool leftover = hc[cur * 4] || hc[cur * 4 + 1] || hc[cur * 4 + 2] || hc[cur * 4 + 3];
-    if (hc[9] & ERR_CELL_OVERFLOW) {
+    if (overflow) {
       want_q *= 2;
       continue;
     }
     if (leftover) {
-      err = "meshing: cell generation did not finish within the octree depth";
+      err = "meshing: cell generation did not finish within the level limit";
       return 6;
     }
     ncells = hc[8];
@@ -1183,11 +1243,14 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   // the key's top field)
   const uint32_t first_corner = ncells - std::min(I.n_corners, ncells);
   const size_t smem = sizeof(WarpScratch) * MESH_WARPS;
-  static bool attr_set = false;
-  if (!attr_set) {
+  static std::atomic<unsigned long long> attr_devices{0};
+  int dev = 0;
+  MCK(cudaGetDevice(&dev));
+  const unsigned long long dbit = 1ull << (dev & 63);
+  if (!(attr_devices.load() & dbit)) {
     MCK(cudaFuncSetAttribute(k_mesh_lattice<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     MCK(cudaFuncSetAttribute(k_mesh_lattice<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set = true;
+    attr_devices.fetch_or(dbit);
   }
   const uint8_t *dmask = I.dirty;
   pi = P.begin(ST_MESH_COUNT, s);

@@ -66,6 +66,8 @@ SIGNATURES = {
     "ff_get_mesh": (_i32, [_vp, _vp, _vp, _vp]),
     "ff_get_mesh_device": (_i32, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "ff_get_mesh_cells": (_i32, [_vp, _vp, _vp]),
+    "ff_alloc_host": (_i32, [_sz, ctypes.POINTER(_vp)]),
+    "ff_free_host": (_i32, [_vp]),
     "ff_get_stats": (_i32, [_vp, ctypes.POINTER(ff_stats)]),
     "ff_get_leaves": (_i32, [_vp, _vp, _vp, _vp]),
     "ff_get_queue": (_i32, [_vp, _vp]),
@@ -134,6 +136,62 @@ class MeshInterleaved:
     faces: np.ndarray     # (nf, 3) uint32
 
 
+class MeshBuffer:
+    """Reusable page-locked host storage for getMeshInterleavedMarchingCubes(out=...).
+
+    The mesh is copied from the device straight into this memory; the arrays
+    of the returned MeshInterleaved are views of it, valid until the buffer is
+    filled again (copy them to keep a mesh)."""
+
+    def __init__(self, n_vertices: int = 0, n_faces: int = 0):
+        self._L = load_library()
+        self._ptr = {}
+        self._cap = {"xyz": 0, "rgb": 0, "faces": 0}
+        self.reserve(n_vertices, n_faces)
+
+    def _grow(self, key: str, nbytes: int):
+        if nbytes <= self._cap[key]:
+            return
+        nbytes = max(nbytes, int(self._cap[key] * 1.5), 4096)
+        p = ctypes.c_void_p()
+        st = self._L.ff_alloc_host(nbytes, ctypes.byref(p))
+        if st != FF_OK:
+            raise FFError(st, f"ff_alloc_host({nbytes}) failed")
+        old = self._ptr.get(key)
+        if old:
+            self._L.ff_free_host(old)
+        self._ptr[key] = p.value
+        self._cap[key] = nbytes
+
+    def reserve(self, n_vertices: int, n_faces: int):
+        self._grow("xyz", 12 * n_vertices)
+        self._grow("rgb", 3 * n_vertices)
+        self._grow("faces", 12 * n_faces)
+
+    def view(self, key: str, dtype, shape):
+        n = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        if n == 0:
+            return np.zeros(shape, dtype)
+        buf = (ctypes.c_char * n).from_address(self._ptr[key])
+        return np.frombuffer(buf, dtype=dtype).reshape(shape)
+
+    def pointers(self):
+        return [ctypes.c_void_p(self._ptr.get(k)) for k in ("xyz", "rgb", "faces")]
+
+    def close(self):
+        for p in self._ptr.values():
+            if p:
+                self._L.ff_free_host(p)
+        self._ptr = {}
+        self._cap = {"xyz": 0, "rgb": 0, "faces": 0}
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class FusionMipMapCPU:
     """Drop-in for the reference's FusionMipMapCPU on one B200."""
 
@@ -199,9 +257,17 @@ class FusionMipMapCPU:
         self._check(self._L.ff_update_meshes(self._h, ctypes.byref(u)))
         return bool(u.value)
 
-    def getMeshInterleavedMarchingCubes(self) -> MeshInterleaved:
+    def getMeshInterleavedMarchingCubes(self, out: MeshBuffer | None = None) -> MeshInterleaved:
+        """The mesh of the last updateMeshes as a host copy (the reference
+        returns its mesh by value).  With `out`, the copy lands in that
+        reusable page-locked buffer and the returned arrays are views of it."""
         nv, nf = ctypes.c_uint64(), ctypes.c_uint64()
         self._check(self._L.ff_get_mesh_counts(self._h, ctypes.byref(nv), ctypes.byref(nf)))
+        if out is not None:
+            out.reserve(nv.value, nf.value)
+            self._check(self._L.ff_get_mesh(self._h, *out.pointers()))
+            return MeshInterleaved(out.view("xyz", np.float32, (nv.value, 3)), out.view("rgb", np.uint8, (nv.value, 3)),
+                                   out.view("faces", np.uint32, (nf.value, 3)))
         xyz = np.zeros((nv.value, 3), np.float32)
         rgb = np.zeros((nv.value, 3), np.uint8)
         faces = np.zeros((nf.value, 3), np.uint32)

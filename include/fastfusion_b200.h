@@ -119,6 +119,12 @@ ff_status ff_get_mesh_counts(ff_handle *h, uint64_t *n_vertices, uint64_t *n_fac
  * getMeshInterleavedMarchingCubes() (geometryfusion_mipmap_cpu.cpp:3359-3374). */
 ff_status ff_get_mesh(ff_handle *h, float *xyz, uint8_t *rgb, uint32_t *faces);
 
+/* Page-locked host memory for ff_get_mesh / ff_add_map_u16 buffers: copies
+ * to and from it run at full PCIe/C2C speed.  Not a counterpart of a
+ * reference call (the reference has no device). */
+ff_status ff_alloc_host(size_t bytes, void **out);
+ff_status ff_free_host(void *p);
+
 /* The mesh cells of the last update (ff_stats.mesh_cells of them), in mesh
  * order: 14 int32 each -- type (0 interior, 1-3 wall x/y/z, 4-6 edge x/y/z,
  * 7 corner), quirk flag, origin x/y/z, size (voxels), the leaf of each side

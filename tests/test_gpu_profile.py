@@ -41,3 +41,26 @@ def test_profile_counts_match_the_work(lib_built):
     m.addMap(depth, ff.CameraInfo(K, R, t), bgr, SCALING, MAXCAM)
     assert all(v[2] == 0 for v in m.profile_read().values())
     m.close()
+
+
+def test_mesh_into_pinned_buffer(lib_built):
+    """getMeshInterleavedMarchingCubes(out=MeshBuffer) returns the same mesh as
+    the plain copy, and the buffer grows as the mesh grows."""
+    from fastfusion_b200 import fusion as ff
+    K, frames = circle_frames(1, 8, 160, 120)
+    m = ff.FusionMipMapCPU(0, 0, 0, 0.005, 0.01, 0, True, leaves_max=271420, branches_max=4793488, rcp="exact")
+    buf = ff.MeshBuffer(16, 16)
+    sizes = []
+    for k, (depth, bgr, R, t) in enumerate(frames):
+        m.addMap(depth, ff.CameraInfo(K, R, t), bgr, SCALING, MAXCAM)
+        if k % 3 == 2 or k == len(frames) - 1:
+            m.updateMeshes()
+            a = m.getMeshInterleavedMarchingCubes()
+            b = m.getMeshInterleavedMarchingCubes(out=buf)
+            assert np.array_equal(a.vertices.view(np.uint32), b.vertices.view(np.uint32))
+            assert np.array_equal(a.colors, b.colors)
+            assert np.array_equal(a.faces, b.faces)
+            sizes.append(len(a.faces))
+    assert sizes[-1] > 0
+    buf.close()
+    m.close()
