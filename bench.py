@@ -56,10 +56,10 @@ CPU_SAMPLE_SECONDS = 20.0
 
 # stage -> kernels it times (for the roofline record)
 STAGE_KERNELS = {
-    "project": "k_project",
-    "dedupe": "k_dedupe",
+    "grow": "k_shift_branches+k_shift_leaves+copies",
+    "dedupe": "k_dedupe (projection + de-duplication)",
     "insert": "k_insert",
-    "finalize": "k_pending_keys+radix sort+k_finalize+k_parents",
+    "finalize": "k_finalize_small",
     "fuse": "k_fuse",
     "mesh_cells": "k_gen_level+k_cell_keys+radix sort+k_gather_cells",
     "mesh_count": "k_mesh_lattice<count>+k_mesh_corner<count>",
@@ -295,6 +295,15 @@ def run_b200(a):
     def mark(mm):
         launches["own0"], launches["lib0"] = ff.kernel_launches()
 
+    dirty, rounds = [], []
+
+    def device_step_stats(mm, s):
+        for k in range(s * FRAMES_PER_STEP, (s + 1) * FRAMES_PER_STEP):
+            mm.addMapDevice(depth[k].data_ptr(), bgr[k].data_ptr(), WIDTH, HEIGHT, cams[k], SCALING, MAXCAM)
+            rounds.append(mm.stats()["dedupe_rounds"])
+        mm.updateMeshes()
+        dirty.append(mm.stats()["mesh_cells_dirty"])
+
     dev_ms, dev_wall = timed(device_step, m, mark)
     own1, lib1 = ff.kernel_launches()
     gpu_launches, lib_calls = own1 - launches["own0"], lib1 - launches["lib0"]
@@ -304,7 +313,7 @@ def run_b200(a):
 
     # 2. per-stage profile of the same steps (separate map; events per stage)
     m = new_map()
-    prof_ms, _ = timed(device_step, m, lambda mm: mm.profile(True))
+    prof_ms, _ = timed(device_step_stats, m, lambda mm: mm.profile(True))
     stages = m.profile_read()
     m.close()
     del m
@@ -319,7 +328,9 @@ def run_b200(a):
         hb = h_bgr.numpy()
         d2h = []
         last_mesh = {}
-        mesh_buf = ff.MeshBuffer()
+        # page-locked mesh buffer reserved before the timed region, like a
+        # viewer would size it for its scene (it grows if the mesh outgrows it)
+        mesh_buf = ff.MeshBuffer(4 << 20, 6 << 20)
 
         def host_step(mm, s):
             for k in range(s * FRAMES_PER_STEP, (s + 1) * FRAMES_PER_STEP):
@@ -388,7 +399,9 @@ def run_b200(a):
             "wall_s_timed": round(dev_wall, 3), "surface_rms_m": rms,
             "map": {"leaves": st["leaves_used"], "leaves_max": st["leaves_max"], "n": st["n"],
                     "mesh_vertices": st["mesh_vertices"], "mesh_faces": st["mesh_faces"],
-                    "mesh_cells": st["mesh_cells"], "grows": st["grows"], "meshing_ok": st["meshing_ok"]},
+                    "mesh_cells": st["mesh_cells"], "grows": st["grows"], "meshing_ok": st["meshing_ok"],
+                    "mesh_cells_dirty_mean": float(np.mean(dirty)) if dirty else None,
+                    "dedupe_rounds_mean": float(np.mean(rounds)) if rounds else None},
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -74,13 +74,14 @@ void launch_first_bbox(const uint16_t *depth, int W, int H, const CamF &p, float
 // round-to-nearest with no fused multiply-add.  w = target brick edge in
 // voxels, floor(max(depth,1)*8) (leafScaleFunc, inline_functions.hpp:128-145),
 // or -1 for invalid depth.
-__global__ void k_project(const uint16_t *depth, int W, int H, const float *pxp, const float *pyp, CamF p,
-                          float scaling, float maxcam, int4 *vox) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= W * H) return;
-  int x = i % W, y = i / W;
-  float d = (float)depth[i];
-  float px = pxp[x], py = pyp[y];
+// Voxel coordinates of a pixel's surface point and its target brick scale
+// (-1: invalid), under the default rounding: ((qxp+qyp)*d)*scaling + t per
+// axis, truncated (traversal_wrapper_functions.cpp:613-630), and
+// leafScaleFunc's floor(max(z,1)*8) (inline_functions.hpp:128-145).
+__device__ __forceinline__ int4 project_pixel(const uint16_t *depth, int W, int x, int y, const float *pxp,
+                                              const float *pyp, const CamF &p, float scaling, float maxcam) {
+  const float d = (float)depth[(size_t)y * W + x];
+  const float px = pxp[x], py = pyp[y];
   int v[3];
 #pragma unroll
   for (int r = 0; r < 3; r++) {
@@ -89,20 +90,13 @@ __global__ void k_project(const uint16_t *depth, int W, int H, const float *pxp,
     float s = __fadd_rn(__fmul_rn(__fmul_rn(__fadd_rn(qx, qy), d), scaling), p.t[r]);
     v[r] = __float2int_rz(s);
   }
-  float ds = __fmul_rn(d, scaling);
+  const float ds = __fmul_rn(d, scaling);
   int target = -1;
   if (ds > 0.0f && ds < maxcam) {
     float f = ds < 1.0f ? 1.0f : ds;
     target = (int)(uint16_t)floorf(__fmul_rn(f, 8.0f));
   }
-  vox[i] = make_int4(v[0], v[1], v[2], target);
-}
-
-void launch_project(const uint16_t *depth, int W, int H, const float *pxp, const float *pyp, const CamF &p,
-                    float scaling, float maxcam, int4 *vox, cudaStream_t s) {
-  int n = W * H;
-  note_launch();
-  k_project<<<(n + 255) / 256, 256, 0, s>>>(depth, W, H, pxp, pyp, p, scaling, maxcam, vox);
+  return make_int4(v[0], v[1], v[2], target);
 }
 
 // ------------------------------------------------------------- dedupe -----
@@ -162,17 +156,24 @@ constexpr int DD_TILES_MAX = 4;  // tiles per warp; the first one is kept in sha
 // above and the column state to the left (read from the previous round's
 // boundary buffers; all-unprocessed in round 0).  Returns the tile's
 // processed bits (bit r of lane l = pixel (l, r) of the tile).
-__device__ __forceinline__ uint32_t dedupe_tile(const int4 *__restrict__ vox, const int4 *tile_s, int W, int H,
+__device__ __forceinline__ uint32_t dedupe_tile(const int4 *vox, const int4 *tile_s, int W, int H,
                                                 int tilesX, int tile, int round, int4 *const right[2],
                                                 int4 *const bottom[2], int &changed) {
   const int lane = threadIdx.x & 31;
   const int in = round & 1, out = in ^ 1;
   const int tx = tile % tilesX, ty = tile / tilesX;
   const int x = tx * 32 + lane;
-  int4 above = make_int4(0, 0, 0, 0);
-  if (round > 0 && ty > 0) above = bottom[in][(size_t)(tile - tilesX) * 32 + lane];
-  int4 prev_bottom = make_int4(0, 0, 0, 0);
-  if (round > 0) prev_bottom = bottom[in][(size_t)tile * 32 + lane];
+  // boundary state of the previous round, fetched up front: the row above
+  // (lane = column), the column to the left and this tile's own right column
+  // (lane = row; broadcast to the row's lane when it is reached)
+  int4 above = make_int4(0, 0, 0, 0), prev_bottom = make_int4(0, 0, 0, 0);
+  int4 leftcol = make_int4(0, 0, 0, 0), owncol = make_int4(0, 0, 0, 0);
+  if (round > 0) {
+    if (ty > 0) above = bottom[in][(size_t)(tile - tilesX) * 32 + lane];
+    prev_bottom = bottom[in][(size_t)tile * 32 + lane];
+    if (tx > 0 && ty * 32 + lane < H) leftcol = right[in][(size_t)(tile - 1) * 32 + lane];
+    if (ty * 32 + lane < H) owncol = right[in][(size_t)tile * 32 + lane];
+  }
   int ak = above.x, bk = above.y, ck = above.z, ap = above.w;
   uint32_t bits = 0;
   for (int r = 0; r < 32; r++) {
@@ -188,14 +189,14 @@ __device__ __forceinline__ uint32_t dedupe_tile(const int4 *__restrict__ vox, co
       k0 = v.x & -8, k1 = v.y & -8, k2 = v.z & -8, valid = v.w >= 0;
     }
     const int a = valid && !(ap && k0 == ak && k1 == bk && k2 == ck);
-    int4 left = make_int4(0, 0, 0, 0);
-    if (lane == 0 && tx > 0 && round > 0) left = right[in][(size_t)(tile - 1) * 32 + r];
+    const int lx = __shfl_sync(0xffffffffu, leftcol.x, r), ly = __shfl_sync(0xffffffffu, leftcol.y, r);
+    const int lz = __shfl_sync(0xffffffffu, leftcol.z, r), lw = __shfl_sync(0xffffffffu, leftcol.w, r);
     const int p0 = __shfl_up_sync(0xffffffffu, k0, 1);
     const int p1 = __shfl_up_sync(0xffffffffu, k1, 1);
     const int p2 = __shfl_up_sync(0xffffffffu, k2, 1);
     uint32_t T;
     if (lane == 0) {
-      const int e = left.w && left.x == k0 && left.y == k1 && left.z == k2;
+      const int e = lw && lx == k0 && ly == k1 && lz == k2;
       const uint32_t c = (a && !e) ? 1u : 0u;
       T = c | (c << 1);
     } else {
@@ -213,15 +214,11 @@ __device__ __forceinline__ uint32_t dedupe_tile(const int4 *__restrict__ vox, co
     ck = k2;
     ap = p;
     bits |= (uint32_t)p << r;
+    const int ox = __shfl_sync(0xffffffffu, owncol.x, r), oy = __shfl_sync(0xffffffffu, owncol.y, r);
+    const int oz = __shfl_sync(0xffffffffu, owncol.z, r), ow = __shfl_sync(0xffffffffu, owncol.w, r);
     if (lane == 31) {
-      const int4 nv = make_int4(k0, k1, k2, p);
-      if (round == 0) {
-        changed = 1;
-      } else {
-        const int4 ov = right[in][(size_t)tile * 32 + r];
-        if (ov.x != nv.x || ov.y != nv.y || ov.z != nv.z || ov.w != nv.w) changed = 1;
-      }
-      right[out][(size_t)tile * 32 + r] = nv;
+      if (round == 0 || ox != k0 || oy != k1 || oz != k2 || ow != p) changed = 1;
+      right[out][(size_t)tile * 32 + r] = make_int4(k0, k1, k2, p);
     }
   }
   const int4 nb = make_int4(ak, bk, ck, ap);
@@ -233,9 +230,10 @@ __device__ __forceinline__ uint32_t dedupe_tile(const int4 *__restrict__ vox, co
 }
 
 // bar: [0] arrivals, [1] generation, [4..6] per-round change counters (rotating)
-__global__ void __launch_bounds__(32 * DD_WARPS) k_dedupe(const int4 *__restrict__ vox, int W, int H, int tilesX,
-                                                          int tilesY, int4 *bnd, uint8_t *processed, Counters *cnt,
-                                                          uint32_t *bar) {
+__global__ void __launch_bounds__(32 * DD_WARPS)
+    k_dedupe(const uint16_t *__restrict__ depth, const float *__restrict__ pxp, const float *__restrict__ pyp, CamF cam,
+             float scaling, float maxcam, int4 *vox, int W, int H, int tilesX, int tilesY, int4 *bnd,
+             uint8_t *processed, Counters *cnt, uint32_t *bar) {
   extern __shared__ int4 dd_tiles[];
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -244,16 +242,23 @@ __global__ void __launch_bounds__(32 * DD_WARPS) k_dedupe(const int4 *__restrict
   // boundary buffers: [2][ntiles][32] right-column states and [2][ntiles][32] bottom-row states
   int4 *const right[2] = {bnd, bnd + (size_t)ntiles * 32};
   int4 *const bottom[2] = {bnd + (size_t)2 * ntiles * 32, bnd + (size_t)3 * ntiles * 32};
-  // the warp's first tile: brick keys and validity, read once for all rounds
+  // project the warp's tiles (voxel keys for the insert that follows); the
+  // first tile's brick keys and validity stay in shared memory for all rounds
   int4 *tile_s = dd_tiles + (size_t)(threadIdx.x >> 5) * 32 * 32;
-  if (warp < ntiles) {
-    const int tx = warp % tilesX, ty = warp / tilesX;
+  for (int ti = 0; ti < DD_TILES_MAX; ti++) {
+    const int tile = warp + ti * nwarps;
+    if (tile >= ntiles) break;
+    const int tx = tile % tilesX, ty = tile / tilesX;
     const int x = tx * 32 + lane;
+#pragma unroll 4
     for (int r = 0; r < 32; r++) {
       const int y = ty * 32 + r;
       int4 v = make_int4(0, 0, 0, -1);
-      if (x < W && y < H) v = vox[(size_t)y * W + x];
-      tile_s[r * 32 + lane] = make_int4(v.x & -8, v.y & -8, v.z & -8, v.w >= 0 ? 1 : 0);
+      if (x < W && y < H) {
+        v = project_pixel(depth, W, x, y, pxp, pyp, cam, scaling, maxcam);
+        vox[(size_t)y * W + x] = v;
+      }
+      if (ti == 0) tile_s[r * 32 + lane] = make_int4(v.x & -8, v.y & -8, v.z & -8, v.w >= 0 ? 1 : 0);
     }
   }
   __syncwarp();
@@ -301,7 +306,8 @@ __global__ void __launch_bounds__(32 * DD_WARPS) k_dedupe(const int4 *__restrict
   }
 }
 
-cudaError_t launch_dedupe(const int4 *vox, int W, int H, int4 *bnd, uint8_t *processed, Counters *cnt,
+cudaError_t launch_dedupe(const uint16_t *depth, const float *pxp, const float *pyp, const CamF &cam, float scaling,
+                          float maxcam, int4 *vox, int W, int H, int4 *bnd, uint8_t *processed, Counters *cnt,
                           uint32_t *barrier, int device, cudaStream_t s) {
   int tilesX = (W + 31) / 32, tilesY = (H + 31) / 32;
   int ntiles = tilesX * tilesY;
@@ -324,7 +330,9 @@ cudaError_t launch_dedupe(const int4 *vox, int W, int H, int4 *bnd, uint8_t *pro
   int blocks = want < maxb ? want : maxb;
   if (blocks < 1) blocks = 1;
   if ((size_t)blocks * DD_WARPS * DD_TILES_MAX < (size_t)ntiles) return cudaErrorInvalidConfiguration;
-  void *args[] = {(void *)&vox, (void *)&W, (void *)&H, (void *)&tilesX, (void *)&tilesY, (void *)&bnd,
+  CamF camv = cam;
+  void *args[] = {(void *)&depth, (void *)&pxp, (void *)&pyp, (void *)&camv, (void *)&scaling, (void *)&maxcam,
+                  (void *)&vox, (void *)&W, (void *)&H, (void *)&tilesX, (void *)&tilesY, (void *)&bnd,
                   (void *)&processed, (void *)&cnt, (void *)&barrier};
   note_launch();
   return cudaLaunchCooperativeKernel((const void *)k_dedupe, dim3(blocks), dim3(threads), args, smem, s);
@@ -483,18 +491,22 @@ cudaError_t sort_pending(const PendingLeaf *pend, int npend, uint32_t *keys_in, 
 // Leaf index = leaves_before + rank of first pixel; indices past the pool are
 // stored in the tree but get no leaf record, like addLeaf's overflow
 // (traversal_functions.cpp:201-210).
-__global__ void k_finalize(const PendingLeaf *pend, const uint32_t *order, int npend, uint32_t leaves_before,
-                           uint32_t leaves_max, uint32_t *tree, ushort4 *leaf, uint32_t frame, uint32_t *stamp,
-                           uint32_t *queue, Counters *cnt) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= npend) return;
-  const PendingLeaf p = pend[order[j]];
-  const uint32_t idx = leaves_before + (uint32_t)j;
+__device__ __forceinline__ void finalize_one(const PendingLeaf &p, uint32_t idx, uint32_t leaves_max, uint32_t *tree,
+                                             ushort4 *leaf, uint32_t frame, uint32_t *stamp, uint32_t *queue,
+                                             Counters *cnt) {
   tree[p.slot] = idx;
   if (idx < leaves_max) {
     leaf[idx] = p.pos;
     queue_leaf(idx, frame, stamp, queue, cnt);
   }
+}
+
+__global__ void k_finalize(const PendingLeaf *pend, const uint32_t *order, int npend, uint32_t leaves_before,
+                           uint32_t leaves_max, uint32_t *tree, ushort4 *leaf, uint32_t frame, uint32_t *stamp,
+                           uint32_t *queue, Counters *cnt) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= npend) return;
+  finalize_one(pend[order[j]], leaves_before + (uint32_t)j, leaves_max, tree, leaf, frame, stamp, queue, cnt);
 }
 
 void launch_finalize(const PendingLeaf *pend, const uint32_t *order, int npend, uint32_t leaves_before,
@@ -510,13 +522,8 @@ void launch_finalize(const PendingLeaf *pend, const uint32_t *order, int npend, 
 // reference records the last leaf met on the descent (`pl`,
 // traversal_functions.cpp:327-333, 376-379); leaves of this frame exist in
 // index order, so that is the finest ancestor with a smaller index.
-__global__ void k_parents(int npend, uint32_t leaves_before, uint32_t leaves_max, const uint32_t *tree, uint32_t n,
-                          const ushort4 *leaf, uint32_t *parent) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= npend) return;
-  const uint32_t idx = leaves_before + (uint32_t)j;
-  if (idx >= leaves_max) return;
-  const ushort4 p = leaf[idx];
+__device__ __forceinline__ uint32_t parent_of(uint32_t idx, uint32_t leaves_max, const uint32_t *tree, uint32_t n,
+                                              const ushort4 &p) {
   const uint32_t edge = (uint32_t)p.w * BL;
   uint32_t ox = 0, oy = 0, oz = 0, half = n >> 1, branch = 0, pl = BRANCHINIT;
   while (half > edge) {
@@ -530,7 +537,65 @@ __global__ void k_parents(int npend, uint32_t leaves_before, uint32_t leaves_max
     oz += half * ((co & 4) != 0);
     half >>= 1;
   }
-  parent[idx] = pl;
+  return pl;
+}
+
+__global__ void k_parents(int npend, uint32_t leaves_before, uint32_t leaves_max, const uint32_t *tree, uint32_t n,
+                          const ushort4 *leaf, uint32_t *parent) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= npend) return;
+  const uint32_t idx = leaves_before + (uint32_t)j;
+  if (idx >= leaves_max) return;
+  parent[idx] = parent_of(idx, leaves_max, tree, n, leaf[idx]);
+}
+
+// The whole frame's pending leaves in one block: order by first pixel (block
+// radix sort), assign indices and fill the leaf table, then the parents.
+constexpr int FIN_THREADS = 1024, FIN_ITEMS = 4;
+constexpr int FIN_MAX = FIN_THREADS * FIN_ITEMS;
+
+__global__ void __launch_bounds__(FIN_THREADS) k_finalize_small(const PendingLeaf *pend, int npend, int end_bit,
+                                                                uint32_t leaves_before, uint32_t leaves_max,
+                                                                uint32_t *tree, ushort4 *leaf, uint32_t frame,
+                                                                uint32_t *stamp, uint32_t *queue, Counters *cnt,
+                                                                uint32_t n, uint32_t *parent) {
+  using Sort = cub::BlockRadixSort<uint32_t, FIN_THREADS, FIN_ITEMS, uint32_t>;
+  __shared__ typename Sort::TempStorage tmp;
+  uint32_t key[FIN_ITEMS], val[FIN_ITEMS];
+  // first pixels are distinct and below 2^end_bit; padding sorts after them
+  // (stable sort, padding placed last)
+  const uint32_t pad = end_bit >= 32 ? 0xFFFFFFFFu : ((1u << end_bit) - 1u);
+#pragma unroll
+  for (int i = 0; i < FIN_ITEMS; i++) {
+    const int j = threadIdx.x * FIN_ITEMS + i;
+    key[i] = j < npend ? pend[j].first_pixel : pad;
+    val[i] = (uint32_t)j;
+  }
+  Sort(tmp).Sort(key, val, 0, end_bit);
+#pragma unroll
+  for (int i = 0; i < FIN_ITEMS; i++) {
+    const int j = threadIdx.x * FIN_ITEMS + i;
+    if (j < npend)
+      finalize_one(pend[val[i]], leaves_before + (uint32_t)j, leaves_max, tree, leaf, frame, stamp, queue, cnt);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < FIN_ITEMS; i++) {
+    const int j = threadIdx.x * FIN_ITEMS + i;
+    const uint32_t idx = leaves_before + (uint32_t)j;
+    if (j < npend && idx < leaves_max) parent[idx] = parent_of(idx, leaves_max, tree, n, leaf[idx]);
+  }
+}
+
+bool launch_finalize_small(const PendingLeaf *pend, int npend, int end_bit, uint32_t leaves_before,
+                           uint32_t leaves_max, uint32_t *tree, ushort4 *leaf, uint32_t frame, uint32_t *stamp,
+                           uint32_t *queue, Counters *cnt, uint32_t n, uint32_t *parent, cudaStream_t s) {
+  if (npend <= 0) return true;
+  if (npend > FIN_MAX) return false;
+  note_launch();
+  k_finalize_small<<<1, FIN_THREADS, 0, s>>>(pend, npend, end_bit, leaves_before, leaves_max, tree, leaf, frame,
+                                             stamp, queue, cnt, n, parent);
+  return true;
 }
 
 void launch_parents(int npend, uint32_t leaves_before, uint32_t leaves_max, const uint32_t *tree, uint32_t n,

@@ -63,7 +63,7 @@ struct ff_handle {
   uint32_t n = 0;
   float offset[3] = {0, 0, 0};
   uint32_t leaves_used = 0, branches_used = 16;
-  uint32_t frames = 0, queued = 0, grows = 0, processed = 0, new_leaves = 0;
+  uint32_t frames = 0, queued = 0, grows = 0, processed = 0, new_leaves = 0, dedupe_rounds = 0;
   bool meshing_ok = true;
   uint16_t bandwidth = 0;
 
@@ -453,12 +453,10 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
   CamF q = cam_grid_to_camera(h, K, R, t);
 
   const double npix = (double)W * H;
-  int pi = h->prof.begin(ST_PROJECT, s);
-  launch_project(d_depth, W, H, h->d_pxp, h->d_pyp, p, scaling, maxcam, h->d_vox, s);
-  h->prof.end(pi, npix * (2 + 16), s);  // depth in, voxel key out
-  pi = h->prof.begin(ST_DEDUPE, s);
-  CK(launch_dedupe(h->d_vox, W, H, h->d_bnd, h->d_proc, h->d_cnt, h->d_barrier, h->cfg.device, s));
-  h->prof.end(pi, npix * (16 + 1), s);  // keys in, processed flags out
+  int pi = h->prof.begin(ST_DEDUPE, s);
+  CK(launch_dedupe(d_depth, h->d_pxp, h->d_pyp, p, scaling, maxcam, h->d_vox, W, H, h->d_bnd, h->d_proc, h->d_cnt,
+                   h->d_barrier, h->cfg.device, s));
+  h->prof.end(pi, npix * (2 + 16 + 1), s);  // depth in; voxel keys and processed flags out
   pi = h->prof.begin(ST_INSERT, s);
   launch_insert(h->d_vox, h->d_proc, W, H, h->n, h->bandwidth, h->d_tree, h->cfg.leaves_max, h->cfg.branches_max,
                 frame, h->d_stamp, h->d_queue, h->d_pend, (uint32_t)(W * H), h->d_cnt, s);
@@ -472,6 +470,7 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
   if (hc.error & ERR_BRANCH_OVERFLOW) h->meshing_ok = false;
   h->branches_used = std::min(hc.branches_used, h->cfg.branches_max);
   h->processed = hc.processed;
+  h->dedupe_rounds = hc.dedupe_iters;
   const uint32_t npend = hc.pending;
   const uint32_t leaves_before = h->leaves_used;
   const uint32_t existing_queued = hc.queued;
@@ -481,10 +480,14 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
              *v_out = h->d_keys + 3 * h->cap_pix;
     int end_bit = 1;
     while ((1u << end_bit) < (uint32_t)(W * H)) end_bit++;
-    CK(sort_pending(h->d_pend, (int)npend, k_in, v_in, k_out, v_out, h->d_sort_tmp, h->sort_tmp_bytes, end_bit, s));
-    launch_finalize(h->d_pend, v_out, (int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->d_leaf, frame,
-                    h->d_stamp, h->d_queue, h->d_cnt, s);
-    launch_parents((int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->n, h->d_leaf, h->d_parent, s);
+    if (!launch_finalize_small(h->d_pend, (int)npend, end_bit, leaves_before, h->cfg.leaves_max, h->d_tree,
+                               h->d_leaf, frame, h->d_stamp, h->d_queue, h->d_cnt, h->n, h->d_parent, s)) {
+      CK(sort_pending(h->d_pend, (int)npend, k_in, v_in, k_out, v_out, h->d_sort_tmp, h->sort_tmp_bytes, end_bit,
+                      s));
+      launch_finalize(h->d_pend, v_out, (int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->d_leaf, frame,
+                      h->d_stamp, h->d_queue, h->d_cnt, s);
+      launch_parents((int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->n, h->d_leaf, h->d_parent, s);
+    }
     h->prof.end(pi, (double)npend * (sizeof(PendingLeaf) + 8 + 4), s);
     h->leaves_used += npend;
   }
@@ -495,7 +498,10 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
   if (h->leaves_used < h->cfg.leaves_max && h->branches_used < h->cfg.branches_max &&
       (hc.box_min[0] < 0 || hc.box_min[1] < 0 || hc.box_min[2] < 0 || hc.box_max[0] >= (int)h->n ||
        hc.box_max[1] >= (int)h->n || hc.box_max[2] >= (int)h->n)) {
+    pi = h->prof.begin(ST_GROW, s);
+    const double tree_bytes = (double)h->branches_used * 4 * 2 + (double)h->leaves_used * 8 * 2;
     ff_status st = grow(h, hc.box_min, hc.box_max);
+    h->prof.end(pi, tree_bytes, s);  // octree and leaf positions read and written
     if (st != FF_OK) return st;
   }
   // fuse: every voxel of every queued brick read and written: SDF, weight
@@ -564,6 +570,7 @@ ff_status ff_get_stats(ff_handle *h, ff_stats *o) {
   o->mesh_cells_dirty = h->mesh.n_dirty;
   o->processed_pixels = h->processed;
   o->new_leaves = h->new_leaves;
+  o->dedupe_rounds = h->dedupe_rounds;
   return FF_OK;
 }
 

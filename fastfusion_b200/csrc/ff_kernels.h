@@ -20,13 +20,12 @@ struct PendingLeaf {
 void launch_first_bbox(const uint16_t *depth, int W, int H, const CamF &p, float scaling, float maxcam, int bw,
                        Counters *cnt, cudaStream_t s);
 
-// Per-pixel voxel coordinates, validity and target brick scale.
-void launch_project(const uint16_t *depth, int W, int H, const float *pxp, const float *pyp, const CamF &p,
-                    float scaling, float maxcam, int4 *vox, cudaStream_t s);
-
-// Row/column de-duplication of brick keys (traversal_wrapper_functions.cpp:636-639, 688-690).
-// bnd: 4 buffers of boundary state; barrier: 2 uint32 words for the grid barrier.
-cudaError_t launch_dedupe(const int4 *vox, int W, int H, int4 *bnd, uint8_t *processed, Counters *cnt,
+// Per-pixel voxel coordinates, validity and target brick scale (written to
+// vox), then the row/column de-duplication of brick keys
+// (traversal_wrapper_functions.cpp:613-639, 688-690).
+// bnd: 4 buffers of boundary state; barrier: 8 zeroed uint32 words.
+cudaError_t launch_dedupe(const uint16_t *depth, const float *pxp, const float *pyp, const CamF &cam, float scaling,
+                          float maxcam, int4 *vox, int W, int H, int4 *bnd, uint8_t *processed, Counters *cnt,
                           uint32_t *barrier, int device, cudaStream_t s);
 
 // Octree descent / allocation of every processed pixel.
@@ -47,6 +46,12 @@ void launch_finalize(const PendingLeaf *pend, const uint32_t *order, int npend, 
 // Parent leaf of each new leaf: finest ancestor leaf created before it.
 void launch_parents(int npend, uint32_t leaves_before, uint32_t leaves_max, const uint32_t *tree, uint32_t n,
                     const ushort4 *leaf, uint32_t *parent, cudaStream_t s);
+
+// Sort, finalize and parents of up to 4096 pending leaves in one launch;
+// false (nothing launched) for more.
+bool launch_finalize_small(const PendingLeaf *pend, int npend, int end_bit, uint32_t leaves_before,
+                           uint32_t leaves_max, uint32_t *tree, ushort4 *leaf, uint32_t frame, uint32_t *stamp,
+                           uint32_t *queue, Counters *cnt, uint32_t n, uint32_t *parent, cudaStream_t s);
 
 // grow(): move child-branch pointers by `shift`, leaf positions by `add`.
 void launch_shift_branches(uint32_t *tree, uint32_t used, uint32_t shift, cudaStream_t s);

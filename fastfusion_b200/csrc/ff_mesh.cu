@@ -1023,19 +1023,53 @@ __global__ void k_fill_counts_from_old(const uint8_t *dirty, const int32_t *old_
 // Host side
 // ---------------------------------------------------------------------------
 
+// The mesher's buffers come from one stream-ordered pool per device that
+// keeps freed memory (release threshold: never), so regrowing a buffer as the
+// map grows neither synchronises nor returns memory to the driver.
+static cudaError_t pool_of_current_device(cudaMemPool_t &pool) {
+  static cudaMemPool_t pools[64] = {};
+  static std::atomic<unsigned long long> made{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!(made.load() & (1ull << dev))) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    e = cudaMemPoolCreate(&p, &props);
+    if (e != cudaSuccess) return e;
+    uint64_t keep_all = ~0ull;
+    e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep_all);
+    if (e != cudaSuccess) return e;
+    pools[dev] = p;
+    made.fetch_or(1ull << dev);
+  }
+  pool = pools[dev];
+  return cudaSuccess;
+}
+
+static cudaError_t pool_alloc(void **p, size_t bytes, cudaStream_t s) {
+  cudaMemPool_t pool;
+  cudaError_t e = pool_of_current_device(pool);
+  if (e != cudaSuccess) return e;
+  return cudaMallocFromPoolAsync(p, bytes, pool, s);
+}
+
 template <typename T>
-static cudaError_t grow_buf(T *&p, size_t &cap, size_t need, bool keep = false, cudaStream_t s = 0) {
+static cudaError_t grow_buf(T *&p, size_t &cap, size_t need, cudaStream_t s) {
   if (need <= cap && p) return cudaSuccess;
   size_t ncap = std::max<size_t>(need + need / 2, 1024);
-  T *q = nullptr;
-  cudaError_t e = cudaMalloc((void **)&q, sizeof(T) * ncap);
+  void *q = nullptr;
+  cudaError_t e = pool_alloc(&q, sizeof(T) * ncap, s);
   if (e != cudaSuccess) return e;
-  if (keep && p && cap) cudaMemcpyAsync(q, p, sizeof(T) * cap, cudaMemcpyDeviceToDevice, s);
   if (p) {
-    cudaStreamSynchronize(s);
-    cudaFree(p);
+    e = cudaFreeAsync(p, s);
+    if (e != cudaSuccess) return e;
   }
-  p = q;
+  p = (T *)q;
   cap = ncap;
   return cudaSuccess;
 }
@@ -1048,6 +1082,7 @@ struct MeshImpl {
   VertItem *vertq[2] = {nullptr, nullptr};
   size_t cap_cellq[2] = {0, 0}, cap_faceq[2] = {0, 0}, cap_edgeq[2] = {0, 0}, cap_vertq[2] = {0, 0};
   uint32_t n_corners = 0;
+  size_t peak[5] = {0, 0, 0, 0, 0};  // last update's largest level of each queue, and its cell count
   // words 8 n_cells, 9 error, 10 n_dirty, 11 n_corners, 12-13 samples;
   // from LEVEL_COUNTS: 4 item counters per generation level
   uint32_t *d_count = nullptr;
@@ -1099,18 +1134,22 @@ static MeshImpl &impl(MeshState &m) {
 
 // Generate, sort and store the mesh cells of the current octree.
 static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uint32_t &ncells, std::string &err) {
+  // queue sizes: a first guess from the octree size, then the previous
+  // update's peaks with headroom (the map grows slowly between updates)
   const uint32_t slots = std::max<uint32_t>(in.branches_used / 2, 64);
-  size_t want_q = (size_t)slots * 2 + 4096;
+  size_t want[5] = {(size_t)slots * 2 + 4096, (size_t)slots * 4 + 4096, (size_t)slots * 4 + 4096,
+                    (size_t)slots * 2 + 4096, (size_t)slots * 16 + 4096};
+  for (int k = 0; k < 5; k++) want[k] = std::max<size_t>(want[k], I.peak[k] + I.peak[k] / 4 + 1024);
   for (int attempt = 0; attempt < 6; attempt++) {
     for (int b = 0; b < 2; b++) {
-      MCK(grow_buf(I.cellq[b], I.cap_cellq[b], want_q));
-      MCK(grow_buf(I.faceq[b], I.cap_faceq[b], want_q * 2));
-      MCK(grow_buf(I.edgeq[b], I.cap_edgeq[b], want_q * 2));
-      MCK(grow_buf(I.vertq[b], I.cap_vertq[b], want_q));
+      MCK(grow_buf(I.cellq[b], I.cap_cellq[b], want[0], s));
+      MCK(grow_buf(I.faceq[b], I.cap_faceq[b], want[1], s));
+      MCK(grow_buf(I.edgeq[b], I.cap_edgeq[b], want[2], s));
+      MCK(grow_buf(I.vertq[b], I.cap_vertq[b], want[3], s));
     }
-    MCK(grow_buf(I.raw, I.cap_raw, want_q * 8));
+    MCK(grow_buf(I.raw, I.cap_raw, want[4], s));
     if (!I.d_count) {
-      MCK(cudaMalloc((void **)&I.d_count, COUNT_WORDS * sizeof(uint32_t)));
+      MCK(pool_alloc((void **)&I.d_count, COUNT_WORDS * sizeof(uint32_t), s));
       MCK(cudaMallocHost((void **)&I.h_count, COUNT_WORDS * sizeof(uint32_t)));
     }
     MCK(cudaMemsetAsync(I.d_count, 0, COUNT_WORDS * sizeof(uint32_t), s));
@@ -1153,9 +1192,13 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
     }
     const uint32_t *hc = I.h_count;
     if (overflow) {
-      want_q *= 2;
+      for (int k = 0; k < 5; k++) want[k] *= 2;
       continue;
     }
+    for (int k = 0; k < 5; k++) I.peak[k] = 0;
+    for (int l = 0; l <= lv; l++)
+      for (int k = 0; k < 4; k++) I.peak[k] = std::max<size_t>(I.peak[k], hc[LEVEL_COUNTS + 4 * l + k]);
+    I.peak[4] = hc[8];
     if (leftover) {
       err = "meshing: cell generation did not finish within the level limit";
       return 6;
@@ -1169,11 +1212,11 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
     return 4;
   }
   // sort by key: deterministic order and a stable identity across updates
-  MCK(grow_buf(I.keys, I.cap_keys, ncells));
-  MCK(grow_buf(I.keys_sorted, I.cap_keys2, ncells));
-  MCK(grow_buf(I.vals, I.cap_vals, ncells));
-  MCK(grow_buf(I.vals_sorted, I.cap_vals2, ncells));
-  MCK(grow_buf(I.cells, I.cap_cells, ncells));
+  MCK(grow_buf(I.keys, I.cap_keys, ncells, s));
+  MCK(grow_buf(I.keys_sorted, I.cap_keys2, ncells, s));
+  MCK(grow_buf(I.vals, I.cap_vals, ncells, s));
+  MCK(grow_buf(I.vals_sorted, I.cap_vals2, ncells, s));
+  MCK(grow_buf(I.cells, I.cap_cells, ncells, s));
   if (ncells) {
     note_launch(2);
     k_cell_keys<<<(ncells + 255) / 256, 256, 0, s>>>(I.raw, ncells, I.keys, I.vals);
@@ -1181,8 +1224,9 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
     cub::DeviceRadixSort::SortPairs(nullptr, bytes, I.keys, I.keys_sorted, I.vals, I.vals_sorted, (int)ncells, 0, 57,
                                     s);
     if (bytes > I.sort_tmp_bytes) {
-      if (I.sort_tmp) cudaFree(I.sort_tmp);
-      MCK(cudaMalloc(&I.sort_tmp, bytes));
+      if (I.sort_tmp) MCK(cudaFreeAsync(I.sort_tmp, s));
+      I.sort_tmp = nullptr;
+      MCK(pool_alloc(&I.sort_tmp, bytes, s));
       I.sort_tmp_bytes = bytes;
     }
     note_lib_call();
@@ -1218,13 +1262,13 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   vs.samples = reinterpret_cast<unsigned long long *>(I.d_count + 12);
   MCK(cudaMemsetAsync(I.d_count + 12, 0, 2 * sizeof(uint32_t), s));
 
-  MCK(grow_buf(I.out, I.cap_out, ncells));
-  MCK(grow_buf(I.dirty, I.cap_dirty, ncells));
-  MCK(grow_buf(I.old_index, I.cap_oi, ncells));
-  MCK(grow_buf(I.nv, I.cap_nv, ncells + 1));
-  MCK(grow_buf(I.nf, I.cap_nf, ncells + 1));
-  MCK(grow_buf(I.vbase, I.cap_vb, ncells + 1));
-  MCK(grow_buf(I.fbase, I.cap_fb, ncells + 1));
+  MCK(grow_buf(I.out, I.cap_out, ncells, s));
+  MCK(grow_buf(I.dirty, I.cap_dirty, ncells, s));
+  MCK(grow_buf(I.old_index, I.cap_oi, ncells, s));
+  MCK(grow_buf(I.nv, I.cap_nv, ncells + 1, s));
+  MCK(grow_buf(I.nf, I.cap_nf, ncells + 1, s));
+  MCK(grow_buf(I.vbase, I.cap_vb, ncells + 1, s));
+  MCK(grow_buf(I.fbase, I.cap_fb, ncells + 1, s));
   const bool incremental = M.valid && I.n_old > 0;
   // dirty cells: all on the first update, otherwise those whose inputs changed
   MCK(cudaMemsetAsync(I.d_count + 10, 0, sizeof(uint32_t), s));
@@ -1272,8 +1316,9 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   size_t bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, bytes, I.nv, I.vbase, (int)ncells + 1, s);
   if (bytes > I.scan_tmp_bytes) {
-    if (I.scan_tmp) cudaFree(I.scan_tmp);
-    MCK(cudaMalloc(&I.scan_tmp, bytes));
+    if (I.scan_tmp) MCK(cudaFreeAsync(I.scan_tmp, s));
+    I.scan_tmp = nullptr;
+    MCK(pool_alloc(&I.scan_tmp, bytes, s));
     I.scan_tmp_bytes = bytes;
   }
   note_lib_call();
@@ -1298,9 +1343,9 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   std::swap(I.cap_orgb, I.cap_rgb);
   std::swap(I.old_faces, M.d_faces);
   std::swap(I.cap_ofaces, I.cap_faces);
-  MCK(grow_buf(M.d_xyz, I.cap_xyz, 3 * tot[0] + 3));
-  MCK(grow_buf(M.d_rgb, I.cap_rgb, 3 * tot[0] + 3));
-  MCK(grow_buf(M.d_faces, I.cap_faces, 3 * tot[1] + 3));
+  MCK(grow_buf(M.d_xyz, I.cap_xyz, 3 * tot[0] + 3, s));
+  MCK(grow_buf(M.d_rgb, I.cap_rgb, 3 * tot[0] + 3, s));
+  MCK(grow_buf(M.d_faces, I.cap_faces, 3 * tot[1] + 3, s));
   pi = P.begin(ST_MESH_EMIT, s);
   note_launch((first_corner ? 1 : 0) + (ncells > first_corner ? 1 : 0) + (incremental && ncells ? 1 : 0));
   if (first_corner)
@@ -1399,14 +1444,15 @@ void mesh_free(MeshState &M) {
                     I.old_vbase, I.old_fbase, I.dirty, I.old_index, I.scan_tmp, I.old_xyz, I.old_rgb,
                     I.old_faces};
     for (void *p : ptrs)
-      if (p) cudaFree(p);
+      if (p) cudaFreeAsync(p, 0);
     if (I.h_count) cudaFreeHost(I.h_count);
     delete &I;
     M.impl = nullptr;
   }
-  if (M.d_xyz) cudaFree(M.d_xyz);
-  if (M.d_rgb) cudaFree(M.d_rgb);
-  if (M.d_faces) cudaFree(M.d_faces);
+  if (M.d_xyz) cudaFreeAsync(M.d_xyz, 0);
+  if (M.d_rgb) cudaFreeAsync(M.d_rgb, 0);
+  if (M.d_faces) cudaFreeAsync(M.d_faces, 0);
+  cudaStreamSynchronize(0);
   M.d_xyz = nullptr;
   M.d_rgb = nullptr;
   M.d_faces = nullptr;

@@ -10,7 +10,7 @@
 namespace ffb {
 
 enum Stage {
-  ST_PROJECT = 0,
+  ST_GROW = 0,
   ST_DEDUPE,
   ST_INSERT,
   ST_FINALIZE,

@@ -49,7 +49,7 @@ class ff_stats(ctypes.Structure):
                 ("meshing_ok", ctypes.c_uint32), ("grows", ctypes.c_uint32), ("mesh_vertices", ctypes.c_uint64),
                 ("mesh_faces", ctypes.c_uint64), ("mesh_cells", ctypes.c_uint64),
                 ("mesh_cells_dirty", ctypes.c_uint64), ("processed_pixels", ctypes.c_uint32),
-                ("new_leaves", ctypes.c_uint32)]
+                ("new_leaves", ctypes.c_uint32), ("dedupe_rounds", ctypes.c_uint32)]
 
 
 # Every entry point of include/fastfusion_b200.h with its ctypes signature.
@@ -152,7 +152,8 @@ class MeshBuffer:
     def _grow(self, key: str, nbytes: int):
         if nbytes <= self._cap[key]:
             return
-        nbytes = max(nbytes, int(self._cap[key] * 1.5), 4096)
+        # page-locking is slow, so grow in large steps
+        nbytes = max(nbytes, 2 * self._cap[key], 1 << 16)
         p = ctypes.c_void_p()
         st = self._L.ff_alloc_host(nbytes, ctypes.byref(p))
         if st != FF_OK:
@@ -295,7 +296,7 @@ class FusionMipMapCPU:
         self._check(self._L.ff_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)))
 
     # -- profiling ----------------------------------------------------------
-    PROFILE_STAGES = ("project", "dedupe", "insert", "finalize", "fuse", "mesh_cells", "mesh_count", "mesh_emit")
+    PROFILE_STAGES = ("grow", "dedupe", "insert", "finalize", "fuse", "mesh_cells", "mesh_count", "mesh_emit")
 
     def profile(self, enable: bool = True):
         """Reset the per-stage CUDA-event profile and switch it on or off."""

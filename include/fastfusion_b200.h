@@ -75,6 +75,7 @@ typedef struct ff_stats {
   uint64_t mesh_cells_dirty;   /* cells re-meshed by the last update */
   uint32_t processed_pixels;   /* pixels that passed the row/column de-duplication */
   uint32_t new_leaves;         /* leaves allocated by the last frame */
+  uint32_t dedupe_rounds;      /* rounds the last frame's de-duplication took to settle */
 } ff_stats;
 
 /* Create a map.  Replaces `new FusionMipMapCPU(0,0,0,scale,threshold,0,color)`
@@ -167,8 +168,9 @@ ff_status ff_set_state(ff_handle *h, uint32_t n, const float offset[3], const ui
  * stream.  ff_profile(h, 1) resets and starts recording; ff_profile_read
  * returns, per stage, the summed milliseconds, the algorithmic bytes (bytes
  * the stage must move at minimum: e.g. 14,336 B per fused FP32 brick) and the
- * number of launches.  Stages, in order: project, dedupe, insert, finalize
- * (leaf indices and parents), fuse, mesh_cells (cell generation and sort),
+ * number of launches.  Stages, in order: grow (volume extension), dedupe
+ * (projection and de-duplication of the pixels), insert, finalize (leaf
+ * indices and parents), fuse, mesh_cells (cell generation and sort),
  * mesh_count, mesh_emit. */
 #define FF_PROFILE_STAGES 8
 ff_status ff_profile(ff_handle *h, int enable);

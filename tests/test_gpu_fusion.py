@@ -137,3 +137,21 @@ def test_bit_exact_with_reference_binary(lib_built):
     assert np.array_equal(dg.view(np.uint32), dr.view(np.uint32))
     assert np.array_equal(wg.view(np.uint32), wr.view(np.uint32))
     assert np.array_equal(cg, cr)
+
+
+def test_many_new_leaves_per_frame(lib_built, port_lib):
+    """2 mm voxels on 1280x960 frames create several thousand bricks per
+    frame, more than the single-block leaf finalisation takes, so the
+    multi-kernel sort path runs; results stay bit-exact."""
+    from fastfusion_b200.fusion import FusionMipMapCPU
+    K, frames = circle_frames(0, 3, 1280, 960)
+    g = FusionMipMapCPU(0, 0, 0, 0.002, 0.004, 0, True, leaves_max=400000, branches_max=8000000, rcp="exact")
+    p = port_lib.PortFusion(0.002, 0.004, True, leaves_total=400000, branches_total=8000000, update_mode=1)
+    news = []
+    for depth, bgr, R, t in frames:
+        qg = g.addMap(depth, _cam(K, R, t), bgr, SCALING, MAXCAM)
+        qp = p.add_map(depth, bgr, K, R, t, SCALING, MAXCAM)
+        assert qg == qp
+        news.append(g.stats()["new_leaves"])
+        _compare_frame(g, p)
+    assert max(news) > 4096, news

@@ -23,7 +23,7 @@ def test_profile_counts_match_the_work(lib_built):
     assert set(prof) == set(ff.FusionMipMapCPU.PROFILE_STAGES)
     # one launch of each per-frame stage per frame; the fuse bytes are the
     # 14,336 B of every queued FP32 brick
-    for stage in ("project", "dedupe", "insert", "fuse"):
+    for stage in ("dedupe", "insert", "fuse"):
         assert prof[stage][2] == len(frames), (stage, prof[stage])
         assert prof[stage][0] > 0.0
     assert prof["fuse"][1] == pytest.approx(14336.0 * queued)
@@ -32,8 +32,8 @@ def test_profile_counts_match_the_work(lib_built):
     assert prof["mesh_count"][1] > 0
     st = m.stats()
     assert prof["mesh_emit"][1] >= st["mesh_vertices"] * 15 + st["mesh_faces"] * 12
-    # own kernels: at least project, dedupe, insert, fuse per frame plus the mesher's
-    assert own1 - own0 >= 4 * len(frames) + 4
+    # own kernels: at least dedupe, insert, fuse per frame plus the mesher's
+    assert own1 - own0 >= 3 * len(frames) + 4
     assert lib1 - lib0 >= 3  # cell sort and the two scans
     # switching off: nothing more is recorded
     m.profile(False)
