@@ -59,7 +59,7 @@ STAGE_KERNELS = {
     "grow": "k_shift_branches+k_shift_leaves+copies",
     "dedupe": "k_dedupe (projection + de-duplication)",
     "insert": "k_insert",
-    "finalize": "k_finalize_small",
+    "finalize": "k_finalize_bitmap",
     "fuse": "k_fuse",
     "mesh_cells": "k_gen_level+k_cell_keys+radix sort+k_gather_cells",
     "mesh_count": "k_mesh_lattice<count>+k_mesh_corner<count>",

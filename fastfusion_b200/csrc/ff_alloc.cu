@@ -106,23 +106,15 @@ __device__ __forceinline__ int4 project_pixel(const uint16_t *depth, int W, int 
 // s = k if processed and -1 otherwise (traversal_wrapper_functions.cpp:636-639,
 // 688-690).  This is a recurrence over the two predecessors only, so it has a
 // unique solution.  Each warp solves one 32x32 tile exactly, given the state
-// of the column to its left and the row above it: rows top to bottom, and
-// within a row the left-to-right dependency p(x) = a(x) && !(p(x-1) && k(x)==k(x-1))
-// as an inclusive warp scan over the composition of maps {0,1}->{0,1}.
-// Tiles exchange boundary states and repeat until no boundary changes; a
-// chain of dependencies crosses at most tilesX+tilesY tiles, which bounds the
-// number of rounds.
-
-struct TileSt {
-  int kx, ky, kz, p;
-};
-
-__device__ __forceinline__ uint32_t compose(uint32_t g, uint32_t f) {
-  // maps encoded as (bit0 = f(0), bit1 = f(1)); returns g o f
-  uint32_t h0 = (g >> (f & 1u)) & 1u;
-  uint32_t h1 = (g >> ((f >> 1) & 1u)) & 1u;
-  return h0 | (h1 << 1);
-}
+// of the column to its left and the row above it, rows top to bottom.  The
+// key comparisons never change, so they are made once, as bit masks: per lane
+// valid(r), up(r) = k(x,r)==k(x,r-1), left(r) = k(x,r)==k(x-1,r).  In a row,
+// a(x) = valid && !(p(x,r-1) && up) and p(x) = a(x) && !(p(x-1) && left(x)):
+// p copies a(x) at a lane that is not chained to its left neighbour
+// (a(x)==0 or left(x)==0) and alternates along a chain, so one ballot of the
+// chained lanes and one of the chain starts give the row.  Tiles exchange
+// boundary bits and repeat until no boundary changes; a chain of dependencies
+// crosses at most tilesX+tilesY tiles, which bounds the number of rounds.
 
 __device__ void grid_barrier(uint32_t *bar, uint32_t nblocks, Counters *cnt) {
   __syncthreads();
@@ -149,133 +141,111 @@ __device__ void grid_barrier(uint32_t *bar, uint32_t nblocks, Counters *cnt) {
   __syncthreads();
 }
 
-constexpr int DD_WARPS = 4;      // tiles (warps) per block
-constexpr int DD_TILES_MAX = 4;  // tiles per warp; the first one is kept in shared memory
+constexpr int DD_WARPS = 4;  // tiles (warps) per block
 
-// One tile of one warp, one round: rows top to bottom from the row state
-// above and the column state to the left (read from the previous round's
-// boundary buffers; all-unprocessed in round 0).  Returns the tile's
-// processed bits (bit r of lane l = pixel (l, r) of the tile).
-__device__ __forceinline__ uint32_t dedupe_tile(const int4 *vox, const int4 *tile_s, int W, int H,
-                                                int tilesX, int tile, int round, int4 *const right[2],
-                                                int4 *const bottom[2], int &changed) {
-  const int lane = threadIdx.x & 31;
-  const int in = round & 1, out = in ^ 1;
-  const int tx = tile % tilesX, ty = tile / tilesX;
-  const int x = tx * 32 + lane;
-  // boundary state of the previous round, fetched up front: the row above
-  // (lane = column), the column to the left and this tile's own right column
-  // (lane = row; broadcast to the row's lane when it is reached)
-  int4 above = make_int4(0, 0, 0, 0), prev_bottom = make_int4(0, 0, 0, 0);
-  int4 leftcol = make_int4(0, 0, 0, 0), owncol = make_int4(0, 0, 0, 0);
-  if (round > 0) {
-    if (ty > 0) above = bottom[in][(size_t)(tile - tilesX) * 32 + lane];
-    prev_bottom = bottom[in][(size_t)tile * 32 + lane];
-    if (tx > 0 && ty * 32 + lane < H) leftcol = right[in][(size_t)(tile - 1) * 32 + lane];
-    if (ty * 32 + lane < H) owncol = right[in][(size_t)tile * 32 + lane];
-  }
-  int ak = above.x, bk = above.y, ck = above.z, ap = above.w;
-  uint32_t bits = 0;
-  for (int r = 0; r < 32; r++) {
-    const int y = ty * 32 + r;
-    if (y >= H) break;
-    int k0, k1, k2, valid;
-    if (tile_s) {
-      const int4 t = tile_s[r * 32 + lane];
-      k0 = t.x, k1 = t.y, k2 = t.z, valid = t.w;
-    } else {
-      int4 v = make_int4(0, 0, 0, -1);
-      if (x < W) v = vox[(size_t)y * W + x];
-      k0 = v.x & -8, k1 = v.y & -8, k2 = v.z & -8, valid = v.w >= 0;
-    }
-    const int a = valid && !(ap && k0 == ak && k1 == bk && k2 == ck);
-    const int lx = __shfl_sync(0xffffffffu, leftcol.x, r), ly = __shfl_sync(0xffffffffu, leftcol.y, r);
-    const int lz = __shfl_sync(0xffffffffu, leftcol.z, r), lw = __shfl_sync(0xffffffffu, leftcol.w, r);
-    const int p0 = __shfl_up_sync(0xffffffffu, k0, 1);
-    const int p1 = __shfl_up_sync(0xffffffffu, k1, 1);
-    const int p2 = __shfl_up_sync(0xffffffffu, k2, 1);
-    uint32_t T;
-    if (lane == 0) {
-      const int e = lw && lx == k0 && ly == k1 && lz == k2;
-      const uint32_t c = (a && !e) ? 1u : 0u;
-      T = c | (c << 1);
-    } else {
-      const int e = (p0 == k0 && p1 == k1 && p2 == k2);
-      T = !a ? 0u : (e ? 1u /* NOT: f(0)=1,f(1)=0 */ : 3u);
-    }
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t other = __shfl_up_sync(0xffffffffu, T, o);
-      if (lane >= o) T = compose(T, other);
-    }
-    const int p = T & 1u;
-    ak = k0;
-    bk = k1;
-    ck = k2;
-    ap = p;
-    bits |= (uint32_t)p << r;
-    const int ox = __shfl_sync(0xffffffffu, owncol.x, r), oy = __shfl_sync(0xffffffffu, owncol.y, r);
-    const int oz = __shfl_sync(0xffffffffu, owncol.z, r), ow = __shfl_sync(0xffffffffu, owncol.w, r);
-    if (lane == 31) {
-      if (round == 0 || ox != k0 || oy != k1 || oz != k2 || ow != p) changed = 1;
-      right[out][(size_t)tile * 32 + r] = make_int4(k0, k1, k2, p);
-    }
-  }
-  const int4 nb = make_int4(ak, bk, ck, ap);
-  if (round == 0 || nb.x != prev_bottom.x || nb.y != prev_bottom.y || nb.z != prev_bottom.z ||
-      nb.w != prev_bottom.w)
-    changed = 1;
-  bottom[out][(size_t)tile * 32 + lane] = nb;
-  return bits;
+__device__ __forceinline__ bool same3(int a0, int a1, int a2, int b0, int b1, int b2) {
+  return a0 == b0 && a1 == b1 && a2 == b2;
 }
 
+// bnd layout: right-column keys [ntiles][32] int4, bottom-row keys [ntiles][32]
+// int4 (written once, before the first barrier), then processed bits of the
+// right column and of the bottom row, [2 rounds][ntiles] uint32 each.
 // bar: [0] arrivals, [1] generation, [4..6] per-round change counters (rotating)
 __global__ void __launch_bounds__(32 * DD_WARPS)
     k_dedupe(const uint16_t *__restrict__ depth, const float *__restrict__ pxp, const float *__restrict__ pyp, CamF cam,
              float scaling, float maxcam, int4 *vox, int W, int H, int tilesX, int tilesY, int4 *bnd,
              uint8_t *processed, Counters *cnt, uint32_t *bar) {
-  extern __shared__ int4 dd_tiles[];
   const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int ntiles = tilesX * tilesY;
-  // boundary buffers: [2][ntiles][32] right-column states and [2][ntiles][32] bottom-row states
-  int4 *const right[2] = {bnd, bnd + (size_t)ntiles * 32};
-  int4 *const bottom[2] = {bnd + (size_t)2 * ntiles * 32, bnd + (size_t)3 * ntiles * 32};
-  // project the warp's tiles (voxel keys for the insert that follows); the
-  // first tile's brick keys and validity stay in shared memory for all rounds
-  int4 *tile_s = dd_tiles + (size_t)(threadIdx.x >> 5) * 32 * 32;
-  for (int ti = 0; ti < DD_TILES_MAX; ti++) {
-    const int tile = warp + ti * nwarps;
-    if (tile >= ntiles) break;
-    const int tx = tile % tilesX, ty = tile / tilesX;
-    const int x = tx * 32 + lane;
-#pragma unroll 4
-    for (int r = 0; r < 32; r++) {
-      const int y = ty * 32 + r;
-      int4 v = make_int4(0, 0, 0, -1);
-      if (x < W && y < H) {
-        v = project_pixel(depth, W, x, y, pxp, pyp, cam, scaling, maxcam);
-        vox[(size_t)y * W + x] = v;
-      }
-      if (ti == 0) tile_s[r * 32 + lane] = make_int4(v.x & -8, v.y & -8, v.z & -8, v.w >= 0 ? 1 : 0);
+  const bool active = tile < ntiles;  // warps past the last tile only join the barriers
+  int4 *keyR = bnd, *keyB = bnd + (size_t)ntiles * 32;
+  uint32_t *pR = reinterpret_cast<uint32_t *>(bnd + (size_t)2 * ntiles * 32);
+  uint32_t *pB = pR + 2 * (size_t)ntiles;
+  const int tx = active ? tile % tilesX : 0, ty = active ? tile / tilesX : 0;
+  const int x = tx * 32 + lane;
+  const int rows = active ? min(32, H - ty * 32) : 0;
+  // project the tile (voxel keys for the insert that follows) and make the
+  // key comparisons
+  uint32_t valid = 0, up = 0, left = 0;
+  int c0 = 0, c1 = 0, c2 = 0;     // key at (lane 0, row = lane): compared with the left tile
+  int t0 = 0, t1 = 0, t2 = 0;     // key at (lane, row 0): compared with the tile above
+  int u0 = 0, u1 = 0, u2 = 0;     // key of the previous row
+  for (int r = 0; r < rows; r++) {
+    const int y = ty * 32 + r;
+    int4 v = make_int4(0, 0, 0, -1);
+    if (x < W) {
+      v = project_pixel(depth, W, x, y, pxp, pyp, cam, scaling, maxcam);
+      vox[(size_t)y * W + x] = v;
     }
+    const int k0 = v.x & -8, k1 = v.y & -8, k2 = v.z & -8;
+    const int l0 = __shfl_up_sync(0xffffffffu, k0, 1);
+    const int l1 = __shfl_up_sync(0xffffffffu, k1, 1);
+    const int l2 = __shfl_up_sync(0xffffffffu, k2, 1);
+    const int f0 = __shfl_sync(0xffffffffu, k0, 0);
+    const int f1 = __shfl_sync(0xffffffffu, k1, 0);
+    const int f2 = __shfl_sync(0xffffffffu, k2, 0);
+    if (lane == r) c0 = f0, c1 = f1, c2 = f2;
+    if (r == 0) t0 = k0, t1 = k1, t2 = k2;
+    if (x < W && v.w >= 0) valid |= 1u << r;
+    if (r > 0 && same3(k0, k1, k2, u0, u1, u2)) up |= 1u << r;
+    if (lane > 0 && same3(k0, k1, k2, l0, l1, l2)) left |= 1u << r;
+    u0 = k0, u1 = k1, u2 = k2;
+    if (lane == 31) keyR[(size_t)tile * 32 + r] = make_int4(k0, k1, k2, 0);
+    if (r == rows - 1) keyB[(size_t)tile * 32 + lane] = make_int4(k0, k1, k2, 0);
   }
-  __syncwarp();
-  uint32_t bits[DD_TILES_MAX];
+  uint32_t eq_left = 0;  // row bits: lane 0's key equals the left tile's right column
+  bool eq_above = false;  // this lane's row-0 key equals the above tile's bottom row
+  uint32_t bits = 0, last_r = 0, last_b = 0;
   const int max_rounds = tilesX + tilesY + 1;
   volatile uint32_t *chg = bar + 4;
   int round = 0;
   bool converged = false;
   for (; round < max_rounds; round++) {
+    const int in = round & 1, out = in ^ 1;
     int changed = 0;
-#pragma unroll
-    for (int ti = 0; ti < DD_TILES_MAX; ti++) {
-      const int tile = warp + ti * nwarps;
-      if (tile < ntiles)
-        bits[ti] = dedupe_tile(vox, ti == 0 ? tile_s : nullptr, W, H, tilesX, tile, round, right, bottom, changed);
+    if (active) {
+      uint32_t left_p = 0, above_p = 0;
+      if (round > 0) {
+        if (round == 1) {
+          // boundary keys were published before the first barrier
+          bool eq = false;
+          if (tx > 0 && lane < rows) {
+            const int4 k = keyR[(size_t)(tile - 1) * 32 + lane];
+            eq = same3(k.x, k.y, k.z, c0, c1, c2);
+          }
+          eq_left = __ballot_sync(0xffffffffu, eq);
+          if (ty > 0) {
+            const int4 k = keyB[(size_t)(tile - tilesX) * 32 + lane];
+            eq_above = same3(k.x, k.y, k.z, t0, t1, t2);
+          }
+        }
+        if (tx > 0) left_p = pR[(size_t)in * ntiles + tile - 1];
+        if (ty > 0) above_p = pB[(size_t)in * ntiles + tile - tilesX];
+      }
+      const uint32_t below = (2u << lane) - 1u;  // lanes 0..lane
+      int ap = (int)((above_p >> lane) & 1u) & (int)eq_above;  // p above, where its key matches
+      bits = 0;
+      for (int r = 0; r < rows; r++) {
+        const int a = ((valid >> r) & 1u) && !(ap && (r == 0 || ((up >> r) & 1u)));
+        const int start_p = lane == 0 ? (a && !(((left_p & eq_left) >> r) & 1u)) : a;
+        const uint32_t chained = __ballot_sync(0xffffffffu, lane > 0 && a && ((left >> r) & 1u));
+        const uint32_t start_bits = __ballot_sync(0xffffffffu, start_p);
+        const int st = 31 - __clz(~chained & below);
+        const int p = (int)((start_bits >> st) & 1u) ^ ((lane - st) & 1);
+        bits |= (uint32_t)p << r;
+        ap = p;
+      }
+      const uint32_t rb = __shfl_sync(0xffffffffu, bits, 31);
+      const uint32_t bb = __ballot_sync(0xffffffffu, (bits >> (rows - 1)) & 1u);
+      changed = round == 0 || rb != last_r || bb != last_b;
+      last_r = rb;
+      last_b = bb;
+      if (lane == 0) {
+        pR[(size_t)out * ntiles + tile] = rb;
+        pB[(size_t)out * ntiles + tile] = bb;
+      }
     }
-    changed = __any_sync(0xffffffffu, changed);
     if (changed && lane == 0) atomicAdd((uint32_t *)&chg[round % 3], 1u);
     // counter (round + 1) % 3 was last read before the previous barrier
     if (blockIdx.x == 0 && threadIdx.x == 0) chg[(round + 1) % 3] = 0;
@@ -287,18 +257,8 @@ __global__ void __launch_bounds__(32 * DD_WARPS)
     }
     if (*(volatile uint32_t *)&cnt->error & ERR_SPIN_TIMEOUT) break;
   }
-#pragma unroll
-  for (int ti = 0; ti < DD_TILES_MAX; ti++) {
-    const int tile = warp + ti * nwarps;
-    if (tile >= ntiles) continue;
-    const int tx = tile % tilesX, ty = tile / tilesX;
-    const int x = tx * 32 + lane;
-    if (x >= W) continue;
-    for (int r = 0; r < 32; r++) {
-      const int y = ty * 32 + r;
-      if (y >= H) break;
-      processed[(size_t)y * W + x] = (uint8_t)((bits[ti] >> r) & 1u);
-    }
+  if (active && x < W) {
+    for (int r = 0; r < rows; r++) processed[(size_t)(ty * 32 + r) * W + x] = (uint8_t)((bits >> r) & 1u);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     cnt->dedupe_iters = round + 1;
@@ -312,30 +272,26 @@ cudaError_t launch_dedupe(const uint16_t *depth, const float *pxp, const float *
   int tilesX = (W + 31) / 32, tilesY = (H + 31) / 32;
   int ntiles = tilesX * tilesY;
   const int threads = 32 * DD_WARPS;
-  const size_t smem = sizeof(int4) * 32 * 32 * DD_WARPS;
-  static std::atomic<unsigned long long> attr_devices{0};
-  const unsigned long long bit = 1ull << (device & 63);
-  if (!(attr_devices.load() & bit)) {
-    cudaError_t e = cudaFuncSetAttribute(k_dedupe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // co-resident blocks of the cooperative launch, per device (queried once)
+  static int resident[64] = {};
+  const int dslot = device & 63;
+  if (!resident[dslot]) {
+    int per_sm = 0, sms = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dedupe, threads, 0);
     if (e != cudaSuccess) return e;
-    attr_devices.fetch_or(bit);
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    resident[dslot] = per_sm * sms;
   }
-  int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dedupe, threads, smem);
-  if (e != cudaSuccess) return e;
-  int sms = 0;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  int want = (ntiles + DD_WARPS - 1) / DD_WARPS;
-  int maxb = per_sm * sms;
-  int blocks = want < maxb ? want : maxb;
-  if (blocks < 1) blocks = 1;
-  if ((size_t)blocks * DD_WARPS * DD_TILES_MAX < (size_t)ntiles) return cudaErrorInvalidConfiguration;
+  // one warp per tile, all resident at once
+  const int blocks = (ntiles + DD_WARPS - 1) / DD_WARPS;
+  if (blocks > resident[dslot]) return cudaErrorInvalidConfiguration;
   CamF camv = cam;
   void *args[] = {(void *)&depth, (void *)&pxp, (void *)&pyp, (void *)&camv, (void *)&scaling, (void *)&maxcam,
                   (void *)&vox, (void *)&W, (void *)&H, (void *)&tilesX, (void *)&tilesY, (void *)&bnd,
                   (void *)&processed, (void *)&cnt, (void *)&barrier};
   note_launch();
-  return cudaLaunchCooperativeKernel((const void *)k_dedupe, dim3(blocks), dim3(threads), args, smem, s);
+  return cudaLaunchCooperativeKernel((const void *)k_dedupe, dim3(blocks), dim3(threads), args, 0, s);
 }
 
 // -------------------------------------------------------------- insert ----
@@ -549,52 +505,76 @@ __global__ void k_parents(int npend, uint32_t leaves_before, uint32_t leaves_max
   parent[idx] = parent_of(idx, leaves_max, tree, n, leaf[idx]);
 }
 
-// The whole frame's pending leaves in one block: order by first pixel (block
-// radix sort), assign indices and fill the leaf table, then the parents.
-constexpr int FIN_THREADS = 1024, FIN_ITEMS = 4;
-constexpr int FIN_MAX = FIN_THREADS * FIN_ITEMS;
+// The whole frame's pending leaves in one block.  A leaf's creation rank is
+// the number of pending leaves with a smaller first pixel; first pixels are
+// distinct (a pixel creates at most one leaf), so the rank is a prefix count
+// over a bitmap of the image's pixels held in shared memory.  Then indices,
+// the leaf table and the parents.
+constexpr int FIN_THREADS = 1024;
+constexpr size_t FIN_SMEM_MAX = 200 * 1024;
 
-__global__ void __launch_bounds__(FIN_THREADS) k_finalize_small(const PendingLeaf *pend, int npend, int end_bit,
-                                                                uint32_t leaves_before, uint32_t leaves_max,
-                                                                uint32_t *tree, ushort4 *leaf, uint32_t frame,
-                                                                uint32_t *stamp, uint32_t *queue, Counters *cnt,
-                                                                uint32_t n, uint32_t *parent) {
-  using Sort = cub::BlockRadixSort<uint32_t, FIN_THREADS, FIN_ITEMS, uint32_t>;
-  __shared__ typename Sort::TempStorage tmp;
-  uint32_t key[FIN_ITEMS], val[FIN_ITEMS];
-  // first pixels are distinct and below 2^end_bit; padding sorts after them
-  // (stable sort, padding placed last)
-  const uint32_t pad = end_bit >= 32 ? 0xFFFFFFFFu : ((1u << end_bit) - 1u);
-#pragma unroll
-  for (int i = 0; i < FIN_ITEMS; i++) {
-    const int j = threadIdx.x * FIN_ITEMS + i;
-    key[i] = j < npend ? pend[j].first_pixel : pad;
-    val[i] = (uint32_t)j;
-  }
-  Sort(tmp).Sort(key, val, 0, end_bit);
-#pragma unroll
-  for (int i = 0; i < FIN_ITEMS; i++) {
-    const int j = threadIdx.x * FIN_ITEMS + i;
-    if (j < npend)
-      finalize_one(pend[val[i]], leaves_before + (uint32_t)j, leaves_max, tree, leaf, frame, stamp, queue, cnt);
+__global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const PendingLeaf *pend, int npend, uint32_t npix,
+                                                                 uint32_t *rank, uint32_t leaves_before,
+                                                                 uint32_t leaves_max, uint32_t *tree, ushort4 *leaf,
+                                                                 uint32_t frame, uint32_t *stamp, uint32_t *queue,
+                                                                 Counters *cnt, uint32_t n, uint32_t *parent) {
+  extern __shared__ uint32_t fin_smem[];
+  const uint32_t nwords = (npix + 31) / 32;
+  uint32_t *bitmap = fin_smem;
+  uint32_t *chunk_base = fin_smem + nwords;  // [FIN_THREADS]
+  const uint32_t chunk = (nwords + FIN_THREADS - 1) / FIN_THREADS;
+  const int t = threadIdx.x;
+  for (uint32_t w = t; w < nwords; w += FIN_THREADS) bitmap[w] = 0;
+  __syncthreads();
+  for (int j = t; j < npend; j += FIN_THREADS) {
+    const uint32_t fp = pend[j].first_pixel;
+    atomicOr(&bitmap[fp >> 5], 1u << (fp & 31));
   }
   __syncthreads();
-#pragma unroll
-  for (int i = 0; i < FIN_ITEMS; i++) {
-    const int j = threadIdx.x * FIN_ITEMS + i;
-    const uint32_t idx = leaves_before + (uint32_t)j;
-    if (j < npend && idx < leaves_max) parent[idx] = parent_of(idx, leaves_max, tree, n, leaf[idx]);
+  // exclusive prefix of the per-thread chunk counts
+  uint32_t mine = 0;
+  const uint32_t w0 = (uint32_t)t * chunk, w1 = min(nwords, w0 + chunk);
+  for (uint32_t w = w0; w < w1; w++) mine += __popc(bitmap[w]);
+  using Scan = cub::BlockScan<uint32_t, FIN_THREADS>;
+  __shared__ typename Scan::TempStorage scan_tmp;
+  uint32_t before = 0;
+  Scan(scan_tmp).ExclusiveSum(mine, before);
+  chunk_base[t] = before;
+  __syncthreads();
+  for (int j = t; j < npend; j += FIN_THREADS) {
+    const PendingLeaf p = pend[j];
+    const uint32_t w = p.first_pixel >> 5, c = w / chunk;
+    uint32_t r = chunk_base[c];
+    for (uint32_t k = c * chunk; k < w; k++) r += __popc(bitmap[k]);
+    r += __popc(bitmap[w] & ((1u << (p.first_pixel & 31)) - 1u));
+    rank[j] = r;
+    finalize_one(p, leaves_before + r, leaves_max, tree, leaf, frame, stamp, queue, cnt);
+  }
+  __syncthreads();
+  for (int j = t; j < npend; j += FIN_THREADS) {
+    const uint32_t idx = leaves_before + rank[j];
+    if (idx < leaves_max) parent[idx] = parent_of(idx, leaves_max, tree, n, leaf[idx]);
   }
 }
 
-bool launch_finalize_small(const PendingLeaf *pend, int npend, int end_bit, uint32_t leaves_before,
-                           uint32_t leaves_max, uint32_t *tree, ushort4 *leaf, uint32_t frame, uint32_t *stamp,
-                           uint32_t *queue, Counters *cnt, uint32_t n, uint32_t *parent, cudaStream_t s) {
+bool launch_finalize_small(const PendingLeaf *pend, int npend, uint32_t npix, uint32_t *rank_scratch,
+                           uint32_t leaves_before, uint32_t leaves_max, uint32_t *tree, ushort4 *leaf,
+                           uint32_t frame, uint32_t *stamp, uint32_t *queue, Counters *cnt, uint32_t n,
+                           uint32_t *parent, int device, cudaStream_t s) {
   if (npend <= 0) return true;
-  if (npend > FIN_MAX) return false;
+  const size_t smem = sizeof(uint32_t) * (((size_t)npix + 31) / 32 + FIN_THREADS);
+  if (smem > FIN_SMEM_MAX) return false;
+  static std::atomic<unsigned long long> attr_devices{0};
+  const unsigned long long bit = 1ull << (device & 63);
+  if (!(attr_devices.load() & bit)) {
+    if (cudaFuncSetAttribute(k_finalize_bitmap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FIN_SMEM_MAX) !=
+        cudaSuccess)
+      return false;
+    attr_devices.fetch_or(bit);
+  }
   note_launch();
-  k_finalize_small<<<1, FIN_THREADS, 0, s>>>(pend, npend, end_bit, leaves_before, leaves_max, tree, leaf, frame,
-                                             stamp, queue, cnt, n, parent);
+  k_finalize_bitmap<<<1, FIN_THREADS, smem, s>>>(pend, npend, npix, rank_scratch, leaves_before, leaves_max, tree,
+                                                 leaf, frame, stamp, queue, cnt, n, parent);
   return true;
 }
 

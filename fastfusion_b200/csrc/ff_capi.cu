@@ -43,7 +43,8 @@ struct ff_handle {
   Counters *d_cnt = nullptr;
   Counters *h_cnt = nullptr;  // pinned
   uint32_t *d_barrier = nullptr;
-  uint32_t *d_rcp_tab = nullptr;  // FF_RCP_HOST: the host CPU's RCPPS per mantissa
+  uint32_t *d_rcp_tab = nullptr;  // FF_RCP_HOST: the host CPU's RCPPS per mantissa >> rcp_shift
+  int rcp_shift = 0;
 
   // per-image scratch
   int img_w = 0, img_h = 0, cap_pix = 0;
@@ -336,7 +337,7 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
     if (cudaMallocHost((void **)&h->h_cnt, sizeof(Counters)) != cudaSuccess) { fail(FF_ERR_CUDA, "pinned"); break; }
     if (cfg->rcp_mode == FF_RCP_HOST) {
       std::vector<uint32_t> tab;
-      if (!build_rcp_table(tab)) {
+      if (!build_rcp_table(tab, h->rcp_shift)) {
         g_create_error = "ff_create: FF_RCP_HOST needs an x86-64 host whose RCPPS follows the mantissa-table rules";
         st = FF_ERR_BAD_ARG;
         break;
@@ -480,8 +481,9 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
              *v_out = h->d_keys + 3 * h->cap_pix;
     int end_bit = 1;
     while ((1u << end_bit) < (uint32_t)(W * H)) end_bit++;
-    if (!launch_finalize_small(h->d_pend, (int)npend, end_bit, leaves_before, h->cfg.leaves_max, h->d_tree,
-                               h->d_leaf, frame, h->d_stamp, h->d_queue, h->d_cnt, h->n, h->d_parent, s)) {
+    if (!launch_finalize_small(h->d_pend, (int)npend, (uint32_t)(W * H), v_out, leaves_before, h->cfg.leaves_max,
+                               h->d_tree, h->d_leaf, frame, h->d_stamp, h->d_queue, h->d_cnt, h->n, h->d_parent,
+                               h->cfg.device, s)) {
       CK(sort_pending(h->d_pend, (int)npend, k_in, v_in, k_out, v_out, h->d_sort_tmp, h->sort_tmp_bytes, end_bit,
                       s));
       launch_finalize(h->d_pend, v_out, (int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->d_leaf, frame,
@@ -510,7 +512,7 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
   pi = h->prof.begin(ST_FUSE, s);
   launch_fuse(h->d_queue, (int)nq, h->d_leaf, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
               h->cfg.storage, h->cfg.leaves_max, d_depth, d_bgr, W, H, q, h->cfg.scale, h->cfg.threshold, scaling,
-              maxcam, h->d_rcp_tab, s);
+              maxcam, h->d_rcp_tab, h->rcp_shift, s);
   h->prof.end(pi, (double)nq * brick_bytes, s);
   CK(cudaGetLastError());
   if (h->leaves_used > h->cfg.leaves_max) h->meshing_ok = false;

@@ -33,26 +33,27 @@ __device__ __forceinline__ int cvt_x86_rz(float f) {
 }
 
 // Reciprocal as the host CPU's RCPPS computes it: the result mantissa is a
-// function of the input mantissa alone (tab, measured from the instruction
-// for x in [1,2)), the exponent is negated; zero and denormal inputs give
+// function of the input mantissa alone -- in practice of its top 23 - shift
+// bits (tab, measured from the instruction for x in [1,2)) --, the exponent
+// is negated; zero and denormal inputs give
 // infinity, infinity gives zero, results below the normal range are flushed
 // to zero, NaN stays NaN -- the behaviour checked when the table is built.
-__device__ __forceinline__ float rcp_host(float x, const uint32_t *__restrict__ tab) {
+__device__ __forceinline__ float rcp_host(float x, const uint32_t *__restrict__ tab, int shift) {
   const uint32_t u = __float_as_uint(x);
   const uint32_t sgn = u & 0x80000000u;
   const int e = (int)((u >> 23) & 255u);
   const uint32_t m = u & 0x7fffffu;
   if (e == 255) return m ? __uint_as_float(u | 0x400000u) : __uint_as_float(sgn);
   if (e == 0) return __uint_as_float(sgn | 0x7f800000u);
-  const uint32_t t = __ldg(tab + m);
+  const uint32_t t = __ldg(tab + (m >> shift));
   const int te = (int)((t >> 23) & 255u) - (e - 127);
   if (te <= 0) return __uint_as_float(sgn);
   return __uint_as_float(sgn | (t & 0x7fffffu) | ((uint32_t)te << 23));
 }
 
 template <bool RCP_HOST>
-__device__ __forceinline__ float rcp_upd(float x, const uint32_t *tab) {
-  return RCP_HOST ? rcp_host(x, tab) : __frcp_rz(x);
+__device__ __forceinline__ float rcp_upd(float x, const uint32_t *tab, int shift) {
+  return RCP_HOST ? rcp_host(x, tab, shift) : __frcp_rz(x);
 }
 
 template <bool FP16, bool RCP_HOST>
@@ -62,7 +63,7 @@ __global__ void __launch_bounds__(512) k_fuse(const uint32_t *__restrict__ queue
                                               uint16_t *__restrict__ col, uint32_t leaves_max,
                                               const uint16_t *__restrict__ depth, const uint8_t *__restrict__ bgr,
                                               int W, int H, CamF q, float scale, float thr, float scaling,
-                                              float maxcam, const uint32_t *__restrict__ rtab) {
+                                              float maxcam, const uint32_t *__restrict__ rtab, int rshift) {
   const uint32_t brick = queue[blockIdx.x];
   const int v = threadIdx.x;
   const int x = v & 7, y = (v >> 3) & 7, z = v >> 6;
@@ -97,7 +98,7 @@ __global__ void __launch_bounds__(512) k_fuse(const uint32_t *__restrict__ queue
   const float px = __fadd_rz(pzx, kx), py = __fadd_rz(pzy, ky), pz = __fadd_rz(pzz, kz);
 
   const float len = __fsqrt_rz(__fadd_rz(__fadd_rz(__fmul_rz(px, px), __fmul_rz(py, py)), __fmul_rz(pz, pz)));
-  const float rc = rcp_upd<RCP_HOST>(pz, rtab);
+  const float rc = rcp_upd<RCP_HOST>(pz, rtab, rshift);
   const int imx = cvt_x86_rz(__fadd_rz(q.cx, __fmul_rz(q.fx, __fmul_rz(px, rc))));
   const int imy = cvt_x86_rz(__fadd_rz(q.cy, __fmul_rz(q.fy, __fmul_rz(py, rc))));
   const int cyi = max(min(imy, H - 1), 0);
@@ -110,7 +111,7 @@ __global__ void __launch_bounds__(512) k_fuse(const uint32_t *__restrict__ queue
   const float thrW = __fmul_rz(__fmul_rz(WEIGHT_FACTOR, thr), ls);
   const float front = dInc < DIST_W_EPS ? 1.0f : 0.0f;
   const float back = (dInc >= DIST_W_EPS && dInc < thrW) ? 1.0f : 0.0f;
-  const float fall = __fmul_rz(__fsub_rz(thrW, dInc), rcp_upd<RCP_HOST>(__fsub_rz(thrW, DIST_W_EPS), rtab));
+  const float fall = __fmul_rz(__fsub_rz(thrW, dInc), rcp_upd<RCP_HOST>(__fsub_rz(thrW, DIST_W_EPS), rtab, rshift));
   const float wInc = mask ? __fadd_rz(front, __fmul_rz(fall, back)) : 0.0f;
 
   const size_t vi = (size_t)brick * 512 + v;
@@ -123,7 +124,7 @@ __global__ void __launch_bounds__(512) k_fuse(const uint32_t *__restrict__ queue
     dAcc = sdf[vi];
   }
   const float wNew = __fadd_rz(wAcc, wInc);
-  const float factor = rcp_upd<RCP_HOST>(__fadd_rz(wNew, wNew <= 0.0f ? 1.0f : 0.0f), rtab);
+  const float factor = rcp_upd<RCP_HOST>(__fadd_rz(wNew, wNew <= 0.0f ? 1.0f : 0.0f), rtab, rshift);
   float tr = dInc < thrD ? dInc : thrD;
   const float lo = -thrD;
   tr = tr > lo ? tr : lo;
@@ -152,11 +153,11 @@ __global__ void __launch_bounds__(512) k_fuse(const uint32_t *__restrict__ queue
 void launch_fuse(const uint32_t *queue, int nq, const ushort4 *leaf, float *sdf, float *wgt, __half *sdf16,
                  __half *wgt16, uint16_t *col, int storage, uint32_t leaves_max, const uint16_t *depth,
                  const uint8_t *bgr, int W, int H, const CamF &q, float scale, float thr, float scaling,
-                 float maxcam, const uint32_t *rcp_tab, cudaStream_t s) {
+                 float maxcam, const uint32_t *rcp_tab, int rcp_shift, cudaStream_t s) {
   if (nq <= 0) return;
 #define FF_FUSE(F16, RH)                                                                                         \
   k_fuse<F16, RH><<<nq, 512, 0, s>>>(queue, leaf, sdf, wgt, sdf16, wgt16, col, leaves_max, depth, bgr, W, H, q, \
-                                     scale, thr, scaling, maxcam, rcp_tab)
+                                     scale, thr, scaling, maxcam, rcp_tab, rcp_shift)
   const bool rh = rcp_tab != nullptr;
   note_launch();
   if (storage == 1) {
@@ -169,7 +170,7 @@ void launch_fuse(const uint32_t *queue, int nq, const ushort4 *leaf, float *sdf,
 
 // Measure the host CPU's RCPPS for every mantissa of [1,2) and check the
 // exponent/sign/special-value rules that rcp_host() relies on.
-bool build_rcp_table(std::vector<uint32_t> &tab) {
+bool build_rcp_table(std::vector<uint32_t> &tab, int &shift) {
 #if defined(__x86_64__) || defined(_M_X64)
   tab.resize(1u << 23);
   for (uint32_t m = 0; m < (1u << 23); m += 4) {
@@ -196,9 +197,28 @@ bool build_rcp_table(std::vector<uint32_t> &tab) {
   }
   if (bits(rcp1(0.0f)) != 0x7f800000u || bits(rcp1(1e-40f)) != 0x7f800000u) return false;
   if (bits(rcp1(__builtin_inff())) != 0u) return false;
+  // keep only the mantissa bits the result depends on (the instruction is a
+  // table lookup on the leading bits: 11 of them on recent Intel cores), so
+  // the device table stays small enough to live in L1
+  shift = 0;
+  for (int sh = 23; sh > 0; sh--) {
+    const uint32_t low = (1u << sh) - 1u;
+    bool same = true;
+    for (uint32_t m = 0; m < (1u << 23) && same; m++) same = tab[m] == tab[m & ~low];
+    if (same) {
+      shift = sh;
+      break;
+    }
+  }
+  if (shift) {
+    std::vector<uint32_t> c(1u << (23 - shift));
+    for (uint32_t i = 0; i < c.size(); i++) c[i] = tab[(size_t)i << shift];
+    tab.swap(c);
+  }
   return true;
 #else
   (void)tab;
+  shift = 0;
   return false;
 #endif
 }

@@ -47,11 +47,13 @@ void launch_finalize(const PendingLeaf *pend, const uint32_t *order, int npend, 
 void launch_parents(int npend, uint32_t leaves_before, uint32_t leaves_max, const uint32_t *tree, uint32_t n,
                     const ushort4 *leaf, uint32_t *parent, cudaStream_t s);
 
-// Sort, finalize and parents of up to 4096 pending leaves in one launch;
-// false (nothing launched) for more.
-bool launch_finalize_small(const PendingLeaf *pend, int npend, int end_bit, uint32_t leaves_before,
-                           uint32_t leaves_max, uint32_t *tree, ushort4 *leaf, uint32_t frame, uint32_t *stamp,
-                           uint32_t *queue, Counters *cnt, uint32_t n, uint32_t *parent, cudaStream_t s);
+// Ranks (creation order), leaf table and parents of the frame's pending
+// leaves in one launch, for images of up to about 1.6 million pixels; false
+// (nothing launched) for larger ones.  rank_scratch: npend uint32.
+bool launch_finalize_small(const PendingLeaf *pend, int npend, uint32_t npix, uint32_t *rank_scratch,
+                           uint32_t leaves_before, uint32_t leaves_max, uint32_t *tree, ushort4 *leaf,
+                           uint32_t frame, uint32_t *stamp, uint32_t *queue, Counters *cnt, uint32_t n,
+                           uint32_t *parent, int device, cudaStream_t s);
 
 // grow(): move child-branch pointers by `shift`, leaf positions by `add`.
 void launch_shift_branches(uint32_t *tree, uint32_t used, uint32_t shift, cudaStream_t s);
@@ -62,10 +64,12 @@ void launch_fill(uint32_t *p, size_t n, uint32_t v, cudaStream_t s);
 void launch_fuse(const uint32_t *queue, int nq, const ushort4 *leaf, float *sdf, float *wgt, __half *sdf16,
                  __half *wgt16, uint16_t *col, int storage, uint32_t leaves_max, const uint16_t *depth,
                  const uint8_t *bgr, int W, int H, const CamF &q, float scale, float thr, float scaling,
-                 float maxcam, const uint32_t *rcp_tab, cudaStream_t s);
+                 float maxcam, const uint32_t *rcp_tab, int rcp_shift, cudaStream_t s);
 
-// Table of the host CPU's RCPPS over the mantissas of [1,2); false when the
-// host is not x86-64 or the instruction does not follow the expected rules.
-bool build_rcp_table(std::vector<uint32_t> &tab);
+// Table of the host CPU's RCPPS over the mantissas of [1,2), indexed by the
+// mantissa >> shift (the low bits the instruction ignores are dropped); false
+// when the host is not x86-64 or the instruction does not follow the
+// expected rules.
+bool build_rcp_table(std::vector<uint32_t> &tab, int &shift);
 
 }  // namespace ffb

@@ -37,9 +37,11 @@ enum { FF_STORAGE_FP32 = 0, FF_STORAGE_FP16 = 1 };
  * approximate x86 RCPPS instruction (update_functions.cpp:1246,1373,1386),
  * whose result bits depend on the CPU model.
  *   FF_RCP_HOST:  reproduce the RCPPS of the CPU this library runs on (a
- *                 2^23-entry table measured from the instruction at
- *                 ff_create, 32 MB of device memory); results are bit-identical
- *                 to the reference binary on the same host.  x86-64 only.
+ *                 table measured from the instruction at ff_create over all
+ *                 2^23 mantissas, stored by the leading mantissa bits the
+ *                 result depends on: 8 KB on recent Intel cores, at most
+ *                 32 MB); results are bit-identical to the reference binary
+ *                 on the same host.  x86-64 only.
  *   FF_RCP_EXACT: exact round-toward-zero reciprocal; host-independent. */
 enum { FF_RCP_HOST = 0, FF_RCP_EXACT = 1 };
 

@@ -139,12 +139,14 @@ def test_bit_exact_with_reference_binary(lib_built):
     assert np.array_equal(cg, cr)
 
 
-def test_many_new_leaves_per_frame(lib_built, port_lib):
-    """2 mm voxels on 1280x960 frames create several thousand bricks per
-    frame, more than the single-block leaf finalisation takes, so the
-    multi-kernel sort path runs; results stay bit-exact."""
+@pytest.mark.parametrize("wh", [(1280, 960), (1600, 1200)])
+def test_many_new_leaves_per_frame(lib_built, port_lib, wh):
+    """2 mm voxels on large frames create several thousand bricks per frame.
+    1280x960 still takes the one-block leaf finalisation (pixel bitmap in
+    shared memory); 1600x1200 is past its limit and takes the sort-based
+    kernels.  Results stay bit-exact either way."""
     from fastfusion_b200.fusion import FusionMipMapCPU
-    K, frames = circle_frames(0, 3, 1280, 960)
+    K, frames = circle_frames(0, 2, *wh)
     g = FusionMipMapCPU(0, 0, 0, 0.002, 0.004, 0, True, leaves_max=400000, branches_max=8000000, rcp="exact")
     p = port_lib.PortFusion(0.002, 0.004, True, leaves_total=400000, branches_total=8000000, update_mode=1)
     news = []
