@@ -78,10 +78,8 @@ void launch_first_bbox(const uint16_t *depth, int W, int H, const CamF &p, float
 // (-1: invalid), under the default rounding: ((qxp+qyp)*d)*scaling + t per
 // axis, truncated (traversal_wrapper_functions.cpp:613-630), and
 // leafScaleFunc's floor(max(z,1)*8) (inline_functions.hpp:128-145).
-__device__ __forceinline__ int4 project_pixel(const uint16_t *depth, int W, int x, int y, const float *pxp,
-                                              const float *pyp, const CamF &p, float scaling, float maxcam) {
-  const float d = (float)depth[(size_t)y * W + x];
-  const float px = pxp[x], py = pyp[y];
+__device__ __forceinline__ int4 project_point(float d, float px, float py, const CamF &p, float scaling,
+                                              float maxcam) {
   int v[3];
 #pragma unroll
   for (int r = 0; r < 3; r++) {
@@ -166,16 +164,26 @@ __global__ void __launch_bounds__(32 * DD_WARPS)
   const int x = tx * 32 + lane;
   const int rows = active ? min(32, H - ty * 32) : 0;
   // project the tile (voxel keys for the insert that follows) and make the
-  // key comparisons
+  // key comparisons; the tile's depth and row factors are fetched first so
+  // the loads overlap
+  uint16_t dv[32];
+  const bool col_ok = active && x < W;
+#pragma unroll
+  for (int r = 0; r < 32; r++) dv[r] = (col_ok && r < rows) ? __ldg(&depth[(size_t)(ty * 32 + r) * W + x]) : 0;
+  const float px = col_ok ? __ldg(&pxp[x]) : 0.0f;
+  const float py_lane = (active && lane < rows) ? __ldg(&pyp[ty * 32 + lane]) : 0.0f;
   uint32_t valid = 0, up = 0, left = 0;
   int c0 = 0, c1 = 0, c2 = 0;     // key at (lane 0, row = lane): compared with the left tile
   int t0 = 0, t1 = 0, t2 = 0;     // key at (lane, row 0): compared with the tile above
   int u0 = 0, u1 = 0, u2 = 0;     // key of the previous row
-  for (int r = 0; r < rows; r++) {
+#pragma unroll
+  for (int r = 0; r < 32; r++) {
+    if (r >= rows) break;
     const int y = ty * 32 + r;
+    const float py = __shfl_sync(0xffffffffu, py_lane, r);
     int4 v = make_int4(0, 0, 0, -1);
     if (x < W) {
-      v = project_pixel(depth, W, x, y, pxp, pyp, cam, scaling, maxcam);
+      v = project_point((float)dv[r], px, py, cam, scaling, maxcam);
       vox[(size_t)y * W + x] = v;
     }
     const int k0 = v.x & -8, k1 = v.y & -8, k2 = v.z & -8;

@@ -714,7 +714,7 @@ __device__ __forceinline__ int warp_excl_scan(int v, int lane, int &total) {
 template <bool EMIT>
 __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, const Cell *__restrict__ cells,
                                                                   uint32_t first, uint32_t ncell,
-                                                                  const uint8_t *__restrict__ dirty, CellOut *out,
+                                                                  const uint32_t *__restrict__ list, const uint32_t *list_n, CellOut *out,
                                                                   const uint64_t *vbase, const uint64_t *fbase,
                                                                   float *xyz, uint8_t *rgb, uint32_t *faces) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -722,9 +722,10 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
   const int lane = threadIdx.x & 31;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t ci = gw; ci < ncell; ci += nw) {
-    const uint32_t cid = first + ci;
-    if (dirty && !dirty[cid]) continue;
+  // the dirty cells: a list of ids, or all cells of [first, first + ncell)
+  const uint32_t n = list ? *list_n : ncell;
+  for (uint32_t ci = gw; ci < n; ci += nw) {
+    const uint32_t cid = list ? list[ci] : first + ci;
     const Cell c = cells[cid];
     const CellGeom G = cell_geom(m, c);
     if (G.empty) {
@@ -850,12 +851,12 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
 // addBrickMiddle_indexed_incremental: one thread per corner cell
 template <bool EMIT>
 __global__ void k_mesh_corner(VoxSrc m, const Cell *__restrict__ cells, uint32_t first, uint32_t ncell,
-                              const uint8_t *__restrict__ dirty, CellOut *out, const uint64_t *vbase,
-                              const uint64_t *fbase, float *xyz, uint8_t *rgb, uint32_t *faces) {
+                              const uint32_t *__restrict__ list, const uint32_t *list_n, CellOut *out,
+                              const uint64_t *vbase, const uint64_t *fbase, float *xyz, uint8_t *rgb,
+                              uint32_t *faces) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= ncell) return;
-  const uint32_t cid = first + i;
-  if (dirty && !dirty[cid]) return;
+  if (i >= (list ? *list_n : ncell)) return;
+  const uint32_t cid = list ? list[i] : first + i;
   const Cell c = cells[cid];
   int stretch = m.leaf[c.L[0]].w;
   for (int k = 1; k < 7; k++) stretch = max(stretch, (int)m.leaf[c.L[k]].w);
@@ -950,7 +951,7 @@ __global__ void k_mesh_corner(VoxSrc m, const Cell *__restrict__ cells, uint32_t
 __global__ void k_mark_dirty(const Cell *cells, uint32_t n, const Cell *old_cells, uint32_t n_old,
                              const uint64_t *old_keys, const uint32_t *stamp, const uint32_t *parent,
                              uint32_t leaves_used, uint32_t since, uint8_t *dirty, int32_t *old_index,
-                             uint32_t *n_dirty) {
+                             uint32_t *n_dirty, uint32_t first_corner, uint32_t *list, uint32_t *n_list) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Cell c = cells[i];
@@ -981,7 +982,12 @@ __global__ void k_mark_dirty(const Cell *cells, uint32_t n, const Cell *old_cell
   }
   dirty[i] = d ? 1 : 0;
   old_index[i] = found;
-  if (d) atomicAdd(n_dirty, 1u);
+  if (d) {
+    atomicAdd(n_dirty, 1u);
+    // lattice cells listed from the front, corner cells from first_corner
+    if (i < first_corner) list[claim(n_list)] = i;
+    else list[first_corner + claim(n_list + 1)] = i;
+  }
 }
 
 __global__ void k_counts_to_arrays(const CellOut *out, uint32_t n, uint64_t *nv, uint64_t *nf) {
@@ -1107,6 +1113,8 @@ struct MeshImpl {
   size_t cap_dirty = 0;
   int32_t *old_index = nullptr;
   size_t cap_oi = 0;
+  uint32_t *dlist = nullptr;  // dirty cell ids: lattice cells, then (from first_corner) corner cells
+  size_t cap_dlist = 0;
   void *scan_tmp = nullptr;
   size_t scan_tmp_bytes = 0;
   // previous mesh (the current output moves here before the next update)
@@ -1269,23 +1277,25 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   MCK(grow_buf(I.nf, I.cap_nf, ncells + 1, s));
   MCK(grow_buf(I.vbase, I.cap_vb, ncells + 1, s));
   MCK(grow_buf(I.fbase, I.cap_fb, ncells + 1, s));
+  MCK(grow_buf(I.dlist, I.cap_dlist, ncells, s));
   const bool incremental = M.valid && I.n_old > 0;
+  // the sorted cell list holds interiors, walls, edges, then corners (type is
+  // the key's top field)
+  const uint32_t first_corner = ncells - std::min(I.n_corners, ncells);
   // dirty cells: all on the first update, otherwise those whose inputs changed
   MCK(cudaMemsetAsync(I.d_count + 10, 0, sizeof(uint32_t), s));
+  MCK(cudaMemsetAsync(I.d_count + 14, 0, 2 * sizeof(uint32_t), s));
   if (ncells) {
     if (incremental) {
       note_launch(2);
       k_mark_dirty<<<(ncells + 255) / 256, 256, 0, s>>>(I.cells, ncells, I.old_cells, I.n_old, I.old_keys, in.stamp,
                                                         in.parent, in.leaves_used, I.since, I.dirty, I.old_index,
-                                                        I.d_count + 10);
+                                                        I.d_count + 10, first_corner, I.dlist, I.d_count + 14);
       k_fill_counts_from_old<<<(ncells + 255) / 256, 256, 0, s>>>(I.dirty, I.old_index, ncells, I.old_out, I.out);
     } else {
       MCK(cudaMemsetAsync(I.dirty, 1, ncells, s));
     }
   }
-  // the sorted cell list holds interiors, walls, edges, then corners (type is
-  // the key's top field)
-  const uint32_t first_corner = ncells - std::min(I.n_corners, ncells);
   const size_t smem = sizeof(WarpScratch) * MESH_WARPS;
   static std::atomic<unsigned long long> attr_devices{0};
   int dev = 0;
@@ -1296,16 +1306,19 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
     MCK(cudaFuncSetAttribute(k_mesh_lattice<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr_devices.fetch_or(dbit);
   }
-  const uint8_t *dmask = I.dirty;
+  const uint32_t *lat_list = incremental ? I.dlist : nullptr;
+  const uint32_t *cor_list = incremental ? I.dlist + first_corner : nullptr;
   pi = P.begin(ST_MESH_COUNT, s);
   const int lat_blocks = std::max(1, std::min<int>(148 * 8, (int)((first_corner + MESH_WARPS - 1) / MESH_WARPS)));
   note_launch((first_corner ? 1 : 0) + (ncells > first_corner ? 1 : 0) + (ncells ? 1 : 0));
   if (first_corner)
-    k_mesh_lattice<false><<<lat_blocks, 32 * MESH_WARPS, smem, s>>>(vs, I.cells, 0, first_corner, dmask, I.out,
-                                                                    nullptr, nullptr, nullptr, nullptr, nullptr);
+    k_mesh_lattice<false><<<lat_blocks, 32 * MESH_WARPS, smem, s>>>(vs, I.cells, 0, first_corner, lat_list,
+                                                                    I.d_count + 14, I.out, nullptr, nullptr, nullptr,
+                                                                    nullptr, nullptr);
   if (ncells > first_corner)
     k_mesh_corner<false><<<(ncells - first_corner + 127) / 128, 128, 0, s>>>(
-        vs, I.cells, first_corner, ncells - first_corner, dmask, I.out, nullptr, nullptr, nullptr, nullptr, nullptr);
+        vs, I.cells, first_corner, ncells - first_corner, cor_list, I.d_count + 15, I.out, nullptr, nullptr, nullptr,
+        nullptr, nullptr);
   const int pi_count = pi;
   P.end(pi_count, 0.0, s);
   MCK(cudaGetLastError());
@@ -1349,12 +1362,13 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   pi = P.begin(ST_MESH_EMIT, s);
   note_launch((first_corner ? 1 : 0) + (ncells > first_corner ? 1 : 0) + (incremental && ncells ? 1 : 0));
   if (first_corner)
-    k_mesh_lattice<true><<<lat_blocks, 32 * MESH_WARPS, smem, s>>>(vs, I.cells, 0, first_corner, dmask, I.out,
-                                                                   I.vbase, I.fbase, M.d_xyz, M.d_rgb, M.d_faces);
+    k_mesh_lattice<true><<<lat_blocks, 32 * MESH_WARPS, smem, s>>>(vs, I.cells, 0, first_corner, lat_list,
+                                                                   I.d_count + 14, I.out, I.vbase, I.fbase, M.d_xyz,
+                                                                   M.d_rgb, M.d_faces);
   if (ncells > first_corner)
     k_mesh_corner<true><<<(ncells - first_corner + 127) / 128, 128, 0, s>>>(
-        vs, I.cells, first_corner, ncells - first_corner, dmask, I.out, I.vbase, I.fbase, M.d_xyz, M.d_rgb,
-        M.d_faces);
+        vs, I.cells, first_corner, ncells - first_corner, cor_list, I.d_count + 15, I.out, I.vbase, I.fbase, M.d_xyz,
+        M.d_rgb, M.d_faces);
   if (incremental && ncells)
     k_copy_clean<<<148 * 8, 256, 0, s>>>(I.dirty, I.old_index, ncells, I.out, I.vbase, I.fbase, I.old_vbase,
                                          I.old_fbase, I.old_xyz, I.old_rgb, I.old_faces, M.d_xyz, M.d_rgb,
@@ -1442,7 +1456,7 @@ void mesh_free(MeshState &M) {
                     I.vertq[1], I.d_count, I.raw, I.cells, I.old_cells, I.keys, I.keys_sorted, I.old_keys,
                     I.vals, I.vals_sorted, I.sort_tmp, I.out, I.old_out, I.nv, I.nf, I.vbase, I.fbase,
                     I.old_vbase, I.old_fbase, I.dirty, I.old_index, I.scan_tmp, I.old_xyz, I.old_rgb,
-                    I.old_faces};
+                    I.old_faces, I.dlist};
     for (void *p : ptrs)
       if (p) cudaFreeAsync(p, 0);
     if (I.h_count) cudaFreeHost(I.h_count);
