@@ -104,6 +104,7 @@ struct GenQueues {
 constexpr int LEVEL_COUNTS = 32;
 constexpr int MAX_GEN_LEVELS = 48;
 constexpr int COUNT_WORDS = LEVEL_COUNTS + 4 * (MAX_GEN_LEVELS + 1) + 28;
+constexpr int HOST_TOTALS = COUNT_WORDS - 8;  // host mirror only: 3 uint64 + 1 uint32 read back per update
 
 struct GenCtx {
   const uint32_t *tree;
@@ -592,9 +593,24 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
 #pragma unroll
       for (int k = 0; k < 8; k++)
         vi[k] = vox_index(m, leaf, (k & 1) ? lh[0] : ll[0], (k & 2) ? lh[1] : ll[1], (k & 4) ? lh[2] : ll[2]);
+      // a sample on the leaf's own lattice reads one voxel 8 times: load it once
+      const bool on_lattice = lh[0] == ll[0] && lh[1] == ll[1] && lh[2] == ll[2];
       float df[8];
+      float cf3[3][8];
+      if (on_lattice) {
+        const float d0 = vd(m, vi[0]);
+        const float c0 = (float)vc(m, vi[0], 0), c1 = (float)vc(m, vi[0], 1), c2 = (float)vc(m, vi[0], 2);
 #pragma unroll
-      for (int k = 0; k < 8; k++) df[k] = vd(m, vi[k]);
+        for (int k = 0; k < 8; k++) df[k] = d0, cf3[0][k] = c0, cf3[1][k] = c1, cf3[2][k] = c2;
+      } else {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          df[k] = vd(m, vi[k]);
+          cf3[0][k] = (float)vc(m, vi[k], 0);
+          cf3[1][k] = (float)vc(m, vi[k], 1);
+          cf3[2][k] = (float)vc(m, vi[k], 2);
+        }
+      }
       s.w = __fadd_rn(s.w, vw(m, vi[0]));
       s.d = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(f[0], df[0]), __fmul_rn(f[4], df[4])),
                                 __fadd_rn(__fmul_rn(f[1], df[1]), __fmul_rn(f[5], df[5]))),
@@ -602,9 +618,7 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
                                 __fadd_rn(__fmul_rn(f[3], df[3]), __fmul_rn(f[7], df[7]))));
 #pragma unroll
       for (int r = 0; r < 3; r++) {
-        float cf[8];
-#pragma unroll
-        for (int k = 0; k < 8; k++) cf[k] = (float)vc(m, vi[k], r);
+        const float *cf = cf3[r];
         const float v = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(f[0], cf[0]), __fmul_rn(f[4], cf[4])),
                                             __fadd_rn(__fmul_rn(f[1], cf[1]), __fmul_rn(f[5], cf[5]))),
                                   __fadd_rn(__fadd_rn(__fmul_rn(f[2], cf[2]), __fmul_rn(f[6], cf[6])),
@@ -624,11 +638,22 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
         l3[b] = (k & 2) ? lh[b] : ll[b];
         vi[k] = vox_index(m, leaf, l3[0], l3[1], l3[2]);
       }
-      float wf[4], df[4];
+      float wf[4], df[4], cf3[3][4];
+      if (lh[a] == ll[a] && lh[b] == ll[b]) {
+        // on the leaf's own lattice: one voxel
+        const float w0 = vw(m, vi[0]), d0 = vd(m, vi[0]);
+        const float c0 = (float)vc(m, vi[0], 0), c1 = (float)vc(m, vi[0], 1), c2 = (float)vc(m, vi[0], 2);
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
-        wf[k] = vw(m, vi[k]);
-        df[k] = vd(m, vi[k]);
+        for (int k = 0; k < 4; k++) wf[k] = w0, df[k] = d0, cf3[0][k] = c0, cf3[1][k] = c1, cf3[2][k] = c2;
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          wf[k] = vw(m, vi[k]);
+          df[k] = vd(m, vi[k]);
+          cf3[0][k] = (float)vc(m, vi[k], 0);
+          cf3[1][k] = (float)vc(m, vi[k], 1);
+          cf3[2][k] = (float)vc(m, vi[k], 2);
+        }
       }
       const float wsum = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(f[0], wf[0]), __fmul_rn(f[1], wf[1])),
                                              __fmul_rn(f[2], wf[2])),
@@ -638,9 +663,7 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
                       __fmul_rn(f[3], df[3]));
 #pragma unroll
       for (int r = 0; r < 3; r++) {
-        float cf[4];
-#pragma unroll
-        for (int k = 0; k < 4; k++) cf[k] = (float)vc(m, vi[k], r);
+        const float *cf = cf3[r];
         const float v = __fadd_rn(
             __fadd_rn(__fadd_rn(__fmul_rn(f[0], cf[0]), __fmul_rn(f[1], cf[1])), __fmul_rn(f[2], cf[2])),
             __fmul_rn(f[3], cf[3]));
@@ -741,7 +764,7 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
       fit &= lattice_sample(m, c, G, bx, by, bz, s);
       W.s[(bz * 8 + by) * 8 + bx] = s;
     }
-    for (int k = lane; k < 512 * 3; k += 32) W.edge_set[k] = 0;
+    for (int k = lane; k < 512 * 3 / 4; k += 32) reinterpret_cast<uint32_t *>(W.edge_set)[k] = 0;
     fit = __all_sync(0xffffffffu, fit);
     __syncwarp();
     if (!EMIT && lane == 0) atomicAdd(m.samples, (unsigned long long)nsamp);
@@ -1338,14 +1361,16 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   note_lib_call();
   MCK(cub::DeviceScan::ExclusiveSum(I.scan_tmp, I.scan_tmp_bytes, I.nv, I.vbase, (int)ncells + 1, s));
   MCK(cub::DeviceScan::ExclusiveSum(I.scan_tmp, I.scan_tmp_bytes, I.nf, I.fbase, (int)ncells + 1, s));
-  uint64_t tot[2];
-  unsigned long long nsamples = 0;
-  uint32_t ndirty = ncells;
-  MCK(cudaMemcpyAsync(&tot[0], I.vbase + ncells, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-  MCK(cudaMemcpyAsync(&tot[1], I.fbase + ncells, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-  if (incremental) MCK(cudaMemcpyAsync(&ndirty, I.d_count + 10, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  MCK(cudaMemcpyAsync(&nsamples, I.d_count + 12, sizeof(nsamples), cudaMemcpyDeviceToHost, s));
+  // totals, dirty count and samples through the pinned counter mirror
+  uint64_t *h_tot = reinterpret_cast<uint64_t *>(I.h_count + HOST_TOTALS);
+  MCK(cudaMemcpyAsync(h_tot + 0, I.vbase + ncells, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  MCK(cudaMemcpyAsync(h_tot + 1, I.fbase + ncells, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  MCK(cudaMemcpyAsync(h_tot + 2, I.d_count + 12, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  MCK(cudaMemcpyAsync(I.h_count + HOST_TOTALS + 6, I.d_count + 10, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   MCK(cudaStreamSynchronize(s));
+  const uint64_t tot[2] = {h_tot[0], h_tot[1]};
+  const unsigned long long nsamples = h_tot[2];
+  const uint32_t ndirty = incremental ? I.h_count[HOST_TOTALS + 6] : ncells;
   // count pass: SDF, weight and colour of every sample of the dirty cells
   const double sample_bytes = vs.fp16 ? 10.0 : 14.0;
   P.set_bytes(pi_count, (double)nsamples * sample_bytes);

@@ -115,6 +115,8 @@ class CameraInfo:
         self.K = np.ascontiguousarray(K, dtype=np.float64).reshape(4)
         self.R = np.ascontiguousarray(R, dtype=np.float64).reshape(3, 3)
         self.t = np.ascontiguousarray(t, dtype=np.float64).reshape(3)
+        # addresses for the C calls (the arrays live as long as this object)
+        self._ptrs = (self.K.ctypes.data, self.R.ctypes.data, self.t.ctypes.data)
 
     def getIntrinsic(self):
         fx, fy, cx, cy = self.K
@@ -212,6 +214,10 @@ class FusionMipMapCPU:
             raise FFError(st, self._L.ff_last_error(None).decode())
         self._h = h
         self.storage = storage
+        self._q = ctypes.c_int32()
+        self._qref = ctypes.byref(self._q)
+        self._u = ctypes.c_int()
+        self._uref = ctypes.byref(self._u)
 
     # -- lifetime --------------------------------------------------------
     def close(self):
@@ -236,27 +242,29 @@ class FusionMipMapCPU:
         rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
         if depth.ndim != 2 or rgb.shape != depth.shape + (3,):
             raise FFError(1, "addMap: depth must be HxW uint16 and rgb HxWx3 uint8")
-        q = ctypes.c_int32()
         h, w = depth.shape
-        self._check(self._L.ff_add_map_u16(self._h, _p(depth), w, h, 0, _p(rgb), 0, _p(caminfo.K),
-                                           _p(caminfo.R), _p(caminfo.t), ctypes.c_float(scaling),
-                                           ctypes.c_float(maxcamdistance), ctypes.byref(q)))
-        return q.value
+        pK, pR, pt = caminfo._ptrs
+        st = self._L.ff_add_map_u16(self._h, depth.ctypes.data, w, h, 0, rgb.ctypes.data, 0, pK, pR, pt, scaling,
+                                    maxcamdistance, self._qref)
+        if st != FF_OK:
+            self._check(st)
+        return self._q.value
 
     def addMapDevice(self, d_depth: int, d_bgr: int, width: int, height: int, caminfo: CameraInfo,
                      scaling: float = 1.0 / 5000.0, maxcamdistance: float = 10.0) -> int:
         """addMap with depth/bgr already in device memory (raw device pointers)."""
-        q = ctypes.c_int32()
-        self._check(self._L.ff_add_map_u16_device(self._h, ctypes.c_void_p(d_depth), ctypes.c_void_p(d_bgr), width,
-                                                  height, _p(caminfo.K), _p(caminfo.R), _p(caminfo.t),
-                                                  ctypes.c_float(scaling), ctypes.c_float(maxcamdistance),
-                                                  ctypes.byref(q)))
-        return q.value
+        pK, pR, pt = caminfo._ptrs
+        st = self._L.ff_add_map_u16_device(self._h, d_depth, d_bgr, width, height, pK, pR, pt, scaling,
+                                           maxcamdistance, self._qref)
+        if st != FF_OK:
+            self._check(st)
+        return self._q.value
 
     def updateMeshes(self) -> bool:
-        u = ctypes.c_int()
-        self._check(self._L.ff_update_meshes(self._h, ctypes.byref(u)))
-        return bool(u.value)
+        st = self._L.ff_update_meshes(self._h, self._uref)
+        if st != FF_OK:
+            self._check(st)
+        return bool(self._u.value)
 
     def getMeshInterleavedMarchingCubes(self, out: MeshBuffer | None = None) -> MeshInterleaved:
         """The mesh of the last updateMeshes as a host copy (the reference
