@@ -637,4 +637,19 @@ void launch_fill(uint32_t *p, size_t n, uint32_t v, cudaStream_t s) {
   k_fill<<<(unsigned)blocks, 256, 0, s>>>(p, n, v);
 }
 
+// Load this file's kernels now (modules load lazily on first launch, which
+// would otherwise land inside the first frame that needs a kernel).
+cudaError_t prewarm_alloc_kernels() {
+  const void *fns[] = {(const void *)k_first_bbox, (const void *)k_dedupe, (const void *)k_insert,
+                       (const void *)k_pending_keys, (const void *)k_finalize, (const void *)k_parents,
+                       (const void *)k_finalize_bitmap, (const void *)k_shift_branches,
+                       (const void *)k_shift_leaves, (const void *)k_fill};
+  for (const void *f : fns) {
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, f);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 }  // namespace ffb

@@ -348,6 +348,11 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
         break;
       }
     }
+    if (prewarm_alloc_kernels() != cudaSuccess || prewarm_fuse_kernels() != cudaSuccess ||
+        prewarm_mesh_kernels() != cudaSuccess) {
+      fail(FF_ERR_CUDA, "kernel load");
+      break;
+    }
     launch_fill(h->d_tree, h->cfg.branches_max, BRANCHINIT, h->stream);
     cudaMemsetAsync(h->d_stamp, 0, sizeof(uint32_t) * L, h->stream);
     cudaMemsetAsync(h->d_parent, 0xFF, sizeof(uint32_t) * L, h->stream);

@@ -223,4 +223,15 @@ bool build_rcp_table(std::vector<uint32_t> &tab, int &shift) {
 #endif
 }
 
+cudaError_t prewarm_fuse_kernels() {
+  const void *fns[] = {(const void *)k_fuse<false, false>, (const void *)k_fuse<false, true>,
+                       (const void *)k_fuse<true, false>, (const void *)k_fuse<true, true>};
+  for (const void *f : fns) {
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, f);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 }  // namespace ffb

@@ -55,6 +55,11 @@ bool launch_finalize_small(const PendingLeaf *pend, int npend, uint32_t npix, ui
                            uint32_t frame, uint32_t *stamp, uint32_t *queue, Counters *cnt, uint32_t n,
                            uint32_t *parent, int device, cudaStream_t s);
 
+// Load the kernels of each file ahead of their first launch.
+cudaError_t prewarm_alloc_kernels();
+cudaError_t prewarm_fuse_kernels();
+cudaError_t prewarm_mesh_kernels();
+
 // grow(): move child-branch pointers by `shift`, leaf positions by `add`.
 void launch_shift_branches(uint32_t *tree, uint32_t used, uint32_t shift, cudaStream_t s);
 void launch_shift_leaves(ushort4 *leaf, uint32_t n_leaves, ushort3 add, cudaStream_t s);

@@ -52,8 +52,28 @@ __constant__ uint8_t c_edge_slot[12][4] = {{0, 0, 0, 0}, {1, 0, 0, 1}, {0, 1, 0,
 __constant__ uint8_t c_edge_a[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
 __constant__ uint8_t c_edge_b[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
 
-__device__ __forceinline__ int mc_ntri(int c) { return (int)(c_mc_tri[c] >> 60); }
-__device__ __forceinline__ int mc_edge(int c, int k) { return (int)((c_mc_tri[c] >> (4 * k)) & 15ull); }
+// The tables as the meshing kernels read them: from shared memory, since
+// the lanes of a warp index them by different cube cases.
+struct McTab {
+  unsigned long long tri[256];
+  uint32_t slot[12];  // c_edge_slot packed: dx | dy << 8 | dz << 16 | axis << 24
+};
+
+// Copy the tables into the block's shared memory (all threads of the block).
+__device__ __forceinline__ void load_mc(McTab &T) {
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) T.tri[i] = c_mc_tri[i];
+  for (int i = threadIdx.x; i < 12; i += blockDim.x)
+    T.slot[i] = (uint32_t)c_edge_slot[i][0] | ((uint32_t)c_edge_slot[i][1] << 8) |
+                ((uint32_t)c_edge_slot[i][2] << 16) | ((uint32_t)c_edge_slot[i][3] << 24);
+  __syncthreads();
+}
+__device__ __forceinline__ int mc_ntri(const McTab &T, int c) { return (int)(T.tri[c] >> 60); }
+__device__ __forceinline__ int mc_edge(const McTab &T, int c, int k) { return (int)((T.tri[c] >> (4 * k)) & 15ull); }
+// flat lattice-edge slot (3 * voxel index + axis) of a cube edge, relative to the cube's voxel index
+__device__ __forceinline__ int mc_slot(const McTab &T, int e) {
+  const uint32_t v = T.slot[e];
+  return 3 * ((int)(v & 255u) + 8 * (int)((v >> 8) & 255u) + 64 * (int)((v >> 16) & 255u)) + (int)(v >> 24);
+}
 
 // ---------------------------------------------------------------------------
 // Cell generation
@@ -741,6 +761,8 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
                                                                   const uint64_t *vbase, const uint64_t *fbase,
                                                                   float *xyz, uint8_t *rgb, uint32_t *faces) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ McTab T;
+  load_mc(T);
   WarpScratch &W = reinterpret_cast<WarpScratch *>(smem_raw)[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -788,11 +810,8 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
       }
       if (zero) ci8 = 0;
       W.cube_case[idx] = (uint8_t)ci8;
-      const int nt = mc_ntri(ci8);
-      for (int q = 0; q < 3 * nt; q++) {
-        const uint8_t *es = c_edge_slot[mc_edge(ci8, q)];
-        W.edge_set[3 * (idx + es[0] + 8 * es[1] + 64 * es[2]) + es[3]] = 1;
-      }
+      const int nt = mc_ntri(T, ci8);
+      for (int q = 0; q < 3 * nt; q++) W.edge_set[3 * idx + mc_slot(T, mc_edge(T, ci8, q))] = 1;
     }
     __syncwarp();
     // vertices, in the reference's loop order of this cell type
@@ -850,7 +869,7 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
         int b0, b1, b2;
         idx = lattice_idx(G, k, nc3o, b0, b1, b2);
         ci8 = W.cube_case[idx];
-        nt = mc_ntri(ci8);
+        nt = mc_ntri(T, ci8);
       }
       int tot;
       int ex = warp_excl_scan(nt, lane, tot);
@@ -858,10 +877,8 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
         for (int t = 0; t < nt; t++) {
           const uint64_t gf = fb + frun + (uint32_t)ex + t;
 #pragma unroll
-          for (int q = 0; q < 3; q++) {
-            const uint8_t *es = c_edge_slot[mc_edge(ci8, 3 * t + q)];
-            faces[3 * gf + q] = (uint32_t)(vb + W.vidx[3 * (idx + es[0] + 8 * es[1] + 64 * es[2]) + es[3]]);
-          }
+          for (int q = 0; q < 3; q++)
+            faces[3 * gf + q] = (uint32_t)(vb + W.vidx[3 * idx + mc_slot(T, mc_edge(T, ci8, 3 * t + q))]);
         }
       }
       frun += (uint32_t)tot;
@@ -877,6 +894,8 @@ __global__ void k_mesh_corner(VoxSrc m, const Cell *__restrict__ cells, uint32_t
                               const uint32_t *__restrict__ list, const uint32_t *list_n, CellOut *out,
                               const uint64_t *vbase, const uint64_t *fbase, float *xyz, uint8_t *rgb,
                               uint32_t *faces) {
+  __shared__ McTab T;
+  load_mc(T);
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (list ? *list_n : ncell)) return;
   const uint32_t cid = list ? list[i] : first + i;
@@ -939,11 +958,11 @@ __global__ void k_mesh_corner(VoxSrc m, const Cell *__restrict__ cells, uint32_t
       cinterp(col[mcv[a]], col[mcv[b]], val[a], val[b], cl[e]);
     }
   }
-  const int nt = mc_ntri(ci8);
+  const int nt = mc_ntri(T, ci8);
   uint32_t kept = 0;
   const uint64_t vb = EMIT ? vbase[cid] : 0, fb = EMIT ? fbase[cid] : 0;
   for (int t = 0; t < nt; t++) {
-    const int e0 = mc_edge(ci8, 3 * t), e1 = mc_edge(ci8, 3 * t + 1), e2 = mc_edge(ci8, 3 * t + 2);
+    const int e0 = mc_edge(T, ci8, 3 * t), e1 = mc_edge(T, ci8, 3 * t + 1), e2 = mc_edge(T, ci8, 3 * t + 2);
     const float *v0 = vl[e0], *v1 = vl[e1], *v2 = vl[e2];
     const bool deg = (v0[0] == v1[0] && v0[1] == v1[1] && v0[2] == v1[2]) ||
                      (v2[0] == v1[0] && v2[1] == v1[1] && v2[2] == v1[2]) ||
@@ -1503,5 +1522,20 @@ void mesh_invalidate(MeshState &M) {
 }
 
 void mesh_note_frame(MeshState &) {}
+
+cudaError_t prewarm_mesh_kernels() {
+  const void *fns[] = {(const void *)k_gen_level,          (const void *)k_cell_keys,
+                       (const void *)k_gather_cells,       (const void *)k_mesh_lattice<false>,
+                       (const void *)k_mesh_lattice<true>, (const void *)k_mesh_corner<false>,
+                       (const void *)k_mesh_corner<true>,  (const void *)k_mark_dirty,
+                       (const void *)k_counts_to_arrays,   (const void *)k_copy_clean,
+                       (const void *)k_fill_counts_from_old, (const void *)k_export_cells};
+  for (const void *f : fns) {
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, f);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
 
 }  // namespace ffb
