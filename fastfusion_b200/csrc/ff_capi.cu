@@ -811,6 +811,15 @@ ff_status ff_get_mesh_cells(ff_handle *h, int32_t *cells, int64_t *ranges) {
   return FF_OK;
 }
 
+ff_status ff_get_mesh_cells_noalloc(ff_handle *h, int32_t *cells, int64_t *ranges) {
+  if (!h || (h->mesh.n_cells && (!cells || !ranges))) return FF_ERR_BAD_ARG;
+  CK(cudaSetDevice(h->cfg.device));
+  std::string err;
+  int rc = mesh_copy_cells_noalloc(h->mesh, cells, ranges, h->stream, err);
+  if (rc != 0) return set_err(h, (ff_status)rc, err);
+  return FF_OK;
+}
+
 ff_status ff_get_mesh_device(ff_handle *h, const float **xyz, const uint8_t **rgb, const uint32_t **faces) {
   if (!h || !xyz || !rgb || !faces) return FF_ERR_BAD_ARG;
   *xyz = h->mesh.d_xyz;

@@ -27,6 +27,8 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "ff_mesh.h"
@@ -1489,6 +1491,67 @@ int mesh_copy_cells(MeshState &M, int32_t *rows, int64_t *ranges, cudaStream_t s
   MCK(cudaMemcpyAsync(ranges, d_ranges, sizeof(int64_t) * 4 * n, cudaMemcpyDeviceToHost, s));
   MCK(cudaFreeAsync(d_rows, s));
   MCK(cudaFreeAsync(d_ranges, s));
+  MCK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Cell export without allocation
+//
+// For callers that must not allocate device memory during the call (a fixed
+// memory budget, an allocator they do not control, code that runs where
+// cudaMalloc is not allowed): the export kernel's staging area is this
+// file-scope device array instead of stream-ordered allocations.  It is
+// shared by every call in the process, on every handle.
+// ---------------------------------------------------------------------------
+constexpr uint32_t NOALLOC_MAX_CELLS = 65536;
+constexpr size_t NOALLOC_RANGES_BYTES = sizeof(int64_t) * 4 * NOALLOC_MAX_CELLS;
+constexpr size_t NOALLOC_ROWS_BYTES = sizeof(int32_t) * 14 * NOALLOC_MAX_CELLS;
+static __device__ __align__(256) unsigned char g_export_scratch[NOALLOC_RANGES_BYTES + NOALLOC_ROWS_BYTES];
+
+// The array's device address, looked up once per device with that device
+// current (in host code the symbol names a host-side stand-in, never the
+// device memory itself).
+static std::mutex g_export_scratch_mu;
+static unsigned char *g_export_scratch_dev[64] = {};
+
+static cudaError_t export_scratch_address(unsigned char **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_export_scratch_mu);
+  if (!g_export_scratch_dev[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_export_scratch);
+    if (e != cudaSuccess) return e;
+    g_export_scratch_dev[dev] = static_cast<unsigned char *>(p);
+  }
+  *out = g_export_scratch_dev[dev];
+  return cudaSuccess;
+}
+
+int mesh_copy_cells_noalloc(MeshState &M, int32_t *rows, int64_t *ranges, cudaStream_t s, std::string &err) {
+  if (!M.impl || !M.valid || !M.n_cells) return 0;
+  const uint32_t n = (uint32_t)M.n_cells;
+  if (n > NOALLOC_MAX_CELLS) {
+    err = "ff_get_mesh_cells_noalloc: the mesh has " + std::to_string(n) + " cells, more than the " +
+          std::to_string(NOALLOC_MAX_CELLS) + " its fixed device buffer holds (use ff_get_mesh_cells)";
+    return 1;  // FF_ERR_BAD_ARG
+  }
+  unsigned char *base = nullptr;
+  MCK(export_scratch_address(&base));
+  // every word copied back is written by this call's kernel first, so the
+  // previous call's contents need no clearing
+  int64_t *d_ranges = reinterpret_cast<int64_t *>(base);
+  int32_t *d_rows = reinterpret_cast<int32_t *>(base + NOALLOC_RANGES_BYTES);
+  MeshImpl &I = impl(M);
+  note_launch();
+  k_export_cells<<<(n + 255) / 256, 256, 0, s>>>(I.old_cells, I.old_out, I.old_vbase, I.old_fbase, n, d_rows,
+                                                 d_ranges);
+  MCK(cudaGetLastError());
+  MCK(cudaMemcpyAsync(rows, d_rows, sizeof(int32_t) * 14 * n, cudaMemcpyDeviceToHost, s));
+  MCK(cudaMemcpyAsync(ranges, d_ranges, sizeof(int64_t) * 4 * n, cudaMemcpyDeviceToHost, s));
   MCK(cudaStreamSynchronize(s));
   return 0;
 }

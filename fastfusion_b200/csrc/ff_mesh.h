@@ -51,6 +51,9 @@ int mesh_copy_out(MeshState &m, float *xyz, uint8_t *rgb, uint32_t *faces, cudaS
 // cells of the last update: 14 int32 each (type, quirk, ox, oy, oz, size, L0..L7) and per cell
 // (first vertex, vertex count, first face, face count)
 int mesh_copy_cells(MeshState &m, int32_t *rows, int64_t *ranges, cudaStream_t s, std::string &err);
+// The same through a fixed file-scope device buffer (no allocation), for at
+// most 65536 cells.
+int mesh_copy_cells_noalloc(MeshState &m, int32_t *rows, int64_t *ranges, cudaStream_t s, std::string &err);
 void mesh_free(MeshState &m);
 void mesh_invalidate(MeshState &m);
 void mesh_note_frame(MeshState &m);

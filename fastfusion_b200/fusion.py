@@ -24,6 +24,8 @@ LIB_PATH = os.path.join(_PKG, "libfastfusion_b200.so")
 FF_OK = 0
 _STATUS = {0: "FF_OK", 1: "FF_ERR_BAD_ARG", 2: "FF_ERR_CUDA", 3: "FF_ERR_OOM_POOL", 4: "FF_ERR_OOM_MESH",
            5: "FF_ERR_TIMEOUT", 6: "FF_ERR_STATE", 7: "FF_ERR_NO_DEVICE"}
+NOALLOC_MAX_CELLS = 65536  # FF_NOALLOC_MAX_CELLS
+
 STORAGE = {"fp32": 0, "fp16": 1}
 RCP = {"host": 0, "exact": 1}
 BRANCHINIT = 0xFFFFFFFE
@@ -66,6 +68,7 @@ SIGNATURES = {
     "ff_get_mesh": (_i32, [_vp, _vp, _vp, _vp]),
     "ff_get_mesh_device": (_i32, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "ff_get_mesh_cells": (_i32, [_vp, _vp, _vp]),
+    "ff_get_mesh_cells_noalloc": (_i32, [_vp, _vp, _vp]),
     "ff_alloc_host": (_i32, [_sz, ctypes.POINTER(_vp)]),
     "ff_free_host": (_i32, [_vp]),
     "ff_get_stats": (_i32, [_vp, ctypes.POINTER(ff_stats)]),
@@ -289,6 +292,16 @@ class FusionMipMapCPU:
         cells = np.zeros((n, 14), np.int32)
         ranges = np.zeros((n, 4), np.int64)
         self._check(self._L.ff_get_mesh_cells(self._h, _p(cells), _p(ranges)))
+        return cells, ranges
+
+    def mesh_cells_noalloc(self):
+        """mesh_cells() without device allocation: staged in the library's
+        fixed device buffer (at most NOALLOC_MAX_CELLS cells; calls on one
+        device must not overlap on the GPU)."""
+        n = self.stats()["mesh_cells"]
+        cells = np.zeros((n, 14), np.int32)
+        ranges = np.zeros((n, 4), np.int64)
+        self._check(self._L.ff_get_mesh_cells_noalloc(self._h, _p(cells), _p(ranges)))
         return cells, ranges
 
     def setThreadMeshing(self, threadMeshing: bool):

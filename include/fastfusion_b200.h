@@ -136,6 +136,20 @@ ff_status ff_free_host(void *p);
  * vertex, vertex count, first face, face count of the cell's part of the mesh. */
 ff_status ff_get_mesh_cells(ff_handle *h, int32_t *cells, int64_t *ranges);
 
+/* ff_get_mesh_cells for callers that cannot allocate device memory during the
+ * call: a fixed memory budget, an allocator they do not own, or code where
+ * cudaMalloc is not allowed.  It has no counterpart in the reference.  The
+ * cells are staged in a fixed device buffer that is part of the library
+ * (FF_NOALLOC_MAX_CELLS cells, 5.8 MB, held on every GPU that loads the
+ * library until the process exits); the call allocates nothing.  A mesh with
+ * more cells is rejected with FF_ERR_BAD_ARG and a message.  The first call
+ * on a device looks up the buffer's device address; make that first call
+ * before any stream capture.  Every call on one device uses the same buffer,
+ * so calls whose GPU work overlaps (maps on different streams) race: order
+ * them on the host or on one stream. */
+#define FF_NOALLOC_MAX_CELLS 65536
+ff_status ff_get_mesh_cells_noalloc(ff_handle *h, int32_t *cells, int64_t *ranges);
+
 /* Device pointers to the same mesh, valid until the next ff_update_meshes. */
 ff_status ff_get_mesh_device(ff_handle *h, const float **xyz, const uint8_t **rgb, const uint32_t **faces);
 
