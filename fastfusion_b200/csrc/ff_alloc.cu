@@ -140,12 +140,14 @@ __device__ void grid_barrier(uint32_t *bar, uint32_t nblocks, Counters *cnt) {
 }
 
 constexpr int DD_WARPS = 4;  // tiles (warps) per block
+constexpr int DD_ROWS = 16;  // tile height: more, shorter tiles shorten each warp's chain of rows
 
 __device__ __forceinline__ bool same3(int a0, int a1, int a2, int b0, int b1, int b2) {
   return a0 == b0 && a1 == b1 && a2 == b2;
 }
 
-// bnd layout: right-column keys [ntiles][32] int4, bottom-row keys [ntiles][32]
+// Tiles are 32 pixels wide and DD_ROWS high.  bnd layout: right-column keys
+// [ntiles][32] int4 (DD_ROWS used), bottom-row keys [ntiles][32]
 // int4 (written once, before the first barrier), then processed bits of the
 // right column and of the bottom row, [2 rounds][ntiles] uint32 each.
 // bar: [0] arrivals, [1] generation, [4..6] per-round change counters (rotating)
@@ -162,24 +164,24 @@ __global__ void __launch_bounds__(32 * DD_WARPS)
   uint32_t *pB = pR + 2 * (size_t)ntiles;
   const int tx = active ? tile % tilesX : 0, ty = active ? tile / tilesX : 0;
   const int x = tx * 32 + lane;
-  const int rows = active ? min(32, H - ty * 32) : 0;
+  const int rows = active ? min(DD_ROWS, H - ty * DD_ROWS) : 0;
   // project the tile (voxel keys for the insert that follows) and make the
   // key comparisons; the tile's depth and row factors are fetched first so
   // the loads overlap
-  uint16_t dv[32];
+  uint16_t dv[DD_ROWS];
   const bool col_ok = active && x < W;
 #pragma unroll
-  for (int r = 0; r < 32; r++) dv[r] = (col_ok && r < rows) ? __ldg(&depth[(size_t)(ty * 32 + r) * W + x]) : 0;
+  for (int r = 0; r < DD_ROWS; r++) dv[r] = (col_ok && r < rows) ? __ldg(&depth[(size_t)(ty * DD_ROWS + r) * W + x]) : 0;
   const float px = col_ok ? __ldg(&pxp[x]) : 0.0f;
-  const float py_lane = (active && lane < rows) ? __ldg(&pyp[ty * 32 + lane]) : 0.0f;
+  const float py_lane = (active && lane < rows) ? __ldg(&pyp[ty * DD_ROWS + lane]) : 0.0f;
   uint32_t valid = 0, up = 0, left = 0;
   int c0 = 0, c1 = 0, c2 = 0;     // key at (lane 0, row = lane): compared with the left tile
   int t0 = 0, t1 = 0, t2 = 0;     // key at (lane, row 0): compared with the tile above
   int u0 = 0, u1 = 0, u2 = 0;     // key of the previous row
 #pragma unroll
-  for (int r = 0; r < 32; r++) {
+  for (int r = 0; r < DD_ROWS; r++) {
     if (r >= rows) break;
-    const int y = ty * 32 + r;
+    const int y = ty * DD_ROWS + r;
     const float py = __shfl_sync(0xffffffffu, py_lane, r);
     int4 v = make_int4(0, 0, 0, -1);
     if (x < W) {
@@ -266,7 +268,7 @@ __global__ void __launch_bounds__(32 * DD_WARPS)
     if (*(volatile uint32_t *)&cnt->error & ERR_SPIN_TIMEOUT) break;
   }
   if (active && x < W) {
-    for (int r = 0; r < rows; r++) processed[(size_t)(ty * 32 + r) * W + x] = (uint8_t)((bits >> r) & 1u);
+    for (int r = 0; r < rows; r++) processed[(size_t)(ty * DD_ROWS + r) * W + x] = (uint8_t)((bits >> r) & 1u);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     cnt->dedupe_iters = round + 1;
@@ -274,10 +276,15 @@ __global__ void __launch_bounds__(32 * DD_WARPS)
   }
 }
 
+size_t dedupe_boundary_elems(int W, int H) {
+  const size_t ntiles = (size_t)((W + 31) / 32) * ((H + DD_ROWS - 1) / DD_ROWS);
+  return ntiles * 32 * 2 + ntiles;  // keys of the right column and bottom row, then 4 bit words per tile
+}
+
 cudaError_t launch_dedupe(const uint16_t *depth, const float *pxp, const float *pyp, const CamF &cam, float scaling,
                           float maxcam, int4 *vox, int W, int H, int4 *bnd, uint8_t *processed, Counters *cnt,
                           uint32_t *barrier, int device, cudaStream_t s) {
-  int tilesX = (W + 31) / 32, tilesY = (H + 31) / 32;
+  int tilesX = (W + 31) / 32, tilesY = (H + DD_ROWS - 1) / DD_ROWS;
   int ntiles = tilesX * tilesY;
   const int threads = 32 * DD_WARPS;
   // co-resident blocks of the cooperative launch, per device (queried once)
@@ -521,12 +528,18 @@ __global__ void k_parents(int npend, uint32_t leaves_before, uint32_t leaves_max
 constexpr int FIN_THREADS = 1024;
 constexpr size_t FIN_SMEM_MAX = 200 * 1024;
 
+// npend < 0: read the count on the device (and do nothing after an
+// allocation error, which the host reports).
 __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const PendingLeaf *pend, int npend, uint32_t npix,
                                                                  uint32_t *rank, uint32_t leaves_before,
                                                                  uint32_t leaves_max, uint32_t *tree, ushort4 *leaf,
                                                                  uint32_t frame, uint32_t *stamp, uint32_t *queue,
                                                                  Counters *cnt, uint32_t n, uint32_t *parent) {
   extern __shared__ uint32_t fin_smem[];
+  if (npend < 0) {
+    if (cnt->error & (ERR_SPIN_TIMEOUT | ERR_DEDUPE_NOT_CONVERGED | ERR_PENDING_OVERFLOW)) return;
+    npend = (int)cnt->pending;
+  }
   const uint32_t nwords = (npix + 31) / 32;
   uint32_t *bitmap = fin_smem;
   uint32_t *chunk_base = fin_smem + nwords;  // [FIN_THREADS]
@@ -565,11 +578,15 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const PendingLe
   }
 }
 
+bool finalize_small_fits(uint32_t npix) {
+  return sizeof(uint32_t) * (((size_t)npix + 31) / 32 + FIN_THREADS) <= FIN_SMEM_MAX;
+}
+
 bool launch_finalize_small(const PendingLeaf *pend, int npend, uint32_t npix, uint32_t *rank_scratch,
                            uint32_t leaves_before, uint32_t leaves_max, uint32_t *tree, ushort4 *leaf,
                            uint32_t frame, uint32_t *stamp, uint32_t *queue, Counters *cnt, uint32_t n,
                            uint32_t *parent, int device, cudaStream_t s) {
-  if (npend <= 0) return true;
+  if (npend == 0) return true;
   const size_t smem = sizeof(uint32_t) * (((size_t)npix + 31) / 32 + FIN_THREADS);
   if (smem > FIN_SMEM_MAX) return false;
   static std::atomic<unsigned long long> attr_devices{0};

@@ -244,10 +244,10 @@ static ff_status ensure_image(ff_handle *h, int W, int H) {
     CK(cudaMalloc(&h->d_sort_tmp, std::max<size_t>(h->sort_tmp_bytes, 16)));
     h->cap_pix = npix;
   }
-  size_t tiles = (size_t)((W + 31) / 32) * ((H + 31) / 32);
-  if (tiles * 32 * 4 > h->bnd_elems) {
+  const size_t bnd_need = dedupe_boundary_elems(W, H);
+  if (bnd_need > h->bnd_elems) {
     cudaFree(h->d_bnd);
-    h->bnd_elems = tiles * 32 * 4;
+    h->bnd_elems = bnd_need;
     CK(alloc(&h->d_bnd, h->bnd_elems));
   }
   return FF_OK;
@@ -468,6 +468,30 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
                 frame, h->d_stamp, h->d_queue, h->d_pend, (uint32_t)(W * H), h->d_cnt, s);
   h->prof.end(pi, npix * (16 + 1), s);  // keys and flags in (tree walks counted below)
   CK(cudaGetLastError());
+  // fuse: every voxel of every queued brick read and written: SDF, weight
+  // (4+4 B, or 2+2 B in FP16) and three 16-bit colour channels
+  const double brick_bytes = 512.0 * 2 * ((h->cfg.storage == FF_STORAGE_FP16 ? 4 : 8) + 6);
+  const uint32_t leaves_before = h->leaves_used;
+  const FuseGate no_gate = {nullptr, 0, 0, 0, 0};
+  const bool one_sync = finalize_small_fits((uint32_t)(W * H));
+  int pi_fin = -1, pi_fuse = -1;
+  if (one_sync) {
+    // the leaf finalisation and the voxel update read this frame's counts
+    // on the device; the update stands aside when the volume must grow first
+    uint32_t *rank_scratch = h->d_keys + 3 * h->cap_pix;
+    pi_fin = h->prof.begin(ST_FINALIZE, s);
+    launch_finalize_small(h->d_pend, -1, (uint32_t)(W * H), rank_scratch, leaves_before, h->cfg.leaves_max,
+                          h->d_tree, h->d_leaf, frame, h->d_stamp, h->d_queue, h->d_cnt, h->n, h->d_parent,
+                          h->cfg.device, s);
+    h->prof.end(pi_fin, 0.0, s);
+    const FuseGate gate = {h->d_cnt, h->n, leaves_before, h->cfg.leaves_max, h->cfg.branches_max};
+    pi_fuse = h->prof.begin(ST_FUSE, s);
+    launch_fuse(h->d_queue, 0, gate, h->d_leaf, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
+                h->cfg.storage, d_depth, d_bgr, W, H, q, h->cfg.scale, h->cfg.threshold, scaling, maxcam,
+                h->d_rcp_tab, h->rcp_shift, s);
+    h->prof.end(pi_fuse, 0.0, s);
+    CK(cudaGetLastError());
+  }
   CK(cudaMemcpyAsync(&hc, h->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   if (hc.error & (ERR_SPIN_TIMEOUT | ERR_DEDUPE_NOT_CONVERGED))
@@ -478,47 +502,45 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
   h->processed = hc.processed;
   h->dedupe_rounds = hc.dedupe_iters;
   const uint32_t npend = hc.pending;
-  const uint32_t leaves_before = h->leaves_used;
-  const uint32_t existing_queued = hc.queued;
-  if (npend) {
-    pi = h->prof.begin(ST_FINALIZE, s);
+  uint32_t new_queued = 0;
+  if (leaves_before < h->cfg.leaves_max) new_queued = std::min(npend, h->cfg.leaves_max - leaves_before);
+  // with one synchronisation the counters already include the new leaves
+  const uint32_t nq = one_sync ? hc.queued : hc.queued + new_queued;
+  if (!one_sync && npend) {
+    pi_fin = h->prof.begin(ST_FINALIZE, s);
     uint32_t *k_in = h->d_keys, *v_in = h->d_keys + h->cap_pix, *k_out = h->d_keys + 2 * h->cap_pix,
              *v_out = h->d_keys + 3 * h->cap_pix;
     int end_bit = 1;
     while ((1u << end_bit) < (uint32_t)(W * H)) end_bit++;
-    if (!launch_finalize_small(h->d_pend, (int)npend, (uint32_t)(W * H), v_out, leaves_before, h->cfg.leaves_max,
-                               h->d_tree, h->d_leaf, frame, h->d_stamp, h->d_queue, h->d_cnt, h->n, h->d_parent,
-                               h->cfg.device, s)) {
-      CK(sort_pending(h->d_pend, (int)npend, k_in, v_in, k_out, v_out, h->d_sort_tmp, h->sort_tmp_bytes, end_bit,
-                      s));
-      launch_finalize(h->d_pend, v_out, (int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->d_leaf, frame,
-                      h->d_stamp, h->d_queue, h->d_cnt, s);
-      launch_parents((int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->n, h->d_leaf, h->d_parent, s);
-    }
-    h->prof.end(pi, (double)npend * (sizeof(PendingLeaf) + 8 + 4), s);
-    h->leaves_used += npend;
+    CK(sort_pending(h->d_pend, (int)npend, k_in, v_in, k_out, v_out, h->d_sort_tmp, h->sort_tmp_bytes, end_bit, s));
+    launch_finalize(h->d_pend, v_out, (int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->d_leaf, frame,
+                    h->d_stamp, h->d_queue, h->d_cnt, s);
+    launch_parents((int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->n, h->d_leaf, h->d_parent, s);
+    h->prof.end(pi_fin, 0.0, s);
   }
-  uint32_t new_queued = 0;
-  if (leaves_before < h->cfg.leaves_max) new_queued = std::min(npend, h->cfg.leaves_max - leaves_before);
+  h->prof.set_bytes(pi_fin, (double)npend * (sizeof(PendingLeaf) + 8 + 4));
+  h->leaves_used += npend;
   h->new_leaves = npend;
-  const uint32_t nq = existing_queued + new_queued;
+  bool fuse_now = !one_sync;
   if (h->leaves_used < h->cfg.leaves_max && h->branches_used < h->cfg.branches_max &&
       (hc.box_min[0] < 0 || hc.box_min[1] < 0 || hc.box_min[2] < 0 || hc.box_max[0] >= (int)h->n ||
        hc.box_max[1] >= (int)h->n || hc.box_max[2] >= (int)h->n)) {
-    pi = h->prof.begin(ST_GROW, s);
+    // (with one synchronisation the update stood aside for this)
+    int pi = h->prof.begin(ST_GROW, s);
     const double tree_bytes = (double)h->branches_used * 4 * 2 + (double)h->leaves_used * 8 * 2;
     ff_status st = grow(h, hc.box_min, hc.box_max);
     h->prof.end(pi, tree_bytes, s);  // octree and leaf positions read and written
     if (st != FF_OK) return st;
+    fuse_now = true;
   }
-  // fuse: every voxel of every queued brick read and written: SDF, weight
-  // (4+4 B, or 2+2 B in FP16) and three 16-bit colour channels
-  const double brick_bytes = 512.0 * 2 * ((h->cfg.storage == FF_STORAGE_FP16 ? 4 : 8) + 6);
-  pi = h->prof.begin(ST_FUSE, s);
-  launch_fuse(h->d_queue, (int)nq, h->d_leaf, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
-              h->cfg.storage, h->cfg.leaves_max, d_depth, d_bgr, W, H, q, h->cfg.scale, h->cfg.threshold, scaling,
-              maxcam, h->d_rcp_tab, h->rcp_shift, s);
-  h->prof.end(pi, (double)nq * brick_bytes, s);
+  if (fuse_now) {
+    pi_fuse = h->prof.begin(ST_FUSE, s);
+    launch_fuse(h->d_queue, (int)nq, no_gate, h->d_leaf, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
+                h->cfg.storage, d_depth, d_bgr, W, H, q, h->cfg.scale, h->cfg.threshold, scaling, maxcam,
+                h->d_rcp_tab, h->rcp_shift, s);
+    h->prof.end(pi_fuse, 0.0, s);
+  }
+  h->prof.set_bytes(pi_fuse, (double)nq * brick_bytes);
   CK(cudaGetLastError());
   if (h->leaves_used > h->cfg.leaves_max) h->meshing_ok = false;
   h->queued = nq;

@@ -57,14 +57,13 @@ __device__ __forceinline__ float rcp_upd(float x, const uint32_t *tab, int shift
 }
 
 template <bool FP16, bool RCP_HOST>
-__global__ void __launch_bounds__(512) k_fuse(const uint32_t *__restrict__ queue, const ushort4 *__restrict__ leaf,
-                                              float *__restrict__ sdf, float *__restrict__ wgt,
-                                              __half *__restrict__ sdf16, __half *__restrict__ wgt16,
-                                              uint16_t *__restrict__ col, uint32_t leaves_max,
-                                              const uint16_t *__restrict__ depth, const uint8_t *__restrict__ bgr,
-                                              int W, int H, CamF q, float scale, float thr, float scaling,
-                                              float maxcam, const uint32_t *__restrict__ rtab, int rshift) {
-  const uint32_t brick = queue[blockIdx.x];
+__device__ __forceinline__ void fuse_brick(const uint32_t brick, const ushort4 *__restrict__ leaf,
+                                           float *__restrict__ sdf, float *__restrict__ wgt,
+                                           __half *__restrict__ sdf16, __half *__restrict__ wgt16,
+                                           uint16_t *__restrict__ col, const uint16_t *__restrict__ depth,
+                                           const uint8_t *__restrict__ bgr, int W, int H, const CamF &q, float scale,
+                                           float thr, float scaling, float maxcam, const uint32_t *__restrict__ rtab,
+                                           int rshift) {
   const int v = threadIdx.x;
   const int x = v & 7, y = (v >> 3) & 7, z = v >> 6;
   const ushort4 o = leaf[brick];
@@ -150,14 +149,52 @@ __global__ void __launch_bounds__(512) k_fuse(const uint32_t *__restrict__ queue
   }
 }
 
-void launch_fuse(const uint32_t *queue, int nq, const ushort4 *leaf, float *sdf, float *wgt, __half *sdf16,
-                 __half *wgt16, uint16_t *col, int storage, uint32_t leaves_max, const uint16_t *depth,
-                 const uint8_t *bgr, int W, int H, const CamF &q, float scale, float thr, float scaling,
-                 float maxcam, const uint32_t *rcp_tab, int rcp_shift, cudaStream_t s) {
-  if (nq <= 0) return;
-#define FF_FUSE(F16, RH)                                                                                         \
-  k_fuse<F16, RH><<<nq, 512, 0, s>>>(queue, leaf, sdf, wgt, sdf16, wgt16, col, leaves_max, depth, bgr, W, H, q, \
-                                     scale, thr, scaling, maxcam, rcp_tab, rcp_shift)
+// Whether this frame's update must wait for the host: an allocation error, or
+// the volume must grow first (the host then grows and launches the update
+// again).  Mirrors the host's test after the traversal.
+__device__ __forceinline__ bool fuse_deferred(const FuseGate &g) {
+  const Counters *c = g.cnt;
+  if (c->error & (ERR_SPIN_TIMEOUT | ERR_DEDUPE_NOT_CONVERGED | ERR_PENDING_OVERFLOW)) return true;
+  const uint32_t leaves = g.leaves_before + c->pending;
+  const uint32_t branches = min(c->branches_used, g.branches_max);
+  const int n = (int)g.n;
+  const bool outside = c->box_min[0] < 0 || c->box_min[1] < 0 || c->box_min[2] < 0 || c->box_max[0] >= n ||
+                       c->box_max[1] >= n || c->box_max[2] >= n;
+  return leaves < g.leaves_max && branches < g.branches_max && outside;
+}
+
+// One 512-thread block per brick, one thread per voxel.  With a gate, the
+// brick count is read on the device (the queue after this frame's new
+// leaves) and the blocks loop over it.
+template <bool FP16, bool RCP_HOST>
+__global__ void __launch_bounds__(512) k_fuse(const uint32_t *__restrict__ queue, uint32_t nq, FuseGate gate,
+                                              const ushort4 *__restrict__ leaf, float *__restrict__ sdf,
+                                              float *__restrict__ wgt, __half *__restrict__ sdf16,
+                                              __half *__restrict__ wgt16, uint16_t *__restrict__ col,
+                                              const uint16_t *__restrict__ depth, const uint8_t *__restrict__ bgr,
+                                              int W, int H, CamF q, float scale, float thr, float scaling,
+                                              float maxcam, const uint32_t *__restrict__ rtab, int rshift) {
+  if (gate.cnt) {
+    if (fuse_deferred(gate)) return;
+    nq = gate.cnt->queued;
+  }
+  for (uint32_t b = blockIdx.x; b < nq; b += gridDim.x)
+    fuse_brick<FP16, RCP_HOST>(queue[b], leaf, sdf, wgt, sdf16, wgt16, col, depth, bgr, W, H, q, scale, thr, scaling,
+                               maxcam, rtab, rshift);
+}
+
+void launch_fuse(const uint32_t *queue, int nq, const FuseGate &gate, const ushort4 *leaf, float *sdf, float *wgt,
+                 __half *sdf16, __half *wgt16, uint16_t *col, int storage, const uint16_t *depth, const uint8_t *bgr,
+                 int W, int H, const CamF &q, float scale, float thr, float scaling, float maxcam,
+                 const uint32_t *rcp_tab, int rcp_shift, cudaStream_t s) {
+  // host count: one block per brick; device count: 4 resident blocks per SM
+  // loop over the bricks
+  int grid = nq;
+  if (gate.cnt) grid = 148 * 4;
+  if (grid <= 0) return;
+#define FF_FUSE(F16, RH)                                                                                           \
+  k_fuse<F16, RH><<<grid, 512, 0, s>>>(queue, (uint32_t)(nq > 0 ? nq : 0), gate, leaf, sdf, wgt, sdf16, wgt16, col, \
+                                       depth, bgr, W, H, q, scale, thr, scaling, maxcam, rcp_tab, rcp_shift)
   const bool rh = rcp_tab != nullptr;
   note_launch();
   if (storage == 1) {
