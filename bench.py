@@ -192,8 +192,10 @@ def measured_hbm_peak():
 
 
 def read_traffic_table() -> dict:
-    """Per-brick / per-sample DRAM traffic from the committed ncu summaries
-    (lines `traffic <stage> <bytes per unit> <unit>`)."""
+    """DRAM traffic per algorithmic byte of each stage, from the committed ncu
+    capture (lines `traffic <stage> <dram bytes / algorithmic byte> ratio`).
+    A stage's traffic per launch is that ratio times its algorithmic bytes per
+    launch measured here: the capture's traffic scaled to this launch size."""
     out = {}
     p = os.path.join(HERE, "profiles", "traffic.txt")
     if not os.path.exists(p):
@@ -201,8 +203,8 @@ def read_traffic_table() -> dict:
     with open(p) as f:
         for line in f:
             parts = line.split()
-            if len(parts) >= 4 and parts[0] == "traffic":
-                out[parts[1]] = (float(parts[2]), parts[3])
+            if len(parts) >= 4 and parts[0] == "traffic" and parts[3] == "ratio":
+                out[parts[1]] = float(parts[2])
     return out
 
 
@@ -369,17 +371,16 @@ def run_b200(a):
     traffic = None
     tt = read_traffic_table()
     if dom in tt and n_d:
-        per_unit, unit = tt[dom]
-        unit_bytes = {"brick": 14336.0 if a.storage == "fp32" else 10240.0}.get(unit)
-        if unit_bytes:
-            traffic = per_unit * (bytes_d / unit_bytes) / n_d
+        traffic = round(tt[dom] * bytes_d / n_d)
     roofline = {"bound": "hbm", "kernel": STAGE_KERNELS[dom], "stage": dom, "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "peak_source": f"{peak_kind} (copy bandwidth)",
                 "algorithmic_bytes_per_launch": bytes_d / n_d if n_d else 0, "launches": n_d,
                 "avg_launch_us": 1e3 * ms_d / n_d if n_d else 0, "traffic": traffic}
     stage_rec = {k: {"ms": round(v[0], 3), "share": round(v[0] / prof_ms, 4) if prof_ms else 0,
-                     "GB/s": round(v[1] / (v[0] / 1e3) / 1e9, 1) if v[0] > 0 else 0, "launches": v[2]}
+                     "GB/s": round(v[1] / (v[0] / 1e3) / 1e9, 1) if v[0] > 0 else 0, "launches": v[2],
+                     "bytes_per_launch": round(v[1] / v[2]) if v[2] else 0,
+                     "traffic_per_launch": round(tt[k] * v[1] / v[2]) if (k in tt and v[2]) else None}
                  for k, v in stages.items()}
 
     cpu = None
