@@ -114,29 +114,8 @@ __device__ __forceinline__ int4 project_point(float d, float px, float py, const
 // boundary bits and repeat until no boundary changes; a chain of dependencies
 // crosses at most tilesX+tilesY tiles, which bounds the number of rounds.
 
-__device__ void grid_barrier(uint32_t *bar, uint32_t nblocks, Counters *cnt) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    volatile uint32_t *gen = bar + 1;
-    uint32_t g = *gen;
-    __threadfence();
-    if (atomicAdd(bar, 1u) == nblocks - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      int spins = 0;
-      while (*gen == g) {
-        if (++spins > SPIN_LIMIT) {
-          atomicOr(&cnt->error, ERR_SPIN_TIMEOUT);
-          break;
-        }
-        __nanosleep(32);
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
+__device__ __forceinline__ void grid_barrier(uint32_t *bar, uint32_t nblocks, Counters *cnt) {
+  grid_barrier_bounded(bar, nblocks, &cnt->error, ERR_SPIN_TIMEOUT);
 }
 
 constexpr int DD_WARPS = 4;  // tiles (warps) per block

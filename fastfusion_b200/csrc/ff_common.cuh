@@ -69,4 +69,32 @@ struct CamF {
   float fx, fy, cx, cy;
 };
 
+// Barrier over all blocks of a cooperative launch (every block resident).
+// bar[0] counts arrivals, bar[1] is the generation; both start at zero.
+// A wait that exceeds SPIN_LIMIT sets err_bit in *err and stops waiting.
+__device__ __forceinline__ void grid_barrier_bounded(uint32_t *bar, uint32_t nblocks, uint32_t *err, uint32_t err_bit) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile uint32_t *gen = bar + 1;
+    const uint32_t g = *gen;
+    __threadfence();
+    if (atomicAdd(bar, 1u) == nblocks - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      int spins = 0;
+      while (*gen == g) {
+        if (++spins > SPIN_LIMIT) {
+          atomicOr(err, err_bit);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
 }  // namespace ffb

@@ -232,115 +232,143 @@ __device__ __forceinline__ void push_vert(const GenQueues &Q, const Out &O, cons
   push(O.vertq, O.count + 3, Q.cap_vert, v, Q.error);
 }
 
-__device__ void vert_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot *S8) {
+// The item functions are templated on their axis and fully unrolled, so every
+// slot array index is a compile-time constant and the slots stay in registers.
+
+__device__ __forceinline__ void vert_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot (&S8)[8]) {
   bool any = false;
+#pragma unroll
   for (int j = 0; j < 8; j++) any |= is_sub(g, S8[j]);
   if (any) {
     Slot C[8];
+#pragma unroll
     for (int j = 0; j < 8; j++) C[j] = ch(g, S8[j], 7 - j);
     push_vert(Q, O, C);
     return;
   }
   // the vertex is a corner of the smallest slot around it
   int size = S8[0].size, small = 0;
+#pragma unroll
   for (int j = 1; j < 8; j++)
     if (S8[j].size < size) size = S8[j].size, small = j;
-  int o[3];
-  for (int r = 0; r < 3; r++) o[r] = (int)S8[small].o[r] + (((small >> r) & 1) ? 0 : size) - size;
+  int o[3] = {0, 0, 0};
+#pragma unroll
+  for (int j = 0; j < 8; j++)
+    if (j == small) {
+#pragma unroll
+      for (int r = 0; r < 3; r++) o[r] = (int)S8[j].o[r] + (((j >> r) & 1) ? 0 : size) - size;
+    }
   uint32_t L[8];
+#pragma unroll
   for (int j = 0; j < 8; j++) L[j] = S8[j].la;
   emit_cell(Q, 7, 0, o, size, L, 8);
 }
 
-__device__ void edge_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot *S4, int e) {
+template <int E>
+__device__ __forceinline__ void edge_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot (&S4)[4]) {
+  constexpr int P = E == 0 ? 1 : 0, Qx = E == 2 ? 1 : 2;  // the two axes across the edge line
   bool any = false;
+#pragma unroll
   for (int j = 0; j < 4; j++) any |= is_sub(g, S4[j]);
-  int p, q;
-  others(e, p, q);
   if (!any) {
     // the edge line runs along a side of the smallest slot
     int size = S4[0].size, small = 0;
+#pragma unroll
     for (int j = 1; j < 4; j++)
       if (S4[j].size < size) size = S4[j].size, small = j;
-    int o[3];
-    o[e] = S4[small].o[e];
-    o[p] = (int)S4[small].o[p] + ((small & 1) ? 0 : size) - size;
-    o[q] = (int)S4[small].o[q] + ((small & 2) ? 0 : size) - size;
+    int o[3] = {0, 0, 0};
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (j == small) {
+        o[E] = S4[j].o[E];
+        o[P] = (int)S4[j].o[P] + ((j & 1) ? 0 : size) - size;
+        o[Qx] = (int)S4[j].o[Qx] + ((j & 2) ? 0 : size) - size;
+      }
     uint32_t L[4] = {S4[0].la, S4[1].la, S4[2].la, S4[3].la};
-    emit_cell(Q, 4 + e, 0, o, size, L, 4);
+    emit_cell(Q, 4 + E, 0, o, size, L, 4);
     return;
   }
+#pragma unroll
   for (int half = 0; half < 2; half++) {
     Slot H[4];
+#pragma unroll
     for (int j = 0; j < 4; j++) {
-      int k = ((j & 1) ? 0 : (1 << p)) | (((j >> 1) & 1) ? 0 : (1 << q)) | (half ? (1 << e) : 0);
+      const int k = ((j & 1) ? 0 : (1 << P)) | (((j >> 1) & 1) ? 0 : (1 << Qx)) | (half ? (1 << E) : 0);
       H[j] = ch(g, S4[j], k);
     }
-    push_edge(Q, O, H, e);
+    push_edge(Q, O, H, E);
   }
   Slot S8[8];
+#pragma unroll
   for (int j = 0; j < 8; j++) {
     // across the edge line: the half of the slot next to the line; along the
     // edge: the half on the vertex's own side of the midpoint
-    int pj = (j >> p) & 1, qj = (j >> q) & 1, ej = (j >> e) & 1;
-    int k = (pj ? 0 : (1 << p)) | (qj ? 0 : (1 << q)) | (ej ? (1 << e) : 0);
+    const int pj = (j >> P) & 1, qj = (j >> Qx) & 1, ej = (j >> E) & 1;
+    const int k = (pj ? 0 : (1 << P)) | (qj ? 0 : (1 << Qx)) | (ej ? (1 << E) : 0);
     S8[j] = ch(g, S4[pj | (qj << 1)], k);
   }
   push_vert(Q, O, S8);
 }
 
-__device__ void face_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot &A, const Slot &B, int ax) {
+template <int AX>
+__device__ __forceinline__ void face_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot &A,
+                                          const Slot &B) {
   if (!is_sub(g, A) && !is_sub(g, B)) {
-    int size = min((int)A.size, (int)B.size);
-    const Slot &small = A.size <= B.size ? A : B;
-    int o[3] = {small.o[0], small.o[1], small.o[2]};
-    o[ax] = (int)B.o[ax] - size;
+    const int size = min((int)A.size, (int)B.size);
+    const bool a_small = A.size <= B.size;
+    int o[3] = {a_small ? A.o[0] : B.o[0], a_small ? A.o[1] : B.o[1], a_small ? A.o[2] : B.o[2]};
+    o[AX] = (int)B.o[AX] - size;
     uint32_t L[2] = {A.la, B.la};
-    emit_cell(Q, 1 + ax, 0, o, size, L, 2);
+    emit_cell(Q, 1 + AX, 0, o, size, L, 2);
     return;
   }
-  const int bit = 1 << ax;
-  int u, v;
-  others(ax, u, v);
+  constexpr int bit = 1 << AX;
+  constexpr int U = AX == 0 ? 1 : 0, V = AX == 2 ? 1 : 2;
   // the two sides' halves next to the face: A's children on its +ax side, B's
   // on its -ax side (a slot that is not subdivided stands for all of them)
   Slot a[8], b[8];
+#pragma unroll
   for (int k = 0; k < 8; k++) {
     if (k & bit) continue;
     a[k] = ch(g, A, k | bit);
     b[k] = ch(g, B, k);
   }
+#pragma unroll
   for (int qd = 0; qd < 4; qd++) {
-    int k = ((qd & 1) ? (1 << u) : 0) | ((qd & 2) ? (1 << v) : 0);
-    push_face(Q, O, a[k], b[k], ax);
+    const int k = ((qd & 1) ? (1 << U) : 0) | ((qd & 2) ? (1 << V) : 0);
+    push_face(Q, O, a[k], b[k], AX);
   }
+#pragma unroll
   for (int t = 0; t < 2; t++) {
-    const int e = t == 0 ? u : v;
-    const int other = t == 0 ? v : u;
-    int p, q;
-    others(e, p, q);
+    const int e = t == 0 ? U : V;
+    const int other = t == 0 ? V : U;
+    const int p = e == 0 ? 1 : 0, q = e == 2 ? 1 : 2;
+#pragma unroll
     for (int half = 0; half < 2; half++) {
       Slot S4[4];
+#pragma unroll
       for (int j = 0; j < 4; j++) {
         int side[3] = {0, 0, 0};
         side[p] = j & 1;
         side[q] = (j >> 1) & 1;
-        int k = (half ? (1 << e) : 0) | (side[other] ? (1 << other) : 0);
-        S4[j] = side[ax] ? b[k] : a[k];
+        const int k = (half ? (1 << e) : 0) | (side[other] ? (1 << other) : 0);
+        S4[j] = side[AX] ? b[k] : a[k];
       }
       push_edge(Q, O, S4, e);
     }
   }
   Slot S8[8];
+#pragma unroll
   for (int j = 0; j < 8; j++) {
-    int k = j & ~bit;
-    S8[j] = ((j >> ax) & 1) ? b[k] : a[k];
+    const int k = j & ~bit;
+    S8[j] = ((j >> AX) & 1) ? b[k] : a[k];
   }
   push_vert(Q, O, S8);
 }
 
 // one subdivided slot: its children, their 12 faces, 6 edges and centre
-__device__ void cell_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot *C) {
+__device__ __forceinline__ void cell_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot (&C)[8]) {
+#pragma unroll
   for (int j = 0; j < 8; j++) {
     if (is_sub(g, C[j])) {
       push_cell(Q, O, C[j]);
@@ -350,17 +378,23 @@ __device__ void cell_item(const GenCtx &g, const GenQueues &Q, const Out &O, con
       emit_cell(Q, 0, 0, o, C[j].size, L, 1);
     }
   }
-  const int F[3][4][2] = {{{0, 1}, {2, 3}, {4, 5}, {6, 7}}, {{0, 2}, {1, 3}, {4, 6}, {5, 7}}, {{0, 4}, {1, 5}, {2, 6}, {3, 7}}};
+  constexpr int F[3][4][2] = {{{0, 1}, {2, 3}, {4, 5}, {6, 7}}, {{0, 2}, {1, 3}, {4, 6}, {5, 7}},
+                              {{0, 4}, {1, 5}, {2, 6}, {3, 7}}};
+#pragma unroll
   for (int ax = 0; ax < 3; ax++)
+#pragma unroll
     for (int i = 0; i < 4; i++) push_face(Q, O, C[F[ax][i][0]], C[F[ax][i][1]], ax);
+#pragma unroll
   for (int x = 0; x < 2; x++) {
     Slot S4[4] = {C[x], C[x | 2], C[x | 4], C[x | 6]};
     push_edge(Q, O, S4, 0);
   }
+#pragma unroll
   for (int y = 0; y < 4; y += 2) {
     Slot S4[4] = {C[y], C[y | 1], C[y | 4], C[y | 5]};
     push_edge(Q, O, S4, 1);
   }
+#pragma unroll
   for (int z = 0; z < 8; z += 4) {
     Slot S4[4] = {C[z], C[z | 1], C[z | 2], C[z | 3]};
     push_edge(Q, O, S4, 2);
@@ -370,7 +404,7 @@ __device__ void cell_item(const GenCtx &g, const GenQueues &Q, const Out &O, con
 
 // Items of level `lv` (queue buffer lv & 1, counters lvl + 4 lv) expand into
 // level lv + 1 or emit cells.  Level 0 is the root: the volume's 8 octants.
-__global__ void __launch_bounds__(128) k_gen_level(GenCtx g, GenQueues Q, int lv, uint32_t n) {
+__device__ __forceinline__ void gen_level(const GenCtx &g, const GenQueues &Q, int lv, uint32_t n) {
   const int cur = lv & 1, nb = cur ^ 1;
   const bool root = lv == 0;
   const uint32_t *cnt = Q.lvl + 4 * lv;
@@ -399,14 +433,31 @@ __global__ void __launch_bounds__(128) k_gen_level(GenCtx g, GenQueues Q, int lv
       cell_item(g, Q, O, C);
     } else if (i < nc + nf) {
       const FaceItem f = Q.faceq[cur][i - nc];
-      face_item(g, Q, O, f.a, f.b, f.axis);
+      if (f.axis == 0) face_item<0>(g, Q, O, f.a, f.b);
+      else if (f.axis == 1) face_item<1>(g, Q, O, f.a, f.b);
+      else face_item<2>(g, Q, O, f.a, f.b);
     } else if (i < nc + nf + ne) {
       const EdgeItem e = Q.edgeq[cur][i - nc - nf];
-      edge_item(g, Q, O, e.s, e.axis);
+      if (e.axis == 0) edge_item<0>(g, Q, O, e.s);
+      else if (e.axis == 1) edge_item<1>(g, Q, O, e.s);
+      else edge_item<2>(g, Q, O, e.s);
     } else {
       const VertItem v = Q.vertq[cur][i - nc - nf - ne];
       vert_item(g, Q, O, v.s);
     }
+  }
+}
+
+// All levels in one cooperative launch, a grid barrier between levels; stops
+// after the first level that queued nothing (or at max_levels).
+// bar: 2 zeroed words.
+__global__ void __launch_bounds__(128) k_gen_level(GenCtx g, GenQueues Q, uint32_t n, int max_levels, uint32_t *bar) {
+  for (int lv = 0; lv < max_levels; lv++) {
+    gen_level(g, Q, lv, n);
+    grid_barrier_bounded(bar, gridDim.x, Q.error, ERR_SPIN_TIMEOUT);
+    const volatile uint32_t *c = Q.lvl + 4 * (lv + 1);
+    if (c[0] == 0 && c[1] == 0 && c[2] == 0 && c[3] == 0) break;
+    if (*(volatile uint32_t *)Q.error & ERR_SPIN_TIMEOUT) break;
   }
 }
 
@@ -590,17 +641,45 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
     }
     uint16_t ll[3], lh[3];
     float rr[3];
+    // leaf scales are powers of two: divide by shifting (same truncating
+    // quotient and remainder as / and %), and rem / ls is exact
+    const bool pow2 = ls > 0 && (ls & (ls - 1)) == 0;
+    const int sh = __ffs(ls) - 1;
+    const float inv_ls = __int_as_float((127 - sh) << 23);
 #pragma unroll
     for (int r = 0; r < 3; r++) {
       const int p = sample_pos(G, r, bb[r]);
-      ll[r] = (uint16_t)((p - lo[r]) / ls);
+      const int num = p - lo[r];
+      int q, rm;
+      if (pow2) {
+        const int mag = num < 0 ? -num : num;
+        q = num < 0 ? -(mag >> sh) : (mag >> sh);
+        rm = num < 0 ? -(mag & (ls - 1)) : (mag & (ls - 1));
+      } else {
+        q = num / ls;
+        rm = num % ls;
+      }
+      ll[r] = (uint16_t)q;
       if (c_role[t][r]) {
         lh[r] = ll[r];
         rr[r] = 0.0f;
       } else {
-        const uint16_t rem = (uint16_t)((p - lo[r]) % ls);
-        rr[r] = __fdiv_rn((float)rem, (float)ls);
+        const uint16_t rem = (uint16_t)rm;
+        rr[r] = pow2 ? __fmul_rn((float)rem, inv_ls) : __fdiv_rn((float)rem, (float)ls);
         lh[r] = (uint16_t)(ll[r] + ((double)rr[r] > 0.0 && ll[r] < 7));
+      }
+    }
+    if (t == 0 && rr[0] == 0.0f && rr[1] == 0.0f && rr[2] == 0.0f) {
+      // on the leaf's lattice the weights are (1, 0, ..., 0) and the
+      // trilinear sums reduce to the voxel itself (finite values)
+      const size_t v0 = vox_index(m, leaf, ll[0], ll[1], ll[2]);
+      const float d0 = vd(m, v0);
+      if (isfinite(d0)) {
+        s.w = __fadd_rn(s.w, vw(m, v0));
+        s.d = d0;
+#pragma unroll
+        for (int r = 0; r < 3; r++) s.c[r] = vc(m, v0, r);
+        continue;
       }
     }
     if (t == 0) {
@@ -651,6 +730,18 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
       // bilinear over the two lattice axes a < b (addBrickWallX/Y/Z)
       const int a = t == 1 ? 1 : 0, b = t == 3 ? 1 : 2;
       const float ra = rr[a], rb = rr[b], ran = __fsub_rn(1.0f, ra), rbn = __fsub_rn(1.0f, rb);
+      if (ra == 0.0f && rb == 0.0f) {
+        // weights (1, 0, 0, 0): the sums reduce to the voxel itself (finite values)
+        const size_t v0 = vox_index(m, leaf, ll[0], ll[1], ll[2]);
+        const float w0 = vw(m, v0), d0 = vd(m, v0);
+        if (isfinite(w0) && isfinite(d0)) {
+          s.w = __fadd_rn(s.w, w0);
+          s.d = d0;
+#pragma unroll
+          for (int r = 0; r < 3; r++) s.c[r] = vc(m, v0, r);
+          continue;
+        }
+      }
       const float f[4] = {__fmul_rn(rbn, ran), __fmul_rn(rbn, ra), __fmul_rn(rb, ran), __fmul_rn(rb, ra)};
       size_t vi[4];
 #pragma unroll
@@ -1223,24 +1314,32 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
     Q.error = I.d_count + 9;
     Q.n_corners = I.d_count + 11;
     GenCtx g{in.tree, in.leaves_max};
-    // a chain cell -> face -> edge -> vertex adds up to three levels below
-    // the octree's depth; more levels run if items are left
-    int depth = 1;
-    for (uint32_t h = in.n; h > 8; h >>= 1) depth++;
-    int lv = 0, batch = depth + 4;
-    bool leftover = true, overflow = false;
-    while (leftover && lv < MAX_GEN_LEVELS) {
-      const int end = std::min(lv + batch, MAX_GEN_LEVELS);
-      note_launch((unsigned)(end - lv));
-      for (; lv < end; lv++) k_gen_level<<<148 * 8, 128, 0, s>>>(g, Q, lv, in.n);
-      MCK(cudaGetLastError());
-      MCK(cudaMemcpyAsync(I.h_count, I.d_count, COUNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-      MCK(cudaStreamSynchronize(s));
-      const uint32_t *c = I.h_count + LEVEL_COUNTS + 4 * lv;
-      leftover = c[0] || c[1] || c[2] || c[3];
-      overflow = (I.h_count[9] & ERR_CELL_OVERFLOW) != 0;
-      if (overflow) break;
-      batch = 4;
+    // all levels in one cooperative launch (every block resident)
+    static int resident[64] = {};
+    int dev = 0;
+    MCK(cudaGetDevice(&dev));
+    if (!resident[dev & 63]) {
+      int per_sm = 0, sms = 0;
+      MCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gen_level, 128, 0));
+      MCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      resident[dev & 63] = std::max(1, per_sm * sms);
+    }
+    int blocks = resident[dev & 63];
+    uint32_t nn = in.n;
+    int max_levels = MAX_GEN_LEVELS;
+    uint32_t *bar = I.d_count + 16;
+    void *args[] = {(void *)&g, (void *)&Q, (void *)&nn, (void *)&max_levels, (void *)&bar};
+    note_launch();
+    MCK(cudaLaunchCooperativeKernel((const void *)k_gen_level, dim3(blocks), dim3(128), args, 0, s));
+    MCK(cudaMemcpyAsync(I.h_count, I.d_count, COUNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    MCK(cudaStreamSynchronize(s));
+    const int lv = MAX_GEN_LEVELS;
+    const uint32_t *cl = I.h_count + LEVEL_COUNTS + 4 * lv;
+    const bool leftover = cl[0] || cl[1] || cl[2] || cl[3];
+    const bool overflow = (I.h_count[9] & ERR_CELL_OVERFLOW) != 0;
+    if (I.h_count[9] & ERR_SPIN_TIMEOUT) {
+      err = "meshing: a bounded device-side wait gave up during cell generation";
+      return 5;
     }
     const uint32_t *hc = I.h_count;
     if (overflow) {
