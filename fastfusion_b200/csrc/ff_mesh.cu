@@ -451,7 +451,10 @@ __device__ __forceinline__ void gen_level(const GenCtx &g, const GenQueues &Q, i
 // All levels in one cooperative launch, a grid barrier between levels; stops
 // after the first level that queued nothing (or at max_levels).
 // bar: 2 zeroed words.
-__global__ void __launch_bounds__(128) k_gen_level(GenCtx g, GenQueues Q, uint32_t n, int max_levels, uint32_t *bar) {
+// Few large blocks keep the grid barrier's arrivals few.
+constexpr int GEN_THREADS = 512;
+__global__ void __launch_bounds__(GEN_THREADS) k_gen_level(GenCtx g, GenQueues Q, uint32_t n, int max_levels,
+                                                           uint32_t *bar) {
   for (int lv = 0; lv < max_levels; lv++) {
     gen_level(g, Q, lv, n);
     grid_barrier_bounded(bar, gridDim.x, Q.error, ERR_SPIN_TIMEOUT);
@@ -1202,7 +1205,7 @@ static cudaError_t pool_alloc(void **p, size_t bytes, cudaStream_t s) {
 template <typename T>
 static cudaError_t grow_buf(T *&p, size_t &cap, size_t need, cudaStream_t s) {
   if (need <= cap && p) return cudaSuccess;
-  size_t ncap = std::max<size_t>(need + need / 2, 1024);
+  size_t ncap = std::max<size_t>(2 * need, 4096);
   void *q = nullptr;
   cudaError_t e = pool_alloc(&q, sizeof(T) * ncap, s);
   if (e != cudaSuccess) return e;
@@ -1320,7 +1323,7 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
     MCK(cudaGetDevice(&dev));
     if (!resident[dev & 63]) {
       int per_sm = 0, sms = 0;
-      MCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gen_level, 128, 0));
+      MCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gen_level, GEN_THREADS, 0));
       MCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
       resident[dev & 63] = std::max(1, per_sm * sms);
     }
@@ -1330,7 +1333,7 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
     uint32_t *bar = I.d_count + 16;
     void *args[] = {(void *)&g, (void *)&Q, (void *)&nn, (void *)&max_levels, (void *)&bar};
     note_launch();
-    MCK(cudaLaunchCooperativeKernel((const void *)k_gen_level, dim3(blocks), dim3(128), args, 0, s));
+    MCK(cudaLaunchCooperativeKernel((const void *)k_gen_level, dim3(blocks), dim3(GEN_THREADS), args, 0, s));
     MCK(cudaMemcpyAsync(I.h_count, I.d_count, COUNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     MCK(cudaStreamSynchronize(s));
     const int lv = MAX_GEN_LEVELS;
@@ -1388,7 +1391,27 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
   return 0;
 }
 
+// Reserve pool memory once (allocate and free a block): later buffer growth
+// is served from it instead of fresh driver allocations.
+static cudaError_t reserve_pool(size_t bytes, cudaStream_t s) {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done[dev & 63]) return cudaSuccess;
+  void *p = nullptr;
+  e = pool_alloc(&p, bytes, s);
+  if (e != cudaSuccess) return e;
+  e = cudaFreeAsync(p, s);
+  if (e == cudaSuccess) done[dev & 63] = true;
+  return e;
+}
+
 int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string &err) {
+  // about 2 KB of mesher memory per brick of capacity, at most 512 MB
+  MCK(reserve_pool(std::min<size_t>((size_t)in.leaves_max * 2048, (size_t)512 << 20), s));
   MeshImpl &I = impl(M);
   uint32_t ncells = 0;
   Prof &P = *in.prof;
