@@ -448,20 +448,8 @@ __device__ __forceinline__ void gen_level(const GenCtx &g, const GenQueues &Q, i
   }
 }
 
-// All levels in one cooperative launch, a grid barrier between levels; stops
-// after the first level that queued nothing (or at max_levels).
-// bar: 2 zeroed words.
-// Few large blocks keep the grid barrier's arrivals few.
-constexpr int GEN_THREADS = 512;
-__global__ void __launch_bounds__(GEN_THREADS) k_gen_level(GenCtx g, GenQueues Q, uint32_t n, int max_levels,
-                                                           uint32_t *bar) {
-  for (int lv = 0; lv < max_levels; lv++) {
-    gen_level(g, Q, lv, n);
-    grid_barrier_bounded(bar, gridDim.x, Q.error, ERR_SPIN_TIMEOUT);
-    const volatile uint32_t *c = Q.lvl + 4 * (lv + 1);
-    if (c[0] == 0 && c[1] == 0 && c[2] == 0 && c[3] == 0) break;
-    if (*(volatile uint32_t *)Q.error & ERR_SPIN_TIMEOUT) break;
-  }
+__global__ void __launch_bounds__(128) k_gen_level(GenCtx g, GenQueues Q, int lv, uint32_t n) {
+  gen_level(g, Q, lv, n);
 }
 
 __device__ __forceinline__ uint64_t cell_key(const Cell &c) {
@@ -1317,33 +1305,25 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
     Q.error = I.d_count + 9;
     Q.n_corners = I.d_count + 11;
     GenCtx g{in.tree, in.leaves_max};
-    // all levels in one cooperative launch (every block resident)
-    static int resident[64] = {};
-    int dev = 0;
-    MCK(cudaGetDevice(&dev));
-    if (!resident[dev & 63]) {
-      int per_sm = 0, sms = 0;
-      MCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gen_level, GEN_THREADS, 0));
-      MCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-      resident[dev & 63] = std::max(1, per_sm * sms);
+    // a chain cell -> face -> edge -> vertex adds up to three levels below
+    // the octree's depth; more levels run if items are left
+    int depth = 1;
+    for (uint32_t h = in.n; h > 8; h >>= 1) depth++;
+    int lv = 0, batch = depth + 4;
+    bool leftover = true;
+    while (leftover && lv < MAX_GEN_LEVELS) {
+      const int end = std::min(lv + batch, MAX_GEN_LEVELS);
+      note_launch((unsigned)(end - lv));
+      for (; lv < end; lv++) k_gen_level<<<148 * 8, 128, 0, s>>>(g, Q, lv, in.n);
+      MCK(cudaGetLastError());
+      MCK(cudaMemcpyAsync(I.h_count, I.d_count, COUNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      MCK(cudaStreamSynchronize(s));
+      const uint32_t *cl = I.h_count + LEVEL_COUNTS + 4 * lv;
+      leftover = cl[0] || cl[1] || cl[2] || cl[3];
+      if (I.h_count[9] & ERR_CELL_OVERFLOW) break;
+      batch = 4;
     }
-    int blocks = resident[dev & 63];
-    uint32_t nn = in.n;
-    int max_levels = MAX_GEN_LEVELS;
-    uint32_t *bar = I.d_count + 16;
-    void *args[] = {(void *)&g, (void *)&Q, (void *)&nn, (void *)&max_levels, (void *)&bar};
-    note_launch();
-    MCK(cudaLaunchCooperativeKernel((const void *)k_gen_level, dim3(blocks), dim3(GEN_THREADS), args, 0, s));
-    MCK(cudaMemcpyAsync(I.h_count, I.d_count, COUNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    MCK(cudaStreamSynchronize(s));
-    const int lv = MAX_GEN_LEVELS;
-    const uint32_t *cl = I.h_count + LEVEL_COUNTS + 4 * lv;
-    const bool leftover = cl[0] || cl[1] || cl[2] || cl[3];
     const bool overflow = (I.h_count[9] & ERR_CELL_OVERFLOW) != 0;
-    if (I.h_count[9] & ERR_SPIN_TIMEOUT) {
-      err = "meshing: a bounded device-side wait gave up during cell generation";
-      return 5;
-    }
     const uint32_t *hc = I.h_count;
     if (overflow) {
       for (int k = 0; k < 5; k++) want[k] *= 2;
