@@ -30,6 +30,10 @@ struct ff_handle {
   std::string err;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  // host-input frames: the colour image is copied on a second stream while
+  // the allocation kernels run (it is first read by the voxel update)
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_bgr_free = nullptr, ev_bgr_ready = nullptr;
 
   // map state on the device
   uint32_t *d_tree = nullptr;
@@ -314,6 +318,12 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
   do {
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { fail(FF_ERR_CUDA, "stream"); break; }
     h->own_stream = true;
+    if (cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_bgr_free, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_bgr_ready, cudaEventDisableTiming) != cudaSuccess) {
+      fail(FF_ERR_CUDA, "copy stream");
+      break;
+    }
     size_t L = h->cfg.leaves_max;
     if (alloc(&h->d_tree, h->cfg.branches_max) != cudaSuccess) { fail(FF_ERR_OOM_POOL, "tree"); break; }
     if (alloc(&h->d_leaf, L) != cudaSuccess || alloc(&h->d_parent, L) != cudaSuccess ||
@@ -388,6 +398,12 @@ ff_status ff_destroy(ff_handle *h) {
     if (p) cudaFree(p);
   if (h->h_cnt) cudaFreeHost(h->h_cnt);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  if (h->copy_stream) {
+    cudaStreamSynchronize(h->copy_stream);
+    cudaStreamDestroy(h->copy_stream);
+  }
+  if (h->ev_bgr_free) cudaEventDestroy(h->ev_bgr_free);
+  if (h->ev_bgr_ready) cudaEventDestroy(h->ev_bgr_ready);
   delete h;
   return FF_OK;
 }
@@ -408,8 +424,9 @@ ff_status ff_set_stream(ff_handle *h, void *cuda_stream) {
 }
 
 // The frame, with depth/bgr already on the device (h->d_depth/h->d_bgr or caller memory).
-static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uint8_t *d_bgr, int W, int H,
-                                const double *K, const double *R, const double *t, float scaling, float maxcam,
+static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uint8_t *d_bgr, bool bgr_pending,
+                                int W, int H, const double *K, const double *R, const double *t, float scaling,
+                                float maxcam,
                                 int32_t *queued) {
   cudaStream_t s = h->stream;
   CamF p = cam_world_to_grid(h, K, R, t);
@@ -468,6 +485,7 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
                 frame, h->d_stamp, h->d_queue, h->d_pend, (uint32_t)(W * H), h->d_cnt, s);
   h->prof.end(pi, npix * (16 + 1), s);  // keys and flags in (tree walks counted below)
   CK(cudaGetLastError());
+  if (bgr_pending) CK(cudaStreamWaitEvent(s, h->ev_bgr_ready, 0));
   // fuse: every voxel of every queued brick read and written: SDF, weight
   // (4+4 B, or 2+2 B in FP16) and three 16-bit colour channels
   const double brick_bytes = 512.0 * 2 * ((h->cfg.storage == FF_STORAGE_FP16 ? 4 : 8) + 6);
@@ -563,9 +581,17 @@ ff_status ff_add_map_u16(ff_handle *h, const uint16_t *depth, int width, int hei
   if (!bgr_pitch) bgr_pitch = 3 * (size_t)width;
   CK(cudaMemcpy2DAsync(h->d_depth, sizeof(uint16_t) * width, depth, depth_pitch, sizeof(uint16_t) * width, height,
                        cudaMemcpyHostToDevice, h->stream));
+  // the colour copy waits for the previous frame's update (the last reader of
+  // d_bgr) and overlaps this frame's allocation kernels
+  CK(cudaEventRecord(h->ev_bgr_free, h->stream));
+  CK(cudaStreamWaitEvent(h->copy_stream, h->ev_bgr_free, 0));
   CK(cudaMemcpy2DAsync(h->d_bgr, 3 * (size_t)width, bgr, bgr_pitch, 3 * (size_t)width, height,
-                       cudaMemcpyHostToDevice, h->stream));
-  return add_map_device(h, h->d_depth, h->d_bgr, width, height, K, R, t, scaling, maxcam, queued);
+                       cudaMemcpyHostToDevice, h->copy_stream));
+  CK(cudaEventRecord(h->ev_bgr_ready, h->copy_stream));
+  st = add_map_device(h, h->d_depth, h->d_bgr, true, width, height, K, R, t, scaling, maxcam, queued);
+  // the caller's image must not be read after return, error paths included
+  cudaStreamSynchronize(h->copy_stream);
+  return st;
 }
 
 ff_status ff_add_map_u16_device(ff_handle *h, const uint16_t *d_depth, const uint8_t *d_bgr, int width, int height,
@@ -577,7 +603,7 @@ ff_status ff_add_map_u16_device(ff_handle *h, const uint16_t *d_depth, const uin
   CK(cudaSetDevice(h->cfg.device));
   ff_status st = ensure_image(h, width, height);
   if (st != FF_OK) return st;
-  return add_map_device(h, d_depth, d_bgr, width, height, K, R, t, scaling, maxcam, queued);
+  return add_map_device(h, d_depth, d_bgr, false, width, height, K, R, t, scaling, maxcam, queued);
 }
 
 ff_status ff_get_stats(ff_handle *h, ff_stats *o) {
