@@ -140,6 +140,55 @@ class MeshInterleaved:
     colors: np.ndarray    # (nv, 3) uint8 (r, g, b)
     faces: np.ndarray     # (nf, 3) uint32
 
+    def writePLY(self, filename: str, binary: bool = True) -> bool:
+        """Write `filename` + ".ply" byte for byte as the reference's
+        MeshInterleaved::writePLY (mesh_interleaved.cpp:137-198): a header
+        with float32 x/y/z, uchar red/green/blue (when there are colours) and
+        a uint8/int32 face list, then the vertices (position and colour
+        interleaved) and the faces; ascii numbers as C++ streams print them
+        (%g with 6 significant digits)."""
+        v = np.ascontiguousarray(self.vertices, np.float32).reshape(-1, 3)
+        c = np.ascontiguousarray(self.colors, np.uint8).reshape(-1, 3)
+        f = np.ascontiguousarray(self.faces, np.uint32).reshape(-1, 3)
+        head = ["ply", "format binary_little_endian 1.0" if binary else "format ascii 1.0",
+                f"element vertex {len(v)}", "property float32 x\nproperty float32 y\nproperty float32 z"]
+        if len(c):
+            head.append("property uchar red\nproperty uchar green\nproperty uchar blue")
+        if len(f):
+            head.append(f"element face {len(f)}")
+            head.append("property list uint8 int32 vertex_indices")
+        head.append("end_header")
+        try:
+            out = open(filename + ".ply", "wb")
+        except OSError:
+            return False
+        with out:
+            out.write("\n".join(head).encode())
+            if binary:
+                out.write(b"\n")
+                if len(c):
+                    rec = np.zeros(len(v), dtype=[("p", "<f4", 3), ("c", "u1", 3)])
+                    rec["c"] = c
+                else:
+                    rec = np.zeros(len(v), dtype=[("p", "<f4", 3)])
+                rec["p"] = v
+                out.write(rec.tobytes())
+                frec = np.zeros(len(f), dtype=[("n", "u1"), ("i", "<u4", 3)])
+                frec["n"] = 3
+                frec["i"] = f
+                out.write(frec.tobytes())
+            else:
+                lines = []
+                for k in range(len(v)):
+                    s = "\n%g %g %g" % (float(v[k, 0]), float(v[k, 1]), float(v[k, 2]))
+                    if len(c):
+                        s += " %d %d %d" % (c[k, 0], c[k, 1], c[k, 2])
+                    lines.append(s)
+                for k in range(len(f)):
+                    lines.append("\n3 %d %d %d" % (f[k, 0], f[k, 1], f[k, 2]))
+                out.write("".join(lines).encode())
+        return True
+
 
 class MeshBuffer:
     """Reusable page-locked host storage for getMeshInterleavedMarchingCubes(out=...).

@@ -43,6 +43,8 @@ def lib():
         L.ref_update_meshes.argtypes = [vp]
         L.ref_mesh_counts.argtypes = [vp, ctypes.POINTER(ll), ctypes.POINTER(ll)]
         L.ref_mesh_copy.argtypes = [vp, vp, vp, vp]
+        L.ref_write_ply.restype = i32
+        L.ref_write_ply.argtypes = [vp, ctypes.c_char_p, i32]
         L.ref_state.argtypes = [vp, vp, vp]
         L.ref_leaves.argtypes = [vp, ll, vp, vp, vp]
         L.ref_queue.argtypes = [vp, vp]
@@ -105,6 +107,10 @@ class RefFusion:
         faces = np.zeros((nf.value, 3), np.uint32)
         self.L.ref_mesh_copy(self.h, _p(xyz), _p(rgb), _p(faces))
         return xyz, rgb, faces
+
+    def write_ply(self, stem: str, binary: bool = True) -> bool:
+        """The reference's MeshInterleaved::writePLY of its current mesh (writes stem + ".ply")."""
+        return bool(self.L.ref_write_ply(self.h, stem.encode(), 1 if binary else 0))
 
     def state(self) -> dict:
         ints = np.zeros(16, np.int64)

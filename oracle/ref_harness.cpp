@@ -104,6 +104,13 @@ void ref_mesh_counts(void *h, long long *nv, long long *nf) {
   *nf = (long long)f->_meshCurrent->faces.size() / 3;
 }
 
+/* The reference's own PLY writer (MeshInterleaved::writePLY) on its current
+ * mesh; `stem` gets ".ply" appended by the writer. */
+int ref_write_ply(void *h, const char *stem, int binary) {
+  FusionMipMapCPU *f = (FusionMipMapCPU *)h;
+  return f->_meshCurrent->writePLY(std::string(stem), binary != 0) ? 1 : 0;
+}
+
 void ref_mesh_copy(void *h, float *xyz, uint8_t *rgb, uint32_t *faces) {
   FusionMipMapCPU *f = (FusionMipMapCPU *)h;
   const MeshInterleaved &m = *f->_meshCurrent;
