@@ -39,6 +39,7 @@ struct ffp_map {
   uint32_t nqueued;
   float *dist, *wgt;
   uint16_t *col; /* 3 per voxel: R, G, B (the reference's colortype3 x, y, z) */
+  double *dist64, *wgt64; /* update mode 3 (FP64 oracle) */
   int img_w, img_h;
   float *pxp, *pyp;
   int box_min[3], box_max[3];
@@ -112,6 +113,8 @@ void ffp_destroy(ffp_map *m) {
   free(m->dist);
   free(m->wgt);
   free(m->col);
+  free(m->dist64);
+  free(m->wgt64);
   free(m->pxp);
   free(m->pyp);
   free(m->cells);
@@ -122,7 +125,13 @@ void ffp_destroy(ffp_map *m) {
   free(m);
 }
 
-void ffp_set_update_mode(ffp_map *m, int mode) { m->rz_exact = mode; }
+void ffp_set_update_mode(ffp_map *m, int mode) {
+  m->rz_exact = mode;
+  if (mode == 3 && !m->dist64) {
+    m->dist64 = (double *)calloc((size_t)m->leaves_total * 512, sizeof(double));
+    m->wgt64 = (double *)calloc((size_t)m->leaves_total * 512, sizeof(double));
+  }
+}
 
 /* Float camera parameters, the reference's camPamsFloat (definitions.h:71-88),
  * built in double and rounded once to float. */
@@ -456,6 +465,65 @@ static void update_brick(ffp_map *m, const campams *q, const uint16_t *depth, co
   }
 }
 
+/* The same update in double precision (update mode 3): voxel positions from
+ * the double pose and the map offset, exact reciprocals, round-to-nearest;
+ * pixel selection and masks as in the reference (truncating conversion). */
+static int cvt_trunc64(double f) {
+  if (!(f > -2147483649.0 && f < 2147483648.0)) return (int)0x80000000;
+  return (int)f;
+}
+
+static void update_brick64(ffp_map *m, const double *r2, const double *t2, const double *K, const uint16_t *depth,
+                           double scaling, double maxcam, uint32_t brick) {
+  const int W = m->img_w, H = m->img_h;
+  const uint16_t *o = m->leaf_pos + 3 * brick;
+  const double ls = (double)m->leaf_scale[brick];
+  const double scale = (double)m->scale;
+  const double thr = (double)m->threshold;
+  const double thrD = thr * ls, thrW = (double)WEIGHT_FACTOR * thr * ls;
+  const double eps = (double)DIST_W_EPS;
+  size_t idx = (size_t)brick * 512;
+  for (int z = 0; z < 8; z++)
+    for (int y = 0; y < 8; y++)
+      for (int x = 0; x < 8; x++, idx++) {
+        const double g[3] = {(double)o[0] + x * ls, (double)o[1] + y * ls, (double)o[2] + z * ls};
+        double p[3];
+        for (int r = 0; r < 3; r++) {
+          double v = t2[r];
+          for (int c = 0; c < 3; c++) v += r2[r * 3 + c] * ((double)m->offset[c] + g[c] * scale);
+          p[r] = v;
+        }
+        const double len = sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+        const double rc = 1.0 / p[2];
+        const int imx = cvt_trunc64(K[2] + K[0] * (p[0] * rc));
+        const int imy = cvt_trunc64(K[3] + K[1] * (p[1] * rc));
+        int cy = imy < H - 1 ? imy : H - 1;
+        cy = cy > 0 ? cy : 0;
+        int cx = imx < W - 1 ? imx : W - 1;
+        cx = cx > 0 ? cx : 0;
+        const double h = scaling * (double)depth[W * cy + cx];
+        const double dInc = len - (len * rc) * h;
+        const int mask = p[2] > 0.0 && imy < H && imy > -1 && imx < W && imx > -1 && h < maxcam;
+        const double front = dInc < eps ? 1.0 : 0.0;
+        const double back = (dInc >= eps && dInc < thrW) ? 1.0 : 0.0;
+        const double fall = (thrW - dInc) / (thrW - eps);
+        const double wInc = mask ? front + fall * back : 0.0;
+        const double wAcc = m->wgt64[idx], dAcc = m->dist64[idx];
+        const double wNew = wAcc + wInc;
+        double tr = dInc < thrD ? dInc : thrD;
+        tr = tr > -thrD ? tr : -thrD;
+        const double add = mask ? tr * wInc : 0.0;
+        m->dist64[idx] = (dAcc * wAcc + add) / (wNew + (wNew <= 0.0 ? 1.0 : 0.0));
+        m->wgt64[idx] = wNew;
+      }
+}
+
+void ffp_bricks64(const ffp_map *m, int64_t n, double *dist, double *wgt) {
+  if (!m->dist64) return;
+  memcpy(dist, m->dist64, sizeof(double) * 512 * (size_t)n);
+  memcpy(wgt, m->wgt64, sizeof(double) * 512 * (size_t)n);
+}
+
 /* ---------------------------------------------------------------- addMap */
 
 int ffp_add_map(ffp_map *m, const uint16_t *depth, const uint8_t *bgr, int w, int h, const double *K,
@@ -491,9 +559,21 @@ int ffp_add_map(ffp_map *m, const uint16_t *depth, const uint8_t *bgr, int w, in
        m->box_max[1] >= m->n || m->box_max[2] >= m->n))
     grow(m);
   int saved = fegetround();
-  fesetround(m->rz_exact ? FE_TOWARDZERO : FE_TONEAREST);
-  g_rcp_mode = m->rz_exact == 2 ? 2 : 1;
-  for (uint32_t i = 0; i < m->nqueued; i++) update_brick(m, &q, depth, bgr, scaling, maxcam, m->queue[i]);
+  if (m->rz_exact == 3) {
+    /* FP64 oracle: the extrinsic inverse [R^T | -R^T t] in double */
+    double r2[9], t2[3];
+    for (int r = 0; r < 3; r++) {
+      for (int c = 0; c < 3; c++) r2[r * 3 + c] = R[c * 3 + r];
+      t2[r] = -(R[0 * 3 + r] * t[0] + R[1 * 3 + r] * t[1] + R[2 * 3 + r] * t[2]);
+    }
+    fesetround(FE_TONEAREST);
+    for (uint32_t i = 0; i < m->nqueued; i++)
+      update_brick64(m, r2, t2, K, depth, (double)scaling, (double)maxcam, m->queue[i]);
+  } else {
+    fesetround(m->rz_exact ? FE_TOWARDZERO : FE_TONEAREST);
+    g_rcp_mode = m->rz_exact == 2 ? 2 : 1;
+    for (uint32_t i = 0; i < m->nqueued; i++) update_brick(m, &q, depth, bgr, scaling, maxcam, m->queue[i]);
+  }
   fesetround(saved);
   if (m->branch_overflow || m->leaves_used > m->leaves_total) m->meshing_ok = 0;
   m->frames++;

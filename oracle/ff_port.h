@@ -22,7 +22,12 @@
  *   2 round-toward-zero with the host CPU's RCPPS -- the reference's own
  *     instruction, used only to check this restatement against the compiled
  *     reference on the same machine;
- *   0 round-to-nearest, exact reciprocal (rounding-sensitivity tests).
+ *   0 round-to-nearest, exact reciprocal (rounding-sensitivity tests);
+ *   3 the FP64 oracle: the same allocation, and the update's geometry and
+ *     running averages in double precision from the double pose (no float
+ *     camera parameters, exact reciprocals, round-to-nearest) into separate
+ *     double SDF/weight arrays (ffp_bricks64) -- the reference against which
+ *     the FP32 and FP16-storage results state their error.
  */
 #ifndef FF_PORT_H
 #define FF_PORT_H
@@ -54,6 +59,8 @@ void ffp_queue(const ffp_map *m, uint32_t *q);
 void ffp_tree(const ffp_map *m, uint32_t *tree);
 /* Brick contents of leaves [0, n): 512 SDF, 512 weights, 512 x 3 colour (R, G, B) each. */
 void ffp_bricks(const ffp_map *m, int64_t n, float *dist, float *wgt, uint16_t *col);
+/* FP64-oracle brick contents of leaves [0, n) (update mode 3 only). */
+void ffp_bricks64(const ffp_map *m, int64_t n, double *dist, double *wgt);
 /* Replace brick contents (used to start the update from a given state). */
 void ffp_set_bricks(ffp_map *m, int64_t n, const float *dist, const float *wgt, const uint16_t *col);
 

@@ -41,6 +41,7 @@ def lib():
         L.ffp_queue.argtypes = [vp, vp]
         L.ffp_tree.argtypes = [vp, vp]
         L.ffp_bricks.argtypes = [vp, i64, vp, vp, vp]
+        L.ffp_bricks64.argtypes = [vp, i64, vp, vp]
         L.ffp_set_bricks.argtypes = [vp, i64, vp, vp, vp]
         L.ffp_update_meshes.restype = i64
         L.ffp_update_meshes.argtypes = [vp]
@@ -125,6 +126,16 @@ class PortFusion:
         c = np.zeros((n, 512, 3), np.uint16)
         lib().ffp_bricks(self.h, n, _p(d), _p(w), _p(c))
         return d, w, c
+
+    def bricks64(self, n=None):
+        """SDF and weights of the FP64 oracle (update_mode=3)."""
+        st = self.state()
+        if n is None:
+            n = min(st["leaves_used"], st["leaves_total"])
+        d = np.zeros((n, 512), np.float64)
+        w = np.zeros((n, 512), np.float64)
+        lib().ffp_bricks64(self.h, n, _p(d), _p(w))
+        return d, w
 
     def set_bricks(self, d, w, c):
         d = np.ascontiguousarray(d, np.float32)

@@ -1,0 +1,84 @@
+"""FP32 and FP16-storage fusion against the FP64 oracle, and their surface
+error against the analytic scene.
+
+The FP64 oracle (oracle/ff_port.c, update mode 3) allocates exactly as the
+reference and runs the voxel update in double precision from the double
+pose.  Both GPU forms share that allocation, so their SDF/weight arrays are
+compared voxel by voxel wherever the oracle has weight:
+
+* FP32 (the reference's arithmetic): differences come from float pose
+  parameters and rounding; a few voxels whose ray lands on a different
+  pixel in float than in double differ by up to the truncation distance,
+  so the bound is on the 99th percentile and the RMS.
+* FP16 storage (SDF and weight stored as half, update in FP32): adds the
+  half-precision rounding of the stored values.
+
+Tolerances (metres): FP32 p99 <= 2e-6, RMS <= 3e-4; FP16 p99 <= 6e-5,
+RMS <= 3e-4; surface RMS of the FP16 mesh within 2 % (+1 um) of the FP32
+mesh's.  The measured figures are printed for the record.
+"""
+import numpy as np
+import pytest
+
+from tests.helpers import MAXCAM, SCALING
+
+pytestmark = pytest.mark.gpu
+
+N_FRAMES = 20
+
+
+def _walk_frames():
+    """The first frames of the 640x480 walk, rendered on the GPU."""
+    from fastfusion_b200 import scene
+    seq = scene.room_walk_sequence(0, n_frames=1000, width=640, height=480)
+    frames = []
+    for k in range(N_FRAMES):
+        R, t = seq.poses[k]
+        d, c = scene.render_torch(seq.scene, R, t, 640, 480, seq.K, seq.seed, k, device="cuda")
+        frames.append((d.cpu().numpy().view(np.uint16), c.cpu().numpy(), R, t))
+    return seq, frames
+
+
+def _err(d, d64, m):
+    e = np.abs(d[m].astype(np.float64) - d64[m])
+    return {"rms": float(np.sqrt(np.mean(e * e))), "p99": float(np.percentile(e, 99)), "max": float(e.max()),
+            "voxels": int(m.sum())}
+
+
+def test_fp32_and_fp16_against_fp64_oracle(lib_built, port_lib):
+    from fastfusion_b200.fusion import CameraInfo, FusionMipMapCPU
+    seq, frames = _walk_frames()
+    g32 = FusionMipMapCPU(0, 0, 0, 0.005, 0.01, 0, True, leaves_max=271420, branches_max=4793488, rcp="exact")
+    g16 = FusionMipMapCPU(0, 0, 0, 0.005, 0.01, 0, True, leaves_max=271420, branches_max=4793488, rcp="exact",
+                          storage="fp16")
+    p64 = port_lib.PortFusion(leaves_total=271420, branches_total=4793488, update_mode=3)
+    for depth, bgr, R, t in frames:
+        cam = CameraInfo(seq.K, R, t)
+        q32 = g32.addMap(depth, cam, bgr, SCALING, MAXCAM)
+        q16 = g16.addMap(depth, cam, bgr, SCALING, MAXCAM)
+        q64 = p64.add_map(depth, bgr, seq.K, R, t, SCALING, MAXCAM)
+        assert q32 == q16 == q64
+    d64, w64 = p64.bricks64()
+    d32, w32, _ = g32.bricks()
+    d16, w16, _ = g16.bricks()
+    assert d32.shape == d64.shape == d16.shape
+    m = w64 > 0
+    e32, e16 = _err(d32, d64, m), _err(d16, d64, m)
+    print("\nSDF error vs FP64 oracle, FP32:", e32, "\nSDF error vs FP64 oracle, FP16 storage:", e16)
+    assert e32["p99"] <= 2e-6 and e32["rms"] <= 3e-4
+    assert e16["p99"] <= 6e-5 and e16["rms"] <= 3e-4
+    # weights: identical where the pixel choice agrees (integers and ramps)
+    assert np.percentile(np.abs(w32[m] - w64[m]), 99) <= 1e-5
+    assert np.percentile(np.abs(w16[m] - w64[m]), 99) <= 1e-2
+
+    # surface error of the two meshes against the analytic scene
+    rms = {}
+    for name, g in (("fp32", g32), ("fp16", g16)):
+        g.updateMeshes()
+        v = g.getMeshInterleavedMarchingCubes().vertices
+        assert len(v) > 1000
+        rms[name] = float(np.sqrt(np.mean(seq.scene.sdf(v.astype(np.float64)) ** 2)))
+    print("surface RMS vs analytic SDF (m):", rms)
+    assert rms["fp16"] <= 1.02 * rms["fp32"] + 1e-6
+    g32.close()
+    g16.close()
