@@ -208,6 +208,28 @@ def read_traffic_table() -> dict:
     return out
 
 
+# -- ranks -----------------------------------------------------------------------
+def reduce_over_ranks(x: float, op: str, device=None) -> float:
+    """Max or sum of a per-rank scalar over the process group (the value
+    itself without one).  The timed region of a multi-GPU run is the max over
+    ranks; the work done is the sum."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def whole_job_rate(frames_this_rank: float, ms_this_rank: float, device=None):
+    """(frames/s of the whole job, slowest rank's ms): every rank's frames
+    over the max-over-ranks device time."""
+    frames = reduce_over_ranks(frames_this_rank, "sum", device)
+    ms = reduce_over_ranks(ms_this_rank, "max", device)
+    return frames / (ms / 1e3), ms
+
+
 # -- the B200 arm ------------------------------------------------------------------
 def run_b200(a):
     import torch
@@ -230,20 +252,6 @@ def run_b200(a):
     def barrier():
         if world > 1:
             dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
 
     nf = n_frames_needed(a)
     seq = make_sequence(a.seed + rank, nf)
@@ -346,8 +354,8 @@ def run_b200(a):
         e2e_ms, _ = timed(host_step, m, lambda mm: d2h.clear())
         m.close()
         del m
-        e2e_ms = max_over_ranks(e2e_ms)
-        e2e = {"value": sum_over_ranks(a.steps * FRAMES_PER_STEP) / (e2e_ms / 1e3), "unit": UNIT,
+        e2e_value, e2e_ms = whole_job_rate(a.steps * FRAMES_PER_STEP, e2e_ms, dev)
+        e2e = {"value": e2e_value, "unit": UNIT,
                "h2d_bytes_per_step": FRAMES_PER_STEP * (WIDTH * HEIGHT * 2 + WIDTH * HEIGHT * 3),
                "d2h_bytes_per_step": int(np.mean(d2h)) if d2h else 0,
                "ms_per_step": e2e_ms / a.steps}
@@ -359,9 +367,7 @@ def run_b200(a):
         mesh_buf.close()
     clocks = clk.stop() if clk else None
 
-    dev_ms_max = max_over_ranks(dev_ms)
-    frames_all = sum_over_ranks(a.steps * FRAMES_PER_STEP)
-    value = frames_all / (dev_ms_max / 1e3)
+    value, dev_ms_max = whole_job_rate(a.steps * FRAMES_PER_STEP, dev_ms, dev)
 
     # roofline of the dominant stage
     peak, peak_kind = measured_hbm_peak()
