@@ -13,9 +13,9 @@ compared voxel by voxel wherever the oracle has weight:
 * FP16 storage (SDF and weight stored as half, update in FP32): adds the
   half-precision rounding of the stored values.
 
-Tolerances (metres): FP32 p99 <= 2e-6, RMS <= 3e-4; FP16 p99 <= 6e-5,
-RMS <= 3e-4; surface RMS of the FP16 mesh within 2 % (+1 um) of the FP32
-mesh's.  The measured figures are printed for the record.
+Tolerances: SDF (metres) FP32 p99 <= 2e-6, RMS <= 3e-4; FP16 p99 <= 6e-5,
+RMS <= 3e-4; weight p99 FP32 <= 1e-3, FP16 <= 2e-2; surface RMS of the FP16
+mesh within 2 % (+1 um) of the FP32 mesh's.  The measured figures are printed for the record.
 """
 import numpy as np
 import pytest
@@ -67,9 +67,13 @@ def test_fp32_and_fp16_against_fp64_oracle(lib_built, port_lib):
     print("\nSDF error vs FP64 oracle, FP32:", e32, "\nSDF error vs FP64 oracle, FP16 storage:", e16)
     assert e32["p99"] <= 2e-6 and e32["rms"] <= 3e-4
     assert e16["p99"] <= 6e-5 and e16["rms"] <= 3e-4
-    # weights: identical where the pixel choice agrees (integers and ramps)
-    assert np.percentile(np.abs(w32[m] - w64[m]), 99) <= 1e-5
-    assert np.percentile(np.abs(w16[m] - w64[m]), 99) <= 1e-2
+    # weights: the fall-off ramp turns a distance error of ~1e-6 m into ~1e-4
+    # of weight (thrW is a few mm); half precision adds ~1e-3 relative
+    w_e32 = float(np.percentile(np.abs(w32[m] - w64[m]), 99))
+    w_e16 = float(np.percentile(np.abs(w16[m] - w64[m]), 99))
+    print("weight error p99 vs FP64 oracle: FP32", w_e32, "FP16 storage", w_e16)
+    assert w_e32 <= 1e-3
+    assert w_e16 <= 2e-2
 
     # surface error of the two meshes against the analytic scene
     rms = {}
