@@ -440,6 +440,25 @@ class FusionMipMapCPU:
                                          _p(parent), pos.shape[0], *ptrs))
 
 
+    # -- snapshot / resume (the reference's copyCPU2HDD / copyHDD2CPU,
+    # geometryfusion_mipmap_cpu.cpp:1135-1184, as one .npz file) ----------------
+    def save_snapshot(self, path: str):
+        """Write the whole map state (volume, octree, leaf table, bricks) to
+        `path` (.npz).  load_snapshot on any map of enough capacity resumes it:
+        further frames fuse exactly as they would have in this map."""
+        st = self.stats()
+        pos, scl, par = self.leaves()
+        d, w, c = self.bricks()
+        np.savez(path, n=np.uint32(st["n"]), offset=st["offset"], tree=self.tree(), pos=pos, scale=scl,
+                 parent=par, sdf=d, weight=w, rgb=c, meshing_ok=np.uint32(st["meshing_ok"]))
+
+    def load_snapshot(self, path: str):
+        """Replace this map's state by a snapshot written by save_snapshot."""
+        z = np.load(path)
+        self.set_state(int(z["n"]), z["offset"], z["tree"], z["pos"], z["scale"], z["parent"], z["sdf"],
+                       z["weight"], z["rgb"])
+
+
 def version() -> str:
     return load_library().ff_version().decode()
 

@@ -1,0 +1,42 @@
+"""Snapshot and resume: a map saved after some frames and loaded into a new
+map fuses the following frames bit for bit like the original, and meshes to
+the same mesh."""
+import numpy as np
+import pytest
+
+from tests.helpers import MAXCAM, SCALING, circle_frames
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("storage", ["fp32", "fp16"])
+def test_snapshot_resume_is_exact(lib_built, tmp_path, storage):
+    from fastfusion_b200.fusion import CameraInfo, FusionMipMapCPU
+    K, frames = circle_frames(0, 12, 160, 120)
+    kw = dict(leaves_max=271420, branches_max=4793488, rcp="exact", storage=storage)
+    a = FusionMipMapCPU(0, 0, 0, 0.005, 0.01, 0, True, **kw)
+    for depth, bgr, R, t in frames[:6]:
+        a.addMap(depth, CameraInfo(K, R, t), bgr, SCALING, MAXCAM)
+    path = str(tmp_path / "map.npz")
+    a.save_snapshot(path)
+    b = FusionMipMapCPU(0, 0, 0, 0.005, 0.01, 0, True, **kw)
+    b.load_snapshot(path)
+    for depth, bgr, R, t in frames[6:]:
+        qa = a.addMap(depth, CameraInfo(K, R, t), bgr, SCALING, MAXCAM)
+        qb = b.addMap(depth, CameraInfo(K, R, t), bgr, SCALING, MAXCAM)
+        assert qa == qb
+    sa, sb = a.stats(), b.stats()
+    assert sa["n"] == sb["n"] and np.array_equal(sa["offset"], sb["offset"])
+    assert np.array_equal(a.tree(), b.tree())
+    for x, y in zip(a.leaves(), b.leaves()):
+        assert np.array_equal(x, y)
+    for x, y in zip(a.bricks(), b.bricks()):
+        assert np.array_equal(x.view(np.uint8), y.view(np.uint8))
+    a.updateMeshes()
+    b.updateMeshes()
+    ma, mb = a.getMeshInterleavedMarchingCubes(), b.getMeshInterleavedMarchingCubes()
+    assert len(ma.faces) > 0
+    assert np.array_equal(ma.vertices.view(np.uint32), mb.vertices.view(np.uint32))
+    assert np.array_equal(ma.faces, mb.faces) and np.array_equal(ma.colors, mb.colors)
+    a.close()
+    b.close()
