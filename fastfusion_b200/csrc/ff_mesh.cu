@@ -27,6 +27,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstddef>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -794,13 +795,22 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
   return true;
 }
 
-// Per-warp shared scratch of one lattice cell.
+// Per-warp shared scratch of one lattice cell.  Only the zero test of a
+// sample's weight is needed after sampling; vidx is used by the emit pass
+// alone, so the count pass's scratch stops before it (more warps per SM).
 struct WarpScratch {
-  Sample s[512];
-  uint8_t cube_case[512];
-  uint8_t edge_set[512 * 3];
-  uint16_t vidx[512 * 3];
+  float sd[512];           // SDF of each lattice sample
+  uint16_t sc[512 * 3];    // colour (R, G, B) of each sample
+  uint8_t wzero[512];      // the sample's weight is zero
+  uint8_t cube_case[512];  // marching-cubes case of each cube
+  uint32_t edge_bits[48];  // lattice-edge slots (3 per voxel) that carry a vertex
+  uint16_t vidx[512 * 3];  // emit pass: the vertex number of each such slot
 };
+constexpr size_t SCRATCH_COUNT_BYTES = offsetof(WarpScratch, vidx);
+constexpr size_t SCRATCH_EMIT_BYTES = sizeof(WarpScratch);
+static_assert(SCRATCH_COUNT_BYTES % 16 == 0 && SCRATCH_EMIT_BYTES % 16 == 0, "scratch alignment");
+
+__device__ __forceinline__ int edge_bit(const WarpScratch &W, int slot) { return (W.edge_bits[slot >> 5] >> (slot & 31)) & 1; }
 
 constexpr int MESH_WARPS = 4;
 
@@ -847,7 +857,8 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ McTab T;
   load_mc(T);
-  WarpScratch &W = reinterpret_cast<WarpScratch *>(smem_raw)[threadIdx.x >> 5];
+  WarpScratch &W = *reinterpret_cast<WarpScratch *>(smem_raw + (size_t)(threadIdx.x >> 5) *
+                                                                      (EMIT ? SCRATCH_EMIT_BYTES : SCRATCH_COUNT_BYTES));
   const int lane = threadIdx.x & 31;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
@@ -868,9 +879,14 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
       const int bx = k % n3[0], by = (k / n3[0]) % n3[1], bz = k / (n3[0] * n3[1]);
       Sample s;
       fit &= lattice_sample(m, c, G, bx, by, bz, s);
-      W.s[(bz * 8 + by) * 8 + bx] = s;
+      const int si = (bz * 8 + by) * 8 + bx;
+      W.sd[si] = s.d;
+      W.sc[3 * si] = s.c[0];
+      W.sc[3 * si + 1] = s.c[1];
+      W.sc[3 * si + 2] = s.c[2];
+      W.wzero[si] = s.w == 0.0f;
     }
-    for (int k = lane; k < 512 * 3 / 4; k += 32) reinterpret_cast<uint32_t *>(W.edge_set)[k] = 0;
+    for (int k = lane; k < 48; k += 32) W.edge_bits[k] = 0;
     fit = __all_sync(0xffffffffu, fit);
     __syncwarp();
     if (!EMIT && lane == 0) atomicAdd(m.samples, (unsigned long long)nsamp);
@@ -888,14 +904,16 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
       int ci8 = 0;
 #pragma unroll
       for (int q = 0; q < 8; q++) {
-        const Sample &sq = W.s[idx + off[q]];
-        zero |= sq.w == 0.0f;
-        if (sq.d < 0.0f) ci8 |= 1 << q;
+        zero |= W.wzero[idx + off[q]] != 0;
+        if (W.sd[idx + off[q]] < 0.0f) ci8 |= 1 << q;
       }
       if (zero) ci8 = 0;
       W.cube_case[idx] = (uint8_t)ci8;
       const int nt = mc_ntri(T, ci8);
-      for (int q = 0; q < 3 * nt; q++) W.edge_set[3 * idx + mc_slot(T, mc_edge(T, ci8, q))] = 1;
+      for (int q = 0; q < 3 * nt; q++) {
+        const int slot = 3 * idx + mc_slot(T, mc_edge(T, ci8, q));
+        atomicOr(&W.edge_bits[slot >> 5], 1u << (slot & 31));
+      }
     }
     __syncwarp();
     // vertices, in the reference's loop order of this cell type
@@ -906,7 +924,7 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
       int b0 = 0, b1 = 0, b2 = 0, idx = 0, cntv = 0;
       if (k < nsamp) {
         idx = lattice_idx(G, k, n3, b0, b1, b2);
-        cntv = W.edge_set[3 * idx] + W.edge_set[3 * idx + 1] + W.edge_set[3 * idx + 2];
+        cntv = edge_bit(W, 3 * idx) + edge_bit(W, 3 * idx + 1) + edge_bit(W, 3 * idx + 2);
       }
       int tot;
       int ex = warp_excl_scan(cntv, lane, tot);
@@ -918,16 +936,16 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
           P0[r] = __fadd_rn(m.offset[r], __fmul_rn((float)sample_pos(G, r, bb[r]), m.scale));
         uint32_t local = vrun + (uint32_t)ex;
         for (int a = 0; a < 3; a++) {
-          if (!W.edge_set[3 * idx + a]) continue;
+          if (!edge_bit(W, 3 * idx + a)) continue;
           const int step = a == 0 ? 1 : (a == 1 ? 8 : 64);
           float P1[3] = {P0[0], P0[1], P0[2]};
           const int q2 = sample_pos(G, a, bb[a]) + (c_role[G.type][a] ? G.stretch : G.sizeMin);
           P1[a] = __fadd_rn(m.offset[a], __fmul_rn((float)q2, m.scale));
           float v[3];
           uint16_t col[3];
-          const Sample &s0 = W.s[idx], &s1 = W.s[idx + step];
-          vinterp(P0, P1, (double)s0.d, (double)s1.d, v);
-          cinterp(s0.c, s1.c, s0.d, s1.d, col);
+          const float d0 = W.sd[idx], d1 = W.sd[idx + step];
+          vinterp(P0, P1, (double)d0, (double)d1, v);
+          cinterp(&W.sc[3 * idx], &W.sc[3 * (idx + step)], d0, d1, col);
           const uint64_t gi = vb + local;
           xyz[3 * gi] = v[0];
           xyz[3 * gi + 1] = v[1];
@@ -1442,14 +1460,14 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
       MCK(cudaMemsetAsync(I.dirty, 1, ncells, s));
     }
   }
-  const size_t smem = sizeof(WarpScratch) * MESH_WARPS;
+  const size_t smem_count = SCRATCH_COUNT_BYTES * MESH_WARPS, smem_emit = SCRATCH_EMIT_BYTES * MESH_WARPS;
   static std::atomic<unsigned long long> attr_devices{0};
   int dev = 0;
   MCK(cudaGetDevice(&dev));
   const unsigned long long dbit = 1ull << (dev & 63);
   if (!(attr_devices.load() & dbit)) {
-    MCK(cudaFuncSetAttribute(k_mesh_lattice<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    MCK(cudaFuncSetAttribute(k_mesh_lattice<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    MCK(cudaFuncSetAttribute(k_mesh_lattice<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_count));
+    MCK(cudaFuncSetAttribute(k_mesh_lattice<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_emit));
     attr_devices.fetch_or(dbit);
   }
   const uint32_t *lat_list = incremental ? I.dlist : nullptr;
@@ -1458,7 +1476,7 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   const int lat_blocks = std::max(1, std::min<int>(148 * 8, (int)((first_corner + MESH_WARPS - 1) / MESH_WARPS)));
   note_launch((first_corner ? 1 : 0) + (ncells > first_corner ? 1 : 0) + (ncells ? 1 : 0));
   if (first_corner)
-    k_mesh_lattice<false><<<lat_blocks, 32 * MESH_WARPS, smem, s>>>(vs, I.cells, 0, first_corner, lat_list,
+    k_mesh_lattice<false><<<lat_blocks, 32 * MESH_WARPS, smem_count, s>>>(vs, I.cells, 0, first_corner, lat_list,
                                                                     I.d_count + 14, I.out, nullptr, nullptr, nullptr,
                                                                     nullptr, nullptr);
   if (ncells > first_corner)
@@ -1510,7 +1528,7 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   pi = P.begin(ST_MESH_EMIT, s);
   note_launch((first_corner ? 1 : 0) + (ncells > first_corner ? 1 : 0) + (incremental && ncells ? 1 : 0));
   if (first_corner)
-    k_mesh_lattice<true><<<lat_blocks, 32 * MESH_WARPS, smem, s>>>(vs, I.cells, 0, first_corner, lat_list,
+    k_mesh_lattice<true><<<lat_blocks, 32 * MESH_WARPS, smem_emit, s>>>(vs, I.cells, 0, first_corner, lat_list,
                                                                    I.d_count + 14, I.out, I.vbase, I.fbase, M.d_xyz,
                                                                    M.d_rgb, M.d_faces);
   if (ncells > first_corner)
