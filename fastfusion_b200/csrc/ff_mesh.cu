@@ -798,19 +798,20 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
 // Per-warp shared scratch of one lattice cell.  Only the zero test of a
 // sample's weight is needed after sampling; vidx is used by the emit pass
 // alone, so the count pass's scratch stops before it (more warps per SM).
+// Edge flags are bytes: plain stores, where bits would need atomics.
 struct WarpScratch {
   float sd[512];           // SDF of each lattice sample
   uint16_t sc[512 * 3];    // colour (R, G, B) of each sample
   uint8_t wzero[512];      // the sample's weight is zero
   uint8_t cube_case[512];  // marching-cubes case of each cube
-  uint32_t edge_bits[48];  // lattice-edge slots (3 per voxel) that carry a vertex
+  uint8_t edge_set[512 * 3];  // lattice-edge slots (3 per voxel) that carry a vertex
   uint16_t vidx[512 * 3];  // emit pass: the vertex number of each such slot
 };
 constexpr size_t SCRATCH_COUNT_BYTES = offsetof(WarpScratch, vidx);
 constexpr size_t SCRATCH_EMIT_BYTES = sizeof(WarpScratch);
 static_assert(SCRATCH_COUNT_BYTES % 16 == 0 && SCRATCH_EMIT_BYTES % 16 == 0, "scratch alignment");
 
-__device__ __forceinline__ int edge_bit(const WarpScratch &W, int slot) { return (W.edge_bits[slot >> 5] >> (slot & 31)) & 1; }
+__device__ __forceinline__ int edge_bit(const WarpScratch &W, int slot) { return W.edge_set[slot]; }
 
 constexpr int MESH_WARPS = 4;
 
@@ -886,7 +887,7 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
       W.sc[3 * si + 2] = s.c[2];
       W.wzero[si] = s.w == 0.0f;
     }
-    for (int k = lane; k < 48; k += 32) W.edge_bits[k] = 0;
+    for (int k = lane; k < 384; k += 32) reinterpret_cast<uint32_t *>(W.edge_set)[k] = 0;
     fit = __all_sync(0xffffffffu, fit);
     __syncwarp();
     if (!EMIT && lane == 0) atomicAdd(m.samples, (unsigned long long)nsamp);
@@ -912,7 +913,7 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
       const int nt = mc_ntri(T, ci8);
       for (int q = 0; q < 3 * nt; q++) {
         const int slot = 3 * idx + mc_slot(T, mc_edge(T, ci8, q));
-        atomicOr(&W.edge_bits[slot >> 5], 1u << (slot & 31));
+        W.edge_set[slot] = 1;  // lanes that set the same slot store the same byte
       }
     }
     __syncwarp();
