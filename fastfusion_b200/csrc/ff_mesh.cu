@@ -170,6 +170,19 @@ __device__ __forceinline__ uint32_t claim(uint32_t *ctr) {
   return base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
 }
 
+// n slots per lane; n must be the same for every lane that reaches the call
+// together (a constant at the call site).
+__device__ __forceinline__ uint32_t claim_n(uint32_t *ctr, uint32_t n) {
+  const unsigned mask = __activemask();
+  const unsigned peers = __match_any_sync(mask, (unsigned long long)(uintptr_t)ctr);
+  const int leader = __ffs(peers) - 1;
+  const unsigned lane = threadIdx.x & 31;
+  uint32_t base = 0;
+  if ((int)lane == leader) base = atomicAdd(ctr, (uint32_t)__popc(peers) * n);
+  base = __shfl_sync(peers, base, leader);
+  return base + (uint32_t)__popc(peers & ((1u << lane) - 1u)) * n;
+}
+
 __device__ void emit_cell(const GenQueues &Q, int type, int quirk, const int *o, int size, const uint32_t *L, int nl) {
   for (int k = 0; k < nl; k++)
     if (L[k] >= BRANCHINIT) return;  // a side without a leaf is never meshed
@@ -199,6 +212,16 @@ __device__ __forceinline__ void push(T *q, uint32_t *count, uint32_t cap, const 
   q[i] = v;
 }
 
+// Store at a slot claimed before (claim_n), unless past the queue's end.
+template <typename T>
+__device__ __forceinline__ void put(T *q, uint32_t i, uint32_t cap, const T &v, uint32_t *error) {
+  if (i >= cap) {
+    atomicOr(error, ERR_CELL_OVERFLOW);
+    return;
+  }
+  q[i] = v;
+}
+
 // Every item is a pure function of its slots, so an item found while
 // expanding another is queued for the next launch rather than expanded by the
 // same thread: each thread does a bounded amount of work (a few independent
@@ -214,23 +237,24 @@ struct Out {
 __device__ __forceinline__ void push_cell(const GenQueues &Q, const Out &O, const Slot &s) {
   push(O.cellq, O.count + 0, Q.cap_cell, s, Q.error);
 }
-__device__ __forceinline__ void push_face(const GenQueues &Q, const Out &O, const Slot &a, const Slot &b, int ax) {
-  FaceItem f;
-  f.a = a;
-  f.b = b;
-  f.axis = ax;
-  push(O.faceq, O.count + 1, Q.cap_face, f, Q.error);
-}
-__device__ __forceinline__ void push_edge(const GenQueues &Q, const Out &O, const Slot *S4, int e) {
-  EdgeItem it;
-  it.axis = e;
-  for (int j = 0; j < 4; j++) it.s[j] = S4[j];
-  push(O.edgeq, O.count + 2, Q.cap_edge, it, Q.error);
-}
 __device__ __forceinline__ void push_vert(const GenQueues &Q, const Out &O, const Slot *S8) {
   VertItem v;
   for (int j = 0; j < 8; j++) v.s[j] = S8[j];
   push(O.vertq, O.count + 3, Q.cap_vert, v, Q.error);
+}
+__device__ __forceinline__ void put_face(const GenQueues &Q, const Out &O, uint32_t i, const Slot &a, const Slot &b,
+                                         int ax) {
+  FaceItem f;
+  f.a = a;
+  f.b = b;
+  f.axis = ax;
+  put(O.faceq, i, Q.cap_face, f, Q.error);
+}
+__device__ __forceinline__ void put_edge(const GenQueues &Q, const Out &O, uint32_t i, const Slot *S4, int e) {
+  EdgeItem it;
+  it.axis = e;
+  for (int j = 0; j < 4; j++) it.s[j] = S4[j];
+  put(O.edgeq, i, Q.cap_edge, it, Q.error);
 }
 
 // The item functions are templated on their axis and fully unrolled, so every
@@ -289,6 +313,7 @@ __device__ __forceinline__ void edge_item(const GenCtx &g, const GenQueues &Q, c
     emit_cell(Q, 4 + E, 0, o, size, L, 4);
     return;
   }
+  const uint32_t eb = claim_n(O.count + 2, 2);
 #pragma unroll
   for (int half = 0; half < 2; half++) {
     Slot H[4];
@@ -297,7 +322,7 @@ __device__ __forceinline__ void edge_item(const GenCtx &g, const GenQueues &Q, c
       const int k = ((j & 1) ? 0 : (1 << P)) | (((j >> 1) & 1) ? 0 : (1 << Qx)) | (half ? (1 << E) : 0);
       H[j] = ch(g, S4[j], k);
     }
-    push_edge(Q, O, H, E);
+    put_edge(Q, O, eb + half, H, E);
   }
   Slot S8[8];
 #pragma unroll
@@ -334,11 +359,13 @@ __device__ __forceinline__ void face_item(const GenCtx &g, const GenQueues &Q, c
     a[k] = ch(g, A, k | bit);
     b[k] = ch(g, B, k);
   }
+  const uint32_t fb = claim_n(O.count + 1, 4);
 #pragma unroll
   for (int qd = 0; qd < 4; qd++) {
     const int k = ((qd & 1) ? (1 << U) : 0) | ((qd & 2) ? (1 << V) : 0);
-    push_face(Q, O, a[k], b[k], AX);
+    put_face(Q, O, fb + qd, a[k], b[k], AX);
   }
+  const uint32_t eb = claim_n(O.count + 2, 4);
 #pragma unroll
   for (int t = 0; t < 2; t++) {
     const int e = t == 0 ? U : V;
@@ -355,7 +382,7 @@ __device__ __forceinline__ void face_item(const GenCtx &g, const GenQueues &Q, c
         const int k = (half ? (1 << e) : 0) | (side[other] ? (1 << other) : 0);
         S4[j] = side[AX] ? b[k] : a[k];
       }
-      push_edge(Q, O, S4, e);
+      put_edge(Q, O, eb + 2 * t + half, S4, e);
     }
   }
   Slot S8[8];
@@ -381,24 +408,26 @@ __device__ __forceinline__ void cell_item(const GenCtx &g, const GenQueues &Q, c
   }
   constexpr int F[3][4][2] = {{{0, 1}, {2, 3}, {4, 5}, {6, 7}}, {{0, 2}, {1, 3}, {4, 6}, {5, 7}},
                               {{0, 4}, {1, 5}, {2, 6}, {3, 7}}};
+  const uint32_t fb = claim_n(O.count + 1, 12);
 #pragma unroll
   for (int ax = 0; ax < 3; ax++)
 #pragma unroll
-    for (int i = 0; i < 4; i++) push_face(Q, O, C[F[ax][i][0]], C[F[ax][i][1]], ax);
+    for (int i = 0; i < 4; i++) put_face(Q, O, fb + 4 * ax + i, C[F[ax][i][0]], C[F[ax][i][1]], ax);
+  const uint32_t eb = claim_n(O.count + 2, 6);
 #pragma unroll
   for (int x = 0; x < 2; x++) {
     Slot S4[4] = {C[x], C[x | 2], C[x | 4], C[x | 6]};
-    push_edge(Q, O, S4, 0);
+    put_edge(Q, O, eb + x, S4, 0);
   }
 #pragma unroll
   for (int y = 0; y < 4; y += 2) {
     Slot S4[4] = {C[y], C[y | 1], C[y | 4], C[y | 5]};
-    push_edge(Q, O, S4, 1);
+    put_edge(Q, O, eb + 2 + y / 2, S4, 1);
   }
 #pragma unroll
   for (int z = 0; z < 8; z += 4) {
     Slot S4[4] = {C[z], C[z | 1], C[z | 2], C[z | 3]};
-    push_edge(Q, O, S4, 2);
+    put_edge(Q, O, eb + 4 + z / 4, S4, 2);
   }
   push_vert(Q, O, C);
 }
