@@ -41,6 +41,7 @@ enum : uint32_t {
   ERR_CELL_OVERFLOW = 8u,
   ERR_MESH_OVERFLOW = 16u,
   ERR_DEDUPE_NOT_CONVERGED = 32u,
+  ERR_CELL_KEY = 64u,  // a mesh cell's origin does not fit its sort key
 };
 
 // Per-map counters kept in device memory; read back once per frame.

@@ -127,7 +127,7 @@ struct GenQueues {
 constexpr int LEVEL_COUNTS = 32;
 constexpr int MAX_GEN_LEVELS = 48;
 constexpr int COUNT_WORDS = LEVEL_COUNTS + 4 * (MAX_GEN_LEVELS + 1) + 28;
-constexpr int HOST_TOTALS = COUNT_WORDS - 8;  // host mirror only: 3 uint64 + 1 uint32 read back per update
+constexpr int HOST_TOTALS = COUNT_WORDS - 8;  // host mirror only: 3 uint64 + 2 uint32 read back per update
 
 struct GenCtx {
   const uint32_t *tree;
@@ -482,17 +482,23 @@ __global__ void __launch_bounds__(128) k_gen_level(GenCtx g, GenQueues Q, int lv
   gen_level(g, Q, lv, n);
 }
 
-__device__ __forceinline__ uint64_t cell_key(const Cell &c) {
+// Sort key of a cell: (type, log2 size, origin x, y, z), the order of the
+// mesh; B bits per origin coordinate (origins lie inside the volume, below
+// 2^B), so the radix sort runs over 3B + 7 bits only.
+__device__ __forceinline__ uint64_t cell_key(const Cell &c, int B) {
   int lsz = 0;
   while ((1 << lsz) < c.size) lsz++;
-  return ((uint64_t)c.type << 54) | ((uint64_t)c.quirk << 53) | ((uint64_t)lsz << 48) | ((uint64_t)c.o[0] << 32) |
-         ((uint64_t)c.o[1] << 16) | (uint64_t)c.o[2];
+  return ((uint64_t)c.type << (3 * B + 4)) | ((uint64_t)lsz << (3 * B)) | ((uint64_t)c.o[0] << (2 * B)) |
+         ((uint64_t)c.o[1] << B) | (uint64_t)c.o[2];
 }
 
-__global__ void k_cell_keys(const Cell *cells, uint32_t n, uint64_t *keys, uint32_t *vals) {
+__global__ void k_cell_keys(const Cell *cells, uint32_t n, int B, uint64_t *keys, uint32_t *vals, uint32_t *error) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  keys[i] = cell_key(cells[i]);
+  const Cell c = cells[i];
+  const uint32_t lim = 1u << B;
+  if (c.o[0] >= lim || c.o[1] >= lim || c.o[2] >= lim) atomicOr(error, ERR_CELL_KEY);
+  keys[i] = cell_key(c, B);
   vals[i] = i;
 }
 
@@ -1125,11 +1131,11 @@ __global__ void k_mesh_corner(VoxSrc m, const Cell *__restrict__ cells, uint32_t
 __global__ void k_mark_dirty(const Cell *cells, uint32_t n, const Cell *old_cells, uint32_t n_old,
                              const uint64_t *old_keys, const uint32_t *stamp, const uint32_t *parent,
                              uint32_t leaves_used, uint32_t since, uint8_t *dirty, int32_t *old_index,
-                             uint32_t *n_dirty, uint32_t first_corner, uint32_t *list, uint32_t *n_list) {
+                             uint32_t *n_dirty, uint32_t first_corner, uint32_t *list, uint32_t *n_list, int B) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Cell c = cells[i];
-  const uint64_t key = cell_key(c);
+  const uint64_t key = cell_key(c, B);
   int32_t found = -1;
   uint32_t lo = 0, hi = n_old;
   while (lo < hi) {
@@ -1263,6 +1269,7 @@ struct MeshImpl {
   size_t cap_cellq[2] = {0, 0}, cap_faceq[2] = {0, 0}, cap_edgeq[2] = {0, 0}, cap_vertq[2] = {0, 0};
   uint32_t n_corners = 0;
   size_t peak[5] = {0, 0, 0, 0, 0};  // last update's largest level of each queue, and its cell count
+  int key_bits = 0;                   // bits per origin coordinate of old_keys / keys
   // words 8 n_cells, 9 error, 10 n_dirty, 11 n_corners, 12-13 samples;
   // from LEVEL_COUNTS: 4 item counters per generation level
   uint32_t *d_count = nullptr;
@@ -1315,7 +1322,15 @@ static MeshImpl &impl(MeshState &m) {
   } while (0)
 
 // Generate, sort and store the mesh cells of the current octree.
+// Bits per origin coordinate in the cell keys of a volume of side n.
+static int key_bits_for(uint32_t n) {
+  int b = 1;
+  while ((1u << b) < n) b++;
+  return std::min(b + 1, 16);
+}
+
 static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uint32_t &ncells, std::string &err) {
+  const int key_bits = key_bits_for(in.n);
   // queue sizes: a first guess from the octree size, then the previous
   // update's peaks with headroom (the map grows slowly between updates)
   const uint32_t slots = std::max<uint32_t>(in.branches_used / 2, 64);
@@ -1401,10 +1416,11 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
   MCK(grow_buf(I.cells, I.cap_cells, ncells, s));
   if (ncells) {
     note_launch(2);
-    k_cell_keys<<<(ncells + 255) / 256, 256, 0, s>>>(I.raw, ncells, I.keys, I.vals);
+    k_cell_keys<<<(ncells + 255) / 256, 256, 0, s>>>(I.raw, ncells, key_bits, I.keys, I.vals, I.d_count + 9);
+    const int end_bit = 3 * key_bits + 7;
     size_t bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, bytes, I.keys, I.keys_sorted, I.vals, I.vals_sorted, (int)ncells, 0, 57,
-                                    s);
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, I.keys, I.keys_sorted, I.vals, I.vals_sorted, (int)ncells, 0,
+                                    end_bit, s);
     if (bytes > I.sort_tmp_bytes) {
       if (I.sort_tmp) MCK(cudaFreeAsync(I.sort_tmp, s));
       I.sort_tmp = nullptr;
@@ -1413,7 +1429,7 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
     }
     note_lib_call();
     MCK(cub::DeviceRadixSort::SortPairs(I.sort_tmp, I.sort_tmp_bytes, I.keys, I.keys_sorted, I.vals, I.vals_sorted,
-                                        (int)ncells, 0, 57, s));
+                                        (int)ncells, 0, end_bit, s));
     k_gather_cells<<<(ncells + 255) / 256, 256, 0, s>>>(I.raw, I.vals_sorted, ncells, I.cells);
   }
   return 0;
@@ -1472,7 +1488,9 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   MCK(grow_buf(I.vbase, I.cap_vb, ncells + 1, s));
   MCK(grow_buf(I.fbase, I.cap_fb, ncells + 1, s));
   MCK(grow_buf(I.dlist, I.cap_dlist, ncells, s));
-  const bool incremental = M.valid && I.n_old > 0;
+  // the previous update's keys are comparable only with the same key layout
+  const int kb = key_bits_for(in.n);
+  const bool incremental = M.valid && I.n_old > 0 && I.key_bits == kb;
   // the sorted cell list holds interiors, walls, edges, then corners (type is
   // the key's top field)
   const uint32_t first_corner = ncells - std::min(I.n_corners, ncells);
@@ -1484,7 +1502,8 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
       note_launch(2);
       k_mark_dirty<<<(ncells + 255) / 256, 256, 0, s>>>(I.cells, ncells, I.old_cells, I.n_old, I.old_keys, in.stamp,
                                                         in.parent, in.leaves_used, I.since, I.dirty, I.old_index,
-                                                        I.d_count + 10, first_corner, I.dlist, I.d_count + 14);
+                                                        I.d_count + 10, first_corner, I.dlist, I.d_count + 14,
+                                                        kb);
       k_fill_counts_from_old<<<(ncells + 255) / 256, 256, 0, s>>>(I.dirty, I.old_index, ncells, I.old_out, I.out);
     } else {
       MCK(cudaMemsetAsync(I.dirty, 1, ncells, s));
@@ -1538,7 +1557,13 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   MCK(cudaMemcpyAsync(h_tot + 1, I.fbase + ncells, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
   MCK(cudaMemcpyAsync(h_tot + 2, I.d_count + 12, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
   MCK(cudaMemcpyAsync(I.h_count + HOST_TOTALS + 6, I.d_count + 10, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  MCK(cudaMemcpyAsync(I.h_count + HOST_TOTALS + 7, I.d_count + 9, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   MCK(cudaStreamSynchronize(s));
+  if (I.h_count[HOST_TOTALS + 7] & ERR_CELL_KEY) {
+    mesh_invalidate(M);
+    err = "meshing: a mesh cell lies outside the volume";
+    return 6;
+  }
   const uint64_t tot[2] = {h_tot[0], h_tot[1]};
   const unsigned long long nsamples = h_tot[2];
   const uint32_t ndirty = incremental ? I.h_count[HOST_TOTALS + 6] : ncells;
@@ -1585,6 +1610,7 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   std::swap(I.fbase, I.old_fbase);
   std::swap(I.cap_fb, I.cap_ofb);
   I.n_old = ncells;
+  I.key_bits = kb;
   I.since = in.frame;
   MCK(cudaStreamSynchronize(s));
   M.n_vertices = tot[0];
