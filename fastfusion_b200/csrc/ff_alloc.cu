@@ -130,14 +130,29 @@ __device__ __forceinline__ bool same3(int a0, int a1, int a2, int b0, int b1, in
 // int4 (written once, before the first barrier), then processed bits of the
 // right column and of the bottom row, [2 rounds][ntiles] uint32 each.
 // bar: [0] arrivals, [1] generation, [4..6] per-round change counters (rotating)
-__global__ void __launch_bounds__(32 * DD_WARPS)
-    k_dedupe(const uint16_t *__restrict__ depth, const float *__restrict__ pxp, const float *__restrict__ pyp, CamF cam,
-             float scaling, float maxcam, int4 *vox, int W, int H, int tilesX, int tilesY, int4 *bnd,
-             uint8_t *processed, Counters *cnt, uint32_t *bar) {
+// One launch for all frames of a batch: warps are dealt out over the maps'
+// tiles in order; the rounds and their barrier are shared (a map whose tiles
+// have settled recomputes the same bits until every map has).
+__global__ void __launch_bounds__(32 * DD_WARPS) k_dedupe(const BatchDesc *__restrict__ bd, uint32_t *bar) {
   const int lane = threadIdx.x & 31;
-  const int tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t gtile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nmaps = bd->n;
+  int m = 0;
+  while (m < nmaps - 1 && gtile >= bd->tile_end[m]) m++;
+  const MapFrame &F = bd->f[m];
+  const int tile = (int)(gtile - (m ? bd->tile_end[m - 1] : 0u));
+  const bool active = gtile < bd->tile_end[nmaps - 1];  // warps past the last tile only join the barriers
+  const uint16_t *__restrict__ depth = F.depth;
+  const float *__restrict__ pxp = F.pxp;
+  const float *__restrict__ pyp = F.pyp;
+  const CamF cam = F.p;
+  const float scaling = F.scaling, maxcam = F.maxcam;
+  int4 *vox = F.vox;
+  const int W = F.W, H = F.H, tilesX = F.tilesX, tilesY = F.tilesY;
+  int4 *bnd = F.bnd;
+  uint8_t *processed = F.proc;
+  Counters *cnt = F.cnt;
   const int ntiles = tilesX * tilesY;
-  const bool active = tile < ntiles;  // warps past the last tile only join the barriers
   int4 *keyR = bnd, *keyB = bnd + (size_t)ntiles * 32;
   uint32_t *pR = reinterpret_cast<uint32_t *>(bnd + (size_t)2 * ntiles * 32);
   uint32_t *pB = pR + 2 * (size_t)ntiles;
@@ -186,7 +201,7 @@ __global__ void __launch_bounds__(32 * DD_WARPS)
   uint32_t eq_left = 0;  // row bits: lane 0's key equals the left tile's right column
   bool eq_above = false;  // this lane's row-0 key equals the above tile's bottom row
   uint32_t bits = 0, last_r = 0, last_b = 0;
-  const int max_rounds = tilesX + tilesY + 1;
+  const int max_rounds = bd->max_rounds;
   volatile uint32_t *chg = bar + 4;
   int round = 0;
   bool converged = false;
@@ -238,20 +253,23 @@ __global__ void __launch_bounds__(32 * DD_WARPS)
     if (changed && lane == 0) atomicAdd((uint32_t *)&chg[round % 3], 1u);
     // counter (round + 1) % 3 was last read before the previous barrier
     if (blockIdx.x == 0 && threadIdx.x == 0) chg[(round + 1) % 3] = 0;
-    grid_barrier(bar, gridDim.x, cnt);
+    // a barrier that gives up marks the first map; every map's frame reports it
+    grid_barrier(bar, gridDim.x, bd->f[0].cnt);
     const uint32_t any = chg[round % 3];
     if (!any) {
       converged = true;
       break;
     }
-    if (*(volatile uint32_t *)&cnt->error & ERR_SPIN_TIMEOUT) break;
+    if (*(volatile uint32_t *)&bd->f[0].cnt->error & ERR_SPIN_TIMEOUT) break;
   }
   if (active && x < W) {
     for (int r = 0; r < rows; r++) processed[(size_t)(ty * DD_ROWS + r) * W + x] = (uint8_t)((bits >> r) & 1u);
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    cnt->dedupe_iters = round + 1;
-    if (!converged) atomicOr(&cnt->error, ERR_DEDUPE_NOT_CONVERGED);
+  if (blockIdx.x == 0 && threadIdx.x < nmaps) {
+    Counters *c = bd->f[threadIdx.x].cnt;
+    c->dedupe_iters = round + 1;
+    if (!converged) atomicOr(&c->error, ERR_DEDUPE_NOT_CONVERGED);
+    if (*(volatile uint32_t *)&bd->f[0].cnt->error & ERR_SPIN_TIMEOUT) atomicOr(&c->error, ERR_SPIN_TIMEOUT);
   }
 }
 
@@ -260,11 +278,15 @@ size_t dedupe_boundary_elems(int W, int H) {
   return ntiles * 32 * 2 + ntiles;  // keys of the right column and bottom row, then 4 bit words per tile
 }
 
-cudaError_t launch_dedupe(const uint16_t *depth, const float *pxp, const float *pyp, const CamF &cam, float scaling,
-                          float maxcam, int4 *vox, int W, int H, int4 *bnd, uint8_t *processed, Counters *cnt,
-                          uint32_t *barrier, int device, cudaStream_t s) {
-  int tilesX = (W + 31) / 32, tilesY = (H + DD_ROWS - 1) / DD_ROWS;
-  int ntiles = tilesX * tilesY;
+int dedupe_tiles(int W, int H, int *tilesX, int *tilesY) {
+  const int tx = (W + 31) / 32, ty = (H + DD_ROWS - 1) / DD_ROWS;
+  if (tilesX) *tilesX = tx;
+  if (tilesY) *tilesY = ty;
+  return tx * ty;
+}
+
+cudaError_t launch_dedupe(const BatchDesc *d_batch, uint32_t total_tiles, uint32_t *barrier, int device,
+                          cudaStream_t s) {
   const int threads = 32 * DD_WARPS;
   // co-resident blocks of the cooperative launch, per device (queried once)
   static int resident[64] = {};
@@ -278,12 +300,9 @@ cudaError_t launch_dedupe(const uint16_t *depth, const float *pxp, const float *
     resident[dslot] = per_sm * sms;
   }
   // one warp per tile, all resident at once
-  const int blocks = (ntiles + DD_WARPS - 1) / DD_WARPS;
-  if (blocks > resident[dslot]) return cudaErrorInvalidConfiguration;
-  CamF camv = cam;
-  void *args[] = {(void *)&depth, (void *)&pxp, (void *)&pyp, (void *)&camv, (void *)&scaling, (void *)&maxcam,
-                  (void *)&vox, (void *)&W, (void *)&H, (void *)&tilesX, (void *)&tilesY, (void *)&bnd,
-                  (void *)&processed, (void *)&cnt, (void *)&barrier};
+  const int blocks = (int)((total_tiles + DD_WARPS - 1) / DD_WARPS);
+  if (blocks > resident[dslot] || blocks < 1) return cudaErrorInvalidConfiguration;
+  void *args[] = {(void *)&d_batch, (void *)&barrier};
   note_launch();
   return cudaLaunchCooperativeKernel((const void *)k_dedupe, dim3(blocks), dim3(threads), args, 0, s);
 }
@@ -317,10 +336,27 @@ __device__ __forceinline__ uint32_t wait_unlocked(uint32_t *tree, uint32_t ptr, 
 // One processed pixel: bounding-box growth, then (inside the volume) the
 // descent of queryPointDepthSingle_func_subtree: queue the existing coarser
 // leaves on the path, allocate missing branches, claim the final leaf.
-__global__ void k_insert(const int4 *__restrict__ vox, const uint8_t *__restrict__ processed, int npix, uint32_t n,
-                         int bw, uint32_t *tree, uint32_t leaves_max, uint32_t branches_max, uint32_t frame,
-                         uint32_t *stamp, uint32_t *queue, PendingLeaf *pend, uint32_t pend_cap, Counters *cnt) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+// One thread per pixel of every frame of the batch (each map's pixels padded
+// to whole warps, so a warp never spans two maps).
+__global__ void k_insert(const BatchDesc *__restrict__ bd) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nmaps = bd->n;
+  if (g >= bd->pix_end[nmaps - 1]) return;
+  int mi = 0;
+  while (mi < nmaps - 1 && g >= bd->pix_end[mi]) mi++;
+  const MapFrame &F = bd->f[mi];
+  const int i = (int)(g - (mi ? bd->pix_end[mi - 1] : 0u));
+  const int npix = (int)F.npix;
+  const int4 *__restrict__ vox = F.vox;
+  const uint8_t *__restrict__ processed = F.proc;
+  const uint32_t n = F.n;
+  const int bw = (int)F.bw;
+  uint32_t *tree = F.tree;
+  const uint32_t leaves_max = F.leaves_max, branches_max = F.branches_max, frame = F.frame;
+  uint32_t *stamp = F.stamp, *queue = F.queue;
+  PendingLeaf *pend = F.pend;
+  const uint32_t pend_cap = F.pend_cap;
+  Counters *cnt = F.cnt;
   bool act = i < npix && processed[i];
   unsigned m = __ballot_sync(0xffffffffu, act);
   if (!act) return;
@@ -403,13 +439,10 @@ __global__ void k_insert(const int4 *__restrict__ vox, const uint8_t *__restrict
   }
 }
 
-void launch_insert(const int4 *vox, const uint8_t *processed, int W, int H, uint32_t n, int bw, uint32_t *tree,
-                   uint32_t leaves_max, uint32_t branches_max, uint32_t frame, uint32_t *stamp, uint32_t *queue,
-                   PendingLeaf *pend, uint32_t pend_cap, Counters *cnt, cudaStream_t s) {
-  int npix = W * H;
+void launch_insert(const BatchDesc *d_batch, uint32_t total_pix, cudaStream_t s) {
+  if (!total_pix) return;
   note_launch();
-  k_insert<<<(npix + 255) / 256, 256, 0, s>>>(vox, processed, npix, n, bw, tree, leaves_max, branches_max, frame,
-                                              stamp, queue, pend, pend_cap, cnt);
+  k_insert<<<(total_pix + 255) / 256, 256, 0, s>>>(d_batch);
 }
 
 // ------------------------------------------------- pending leaf order -----
@@ -507,18 +540,19 @@ __global__ void k_parents(int npend, uint32_t leaves_before, uint32_t leaves_max
 constexpr int FIN_THREADS = 1024;
 constexpr size_t FIN_SMEM_MAX = 200 * 1024;
 
-// npend < 0: read the count on the device (and do nothing after an
-// allocation error, which the host reports).
-__global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const PendingLeaf *pend, int npend, uint32_t npix,
-                                                                 uint32_t *rank, uint32_t leaves_before,
-                                                                 uint32_t leaves_max, uint32_t *tree, ushort4 *leaf,
-                                                                 uint32_t frame, uint32_t *stamp, uint32_t *queue,
-                                                                 Counters *cnt, uint32_t n, uint32_t *parent) {
+// One block per map of the batch; the pending count is read on the device
+// (nothing is done after an allocation error, which the host reports).
+__global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc *__restrict__ bd) {
   extern __shared__ uint32_t fin_smem[];
-  if (npend < 0) {
-    if (cnt->error & (ERR_SPIN_TIMEOUT | ERR_DEDUPE_NOT_CONVERGED | ERR_PENDING_OVERFLOW)) return;
-    npend = (int)cnt->pending;
-  }
+  const MapFrame &F = bd->f[blockIdx.x];
+  Counters *cnt = F.cnt;
+  if (cnt->error & (ERR_SPIN_TIMEOUT | ERR_DEDUPE_NOT_CONVERGED | ERR_PENDING_OVERFLOW)) return;
+  const int npend = (int)cnt->pending;
+  const PendingLeaf *pend = F.pend;
+  const uint32_t npix = F.npix, leaves_before = F.leaves_before, leaves_max = F.leaves_max, frame = F.frame;
+  const uint32_t n = F.n;
+  uint32_t *rank = F.rank, *tree = F.tree, *stamp = F.stamp, *queue = F.queue, *parent = F.parent;
+  ushort4 *leaf = F.leaf;
   const uint32_t nwords = (npix + 31) / 32;
   uint32_t *bitmap = fin_smem;
   uint32_t *chunk_base = fin_smem + nwords;  // [FIN_THREADS]
@@ -561,13 +595,9 @@ bool finalize_small_fits(uint32_t npix) {
   return sizeof(uint32_t) * (((size_t)npix + 31) / 32 + FIN_THREADS) <= FIN_SMEM_MAX;
 }
 
-bool launch_finalize_small(const PendingLeaf *pend, int npend, uint32_t npix, uint32_t *rank_scratch,
-                           uint32_t leaves_before, uint32_t leaves_max, uint32_t *tree, ushort4 *leaf,
-                           uint32_t frame, uint32_t *stamp, uint32_t *queue, Counters *cnt, uint32_t n,
-                           uint32_t *parent, int device, cudaStream_t s) {
-  if (npend == 0) return true;
-  const size_t smem = sizeof(uint32_t) * (((size_t)npix + 31) / 32 + FIN_THREADS);
-  if (smem > FIN_SMEM_MAX) return false;
+bool launch_finalize_small(const BatchDesc *d_batch, int nmaps, uint32_t max_npix, int device, cudaStream_t s) {
+  const size_t smem = sizeof(uint32_t) * (((size_t)max_npix + 31) / 32 + FIN_THREADS);
+  if (smem > FIN_SMEM_MAX || nmaps < 1) return false;
   static std::atomic<unsigned long long> attr_devices{0};
   const unsigned long long bit = 1ull << (device & 63);
   if (!(attr_devices.load() & bit)) {
@@ -577,8 +607,7 @@ bool launch_finalize_small(const PendingLeaf *pend, int npend, uint32_t npix, ui
     attr_devices.fetch_or(bit);
   }
   note_launch();
-  k_finalize_bitmap<<<1, FIN_THREADS, smem, s>>>(pend, npend, npix, rank_scratch, leaves_before, leaves_max, tree,
-                                                 leaf, frame, stamp, queue, cnt, n, parent);
+  k_finalize_bitmap<<<nmaps, FIN_THREADS, smem, s>>>(d_batch);
   return true;
 }
 

@@ -34,6 +34,9 @@ struct ff_handle {
   // the allocation kernels run (it is first read by the voxel update)
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_bgr_free = nullptr, ev_bgr_ready = nullptr;
+  // the frame descriptor(s) the per-frame kernels read: this map's own, or a
+  // whole batch when this handle leads ff_add_maps_u16_device
+  BatchDesc *d_batch = nullptr, *h_batch = nullptr;
 
   // map state on the device
   uint32_t *d_tree = nullptr;
@@ -345,6 +348,11 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
     if (alloc(&h->d_col, L * 1536) != cudaSuccess) { fail(FF_ERR_OOM_POOL, "colour pool"); break; }
     if (alloc(&h->d_cnt, 1) != cudaSuccess || alloc(&h->d_barrier, 8) != cudaSuccess) { fail(FF_ERR_CUDA, "counters"); break; }
     if (cudaMallocHost((void **)&h->h_cnt, sizeof(Counters)) != cudaSuccess) { fail(FF_ERR_CUDA, "pinned"); break; }
+    if (cudaMalloc((void **)&h->d_batch, sizeof(BatchDesc)) != cudaSuccess ||
+        cudaMallocHost((void **)&h->h_batch, sizeof(BatchDesc)) != cudaSuccess) {
+      fail(FF_ERR_CUDA, "frame descriptors");
+      break;
+    }
     if (cfg->rcp_mode == FF_RCP_HOST) {
       std::vector<uint32_t> tab;
       if (!build_rcp_table(tab, h->rcp_shift)) {
@@ -397,6 +405,8 @@ ff_status ff_destroy(ff_handle *h) {
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->h_cnt) cudaFreeHost(h->h_cnt);
+  if (h->d_batch) cudaFree(h->d_batch);
+  if (h->h_batch) cudaFreeHost(h->h_batch);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   if (h->copy_stream) {
     cudaStreamSynchronize(h->copy_stream);
@@ -423,15 +433,35 @@ ff_status ff_set_stream(ff_handle *h, void *cuda_stream) {
   return FF_OK;
 }
 
-// The frame, with depth/bgr already on the device (h->d_depth/h->d_bgr or caller memory).
-static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uint8_t *d_bgr, bool bgr_pending,
-                                int W, int H, const double *K, const double *R, const double *t, float scaling,
-                                float maxcam,
-                                int32_t *queued) {
+// ---------------------------------------------------------------- frames ----
+//
+// A frame runs in three phases, shared by the single-map entry points and
+// the batched one:
+//   prepare  -- host side: first-frame volume, ray factors, counter reset,
+//               the frame's descriptor (camera parameters in FP64 -> FP32);
+//   launch   -- de-duplication, insert, leaf finalisation and the gated voxel
+//               update of every frame of the batch, one launch each;
+//   finish   -- after the one synchronisation: errors, bookkeeping, and the
+//               volume growth (with its update launched again) where needed.
+
+struct FramePlan {
+  const uint16_t *d_depth;
+  const uint8_t *d_bgr;
+  int W, H;
+  float scaling, maxcam;
+  uint32_t frame, leaves_before;
+  bool one_sync;
+};
+
+static uint32_t pad32(uint32_t v) { return (v + 31u) & ~31u; }
+
+// Host part before the launches; fills the frame's descriptor.
+static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint8_t *d_bgr, int W, int H,
+                               const double *K, const double *R, const double *t, float scaling, float maxcam,
+                               MapFrame &mf, FramePlan &plan) {
   cudaStream_t s = h->stream;
   CamF p = cam_world_to_grid(h, K, R, t);
   Counters &hc = *h->h_cnt;
-
   if (!h->n) {
     // first frame: integer bounding box of the valid points (computeBoundingboxIntCPU)
     memset(&hc, 0, sizeof(Counters));
@@ -462,7 +492,15 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
     h->img_w = W;
     h->img_h = H;
   }
-  const uint32_t frame = h->frames + 1;
+  plan.d_depth = d_depth;
+  plan.d_bgr = d_bgr;
+  plan.W = W;
+  plan.H = H;
+  plan.scaling = scaling;
+  plan.maxcam = maxcam;
+  plan.frame = h->frames + 1;
+  plan.leaves_before = h->leaves_used;
+  plan.one_sync = finalize_small_fits((uint32_t)(W * H));
   memset(&hc, 0, sizeof(Counters));
   hc.branches_used = h->branches_used;
   for (int r = 0; r < 3; r++) {
@@ -470,52 +508,110 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
     hc.box_max[r] = (int)h->n - 1;
   }
   CK(cudaMemcpyAsync(h->d_cnt, &hc, sizeof(Counters), cudaMemcpyHostToDevice, s));
-  CK(cudaMemsetAsync(h->d_barrier, 0, 8 * sizeof(uint32_t), s));
+  memset(&mf, 0, sizeof(MapFrame));
+  mf.depth = d_depth;
+  mf.bgr = d_bgr;
+  mf.pxp = h->d_pxp;
+  mf.pyp = h->d_pyp;
+  mf.p = p;
   // voxel -> camera parameters are taken before any grow() of this frame,
   // as in the reference (pInv is built before the traversal)
-  CamF q = cam_grid_to_camera(h, K, R, t);
+  mf.q = cam_grid_to_camera(h, K, R, t);
+  mf.scaling = scaling;
+  mf.maxcam = maxcam;
+  mf.scale = h->cfg.scale;
+  mf.thr = h->cfg.threshold;
+  mf.W = W;
+  mf.H = H;
+  dedupe_tiles(W, H, &mf.tilesX, &mf.tilesY);
+  mf.npix = (uint32_t)(W * H);
+  mf.frame = plan.frame;
+  mf.n = h->n;
+  mf.bw = (uint32_t)h->bandwidth;
+  mf.leaves_max = h->cfg.leaves_max;
+  mf.branches_max = h->cfg.branches_max;
+  mf.leaves_before = plan.leaves_before;
+  mf.pend_cap = (uint32_t)(W * H);
+  mf.nq_host = 0;
+  mf.tree = h->d_tree;
+  mf.leaf = h->d_leaf;
+  mf.parent = h->d_parent;
+  mf.sdf = h->d_sdf;
+  mf.wgt = h->d_wgt;
+  mf.sdf16 = h->d_sdf16;
+  mf.wgt16 = h->d_wgt16;
+  mf.col = h->d_col;
+  mf.stamp = h->d_stamp;
+  mf.queue = h->d_queue;
+  mf.rank = h->d_keys + 3 * h->cap_pix;
+  mf.pend = h->d_pend;
+  mf.vox = h->d_vox;
+  mf.proc = h->d_proc;
+  mf.bnd = h->d_bnd;
+  mf.cnt = h->d_cnt;
+  mf.rcp_tab = h->d_rcp_tab;
+  mf.rcp_shift = h->rcp_shift;
+  return FF_OK;
+}
 
-  const double npix = (double)W * H;
-  int pi = h->prof.begin(ST_DEDUPE, s);
-  CK(launch_dedupe(d_depth, h->d_pxp, h->d_pyp, p, scaling, maxcam, h->d_vox, W, H, h->d_bnd, h->d_proc, h->d_cnt,
-                   h->d_barrier, h->cfg.device, s));
-  h->prof.end(pi, npix * (2 + 16 + 1), s);  // depth in; voxel keys and processed flags out
-  pi = h->prof.begin(ST_INSERT, s);
-  launch_insert(h->d_vox, h->d_proc, W, H, h->n, h->bandwidth, h->d_tree, h->cfg.leaves_max, h->cfg.branches_max,
-                frame, h->d_stamp, h->d_queue, h->d_pend, (uint32_t)(W * H), h->d_cnt, s);
-  h->prof.end(pi, npix * (16 + 1), s);  // keys and flags in (tree walks counted below)
-  CK(cudaGetLastError());
-  if (bgr_pending) CK(cudaStreamWaitEvent(s, h->ev_bgr_ready, 0));
-  // fuse: every voxel of every queued brick read and written: SDF, weight
-  // (4+4 B, or 2+2 B in FP16) and three 16-bit colour channels
-  const double brick_bytes = 512.0 * 2 * ((h->cfg.storage == FF_STORAGE_FP16 ? 4 : 8) + 6);
-  const uint32_t leaves_before = h->leaves_used;
-  const FuseGate no_gate = {nullptr, 0, 0, 0, 0};
-  const bool one_sync = finalize_small_fits((uint32_t)(W * H));
-  int pi_fin = -1, pi_fuse = -1;
-  if (one_sync) {
-    // the leaf finalisation and the voxel update read this frame's counts
-    // on the device; the update stands aside when the volume must grow first
-    uint32_t *rank_scratch = h->d_keys + 3 * h->cap_pix;
-    pi_fin = h->prof.begin(ST_FINALIZE, s);
-    launch_finalize_small(h->d_pend, -1, (uint32_t)(W * H), rank_scratch, leaves_before, h->cfg.leaves_max,
-                          h->d_tree, h->d_leaf, frame, h->d_stamp, h->d_queue, h->d_cnt, h->n, h->d_parent,
-                          h->cfg.device, s);
-    h->prof.end(pi_fin, 0.0, s);
-    const FuseGate gate = {h->d_cnt, h->n, leaves_before, h->cfg.leaves_max, h->cfg.branches_max};
-    pi_fuse = h->prof.begin(ST_FUSE, s);
-    launch_fuse(h->d_queue, 0, gate, h->d_leaf, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
-                h->cfg.storage, d_depth, d_bgr, W, H, q, h->cfg.scale, h->cfg.threshold, scaling, maxcam,
-                h->d_rcp_tab, h->rcp_shift, s);
-    h->prof.end(pi_fuse, 0.0, s);
-    CK(cudaGetLastError());
+// Upload the batch held in lead->h_batch (n frames) and launch its
+// de-duplication and insert on the lead's stream.
+static ff_status frame_launch(ff_handle *lead, int n) {
+  ff_handle *h = lead;  // (error reporting)
+  cudaStream_t s = lead->stream;
+  BatchDesc &B = *lead->h_batch;
+  B.n = n;
+  int rounds = 1;
+  uint32_t tiles = 0, pix = 0;
+  for (int i = 0; i < n; i++) {
+    rounds = std::max(rounds, B.f[i].tilesX + B.f[i].tilesY + 1);
+    tiles += (uint32_t)(B.f[i].tilesX * B.f[i].tilesY);
+    pix += pad32(B.f[i].npix);
+    B.tile_end[i] = tiles;
+    B.pix_end[i] = pix;
   }
-  CK(cudaMemcpyAsync(&hc, h->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
+  B.max_rounds = rounds;
+  CK(cudaMemcpyAsync(lead->d_batch, lead->h_batch, batch_desc_bytes(n), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(lead->d_barrier, 0, 8 * sizeof(uint32_t), s));
+  double npix = 0;
+  for (int i = 0; i < n; i++) npix += (double)B.f[i].npix;
+  int pi = lead->prof.begin(ST_DEDUPE, s);
+  CK(launch_dedupe(lead->d_batch, tiles, lead->d_barrier, lead->cfg.device, s));
+  lead->prof.end(pi, npix * (2 + 16 + 1), s);  // depth in; voxel keys and processed flags out
+  pi = lead->prof.begin(ST_INSERT, s);
+  launch_insert(lead->d_batch, pix, s);
+  lead->prof.end(pi, npix * (16 + 1), s);  // keys and flags in (tree walks counted below)
+  CK(cudaGetLastError());
+  return FF_OK;
+}
+
+// The device-count finalisation and gated voxel update of the uploaded batch.
+static ff_status frame_launch_update(ff_handle *lead, int n, uint32_t max_npix, int &pi_fin, int &pi_fuse) {
+  ff_handle *h = lead;  // (error reporting)
+  cudaStream_t s = lead->stream;
+  pi_fin = lead->prof.begin(ST_FINALIZE, s);
+  if (!launch_finalize_small(lead->d_batch, n, max_npix, lead->cfg.device, s))
+    return set_err(lead, FF_ERR_CUDA, "leaf finalisation could not be launched");
+  lead->prof.end(pi_fin, 0.0, s);
+  pi_fuse = lead->prof.begin(ST_FUSE, s);
+  launch_fuse(lead->d_batch, n, true, lead->cfg.storage, lead->d_rcp_tab != nullptr, 148 * 4, s);
+  lead->prof.end(pi_fuse, 0.0, s);
+  CK(cudaGetLastError());
+  return FF_OK;
+}
+
+// After the synchronisation: one map's frame.  mf is its descriptor (for the
+// update that runs now when the frame took the sort path or had to grow).
+static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf, int pi_fin, int pi_fuse,
+                              int32_t *queued) {
+  cudaStream_t s = h->stream;
+  const Counters &hc = *h->h_cnt;
   if (hc.error & (ERR_SPIN_TIMEOUT | ERR_DEDUPE_NOT_CONVERGED))
     return set_err(h, FF_ERR_TIMEOUT, "a bounded device-side wait gave up during allocation");
   if (hc.error & ERR_PENDING_OVERFLOW) return set_err(h, FF_ERR_STATE, "pending-leaf buffer overflow");
   if (hc.error & ERR_BRANCH_OVERFLOW) h->meshing_ok = false;
+  const uint32_t leaves_before = plan.leaves_before;
+  const int W = plan.W, H = plan.H;
   h->branches_used = std::min(hc.branches_used, h->cfg.branches_max);
   h->processed = hc.processed;
   h->dedupe_rounds = hc.dedupe_iters;
@@ -523,23 +619,23 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
   uint32_t new_queued = 0;
   if (leaves_before < h->cfg.leaves_max) new_queued = std::min(npend, h->cfg.leaves_max - leaves_before);
   // with one synchronisation the counters already include the new leaves
-  const uint32_t nq = one_sync ? hc.queued : hc.queued + new_queued;
-  if (!one_sync && npend) {
+  const uint32_t nq = plan.one_sync ? hc.queued : hc.queued + new_queued;
+  if (!plan.one_sync && npend) {
     pi_fin = h->prof.begin(ST_FINALIZE, s);
     uint32_t *k_in = h->d_keys, *v_in = h->d_keys + h->cap_pix, *k_out = h->d_keys + 2 * h->cap_pix,
              *v_out = h->d_keys + 3 * h->cap_pix;
     int end_bit = 1;
     while ((1u << end_bit) < (uint32_t)(W * H)) end_bit++;
     CK(sort_pending(h->d_pend, (int)npend, k_in, v_in, k_out, v_out, h->d_sort_tmp, h->sort_tmp_bytes, end_bit, s));
-    launch_finalize(h->d_pend, v_out, (int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->d_leaf, frame,
-                    h->d_stamp, h->d_queue, h->d_cnt, s);
+    launch_finalize(h->d_pend, v_out, (int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->d_leaf,
+                    plan.frame, h->d_stamp, h->d_queue, h->d_cnt, s);
     launch_parents((int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->n, h->d_leaf, h->d_parent, s);
     h->prof.end(pi_fin, 0.0, s);
   }
   h->prof.set_bytes(pi_fin, (double)npend * (sizeof(PendingLeaf) + 8 + 4));
   h->leaves_used += npend;
   h->new_leaves = npend;
-  bool fuse_now = !one_sync;
+  bool fuse_now = !plan.one_sync;
   if (h->leaves_used < h->cfg.leaves_max && h->branches_used < h->cfg.branches_max &&
       (hc.box_min[0] < 0 || hc.box_min[1] < 0 || hc.box_min[2] < 0 || hc.box_max[0] >= (int)h->n ||
        hc.box_max[1] >= (int)h->n || hc.box_max[2] >= (int)h->n)) {
@@ -551,12 +647,24 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
     if (st != FF_OK) return st;
     fuse_now = true;
   }
-  if (fuse_now) {
+  // fuse: every voxel of every queued brick read and written: SDF, weight
+  // (4+4 B, or 2+2 B in FP16) and three 16-bit colour channels
+  const double brick_bytes = 512.0 * 2 * ((h->cfg.storage == FF_STORAGE_FP16 ? 4 : 8) + 6);
+  if (fuse_now && nq) {
+    // this map's own descriptor, with the host's count (leaf positions may
+    // have moved with the growth; the camera parameters are the frame's)
+    mf.nq_host = nq;
+    h->h_batch->n = 1;
+    h->h_batch->max_rounds = 1;
+    h->h_batch->tile_end[0] = 0;
+    h->h_batch->pix_end[0] = 0;
+    h->h_batch->f[0] = mf;
+    CK(cudaMemcpyAsync(h->d_batch, h->h_batch, batch_desc_bytes(1), cudaMemcpyHostToDevice, s));
     pi_fuse = h->prof.begin(ST_FUSE, s);
-    launch_fuse(h->d_queue, (int)nq, no_gate, h->d_leaf, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
-                h->cfg.storage, d_depth, d_bgr, W, H, q, h->cfg.scale, h->cfg.threshold, scaling, maxcam,
-                h->d_rcp_tab, h->rcp_shift, s);
+    launch_fuse(h->d_batch, 1, false, h->cfg.storage, h->d_rcp_tab != nullptr, (int)nq, s);
     h->prof.end(pi_fuse, 0.0, s);
+    // the descriptor is read by the update: keep it until it has run
+    CK(cudaStreamSynchronize(s));
   }
   h->prof.set_bytes(pi_fuse, (double)nq * brick_bytes);
   CK(cudaGetLastError());
@@ -566,6 +674,29 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
   mesh_note_frame(h->mesh);
   if (queued) *queued = (int32_t)nq;
   return FF_OK;
+}
+
+// The frame, with depth/bgr already on the device (h->d_depth/h->d_bgr or caller memory).
+static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uint8_t *d_bgr, bool bgr_pending,
+                                int W, int H, const double *K, const double *R, const double *t, float scaling,
+                                float maxcam, int32_t *queued) {
+  cudaStream_t s = h->stream;
+  FramePlan plan;
+  MapFrame mf;
+  ff_status st = frame_prepare(h, d_depth, d_bgr, W, H, K, R, t, scaling, maxcam, mf, plan);
+  if (st != FF_OK) return st;
+  h->h_batch->f[0] = mf;
+  st = frame_launch(h, 1);
+  if (st != FF_OK) return st;
+  if (bgr_pending) CK(cudaStreamWaitEvent(s, h->ev_bgr_ready, 0));
+  int pi_fin = -1, pi_fuse = -1;
+  if (plan.one_sync) {
+    st = frame_launch_update(h, 1, (uint32_t)(W * H), pi_fin, pi_fuse);
+    if (st != FF_OK) return st;
+  }
+  CK(cudaMemcpyAsync(h->h_cnt, h->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return frame_finish(h, plan, mf, pi_fin, pi_fuse, queued);
 }
 
 ff_status ff_add_map_u16(ff_handle *h, const uint16_t *depth, int width, int height, size_t depth_pitch,
@@ -604,6 +735,74 @@ ff_status ff_add_map_u16_device(ff_handle *h, const uint16_t *d_depth, const uin
   ff_status st = ensure_image(h, width, height);
   if (st != FF_OK) return st;
   return add_map_device(h, d_depth, d_bgr, false, width, height, K, R, t, scaling, maxcam, queued);
+}
+
+ff_status ff_add_maps_u16_device(ff_handle *const *maps, int n, const uint16_t *const *d_depth,
+                                 const uint8_t *const *d_bgr, const int *width, const int *height, const double *K,
+                                 const double *R, const double *t, const float *scaling, const float *maxcam,
+                                 int32_t *queued) {
+  if (!maps || n < 1 || !maps[0]) return FF_ERR_BAD_ARG;
+  ff_handle *lead = maps[0];
+  ff_handle *h = lead;  // (error reporting)
+  if (n > BATCH_MAX) return set_err(lead, FF_ERR_BAD_ARG, "ff_add_maps_u16_device: more maps than a batch holds");
+  if (!d_depth || !d_bgr || !width || !height || !K || !R || !t || !scaling || !maxcam)
+    return set_err(lead, FF_ERR_BAD_ARG, "ff_add_maps_u16_device: NULL array");
+  for (int i = 0; i < n; i++) {
+    ff_handle *m = maps[i];
+    if (!m || !d_depth[i] || !d_bgr[i] || width[i] <= 0 || height[i] <= 0)
+      return set_err(lead, FF_ERR_BAD_ARG, "ff_add_maps_u16_device: NULL map or image, or empty image");
+    if (m->cfg.device != lead->cfg.device || m->cfg.storage != lead->cfg.storage ||
+        (m->d_rcp_tab != nullptr) != (lead->d_rcp_tab != nullptr))
+      return set_err(lead, FF_ERR_BAD_ARG, "ff_add_maps_u16_device: maps differ in device, storage or reciprocal mode");
+    for (int j = 0; j < i; j++)
+      if (maps[j] == m) return set_err(lead, FF_ERR_BAD_ARG, "ff_add_maps_u16_device: a map appears twice");
+  }
+  CK(cudaSetDevice(lead->cfg.device));
+  // frames whose finalisation needs the sort path (very large images) are
+  // fused one by one
+  uint32_t max_npix = 0;
+  bool all_small = true;
+  for (int i = 0; i < n; i++) {
+    const uint32_t np = (uint32_t)(width[i] * height[i]);
+    max_npix = std::max(max_npix, np);
+    all_small = all_small && finalize_small_fits(np);
+  }
+  if (!all_small) {
+    for (int i = 0; i < n; i++) {
+      ff_status st = ff_add_map_u16_device(maps[i], d_depth[i], d_bgr[i], width[i], height[i], K + 4 * i, R + 9 * i,
+                                           t + 3 * i, scaling[i], maxcam[i], queued ? queued + i : nullptr);
+      if (st != FF_OK) return st;
+    }
+    return FF_OK;
+  }
+  std::vector<FramePlan> plan(n);
+  std::vector<MapFrame> mf(n);
+  for (int i = 0; i < n; i++) {
+    ff_handle *m = maps[i];
+    CK(cudaStreamSynchronize(m->stream));
+    ff_status st = ensure_image(m, width[i], height[i]);
+    if (st != FF_OK) return st;
+    st = frame_prepare(m, d_depth[i], d_bgr[i], width[i], height[i], K + 4 * i, R + 9 * i, t + 3 * i, scaling[i],
+                       maxcam[i], mf[i], plan[i]);
+    if (st != FF_OK) return st;
+  }
+  // the counter resets went out on each map's stream; the batch runs on the lead's
+  for (int i = 1; i < n; i++) CK(cudaStreamSynchronize(maps[i]->stream));
+  for (int i = 0; i < n; i++) lead->h_batch->f[i] = mf[i];
+  ff_status st = frame_launch(lead, n);
+  if (st != FF_OK) return st;
+  int pi_fin = -1, pi_fuse = -1;
+  st = frame_launch_update(lead, n, max_npix, pi_fin, pi_fuse);
+  if (st != FF_OK) return st;
+  for (int i = 0; i < n; i++)
+    CK(cudaMemcpyAsync(maps[i]->h_cnt, maps[i]->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, lead->stream));
+  CK(cudaStreamSynchronize(lead->stream));
+  for (int i = 0; i < n; i++) {
+    st = frame_finish(maps[i], plan[i], mf[i], i == 0 ? pi_fin : -1, i == 0 ? pi_fuse : -1,
+                      queued ? queued + i : nullptr);
+    if (st != FF_OK) return st;
+  }
+  return FF_OK;
 }
 
 ff_status ff_get_stats(ff_handle *h, ff_stats *o) {

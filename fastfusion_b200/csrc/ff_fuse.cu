@@ -149,58 +149,57 @@ __device__ __forceinline__ void fuse_brick(const uint32_t brick, const ushort4 *
   }
 }
 
-// Whether this frame's update must wait for the host: an allocation error, or
+// Whether a frame's update must wait for the host: an allocation error, or
 // the volume must grow first (the host then grows and launches the update
 // again).  Mirrors the host's test after the traversal.
-__device__ __forceinline__ bool fuse_deferred(const FuseGate &g) {
-  const Counters *c = g.cnt;
+__device__ __forceinline__ bool fuse_deferred(const MapFrame &F) {
+  const Counters *c = F.cnt;
   if (c->error & (ERR_SPIN_TIMEOUT | ERR_DEDUPE_NOT_CONVERGED | ERR_PENDING_OVERFLOW)) return true;
-  const uint32_t leaves = g.leaves_before + c->pending;
-  const uint32_t branches = min(c->branches_used, g.branches_max);
-  const int n = (int)g.n;
+  const uint32_t leaves = F.leaves_before + c->pending;
+  const uint32_t branches = min(c->branches_used, F.branches_max);
+  const int n = (int)F.n;
   const bool outside = c->box_min[0] < 0 || c->box_min[1] < 0 || c->box_min[2] < 0 || c->box_max[0] >= n ||
                        c->box_max[1] >= n || c->box_max[2] >= n;
-  return leaves < g.leaves_max && branches < g.branches_max && outside;
+  return leaves < F.leaves_max && branches < F.branches_max && outside;
 }
 
-// One 512-thread block per brick, one thread per voxel.  With a gate, the
-// brick count is read on the device (the queue after this frame's new
-// leaves) and the blocks loop over it.
+// One 512-thread block per brick, one thread per voxel, blocks looping over
+// the bricks of every map of the batch in order.  Gated: each map's count is
+// read on the device; otherwise the host's count (nq_host) is used.
 template <bool FP16, bool RCP_HOST>
-__global__ void __launch_bounds__(512) k_fuse(const uint32_t *__restrict__ queue, uint32_t nq, FuseGate gate,
-                                              const ushort4 *__restrict__ leaf, float *__restrict__ sdf,
-                                              float *__restrict__ wgt, __half *__restrict__ sdf16,
-                                              __half *__restrict__ wgt16, uint16_t *__restrict__ col,
-                                              const uint16_t *__restrict__ depth, const uint8_t *__restrict__ bgr,
-                                              int W, int H, CamF q, float scale, float thr, float scaling,
-                                              float maxcam, const uint32_t *__restrict__ rtab, int rshift) {
-  if (gate.cnt) {
-    if (fuse_deferred(gate)) return;
-    nq = gate.cnt->queued;
+__global__ void __launch_bounds__(512) k_fuse(const BatchDesc *__restrict__ bd, int gated) {
+  __shared__ uint32_t end[BATCH_MAX];  // inclusive prefix of the maps' brick counts
+  const int nmaps = bd->n;
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (int m = 0; m < nmaps; m++) {
+      const MapFrame &F = bd->f[m];
+      acc += gated ? (fuse_deferred(F) ? 0u : F.cnt->queued) : F.nq_host;
+      end[m] = acc;
+    }
   }
-  for (uint32_t b = blockIdx.x; b < nq; b += gridDim.x)
-    fuse_brick<FP16, RCP_HOST>(queue[b], leaf, sdf, wgt, sdf16, wgt16, col, depth, bgr, W, H, q, scale, thr, scaling,
-                               maxcam, rtab, rshift);
+  __syncthreads();
+  const uint32_t total = end[nmaps - 1];
+  int m = 0;
+  for (uint32_t b = blockIdx.x; b < total; b += gridDim.x) {
+    while (b >= end[m]) m++;
+    const MapFrame &F = bd->f[m];
+    const uint32_t local = b - (m ? end[m - 1] : 0u);
+    fuse_brick<FP16, RCP_HOST>(F.queue[local], F.leaf, F.sdf, F.wgt, F.sdf16, F.wgt16, F.col, F.depth, F.bgr, F.W,
+                               F.H, F.q, F.scale, F.thr, F.scaling, F.maxcam, F.rcp_tab, F.rcp_shift);
+  }
 }
 
-void launch_fuse(const uint32_t *queue, int nq, const FuseGate &gate, const ushort4 *leaf, float *sdf, float *wgt,
-                 __half *sdf16, __half *wgt16, uint16_t *col, int storage, const uint16_t *depth, const uint8_t *bgr,
-                 int W, int H, const CamF &q, float scale, float thr, float scaling, float maxcam,
-                 const uint32_t *rcp_tab, int rcp_shift, cudaStream_t s) {
-  // host count: one block per brick; device count: 4 resident blocks per SM
-  // loop over the bricks
-  int grid = nq;
-  if (gate.cnt) grid = 148 * 4;
-  if (grid <= 0) return;
-#define FF_FUSE(F16, RH)                                                                                           \
-  k_fuse<F16, RH><<<grid, 512, 0, s>>>(queue, (uint32_t)(nq > 0 ? nq : 0), gate, leaf, sdf, wgt, sdf16, wgt16, col, \
-                                       depth, bgr, W, H, q, scale, thr, scaling, maxcam, rcp_tab, rcp_shift)
-  const bool rh = rcp_tab != nullptr;
+void launch_fuse(const BatchDesc *d_batch, int nmaps, bool gated, int storage, bool rcp_host, int grid,
+                 cudaStream_t s) {
+  if (grid <= 0 || nmaps < 1) return;
+  const int g = gated ? 1 : 0;
+#define FF_FUSE(F16, RH) k_fuse<F16, RH><<<grid, 512, 0, s>>>(d_batch, g)
   note_launch();
   if (storage == 1) {
-    if (rh) FF_FUSE(true, true); else FF_FUSE(true, false);
+    if (rcp_host) FF_FUSE(true, true); else FF_FUSE(true, false);
   } else {
-    if (rh) FF_FUSE(false, true); else FF_FUSE(false, false);
+    if (rcp_host) FF_FUSE(false, true); else FF_FUSE(false, false);
   }
 #undef FF_FUSE
 }

@@ -3,11 +3,57 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cstddef>
 #include <vector>
 
 #include "ff_common.cuh"
 
 namespace ffb {
+
+// One map's frame as the per-frame kernels see it (device-resident, in a
+// BatchDesc).  A batch holds the frames of several independent maps that
+// the same launches process together; a single map is a batch of one.
+struct PendingLeaf;
+struct MapFrame {
+  // the frame
+  const uint16_t *depth;
+  const uint8_t *bgr;
+  const float *pxp, *pyp;  // per-column / per-row ray factors
+  CamF p;                  // world -> voxel grid (traversal)
+  CamF q;                  // voxel grid -> camera (update)
+  float scaling, maxcam, scale, thr;
+  int W, H, tilesX, tilesY;
+  uint32_t npix, frame;
+  // the map
+  uint32_t n, bw, leaves_max, branches_max, leaves_before, pend_cap, nq_host;
+  uint32_t *tree;
+  ushort4 *leaf;
+  uint32_t *parent;
+  float *sdf, *wgt;
+  __half *sdf16, *wgt16;
+  uint16_t *col;
+  uint32_t *stamp, *queue, *rank;
+  PendingLeaf *pend;
+  int4 *vox;
+  uint8_t *proc;
+  int4 *bnd;
+  Counters *cnt;
+  const uint32_t *rcp_tab;
+  int rcp_shift;
+};
+
+constexpr int BATCH_MAX = 32;
+
+struct BatchDesc {
+  int n;                          // maps in the batch
+  int max_rounds;                 // de-duplication round limit (largest image)
+  uint32_t tile_end[BATCH_MAX];   // inclusive prefix of each map's de-duplication tiles
+  uint32_t pix_end[BATCH_MAX];    // inclusive prefix of each map's pixels, each padded to 32
+  MapFrame f[BATCH_MAX];
+};
+
+// Bytes of a BatchDesc holding n maps (the tail past f[n-1] is not uploaded).
+inline size_t batch_desc_bytes(int n) { return offsetof(BatchDesc, f) + sizeof(MapFrame) * (size_t)n; }
 
 // A leaf claimed during the frame's traversal, before its index is assigned.
 struct PendingLeaf {
@@ -20,20 +66,19 @@ struct PendingLeaf {
 void launch_first_bbox(const uint16_t *depth, int W, int H, const CamF &p, float scaling, float maxcam, int bw,
                        Counters *cnt, cudaStream_t s);
 
-// Per-pixel voxel coordinates, validity and target brick scale (written to
-// vox), then the row/column de-duplication of brick keys
-// (traversal_wrapper_functions.cpp:613-639, 688-690).
-// bnd: 4 buffers of boundary state; barrier: 8 zeroed uint32 words.
+// Tiles of the de-duplication for a W x H image (and the tile grid).
+int dedupe_tiles(int W, int H, int *tilesX, int *tilesY);
 // int4 elements of the boundary buffer launch_dedupe needs for a W x H image.
 size_t dedupe_boundary_elems(int W, int H);
-cudaError_t launch_dedupe(const uint16_t *depth, const float *pxp, const float *pyp, const CamF &cam, float scaling,
-                          float maxcam, int4 *vox, int W, int H, int4 *bnd, uint8_t *processed, Counters *cnt,
-                          uint32_t *barrier, int device, cudaStream_t s);
+// Per-pixel voxel coordinates, validity and target brick scale (written to
+// each frame's vox), then the row/column de-duplication of brick keys
+// (traversal_wrapper_functions.cpp:613-639, 688-690), for every frame of the
+// batch in one cooperative launch.  barrier: 8 zeroed uint32 words.
+cudaError_t launch_dedupe(const BatchDesc *d_batch, uint32_t total_tiles, uint32_t *barrier, int device,
+                          cudaStream_t s);
 
-// Octree descent / allocation of every processed pixel.
-void launch_insert(const int4 *vox, const uint8_t *processed, int W, int H, uint32_t n, int bw, uint32_t *tree,
-                   uint32_t leaves_max, uint32_t branches_max, uint32_t frame, uint32_t *stamp, uint32_t *queue,
-                   PendingLeaf *pend, uint32_t pend_cap, Counters *cnt, cudaStream_t s);
+// Octree descent / allocation of every processed pixel of the batch.
+void launch_insert(const BatchDesc *d_batch, uint32_t total_pix, cudaStream_t s);
 
 // Sort scratch size for `n` pending leaves.
 size_t pending_sort_bytes(int n);
@@ -52,14 +97,10 @@ void launch_parents(int npend, uint32_t leaves_before, uint32_t leaves_max, cons
 // Whether launch_finalize_small takes a W x H frame.
 bool finalize_small_fits(uint32_t npix);
 
-// Ranks (creation order), leaf table and parents of the frame's pending
-// leaves in one launch, for images of up to about 1.6 million pixels; false
-// (nothing launched) for larger ones.  npend < 0: the count is read on the
-// device.  rank_scratch: W*H uint32.
-bool launch_finalize_small(const PendingLeaf *pend, int npend, uint32_t npix, uint32_t *rank_scratch,
-                           uint32_t leaves_before, uint32_t leaves_max, uint32_t *tree, ushort4 *leaf,
-                           uint32_t frame, uint32_t *stamp, uint32_t *queue, Counters *cnt, uint32_t n,
-                           uint32_t *parent, int device, cudaStream_t s);
+// Ranks (creation order), leaf table and parents of each map's pending
+// leaves, one block per map, counts read on the device; for images of up to
+// about 1.6 million pixels (false, nothing launched, for larger ones).
+bool launch_finalize_small(const BatchDesc *d_batch, int nmaps, uint32_t max_npix, int device, cudaStream_t s);
 
 // Load the kernels of each file ahead of their first launch.
 cudaError_t prewarm_alloc_kernels();
@@ -71,18 +112,12 @@ void launch_shift_branches(uint32_t *tree, uint32_t used, uint32_t shift, cudaSt
 void launch_shift_leaves(ushort4 *leaf, uint32_t n_leaves, ushort3 add, cudaStream_t s);
 void launch_fill(uint32_t *p, size_t n, uint32_t v, cudaStream_t s);
 
-// Device-side gate of a frame's voxel update whose brick count the host has
-// not read yet (cnt == nullptr: no gate, the host passes the count).
-struct FuseGate {
-  const Counters *cnt;
-  uint32_t n, leaves_before, leaves_max, branches_max;
-};
-
-// Voxel update of the queued bricks (update_functions.cpp:1187-1444).
-void launch_fuse(const uint32_t *queue, int nq, const FuseGate &gate, const ushort4 *leaf, float *sdf, float *wgt,
-                 __half *sdf16, __half *wgt16, uint16_t *col, int storage, const uint16_t *depth, const uint8_t *bgr,
-                 int W, int H, const CamF &q, float scale, float thr, float scaling, float maxcam,
-                 const uint32_t *rcp_tab, int rcp_shift, cudaStream_t s);
+// Voxel update of the queued bricks of every frame of the batch
+// (update_functions.cpp:1187-1444).  gated: each map's brick count is read
+// on the device (its queue after the new leaves) and a map whose volume must
+// grow first is left for the host; otherwise MapFrame::nq_host is used.
+void launch_fuse(const BatchDesc *d_batch, int nmaps, bool gated, int storage, bool rcp_host, int grid,
+                 cudaStream_t s);
 
 // Table of the host CPU's RCPPS over the mantissas of [1,2), indexed by the
 // mantissa >> shift (the low bits the instruction ignores are dropped); false

@@ -63,6 +63,7 @@ SIGNATURES = {
     "ff_set_stream": (_i32, [_vp, _vp]),
     "ff_add_map_u16": (_i32, [_vp, _vp, _i32, _i32, _sz, _vp, _sz, _vp, _vp, _vp, _f32, _f32, _vp]),
     "ff_add_map_u16_device": (_i32, [_vp, _vp, _vp, _i32, _i32, _vp, _vp, _vp, _f32, _f32, _vp]),
+    "ff_add_maps_u16_device": (_i32, [_vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ff_update_meshes": (_i32, [_vp, _vp]),
     "ff_get_mesh_counts": (_i32, [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
     "ff_get_mesh": (_i32, [_vp, _vp, _vp, _vp]),
@@ -457,6 +458,30 @@ class FusionMipMapCPU:
         z = np.load(path)
         self.set_state(int(z["n"]), z["offset"], z["tree"], z["pos"], z["scale"], z["parent"], z["sdf"],
                        z["weight"], z["rgb"])
+
+
+def add_maps_device(maps, d_depth, d_bgr, widths, heights, cams, scaling, maxcam) -> list:
+    """One frame for each of several maps in one set of launches
+    (ff_add_maps_u16_device): d_depth/d_bgr are device pointers (ints), cams
+    CameraInfo objects, scaling/maxcam scalars or per-map sequences.  Returns
+    each map's queued count; same results as addMapDevice on each map."""
+    L = load_library()
+    n = len(maps)
+    sc = np.broadcast_to(np.asarray(scaling, np.float32), (n,)).copy()
+    mc = np.broadcast_to(np.asarray(maxcam, np.float32), (n,)).copy()
+    hs = (ctypes.c_void_p * n)(*[m._h for m in maps])
+    dd = (ctypes.c_void_p * n)(*[int(p) for p in d_depth])
+    db = (ctypes.c_void_p * n)(*[int(p) for p in d_bgr])
+    w = np.asarray(widths, np.int32)
+    h = np.asarray(heights, np.int32)
+    K = np.ascontiguousarray(np.stack([c.K for c in cams]), np.float64)
+    R = np.ascontiguousarray(np.stack([c.R.reshape(9) for c in cams]), np.float64)
+    t = np.ascontiguousarray(np.stack([c.t for c in cams]), np.float64)
+    q = np.zeros(n, np.int32)
+    st = L.ff_add_maps_u16_device(hs, n, dd, db, _p(w), _p(h), _p(K), _p(R), _p(t), _p(sc), _p(mc), _p(q))
+    if st != FF_OK:
+        raise FFError(st, L.ff_last_error(maps[0]._h).decode())
+    return [int(x) for x in q]
 
 
 def version() -> str:

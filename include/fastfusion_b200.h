@@ -108,6 +108,21 @@ ff_status ff_add_map_u16_device(ff_handle *h, const uint16_t *d_depth, const uin
                                 const double K[4], const double R[9], const double t[3], float scaling,
                                 float maxcam, int32_t *queued);
 
+/* Several independent maps fuse one frame each, in one set of launches (the
+ * de-duplication of all frames in one cooperative launch, their inserts,
+ * leaf finalisations and voxel updates in one launch each) -- for many maps
+ * of uneven size on one GPU.  Same results as ff_add_map_u16_device on each
+ * map in turn.  maps: n distinct handles on one device with the same storage
+ * and reciprocal mode, n <= 32; per map i: device images d_depth[i], d_bgr[i]
+ * of width[i] x height[i], K + 4i, R + 9i, t + 3i, scaling[i], maxcam[i];
+ * queued[i] (may be NULL) receives each map's count.  The work runs on
+ * maps[0]'s stream.  The reference fuses one map per call; this is the
+ * batched form of its addMap (geometryfusion_mipmap_cpu.cpp:1603-2034). */
+ff_status ff_add_maps_u16_device(ff_handle *const *maps, int n, const uint16_t *const *d_depth,
+                                 const uint8_t *const *d_bgr, const int *width, const int *height, const double *K,
+                                 const double *R, const double *t, const float *scaling, const float *maxcam,
+                                 int32_t *queued);
+
 /* Re-mesh the cells touched since the last update and rebuild the
  * interleaved mesh.  Replaces FusionMipMapCPU::updateMeshes()
  * (geometryfusion_mipmap_cpu.cpp:2884-2954) with threaded meshing off;
