@@ -119,7 +119,9 @@ __device__ __forceinline__ void grid_barrier(uint32_t *bar, uint32_t nblocks, Co
 }
 
 constexpr int DD_WARPS = 4;  // tiles (warps) per block
-constexpr int DD_ROWS = 16;  // tile height: more, shorter tiles shorten each warp's chain of rows
+// tile height: 16 rows (more, shorter tiles shorten each warp's chain of
+// rows), or 32 when the image has more 16-row tiles than resident warps
+constexpr int DD_ROWS_SHORT = 16, DD_ROWS_TALL = 32;
 
 __device__ __forceinline__ bool same3(int a0, int a1, int a2, int b0, int b1, int b2) {
   return a0 == b0 && a1 == b1 && a2 == b2;
@@ -133,6 +135,7 @@ __device__ __forceinline__ bool same3(int a0, int a1, int a2, int b0, int b1, in
 // One launch for all frames of a batch: warps are dealt out over the maps'
 // tiles in order; the rounds and their barrier are shared (a map whose tiles
 // have settled recomputes the same bits until every map has).
+template <int DD_ROWS>
 __global__ void __launch_bounds__(32 * DD_WARPS) k_dedupe(const BatchDesc *__restrict__ bd, uint32_t *bar) {
   const int lane = threadIdx.x & 31;
   const uint32_t gtile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -273,38 +276,56 @@ __global__ void __launch_bounds__(32 * DD_WARPS) k_dedupe(const BatchDesc *__res
   }
 }
 
-size_t dedupe_boundary_elems(int W, int H) {
-  const size_t ntiles = (size_t)((W + 31) / 32) * ((H + DD_ROWS - 1) / DD_ROWS);
-  return ntiles * 32 * 2 + ntiles;  // keys of the right column and bottom row, then 4 bit words per tile
-}
-
-int dedupe_tiles(int W, int H, int *tilesX, int *tilesY) {
-  const int tx = (W + 31) / 32, ty = (H + DD_ROWS - 1) / DD_ROWS;
+int dedupe_tiles(int W, int H, int *tilesX, int *tilesY, int rows) {
+  const int tx = (W + 31) / 32, ty = (H + rows - 1) / rows;
   if (tilesX) *tilesX = tx;
   if (tilesY) *tilesY = ty;
   return tx * ty;
 }
 
-cudaError_t launch_dedupe(const BatchDesc *d_batch, uint32_t total_tiles, uint32_t *barrier, int device,
-                          cudaStream_t s) {
-  const int threads = 32 * DD_WARPS;
-  // co-resident blocks of the cooperative launch, per device (queried once)
+size_t dedupe_boundary_elems(int W, int H) {
+  // sized for the shorter tiles (the larger count)
+  const size_t ntiles = (size_t)dedupe_tiles(W, H, nullptr, nullptr, DD_ROWS_SHORT);
+  return ntiles * 32 * 2 + ntiles;  // keys of the right column and bottom row, then 4 bit words per tile
+}
+
+template <int ROWS>
+static cudaError_t resident_dedupe_warps(int device, int &warps) {
   static int resident[64] = {};
   const int dslot = device & 63;
   if (!resident[dslot]) {
     int per_sm = 0, sms = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dedupe, threads, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dedupe<ROWS>, 32 * DD_WARPS, 0);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
     resident[dslot] = per_sm * sms;
   }
+  warps = resident[dslot] * DD_WARPS;
+  return cudaSuccess;
+}
+
+cudaError_t dedupe_tile_rows(uint32_t tiles_short, int device, int &rows) {
+  int warps = 0;
+  cudaError_t e = resident_dedupe_warps<DD_ROWS_SHORT>(device, warps);
+  if (e != cudaSuccess) return e;
+  rows = (int)tiles_short <= warps ? DD_ROWS_SHORT : DD_ROWS_TALL;
+  return cudaSuccess;
+}
+
+cudaError_t launch_dedupe(const BatchDesc *d_batch, uint32_t total_tiles, int rows, uint32_t *barrier, int device,
+                          cudaStream_t s) {
+  int warps = 0;
+  cudaError_t e = rows == DD_ROWS_SHORT ? resident_dedupe_warps<DD_ROWS_SHORT>(device, warps)
+                                        : resident_dedupe_warps<DD_ROWS_TALL>(device, warps);
+  if (e != cudaSuccess) return e;
   // one warp per tile, all resident at once
   const int blocks = (int)((total_tiles + DD_WARPS - 1) / DD_WARPS);
-  if (blocks > resident[dslot] || blocks < 1) return cudaErrorInvalidConfiguration;
+  if (blocks * DD_WARPS > warps || blocks < 1) return cudaErrorInvalidConfiguration;
   void *args[] = {(void *)&d_batch, (void *)&barrier};
   note_launch();
-  return cudaLaunchCooperativeKernel((const void *)k_dedupe, dim3(blocks), dim3(threads), args, 0, s);
+  const void *fn = rows == DD_ROWS_SHORT ? (const void *)k_dedupe<DD_ROWS_SHORT> : (const void *)k_dedupe<DD_ROWS_TALL>;
+  return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(32 * DD_WARPS), args, 0, s);
 }
 
 // -------------------------------------------------------------- insert ----
@@ -665,7 +686,8 @@ void launch_fill(uint32_t *p, size_t n, uint32_t v, cudaStream_t s) {
 // Load this file's kernels now (modules load lazily on first launch, which
 // would otherwise land inside the first frame that needs a kernel).
 cudaError_t prewarm_alloc_kernels() {
-  const void *fns[] = {(const void *)k_first_bbox, (const void *)k_dedupe, (const void *)k_insert,
+  const void *fns[] = {(const void *)k_first_bbox, (const void *)k_dedupe<DD_ROWS_SHORT>,
+                       (const void *)k_dedupe<DD_ROWS_TALL>, (const void *)k_insert,
                        (const void *)k_pending_keys, (const void *)k_finalize, (const void *)k_parents,
                        (const void *)k_finalize_bitmap, (const void *)k_shift_branches,
                        (const void *)k_shift_leaves, (const void *)k_fill};

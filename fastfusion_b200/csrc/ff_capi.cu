@@ -523,7 +523,7 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
   mf.thr = h->cfg.threshold;
   mf.W = W;
   mf.H = H;
-  dedupe_tiles(W, H, &mf.tilesX, &mf.tilesY);
+  dedupe_tiles(W, H, &mf.tilesX, &mf.tilesY, 16);  // frame_launch may choose taller tiles
   mf.npix = (uint32_t)(W * H);
   mf.frame = plan.frame;
   mf.n = h->n;
@@ -561,6 +561,11 @@ static ff_status frame_launch(ff_handle *lead, int n) {
   cudaStream_t s = lead->stream;
   BatchDesc &B = *lead->h_batch;
   B.n = n;
+  uint32_t tiles16 = 0;
+  for (int i = 0; i < n; i++) tiles16 += (uint32_t)dedupe_tiles(B.f[i].W, B.f[i].H, nullptr, nullptr, 16);
+  int rows = 16;
+  CK(dedupe_tile_rows(tiles16, lead->cfg.device, rows));
+  for (int i = 0; i < n; i++) dedupe_tiles(B.f[i].W, B.f[i].H, &B.f[i].tilesX, &B.f[i].tilesY, rows);
   int rounds = 1;
   uint32_t tiles = 0, pix = 0;
   for (int i = 0; i < n; i++) {
@@ -576,7 +581,7 @@ static ff_status frame_launch(ff_handle *lead, int n) {
   double npix = 0;
   for (int i = 0; i < n; i++) npix += (double)B.f[i].npix;
   int pi = lead->prof.begin(ST_DEDUPE, s);
-  CK(launch_dedupe(lead->d_batch, tiles, lead->d_barrier, lead->cfg.device, s));
+  CK(launch_dedupe(lead->d_batch, tiles, rows, lead->d_barrier, lead->cfg.device, s));
   lead->prof.end(pi, npix * (2 + 16 + 1), s);  // depth in; voxel keys and processed flags out
   pi = lead->prof.begin(ST_INSERT, s);
   launch_insert(lead->d_batch, pix, s);

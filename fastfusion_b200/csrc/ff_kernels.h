@@ -66,15 +66,18 @@ struct PendingLeaf {
 void launch_first_bbox(const uint16_t *depth, int W, int H, const CamF &p, float scaling, float maxcam, int bw,
                        Counters *cnt, cudaStream_t s);
 
-// Tiles of the de-duplication for a W x H image (and the tile grid).
-int dedupe_tiles(int W, int H, int *tilesX, int *tilesY);
+// Tiles of the de-duplication for a W x H image with tiles `rows` high (and
+// the tile grid); 16-row tiles unless the batch has more of them than warps
+// can be resident, then 32-row tiles (dedupe_tile_rows).
+int dedupe_tiles(int W, int H, int *tilesX, int *tilesY, int rows);
+cudaError_t dedupe_tile_rows(uint32_t tiles_short, int device, int &rows);
 // int4 elements of the boundary buffer launch_dedupe needs for a W x H image.
 size_t dedupe_boundary_elems(int W, int H);
 // Per-pixel voxel coordinates, validity and target brick scale (written to
 // each frame's vox), then the row/column de-duplication of brick keys
 // (traversal_wrapper_functions.cpp:613-639, 688-690), for every frame of the
 // batch in one cooperative launch.  barrier: 8 zeroed uint32 words.
-cudaError_t launch_dedupe(const BatchDesc *d_batch, uint32_t total_tiles, uint32_t *barrier, int device,
+cudaError_t launch_dedupe(const BatchDesc *d_batch, uint32_t total_tiles, int rows, uint32_t *barrier, int device,
                           cudaStream_t s);
 
 // Octree descent / allocation of every processed pixel of the batch.
