@@ -599,7 +599,8 @@ static ff_status frame_launch_update(ff_handle *lead, int n, uint32_t max_npix, 
     return set_err(lead, FF_ERR_CUDA, "leaf finalisation could not be launched");
   lead->prof.end(pi_fin, 0.0, s);
   pi_fuse = lead->prof.begin(ST_FUSE, s);
-  launch_fuse(lead->d_batch, n, true, lead->cfg.storage, lead->d_rcp_tab != nullptr, 148 * 4, s);
+  // enough blocks for a frame's bricks in one pass; blocks loop over larger batches
+  launch_fuse(lead->d_batch, n, true, lead->cfg.storage, lead->d_rcp_tab != nullptr, 148 * 8, s);
   lead->prof.end(pi_fuse, 0.0, s);
   CK(cudaGetLastError());
   return FF_OK;
@@ -802,11 +803,18 @@ ff_status ff_add_maps_u16_device(ff_handle *const *maps, int n, const uint16_t *
   for (int i = 0; i < n; i++)
     CK(cudaMemcpyAsync(maps[i]->h_cnt, maps[i]->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, lead->stream));
   CK(cudaStreamSynchronize(lead->stream));
+  double bricks = 0, pending = 0;
   for (int i = 0; i < n; i++) {
     st = frame_finish(maps[i], plan[i], mf[i], i == 0 ? pi_fin : -1, i == 0 ? pi_fuse : -1,
                       queued ? queued + i : nullptr);
     if (st != FF_OK) return st;
+    bricks += maps[i]->queued;
+    pending += maps[i]->new_leaves;
   }
+  // the lead's profile holds the batch's launches: count every map's work
+  const double brick_bytes = 512.0 * 2 * ((lead->cfg.storage == FF_STORAGE_FP16 ? 4 : 8) + 6);
+  lead->prof.set_bytes(pi_fuse, bricks * brick_bytes);
+  lead->prof.set_bytes(pi_fin, pending * (sizeof(PendingLeaf) + 8 + 4));
   return FF_OK;
 }
 

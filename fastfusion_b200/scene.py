@@ -326,3 +326,30 @@ def render_torch(scene: Scene, R, t, width: int, height: int, K, seed: int, fram
     depth = depth.to(torch.int32).to(torch.int16)  # bit pattern of the uint16 value
     bgr = colour.flip(-1).reshape(height, width, 3).contiguous()
     return depth, bgr
+
+
+def batch_sequences(n_maps: int = 16, n_frames: int = 200, seed0: int = 100):
+    """Independent maps of uneven size (the batched workload): per map i, seed
+    seed0 + i draws room sides U(2, 12) m (3 m high), U{10..150} primitives,
+    an image size from 320x240 / 640x480 / 1280x960 and a voxel size U(4, 10)
+    mm; each map walks its own room.  Returns [(Sequence, voxel metres)]."""
+    out = []
+    sizes = [(320, 240), (640, 480), (1280, 960)]
+    for i in range(n_maps):
+        rng = np.random.default_rng(seed0 + i)
+        room = (float(rng.uniform(2, 12)), float(rng.uniform(2, 12)), 3.0)
+        prims = int(rng.integers(10, 151))
+        w, h = sizes[int(rng.integers(0, 3))]
+        voxel = float(rng.uniform(0.004, 0.010))
+        margin = min(0.8, 0.3 * min(room[0], room[1]))
+        s = w / 640.0
+        K = np.array([525.0 * s, 525.0 * s, (w - 1) / 2.0, (h - 1) / 2.0])
+        poses = random_walk_trajectory(n_frames, seed0 + i, room=room, margin=margin)
+        cams = np.array([p[1] for p in poses])
+
+        def clear(c, rad, cams=cams):
+            return np.min(np.linalg.norm(cams - c[None, :], axis=1)) > rad + 0.3
+
+        scene = make_scene(seed0 + i, room=room, n_prims=prims, keep_clear=clear)
+        out.append((Sequence(scene=scene, K=K, width=w, height=h, poses=poses, seed=seed0 + i), voxel))
+    return out
