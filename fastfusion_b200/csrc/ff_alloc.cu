@@ -135,16 +135,18 @@ __device__ __forceinline__ bool same3(int a0, int a1, int a2, int b0, int b1, in
 // One launch for all frames of a batch: warps are dealt out over the maps'
 // tiles in order; the rounds and their barrier are shared (a map whose tiles
 // have settled recomputes the same bits until every map has).
+// Maps [m0, m1) of the batch (their tiles must all be resident at once).
 template <int DD_ROWS>
-__global__ void __launch_bounds__(32 * DD_WARPS) k_dedupe(const BatchDesc *__restrict__ bd, uint32_t *bar) {
+__global__ void __launch_bounds__(32 * DD_WARPS) k_dedupe(const BatchDesc *__restrict__ bd, int m0, int m1,
+                                                          uint32_t *bar) {
   const int lane = threadIdx.x & 31;
-  const uint32_t gtile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nmaps = bd->n;
-  int m = 0;
-  while (m < nmaps - 1 && gtile >= bd->tile_end[m]) m++;
+  const uint32_t base = m0 ? bd->tile_end[m0 - 1] : 0u;
+  const uint32_t gtile = base + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  int m = m0;
+  while (m < m1 - 1 && gtile >= bd->tile_end[m]) m++;
   const MapFrame &F = bd->f[m];
   const int tile = (int)(gtile - (m ? bd->tile_end[m - 1] : 0u));
-  const bool active = gtile < bd->tile_end[nmaps - 1];  // warps past the last tile only join the barriers
+  const bool active = gtile < bd->tile_end[m1 - 1];  // warps past the last tile only join the barriers
   const uint16_t *__restrict__ depth = F.depth;
   const float *__restrict__ pxp = F.pxp;
   const float *__restrict__ pyp = F.pyp;
@@ -257,22 +259,22 @@ __global__ void __launch_bounds__(32 * DD_WARPS) k_dedupe(const BatchDesc *__res
     // counter (round + 1) % 3 was last read before the previous barrier
     if (blockIdx.x == 0 && threadIdx.x == 0) chg[(round + 1) % 3] = 0;
     // a barrier that gives up marks the first map; every map's frame reports it
-    grid_barrier(bar, gridDim.x, bd->f[0].cnt);
+    grid_barrier(bar, gridDim.x, bd->f[m0].cnt);
     const uint32_t any = chg[round % 3];
     if (!any) {
       converged = true;
       break;
     }
-    if (*(volatile uint32_t *)&bd->f[0].cnt->error & ERR_SPIN_TIMEOUT) break;
+    if (*(volatile uint32_t *)&bd->f[m0].cnt->error & ERR_SPIN_TIMEOUT) break;
   }
   if (active && x < W) {
     for (int r = 0; r < rows; r++) processed[(size_t)(ty * DD_ROWS + r) * W + x] = (uint8_t)((bits >> r) & 1u);
   }
-  if (blockIdx.x == 0 && threadIdx.x < nmaps) {
-    Counters *c = bd->f[threadIdx.x].cnt;
+  if (blockIdx.x == 0 && (int)threadIdx.x < m1 - m0) {
+    Counters *c = bd->f[m0 + threadIdx.x].cnt;
     c->dedupe_iters = round + 1;
     if (!converged) atomicOr(&c->error, ERR_DEDUPE_NOT_CONVERGED);
-    if (*(volatile uint32_t *)&bd->f[0].cnt->error & ERR_SPIN_TIMEOUT) atomicOr(&c->error, ERR_SPIN_TIMEOUT);
+    if (*(volatile uint32_t *)&bd->f[m0].cnt->error & ERR_SPIN_TIMEOUT) atomicOr(&c->error, ERR_SPIN_TIMEOUT);
   }
 }
 
@@ -305,24 +307,23 @@ static cudaError_t resident_dedupe_warps(int device, int &warps) {
   return cudaSuccess;
 }
 
-cudaError_t dedupe_tile_rows(uint32_t tiles_short, int device, int &rows) {
-  int warps = 0;
-  cudaError_t e = resident_dedupe_warps<DD_ROWS_SHORT>(device, warps);
-  if (e != cudaSuccess) return e;
-  rows = (int)tiles_short <= warps ? DD_ROWS_SHORT : DD_ROWS_TALL;
-  return cudaSuccess;
-}
-
-cudaError_t launch_dedupe(const BatchDesc *d_batch, uint32_t total_tiles, int rows, uint32_t *barrier, int device,
-                          cudaStream_t s) {
+cudaError_t dedupe_capacity(int device, int rows, uint32_t &tiles) {
   int warps = 0;
   cudaError_t e = rows == DD_ROWS_SHORT ? resident_dedupe_warps<DD_ROWS_SHORT>(device, warps)
                                         : resident_dedupe_warps<DD_ROWS_TALL>(device, warps);
+  tiles = (uint32_t)warps;
+  return e;
+}
+
+cudaError_t launch_dedupe(const BatchDesc *d_batch, int m0, int m1, uint32_t tiles, int rows, uint32_t *barrier,
+                          int device, cudaStream_t s) {
+  uint32_t cap = 0;
+  cudaError_t e = dedupe_capacity(device, rows, cap);
   if (e != cudaSuccess) return e;
   // one warp per tile, all resident at once
-  const int blocks = (int)((total_tiles + DD_WARPS - 1) / DD_WARPS);
-  if (blocks * DD_WARPS > warps || blocks < 1) return cudaErrorInvalidConfiguration;
-  void *args[] = {(void *)&d_batch, (void *)&barrier};
+  const int blocks = (int)((tiles + DD_WARPS - 1) / DD_WARPS);
+  if ((uint32_t)blocks * DD_WARPS > cap || blocks < 1) return cudaErrorInvalidConfiguration;
+  void *args[] = {(void *)&d_batch, (void *)&m0, (void *)&m1, (void *)&barrier};
   note_launch();
   const void *fn = rows == DD_ROWS_SHORT ? (const void *)k_dedupe<DD_ROWS_SHORT> : (const void *)k_dedupe<DD_ROWS_TALL>;
   return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(32 * DD_WARPS), args, 0, s);

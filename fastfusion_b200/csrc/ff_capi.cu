@@ -25,6 +25,9 @@ std::atomic<unsigned long long> g_own_launches{0}, g_lib_calls{0};
 
 using namespace ffb;
 
+// grid-barrier words: 8 per de-duplication launch of a batch
+constexpr int BARRIER_WORDS = 8 * BATCH_MAX;
+
 struct ff_handle {
   ff_config cfg;
   std::string err;
@@ -346,7 +349,7 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
       }
     }
     if (alloc(&h->d_col, L * 1536) != cudaSuccess) { fail(FF_ERR_OOM_POOL, "colour pool"); break; }
-    if (alloc(&h->d_cnt, 1) != cudaSuccess || alloc(&h->d_barrier, 8) != cudaSuccess) { fail(FF_ERR_CUDA, "counters"); break; }
+    if (alloc(&h->d_cnt, 1) != cudaSuccess || alloc(&h->d_barrier, BARRIER_WORDS) != cudaSuccess) { fail(FF_ERR_CUDA, "counters"); break; }
     if (cudaMallocHost((void **)&h->h_cnt, sizeof(Counters)) != cudaSuccess) { fail(FF_ERR_CUDA, "pinned"); break; }
     if (cudaMalloc((void **)&h->d_batch, sizeof(BatchDesc)) != cudaSuccess ||
         cudaMallocHost((void **)&h->h_batch, sizeof(BatchDesc)) != cudaSuccess) {
@@ -561,11 +564,18 @@ static ff_status frame_launch(ff_handle *lead, int n) {
   cudaStream_t s = lead->stream;
   BatchDesc &B = *lead->h_batch;
   B.n = n;
-  uint32_t tiles16 = 0;
+  // 16-row tiles when they fit one cooperative launch, else 32-row tiles in
+  // as many launches (groups of whole maps) as needed
+  uint32_t tiles16 = 0, cap16 = 0, cap32 = 0;
   for (int i = 0; i < n; i++) tiles16 += (uint32_t)dedupe_tiles(B.f[i].W, B.f[i].H, nullptr, nullptr, 16);
-  int rows = 16;
-  CK(dedupe_tile_rows(tiles16, lead->cfg.device, rows));
-  for (int i = 0; i < n; i++) dedupe_tiles(B.f[i].W, B.f[i].H, &B.f[i].tilesX, &B.f[i].tilesY, rows);
+  CK(dedupe_capacity(lead->cfg.device, 16, cap16));
+  CK(dedupe_capacity(lead->cfg.device, 32, cap32));
+  const int rows = tiles16 <= cap16 ? 16 : 32;
+  const uint32_t cap = rows == 16 ? cap16 : cap32;
+  for (int i = 0; i < n; i++) {
+    const uint32_t nt = (uint32_t)dedupe_tiles(B.f[i].W, B.f[i].H, &B.f[i].tilesX, &B.f[i].tilesY, rows);
+    if (nt > cap) return set_err(lead, FF_ERR_BAD_ARG, "image too large for the de-duplication launch");
+  }
   int rounds = 1;
   uint32_t tiles = 0, pix = 0;
   for (int i = 0; i < n; i++) {
@@ -577,11 +587,19 @@ static ff_status frame_launch(ff_handle *lead, int n) {
   }
   B.max_rounds = rounds;
   CK(cudaMemcpyAsync(lead->d_batch, lead->h_batch, batch_desc_bytes(n), cudaMemcpyHostToDevice, s));
-  CK(cudaMemsetAsync(lead->d_barrier, 0, 8 * sizeof(uint32_t), s));
+  CK(cudaMemsetAsync(lead->d_barrier, 0, BARRIER_WORDS * sizeof(uint32_t), s));
   double npix = 0;
   for (int i = 0; i < n; i++) npix += (double)B.f[i].npix;
   int pi = lead->prof.begin(ST_DEDUPE, s);
-  CK(launch_dedupe(lead->d_batch, tiles, rows, lead->d_barrier, lead->cfg.device, s));
+  for (int m0 = 0, launch = 0; m0 < n; launch++) {
+    int m1 = m0;
+    uint32_t group = 0;
+    while (m1 < n && group + (uint32_t)(B.f[m1].tilesX * B.f[m1].tilesY) <= cap)
+      group += (uint32_t)(B.f[m1].tilesX * B.f[m1].tilesY), m1++;
+    if (launch >= BARRIER_WORDS / 8) return set_err(lead, FF_ERR_BAD_ARG, "batch too large for the de-duplication");
+    CK(launch_dedupe(lead->d_batch, m0, m1, group, rows, lead->d_barrier + 8 * launch, lead->cfg.device, s));
+    m0 = m1;
+  }
   lead->prof.end(pi, npix * (2 + 16 + 1), s);  // depth in; voxel keys and processed flags out
   pi = lead->prof.begin(ST_INSERT, s);
   launch_insert(lead->d_batch, pix, s);

@@ -70,15 +70,17 @@ void launch_first_bbox(const uint16_t *depth, int W, int H, const CamF &p, float
 // the tile grid); 16-row tiles unless the batch has more of them than warps
 // can be resident, then 32-row tiles (dedupe_tile_rows).
 int dedupe_tiles(int W, int H, int *tilesX, int *tilesY, int rows);
-cudaError_t dedupe_tile_rows(uint32_t tiles_short, int device, int &rows);
+// Tiles one cooperative de-duplication launch holds (all warps resident).
+cudaError_t dedupe_capacity(int device, int rows, uint32_t &tiles);
 // int4 elements of the boundary buffer launch_dedupe needs for a W x H image.
 size_t dedupe_boundary_elems(int W, int H);
 // Per-pixel voxel coordinates, validity and target brick scale (written to
 // each frame's vox), then the row/column de-duplication of brick keys
 // (traversal_wrapper_functions.cpp:613-639, 688-690), for every frame of the
-// batch in one cooperative launch.  barrier: 8 zeroed uint32 words.
-cudaError_t launch_dedupe(const BatchDesc *d_batch, uint32_t total_tiles, int rows, uint32_t *barrier, int device,
-                          cudaStream_t s);
+// batch in one cooperative launch per group of maps [m0, m1) whose `tiles`
+// fit the launch.  barrier: 8 zeroed uint32 words per launch.
+cudaError_t launch_dedupe(const BatchDesc *d_batch, int m0, int m1, uint32_t tiles, int rows, uint32_t *barrier,
+                          int device, cudaStream_t s);
 
 // Octree descent / allocation of every processed pixel of the batch.
 void launch_insert(const BatchDesc *d_batch, uint32_t total_pix, cudaStream_t s);
