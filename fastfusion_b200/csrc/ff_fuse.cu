@@ -67,6 +67,19 @@ __device__ __forceinline__ void fuse_brick(const uint32_t brick, const ushort4 *
   const int v = threadIdx.x;
   const int x = v & 7, y = (v >> 3) & 7, z = v >> 6;
   const ushort4 o = leaf[brick];
+  // the voxel's stored state does not depend on the projection: load it first
+  // so that its latency overlaps the arithmetic and the image gathers
+  const size_t vi = (size_t)brick * 512 + v;
+  float wAcc, dAcc;
+  if (FP16) {
+    wAcc = __half2float(wgt16[vi]);
+    dAcc = __half2float(sdf16[vi]);
+  } else {
+    wAcc = wgt[vi];
+    dAcc = sdf[vi];
+  }
+  uint16_t *cb = col + (size_t)brick * 1536 + v;
+  const uint16_t acc0 = cb[0], acc1 = cb[512], acc2 = cb[1024];
   const float *M = q.r;
   const float ls = (float)o.w;
   const float fls = __fmul_rz(ls, scale);
@@ -113,15 +126,6 @@ __device__ __forceinline__ void fuse_brick(const uint32_t brick, const ushort4 *
   const float fall = __fmul_rz(__fsub_rz(thrW, dInc), rcp_upd<RCP_HOST>(__fsub_rz(thrW, DIST_W_EPS), rtab, rshift));
   const float wInc = mask ? __fadd_rz(front, __fmul_rz(fall, back)) : 0.0f;
 
-  const size_t vi = (size_t)brick * 512 + v;
-  float wAcc, dAcc;
-  if (FP16) {
-    wAcc = __half2float(wgt16[vi]);
-    dAcc = __half2float(sdf16[vi]);
-  } else {
-    wAcc = wgt[vi];
-    dAcc = sdf[vi];
-  }
   const float wNew = __fadd_rz(wAcc, wInc);
   const float factor = rcp_upd<RCP_HOST>(__fadd_rz(wNew, wNew <= 0.0f ? 1.0f : 0.0f), rtab, rshift);
   float tr = dInc < thrD ? dInc : thrD;
@@ -139,10 +143,10 @@ __device__ __forceinline__ void fuse_brick(const uint32_t brick, const ushort4 *
   const uint8_t *p8 = bgr + 3 * (size_t)ii;
   const float inc[3] = {__fmul_rz((float)__ldg(p8 + 2), COLOR_MUL), __fmul_rz((float)__ldg(p8 + 1), COLOR_MUL),
                         __fmul_rz((float)__ldg(p8 + 0), COLOR_MUL)};
-  uint16_t *cb = col + (size_t)brick * 1536 + v;
+  const uint16_t accs[3] = {acc0, acc1, acc2};
 #pragma unroll
   for (int c = 0; c < 3; c++) {
-    const float acc = (float)cb[c * 512];
+    const float acc = (float)accs[c];
     float val = __fmul_rz(__fadd_rz(__fmul_rz(acc, wAcc), __fmul_rz(inc[c], wInc)), factor);
     val = val < 65280.0f ? val : 65280.0f;
     cb[c * 512] = (uint16_t)__float2int_rz(val);
@@ -180,13 +184,22 @@ __global__ void __launch_bounds__(512) k_fuse(const BatchDesc *__restrict__ bd, 
   }
   __syncthreads();
   const uint32_t total = end[nmaps - 1];
-  int m = 0;
+  // the current map's camera parameters, shared by the block
+  __shared__ CamF sq;
+  int m = 0, staged = -1;
   for (uint32_t b = blockIdx.x; b < total; b += gridDim.x) {
     while (b >= end[m]) m++;
     const MapFrame &F = bd->f[m];
+    if (m != staged) {  // block-uniform
+      __syncthreads();
+      if (threadIdx.x < sizeof(CamF) / sizeof(float))
+        reinterpret_cast<float *>(&sq)[threadIdx.x] = reinterpret_cast<const float *>(&F.q)[threadIdx.x];
+      __syncthreads();
+      staged = m;
+    }
     const uint32_t local = b - (m ? end[m - 1] : 0u);
     fuse_brick<FP16, RCP_HOST>(F.queue[local], F.leaf, F.sdf, F.wgt, F.sdf16, F.wgt16, F.col, F.depth, F.bgr, F.W,
-                               F.H, F.q, F.scale, F.thr, F.scaling, F.maxcam, F.rcp_tab, F.rcp_shift);
+                               F.H, sq, F.scale, F.thr, F.scaling, F.maxcam, F.rcp_tab, F.rcp_shift);
   }
 }
 
