@@ -171,7 +171,7 @@ __device__ __forceinline__ bool fuse_deferred(const MapFrame &F) {
 // the bricks of every map of the batch in order.  Gated: each map's count is
 // read on the device; otherwise the host's count (nq_host) is used.
 template <bool FP16, bool RCP_HOST>
-__global__ void __launch_bounds__(512) k_fuse(const BatchDesc *__restrict__ bd, int gated) {
+__global__ void __launch_bounds__(512, 4) k_fuse(const BatchDesc *__restrict__ bd, int gated) {
   __shared__ uint32_t end[BATCH_MAX];  // inclusive prefix of the maps' brick counts
   const int nmaps = bd->n;
   if (threadIdx.x == 0) {
