@@ -64,6 +64,7 @@ STAGE_KERNELS = {
     "mesh_cells": "k_gen_level+k_cell_keys+radix sort+k_gather_cells",
     "mesh_count": "k_mesh_lattice<count>+k_mesh_corner<count>",
     "mesh_emit": "k_mesh_lattice<emit>+k_mesh_corner<emit>+k_copy_clean",
+    "confidence": "k_cnn_features+k_conv x3 (learned weight)",
 }
 
 
@@ -76,6 +77,8 @@ def parse_args(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--storage", choices=["fp32", "fp16"], default="fp32")
     ap.add_argument("--rcp", choices=["host", "exact"], default="host")
+    ap.add_argument("--weight", choices=["plain", "learned"], default="plain",
+                    help="learned: the trained per-pixel confidence network weights every frame")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workers", type=int, default=0, help="reference arm: maps in parallel (0 = all cores)")
@@ -129,6 +132,7 @@ def workload_config(a, n_frames: int) -> dict:
         "maxcam_m": MAXCAM,
         "storage": a.storage,
         "rcp": a.rcp,
+        "weight": getattr(a, "weight", "plain"),
         "seed": a.seed,
         "l2": "flushed between timed steps (256 MB write)",
     }
@@ -256,6 +260,10 @@ def run_b200(a):
         if world > 1:
             dist.barrier()
 
+    learned = None
+    if a.weight == "learned":
+        from fastfusion_b200.confidence import load_weights
+        learned = load_weights()
     nf = n_frames_needed(a)
     seq = make_sequence(a.seed + rank, nf)
     depth, bgr = render_frames(seq, nf, dev)
@@ -267,6 +275,8 @@ def run_b200(a):
     def new_map():
         m = ff.FusionMipMapCPU(0, 0, 0, VOXEL, THRESHOLD, 0, True, device=local, storage=a.storage, rcp=a.rcp)
         m.set_stream(stream.cuda_stream)
+        if a.weight == "learned":
+            m.set_confidence(*learned)
         return m
 
     def device_step(m, s):

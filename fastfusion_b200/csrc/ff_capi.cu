@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -77,6 +78,15 @@ struct ff_handle {
   uint32_t frames = 0, queued = 0, grows = 0, processed = 0, new_leaves = 0, dedupe_rounds = 0;
   bool meshing_ok = true;
   uint16_t bandwidth = 0;
+
+  // learned confidence weight (ff_set_confidence): BF16 parameters, and the
+  // per-frame features, activations and confidence map
+  __nv_bfloat16 *d_cnn_params = nullptr;
+  float conf_tau_cm = 0.0f;  // > 0: the learned weight is on
+  __nv_bfloat16 *d_feat = nullptr, *d_a1 = nullptr, *d_a2 = nullptr;
+  float *d_conf = nullptr;
+  size_t conf_cap = 0;  // pixels the buffers hold
+  int conf_w = 0, conf_h = 0;  // size of the last confidence map
 
   MeshState mesh;
   Prof prof;
@@ -404,7 +414,8 @@ ff_status ff_destroy(ff_handle *h) {
   h->prof.destroy();
   void *ptrs[] = {h->d_tree, h->d_leaf, h->d_parent, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
                   h->d_stamp, h->d_queue, h->d_cnt, h->d_barrier, h->d_depth, h->d_bgr, h->d_pxp, h->d_pyp,
-                  h->d_vox, h->d_proc, h->d_bnd, h->d_pend, h->d_keys, h->d_sort_tmp, h->d_rcp_tab};
+                  h->d_vox, h->d_proc, h->d_bnd, h->d_pend, h->d_keys, h->d_sort_tmp, h->d_rcp_tab,
+                  h->d_cnn_params, h->d_feat, h->d_a1, h->d_a2, h->d_conf};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->h_cnt) cudaFreeHost(h->h_cnt);
@@ -554,6 +565,34 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
   mf.cnt = h->d_cnt;
   mf.rcp_tab = h->d_rcp_tab;
   mf.rcp_shift = h->rcp_shift;
+  mf.conf = nullptr;
+  if (h->conf_tau_cm > 0.0f) {
+    // the frame's confidence map, ahead of the launches that read it on this stream
+    const size_t npx = (size_t)W * H;
+    if (npx > h->conf_cap) {
+      cudaFree(h->d_feat);
+      cudaFree(h->d_a1);
+      cudaFree(h->d_a2);
+      cudaFree(h->d_conf);
+      h->d_feat = h->d_a1 = h->d_a2 = nullptr;
+      h->d_conf = nullptr;
+      h->conf_cap = 0;
+      CK(alloc(&h->d_feat, npx * CNN_FEAT_CH));
+      CK(alloc(&h->d_a1, npx * CNN_HIDDEN));
+      CK(alloc(&h->d_a2, npx * CNN_HIDDEN));
+      CK(alloc(&h->d_conf, npx));
+      h->conf_cap = npx;
+    }
+    const float kf[4] = {(float)K[0], (float)K[1], (float)K[2], (float)K[3]};
+    const int pc = h->prof.begin(ST_CONFIDENCE, s);
+    CK(cnn_features(d_depth, 1, W, H, scaling, kf, h->d_feat, s));
+    CK(cnn_forward(h->d_cnn_params, h->d_feat, 1, W, H, h->d_a1, h->d_a2, h->d_conf, h->conf_tau_cm, s));
+    // depth -> features -> a1 -> a2 -> confidence, each written once and read once
+    h->prof.end(pc, (double)npx * ((2 + 16) + (16 + 32) + (32 + 32) + (32 + 4)), s);
+    h->conf_w = W;
+    h->conf_h = H;
+    mf.conf = h->d_conf;
+  }
   return FF_OK;
 }
 
@@ -1107,3 +1146,138 @@ ff_status ff_get_mesh_device(ff_handle *h, const float **xyz, const uint8_t **rg
 }
 
 }  // extern "C"
+
+// ------------------------------------------------- learned confidence weight
+
+// FP32 -> BF16, round to nearest even (NaN kept quiet).
+static uint16_t bf16_bits(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  if ((u & 0x7F800000u) == 0x7F800000u && (u & 0x007FFFFFu)) return (uint16_t)((u >> 16) | 0x0040u);
+  const uint32_t lsb = (u >> 16) & 1u;
+  u += 0x7FFFu + lsb;
+  return (uint16_t)(u >> 16);
+}
+
+ff_status ff_set_confidence(ff_handle *h, const float *params, int n_params, float tau_m) {
+  if (!h) return FF_ERR_BAD_ARG;
+  if (!params) {
+    h->conf_tau_cm = 0.0f;
+    return FF_OK;
+  }
+  if (n_params != FF_CNN_PARAMS || !(tau_m > 0.0f) || !std::isfinite(tau_m))
+    return set_err(h, FF_ERR_BAD_ARG, "ff_set_confidence: expected FF_CNN_PARAMS parameters and tau > 0");
+  for (int i = 0; i < n_params; i++)
+    if (!std::isfinite(params[i])) return set_err(h, FF_ERR_BAD_ARG, "ff_set_confidence: non-finite parameter");
+  CK(cudaSetDevice(h->cfg.device));
+  std::vector<uint16_t> b(n_params);
+  for (int i = 0; i < n_params; i++) b[i] = bf16_bits(params[i]);
+  if (!h->d_cnn_params) CK(alloc(&h->d_cnn_params, (size_t)FF_CNN_PARAMS));
+  CK(cudaMemcpyAsync(h->d_cnn_params, b.data(), sizeof(uint16_t) * n_params, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->conf_tau_cm = tau_m * 100.0f;
+  return FF_OK;
+}
+
+ff_status ff_get_confidence_map(ff_handle *h, float *out, int *width, int *height) {
+  if (!h) return FF_ERR_BAD_ARG;
+  if (!(h->conf_tau_cm > 0.0f) || !h->d_conf || !h->conf_w)
+    return set_err(h, FF_ERR_BAD_ARG, "ff_get_confidence_map: no learned weight or no frame yet");
+  if (width) *width = h->conf_w;
+  if (height) *height = h->conf_h;
+  if (out) {
+    CK(cudaSetDevice(h->cfg.device));
+    CK(cudaMemcpyAsync(out, h->d_conf, sizeof(float) * (size_t)h->conf_w * h->conf_h, cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  return FF_OK;
+}
+
+ff_status ff_raycast_depth(ff_handle *h, const double K[4], const double R[9], const double t[3],
+                           const uint16_t *d_depth, int width, int height, float scaling, float window_m,
+                           float step_m, float *d_out) {
+  if (!h) return FF_ERR_BAD_ARG;
+  if (!K || !R || !t || !d_depth || !d_out || width <= 0 || height <= 0)
+    return set_err(h, FF_ERR_BAD_ARG, "ff_raycast_depth: NULL pointer or empty image");
+  if (!(window_m > 0.0f && window_m <= 4.0f) || !(step_m >= 1e-4f && step_m <= window_m))
+    return set_err(h, FF_ERR_BAD_ARG, "ff_raycast_depth: window must be in (0, 4] m and step in [1e-4, window]");
+  if (!h->n) return set_err(h, FF_ERR_BAD_ARG, "ff_raycast_depth: the map holds no frame");
+  CK(cudaSetDevice(h->cfg.device));
+  RaycastMap m;
+  m.tree = h->d_tree;
+  m.leaf = h->d_leaf;
+  m.sdf = h->d_sdf;
+  m.wgt = h->d_wgt;
+  m.sdf16 = h->d_sdf16;
+  m.wgt16 = h->d_wgt16;
+  m.n = h->n;
+  m.leaves_max = std::min(h->leaves_used, h->cfg.leaves_max);  // leaves with storage
+  m.fp16 = h->cfg.storage == FF_STORAGE_FP16;
+  m.thr = h->cfg.threshold;
+  const CamF p = cam_world_to_grid(h, K, R, t);
+  CK(launch_raycast(m, p, width, height, d_depth, scaling, window_m, step_m, d_out, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return FF_OK;
+}
+
+// Training entry points: device pointers owned by the caller, work on the
+// caller's stream; errors are reported through ff_last_error(NULL).
+#define CKN(call)                                                                     \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess) {                                                          \
+      g_create_error = std::string(#call) + ": " + cudaGetErrorString(e_);            \
+      return FF_ERR_CUDA;                                                             \
+    }                                                                                 \
+  } while (0)
+
+static ff_status cnn_bad(const char *m) {
+  g_create_error = m;
+  return FF_ERR_BAD_ARG;
+}
+
+ff_status ff_cnn_features(const uint16_t *d_depth, int n, int width, int height, float scaling, const double K[4],
+                          void *d_feat, void *stream) {
+  if (!d_depth || !K || !d_feat || n <= 0 || width <= 0 || height <= 0) return cnn_bad("ff_cnn_features: bad argument");
+  const float kf[4] = {(float)K[0], (float)K[1], (float)K[2], (float)K[3]};
+  CKN(cnn_features(d_depth, n, width, height, scaling, kf, (__nv_bfloat16 *)d_feat, (cudaStream_t)stream));
+  return FF_OK;
+}
+
+ff_status ff_cnn_forward(const void *d_params, const void *d_feat, int n, int width, int height, void *d_a1,
+                         void *d_a2, float *d_out, float tau_m, void *stream) {
+  if (!d_params || !d_feat || !d_a1 || !d_a2 || !d_out || n <= 0 || width <= 0 || height <= 0)
+    return cnn_bad("ff_cnn_forward: bad argument");
+  CKN(cnn_forward((const __nv_bfloat16 *)d_params, (const __nv_bfloat16 *)d_feat, n, width, height,
+                  (__nv_bfloat16 *)d_a1, (__nv_bfloat16 *)d_a2, d_out, tau_m > 0.0f ? tau_m * 100.0f : 0.0f,
+                  (cudaStream_t)stream));
+  return FF_OK;
+}
+
+ff_status ff_cnn_backward(const void *d_params, const void *d_feat, const void *d_a1, const void *d_a2,
+                          const float *d_dpred, int n, int width, int height, float *d_g1, float *d_g2,
+                          float *d_grads, void *stream) {
+  if (!d_params || !d_feat || !d_a1 || !d_a2 || !d_dpred || !d_g1 || !d_g2 || !d_grads || n <= 0 || width <= 0 ||
+      height <= 0)
+    return cnn_bad("ff_cnn_backward: bad argument");
+  CKN(cnn_backward((const __nv_bfloat16 *)d_params, (const __nv_bfloat16 *)d_feat, (const __nv_bfloat16 *)d_a1,
+                   (const __nv_bfloat16 *)d_a2, d_dpred, n, width, height, d_g1, d_g2, d_grads,
+                   (cudaStream_t)stream));
+  return FF_OK;
+}
+
+ff_status ff_cnn_mse(const float *d_pred, const float *d_target, int64_t count, float inv_count, float *d_dpred,
+                     double *d_loss, void *stream) {
+  if (!d_pred || !d_target || !d_dpred || !d_loss || count <= 0) return cnn_bad("ff_cnn_mse: bad argument");
+  CKN(cnn_mse(d_pred, d_target, count, inv_count, d_dpred, d_loss, (cudaStream_t)stream));
+  return FF_OK;
+}
+
+ff_status ff_cnn_adam(float *d_master, void *d_params, float *d_grads, float *d_m, float *d_v, float lr,
+                      float beta1, float beta2, float eps, int step, void *stream) {
+  if (!d_master || !d_params || !d_grads || !d_m || !d_v || step < 1) return cnn_bad("ff_cnn_adam: bad argument");
+  CKN(cnn_adam(d_master, (__nv_bfloat16 *)d_params, d_grads, d_m, d_v, FF_CNN_PARAMS, lr, beta1, beta2, eps, step,
+               (cudaStream_t)stream));
+  return FF_OK;
+}

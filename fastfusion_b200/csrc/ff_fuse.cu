@@ -63,7 +63,7 @@ __device__ __forceinline__ void fuse_brick(const uint32_t brick, const ushort4 *
                                            uint16_t *__restrict__ col, const uint16_t *__restrict__ depth,
                                            const uint8_t *__restrict__ bgr, int W, int H, const CamF &q, float scale,
                                            float thr, float scaling, float maxcam, const uint32_t *__restrict__ rtab,
-                                           int rshift) {
+                                           int rshift, const float *__restrict__ conf) {
   const int v = threadIdx.x;
   const int x = v & 7, y = (v >> 3) & 7, z = v >> 6;
   const ushort4 o = leaf[brick];
@@ -124,7 +124,9 @@ __device__ __forceinline__ void fuse_brick(const uint32_t brick, const ushort4 *
   const float front = dInc < DIST_W_EPS ? 1.0f : 0.0f;
   const float back = (dInc >= DIST_W_EPS && dInc < thrW) ? 1.0f : 0.0f;
   const float fall = __fmul_rz(__fsub_rz(thrW, dInc), rcp_upd<RCP_HOST>(__fsub_rz(thrW, DIST_W_EPS), rtab, rshift));
-  const float wInc = mask ? __fadd_rz(front, __fmul_rz(fall, back)) : 0.0f;
+  float wInc = mask ? __fadd_rz(front, __fmul_rz(fall, back)) : 0.0f;
+  // learned weight: the ramp's increment scaled by the pixel's confidence
+  if (conf) wInc = __fmul_rz(wInc, __ldg(conf + ii));
 
   const float wNew = __fadd_rz(wAcc, wInc);
   const float factor = rcp_upd<RCP_HOST>(__fadd_rz(wNew, wNew <= 0.0f ? 1.0f : 0.0f), rtab, rshift);
@@ -199,7 +201,7 @@ __global__ void __launch_bounds__(512, 4) k_fuse(const BatchDesc *__restrict__ b
     }
     const uint32_t local = b - (m ? end[m - 1] : 0u);
     fuse_brick<FP16, RCP_HOST>(F.queue[local], F.leaf, F.sdf, F.wgt, F.sdf16, F.wgt16, F.col, F.depth, F.bgr, F.W,
-                               F.H, sq, F.scale, F.thr, F.scaling, F.maxcam, F.rcp_tab, F.rcp_shift);
+                               F.H, sq, F.scale, F.thr, F.scaling, F.maxcam, F.rcp_tab, F.rcp_shift, F.conf);
   }
 }
 

@@ -1,5 +1,6 @@
 // Host-side launchers of the fusion-path kernels (internal to the library).
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -40,6 +41,7 @@ struct MapFrame {
   Counters *cnt;
   const uint32_t *rcp_tab;
   int rcp_shift;
+  const float *conf;  // learned per-pixel confidence of the frame, or null (the reference's weight)
 };
 
 constexpr int BATCH_MAX = 32;
@@ -129,5 +131,37 @@ void launch_fuse(const BatchDesc *d_batch, int nmaps, bool gated, int storage, b
 // when the host is not x86-64 or the instruction does not follow the
 // expected rules.
 bool build_rcp_table(std::vector<uint32_t> &tab, int &shift);
+
+// ---- learned confidence weight (ff_cnn.cu) ----
+
+constexpr int CNN_PARAMS = 8833;   // W1[16][5][25] b1[16] W2[16][16][25] b2[16] W3[1][16][25] b3[1]
+constexpr int CNN_FEAT_CH = 8;     // channels per pixel of the feature map (5 used)
+constexpr int CNN_HIDDEN = 16;
+
+// The fused volume as the raycaster reads it.
+struct RaycastMap {
+  const uint32_t *tree;
+  const ushort4 *leaf;
+  const float *sdf, *wgt;
+  const __half *sdf16, *wgt16;
+  uint32_t n, leaves_max;
+  int fp16;
+  float thr;  // truncation distance (m) of scale-1 bricks
+};
+
+cudaError_t cnn_features(const uint16_t *depth, int n, int W, int H, float scaling, const float K[4],
+                         __nv_bfloat16 *feat, cudaStream_t s);
+// tau_cm > 0: out = the confidence weight; else out = the network's output
+cudaError_t cnn_forward(const __nv_bfloat16 *params, const __nv_bfloat16 *feat, int n, int W, int H,
+                        __nv_bfloat16 *a1, __nv_bfloat16 *a2, float *out, float tau_cm, cudaStream_t s);
+cudaError_t cnn_backward(const __nv_bfloat16 *params, const __nv_bfloat16 *feat, const __nv_bfloat16 *a1,
+                         const __nv_bfloat16 *a2, const float *dpred, int n, int W, int H, float *g1, float *g2,
+                         float *grads, cudaStream_t s);
+cudaError_t cnn_mse(const float *pred, const float *target, int64_t count, float inv_count, float *dpred,
+                    double *loss, cudaStream_t s);
+cudaError_t cnn_adam(float *master, __nv_bfloat16 *params, float *grads, float *m, float *v, int n, float lr,
+                     float b1, float b2, float eps, int step, cudaStream_t s);
+cudaError_t launch_raycast(const RaycastMap &m, const CamF &p, int W, int H, const uint16_t *depth, float scaling,
+                           float window, float step, float *out, cudaStream_t s);
 
 }  // namespace ffb

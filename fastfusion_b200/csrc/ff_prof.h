@@ -18,6 +18,7 @@ enum Stage {
   ST_MESH_CELLS,
   ST_MESH_COUNT,
   ST_MESH_EMIT,
+  ST_CONFIDENCE,  // learned weight: features and the three convolution layers
   ST_COUNT
 };
 

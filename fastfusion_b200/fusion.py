@@ -82,6 +82,14 @@ SIGNATURES = {
     "ff_profile": (_i32, [_vp, _i32]),
     "ff_kernel_launches": (_i32, [ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
     "ff_profile_read": (_i32, [_vp, _vp, _vp, _vp]),
+    "ff_set_confidence": (_i32, [_vp, _vp, _i32, _f32]),
+    "ff_get_confidence_map": (_i32, [_vp, _vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32)]),
+    "ff_raycast_depth": (_i32, [_vp, _vp, _vp, _vp, _vp, _i32, _i32, _f32, _f32, _f32, _vp]),
+    "ff_cnn_features": (_i32, [_vp, _i32, _i32, _i32, _f32, _vp, _vp, _vp]),
+    "ff_cnn_forward": (_i32, [_vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp, _f32, _vp]),
+    "ff_cnn_backward": (_i32, [_vp, _vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp]),
+    "ff_cnn_mse": (_i32, [_vp, _vp, ctypes.c_int64, _f32, _vp, _vp, _vp]),
+    "ff_cnn_adam": (_i32, [_vp, _vp, _vp, _vp, _vp, _f32, _f32, _f32, _f32, _i32, _vp]),
     "ff_last_error": (ctypes.c_char_p, [_vp]),
     "ff_version": (ctypes.c_char_p, []),
 }
@@ -367,7 +375,36 @@ class FusionMipMapCPU:
         self._check(self._L.ff_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)))
 
     # -- profiling ----------------------------------------------------------
-    PROFILE_STAGES = ("grow", "dedupe", "insert", "finalize", "fuse", "mesh_cells", "mesh_count", "mesh_emit")
+    PROFILE_STAGES = ("grow", "dedupe", "insert", "finalize", "fuse", "mesh_cells", "mesh_count", "mesh_emit",
+                      "confidence")
+
+    def set_confidence(self, params, tau_m: float = 0.03):
+        """Learned per-pixel weight: the network's FF_CNN_PARAMS parameters
+        (rounded to BF16 by the library) and the residual tau (m) at which a
+        pixel's weight reaches zero; None turns it off (the reference's
+        weight)."""
+        if params is None:
+            self._check(self._L.ff_set_confidence(self._h, None, 0, 0.0))
+            return
+        p = np.ascontiguousarray(params, dtype=np.float32).reshape(-1)
+        self._check(self._L.ff_set_confidence(self._h, _p(p), int(p.size), float(tau_m)))
+
+    def confidence_map(self) -> np.ndarray:
+        """The last frame's per-pixel confidence (H x W float32)."""
+        w, h = _i32(0), _i32(0)
+        self._check(self._L.ff_get_confidence_map(self._h, None, ctypes.byref(w), ctypes.byref(h)))
+        out = np.empty((h.value, w.value), np.float32)
+        self._check(self._L.ff_get_confidence_map(self._h, _p(out), None, None))
+        return out
+
+    def raycast_depth(self, d_depth: int, width: int, height: int, caminfo: CameraInfo, d_out: int,
+                      scaling: float = 1.0 / 5000.0, window_m: float = 0.15, step_m: float = 0.0025):
+        """Depth of the fused surface along each pixel's ray near its measured
+        depth (device pointers: uint16 depth in, float metres out; 0 = no
+        depth, -1 = no surface within the window)."""
+        pK, pR, pt = caminfo._ptrs
+        self._check(self._L.ff_raycast_depth(self._h, pK, pR, pt, int(d_depth), int(width), int(height),
+                                             float(scaling), float(window_m), float(step_m), int(d_out)))
 
     def profile(self, enable: bool = True):
         """Reset the per-stage CUDA-event profile and switch it on or off."""

@@ -260,10 +260,15 @@ def room_walk_sequence(seed: int = 0, n_frames: int = 1000, width: int = 640, he
 
 
 def render_torch(scene: Scene, R, t, width: int, height: int, K, seed: int, frame: int, device="cuda",
-                 noise_k: float = 0.0012, hole_frac: float = 0.02):
+                 noise_k: float = 0.0012, hole_frac: float = 0.02, flying_frac: float = 0.0,
+                 flying_m: float = 0.1, edge_m: float = 0.05, return_true: bool = False):
     """render() on a torch device in FP64 (same geometry and colour rules;
     noise and holes from a torch generator seeded by (seed, frame)).
-    Returns (depth uint16 [H,W], bgr uint8 [H,W,3]) as device tensors."""
+    flying_frac: that fraction of the depth-edge pixels (a 4-neighbour more
+    than edge_m away in true depth) is displaced by +-flying_m ("flying
+    pixels"), drawn after the noise and the holes.
+    Returns (depth uint16 [H,W], bgr uint8 [H,W,3]) as device tensors, plus
+    the true depth (float64 [H,W], metres) when return_true."""
     import torch
     dev = torch.device(device)
     f64 = torch.float64
@@ -314,17 +319,29 @@ def render_torch(scene: Scene, R, t, width: int, height: int, K, seed: int, fram
         tbest = torch.where(closer, tmin, tbest)
         colour = torch.where(closer[:, None], rgb[idx], colour)
     z = tbest.reshape(height, width)
+    z_true = z
     g = torch.Generator(device=dev)
     g.manual_seed(int(seed) * 1000003 + int(frame))
     if noise_k > 0:
         z = z + torch.randn(z.shape, generator=g, dtype=f64, device=dev) * noise_k * z * z
     if hole_frac > 0:
         z = torch.where(torch.rand(z.shape, generator=g, dtype=f64, device=dev) < hole_frac, torch.zeros_like(z), z)
+    if flying_frac > 0:
+        zt = torch.nan_to_num(z_true, posinf=1e3)
+        pad = torch.nn.functional.pad(zt[None, None], (1, 1, 1, 1), mode="replicate")[0, 0]
+        jump = torch.zeros_like(zt, dtype=torch.bool)
+        for dy, dx in ((0, 1), (2, 1), (1, 0), (1, 2)):
+            jump |= (pad[dy:dy + height, dx:dx + width] - zt).abs() > edge_m
+        pick = torch.rand(z.shape, generator=g, dtype=f64, device=dev) < flying_frac
+        sign = torch.where(torch.rand(z.shape, generator=g, dtype=f64, device=dev) < 0.5, -1.0, 1.0)
+        z = torch.where(jump & pick & (z > 0), z + sign * flying_m, z)
     z = torch.where(torch.isfinite(z) & (z > 0), z, torch.zeros_like(z))
     depth = torch.round(z * DEPTH_UNITS_PER_M)
     depth = torch.where((z >= 13.1) | (depth > 65535), torch.zeros_like(depth), depth)
     depth = depth.to(torch.int32).to(torch.int16)  # bit pattern of the uint16 value
     bgr = colour.flip(-1).reshape(height, width, 3).contiguous()
+    if return_true:
+        return depth, bgr, z_true
     return depth, bgr
 
 

@@ -202,8 +202,8 @@ ff_status ff_set_state(ff_handle *h, uint32_t n, const float offset[3], const ui
  * number of launches.  Stages, in order: grow (volume extension), dedupe
  * (projection and de-duplication of the pixels), insert, finalize (leaf
  * indices and parents), fuse, mesh_cells (cell generation and sort),
- * mesh_count, mesh_emit. */
-#define FF_PROFILE_STAGES 8
+ * mesh_count, mesh_emit, confidence (the learned weight's network). */
+#define FF_PROFILE_STAGES 9
 ff_status ff_profile(ff_handle *h, int enable);
 ff_status ff_profile_read(ff_handle *h, double *ms, double *bytes, uint64_t *launches);
 
@@ -211,6 +211,63 @@ ff_status ff_profile_read(ff_handle *h, double *ms, double *bytes, uint64_t *lau
  * kernel launches and of its calls into CUB (sort and scan, each of which
  * launches a few library kernels). */
 ff_status ff_kernel_launches(uint64_t *own, uint64_t *library);
+
+/* ---- Learned per-pixel confidence weight (no counterpart in the reference) ----
+ *
+ * The reference weights every pixel's update by the same distance ramp
+ * (update_functions.cpp:1187-1444).  With a confidence network set, each
+ * frame's pixels first go through a 3-layer 5x5 CNN (16 channels; BF16
+ * weights and activations, FP32 accumulation) that predicts the pixel's
+ * depth error r; the ramp's weight increment of every voxel the pixel
+ * updates is multiplied by c = (1 - r/tau)^2 for r < tau, else 0.
+ *
+ * Parameters (FF_CNN_PARAMS floats, in order): W1[16][5][25] b1[16]
+ * W2[16][16][25] b2[16] W3[1][16][25] b3[1]; W[out][in][ky*5+kx] of a 'same'
+ * 5x5 correlation, ReLU after layers 1 and 2.  Input per pixel (8 channels,
+ * 5 used): depth z (m), the unit normal from central differences of the
+ * back-projected 4-neighbours (zero unless all are valid), validity.  Output:
+ * the predicted |depth error| in centimetres. */
+#define FF_CNN_PARAMS 8833
+#define FF_CNN_FEAT_CH 8
+#define FF_CNN_HIDDEN 16
+
+/* Turn the learned weight on for this map (params: FF_CNN_PARAMS floats,
+ * rounded to BF16; tau in metres), or off with params NULL. */
+ff_status ff_set_confidence(ff_handle *h, const float *params, int n_params, float tau_m);
+
+/* The confidence map of the last frame (width x height floats, host memory). */
+ff_status ff_get_confidence_map(ff_handle *h, float *out, int *width, int *height);
+
+/* Depth along each pixel's ray of the first surface of the fused map within
+ * +-window_m of the pixel's measured depth (the SDF of the finest brick,
+ * trilinear inside a brick, sampled every step_m of depth): 0 for pixels
+ * without depth, -1 where no surface lies in the window.  d_depth and d_out are
+ * device memory (uint16 and float, width x height); pose as in ff_add_map_u16. */
+ff_status ff_raycast_depth(ff_handle *h, const double K[4], const double R[9], const double t[3],
+                           const uint16_t *d_depth, int width, int height, float scaling, float window_m,
+                           float step_m, float *d_out);
+
+/* Training and inference kernels of the network on caller-owned device
+ * memory (stream: a cudaStream_t, NULL for the default stream).  n images of
+ * width x height; feat bf16 [n][h][w][8]; a1, a2 bf16 [n][h][w][16]; pred /
+ * dpred / target float [n][h][w]; g1, g2 float [n][h][w][16] (scratch);
+ * params bf16 and grads / master / m / v float [FF_CNN_PARAMS].
+ * ff_cnn_forward writes the confidence when tau_m > 0, else the prediction.
+ * ff_cnn_backward adds the parameter gradients of d(loss)/d(pred) to grads.
+ * ff_cnn_mse: loss += sum over target >= 0 of (pred - target)^2 * inv_count,
+ * dpred = 2 (pred - target) * inv_count (0 where target < 0).
+ * ff_cnn_adam: one Adam step of master, BF16 copy into params, grads cleared. */
+ff_status ff_cnn_features(const uint16_t *d_depth, int n, int width, int height, float scaling, const double K[4],
+                          void *d_feat, void *stream);
+ff_status ff_cnn_forward(const void *d_params, const void *d_feat, int n, int width, int height, void *d_a1,
+                         void *d_a2, float *d_out, float tau_m, void *stream);
+ff_status ff_cnn_backward(const void *d_params, const void *d_feat, const void *d_a1, const void *d_a2,
+                          const float *d_dpred, int n, int width, int height, float *d_g1, float *d_g2,
+                          float *d_grads, void *stream);
+ff_status ff_cnn_mse(const float *d_pred, const float *d_target, int64_t count, float inv_count, float *d_dpred,
+                     double *d_loss, void *stream);
+ff_status ff_cnn_adam(float *d_master, void *d_params, float *d_grads, float *d_m, float *d_v, float lr,
+                      float beta1, float beta2, float eps, int step, void *stream);
 
 /* Message of the last failure on this handle (or of ff_create when h is NULL). */
 const char *ff_last_error(const ff_handle *h);

@@ -48,6 +48,7 @@ struct ffp_map {
   int grows;
   int branch_overflow;
   int rz_exact;
+  const float *conf; /* per-pixel confidence of the next frames (learned weight), or NULL */
   /* mesh of the last ffp_update_meshes */
   ffp_cell *cells;
   int64_t ncells;
@@ -124,6 +125,11 @@ void ffp_destroy(ffp_map *m) {
   free(m->mesh.cell_v);
   free(m);
 }
+
+/* Learned weight: the update's weight increment of every voxel is multiplied
+ * by conf[pixel] (W x H floats of the frames that follow; NULL = the
+ * reference's weight).  The array is borrowed, not copied. */
+void ffp_set_confidence(ffp_map *m, const float *conf) { m->conf = conf; }
 
 void ffp_set_update_mode(ffp_map *m, int mode) {
   m->rz_exact = mode;
@@ -441,6 +447,7 @@ static void update_brick(ffp_map *m, const campams *q, const uint16_t *depth, co
         float back = (dInc >= DIST_W_EPS && dInc < thrW) ? 1.0f : 0.0f;
         float fall = (thrW - dInc) * fallRcp;
         float wInc = mask ? front + fall * back : 0.0f;
+        if (m->conf) wInc = wInc * m->conf[ii];
         float wAcc = m->wgt[idx], dAcc = m->dist[idx];
         float wNew = wAcc + wInc;
         float factor = recip(wNew + (wNew <= 0.0f ? 1.0f : 0.0f));

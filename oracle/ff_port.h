@@ -44,6 +44,8 @@ typedef struct ffp_map ffp_map;
 ffp_map *ffp_create(float scale, float threshold, int color, uint32_t leaves_total, uint32_t branches_total);
 void ffp_destroy(ffp_map *m);
 void ffp_set_update_mode(ffp_map *m, int mode);
+/* Per-pixel confidence multiplying the weight increment (borrowed; NULL: off). */
+void ffp_set_confidence(ffp_map *m, const float *conf);
 
 /* One depth frame (uint16, depth*scaling = metres) with BGR colour.
  * K = {fx, fy, cx, cy}; R (row-major 3x3) and t map camera to world.

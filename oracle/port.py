@@ -34,6 +34,7 @@ def lib():
         L.ffp_create.argtypes = [ctypes.c_float, ctypes.c_float, i32, u32, u32]
         L.ffp_destroy.argtypes = [vp]
         L.ffp_set_update_mode.argtypes = [vp, i32]
+        L.ffp_set_confidence.argtypes = [vp, vp]
         L.ffp_add_map.restype = i32
         L.ffp_add_map.argtypes = [vp, vp, vp, i32, i32, vp, vp, vp, ctypes.c_float, ctypes.c_float]
         L.ffp_state.argtypes = [vp, vp, vp]
@@ -77,6 +78,15 @@ class PortFusion:
             self.close()
         except Exception:
             pass
+
+    def set_confidence(self, conf):
+        """Per-pixel confidence (H x W float32) for the next add_map calls, or None."""
+        if conf is None:
+            self._conf = None
+            lib().ffp_set_confidence(self.h, None)
+            return
+        self._conf = np.ascontiguousarray(conf, dtype=np.float32)
+        lib().ffp_set_confidence(self.h, _p(self._conf))
 
     def add_map(self, depth, bgr, K, R, t, scaling=1.0 / 5000.0, maxcam=4.0) -> int:
         depth = np.ascontiguousarray(depth, dtype=np.uint16)
