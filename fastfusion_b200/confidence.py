@@ -36,6 +36,7 @@ import numpy as np
 from fastfusion_b200 import fusion, scene
 
 N_PARAMS = 8833
+PACKED_BYTES = 33280   # FF_CNN_PACKED_BYTES: the weights as tensor-core operands
 LAYOUT = ((0, 2000), (2000, 16), (2016, 6400), (8416, 16), (8432, 400), (8832, 1))  # W1 b1 W2 b2 W3 b3
 UNIT_M = 0.01          # the network predicts centimetres
 CAP_CM = 15.0          # target cap and the raycast window
@@ -88,6 +89,7 @@ class ConfidenceNet:
         self.m = torch.zeros_like(self.grads)
         self.v = torch.zeros_like(self.grads)
         self.loss = torch.zeros(1, dtype=torch.float64, device=self.dev)
+        self.packed = torch.empty(PACKED_BYTES, dtype=torch.uint8, device=self.dev)
         self.step_no = 0
         self._bufs = {}
 
@@ -126,8 +128,9 @@ class ConfidenceNet:
         n, H, W, _ = feat.shape
         b = self.bufs(n, H, W)
         out = self.torch.empty((n, H, W), dtype=self.torch.float32, device=self.dev)
-        self._check(self.L.ff_cnn_forward(self.params.data_ptr(), feat.data_ptr(), n, W, H, b["a1"].data_ptr(),
-                                          b["a2"].data_ptr(), out.data_ptr(), float(tau_m), _stream()))
+        self._check(self.L.ff_cnn_forward(self.params.data_ptr(), self.packed.data_ptr(), feat.data_ptr(), n, W, H,
+                                          b["a1"].data_ptr(), b["a2"].data_ptr(), out.data_ptr(), float(tau_m),
+                                          _stream()))
         return out
 
     def loss_and_grads(self, feat, target, inv_count: float):
@@ -136,8 +139,8 @@ class ConfidenceNet:
         b = self.bufs(n, H, W)
         self.loss.zero_()
         L, s = self.L, _stream()
-        self._check(L.ff_cnn_forward(self.params.data_ptr(), feat.data_ptr(), n, W, H, b["a1"].data_ptr(),
-                                     b["a2"].data_ptr(), b["pred"].data_ptr(), 0.0, s))
+        self._check(L.ff_cnn_forward(self.params.data_ptr(), self.packed.data_ptr(), feat.data_ptr(), n, W, H,
+                                     b["a1"].data_ptr(), b["a2"].data_ptr(), b["pred"].data_ptr(), 0.0, s))
         self._check(L.ff_cnn_mse(b["pred"].data_ptr(), target.data_ptr(), n * H * W, float(inv_count),
                                  b["dpred"].data_ptr(), self.loss.data_ptr(), s))
         self._check(L.ff_cnn_backward(self.params.data_ptr(), feat.data_ptr(), b["a1"].data_ptr(), b["a2"].data_ptr(),

@@ -82,6 +82,8 @@ struct ff_handle {
   // learned confidence weight (ff_set_confidence): BF16 parameters, and the
   // per-frame features, activations and confidence map
   __nv_bfloat16 *d_cnn_params = nullptr;
+  uint8_t *d_cnn_packed = nullptr;  // the weights as tensor-core operands
+  bool cnn_packed_ready = false;
   float conf_tau_cm = 0.0f;  // > 0: the learned weight is on
   __nv_bfloat16 *d_feat = nullptr, *d_a1 = nullptr, *d_a2 = nullptr;
   float *d_conf = nullptr;
@@ -415,7 +417,7 @@ ff_status ff_destroy(ff_handle *h) {
   void *ptrs[] = {h->d_tree, h->d_leaf, h->d_parent, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
                   h->d_stamp, h->d_queue, h->d_cnt, h->d_barrier, h->d_depth, h->d_bgr, h->d_pxp, h->d_pyp,
                   h->d_vox, h->d_proc, h->d_bnd, h->d_pend, h->d_keys, h->d_sort_tmp, h->d_rcp_tab,
-                  h->d_cnn_params, h->d_feat, h->d_a1, h->d_a2, h->d_conf};
+                  h->d_cnn_params, h->d_cnn_packed, h->d_feat, h->d_a1, h->d_a2, h->d_conf};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->h_cnt) cudaFreeHost(h->h_cnt);
@@ -586,7 +588,9 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
     const float kf[4] = {(float)K[0], (float)K[1], (float)K[2], (float)K[3]};
     const int pc = h->prof.begin(ST_CONFIDENCE, s);
     CK(cnn_features(d_depth, 1, W, H, scaling, kf, h->d_feat, s));
-    CK(cnn_forward(h->d_cnn_params, h->d_feat, 1, W, H, h->d_a1, h->d_a2, h->d_conf, h->conf_tau_cm, s));
+    CK(cnn_forward(h->d_cnn_params, h->d_cnn_packed, h->cnn_packed_ready, h->d_feat, 1, W, H, h->d_a1, h->d_a2,
+                   h->d_conf, h->conf_tau_cm, &h->d_cnt->error, s));
+    h->cnn_packed_ready = true;
     // depth -> features -> a1 -> a2 -> confidence, each written once and read once
     h->prof.end(pc, (double)npx * ((2 + 16) + (16 + 32) + (32 + 32) + (32 + 4)), s);
     h->conf_w = W;
@@ -1173,6 +1177,8 @@ ff_status ff_set_confidence(ff_handle *h, const float *params, int n_params, flo
   std::vector<uint16_t> b(n_params);
   for (int i = 0; i < n_params; i++) b[i] = bf16_bits(params[i]);
   if (!h->d_cnn_params) CK(alloc(&h->d_cnn_params, (size_t)FF_CNN_PARAMS));
+  if (!h->d_cnn_packed) CK(alloc(&h->d_cnn_packed, (size_t)CNN_PACKED_BYTES));
+  h->cnn_packed_ready = false;  // packed by the next frame
   CK(cudaMemcpyAsync(h->d_cnn_params, b.data(), sizeof(uint16_t) * n_params, cudaMemcpyHostToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   h->conf_tau_cm = tau_m * 100.0f;
@@ -1245,13 +1251,13 @@ ff_status ff_cnn_features(const uint16_t *d_depth, int n, int width, int height,
   return FF_OK;
 }
 
-ff_status ff_cnn_forward(const void *d_params, const void *d_feat, int n, int width, int height, void *d_a1,
-                         void *d_a2, float *d_out, float tau_m, void *stream) {
-  if (!d_params || !d_feat || !d_a1 || !d_a2 || !d_out || n <= 0 || width <= 0 || height <= 0)
+ff_status ff_cnn_forward(const void *d_params, void *d_packed, const void *d_feat, int n, int width, int height,
+                         void *d_a1, void *d_a2, float *d_out, float tau_m, void *stream) {
+  if (!d_params || !d_packed || !d_feat || !d_a1 || !d_a2 || !d_out || n <= 0 || width <= 0 || height <= 0)
     return cnn_bad("ff_cnn_forward: bad argument");
-  CKN(cnn_forward((const __nv_bfloat16 *)d_params, (const __nv_bfloat16 *)d_feat, n, width, height,
-                  (__nv_bfloat16 *)d_a1, (__nv_bfloat16 *)d_a2, d_out, tau_m > 0.0f ? tau_m * 100.0f : 0.0f,
-                  (cudaStream_t)stream));
+  CKN(cnn_forward((const __nv_bfloat16 *)d_params, (uint8_t *)d_packed, false, (const __nv_bfloat16 *)d_feat, n,
+                  width, height, (__nv_bfloat16 *)d_a1, (__nv_bfloat16 *)d_a2, d_out,
+                  tau_m > 0.0f ? tau_m * 100.0f : 0.0f, nullptr, (cudaStream_t)stream));
   return FF_OK;
 }
 

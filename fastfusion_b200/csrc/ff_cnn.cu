@@ -32,6 +32,7 @@ constexpr int P_W1 = 0, P_B1 = P_W1 + CNN_HID * CNN_IN * TAPS, P_W2 = P_B1 + CNN
               P_B2 = P_W2 + CNN_HID * CNN_HID * TAPS, P_W3 = P_B2 + CNN_HID, P_B3 = P_W3 + CNN_HID * TAPS,
               P_TOTAL = P_B3 + 1;
 static_assert(P_TOTAL == CNN_PARAMS && CNN_HID == CNN_HIDDEN && CNN_IN_STRIDE == CNN_FEAT_CH, "parameter layout");
+static_assert(CNN_PACKED_BYTES == 65 * 512, "packed operand bytes");
 
 // output tile of a convolution block: 32 x 16 pixels, 256 threads, two
 // pixels (rows ty and ty + 8) per thread; input tile with a 2-pixel halo,
@@ -218,6 +219,241 @@ __global__ void __launch_bounds__(256) k_conv(const TIN *__restrict__ in, int W,
       }
     }
   }
+}
+
+// ------------------------------------------------ tensor-core convolution
+//
+// The forward layers as implicit GEMMs on the 5th-generation tensor cores:
+// per output row of a 128-pixel strip, D[128 pixels x 16] (FP32, in tensor
+// memory) accumulates one tcgen05.mma (M=128, N=16, K=16, BF16) per
+// tap (C = 16 input channels: the 16 channels of the tap) or per pair of
+// horizontally adjacent taps (C = 8: the 8 channels of two neighbouring
+// pixels).  Operands are read by the tensor core straight from shared
+// memory through descriptors of the K-major, unswizzled canonical layout:
+// 8 x 16-byte core matrices, rows (pixels) 16 bytes apart, 8-row groups 128
+// bytes apart (SBO), the two K halves LBO apart -- the two channel planes of
+// the tile (C = 16) or the next pixel (C = 8).  A tap's shift is the
+// descriptor's start address.  Layer 3 (16 -> 1) runs with N = 16 (the
+// smallest N of an M = 128 MMA): output channel 0 real, 1..15 zero weights.
+//
+// CTA: 128 threads, output tile 128 x TC_ROWS pixels; input tile
+// (TC_ROWS + 4) x TC_COLS pixels per plane, brought in with cp.async (zero
+// fill outside the image).  One thread issues the MMAs; all wait on an
+// mbarrier (bounded) and read the accumulators back with tcgen05.ld (warp
+// w: pixels 32w..32w+31).
+
+constexpr int TC_ROWS = 8;               // output rows per CTA
+constexpr int TC_COLS = 136;             // 128 + 4 halo + 4 (the pair of taps 4 and 5 reads one more pixel)
+constexpr int TC_TILE_ROWS = TC_ROWS + 4;
+constexpr int TC_PLANE = TC_TILE_ROWS * TC_COLS * 16;  // bytes of one 8-channel plane
+constexpr int TC_WAIT_LIMIT = 1 << 24;
+
+template <int C>
+__host__ __device__ constexpr int tc_mmas_per_row() { return C == 16 ? 25 : 15; }
+template <int N>
+__host__ __device__ constexpr int tc_b_bytes() { return N * 32; }  // one K=16 x N operand (512 B)
+// at least 57 KB, so that at most 4 CTAs share an SM: 4 x 128 columns fill
+// the 512 of tensor memory, and no allocation has to wait for another CTA
+template <int C, int N>
+constexpr size_t tc_smem_bytes() {
+  return std::max<size_t>((size_t)(C / 8) * TC_PLANE + (size_t)tc_mmas_per_row<C>() * tc_b_bytes<N>() + 64,
+                          57 * 1024);
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: K-major, no swizzle (sm_100 version 1)
+__device__ __forceinline__ uint64_t tc_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);
+}
+
+// instruction descriptor: D FP32, A and B BF16, both K-major, M = 128
+template <int N>
+__host__ __device__ constexpr uint32_t tc_idesc() {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+
+// Weight of operand element (n, k) of MMA j: layer with C input channels
+// (C = 8: taps paired along x), output channel n.
+template <int C>
+__device__ __forceinline__ float tc_weight(const __nv_bfloat16 *__restrict__ w, int cin, int cout, int j, int n,
+                                           int k) {
+  if (n >= cout) return 0.0f;
+  if (C == 16) return __bfloat162float(__ldg(w + (n * cin + k) * TAPS + j));
+  const int ky = j / 3, kx = 2 * (j % 3) + (k >> 3), ci = k & 7;
+  return (kx < 5 && ci < cin) ? __bfloat162float(__ldg(w + (n * cin + ci) * TAPS + ky * 5 + kx)) : 0.0f;
+}
+
+// The B operands of all three layers in their shared-memory layout (element
+// (n, k) of MMA j at j*512 + (k/8)*256 + (n/8)*128 + (n%8)*16 + (k%8)*2),
+// written once per parameter set by k_pack_tc and copied by each CTA.
+constexpr int TC_PACK_L1 = 0, TC_PACK_L2 = 15 * 512, TC_PACK_L3 = TC_PACK_L2 + 25 * 512,
+              TC_PACK_BYTES = TC_PACK_L3 + 25 * 512;
+
+__global__ void k_pack_tc(const __nv_bfloat16 *__restrict__ params, __nv_bfloat16 *__restrict__ packed) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= TC_PACK_BYTES / 2) return;
+  const int byte = 2 * i;
+  float v;
+  int rel, layer;
+  if (byte < TC_PACK_L2) rel = byte, layer = 1;
+  else if (byte < TC_PACK_L3) rel = byte - TC_PACK_L2, layer = 2;
+  else rel = byte - TC_PACK_L3, layer = 3;
+  const int j = rel / 512, q = rel % 512;
+  const int k = ((q / 256) << 3) | ((q % 16) / 2), n = ((q / 128) % 2) * 8 + (q % 128) / 16;
+  if (layer == 1) v = tc_weight<8>(params + P_W1, CNN_IN, CNN_HID, j, n, k);
+  else if (layer == 2) v = tc_weight<16>(params + P_W2, CNN_HID, CNN_HID, j, n, k);
+  else v = tc_weight<16>(params + P_W3, CNN_HID, 1, j, n, k);
+  packed[i] = __float2bfloat16_rn(v);
+}
+
+template <int C, int N, int MODE>
+__global__ void __launch_bounds__(128) k_conv_tc(const __nv_bfloat16 *__restrict__ in, int W, int H,
+                                                 const uint8_t *__restrict__ wpack,
+                                                 const __nv_bfloat16 *__restrict__ bias, void *__restrict__ out,
+                                                 float inv_tau, uint32_t *__restrict__ err) {
+  constexpr int NP = C / 8;  // channel planes
+  constexpr int NM = tc_mmas_per_row<C>();
+  constexpr int BB = tc_b_bytes<N>();
+  static_assert(N == 16, "M = 128 MMAs take N in steps of 16");
+  constexpr int TMEM_COLS = TC_ROWS * N;  // 128
+  extern __shared__ __align__(1024) uint8_t tsm[];
+  uint8_t *planes = tsm;                  // NP x [TC_TILE_ROWS][TC_COLS][8] bf16
+  uint8_t *wsm = tsm + NP * TC_PLANE;     // NM x [k half][N][8] bf16
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(wsm + NM * BB);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(wsm + NM * BB + 8);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int img = blockIdx.z;
+  const int x0 = blockIdx.x * 128, y0 = blockIdx.y * TC_ROWS;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(mbar)));
+  // input tile: 16-byte chunks (8 channels), zero outside the image
+  const size_t img_base = (size_t)img * W * H;
+  const uint32_t pbase = smem_addr(planes);
+#pragma unroll 4
+  for (int i = tid; i < TC_TILE_ROWS * TC_COLS * NP; i += 128) {
+    const int pl = i % NP, px = i / NP, col = px % TC_COLS, row = px / TC_COLS;
+    const int gx = x0 - 2 + col, gy = y0 - 2 + row;
+    const bool ok = col < 132 && gx >= 0 && gx < W && gy >= 0 && gy < H;
+    const __nv_bfloat16 *src = ok ? in + (img_base + (size_t)gy * W + gx) * C + pl * 8 : in;
+    cp_async16(pbase + (uint32_t)(pl * TC_PLANE + (row * TC_COLS + col) * 16), src, ok);
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  // B operands, packed in their shared-memory layout
+  const uint32_t wsm_base = smem_addr(wsm);
+#pragma unroll 4
+  for (int i = tid; i < NM * BB / 16; i += 128) cp_async16(wsm_base + (uint32_t)(i * 16), wpack + i * 16, true);
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  // make the shared-memory writes visible to the tensor core (async proxy)
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (tid == 0) {
+    const uint32_t wbase = smem_addr(wsm);
+    const uint32_t lbo = C == 16 ? (uint32_t)TC_PLANE : 16u;
+    for (int r = 0; r < TC_ROWS; r++) {
+      for (int j = 0; j < NM; j++) {
+        const int ky = C == 16 ? j / 5 : j / 3;
+        const int kx = C == 16 ? j % 5 : 2 * (j % 3);
+        const uint64_t ad = tc_desc(pbase + (uint32_t)(((r + ky) * TC_COLS + kx) * 16), lbo, 128);
+        const uint64_t bd = tc_desc(wbase + (uint32_t)(j * BB), BB / 2, 128);
+        const uint32_t acc = j > 0 ? 1u : 0u;
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.u32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem + (uint32_t)(r * N)),
+            "l"(ad), "l"(bd), "r"(tc_idesc<N>()), "r"(acc));
+      }
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_addr(mbar))
+                 : "memory");
+  }
+  uint32_t done = 0;
+  for (int it = 0; it < TC_WAIT_LIMIT && !done; it++) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_addr(mbar)), "r"(0u)
+        : "memory");
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!done && tid == 0 && err) atomicOr(err, ERR_SPIN_TIMEOUT);
+  const int gx = x0 + 32 * warp + lane;
+  const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);
+  if constexpr (MODE == CONV_RELU_BF16) {
+    float b[16];
+#pragma unroll
+    for (int c = 0; c < 16; c++) b[c] = __bfloat162float(bias[c]);
+#pragma unroll 1
+    for (int r = 0; r < TC_ROWS; r++) {
+      uint32_t v[16];
+      if (done) {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(trow + (uint32_t)(r * N)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      } else {
+#pragma unroll
+        for (int c = 0; c < 16; c++) v[c] = 0x7FC00000u;  // NaN: the accumulators were not read
+      }
+      const int gy = y0 + r;
+      if (gx < W && gy < H) {
+        uint4 o[2];
+        __nv_bfloat16 *ob = reinterpret_cast<__nv_bfloat16 *>(o);
+#pragma unroll
+        for (int c = 0; c < 16; c++) ob[c] = __float2bfloat16_rn(fmaxf(__uint_as_float(v[c]) + b[c], 0.0f));
+        uint4 *dst = reinterpret_cast<uint4 *>(reinterpret_cast<__nv_bfloat16 *>(out) +
+                                               (img_base + (size_t)gy * W + gx) * 16);
+        dst[0] = o[0];
+        dst[1] = o[1];
+      }
+    }
+  } else {
+    const float b0 = __bfloat162float(bias[0]);
+    uint32_t v[TC_ROWS];
+    if (done) {
+      // column 0 (output channel 0) of every row's accumulator
+#pragma unroll
+      for (int r = 0; r < TC_ROWS; r++)
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(v[r]) : "r"(trow + (uint32_t)(r * N)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    } else {
+#pragma unroll
+      for (int r = 0; r < TC_ROWS; r++) v[r] = 0x7FC00000u;
+    }
+#pragma unroll
+    for (int r = 0; r < TC_ROWS; r++) {
+      const int gy = y0 + r;
+      if (gx >= W || gy >= H) continue;
+      const float a = __uint_as_float(v[r]) + b0;
+      float o = a;
+      if (MODE == CONV_CONF) {
+        const float c = fmaxf(1.0f - fmaxf(a, 0.0f) * inv_tau, 0.0f);
+        o = c * c;
+      }
+      reinterpret_cast<float *>(out)[img_base + (size_t)gy * W + gx] = o;
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
 }
 
 template <int CIN, int COUT>
@@ -494,6 +730,11 @@ cudaError_t set_conv_attr() {
   return cudaFuncSetAttribute(k_conv<KIN, KOUT, CSTR, TIN, TRANS, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)conv_smem_bytes<KIN, KOUT>());
 }
+template <int C, int N, int MODE>
+cudaError_t set_tc_attr() {
+  return cudaFuncSetAttribute(k_conv_tc<C, N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)tc_smem_bytes<C, N>());
+}
 template <int CIN, int COUT, int CSTR>
 cudaError_t set_wgrad_attr() {
   return cudaFuncSetAttribute(k_conv_wgrad<CIN, COUT, CSTR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -508,10 +749,10 @@ cudaError_t ensure_attrs() {
   const unsigned long long bit = 1ull << (dev & 63);
   if (g_attr_done & bit) return cudaSuccess;
   cudaError_t r[] = {
-      set_conv_attr<CNN_IN, CNN_HID, CNN_IN_STRIDE, __nv_bfloat16, false, CONV_RELU_BF16>(),
-      set_conv_attr<CNN_HID, CNN_HID, CNN_HID, __nv_bfloat16, false, CONV_RELU_BF16>(),
-      set_conv_attr<CNN_HID, 1, CNN_HID, __nv_bfloat16, false, CONV_F32>(),
-      set_conv_attr<CNN_HID, 1, CNN_HID, __nv_bfloat16, false, CONV_CONF>(),
+      set_tc_attr<CNN_IN_STRIDE, 16, CONV_RELU_BF16>(),
+      set_tc_attr<CNN_HID, 16, CONV_RELU_BF16>(),
+      set_tc_attr<CNN_HID, 16, CONV_F32>(),
+      set_tc_attr<CNN_HID, 16, CONV_CONF>(),
       set_conv_attr<1, CNN_HID, 1, float, true, CONV_MASK_F32>(),
       set_conv_attr<CNN_HID, CNN_HID, CNN_HID, float, true, CONV_MASK_F32>(),
       set_wgrad_attr<CNN_HID, 1, CNN_HID>(),
@@ -552,20 +793,27 @@ cudaError_t cnn_features(const uint16_t *depth, int n, int W, int H, float scali
   return cudaGetLastError();
 }
 
-cudaError_t cnn_forward(const __nv_bfloat16 *params, const __nv_bfloat16 *feat, int n, int W, int H,
-                        __nv_bfloat16 *a1, __nv_bfloat16 *a2, float *out, float tau_cm, cudaStream_t s) {
+cudaError_t cnn_forward(const __nv_bfloat16 *params, uint8_t *packed, bool packed_ready, const __nv_bfloat16 *feat,
+                        int n, int W, int H, __nv_bfloat16 *a1, __nv_bfloat16 *a2, float *out, float tau_cm,
+                        uint32_t *err, cudaStream_t s) {
   cudaError_t e = ensure_attrs();
   if (e != cudaSuccess) return e;
-  conv<CNN_IN, CNN_HID, CNN_IN_STRIDE, __nv_bfloat16, false, CONV_RELU_BF16>(feat, n, W, H, params + P_W1,
-                                                                             params + P_B1, a1, nullptr, 0.0f, s);
-  conv<CNN_HID, CNN_HID, CNN_HID, __nv_bfloat16, false, CONV_RELU_BF16>(a1, n, W, H, params + P_W2, params + P_B2, a2,
-                                                                        nullptr, 0.0f, s);
+  if (!packed_ready) {
+    note_launch();
+    k_pack_tc<<<(TC_PACK_BYTES / 2 + 255) / 256, 256, 0, s>>>(params, reinterpret_cast<__nv_bfloat16 *>(packed));
+  }
+  const dim3 tg((W + 127) / 128, (H + TC_ROWS - 1) / TC_ROWS, n);
+  note_launch(3);
+  k_conv_tc<CNN_IN_STRIDE, 16, CONV_RELU_BF16><<<tg, 128, tc_smem_bytes<CNN_IN_STRIDE, 16>(), s>>>(
+      feat, W, H, packed + TC_PACK_L1, params + P_B1, a1, 0.0f, err);
+  k_conv_tc<CNN_HID, 16, CONV_RELU_BF16><<<tg, 128, tc_smem_bytes<CNN_HID, 16>(), s>>>(
+      a1, W, H, packed + TC_PACK_L2, params + P_B2, a2, 0.0f, err);
   if (tau_cm > 0.0f)
-    conv<CNN_HID, 1, CNN_HID, __nv_bfloat16, false, CONV_CONF>(a2, n, W, H, params + P_W3, params + P_B3, out,
-                                                               nullptr, 1.0f / tau_cm, s);
+    k_conv_tc<CNN_HID, 16, CONV_CONF><<<tg, 128, tc_smem_bytes<CNN_HID, 16>(), s>>>(
+        a2, W, H, packed + TC_PACK_L3, params + P_B3, out, 1.0f / tau_cm, err);
   else
-    conv<CNN_HID, 1, CNN_HID, __nv_bfloat16, false, CONV_F32>(a2, n, W, H, params + P_W3, params + P_B3, out,
-                                                              nullptr, 0.0f, s);
+    k_conv_tc<CNN_HID, 16, CONV_F32><<<tg, 128, tc_smem_bytes<CNN_HID, 16>(), s>>>(
+        a2, W, H, packed + TC_PACK_L3, params + P_B3, out, 0.0f, err);
   return cudaGetLastError();
 }
 

@@ -151,9 +151,15 @@ struct RaycastMap {
 
 cudaError_t cnn_features(const uint16_t *depth, int n, int W, int H, float scaling, const float K[4],
                          __nv_bfloat16 *feat, cudaStream_t s);
-// tau_cm > 0: out = the confidence weight; else out = the network's output
-cudaError_t cnn_forward(const __nv_bfloat16 *params, const __nv_bfloat16 *feat, int n, int W, int H,
-                        __nv_bfloat16 *a1, __nv_bfloat16 *a2, float *out, float tau_cm, cudaStream_t s);
+// tau_cm > 0: out = the confidence weight; else out = the network's output.
+// packed: CNN_PACKED_BYTES of device memory for the tensor-core operands of
+// the weights, filled from params first unless packed_ready.
+// err (may be null): ERR_SPIN_TIMEOUT if a tensor-core wait gave up (the
+// layer's output is then NaN).
+constexpr int CNN_PACKED_BYTES = 65 * 512;
+cudaError_t cnn_forward(const __nv_bfloat16 *params, uint8_t *packed, bool packed_ready, const __nv_bfloat16 *feat,
+                        int n, int W, int H, __nv_bfloat16 *a1, __nv_bfloat16 *a2, float *out, float tau_cm,
+                        uint32_t *err, cudaStream_t s);
 cudaError_t cnn_backward(const __nv_bfloat16 *params, const __nv_bfloat16 *feat, const __nv_bfloat16 *a1,
                          const __nv_bfloat16 *a2, const float *dpred, int n, int W, int H, float *g1, float *g2,
                          float *grads, cudaStream_t s);

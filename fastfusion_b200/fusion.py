@@ -86,7 +86,7 @@ SIGNATURES = {
     "ff_get_confidence_map": (_i32, [_vp, _vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32)]),
     "ff_raycast_depth": (_i32, [_vp, _vp, _vp, _vp, _vp, _i32, _i32, _f32, _f32, _f32, _vp]),
     "ff_cnn_features": (_i32, [_vp, _i32, _i32, _i32, _f32, _vp, _vp, _vp]),
-    "ff_cnn_forward": (_i32, [_vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp, _f32, _vp]),
+    "ff_cnn_forward": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp, _f32, _vp]),
     "ff_cnn_backward": (_i32, [_vp, _vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp]),
     "ff_cnn_mse": (_i32, [_vp, _vp, ctypes.c_int64, _f32, _vp, _vp, _vp]),
     "ff_cnn_adam": (_i32, [_vp, _vp, _vp, _vp, _vp, _f32, _f32, _f32, _f32, _i32, _vp]),

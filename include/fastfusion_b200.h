@@ -230,6 +230,7 @@ ff_status ff_kernel_launches(uint64_t *own, uint64_t *library);
 #define FF_CNN_PARAMS 8833
 #define FF_CNN_FEAT_CH 8
 #define FF_CNN_HIDDEN 16
+#define FF_CNN_PACKED_BYTES 33280
 
 /* Turn the learned weight on for this map (params: FF_CNN_PARAMS floats,
  * rounded to BF16; tau in metres), or off with params NULL. */
@@ -251,7 +252,9 @@ ff_status ff_raycast_depth(ff_handle *h, const double K[4], const double R[9], c
  * memory (stream: a cudaStream_t, NULL for the default stream).  n images of
  * width x height; feat bf16 [n][h][w][8]; a1, a2 bf16 [n][h][w][16]; pred /
  * dpred / target float [n][h][w]; g1, g2 float [n][h][w][16] (scratch);
- * params bf16 and grads / master / m / v float [FF_CNN_PARAMS].
+ * params bf16 and grads / master / m / v float [FF_CNN_PARAMS]; packed:
+ * FF_CNN_PACKED_BYTES of scratch that ff_cnn_forward fills with the weights
+ * laid out as tensor-core operands (one per concurrent call).
  * ff_cnn_forward writes the confidence when tau_m > 0, else the prediction.
  * ff_cnn_backward adds the parameter gradients of d(loss)/d(pred) to grads.
  * ff_cnn_mse: loss += sum over target >= 0 of (pred - target)^2 * inv_count,
@@ -259,8 +262,8 @@ ff_status ff_raycast_depth(ff_handle *h, const double K[4], const double R[9], c
  * ff_cnn_adam: one Adam step of master, BF16 copy into params, grads cleared. */
 ff_status ff_cnn_features(const uint16_t *d_depth, int n, int width, int height, float scaling, const double K[4],
                           void *d_feat, void *stream);
-ff_status ff_cnn_forward(const void *d_params, const void *d_feat, int n, int width, int height, void *d_a1,
-                         void *d_a2, float *d_out, float tau_m, void *stream);
+ff_status ff_cnn_forward(const void *d_params, void *d_packed, const void *d_feat, int n, int width, int height,
+                         void *d_a1, void *d_a2, float *d_out, float tau_m, void *stream);
 ff_status ff_cnn_backward(const void *d_params, const void *d_feat, const void *d_a1, const void *d_a2,
                           const float *d_dpred, int n, int width, int height, float *d_g1, float *d_g2,
                           float *d_grads, void *stream);
