@@ -38,6 +38,9 @@ struct ff_handle {
   // the allocation kernels run (it is first read by the voxel update)
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_bgr_free = nullptr, ev_bgr_ready = nullptr;
+  // recorded once a frame's counters have reached the host: a single-map
+  // frame returns then, while its voxel update still runs on the stream
+  cudaEvent_t ev_counters = nullptr;
   // the frame descriptor(s) the per-frame kernels read: this map's own, or a
   // whole batch when this handle leads ff_add_maps_u16_device
   BatchDesc *d_batch = nullptr, *h_batch = nullptr;
@@ -338,7 +341,8 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
     h->own_stream = true;
     if (cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_bgr_free, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h->ev_bgr_ready, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&h->ev_bgr_ready, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_counters, cudaEventDisableTiming) != cudaSuccess) {
       fail(FF_ERR_CUDA, "copy stream");
       break;
     }
@@ -430,7 +434,15 @@ ff_status ff_destroy(ff_handle *h) {
   }
   if (h->ev_bgr_free) cudaEventDestroy(h->ev_bgr_free);
   if (h->ev_bgr_ready) cudaEventDestroy(h->ev_bgr_ready);
+  if (h->ev_counters) cudaEventDestroy(h->ev_counters);
   delete h;
+  return FF_OK;
+}
+
+ff_status ff_sync(ff_handle *h) {
+  if (!h) return FF_ERR_BAD_ARG;
+  CK(cudaSetDevice(h->cfg.device));
+  CK(cudaStreamSynchronize(h->stream));
   return FF_OK;
 }
 
@@ -652,13 +664,20 @@ static ff_status frame_launch(ff_handle *lead, int n) {
 }
 
 // The device-count finalisation and gated voxel update of the uploaded batch.
-static ff_status frame_launch_update(ff_handle *lead, int n, uint32_t max_npix, int &pi_fin, int &pi_fuse) {
+// counters: a single map's counters are copied to the host between the
+// finalisation and the update, and this event recorded after the copy.
+static ff_status frame_launch_update(ff_handle *lead, int n, uint32_t max_npix, int &pi_fin, int &pi_fuse,
+                                     cudaEvent_t counters = nullptr) {
   ff_handle *h = lead;  // (error reporting)
   cudaStream_t s = lead->stream;
   pi_fin = lead->prof.begin(ST_FINALIZE, s);
   if (!launch_finalize_small(lead->d_batch, n, max_npix, lead->cfg.device, s))
     return set_err(lead, FF_ERR_CUDA, "leaf finalisation could not be launched");
   lead->prof.end(pi_fin, 0.0, s);
+  if (counters) {
+    CK(cudaMemcpyAsync(lead->h_cnt, lead->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+    CK(cudaEventRecord(counters, s));
+  }
   pi_fuse = lead->prof.begin(ST_FUSE, s);
   // enough blocks for a frame's bricks in one pass; blocks loop over larger batches
   launch_fuse(lead->d_batch, n, true, lead->cfg.storage, lead->d_rcp_tab != nullptr, 148 * 8, s);
@@ -758,11 +777,16 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
   if (bgr_pending) CK(cudaStreamWaitEvent(s, h->ev_bgr_ready, 0));
   int pi_fin = -1, pi_fuse = -1;
   if (plan.one_sync) {
-    st = frame_launch_update(h, 1, (uint32_t)(W * H), pi_fin, pi_fuse);
+    // the frame returns once its counters are on the host; its voxel update
+    // (gated on the device) keeps running, ordered before anything that
+    // follows on the stream
+    st = frame_launch_update(h, 1, (uint32_t)(W * H), pi_fin, pi_fuse, h->ev_counters);
     if (st != FF_OK) return st;
+    CK(cudaEventSynchronize(h->ev_counters));
+  } else {
+    CK(cudaMemcpyAsync(h->h_cnt, h->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
   }
-  CK(cudaMemcpyAsync(h->h_cnt, h->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
   return frame_finish(h, plan, mf, pi_fin, pi_fuse, queued);
 }
 

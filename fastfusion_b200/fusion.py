@@ -61,6 +61,7 @@ SIGNATURES = {
     "ff_create": (_i32, [ctypes.POINTER(ff_config), ctypes.POINTER(_vp)]),
     "ff_destroy": (_i32, [_vp]),
     "ff_set_stream": (_i32, [_vp, _vp]),
+    "ff_sync": (_i32, [_vp]),
     "ff_add_map_u16": (_i32, [_vp, _vp, _i32, _i32, _sz, _vp, _sz, _vp, _vp, _vp, _f32, _f32, _vp]),
     "ff_add_map_u16_device": (_i32, [_vp, _vp, _vp, _i32, _i32, _vp, _vp, _vp, _f32, _f32, _vp]),
     "ff_add_maps_u16_device": (_i32, [_vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
@@ -313,7 +314,9 @@ class FusionMipMapCPU:
 
     def addMapDevice(self, d_depth: int, d_bgr: int, width: int, height: int, caminfo: CameraInfo,
                      scaling: float = 1.0 / 5000.0, maxcamdistance: float = 10.0) -> int:
-        """addMap with depth/bgr already in device memory (raw device pointers)."""
+        """addMap with depth/bgr already in device memory (raw device pointers).
+        Returns once the frame's bricks are counted; the images must stay
+        unchanged until the next call on this map returns or sync()."""
         pK, pR, pt = caminfo._ptrs
         st = self._L.ff_add_map_u16_device(self._h, d_depth, d_bgr, width, height, pK, pR, pt, scaling,
                                            maxcamdistance, self._qref)
@@ -370,6 +373,10 @@ class FusionMipMapCPU:
 
     def setDepthChecks(self, depthchecks: int):
         """A no-op in the reference too (its code is commented out)."""
+
+    def sync(self):
+        """Wait for the map's outstanding device work (the last voxel update)."""
+        self._check(self._L.ff_sync(self._h))
 
     def set_stream(self, stream_ptr: int | None):
         self._check(self._L.ff_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)))

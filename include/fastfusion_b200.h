@@ -91,6 +91,10 @@ ff_status ff_destroy(ff_handle *h);
  * library's own stream). */
 ff_status ff_set_stream(ff_handle *h, void *cuda_stream);
 
+/* Wait for this map's outstanding device work (the last frame's voxel
+ * update, which an add-map call does not wait for). */
+ff_status ff_sync(ff_handle *h);
+
 /* Fuse one frame.  Replaces FusionMipMapCPU::addMap(const cv::Mat &depth
  * CV_16UC1, CameraInfo, const cv::Mat &rgb CV_8UC3 BGR, float scaling, float
  * maxcamdistance) (geometryfusion_mipmap_cpu.hpp:122-123, .cpp:1603-2034).
@@ -103,7 +107,10 @@ ff_status ff_add_map_u16(ff_handle *h, const uint16_t *depth, int width, int hei
                          const double t[3], float scaling, float maxcam, int32_t *queued);
 
 /* Same as ff_add_map_u16 with depth/bgr already in device memory (tightly
- * packed).  No host<->device copy of the images. */
+ * packed).  No host<->device copy of the images.  The call returns once the
+ * frame's bricks are allocated and counted; its voxel update may still be
+ * running on the map's stream, so the device images must stay unchanged
+ * until the next call on this handle returns or ff_sync(h). */
 ff_status ff_add_map_u16_device(ff_handle *h, const uint16_t *d_depth, const uint8_t *d_bgr, int width, int height,
                                 const double K[4], const double R[9], const double t[3], float scaling,
                                 float maxcam, int32_t *queued);
