@@ -55,6 +55,9 @@ L2_FLUSH_BYTES = 256 << 20
 CPU_SAMPLE_SECONDS = 20.0
 
 # stage -> kernels it times (for the roofline record)
+# the reference's brick pool: its 2 GB cap in bricks (treeandbrick.cpp:169-229)
+REFERENCE_POOL_BRICKS = 271420
+
 STAGE_KERNELS = {
     "grow": "k_shift_branches+k_shift_leaves+copies",
     "dedupe": "k_dedupe (projection + de-duplication)",
@@ -75,17 +78,26 @@ def parse_args(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--storage", choices=["fp32", "fp16"], default="fp32")
+    ap.add_argument("--storage", choices=["fp32", "fp16"], default=None,
+                    help="voxel storage (default fp32; fp16 for the corridor workload)")
     ap.add_argument("--rcp", choices=["host", "exact"], default="host")
     ap.add_argument("--weight", choices=["plain", "learned"], default="plain",
                     help="learned: the trained per-pixel confidence network weights every frame")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workers", type=int, default=0, help="reference arm: maps in parallel (0 = all cores)")
+    ap.add_argument("--workload", choices=["walk", "corridor"], default="walk",
+                    help="corridor: the large-map workload (1280x960, FP16 storage, pool of --pool-gb)")
+    ap.add_argument("--pool-gb", type=float, default=120.0, help="corridor: brick pool size in GB of HBM")
+    ap.add_argument("--stride", type=int, default=10, help="corridor: use every stride-th frame of the path")
+    ap.add_argument("--no-tuning", action="store_true",
+                    help="batched workload: default launch shapes instead of the autotuner's table")
     ap.add_argument("--maps", type=int, default=0,
                     help="batched workload instead: this many independent maps of uneven size fused together "
                          "(ff_add_maps_u16_device), one frame of each per launch set")
     a = ap.parse_args(argv)
+    if a.storage is None:
+        a.storage = "fp16" if a.workload == "corridor" else "fp32"
     if a.warmup < 3:
         ap.error("--warmup must be at least 3")
     if a.steps < 1:
@@ -584,6 +596,11 @@ def run_batch(a):
         maps.append(m)
     widths = [seq.width for seq, _ in seqs]
     heights = [seq.height for seq, _ in seqs]
+    # launch shapes chosen by the autotuner for this GPU (python -m fastfusion_b200.autotune), if any
+    from fastfusion_b200.autotune import DEFAULT, load_tuning
+    tuning = {} if a.no_tuning else load_tuning()
+    if tuning:
+        maps[0].set_tuning(**{**DEFAULT, **tuning})
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
 
     def step(s_):
@@ -620,6 +637,7 @@ def run_batch(a):
                                f"320x240/640x480/1280x960, voxels 4-10 mm, {nf} frames each, one frame of "
                                f"every map per launch set, updateMeshes every {FRAMES_PER_STEP} frames",
                    "maps": len(maps), "widths": widths, "voxels_mm": [round(v * 1e3, 2) for _, v in seqs],
+                   "tuning": tuning or "defaults",
                    "l2": "flushed between timed steps (256 MB write)"},
         "fuse": {"GB/s": round(fuse_gbs, 1), "frac_of_hbm": round(fuse_gbs / peak, 4), "peak": peak,
                  "peak_source": peak_kind, "launches": fl, "avg_launch_us": round(1e3 * fms / fl, 2) if fl else 0,
@@ -631,10 +649,106 @@ def run_batch(a):
         m.close()
 
 
+def run_corridor(a):
+    """The large map: the 50 x 20 x 3 m corridor/office floor (400
+    primitives), 1280x960 depth at fx = fy = 1050 along the seeded
+    10,000-frame spline at 1.0-1.6 m, every --stride-th frame of it (so the
+    path is covered end to end), FP16 storage, the brick pool sized to
+    --pool-gb of HBM, updateMeshes every 10 frames; frames device-resident,
+    CUDA events per step."""
+    import torch
+    from fastfusion_b200 import fusion as ff
+    from fastfusion_b200.scene import corridor_sequence, render_torch
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    nf = n_frames_needed(a)
+    W, H = 1280, 960
+    seq = corridor_sequence(a.seed, n_frames=10000, width=W, height=H)
+    idx = [min(k * a.stride, 9999) for k in range(nf)]
+    depth = torch.empty((nf, H, W), dtype=torch.int16, device=dev)
+    bgr = torch.empty((nf, H, W, 3), dtype=torch.uint8, device=dev)
+    t0 = time.perf_counter()
+    for i, k in enumerate(idx):
+        d, c = render_torch(seq.scene, *seq.poses[k], W, H, seq.K, seq.seed, k, device=dev, cull_m=MAXCAM + 1.0)
+        depth[i].copy_(d)
+        bgr[i].copy_(c)
+    torch.cuda.synchronize(dev)
+    render_s = time.perf_counter() - t0
+    cams = [ff.CameraInfo(seq.K, *seq.poses[k]) for k in idx]
+    stream = torch.cuda.current_stream(dev)
+    free0, total = torch.cuda.mem_get_info(dev)
+    m = ff.FusionMipMapCPU(0, 0, 0, VOXEL, THRESHOLD, 0, True, storage=a.storage, rcp=a.rcp,
+                           pool_bytes=int(a.pool_gb * 1e9))
+    free1, _ = torch.cuda.mem_get_info(dev)
+    m.set_stream(stream.cuda_stream)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    leaves, ref_cap_step = [], None
+
+    def step(s_):
+        for i in range(s_ * FRAMES_PER_STEP, (s_ + 1) * FRAMES_PER_STEP):
+            m.addMapDevice(depth[i].data_ptr(), bgr[i].data_ptr(), W, H, cams[i], SCALING, MAXCAM)
+        m.updateMeshes()
+
+    for s_ in range(a.warmup):
+        step(s_)
+    m.profile(True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    torch.cuda.synchronize(dev)
+    for i in range(a.steps):
+        flush.fill_(i)
+        ev[i][0].record(stream)
+        step(a.warmup + i)
+        ev[i][1].record(stream)
+        st = m.stats()
+        leaves.append(st["leaves_used"])
+        if ref_cap_step is None and st["leaves_used"] > REFERENCE_POOL_BRICKS:
+            ref_cap_step = a.warmup + i
+    torch.cuda.synchronize(dev)
+    ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    stages = m.profile_read()
+    st = m.stats()
+    peak, peak_kind = measured_hbm_peak()
+    fms, fbytes, fl = stages["fuse"]
+    fuse_gbs = fbytes / (fms / 1e3) / 1e9 if fms > 0 else 0.0
+    q = max(1, len(ms) // 4)
+    line = {
+        "metric": METRIC.replace("(640x480, 5 mm)", "(large map, 1280x960, 5 mm)"),
+        "value": round(a.steps * FRAMES_PER_STEP / (sum(ms) / 1e3), 2), "unit": UNIT, "n_gpus": 1,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(sum(ms) / a.steps, 4),
+        "ms_per_step_first_quarter": round(float(np.mean(ms[:q])), 3),
+        "ms_per_step_last_quarter": round(float(np.mean(ms[-q:])), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if a.storage == "fp32" else "f16-storage/f32",
+        "data": "synthetic: seeded corridor/office floor rendered on the GPU (primitives beyond maxcam + 1 m "
+                "culled per frame: no depth below maxcam changes)",
+        "config": {"workload": f"corridor: 50x20x3 m floor, 400 primitives, 1280x960 fx=fy=1050, frames 0, "
+                               f"{a.stride}, 2x{a.stride}, ... of a 10,000-frame spline at 1.0-1.6 m ({nf} frames), "
+                               f"voxel 5 mm, threshold 10 mm, maxcam 4 m, updateMeshes every {FRAMES_PER_STEP} "
+                               f"frames", "storage": a.storage, "pool_gb": a.pool_gb, "stride": a.stride,
+                   "l2": "flushed between timed steps (256 MB write)"},
+        "map": {"leaves": st["leaves_used"], "leaves_max": st["leaves_max"], "n": st["n"], "grows": st["grows"],
+                "mesh_vertices": st["mesh_vertices"], "mesh_faces": st["mesh_faces"], "mesh_cells": st["mesh_cells"],
+                "meshing_ok": st["meshing_ok"], "pool_bytes_on_device": int(free0 - free1),
+                "device_bytes_total": int(total)},
+        "reference_pool": {"bricks": REFERENCE_POOL_BRICKS,
+                           "exceeded_at_step": ref_cap_step,
+                           "note": "the reference's brick pool (2 GB cap) holds 271,420 bricks; past this step "
+                                   "it cannot complete the workload"},
+        "fuse": {"GB/s": round(fuse_gbs, 1), "frac_of_hbm": round(fuse_gbs / peak, 4), "peak": peak,
+                 "peak_source": peak_kind, "avg_launch_us": round(1e3 * fms / fl, 2) if fl else 0},
+        "stages": {k: {"ms": round(v[0], 3), "launches": v[2]} for k, v in stages.items()},
+        "render_s": round(render_s, 1),
+    }
+    print(json.dumps(line), flush=True)
+    m.close()
+
+
 def main(argv=None):
     a = parse_args(argv)
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload == "corridor":
+        run_corridor(a)
     elif a.maps:
         run_batch(a)
     else:

@@ -461,10 +461,11 @@ __global__ void k_insert(const BatchDesc *__restrict__ bd) {
   }
 }
 
-void launch_insert(const BatchDesc *d_batch, uint32_t total_pix, cudaStream_t s) {
+void launch_insert(const BatchDesc *d_batch, uint32_t total_pix, cudaStream_t s, int block) {
   if (!total_pix) return;
+  if (block < 64 || block > 1024 || block % 32) block = 256;
   note_launch();
-  k_insert<<<(total_pix + 255) / 256, 256, 0, s>>>(d_batch);
+  k_insert<<<(total_pix + block - 1) / block, block, 0, s>>>(d_batch);
 }
 
 // ------------------------------------------------- pending leaf order -----
@@ -617,9 +618,7 @@ bool finalize_small_fits(uint32_t npix) {
   return sizeof(uint32_t) * (((size_t)npix + 31) / 32 + FIN_THREADS) <= FIN_SMEM_MAX;
 }
 
-bool launch_finalize_small(const BatchDesc *d_batch, int nmaps, uint32_t max_npix, int device, cudaStream_t s) {
-  const size_t smem = sizeof(uint32_t) * (((size_t)max_npix + 31) / 32 + FIN_THREADS);
-  if (smem > FIN_SMEM_MAX || nmaps < 1) return false;
+bool finalize_small_prepare(int device) {
   static std::atomic<unsigned long long> attr_devices{0};
   const unsigned long long bit = 1ull << (device & 63);
   if (!(attr_devices.load() & bit)) {
@@ -628,6 +627,13 @@ bool launch_finalize_small(const BatchDesc *d_batch, int nmaps, uint32_t max_npi
       return false;
     attr_devices.fetch_or(bit);
   }
+  return true;
+}
+
+bool launch_finalize_small(const BatchDesc *d_batch, int nmaps, uint32_t max_npix, int device, cudaStream_t s) {
+  const size_t smem = sizeof(uint32_t) * (((size_t)max_npix + 31) / 32 + FIN_THREADS);
+  if (smem > FIN_SMEM_MAX || nmaps < 1) return false;
+  if (!finalize_small_prepare(device)) return false;
   note_launch();
   k_finalize_bitmap<<<nmaps, FIN_THREADS, smem, s>>>(d_batch);
   return true;

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -92,6 +93,17 @@ struct ff_handle {
   float *d_conf = nullptr;
   size_t conf_cap = 0;  // pixels the buffers hold
   int conf_w = 0, conf_h = 0;  // size of the last confidence map
+
+  // launch shapes (ff_set_tuning) and the device's SM count
+  ff_tuning tune = {0, 0, 0, 0, 0};
+  int sm_count = 148;
+  // batched calls led by this map: their launches as a CUDA graph, replayed
+  // while the signature (maps, image sizes, shapes) stays the same
+  cudaGraphExec_t graph_exec = nullptr;
+  std::vector<uint64_t> graph_key;
+  uint64_t graph_launches = 0;  // own kernel launches inside the graph
+  uint32_t graph_replays = 0;
+  bool graph_failed = false;
 
   MeshState mesh;
   Prof prof;
@@ -338,6 +350,9 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
   };
   do {
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { fail(FF_ERR_CUDA, "stream"); break; }
+    if (cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->cfg.device) != cudaSuccess ||
+        h->sm_count < 1)
+      h->sm_count = 148;
     h->own_stream = true;
     if (cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_bgr_free, cudaEventDisableTiming) != cudaSuccess ||
@@ -435,7 +450,20 @@ ff_status ff_destroy(ff_handle *h) {
   if (h->ev_bgr_free) cudaEventDestroy(h->ev_bgr_free);
   if (h->ev_bgr_ready) cudaEventDestroy(h->ev_bgr_ready);
   if (h->ev_counters) cudaEventDestroy(h->ev_counters);
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   delete h;
+  return FF_OK;
+}
+
+ff_status ff_set_tuning(ff_handle *h, const ff_tuning *t) {
+  if (!h || !t) return FF_ERR_BAD_ARG;
+  if ((t->dedupe_rows && t->dedupe_rows != 16 && t->dedupe_rows != 32) || t->fuse_shape < 0 ||
+      t->fuse_shape >= FUSE_SHAPE_COUNT || t->fuse_blocks_per_sm < 0 || t->fuse_blocks_per_sm > 64 ||
+      (t->insert_block && (t->insert_block < 64 || t->insert_block > 1024 || t->insert_block % 32)))
+    return set_err(h, FF_ERR_BAD_ARG, "ff_set_tuning: dedupe_rows 0/16/32, fuse_shape 0..3, "
+                                      "fuse_blocks_per_sm 0..64, insert_block 0 or 64..1024 in steps of 32");
+  h->tune = *t;
+  h->graph_key.clear();  // launches change: record again
   return FF_OK;
 }
 
@@ -612,11 +640,19 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
   return FF_OK;
 }
 
-// Upload the batch held in lead->h_batch (n frames) and launch its
-// de-duplication and insert on the lead's stream.
-static ff_status frame_launch(ff_handle *lead, int n) {
+// The launch plan of a batch: tile height, the groups of whole maps that
+// share one cooperative de-duplication launch, padded pixel total.
+struct LaunchPlan {
+  int rows = 16;
+  uint32_t pix = 0;
+  double npix = 0;
+  std::vector<std::array<uint32_t, 3>> groups;  // first map, end map, tiles
+};
+
+// Host part: tiles, prefixes and rounds of the batch in lead->h_batch (n
+// frames), and its launch plan.
+static ff_status frame_plan(ff_handle *lead, int n, LaunchPlan &lp) {
   ff_handle *h = lead;  // (error reporting)
-  cudaStream_t s = lead->stream;
   BatchDesc &B = *lead->h_batch;
   B.n = n;
   // 16-row tiles when they fit one cooperative launch, else 32-row tiles in
@@ -625,7 +661,8 @@ static ff_status frame_launch(ff_handle *lead, int n) {
   for (int i = 0; i < n; i++) tiles16 += (uint32_t)dedupe_tiles(B.f[i].W, B.f[i].H, nullptr, nullptr, 16);
   CK(dedupe_capacity(lead->cfg.device, 16, cap16));
   CK(dedupe_capacity(lead->cfg.device, 32, cap32));
-  const int rows = tiles16 <= cap16 ? 16 : 32;
+  int rows = tiles16 <= cap16 ? 16 : 32;
+  if (lead->tune.dedupe_rows == 32 || (lead->tune.dedupe_rows == 16 && tiles16 <= cap16)) rows = lead->tune.dedupe_rows;
   const uint32_t cap = rows == 16 ? cap16 : cap32;
   for (int i = 0; i < n; i++) {
     const uint32_t nt = (uint32_t)dedupe_tiles(B.f[i].W, B.f[i].H, &B.f[i].tilesX, &B.f[i].tilesY, rows);
@@ -641,29 +678,49 @@ static ff_status frame_launch(ff_handle *lead, int n) {
     B.pix_end[i] = pix;
   }
   B.max_rounds = rounds;
-  CK(cudaMemcpyAsync(lead->d_batch, lead->h_batch, batch_desc_bytes(n), cudaMemcpyHostToDevice, s));
-  CK(cudaMemsetAsync(lead->d_barrier, 0, BARRIER_WORDS * sizeof(uint32_t), s));
-  double npix = 0;
-  for (int i = 0; i < n; i++) npix += (double)B.f[i].npix;
-  int pi = lead->prof.begin(ST_DEDUPE, s);
-  for (int m0 = 0, launch = 0; m0 < n; launch++) {
+  lp.rows = rows;
+  lp.pix = pix;
+  lp.npix = 0;
+  for (int i = 0; i < n; i++) lp.npix += (double)B.f[i].npix;
+  lp.groups.clear();
+  for (int m0 = 0; m0 < n;) {
     int m1 = m0;
     uint32_t group = 0;
     while (m1 < n && group + (uint32_t)(B.f[m1].tilesX * B.f[m1].tilesY) <= cap)
       group += (uint32_t)(B.f[m1].tilesX * B.f[m1].tilesY), m1++;
-    if (launch >= BARRIER_WORDS / 8) return set_err(lead, FF_ERR_BAD_ARG, "batch too large for the de-duplication");
-    CK(launch_dedupe(lead->d_batch, m0, m1, group, rows, lead->d_barrier + 8 * launch, lead->cfg.device, s));
+    if (lp.groups.size() >= (size_t)(BARRIER_WORDS / 8))
+      return set_err(lead, FF_ERR_BAD_ARG, "batch too large for the de-duplication");
+    lp.groups.push_back({(uint32_t)m0, (uint32_t)m1, group});
     m0 = m1;
   }
-  lead->prof.end(pi, npix * (2 + 16 + 1), s);  // depth in; voxel keys and processed flags out
+  return FF_OK;
+}
+
+// Device part: upload the descriptor and launch the de-duplication and the
+// insert on the lead's stream.
+static ff_status frame_issue(ff_handle *lead, int n, const LaunchPlan &lp) {
+  ff_handle *h = lead;  // (error reporting)
+  cudaStream_t s = lead->stream;
+  CK(cudaMemcpyAsync(lead->d_batch, lead->h_batch, batch_desc_bytes(n), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(lead->d_barrier, 0, BARRIER_WORDS * sizeof(uint32_t), s));
+  int pi = lead->prof.begin(ST_DEDUPE, s);
+  for (size_t g = 0; g < lp.groups.size(); g++)
+    CK(launch_dedupe(lead->d_batch, (int)lp.groups[g][0], (int)lp.groups[g][1], lp.groups[g][2], lp.rows,
+                     lead->d_barrier + 8 * g, lead->cfg.device, s));
+  lead->prof.end(pi, lp.npix * (2 + 16 + 1), s);  // depth in; voxel keys and processed flags out
   pi = lead->prof.begin(ST_INSERT, s);
-  launch_insert(lead->d_batch, pix, s);
-  lead->prof.end(pi, npix * (16 + 1), s);  // keys and flags in (tree walks counted below)
+  launch_insert(lead->d_batch, lp.pix, s, lead->tune.insert_block > 0 ? lead->tune.insert_block : 256);
+  lead->prof.end(pi, lp.npix * (16 + 1), s);  // keys and flags in (tree walks counted below)
   CK(cudaGetLastError());
   return FF_OK;
 }
 
-// The device-count finalisation and gated voxel update of the uploaded batch.
+static ff_status frame_launch(ff_handle *lead, int n) {
+  LaunchPlan lp;
+  ff_status st = frame_plan(lead, n, lp);
+  return st != FF_OK ? st : frame_issue(lead, n, lp);
+}
+
 // counters: a single map's counters are copied to the host between the
 // finalisation and the update, and this event recorded after the copy.
 static ff_status frame_launch_update(ff_handle *lead, int n, uint32_t max_npix, int &pi_fin, int &pi_fuse,
@@ -680,7 +737,10 @@ static ff_status frame_launch_update(ff_handle *lead, int n, uint32_t max_npix, 
   }
   pi_fuse = lead->prof.begin(ST_FUSE, s);
   // enough blocks for a frame's bricks in one pass; blocks loop over larger batches
-  launch_fuse(lead->d_batch, n, true, lead->cfg.storage, lead->d_rcp_tab != nullptr, 148 * 8, s);
+  const int shape = lead->tune.fuse_shape;
+  const int per_sm = lead->tune.fuse_blocks_per_sm > 0 ? lead->tune.fuse_blocks_per_sm : 8 / fuse_shape_bricks(shape);
+  launch_fuse(lead->d_batch, n, true, lead->cfg.storage, lead->d_rcp_tab != nullptr, lead->sm_count * per_sm, s,
+              shape);
   lead->prof.end(pi_fuse, 0.0, s);
   CK(cudaGetLastError());
   return FF_OK;
@@ -880,13 +940,68 @@ ff_status ff_add_maps_u16_device(ff_handle *const *maps, int n, const uint16_t *
   // the counter resets went out on each map's stream; the batch runs on the lead's
   for (int i = 1; i < n; i++) CK(cudaStreamSynchronize(maps[i]->stream));
   for (int i = 0; i < n; i++) lead->h_batch->f[i] = mf[i];
-  ff_status st = frame_launch(lead, n);
+  LaunchPlan lp;
+  ff_status st = frame_plan(lead, n, lp);
   if (st != FF_OK) return st;
   int pi_fin = -1, pi_fuse = -1;
-  st = frame_launch_update(lead, n, max_npix, pi_fin, pi_fuse);
-  if (st != FF_OK) return st;
-  for (int i = 0; i < n; i++)
-    CK(cudaMemcpyAsync(maps[i]->h_cnt, maps[i]->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, lead->stream));
+  // the device work of the batch: upload, de-duplication, insert,
+  // finalisation, gated update, every map's counters back to the host
+  auto issue = [&]() -> ff_status {
+    ff_status r = frame_issue(lead, n, lp);
+    if (r == FF_OK) r = frame_launch_update(lead, n, max_npix, pi_fin, pi_fuse);
+    for (int i = 0; i < n && r == FF_OK; i++)
+      if (cudaMemcpyAsync(maps[i]->h_cnt, maps[i]->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost,
+                          lead->stream) != cudaSuccess)
+        r = set_err(lead, FF_ERR_CUDA, "counter copy");
+    return r;
+  };
+  bool use_graph = lead->tune.graph && !lead->prof.on && !lead->graph_failed;
+  if (use_graph) {
+    // the graph's nodes hold the handles' buffers, the launch shapes and the
+    // pixel counts; the descriptor itself is copied from h_batch at replay
+    std::vector<uint64_t> key = {(uint64_t)n, (uint64_t)lp.rows, (uint64_t)lp.pix, (uint64_t)max_npix,
+                                 (uint64_t)lead->tune.fuse_shape, (uint64_t)lead->tune.fuse_blocks_per_sm,
+                                 (uint64_t)lead->tune.insert_block, (uint64_t)(uintptr_t)lead->stream};
+    for (int i = 0; i < n; i++) {
+      key.push_back((uint64_t)(uintptr_t)maps[i]);
+      key.push_back(((uint64_t)width[i] << 32) | (uint32_t)height[i]);
+    }
+    if (!lead->graph_exec || key != lead->graph_key) {
+      if (lead->graph_exec) cudaGraphExecDestroy(lead->graph_exec);
+      lead->graph_exec = nullptr;
+      lead->graph_key.clear();
+      if (!finalize_small_prepare(lead->cfg.device))  // (function attributes are set outside the capture)
+        return set_err(lead, FF_ERR_CUDA, "leaf finalisation could not be prepared");
+      const unsigned long long before = g_own_launches.load();
+      CK(cudaStreamBeginCapture(lead->stream, cudaStreamCaptureModeThreadLocal));
+      st = issue();
+      cudaGraph_t g = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(lead->stream, &g);
+      cudaGraphExec_t ex = nullptr;
+      if (st != FF_OK || ec != cudaSuccess || !g || cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) {
+        // launches that cannot be recorded here: launch them directly from now on
+        cudaGetLastError();
+        g_own_launches.store(before);
+        lead->graph_failed = true;
+        use_graph = false;
+      } else {
+        lead->graph_exec = ex;
+        lead->graph_key = key;
+        lead->graph_launches = g_own_launches.load() - before;
+        g_own_launches.fetch_sub(lead->graph_launches);  // counted when the graph runs
+      }
+      if (g) cudaGraphDestroy(g);
+    }
+    if (use_graph) {
+      note_launch((unsigned)lead->graph_launches);
+      CK(cudaGraphLaunch(lead->graph_exec, lead->stream));
+      lead->graph_replays++;
+    }
+  }
+  if (!use_graph) {
+    st = issue();
+    if (st != FF_OK) return st;
+  }
   CK(cudaStreamSynchronize(lead->stream));
   double bricks = 0, pending = 0;
   for (int i = 0; i < n; i++) {
@@ -923,6 +1038,7 @@ ff_status ff_get_stats(ff_handle *h, ff_stats *o) {
   o->processed_pixels = h->processed;
   o->new_leaves = h->new_leaves;
   o->dedupe_rounds = h->dedupe_rounds;
+  o->graph_replays = h->graph_replays;
   return FF_OK;
 }
 

@@ -63,8 +63,7 @@ __device__ __forceinline__ void fuse_brick(const uint32_t brick, const ushort4 *
                                            uint16_t *__restrict__ col, const uint16_t *__restrict__ depth,
                                            const uint8_t *__restrict__ bgr, int W, int H, const CamF &q, float scale,
                                            float thr, float scaling, float maxcam, const uint32_t *__restrict__ rtab,
-                                           int rshift, const float *__restrict__ conf) {
-  const int v = threadIdx.x;
+                                           int rshift, const float *__restrict__ conf, const int v) {
   const int x = v & 7, y = (v >> 3) & 7, z = v >> 6;
   const ushort4 o = leaf[brick];
   // the voxel's stored state does not depend on the projection: load it first
@@ -169,12 +168,14 @@ __device__ __forceinline__ bool fuse_deferred(const MapFrame &F) {
   return leaves < F.leaves_max && branches < F.branches_max && outside;
 }
 
-// One 512-thread block per brick, one thread per voxel, blocks looping over
-// the bricks of every map of the batch in order.  Gated: each map's count is
-// read on the device; otherwise the host's count (nq_host) is used.
-template <bool FP16, bool RCP_HOST>
-__global__ void __launch_bounds__(512, 4) k_fuse(const BatchDesc *__restrict__ bd, int gated) {
+// BPC bricks per block of 512 BPC threads, one thread per voxel, blocks
+// looping over the bricks of every map of the batch in order.  Gated: each
+// map's count is read on the device; otherwise the host's count (nq_host)
+// is used.  Every map's camera parameters are staged in shared memory once.
+template <bool FP16, bool RCP_HOST, int BPC, int MINB>
+__global__ void __launch_bounds__(512 * BPC, MINB) k_fuse(const BatchDesc *__restrict__ bd, int gated) {
   __shared__ uint32_t end[BATCH_MAX];  // inclusive prefix of the maps' brick counts
+  __shared__ CamF sq[BATCH_MAX];
   const int nmaps = bd->n;
   if (threadIdx.x == 0) {
     uint32_t acc = 0;
@@ -184,40 +185,51 @@ __global__ void __launch_bounds__(512, 4) k_fuse(const BatchDesc *__restrict__ b
       end[m] = acc;
     }
   }
+  constexpr int CF = sizeof(CamF) / sizeof(float);
+  for (int i = threadIdx.x; i < nmaps * CF; i += blockDim.x)
+    reinterpret_cast<float *>(sq)[i] = reinterpret_cast<const float *>(&bd->f[i / CF].q)[i % CF];
   __syncthreads();
   const uint32_t total = end[nmaps - 1];
-  // the current map's camera parameters, shared by the block
-  __shared__ CamF sq;
-  int m = 0, staged = -1;
-  for (uint32_t b = blockIdx.x; b < total; b += gridDim.x) {
+  const int sub = threadIdx.x >> 9, v = threadIdx.x & 511;
+  int m = 0;
+  for (uint32_t b = blockIdx.x * BPC + sub; b < total; b += gridDim.x * BPC) {
     while (b >= end[m]) m++;
     const MapFrame &F = bd->f[m];
-    if (m != staged) {  // block-uniform
-      __syncthreads();
-      if (threadIdx.x < sizeof(CamF) / sizeof(float))
-        reinterpret_cast<float *>(&sq)[threadIdx.x] = reinterpret_cast<const float *>(&F.q)[threadIdx.x];
-      __syncthreads();
-      staged = m;
-    }
     const uint32_t local = b - (m ? end[m - 1] : 0u);
     fuse_brick<FP16, RCP_HOST>(F.queue[local], F.leaf, F.sdf, F.wgt, F.sdf16, F.wgt16, F.col, F.depth, F.bgr, F.W,
-                               F.H, sq, F.scale, F.thr, F.scaling, F.maxcam, F.rcp_tab, F.rcp_shift, F.conf);
+                               F.H, sq[m], F.scale, F.thr, F.scaling, F.maxcam, F.rcp_tab, F.rcp_shift, F.conf, v);
+  }
+}
+
+// Block shapes of the voxel update: (bricks per block, blocks per SM the
+// register budget is cut for).  Shape 0 is the default.
+static const int FUSE_SHAPES[FUSE_SHAPE_COUNT][2] = {{1, 4}, {1, 3}, {2, 2}, {2, 1}};
+
+template <bool F16, bool RH>
+static void launch_fuse_shape(const BatchDesc *d_batch, int g, int grid, int shape, cudaStream_t s) {
+  switch (shape) {
+    case 1: k_fuse<F16, RH, 1, 3><<<grid, 512, 0, s>>>(d_batch, g); break;
+    case 2: k_fuse<F16, RH, 2, 2><<<grid, 1024, 0, s>>>(d_batch, g); break;
+    case 3: k_fuse<F16, RH, 2, 1><<<grid, 1024, 0, s>>>(d_batch, g); break;
+    default: k_fuse<F16, RH, 1, 4><<<grid, 512, 0, s>>>(d_batch, g); break;
   }
 }
 
 void launch_fuse(const BatchDesc *d_batch, int nmaps, bool gated, int storage, bool rcp_host, int grid,
-                 cudaStream_t s) {
+                 cudaStream_t s, int shape) {
   if (grid <= 0 || nmaps < 1) return;
   const int g = gated ? 1 : 0;
-#define FF_FUSE(F16, RH) k_fuse<F16, RH><<<grid, 512, 0, s>>>(d_batch, g)
   note_launch();
   if (storage == 1) {
-    if (rcp_host) FF_FUSE(true, true); else FF_FUSE(true, false);
+    if (rcp_host) launch_fuse_shape<true, true>(d_batch, g, grid, shape, s);
+    else launch_fuse_shape<true, false>(d_batch, g, grid, shape, s);
   } else {
-    if (rcp_host) FF_FUSE(false, true); else FF_FUSE(false, false);
+    if (rcp_host) launch_fuse_shape<false, true>(d_batch, g, grid, shape, s);
+    else launch_fuse_shape<false, false>(d_batch, g, grid, shape, s);
   }
-#undef FF_FUSE
 }
+
+int fuse_shape_bricks(int shape) { return FUSE_SHAPES[(shape >= 0 && shape < FUSE_SHAPE_COUNT) ? shape : 0][0]; }
 
 // Measure the host CPU's RCPPS for every mantissa of [1,2) and check the
 // exponent/sign/special-value rules that rcp_host() relies on.
@@ -275,8 +287,8 @@ bool build_rcp_table(std::vector<uint32_t> &tab, int &shift) {
 }
 
 cudaError_t prewarm_fuse_kernels() {
-  const void *fns[] = {(const void *)k_fuse<false, false>, (const void *)k_fuse<false, true>,
-                       (const void *)k_fuse<true, false>, (const void *)k_fuse<true, true>};
+  const void *fns[] = {(const void *)k_fuse<false, false, 1, 4>, (const void *)k_fuse<false, true, 1, 4>,
+                       (const void *)k_fuse<true, false, 1, 4>,  (const void *)k_fuse<true, true, 1, 4>};
   for (const void *f : fns) {
     cudaFuncAttributes a;
     cudaError_t e = cudaFuncGetAttributes(&a, f);

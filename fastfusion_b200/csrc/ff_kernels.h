@@ -85,7 +85,7 @@ cudaError_t launch_dedupe(const BatchDesc *d_batch, int m0, int m1, uint32_t til
                           int device, cudaStream_t s);
 
 // Octree descent / allocation of every processed pixel of the batch.
-void launch_insert(const BatchDesc *d_batch, uint32_t total_pix, cudaStream_t s);
+void launch_insert(const BatchDesc *d_batch, uint32_t total_pix, cudaStream_t s, int block = 256);
 
 // Sort scratch size for `n` pending leaves.
 size_t pending_sort_bytes(int n);
@@ -108,6 +108,8 @@ bool finalize_small_fits(uint32_t npix);
 // leaves, one block per map, counts read on the device; for images of up to
 // about 1.6 million pixels (false, nothing launched, for larger ones).
 bool launch_finalize_small(const BatchDesc *d_batch, int nmaps, uint32_t max_npix, int device, cudaStream_t s);
+// Set the finalisation kernel's shared-memory limit on this device (once).
+bool finalize_small_prepare(int device);
 
 // Load the kernels of each file ahead of their first launch.
 cudaError_t prewarm_alloc_kernels();
@@ -123,8 +125,12 @@ void launch_fill(uint32_t *p, size_t n, uint32_t v, cudaStream_t s);
 // (update_functions.cpp:1187-1444).  gated: each map's brick count is read
 // on the device (its queue after the new leaves) and a map whose volume must
 // grow first is left for the host; otherwise MapFrame::nq_host is used.
+// shape: block shape of the update, 0..FUSE_SHAPE_COUNT-1 (bricks per block
+// and the blocks per SM its registers are budgeted for; 0 = 1 brick, 4).
+constexpr int FUSE_SHAPE_COUNT = 4;
 void launch_fuse(const BatchDesc *d_batch, int nmaps, bool gated, int storage, bool rcp_host, int grid,
-                 cudaStream_t s);
+                 cudaStream_t s, int shape = 0);
+int fuse_shape_bricks(int shape);
 
 // Table of the host CPU's RCPPS over the mantissas of [1,2), indexed by the
 // mantissa >> shift (the low bits the instruction ignores are dropped); false

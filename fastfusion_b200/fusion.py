@@ -51,7 +51,13 @@ class ff_stats(ctypes.Structure):
                 ("meshing_ok", ctypes.c_uint32), ("grows", ctypes.c_uint32), ("mesh_vertices", ctypes.c_uint64),
                 ("mesh_faces", ctypes.c_uint64), ("mesh_cells", ctypes.c_uint64),
                 ("mesh_cells_dirty", ctypes.c_uint64), ("processed_pixels", ctypes.c_uint32),
-                ("new_leaves", ctypes.c_uint32), ("dedupe_rounds", ctypes.c_uint32)]
+                ("new_leaves", ctypes.c_uint32), ("dedupe_rounds", ctypes.c_uint32),
+                ("graph_replays", ctypes.c_uint32)]
+
+
+class ff_tuning(ctypes.Structure):
+    _fields_ = [("dedupe_rows", ctypes.c_int), ("fuse_shape", ctypes.c_int), ("fuse_blocks_per_sm", ctypes.c_int),
+                ("insert_block", ctypes.c_int), ("graph", ctypes.c_int)]
 
 
 # Every entry point of include/fastfusion_b200.h with its ctypes signature.
@@ -62,6 +68,7 @@ SIGNATURES = {
     "ff_destroy": (_i32, [_vp]),
     "ff_set_stream": (_i32, [_vp, _vp]),
     "ff_sync": (_i32, [_vp]),
+    "ff_set_tuning": (_i32, [_vp, ctypes.POINTER(ff_tuning)]),
     "ff_add_map_u16": (_i32, [_vp, _vp, _i32, _i32, _sz, _vp, _sz, _vp, _vp, _vp, _f32, _f32, _vp]),
     "ff_add_map_u16_device": (_i32, [_vp, _vp, _vp, _i32, _i32, _vp, _vp, _vp, _f32, _f32, _vp]),
     "ff_add_maps_u16_device": (_i32, [_vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
@@ -373,6 +380,12 @@ class FusionMipMapCPU:
 
     def setDepthChecks(self, depthchecks: int):
         """A no-op in the reference too (its code is commented out)."""
+
+    def set_tuning(self, dedupe_rows: int = 0, fuse_shape: int = 0, fuse_blocks_per_sm: int = 0,
+                   insert_block: int = 0, graph: bool = False):
+        """Launch shapes of the calls this map leads (ff_tuning; 0 = default)."""
+        t = ff_tuning(dedupe_rows, fuse_shape, fuse_blocks_per_sm, insert_block, 1 if graph else 0)
+        self._check(self._L.ff_set_tuning(self._h, ctypes.byref(t)))
 
     def sync(self):
         """Wait for the map's outstanding device work (the last voxel update)."""

@@ -259,14 +259,109 @@ def room_walk_sequence(seed: int = 0, n_frames: int = 1000, width: int = 640, he
     return Sequence(scene=scene, K=K, width=width, height=height, poses=poses, seed=seed)
 
 
+def corridor_scene(seed: int, size=(50.0, 20.0, 3.0), n_prims: int = 400, corridor=(9.0, 11.0),
+                   office: float = 5.0, wall: float = 0.1, door: float = 1.2, prim_size=(0.1, 0.8)) -> Scene:
+    """The large-map layout: a size[0] x size[1] x size[2] m floor with a
+    corridor along x (y in `corridor`), offices of `office` m on both sides
+    behind 0.1 m walls with a door each, and n_prims seeded boxes/spheres in
+    the offices (none in the corridor the camera moves along)."""
+    rng = np.random.default_rng(seed)
+    L, Wd, Ht = size
+    lo, hi = [], []
+    for side in (0, 1):
+        y0 = corridor[0] - wall if side == 0 else corridor[1]
+        for i in range(int(round(L / office))):
+            x0 = i * office
+            mid = x0 + office / 2
+            lo.append([x0, y0, 0.0])                       # corridor wall left of the door
+            hi.append([mid - door / 2, y0 + wall, Ht])
+            lo.append([mid + door / 2, y0, 0.0])           # and right of it
+            hi.append([x0 + office, y0 + wall, Ht])
+            if i > 0:                                      # wall between two offices
+                ya, yb = (0.0, corridor[0] - wall) if side == 0 else (corridor[1] + wall, Wd)
+                lo.append([x0 - wall / 2, ya, 0.0])
+                hi.append([x0 + wall / 2, yb, Ht])
+    wall_lo, wall_hi = np.array(lo), np.array(hi)
+    wall_rgb_boxes = rng.integers(60, 230, (len(lo), 3)).astype(np.uint8)
+    box_lo, box_hi, box_rgb, sph_c, sph_r, sph_rgb = [], [], [], [], [], []
+    while len(box_lo) + len(sph_c) < n_prims:
+        c = rng.uniform(0.0, 1.0, 3) * np.array([L, Wd, Ht])
+        if corridor[0] - 0.6 < c[1] < corridor[1] + 0.6:
+            continue
+        rgb = rng.integers(0, 256, 3).astype(np.uint8)
+        if rng.uniform() < 0.5:
+            ext = rng.uniform(prim_size[0], prim_size[1], 3)
+            box_lo.append(c - ext / 2)
+            box_hi.append(c + ext / 2)
+            box_rgb.append(rgb)
+        else:
+            sph_c.append(c)
+            sph_r.append(float(rng.uniform(prim_size[0], prim_size[1]) / 2))
+            sph_rgb.append(rgb)
+    return Scene(room=np.array(size, dtype=np.float64),
+                 box_lo=np.concatenate([wall_lo, np.array(box_lo).reshape(-1, 3)]),
+                 box_hi=np.concatenate([wall_hi, np.array(box_hi).reshape(-1, 3)]),
+                 box_rgb=np.concatenate([wall_rgb_boxes, np.array(box_rgb, dtype=np.uint8).reshape(-1, 3)]),
+                 sph_c=np.array(sph_c).reshape(-1, 3), sph_r=np.array(sph_r, dtype=np.float64),
+                 sph_rgb=np.array(sph_rgb, dtype=np.uint8).reshape(-1, 3),
+                 wall_rgb=rng.integers(40, 256, (6, 3)).astype(np.uint8))
+
+
+def _catmull_rom(p: np.ndarray, t: float) -> np.ndarray:
+    """Point of the uniform Catmull-Rom spline through points p at t in [0, len(p) - 1]."""
+    i = min(int(t), len(p) - 2)
+    u = t - i
+    p0, p1, p2, p3 = p[max(i - 1, 0)], p[i], p[i + 1], p[min(i + 2, len(p) - 1)]
+    return 0.5 * ((2 * p1) + (-p0 + p2) * u + (2 * p0 - 5 * p1 + 4 * p2 - p3) * u * u +
+                  (-p0 + 3 * p1 - 3 * p2 + p3) * u * u * u)
+
+
+def spline_trajectory(n_frames: int, seed: int, x_range=(2.0, 48.0), y_mid: float = 10.0, y_jitter: float = 0.5,
+                      height=(1.0, 1.6), knot_spacing: float = 4.0, yaw_amp_deg: float = 55.0,
+                      yaw_period: int = 400):
+    """Seeded spline along the corridor: knots every knot_spacing m in x with
+    y jitter and heights U(height); the camera looks along the path, swinging
+    its yaw by +-yaw_amp_deg (period yaw_period frames) into the offices."""
+    rng = np.random.default_rng(seed + 104729)
+    xs = np.arange(x_range[0], x_range[1] + 1e-9, knot_spacing)
+    knots = np.stack([xs, y_mid + rng.uniform(-y_jitter, y_jitter, len(xs)),
+                      rng.uniform(height[0], height[1], len(xs))], axis=1)
+    poses = []
+    for k in range(n_frames):
+        t = (len(knots) - 1) * k / max(n_frames - 1, 1)
+        pos = _catmull_rom(knots, t)
+        ahead = _catmull_rom(knots, min(t + 0.05, len(knots) - 1.0)) - pos
+        if np.linalg.norm(ahead[:2]) < 1e-9:
+            ahead = np.array([1.0, 0.0, 0.0])
+        yaw = math.atan2(ahead[1], ahead[0]) + math.radians(yaw_amp_deg) * math.sin(2 * math.pi * k / yaw_period)
+        d = np.array([math.cos(yaw), math.sin(yaw), -0.1])
+        poses.append((look_at(pos, pos + d), pos.copy()))
+    return poses
+
+
+def corridor_sequence(seed: int = 0, n_frames: int = 10000, width: int = 1280, height: int = 960,
+                      n_prims: int = 400) -> Sequence:
+    """The large-map workload: the 50 x 20 x 3 m corridor/office layout with
+    400 primitives, frames along the seeded spline at 1.0-1.6 m; intrinsics
+    fx = fy = 1050 at 1280 x 960 (scaled with the width)."""
+    s = width / 1280.0
+    K = np.array([1050.0 * s, 1050.0 * s, (width - 1) / 2.0, (height - 1) / 2.0])
+    return Sequence(scene=corridor_scene(seed, n_prims=n_prims), K=K, width=width, height=height,
+                    poses=spline_trajectory(n_frames, seed), seed=seed)
+
+
 def render_torch(scene: Scene, R, t, width: int, height: int, K, seed: int, frame: int, device="cuda",
                  noise_k: float = 0.0012, hole_frac: float = 0.02, flying_frac: float = 0.0,
-                 flying_m: float = 0.1, edge_m: float = 0.05, return_true: bool = False):
+                 flying_m: float = 0.1, edge_m: float = 0.05, return_true: bool = False,
+                 cull_m: float | None = None):
     """render() on a torch device in FP64 (same geometry and colour rules;
     noise and holes from a torch generator seeded by (seed, frame)).
     flying_frac: that fraction of the depth-edge pixels (a 4-neighbour more
     than edge_m away in true depth) is displaced by +-flying_m ("flying
     pixels"), drawn after the noise and the holes.
+    cull_m: primitives farther than this from the camera are left out (a
+    surface beyond it cannot hide a nearer one, so every depth below cull_m
+    is unchanged; use maxcam + a margin).
     Returns (depth uint16 [H,W], bgr uint8 [H,W,3]) as device tensors, plus
     the true depth (float64 [H,W], metres) when return_true."""
     import torch
@@ -289,10 +384,20 @@ def render_torch(scene: Scene, R, t, width: int, height: int, K, seed: int, fram
     side = (d.gather(1, axis[:, None])[:, 0] > 0).long()
     wall = torch.as_tensor(scene.wall_rgb, dtype=torch.uint8, device=dev)
     colour = wall[2 * axis + side]
-    if len(scene.box_lo):
-        lo = torch.as_tensor(scene.box_lo, dtype=f64, device=dev)
-        hi = torch.as_tensor(scene.box_hi, dtype=f64, device=dev)
-        rgb = torch.as_tensor(scene.box_rgb, dtype=torch.uint8, device=dev)
+    box_lo, box_hi, box_rgb = scene.box_lo, scene.box_hi, scene.box_rgb
+    sph_c, sph_r, sph_rgb = scene.sph_c, scene.sph_r, scene.sph_rgb
+    if cull_m is not None:
+        on = np.asarray(t, dtype=np.float64).reshape(3)
+        if len(box_lo):
+            near = np.linalg.norm(np.maximum(np.maximum(box_lo - on, on - box_hi), 0.0), axis=1) < cull_m
+            box_lo, box_hi, box_rgb = box_lo[near], box_hi[near], box_rgb[near]
+        if len(sph_c):
+            near = np.linalg.norm(sph_c - on, axis=1) - sph_r < cull_m
+            sph_c, sph_r, sph_rgb = sph_c[near], sph_r[near], sph_rgb[near]
+    if len(box_lo):
+        lo = torch.as_tensor(box_lo, dtype=f64, device=dev)
+        hi = torch.as_tensor(box_hi, dtype=f64, device=dev)
+        rgb = torch.as_tensor(box_rgb, dtype=torch.uint8, device=dev)
         t1 = (lo[None] - o[None, None]) * inv[:, None]
         t2 = (hi[None] - o[None, None]) * inv[:, None]
         tn = torch.nan_to_num(torch.minimum(t1, t2), nan=-float("inf")).amax(-1)
@@ -302,10 +407,10 @@ def render_torch(scene: Scene, R, t, width: int, height: int, K, seed: int, fram
         closer = tmin < tbest
         tbest = torch.where(closer, tmin, tbest)
         colour = torch.where(closer[:, None], rgb[idx], colour)
-    if len(scene.sph_c):
-        c = torch.as_tensor(scene.sph_c, dtype=f64, device=dev)
-        r = torch.as_tensor(scene.sph_r, dtype=f64, device=dev)
-        rgb = torch.as_tensor(scene.sph_rgb, dtype=torch.uint8, device=dev)
+    if len(sph_c):
+        c = torch.as_tensor(sph_c, dtype=f64, device=dev)
+        r = torch.as_tensor(sph_r, dtype=f64, device=dev)
+        rgb = torch.as_tensor(sph_rgb, dtype=torch.uint8, device=dev)
         oc = o[None] - c
         a = (d * d).sum(1)[:, None]
         b = d @ oc.T

@@ -78,6 +78,7 @@ typedef struct ff_stats {
   uint32_t processed_pixels;   /* pixels that passed the row/column de-duplication */
   uint32_t new_leaves;         /* leaves allocated by the last frame */
   uint32_t dedupe_rounds;      /* rounds the last frame's de-duplication took to settle */
+  uint32_t graph_replays;      /* batched calls led by this map that replayed a recorded CUDA graph */
 } ff_stats;
 
 /* Create a map.  Replaces `new FusionMipMapCPU(0,0,0,scale,threshold,0,color)`
@@ -129,6 +130,29 @@ ff_status ff_add_maps_u16_device(ff_handle *const *maps, int n, const uint16_t *
                                  const uint8_t *const *d_bgr, const int *width, const int *height, const double *K,
                                  const double *R, const double *t, const float *scaling, const float *maxcam,
                                  int32_t *queued);
+
+/* Launch shapes of the per-frame kernels (what the autotuner chooses; 0 in
+ * a field = the default).  dedupe_rows: height of a de-duplication tile, 16
+ * or 32 (default: 16 when all tiles of the call fit one cooperative launch);
+ * fuse_shape: block shape of the voxel update, 0..3 = (1 brick per 512-thread
+ * block, registers for 4 blocks per SM), (1, 3), (2 bricks per 1024-thread
+ * block, 2), (2, 1); fuse_blocks_per_sm: grid of the update in blocks per SM
+ * (default 8 for one brick per block, 4 for two); insert_block: threads per
+ * block of the octree insert (default 256); graph: 1 = ff_add_maps_u16_device
+ * records its launches once as a CUDA graph and replays it while the maps
+ * and image sizes stay the same (no effect while profiling).  Launch shapes
+ * never change results. */
+typedef struct {
+  int dedupe_rows;
+  int fuse_shape;
+  int fuse_blocks_per_sm;
+  int insert_block;
+  int graph;
+} ff_tuning;
+
+/* Set the launch shapes used by calls that this map leads (the map itself,
+ * or a batch whose maps[0] it is). */
+ff_status ff_set_tuning(ff_handle *h, const ff_tuning *t);
 
 /* Re-mesh the cells touched since the last update and rebuild the
  * interleaved mesh.  Replaces FusionMipMapCPU::updateMeshes()

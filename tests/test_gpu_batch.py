@@ -18,8 +18,17 @@ def _maps(n, **kw):
                             **kw) for _ in range(n)]
 
 
-@pytest.mark.parametrize("storage", ["fp32", "fp16"])
-def test_batch_equals_one_by_one(lib_built, storage):
+# launch shapes (ff_tuning) must not change any result: default; the other
+# tile height, two bricks per block, a small grid, wide insert blocks and a
+# replayed CUDA graph
+TUNINGS = {"default": {}, "tuned": dict(dedupe_rows=32, fuse_shape=2, fuse_blocks_per_sm=2, insert_block=512,
+                                        graph=True),
+           "graph": dict(fuse_shape=1, graph=True)}
+
+
+@pytest.mark.parametrize("storage,tuning", [("fp32", "default"), ("fp16", "default"), ("fp32", "tuned"),
+                                            ("fp16", "graph")])
+def test_batch_equals_one_by_one(lib_built, storage, tuning):
     import torch
     from fastfusion_b200.fusion import CameraInfo, add_maps_device
     seqs = []
@@ -31,6 +40,7 @@ def test_batch_equals_one_by_one(lib_built, storage):
     seqs.append((K2, f2, 160, 120))
     batched = _maps(len(seqs), storage=storage)
     alone = _maps(len(seqs), storage=storage)
+    batched[0].set_tuning(**TUNINGS[tuning])
     for k in range(6):
         dd, db, cams, keep = [], [], [], []
         for K, frames, w, h in seqs:
@@ -48,6 +58,9 @@ def test_batch_equals_one_by_one(lib_built, storage):
             assert qa == qb[i], (k, i)
             assert queue_set(m.queue()) == queue_set(batched[i].queue())
     assert batched[0].stats()["grows"] >= 1
+    if TUNINGS[tuning].get("graph"):
+        # the batch's launches (cooperative de-duplication included) were recorded and replayed
+        assert batched[0].stats()["graph_replays"] == 6
     for a, b in zip(alone, batched):
         sa, sb = a.stats(), b.stats()
         assert sa["n"] == sb["n"] and np.array_equal(sa["offset"], sb["offset"])
