@@ -20,6 +20,13 @@ namespace ffb {
 
 __device__ __forceinline__ uint32_t ld_volatile(const uint32_t *p) { return *(volatile const uint32_t *)p; }
 
+// Octree read on the descent, cached in L1.  Safe without coherence: a valid
+// leaf index or child pointer never changes while the insert runs (they are
+// written once; grow() runs between kernels), so a cached read that returns
+// one is exact; a slot another thread claims meanwhile may still read as
+// BRANCHINIT here, and the atomicCAS that follows returns its current value.
+__device__ __forceinline__ uint32_t ld_tree(const uint32_t *p) { return __ldca(p); }
+
 // ---------------------------------------------------------------- bbox ----
 
 // computeBoundingboxIntCPU(ushort), geometryfusion_mipmap_cpu.cpp:1270-1303,
@@ -333,6 +340,9 @@ cudaError_t launch_dedupe(const BatchDesc *d_batch, int m0, int m1, uint32_t til
 
 __device__ __forceinline__ void queue_leaf(uint32_t leaf, uint32_t frame, uint32_t *stamp, uint32_t *queue,
                                            Counters *cnt) {
+  // coarse leaves lie on the paths of many pixels: a plain read first keeps
+  // those repeats off the atomic unit (the exchange below decides the winner)
+  if (ld_volatile(&stamp[leaf]) == frame) return;
   if (atomicExch(&stamp[leaf], frame) != frame) {
     uint32_t q = atomicAdd(&cnt->queued, 1u);
     queue[q] = leaf;
@@ -401,9 +411,9 @@ __global__ void k_insert(const BatchDesc *__restrict__ bd) {
   while ((half >> 1) >= target) {
     uint32_t co = (x >= ox + half) * 1u + (y >= oy + half) * 2u + (z >= oz + half) * 4u;
     uint32_t ptr = branch + co + 8;
-    uint32_t leaf = ld_volatile(tree + ptr - 8);
+    uint32_t leaf = ld_tree(tree + ptr - 8);
     if (leaf < leaves_max) queue_leaf(leaf, frame, stamp, queue, cnt);
-    uint32_t child = ld_volatile(tree + ptr);
+    uint32_t child = ld_tree(tree + ptr);
     if (child == BRANCHINIT) {
       uint32_t old = atomicCAS(tree + ptr, BRANCHINIT, LOCKED);
       if (old == BRANCHINIT) {
@@ -430,7 +440,7 @@ __global__ void k_insert(const BatchDesc *__restrict__ bd) {
   }
   uint32_t co = (x >= ox + half) * 1u + (y >= oy + half) * 2u + (z >= oz + half) * 4u;
   uint32_t ptr = branch + co;
-  uint32_t cur = ld_volatile(tree + ptr);
+  uint32_t cur = ld_tree(tree + ptr);
   if (cur == BRANCHINIT) {
     uint32_t old = atomicCAS(tree + ptr, BRANCHINIT, LOCKED);
     if (old == BRANCHINIT) {
