@@ -110,7 +110,7 @@ class BatchWorkload:
 SPACE = [
     ("fuse_shape", [0, 1, 2, 3]),
     ("fuse_blocks_per_sm", [0, 1, 2, 4, 16]),
-    ("dedupe_rows", [0, 16, 32]),
+    ("dedupe_rows", [0, 8, 16, 32]),
     ("insert_block", [0, 128, 512]),
     ("graph", [False, True]),
 ]

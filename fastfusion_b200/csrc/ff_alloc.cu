@@ -129,6 +129,7 @@ constexpr int DD_WARPS = 4;  // tiles (warps) per block
 // tile height: 16 rows (more, shorter tiles shorten each warp's chain of
 // rows), or 32 when the image has more 16-row tiles than resident warps
 constexpr int DD_ROWS_SHORT = 16, DD_ROWS_TALL = 32;
+constexpr int DD_ROWS_LOW = 8;  // more, shorter tiles again (a tuning choice)
 
 __device__ __forceinline__ bool same3(int a0, int a1, int a2, int b0, int b1, int b2) {
   return a0 == b0 && a1 == b1 && a2 == b2;
@@ -293,8 +294,8 @@ int dedupe_tiles(int W, int H, int *tilesX, int *tilesY, int rows) {
 }
 
 size_t dedupe_boundary_elems(int W, int H) {
-  // sized for the shorter tiles (the larger count)
-  const size_t ntiles = (size_t)dedupe_tiles(W, H, nullptr, nullptr, DD_ROWS_SHORT);
+  // sized for the lowest tiles (the largest count)
+  const size_t ntiles = (size_t)dedupe_tiles(W, H, nullptr, nullptr, DD_ROWS_LOW);
   return ntiles * 32 * 2 + ntiles;  // keys of the right column and bottom row, then 4 bit words per tile
 }
 
@@ -316,7 +317,8 @@ static cudaError_t resident_dedupe_warps(int device, int &warps) {
 
 cudaError_t dedupe_capacity(int device, int rows, uint32_t &tiles) {
   int warps = 0;
-  cudaError_t e = rows == DD_ROWS_SHORT ? resident_dedupe_warps<DD_ROWS_SHORT>(device, warps)
+  cudaError_t e = rows == DD_ROWS_SHORT  ? resident_dedupe_warps<DD_ROWS_SHORT>(device, warps)
+                  : rows == DD_ROWS_LOW ? resident_dedupe_warps<DD_ROWS_LOW>(device, warps)
                                         : resident_dedupe_warps<DD_ROWS_TALL>(device, warps);
   tiles = (uint32_t)warps;
   return e;
@@ -332,7 +334,9 @@ cudaError_t launch_dedupe(const BatchDesc *d_batch, int m0, int m1, uint32_t til
   if ((uint32_t)blocks * DD_WARPS > cap || blocks < 1) return cudaErrorInvalidConfiguration;
   void *args[] = {(void *)&d_batch, (void *)&m0, (void *)&m1, (void *)&barrier};
   note_launch();
-  const void *fn = rows == DD_ROWS_SHORT ? (const void *)k_dedupe<DD_ROWS_SHORT> : (const void *)k_dedupe<DD_ROWS_TALL>;
+  const void *fn = rows == DD_ROWS_SHORT  ? (const void *)k_dedupe<DD_ROWS_SHORT>
+                   : rows == DD_ROWS_LOW ? (const void *)k_dedupe<DD_ROWS_LOW>
+                                         : (const void *)k_dedupe<DD_ROWS_TALL>;
   return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(32 * DD_WARPS), args, 0, s);
 }
 
@@ -704,6 +708,7 @@ void launch_fill(uint32_t *p, size_t n, uint32_t v, cudaStream_t s) {
 // would otherwise land inside the first frame that needs a kernel).
 cudaError_t prewarm_alloc_kernels() {
   const void *fns[] = {(const void *)k_first_bbox, (const void *)k_dedupe<DD_ROWS_SHORT>,
+                       (const void *)k_dedupe<DD_ROWS_LOW>,
                        (const void *)k_dedupe<DD_ROWS_TALL>, (const void *)k_insert,
                        (const void *)k_pending_keys, (const void *)k_finalize, (const void *)k_parents,
                        (const void *)k_finalize_bitmap, (const void *)k_shift_branches,

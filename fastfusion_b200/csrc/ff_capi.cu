@@ -457,10 +457,10 @@ ff_status ff_destroy(ff_handle *h) {
 
 ff_status ff_set_tuning(ff_handle *h, const ff_tuning *t) {
   if (!h || !t) return FF_ERR_BAD_ARG;
-  if ((t->dedupe_rows && t->dedupe_rows != 16 && t->dedupe_rows != 32) || t->fuse_shape < 0 ||
+  if ((t->dedupe_rows && t->dedupe_rows != 8 && t->dedupe_rows != 16 && t->dedupe_rows != 32) || t->fuse_shape < 0 ||
       t->fuse_shape >= FUSE_SHAPE_COUNT || t->fuse_blocks_per_sm < 0 || t->fuse_blocks_per_sm > 64 ||
       (t->insert_block && (t->insert_block < 64 || t->insert_block > 1024 || t->insert_block % 32)))
-    return set_err(h, FF_ERR_BAD_ARG, "ff_set_tuning: dedupe_rows 0/16/32, fuse_shape 0..3, "
+    return set_err(h, FF_ERR_BAD_ARG, "ff_set_tuning: dedupe_rows 0/8/16/32, fuse_shape 0..3, "
                                       "fuse_blocks_per_sm 0..64, insert_block 0 or 64..1024 in steps of 32");
   h->tune = *t;
   h->graph_key.clear();  // launches change: record again
@@ -663,7 +663,13 @@ static ff_status frame_plan(ff_handle *lead, int n, LaunchPlan &lp) {
   CK(dedupe_capacity(lead->cfg.device, 32, cap32));
   int rows = tiles16 <= cap16 ? 16 : 32;
   if (lead->tune.dedupe_rows == 32 || (lead->tune.dedupe_rows == 16 && tiles16 <= cap16)) rows = lead->tune.dedupe_rows;
-  const uint32_t cap = rows == 16 ? cap16 : cap32;
+  uint32_t cap = rows == 16 ? cap16 : cap32;
+  if (lead->tune.dedupe_rows == 8) {
+    uint32_t tiles8 = 0, cap8 = 0;
+    for (int i = 0; i < n; i++) tiles8 += (uint32_t)dedupe_tiles(B.f[i].W, B.f[i].H, nullptr, nullptr, 8);
+    CK(dedupe_capacity(lead->cfg.device, 8, cap8));
+    if (tiles8 <= cap8) rows = 8, cap = cap8;
+  }
   for (int i = 0; i < n; i++) {
     const uint32_t nt = (uint32_t)dedupe_tiles(B.f[i].W, B.f[i].H, &B.f[i].tilesX, &B.f[i].tilesY, rows);
     if (nt > cap) return set_err(lead, FF_ERR_BAD_ARG, "image too large for the de-duplication launch");

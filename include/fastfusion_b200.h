@@ -132,8 +132,9 @@ ff_status ff_add_maps_u16_device(ff_handle *const *maps, int n, const uint16_t *
                                  int32_t *queued);
 
 /* Launch shapes of the per-frame kernels (what the autotuner chooses; 0 in
- * a field = the default).  dedupe_rows: height of a de-duplication tile, 16
- * or 32 (default: 16 when all tiles of the call fit one cooperative launch);
+ * a field = the default).  dedupe_rows: height of a de-duplication tile, 8,
+ * 16 or 32 (default: 16 when all tiles of the call fit one cooperative launch;
+ * 8 only where they fit);
  * fuse_shape: block shape of the voxel update, 0..3 = (1 brick per 512-thread
  * block, registers for 4 blocks per SM), (1, 3), (2 bricks per 1024-thread
  * block, 2), (2, 1); fuse_blocks_per_sm: grid of the update in blocks per SM

@@ -23,11 +23,12 @@ def _maps(n, **kw):
 # replayed CUDA graph
 TUNINGS = {"default": {}, "tuned": dict(dedupe_rows=32, fuse_shape=2, fuse_blocks_per_sm=2, insert_block=512,
                                         graph=True),
-           "graph": dict(fuse_shape=1, graph=True)}
+           "graph": dict(fuse_shape=1, graph=True),
+           "low": dict(dedupe_rows=8, fuse_shape=3)}
 
 
 @pytest.mark.parametrize("storage,tuning", [("fp32", "default"), ("fp16", "default"), ("fp32", "tuned"),
-                                            ("fp16", "graph")])
+                                            ("fp16", "graph"), ("fp32", "low")])
 def test_batch_equals_one_by_one(lib_built, storage, tuning):
     import torch
     from fastfusion_b200.fusion import CameraInfo, add_maps_device
