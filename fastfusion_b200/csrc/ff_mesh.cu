@@ -134,18 +134,22 @@ struct GenCtx {
   uint32_t leaves_max;
 };
 
-__device__ __forceinline__ bool is_sub(const GenCtx &g, const Slot &s) { return g.tree[s.S + 8] < PENDING; }
+// the octree is read-only while the mesh is built: reads go through the
+// read-only data cache
+__device__ __forceinline__ uint32_t tree_at(const GenCtx &g, uint32_t i) { return __ldg(g.tree + i); }
+
+__device__ __forceinline__ bool is_sub(const GenCtx &g, const Slot &s) { return tree_at(g, s.S + 8) < PENDING; }
 
 __device__ __forceinline__ Slot child_of(const GenCtx &g, const Slot &s, int co) {
   Slot r;
-  const uint32_t sub = g.tree[s.S + 8];
+  const uint32_t sub = tree_at(g, s.S + 8);
   const uint16_t h = s.size >> 1;
   r.S = sub + (uint32_t)co;
   r.o[0] = (uint16_t)(s.o[0] + h * (co & 1));
   r.o[1] = (uint16_t)(s.o[1] + h * ((co >> 1) & 1));
   r.o[2] = (uint16_t)(s.o[2] + h * ((co >> 2) & 1));
   r.size = h;
-  const uint32_t lf = g.tree[r.S];
+  const uint32_t lf = tree_at(g, r.S);
   r.la = lf < g.leaves_max ? lf : s.la;
   return r;
 }
@@ -453,7 +457,7 @@ __device__ __forceinline__ void gen_level(const GenCtx &g, const GenQueues &Q, i
           C[co].o[1] = (uint16_t)(h * ((co >> 1) & 1));
           C[co].o[2] = (uint16_t)(h * ((co >> 2) & 1));
           C[co].size = h;
-          const uint32_t lf = g.tree[co];
+          const uint32_t lf = tree_at(g, co);
           C[co].la = lf < g.leaves_max ? lf : BRANCHINIT;
         }
       } else {
@@ -478,7 +482,7 @@ __device__ __forceinline__ void gen_level(const GenCtx &g, const GenQueues &Q, i
   }
 }
 
-__global__ void __launch_bounds__(128) k_gen_level(GenCtx g, GenQueues Q, int lv, uint32_t n) {
+__global__ void __launch_bounds__(128, 6) k_gen_level(GenCtx g, GenQueues Q, int lv, uint32_t n) {
   gen_level(g, Q, lv, n);
 }
 
