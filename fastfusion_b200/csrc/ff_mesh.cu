@@ -888,23 +888,33 @@ __device__ __forceinline__ int warp_excl_scan(int v, int lane, int &total) {
 
 // emit = false: count vertices/faces of each cell into out[]; emit = true:
 // write them at vbase/fbase.
+// The next cell for this warp (work: a counter that starts at zero).
+__device__ __forceinline__ uint32_t next_cell(uint32_t *work, int lane) {
+  uint32_t v = 0;
+  if (lane == 0) v = atomicAdd(work, 1u);
+  return __shfl_sync(0xffffffffu, v, 0);
+}
+
 template <bool EMIT>
 __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, const Cell *__restrict__ cells,
                                                                   uint32_t first, uint32_t ncell,
                                                                   const uint32_t *__restrict__ list, const uint32_t *list_n, CellOut *out,
                                                                   const uint64_t *vbase, const uint64_t *fbase,
-                                                                  float *xyz, uint8_t *rgb, uint32_t *faces) {
+                                                                  float *xyz, uint8_t *rgb, uint32_t *faces,
+                                                                  uint32_t *work) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ McTab T;
   load_mc(T);
   WarpScratch &W = *reinterpret_cast<WarpScratch *>(smem_raw + (size_t)(threadIdx.x >> 5) *
                                                                       (EMIT ? SCRATCH_EMIT_BYTES : SCRATCH_COUNT_BYTES));
   const int lane = threadIdx.x & 31;
+  // the dirty cells: a list of ids, or all cells of [first, first + ncell).
+  // Emit: warps take the next cell from a shared counter (cells differ in
+  // cost); count: a fixed stride (its cells are cheap next to the fetch).
+  const uint32_t n = list ? *list_n : ncell;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-  // the dirty cells: a list of ids, or all cells of [first, first + ncell)
-  const uint32_t n = list ? *list_n : ncell;
-  for (uint32_t ci = gw; ci < n; ci += nw) {
+  for (uint32_t ci = EMIT ? next_cell(work, lane) : gw; ci < n; ci = EMIT ? next_cell(work, lane) : ci + nw) {
     const uint32_t cid = list ? list[ci] : first + ci;
     const Cell c = cells[cid];
     const CellGeom G = cell_geom(m, c);
@@ -1531,7 +1541,7 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   if (first_corner)
     k_mesh_lattice<false><<<lat_blocks, 32 * MESH_WARPS, smem_count, s>>>(vs, I.cells, 0, first_corner, lat_list,
                                                                     I.d_count + 14, I.out, nullptr, nullptr, nullptr,
-                                                                    nullptr, nullptr);
+                                                                    nullptr, nullptr, I.d_count + 16);
   if (ncells > first_corner)
     k_mesh_corner<false><<<(ncells - first_corner + 127) / 128, 128, 0, s>>>(
         vs, I.cells, first_corner, ncells - first_corner, cor_list, I.d_count + 15, I.out, nullptr, nullptr, nullptr,
@@ -1589,7 +1599,7 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   if (first_corner)
     k_mesh_lattice<true><<<lat_blocks, 32 * MESH_WARPS, smem_emit, s>>>(vs, I.cells, 0, first_corner, lat_list,
                                                                    I.d_count + 14, I.out, I.vbase, I.fbase, M.d_xyz,
-                                                                   M.d_rgb, M.d_faces);
+                                                                   M.d_rgb, M.d_faces, I.d_count + 17);
   if (ncells > first_corner)
     k_mesh_corner<true><<<(ncells - first_corner + 127) / 128, 128, 0, s>>>(
         vs, I.cells, first_corner, ncells - first_corner, cor_list, I.d_count + 15, I.out, I.vbase, I.fbase, M.d_xyz,
