@@ -40,8 +40,24 @@ struct ff_handle {
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_bgr_free = nullptr, ev_bgr_ready = nullptr;
   // recorded once a frame's counters have reached the host: a single-map
-  // frame returns then, while its voxel update still runs on the stream
+  // frame returns then, while its voxel update still runs
   cudaEvent_t ev_counters = nullptr;
+  // A single-map frame's voxel update runs on fuse_stream, overlapping the
+  // next frame's allocation kernels on the map's stream.  The buffers the
+  // update reads (descriptor, counters, queue, host-input images, confidence
+  // map) come in two sets used by alternate frames; a set is reused only
+  // after the update that read it (ev_fuse[set]) has finished.
+  cudaStream_t fuse_stream = nullptr;
+  cudaEvent_t ev_fin = nullptr;
+  cudaEvent_t ev_fuse[2] = {nullptr, nullptr};
+  int last_fuse = -1;  // set of the last update launched on fuse_stream
+  int set = 0;
+  BatchDesc *d_batch_set[2] = {nullptr, nullptr}, *h_batch_set[2] = {nullptr, nullptr};
+  Counters *d_cnt_set[2] = {nullptr, nullptr}, *h_cnt_set[2] = {nullptr, nullptr};
+  uint32_t *d_queue_set[2] = {nullptr, nullptr};
+  uint16_t *d_depth_set[2] = {nullptr, nullptr};
+  uint8_t *d_bgr_set[2] = {nullptr, nullptr};
+  float *d_conf_set[2] = {nullptr, nullptr};
   // the frame descriptor(s) the per-frame kernels read: this map's own, or a
   // whole batch when this handle leads ff_add_maps_u16_device
   BatchDesc *d_batch = nullptr, *h_batch = nullptr;
@@ -123,6 +139,24 @@ static thread_local std::string g_create_error;
 static ff_status set_err(ff_handle *h, ff_status s, const std::string &m) {
   if (h) h->err = m;
   return s;
+}
+
+// Make the per-frame buffers of set k current.
+static void select_set(ff_handle *h, int k) {
+  h->set = k;
+  h->d_batch = h->d_batch_set[k];
+  h->h_batch = h->h_batch_set[k];
+  h->d_cnt = h->d_cnt_set[k];
+  h->h_cnt = h->h_cnt_set[k];
+  h->d_queue = h->d_queue_set[k];
+  h->d_depth = h->d_depth_set[k];
+  h->d_bgr = h->d_bgr_set[k];
+  h->d_conf = h->d_conf_set[k];
+}
+
+// Order the map's stream after every voxel update launched on fuse_stream.
+static cudaError_t join_fuse(ff_handle *h) {
+  return h->last_fuse >= 0 ? cudaStreamWaitEvent(h->stream, h->ev_fuse[h->last_fuse], 0) : cudaSuccess;
 }
 
 // ----------------------------------------------------------- camera math --
@@ -263,16 +297,22 @@ static cudaError_t alloc(T **p, size_t count) {
 static ff_status ensure_image(ff_handle *h, int W, int H) {
   int npix = W * H;
   if (npix > h->cap_pix) {
-    cudaFree(h->d_depth);
-    cudaFree(h->d_bgr);
+    for (int k = 0; k < 2; k++) {
+      cudaFree(h->d_depth_set[k]);
+      cudaFree(h->d_bgr_set[k]);
+      h->d_depth_set[k] = nullptr;
+      h->d_bgr_set[k] = nullptr;
+    }
     cudaFree(h->d_vox);
     cudaFree(h->d_proc);
     cudaFree(h->d_pend);
     cudaFree(h->d_keys);
     cudaFree(h->d_sort_tmp);
-    h->d_depth = nullptr;
-    CK(alloc(&h->d_depth, npix));
-    CK(alloc(&h->d_bgr, (size_t)npix * 3));
+    for (int k = 0; k < 2; k++) {
+      CK(alloc(&h->d_depth_set[k], npix));
+      CK(alloc(&h->d_bgr_set[k], (size_t)npix * 3));
+    }
+    select_set(h, h->set);
     CK(alloc(&h->d_vox, npix));
     CK(alloc(&h->d_proc, npix));
     CK(alloc(&h->d_pend, npix));
@@ -364,7 +404,8 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
     size_t L = h->cfg.leaves_max;
     if (alloc(&h->d_tree, h->cfg.branches_max) != cudaSuccess) { fail(FF_ERR_OOM_POOL, "tree"); break; }
     if (alloc(&h->d_leaf, L) != cudaSuccess || alloc(&h->d_parent, L) != cudaSuccess ||
-        alloc(&h->d_stamp, L) != cudaSuccess || alloc(&h->d_queue, L) != cudaSuccess) {
+        alloc(&h->d_stamp, L) != cudaSuccess || alloc(&h->d_queue_set[0], L) != cudaSuccess ||
+        alloc(&h->d_queue_set[1], L) != cudaSuccess) {
       fail(FF_ERR_OOM_POOL, "leaf table");
       break;
     }
@@ -380,13 +421,25 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
       }
     }
     if (alloc(&h->d_col, L * 1536) != cudaSuccess) { fail(FF_ERR_OOM_POOL, "colour pool"); break; }
-    if (alloc(&h->d_cnt, 1) != cudaSuccess || alloc(&h->d_barrier, BARRIER_WORDS) != cudaSuccess) { fail(FF_ERR_CUDA, "counters"); break; }
-    if (cudaMallocHost((void **)&h->h_cnt, sizeof(Counters)) != cudaSuccess) { fail(FF_ERR_CUDA, "pinned"); break; }
-    if (cudaMalloc((void **)&h->d_batch, sizeof(BatchDesc)) != cudaSuccess ||
-        cudaMallocHost((void **)&h->h_batch, sizeof(BatchDesc)) != cudaSuccess) {
+    if (alloc(&h->d_cnt_set[0], 1) != cudaSuccess || alloc(&h->d_cnt_set[1], 1) != cudaSuccess ||
+        alloc(&h->d_barrier, BARRIER_WORDS) != cudaSuccess) { fail(FF_ERR_CUDA, "counters"); break; }
+    if (cudaMallocHost((void **)&h->h_cnt_set[0], sizeof(Counters)) != cudaSuccess ||
+        cudaMallocHost((void **)&h->h_cnt_set[1], sizeof(Counters)) != cudaSuccess) { fail(FF_ERR_CUDA, "pinned"); break; }
+    if (cudaMalloc((void **)&h->d_batch_set[0], sizeof(BatchDesc)) != cudaSuccess ||
+        cudaMalloc((void **)&h->d_batch_set[1], sizeof(BatchDesc)) != cudaSuccess ||
+        cudaMallocHost((void **)&h->h_batch_set[0], sizeof(BatchDesc)) != cudaSuccess ||
+        cudaMallocHost((void **)&h->h_batch_set[1], sizeof(BatchDesc)) != cudaSuccess) {
       fail(FF_ERR_CUDA, "frame descriptors");
       break;
     }
+    if (cudaStreamCreateWithFlags(&h->fuse_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_fin, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_fuse[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_fuse[1], cudaEventDisableTiming) != cudaSuccess) {
+      fail(FF_ERR_CUDA, "update stream");
+      break;
+    }
+    select_set(h, 0);
     if (cfg->rcp_mode == FF_RCP_HOST) {
       std::vector<uint32_t> tab;
       if (!build_rcp_table(tab, h->rcp_shift)) {
@@ -430,18 +483,25 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
 ff_status ff_destroy(ff_handle *h) {
   if (!h) return FF_ERR_BAD_ARG;
   cudaSetDevice(h->cfg.device);
+  if (h->fuse_stream) cudaStreamSynchronize(h->fuse_stream);
   if (h->stream) cudaStreamSynchronize(h->stream);
   mesh_free(h->mesh);
   h->prof.destroy();
   void *ptrs[] = {h->d_tree, h->d_leaf, h->d_parent, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
-                  h->d_stamp, h->d_queue, h->d_cnt, h->d_barrier, h->d_depth, h->d_bgr, h->d_pxp, h->d_pyp,
-                  h->d_vox, h->d_proc, h->d_bnd, h->d_pend, h->d_keys, h->d_sort_tmp, h->d_rcp_tab,
-                  h->d_cnn_params, h->d_cnn_packed, h->d_feat, h->d_a1, h->d_a2, h->d_conf};
+                  h->d_stamp, h->d_queue_set[0], h->d_queue_set[1], h->d_cnt_set[0], h->d_cnt_set[1],
+                  h->d_barrier, h->d_depth_set[0], h->d_depth_set[1], h->d_bgr_set[0], h->d_bgr_set[1], h->d_pxp,
+                  h->d_pyp, h->d_vox, h->d_proc, h->d_bnd, h->d_pend, h->d_keys, h->d_sort_tmp, h->d_rcp_tab,
+                  h->d_cnn_params, h->d_cnn_packed, h->d_feat, h->d_a1, h->d_a2, h->d_conf_set[0], h->d_conf_set[1],
+                  h->d_batch_set[0], h->d_batch_set[1]};
   for (void *p : ptrs)
     if (p) cudaFree(p);
-  if (h->h_cnt) cudaFreeHost(h->h_cnt);
-  if (h->d_batch) cudaFree(h->d_batch);
-  if (h->h_batch) cudaFreeHost(h->h_batch);
+  for (int k = 0; k < 2; k++) {
+    if (h->h_cnt_set[k]) cudaFreeHost(h->h_cnt_set[k]);
+    if (h->h_batch_set[k]) cudaFreeHost(h->h_batch_set[k]);
+    if (h->ev_fuse[k]) cudaEventDestroy(h->ev_fuse[k]);
+  }
+  if (h->ev_fin) cudaEventDestroy(h->ev_fin);
+  if (h->fuse_stream) cudaStreamDestroy(h->fuse_stream);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   if (h->copy_stream) {
     cudaStreamSynchronize(h->copy_stream);
@@ -470,6 +530,7 @@ ff_status ff_set_tuning(ff_handle *h, const ff_tuning *t) {
 ff_status ff_sync(ff_handle *h) {
   if (!h) return FF_ERR_BAD_ARG;
   CK(cudaSetDevice(h->cfg.device));
+  CK(join_fuse(h));
   CK(cudaStreamSynchronize(h->stream));
   return FF_OK;
 }
@@ -477,6 +538,7 @@ ff_status ff_sync(ff_handle *h) {
 ff_status ff_set_stream(ff_handle *h, void *cuda_stream) {
   if (!h) return FF_ERR_BAD_ARG;
   cudaSetDevice(h->cfg.device);
+  join_fuse(h);
   cudaStreamSynchronize(h->stream);
   if (h->own_stream) cudaStreamDestroy(h->stream);
   if (cuda_stream) {
@@ -615,14 +677,18 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
       cudaFree(h->d_feat);
       cudaFree(h->d_a1);
       cudaFree(h->d_a2);
-      cudaFree(h->d_conf);
       h->d_feat = h->d_a1 = h->d_a2 = nullptr;
-      h->d_conf = nullptr;
+      for (int k = 0; k < 2; k++) {
+        cudaFree(h->d_conf_set[k]);
+        h->d_conf_set[k] = nullptr;
+      }
       h->conf_cap = 0;
       CK(alloc(&h->d_feat, npx * CNN_FEAT_CH));
       CK(alloc(&h->d_a1, npx * CNN_HIDDEN));
       CK(alloc(&h->d_a2, npx * CNN_HIDDEN));
-      CK(alloc(&h->d_conf, npx));
+      CK(alloc(&h->d_conf_set[0], npx));
+      CK(alloc(&h->d_conf_set[1], npx));
+      h->d_conf = h->d_conf_set[h->set];
       h->conf_cap = npx;
     }
     const float kf[4] = {(float)K[0], (float)K[1], (float)K[2], (float)K[3]};
@@ -730,7 +796,7 @@ static ff_status frame_launch(ff_handle *lead, int n) {
 // counters: a single map's counters are copied to the host between the
 // finalisation and the update, and this event recorded after the copy.
 static ff_status frame_launch_update(ff_handle *lead, int n, uint32_t max_npix, int &pi_fin, int &pi_fuse,
-                                     cudaEvent_t counters = nullptr) {
+                                     cudaEvent_t counters = nullptr, bool side = false) {
   ff_handle *h = lead;  // (error reporting)
   cudaStream_t s = lead->stream;
   pi_fin = lead->prof.begin(ST_FINALIZE, s);
@@ -741,13 +807,24 @@ static ff_status frame_launch_update(ff_handle *lead, int n, uint32_t max_npix, 
     CK(cudaMemcpyAsync(lead->h_cnt, lead->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
     CK(cudaEventRecord(counters, s));
   }
-  pi_fuse = lead->prof.begin(ST_FUSE, s);
+  // side: the update runs on fuse_stream once this frame's leaves are final
+  cudaStream_t fs = s;
+  if (side) {
+    fs = lead->fuse_stream;
+    CK(cudaEventRecord(lead->ev_fin, s));
+    CK(cudaStreamWaitEvent(fs, lead->ev_fin, 0));
+  }
+  pi_fuse = lead->prof.begin(ST_FUSE, fs);
   // enough blocks for a frame's bricks in one pass; blocks loop over larger batches
   const int shape = lead->tune.fuse_shape;
   const int per_sm = lead->tune.fuse_blocks_per_sm > 0 ? lead->tune.fuse_blocks_per_sm : 8 / fuse_shape_bricks(shape);
-  launch_fuse(lead->d_batch, n, true, lead->cfg.storage, lead->d_rcp_tab != nullptr, lead->sm_count * per_sm, s,
+  launch_fuse(lead->d_batch, n, true, lead->cfg.storage, lead->d_rcp_tab != nullptr, lead->sm_count * per_sm, fs,
               shape);
-  lead->prof.end(pi_fuse, 0.0, s);
+  lead->prof.end(pi_fuse, 0.0, fs);
+  if (side) {
+    CK(cudaEventRecord(lead->ev_fuse[lead->set], fs));
+    lead->last_fuse = lead->set;
+  }
   CK(cudaGetLastError());
   return FF_OK;
 }
@@ -791,7 +868,9 @@ static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf,
   if (h->leaves_used < h->cfg.leaves_max && h->branches_used < h->cfg.branches_max &&
       (hc.box_min[0] < 0 || hc.box_min[1] < 0 || hc.box_min[2] < 0 || hc.box_max[0] >= (int)h->n ||
        hc.box_max[1] >= (int)h->n || hc.box_max[2] >= (int)h->n)) {
-    // (with one synchronisation the update stood aside for this)
+    // (with one synchronisation the update stood aside for this); the growth
+    // moves leaf positions that updates still in flight read
+    CK(join_fuse(h));
     int pi = h->prof.begin(ST_GROW, s);
     const double tree_bytes = (double)h->branches_used * 4 * 2 + (double)h->leaves_used * 8 * 2;
     ff_status st = grow(h, hc.box_min, hc.box_max);
@@ -803,6 +882,7 @@ static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf,
   // (4+4 B, or 2+2 B in FP16) and three 16-bit colour channels
   const double brick_bytes = 512.0 * 2 * ((h->cfg.storage == FF_STORAGE_FP16 ? 4 : 8) + 6);
   if (fuse_now && nq) {
+    CK(join_fuse(h));  // after the previous frames' updates
     // this map's own descriptor, with the host's count (leaf positions may
     // have moved with the growth; the camera parameters are the frame's)
     mf.nq_host = nq;
@@ -846,14 +926,26 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
     // the frame returns once its counters are on the host; its voxel update
     // (gated on the device) keeps running, ordered before anything that
     // follows on the stream
-    st = frame_launch_update(h, 1, (uint32_t)(W * H), pi_fin, pi_fuse, h->ev_counters);
+    st = frame_launch_update(h, 1, (uint32_t)(W * H), pi_fin, pi_fuse, h->ev_counters, true);
     if (st != FF_OK) return st;
     CK(cudaEventSynchronize(h->ev_counters));
   } else {
     CK(cudaMemcpyAsync(h->h_cnt, h->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
   }
-  return frame_finish(h, plan, mf, pi_fin, pi_fuse, queued);
+  st = frame_finish(h, plan, mf, pi_fin, pi_fuse, queued);
+  // the previous frame's update has finished reading its images
+  if (st == FF_OK && h->last_fuse >= 0) CK(cudaEventSynchronize(h->ev_fuse[h->set ^ 1]));
+  return st;
+}
+
+// Before a single-map frame: its buffer set, free once the update two frames
+// back has finished with it.
+static ff_status begin_frame(ff_handle *h) {
+  const int k = (int)(h->frames & 1u);
+  select_set(h, k);
+  CK(cudaStreamWaitEvent(h->stream, h->ev_fuse[k], 0));
+  return FF_OK;
 }
 
 ff_status ff_add_map_u16(ff_handle *h, const uint16_t *depth, int width, int height, size_t depth_pitch,
@@ -865,6 +957,8 @@ ff_status ff_add_map_u16(ff_handle *h, const uint16_t *depth, int width, int hei
   CK(cudaSetDevice(h->cfg.device));
   ff_status st = ensure_image(h, width, height);
   if (st != FF_OK) return st;
+  st = begin_frame(h);
+  if (st != FF_OK) return st;
   if (!depth_pitch) depth_pitch = sizeof(uint16_t) * width;
   if (!bgr_pitch) bgr_pitch = 3 * (size_t)width;
   CK(cudaMemcpy2DAsync(h->d_depth, sizeof(uint16_t) * width, depth, depth_pitch, sizeof(uint16_t) * width, height,
@@ -873,6 +967,7 @@ ff_status ff_add_map_u16(ff_handle *h, const uint16_t *depth, int width, int hei
   // d_bgr) and overlaps this frame's allocation kernels
   CK(cudaEventRecord(h->ev_bgr_free, h->stream));
   CK(cudaStreamWaitEvent(h->copy_stream, h->ev_bgr_free, 0));
+  CK(cudaStreamWaitEvent(h->copy_stream, h->ev_fuse[h->set], 0));  // this set's last reader
   CK(cudaMemcpy2DAsync(h->d_bgr, 3 * (size_t)width, bgr, bgr_pitch, 3 * (size_t)width, height,
                        cudaMemcpyHostToDevice, h->copy_stream));
   CK(cudaEventRecord(h->ev_bgr_ready, h->copy_stream));
@@ -890,6 +985,8 @@ ff_status ff_add_map_u16_device(ff_handle *h, const uint16_t *d_depth, const uin
     return set_err(h, FF_ERR_BAD_ARG, "ff_add_map_u16_device: NULL pointer or empty image");
   CK(cudaSetDevice(h->cfg.device));
   ff_status st = ensure_image(h, width, height);
+  if (st != FF_OK) return st;
+  st = begin_frame(h);
   if (st != FF_OK) return st;
   return add_map_device(h, d_depth, d_bgr, false, width, height, K, R, t, scaling, maxcam, queued);
 }
@@ -936,6 +1033,7 @@ ff_status ff_add_maps_u16_device(ff_handle *const *maps, int n, const uint16_t *
   std::vector<MapFrame> mf(n);
   for (int i = 0; i < n; i++) {
     ff_handle *m = maps[i];
+    CK(join_fuse(m));  // single-map frames' updates still in flight
     CK(cudaStreamSynchronize(m->stream));
     ff_status st = ensure_image(m, width[i], height[i]);
     if (st != FF_OK) return st;
@@ -969,7 +1067,7 @@ ff_status ff_add_maps_u16_device(ff_handle *const *maps, int n, const uint16_t *
                                  (uint64_t)lead->tune.fuse_shape, (uint64_t)lead->tune.fuse_blocks_per_sm,
                                  (uint64_t)lead->tune.insert_block, (uint64_t)(uintptr_t)lead->stream};
     for (int i = 0; i < n; i++) {
-      key.push_back((uint64_t)(uintptr_t)maps[i]);
+      key.push_back((uint64_t)(uintptr_t)maps[i] ^ (uint64_t)maps[i]->set);  // (its buffer set)
       key.push_back(((uint64_t)width[i] << 32) | (uint32_t)height[i]);
     }
     if (!lead->graph_exec || key != lead->graph_key) {
@@ -1051,6 +1149,7 @@ ff_status ff_get_stats(ff_handle *h, ff_stats *o) {
 ff_status ff_get_leaves(ff_handle *h, uint16_t *pos, uint16_t *scale, uint32_t *parent) {
   if (!h || !pos || !scale || !parent) return FF_ERR_BAD_ARG;
   CK(cudaSetDevice(h->cfg.device));
+  CK(join_fuse(h));
   uint32_t n = std::min(h->leaves_used, h->cfg.leaves_max);
   std::vector<ushort4> tmp(n);
   if (n) {
@@ -1070,6 +1169,7 @@ ff_status ff_get_leaves(ff_handle *h, uint16_t *pos, uint16_t *scale, uint32_t *
 ff_status ff_get_queue(ff_handle *h, uint32_t *leaves) {
   if (!h || !leaves) return FF_ERR_BAD_ARG;
   CK(cudaSetDevice(h->cfg.device));
+  CK(join_fuse(h));
   if (h->queued) CK(cudaMemcpyAsync(leaves, h->d_queue, sizeof(uint32_t) * h->queued, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return FF_OK;
@@ -1078,6 +1178,7 @@ ff_status ff_get_queue(ff_handle *h, uint32_t *leaves) {
 ff_status ff_get_tree(ff_handle *h, uint32_t *tree) {
   if (!h || !tree) return FF_ERR_BAD_ARG;
   CK(cudaSetDevice(h->cfg.device));
+  CK(join_fuse(h));
   CK(cudaMemcpyAsync(tree, h->d_tree, sizeof(uint32_t) * h->branches_used, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return FF_OK;
@@ -1087,6 +1188,7 @@ ff_status ff_get_bricks(ff_handle *h, uint32_t first, uint32_t count, float *sdf
   if (!h || !sdf || !weight || !rgb) return FF_ERR_BAD_ARG;
   if ((uint64_t)first + count > h->cfg.leaves_max) return set_err(h, FF_ERR_BAD_ARG, "ff_get_bricks: range");
   CK(cudaSetDevice(h->cfg.device));
+  CK(join_fuse(h));
   size_t nv = (size_t)count * 512;
   if (h->cfg.storage == FF_STORAGE_FP16) {
     std::vector<__half> a(nv), b(nv);
@@ -1115,6 +1217,7 @@ ff_status ff_set_bricks(ff_handle *h, uint32_t first, uint32_t count, const floa
   if (!h || !sdf || !weight || !rgb) return FF_ERR_BAD_ARG;
   if ((uint64_t)first + count > h->cfg.leaves_max) return set_err(h, FF_ERR_BAD_ARG, "ff_set_bricks: range");
   CK(cudaSetDevice(h->cfg.device));
+  CK(join_fuse(h));
   size_t nv = (size_t)count * 512;
   if (h->cfg.storage == FF_STORAGE_FP16) {
     std::vector<__half> a(nv), b(nv);
@@ -1146,6 +1249,7 @@ ff_status ff_set_state(ff_handle *h, uint32_t n, const float offset[3], const ui
   if (branches_used > h->cfg.branches_max || leaves_used > h->cfg.leaves_max || (branches_used & 15))
     return set_err(h, FF_ERR_BAD_ARG, "ff_set_state: state larger than this map's capacity");
   CK(cudaSetDevice(h->cfg.device));
+  CK(join_fuse(h));
   launch_fill(h->d_tree, h->cfg.branches_max, BRANCHINIT, h->stream);
   CK(cudaMemcpyAsync(h->d_tree, tree, sizeof(uint32_t) * branches_used, cudaMemcpyHostToDevice, h->stream));
   std::vector<ushort4> lp(leaves_used);
@@ -1172,6 +1276,7 @@ ff_status ff_set_state(ff_handle *h, uint32_t n, const float offset[3], const ui
 ff_status ff_update_meshes(ff_handle *h, int *updated) {
   if (!h) return FF_ERR_BAD_ARG;
   CK(cudaSetDevice(h->cfg.device));
+  CK(join_fuse(h));
   if (!h->meshing_ok || !h->n) {
     if (updated) *updated = 1;
     return FF_OK;
@@ -1222,6 +1327,8 @@ ff_status ff_profile(ff_handle *h, int enable) {
 ff_status ff_profile_read(ff_handle *h, double *ms, double *bytes, uint64_t *launches) {
   if (!h || !ms || !bytes || !launches) return FF_ERR_BAD_ARG;
   CK(cudaSetDevice(h->cfg.device));
+  CK(join_fuse(h));
+  CK(cudaStreamSynchronize(h->fuse_stream));
   h->prof.flush();
   for (int i = 0; i < FF_PROFILE_STAGES; i++) {
     ms[i] = h->prof.ms[i];
@@ -1356,6 +1463,7 @@ ff_status ff_raycast_depth(ff_handle *h, const double K[4], const double R[9], c
     return set_err(h, FF_ERR_BAD_ARG, "ff_raycast_depth: window must be in (0, 4] m and step in [1e-4, window]");
   if (!h->n) return set_err(h, FF_ERR_BAD_ARG, "ff_raycast_depth: the map holds no frame");
   CK(cudaSetDevice(h->cfg.device));
+  CK(join_fuse(h));
   RaycastMap m;
   m.tree = h->d_tree;
   m.leaf = h->d_leaf;
