@@ -110,6 +110,10 @@ struct ff_handle {
   size_t conf_cap = 0;  // pixels the buffers hold
   int conf_w = 0, conf_h = 0;  // size of the last confidence map
 
+  // brick ownership (ff_set_shard) and the voxels grow() has moved the grid by
+  uint32_t shard = 0, shards = 1;
+  int32_t shift[3] = {0, 0, 0};
+
   // launch shapes (ff_set_tuning) and the device's SM count
   ff_tuning tune = {0, 0, 0, 0, 0};
   int sm_count = 148;
@@ -280,7 +284,10 @@ static ff_status grow(ff_handle *h, const int *box_min, const int *box_max) {
   }
   for (auto &l : links) CK(cudaMemcpyAsync(h->d_tree + l.first, &l.second, 4, cudaMemcpyHostToDevice, s));
   CK(cudaStreamSynchronize(s));  // `links` lives on this stack frame
-  for (int r = 0; r < 3; r++) h->offset[r] -= (float)add[r] * h->cfg.scale;
+  for (int r = 0; r < 3; r++) {
+    h->offset[r] -= (float)add[r] * h->cfg.scale;
+    h->shift[r] += (int32_t)add[r];
+  }
   uint32_t nl = std::min(h->leaves_used, h->cfg.leaves_max);
   launch_shift_leaves(h->d_leaf, nl, make_ushort3(add[0], add[1], add[2]), s);
   h->grows++;
@@ -515,6 +522,16 @@ ff_status ff_destroy(ff_handle *h) {
   return FF_OK;
 }
 
+ff_status ff_set_shard(ff_handle *h, int shard, int shards) {
+  if (!h) return FF_ERR_BAD_ARG;
+  if (shards < 1 || shard < 0 || shard >= shards)
+    return set_err(h, FF_ERR_BAD_ARG, "ff_set_shard: need 0 <= shard < shards");
+  if (h->frames || h->n) return set_err(h, FF_ERR_BAD_ARG, "ff_set_shard: set before the first frame");
+  h->shard = (uint32_t)shard;
+  h->shards = (uint32_t)shards;
+  return FF_OK;
+}
+
 ff_status ff_set_tuning(ff_handle *h, const ff_tuning *t) {
   if (!h || !t) return FF_ERR_BAD_ARG;
   if ((t->dedupe_rows && t->dedupe_rows != 8 && t->dedupe_rows != 16 && t->dedupe_rows != 32) || t->fuse_shape < 0 ||
@@ -670,6 +687,9 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
   mf.rcp_tab = h->d_rcp_tab;
   mf.rcp_shift = h->rcp_shift;
   mf.conf = nullptr;
+  mf.shard = h->shard;
+  mf.shards = h->shards;
+  for (int r = 0; r < 3; r++) mf.shift[r] = h->shift[r];
   if (h->conf_tau_cm > 0.0f) {
     // the frame's confidence map, ahead of the launches that read it on this stream
     const size_t npx = (size_t)W * H;

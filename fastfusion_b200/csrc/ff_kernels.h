@@ -42,6 +42,11 @@ struct MapFrame {
   const uint32_t *rcp_tab;
   int rcp_shift;
   const float *conf;  // learned per-pixel confidence of the frame, or null (the reference's weight)
+  // brick ownership: a map that is one of `shards` parts of a larger map
+  // keeps only the bricks whose key hashes to `shard`; shift = the voxels
+  // grow() has moved the grid by, so that keys do not change with growth
+  uint32_t shard, shards;
+  int32_t shift[3];
 };
 
 constexpr int BATCH_MAX = 32;

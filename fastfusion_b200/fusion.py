@@ -69,6 +69,7 @@ SIGNATURES = {
     "ff_set_stream": (_i32, [_vp, _vp]),
     "ff_sync": (_i32, [_vp]),
     "ff_set_tuning": (_i32, [_vp, ctypes.POINTER(ff_tuning)]),
+    "ff_set_shard": (_i32, [_vp, _i32, _i32]),
     "ff_add_map_u16": (_i32, [_vp, _vp, _i32, _i32, _sz, _vp, _sz, _vp, _vp, _vp, _f32, _f32, _vp]),
     "ff_add_map_u16_device": (_i32, [_vp, _vp, _vp, _i32, _i32, _vp, _vp, _vp, _f32, _f32, _vp]),
     "ff_add_maps_u16_device": (_i32, [_vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
@@ -386,6 +387,11 @@ class FusionMipMapCPU:
         """Launch shapes of the calls this map leads (ff_tuning; 0 = default)."""
         t = ff_tuning(dedupe_rows, fuse_shape, fuse_blocks_per_sm, insert_block, 1 if graph else 0)
         self._check(self._L.ff_set_tuning(self._h, ctypes.byref(t)))
+
+    def set_shard(self, shard: int, shards: int):
+        """Make this map part `shard` of `shards` of a larger map (brick
+        ownership by a hash of each brick's key); before the first frame."""
+        self._check(self._L.ff_set_shard(self._h, int(shard), int(shards)))
 
     def sync(self):
         """Wait for the map's outstanding device work (the last voxel update)."""

@@ -151,6 +151,19 @@ typedef struct {
   int graph;
 } ff_tuning;
 
+/* Make this map one of `shards` parts of a larger map (call before its first
+ * frame; no counterpart in the reference, which fuses one map on one
+ * machine).  Every part is given every frame; a part creates and updates only
+ * the bricks whose key -- the brick's origin in units of its own edge,
+ * independent of volume growth, and its size -- hashes to `shard`, and
+ * queues the coarser bricks it holds on a pixel's path exactly as the whole
+ * map would.  The parts' bricks are disjoint and together are the whole
+ * map's, each with the whole map's voxel values; the queued counts add up to
+ * the whole map's.  Leaf indices and parent links are per part.  Meshing a
+ * part covers its own bricks; the cells between bricks of different parts
+ * need the other parts' bricks, which this library does not exchange. */
+ff_status ff_set_shard(ff_handle *h, int shard, int shards);
+
 /* Set the launch shapes used by calls that this map leads (the map itself,
  * or a batch whose maps[0] it is). */
 ff_status ff_set_tuning(ff_handle *h, const ff_tuning *t);
