@@ -115,7 +115,12 @@ __device__ __forceinline__ void fuse_brick(const uint32_t brick, const ushort4 *
   const int cyi = max(min(imy, H - 1), 0);
   const int cxi = max(min(imx, W - 1), 0);
   const int ii = W * cyi + cxi;
-  const float h = __fmul_rz(scaling, (float)__ldg(depth + ii));
+  // every gather at the pixel is issued before any of them is used
+  const uint16_t draw = __ldg(depth + ii);
+  const uint8_t *p8 = bgr + 3 * (size_t)ii;
+  const uint8_t cr = __ldg(p8 + 2), cg = __ldg(p8 + 1), cbl = __ldg(p8 + 0);
+  const float cw = conf ? __ldg(conf + ii) : 1.0f;
+  const float h = __fmul_rz(scaling, (float)draw);
   const float dInc = __fsub_rz(len, __fmul_rz(__fmul_rz(len, rc), h));
   const bool mask = pz > 0.0f && imy < H && imy > -1 && imx < W && imx > -1 && h < maxcam;
   const float thrD = __fmul_rz(thr, ls);
@@ -125,7 +130,7 @@ __device__ __forceinline__ void fuse_brick(const uint32_t brick, const ushort4 *
   const float fall = __fmul_rz(__fsub_rz(thrW, dInc), rcp_upd<RCP_HOST>(__fsub_rz(thrW, DIST_W_EPS), rtab, rshift));
   float wInc = mask ? __fadd_rz(front, __fmul_rz(fall, back)) : 0.0f;
   // learned weight: the ramp's increment scaled by the pixel's confidence
-  if (conf) wInc = __fmul_rz(wInc, __ldg(conf + ii));
+  if (conf) wInc = __fmul_rz(wInc, cw);
 
   const float wNew = __fadd_rz(wAcc, wInc);
   const float factor = rcp_upd<RCP_HOST>(__fadd_rz(wNew, wNew <= 0.0f ? 1.0f : 0.0f), rtab, rshift);
@@ -141,9 +146,8 @@ __device__ __forceinline__ void fuse_brick(const uint32_t brick, const ushort4 *
     sdf[vi] = dNew;
     wgt[vi] = wNew;
   }
-  const uint8_t *p8 = bgr + 3 * (size_t)ii;
-  const float inc[3] = {__fmul_rz((float)__ldg(p8 + 2), COLOR_MUL), __fmul_rz((float)__ldg(p8 + 1), COLOR_MUL),
-                        __fmul_rz((float)__ldg(p8 + 0), COLOR_MUL)};
+  const float inc[3] = {__fmul_rz((float)cr, COLOR_MUL), __fmul_rz((float)cg, COLOR_MUL),
+                        __fmul_rz((float)cbl, COLOR_MUL)};
   const uint16_t accs[3] = {acc0, acc1, acc2};
 #pragma unroll
   for (int c = 0; c < 3; c++) {

@@ -86,3 +86,37 @@ def test_batch_rejects_bad_input(lib_built):
     c = _maps(1, storage="fp16")[0]
     with pytest.raises(FFError):
         add_maps_device([a, c], [1, 1], [1, 1], [160, 160], [120, 120], [cam, cam], SCALING, MAXCAM)
+
+
+def test_batch_with_learned_weight(lib_built):
+    """The learned confidence weight in a batched call equals the same weight
+    map by map (every map runs its own network on its frame)."""
+    import torch
+    from fastfusion_b200.confidence import load_weights
+    from fastfusion_b200.fusion import CameraInfo, add_maps_device
+    params, tau = load_weights()
+    K0, f0 = circle_frames(0, 6, 160, 120)
+    K1, f1 = circle_frames(1, 6, 320, 240)
+    seqs = [(K0, f0, 160, 120), (K1, f1, 320, 240)]
+    batched, alone = _maps(2), _maps(2)
+    for m in batched + alone:
+        m.set_confidence(params, tau)
+    for k in range(6):
+        dd, db, cams, keep = [], [], [], []
+        for K, frames, w, h in seqs:
+            depth, bgr, R, t = frames[k]
+            td = torch.from_numpy(depth.view(np.int16).copy()).cuda()
+            tb = torch.from_numpy(bgr.copy()).cuda()
+            keep += [td, tb]
+            dd.append(td.data_ptr())
+            db.append(tb.data_ptr())
+            cams.append(CameraInfo(K, R, t))
+        torch.cuda.synchronize()
+        qb = add_maps_device(batched, dd, db, [s[2] for s in seqs], [s[3] for s in seqs], cams, SCALING, MAXCAM)
+        for i, m in enumerate(alone):
+            assert m.addMapDevice(dd[i], db[i], seqs[i][2], seqs[i][3], cams[i], SCALING, MAXCAM) == qb[i]
+            m.sync()
+    for a, b in zip(alone, batched):
+        for x, y in zip(a.bricks(), b.bricks()):
+            assert np.array_equal(x.view(np.uint8), y.view(np.uint8))
+        assert np.array_equal(a.confidence_map(), b.confidence_map())
