@@ -14,6 +14,7 @@
 //   pred      f32  [n][H][W]      layer 3 output: predicted |depth residual| in cm
 //   params    bf16 [8833]         W1[16][5][25] b1[16] W2[16][16][25] b2[16] W3[1][16][25] b3[1]
 // Convolutions are 'same' 5x5 correlations with zero padding per image.
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -274,6 +275,40 @@ __host__ __device__ constexpr uint32_t tc_idesc() {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((128u >> 4) << 24);
 }
 
+// TMA tile loads and a bulk copy, completing on an mbarrier (transaction bytes)
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *m, int c0, int c1, int c2, int c3,
+                                            uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(m)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap *m, int c0, int c1, int c2, int c3,
+                                            int c4, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
+      "%6}], [%7];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(m)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ uint32_t mbar_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok = 0;
+  for (int it = 0; it < TC_WAIT_LIMIT && !ok; it++) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+  }
+  return ok;
+}
+
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, bool valid) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0) : "memory");
 }
@@ -313,7 +348,7 @@ __global__ void k_pack_tc(const __nv_bfloat16 *__restrict__ params, __nv_bfloat1
 }
 
 template <int C, int N, int MODE>
-__global__ void __launch_bounds__(128) k_conv_tc(const __nv_bfloat16 *__restrict__ in, int W, int H,
+__global__ void __launch_bounds__(128) k_conv_tc(const __grid_constant__ CUtensorMap tile, int W, int H,
                                                  const uint8_t *__restrict__ wpack,
                                                  const __nv_bfloat16 *__restrict__ bias, void *__restrict__ out,
                                                  float inv_tau, uint32_t *__restrict__ err) {
@@ -325,8 +360,8 @@ __global__ void __launch_bounds__(128) k_conv_tc(const __nv_bfloat16 *__restrict
   extern __shared__ __align__(1024) uint8_t tsm[];
   uint8_t *planes = tsm;                  // NP x [TC_TILE_ROWS][TC_COLS][8] bf16
   uint8_t *wsm = tsm + NP * TC_PLANE;     // NM x [k half][N][8] bf16
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(wsm + NM * BB);
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(wsm + NM * BB + 8);
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(wsm + NM * BB);  // [0], [1]: MMA stages; [2]: loads
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(wsm + NM * BB + 24);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int img = blockIdx.z;
   const int x0 = blockIdx.x * 128, y0 = blockIdx.y * TC_ROWS;
@@ -336,36 +371,38 @@ __global__ void __launch_bounds__(128) k_conv_tc(const __nv_bfloat16 *__restrict
                  "r"(TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(mbar)));
-  // input tile: 16-byte chunks (8 channels), zero outside the image
-  const size_t img_base = (size_t)img * W * H;
-  const uint32_t pbase = smem_addr(planes);
-#pragma unroll 4
-  for (int i = tid; i < TC_TILE_ROWS * TC_COLS * NP; i += 128) {
-    const int pl = i % NP, px = i / NP, col = px % TC_COLS, row = px / TC_COLS;
-    const int gx = x0 - 2 + col, gy = y0 - 2 + row;
-    const bool ok = col < 132 && gx >= 0 && gx < W && gy >= 0 && gy < H;
-    const __nv_bfloat16 *src = ok ? in + (img_base + (size_t)gy * W + gx) * C + pl * 8 : in;
-    cp_async16(pbase + (uint32_t)(pl * TC_PLANE + (row * TC_COLS + col) * 16), src, ok);
+  if (tid == 0) {
+    for (int k = 0; k < 3; k++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(mbar + k)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
-  asm volatile("cp.async.commit_group;" ::: "memory");
-  // B operands, packed in their shared-memory layout
-  const uint32_t wsm_base = smem_addr(wsm);
-#pragma unroll 4
-  for (int i = tid; i < NM * BB / 16; i += 128) cp_async16(wsm_base + (uint32_t)(i * 16), wpack + i * 16, true);
-  asm volatile("cp.async.commit_group;" ::: "memory");
-  asm volatile("cp.async.wait_all;" ::: "memory");
-  // make the shared-memory writes visible to the tensor core (async proxy)
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-
+  const size_t img_base = (size_t)img * W * H;
+  const uint32_t pbase = smem_addr(planes), wbase = smem_addr(wsm), ld_bar = smem_addr(mbar + 2);
+  // the input tile (zero outside the image) and the weight operands, by the
+  // tensor-memory-access unit: one tile copy per 8-channel plane, one bulk copy
   if (tid == 0) {
-    const uint32_t wbase = smem_addr(wsm);
+    const uint32_t bytes = (uint32_t)(NP * TC_PLANE + NM * BB);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(ld_bar), "r"(bytes) : "memory");
+    if constexpr (C == 16) {
+      tma_load_5d(pbase, &tile, 0, 0, x0 - 2, y0 - 2, img, ld_bar);
+      tma_load_5d(pbase + TC_PLANE, &tile, 0, 1, x0 - 2, y0 - 2, img, ld_bar);
+    } else {
+      tma_load_4d(pbase, &tile, 0, x0 - 2, y0 - 2, img, ld_bar);
+    }
+    bulk_load(wbase, wpack, (uint32_t)(NM * BB), ld_bar);
+  }
+  const uint32_t loaded = mbar_wait(ld_bar, 0);
+  if (!loaded && tid == 0 && err) atomicOr(err, ERR_SPIN_TIMEOUT);
+
+  // MMAs in two stages (output rows 0-3, then 4-7), one mbarrier each, so the
+  // read-back of the first overlaps the MMAs of the second
+  auto issue = [&](int r0, int r1, uint64_t *bar) {
     const uint32_t lbo = C == 16 ? (uint32_t)TC_PLANE : 16u;
-    for (int r = 0; r < TC_ROWS; r++) {
+    for (int r = r0; r < r1; r++) {
       for (int j = 0; j < NM; j++) {
         const int ky = C == 16 ? j / 5 : j / 3;
         const int kx = C == 16 ? j % 5 : 2 * (j % 3);
@@ -379,77 +416,87 @@ __global__ void __launch_bounds__(128) k_conv_tc(const __nv_bfloat16 *__restrict
       }
     }
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                     smem_addr(mbar))
+                     smem_addr(bar))
                  : "memory");
+  };
+  if (tid == 0 && loaded) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    issue(0, TC_ROWS / 2, mbar);
+    issue(TC_ROWS / 2, TC_ROWS, mbar + 1);
   }
-  uint32_t done = 0;
-  for (int it = 0; it < TC_WAIT_LIMIT && !done; it++) {
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(smem_addr(mbar)), "r"(0u)
-        : "memory");
-  }
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (!done && tid == 0 && err) atomicOr(err, ERR_SPIN_TIMEOUT);
+
+  auto wait_bar = [&](uint64_t *bar) -> uint32_t {
+    const uint32_t ok = loaded ? mbar_wait(smem_addr(bar), 0) : 0u;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!ok && tid == 0 && err) atomicOr(err, ERR_SPIN_TIMEOUT);
+    return ok;
+  };
   const int gx = x0 + 32 * warp + lane;
   const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);
-  if constexpr (MODE == CONV_RELU_BF16) {
-    float b[16];
+  // read back and store output rows [r0, r1) once their MMAs are done
+  auto epilogue = [&](int r0, int r1, uint32_t done) {
+    if constexpr (MODE == CONV_RELU_BF16) {
+      float b[16];
 #pragma unroll
-    for (int c = 0; c < 16; c++) b[c] = __bfloat162float(bias[c]);
+      for (int c = 0; c < 16; c++) b[c] = __bfloat162float(bias[c]);
 #pragma unroll 1
-    for (int r = 0; r < TC_ROWS; r++) {
-      uint32_t v[16];
+      for (int r = r0; r < r1; r++) {
+        uint32_t v[16];
+        if (done) {
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+              : "r"(trow + (uint32_t)(r * N)));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        } else {
+#pragma unroll
+          for (int c = 0; c < 16; c++) v[c] = 0x7FC00000u;  // NaN: the accumulators were not read
+        }
+        const int gy = y0 + r;
+        if (gx < W && gy < H) {
+          uint4 o[2];
+          __nv_bfloat16 *ob = reinterpret_cast<__nv_bfloat16 *>(o);
+#pragma unroll
+          for (int c = 0; c < 16; c++) ob[c] = __float2bfloat16_rn(fmaxf(__uint_as_float(v[c]) + b[c], 0.0f));
+          uint4 *dst = reinterpret_cast<uint4 *>(reinterpret_cast<__nv_bfloat16 *>(out) +
+                                                 (img_base + (size_t)gy * W + gx) * 16);
+          dst[0] = o[0];
+          dst[1] = o[1];
+        }
+      }
+    } else {
+      const float b0 = __bfloat162float(bias[0]);
+      constexpr int HALF = TC_ROWS / 2;
+      uint32_t v[HALF];
       if (done) {
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-            : "r"(trow + (uint32_t)(r * N)));
+        // column 0 (output channel 0) of each row's accumulator
+#pragma unroll
+        for (int k = 0; k < HALF; k++)
+          asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];"
+                       : "=r"(v[k])
+                       : "r"(trow + (uint32_t)((r0 + k) * N)));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       } else {
 #pragma unroll
-        for (int c = 0; c < 16; c++) v[c] = 0x7FC00000u;  // NaN: the accumulators were not read
+        for (int k = 0; k < HALF; k++) v[k] = 0x7FC00000u;
       }
-      const int gy = y0 + r;
-      if (gx < W && gy < H) {
-        uint4 o[2];
-        __nv_bfloat16 *ob = reinterpret_cast<__nv_bfloat16 *>(o);
 #pragma unroll
-        for (int c = 0; c < 16; c++) ob[c] = __float2bfloat16_rn(fmaxf(__uint_as_float(v[c]) + b[c], 0.0f));
-        uint4 *dst = reinterpret_cast<uint4 *>(reinterpret_cast<__nv_bfloat16 *>(out) +
-                                               (img_base + (size_t)gy * W + gx) * 16);
-        dst[0] = o[0];
-        dst[1] = o[1];
+      for (int k = 0; k < HALF; k++) {
+        const int gy = y0 + r0 + k;
+        if (gx >= W || gy >= H) continue;
+        const float a = __uint_as_float(v[k]) + b0;
+        float o = a;
+        if (MODE == CONV_CONF) {
+          const float c = fmaxf(1.0f - fmaxf(a, 0.0f) * inv_tau, 0.0f);
+          o = c * c;
+        }
+        reinterpret_cast<float *>(out)[img_base + (size_t)gy * W + gx] = o;
       }
     }
-  } else {
-    const float b0 = __bfloat162float(bias[0]);
-    uint32_t v[TC_ROWS];
-    if (done) {
-      // column 0 (output channel 0) of every row's accumulator
-#pragma unroll
-      for (int r = 0; r < TC_ROWS; r++)
-        asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(v[r]) : "r"(trow + (uint32_t)(r * N)));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    } else {
-#pragma unroll
-      for (int r = 0; r < TC_ROWS; r++) v[r] = 0x7FC00000u;
-    }
-#pragma unroll
-    for (int r = 0; r < TC_ROWS; r++) {
-      const int gy = y0 + r;
-      if (gx >= W || gy >= H) continue;
-      const float a = __uint_as_float(v[r]) + b0;
-      float o = a;
-      if (MODE == CONV_CONF) {
-        const float c = fmaxf(1.0f - fmaxf(a, 0.0f) * inv_tau, 0.0f);
-        o = c * c;
-      }
-      reinterpret_cast<float *>(out)[img_base + (size_t)gy * W + gx] = o;
-    }
-  }
+  };
+  epilogue(0, TC_ROWS / 2, wait_bar(mbar));
+  epilogue(TC_ROWS / 2, TC_ROWS, wait_bar(mbar + 1));
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
@@ -765,6 +812,54 @@ cudaError_t ensure_attrs() {
   return cudaSuccess;
 }
 
+// Tensor-map encoder of the driver, looked up once (the library does not
+// link the driver library itself).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+// The tile of a k_conv_tc block over n images of W x H pixels, C = 8 or 16
+// BF16 channels per pixel: a (TC_ROWS + 4) x TC_COLS box of one 8-channel
+// plane, zero outside the image (dimensions: 8 channels, [plane], x, y, image).
+cudaError_t tile_map(CUtensorMap *m, const void *base, int C, int W, int H, int n) {
+  const EncodeTiledFn f = encode_tiled();
+  if (!f) return cudaErrorNotSupported;
+  cuuint64_t dims[5], strides[4];
+  cuuint32_t box[5], es[5] = {1, 1, 1, 1, 1};
+  cuuint32_t rank;
+  if (C == 16) {
+    rank = 5;
+    const cuuint64_t d[5] = {8, 2, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)n};
+    const cuuint64_t st[4] = {16, 32, (cuuint64_t)W * 32, (cuuint64_t)W * H * 32};
+    const cuuint32_t b[5] = {8, 1, TC_COLS, TC_TILE_ROWS, 1};
+    for (int i = 0; i < 5; i++) dims[i] = d[i], box[i] = b[i];
+    for (int i = 0; i < 4; i++) strides[i] = st[i];
+  } else {
+    rank = 4;
+    const cuuint64_t d[4] = {8, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)n};
+    const cuuint64_t st[3] = {16, (cuuint64_t)W * 16, (cuuint64_t)W * H * 16};
+    const cuuint32_t b[4] = {8, TC_COLS, TC_TILE_ROWS, 1};
+    for (int i = 0; i < 4; i++) dims[i] = d[i], box[i] = b[i];
+    for (int i = 0; i < 3; i++) strides[i] = st[i];
+  }
+  const CUresult r = f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, rank, const_cast<void *>(base), dims, strides, box, es,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 dim3 conv_grid(int W, int H, int n) {
   return dim3((W + TX - 1) / TX, (H + conv_ty(CONV_RPT) - 1) / conv_ty(CONV_RPT), n);
 }
@@ -802,18 +897,23 @@ cudaError_t cnn_forward(const __nv_bfloat16 *params, uint8_t *packed, bool packe
     note_launch();
     k_pack_tc<<<(TC_PACK_BYTES / 2 + 255) / 256, 256, 0, s>>>(params, reinterpret_cast<__nv_bfloat16 *>(packed));
   }
+  CUtensorMap m_feat, m_a1, m_a2;
+  if ((e = tile_map(&m_feat, feat, CNN_IN_STRIDE, W, H, n)) != cudaSuccess ||
+      (e = tile_map(&m_a1, a1, CNN_HID, W, H, n)) != cudaSuccess ||
+      (e = tile_map(&m_a2, a2, CNN_HID, W, H, n)) != cudaSuccess)
+    return e;
   const dim3 tg((W + 127) / 128, (H + TC_ROWS - 1) / TC_ROWS, n);
   note_launch(3);
   k_conv_tc<CNN_IN_STRIDE, 16, CONV_RELU_BF16><<<tg, 128, tc_smem_bytes<CNN_IN_STRIDE, 16>(), s>>>(
-      feat, W, H, packed + TC_PACK_L1, params + P_B1, a1, 0.0f, err);
+      m_feat, W, H, packed + TC_PACK_L1, params + P_B1, a1, 0.0f, err);
   k_conv_tc<CNN_HID, 16, CONV_RELU_BF16><<<tg, 128, tc_smem_bytes<CNN_HID, 16>(), s>>>(
-      a1, W, H, packed + TC_PACK_L2, params + P_B2, a2, 0.0f, err);
+      m_a1, W, H, packed + TC_PACK_L2, params + P_B2, a2, 0.0f, err);
   if (tau_cm > 0.0f)
     k_conv_tc<CNN_HID, 16, CONV_CONF><<<tg, 128, tc_smem_bytes<CNN_HID, 16>(), s>>>(
-        a2, W, H, packed + TC_PACK_L3, params + P_B3, out, 1.0f / tau_cm, err);
+        m_a2, W, H, packed + TC_PACK_L3, params + P_B3, out, 1.0f / tau_cm, err);
   else
     k_conv_tc<CNN_HID, 16, CONV_F32><<<tg, 128, tc_smem_bytes<CNN_HID, 16>(), s>>>(
-        a2, W, H, packed + TC_PACK_L3, params + P_B3, out, 0.0f, err);
+        m_a2, W, H, packed + TC_PACK_L3, params + P_B3, out, 0.0f, err);
   return cudaGetLastError();
 }
 
