@@ -372,7 +372,10 @@ __global__ void __launch_bounds__(128) k_conv_tc(const __grid_constant__ CUtenso
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    for (int k = 0; k < 3; k++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(mbar + k)));
+    // stage barriers: one arrival per issuing warp (two warps per stage)
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;" ::"r"(smem_addr(mbar)));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;" ::"r"(smem_addr(mbar + 1)));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(mbar + 2)));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
@@ -399,7 +402,8 @@ __global__ void __launch_bounds__(128) k_conv_tc(const __grid_constant__ CUtenso
   if (!loaded && tid == 0 && err) atomicOr(err, ERR_SPIN_TIMEOUT);
 
   // MMAs in two stages (output rows 0-3, then 4-7), one mbarrier each, so the
-  // read-back of the first overlaps the MMAs of the second
+  // read-back of the first overlaps the MMAs of the second; each warp's
+  // first lane issues the MMAs of two rows (four issuers share the tensor core)
   auto issue = [&](int r0, int r1, uint64_t *bar) {
     const uint32_t lbo = C == 16 ? (uint32_t)TC_PLANE : 16u;
     for (int r = r0; r < r1; r++) {
@@ -419,10 +423,10 @@ __global__ void __launch_bounds__(128) k_conv_tc(const __grid_constant__ CUtenso
                      smem_addr(bar))
                  : "memory");
   };
-  if (tid == 0 && loaded) {
+  static_assert(TC_ROWS == 8, "two rows per warp, two warps per stage");
+  if (lane == 0 && loaded) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    issue(0, TC_ROWS / 2, mbar);
-    issue(TC_ROWS / 2, TC_ROWS, mbar + 1);
+    issue(2 * warp, 2 * warp + 2, mbar + (warp >> 1));
   }
 
   auto wait_bar = [&](uint64_t *bar) -> uint32_t {
