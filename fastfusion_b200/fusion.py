@@ -207,6 +207,34 @@ class MeshInterleaved:
                 out.write("".join(lines).encode())
         return True
 
+    def writeOBJ(self, filename: str) -> bool:
+        """Write `filename` + ".obj" byte for byte as the reference's
+        MeshInterleaved::writeOBJ (mesh_interleaved.cpp:19-134) writes a mesh
+        without normals or textures (the marching-cubes mesh has neither): a
+        comment line, one `v x y z r g b` line per vertex with the colour as
+        float32 channel / 255, then one `f` line per triangle with 1-based
+        vertex indices; numbers as C++ streams print them (%g, 6 significant
+        digits).  No material file is written without textures."""
+        v = np.ascontiguousarray(self.vertices, np.float32).reshape(-1, 3)
+        c = np.ascontiguousarray(self.colors, np.uint8).reshape(-1, 3)
+        f = np.ascontiguousarray(self.faces, np.uint32).reshape(-1, 3)
+        try:
+            out = open(filename + ".obj", "wb")
+        except OSError:
+            return False
+        lines = ["\n#Written from Volume"]
+        cf = (c.astype(np.float32) / np.float32(255.0)) if len(c) else None
+        for k in range(len(v)):
+            s = "\nv %g %g %g" % (float(v[k, 0]), float(v[k, 1]), float(v[k, 2]))
+            if cf is not None:
+                s += " %g %g %g" % (float(cf[k, 0]), float(cf[k, 1]), float(cf[k, 2]))
+            lines.append(s)
+        f1 = f.astype(np.int64) + 1
+        lines.extend("\nf %d %d %d" % (a, b, d) for a, b, d in f1.tolist())
+        with out:
+            out.write("".join(lines).encode())
+        return True
+
 
 class MeshBuffer:
     """Reusable page-locked host storage for getMeshInterleavedMarchingCubes(out=...).

@@ -45,6 +45,8 @@ def lib():
         L.ref_mesh_copy.argtypes = [vp, vp, vp, vp]
         L.ref_write_ply.restype = i32
         L.ref_write_ply.argtypes = [vp, ctypes.c_char_p, i32]
+        L.ref_write_obj.restype = i32
+        L.ref_write_obj.argtypes = [vp, ctypes.c_char_p]
         L.ref_state.argtypes = [vp, vp, vp]
         L.ref_leaves.argtypes = [vp, ll, vp, vp, vp]
         L.ref_queue.argtypes = [vp, vp]
@@ -111,6 +113,10 @@ class RefFusion:
     def write_ply(self, stem: str, binary: bool = True) -> bool:
         """The reference's MeshInterleaved::writePLY of its current mesh (writes stem + ".ply")."""
         return bool(self.L.ref_write_ply(self.h, stem.encode(), 1 if binary else 0))
+
+    def write_obj(self, stem: str) -> bool:
+        """The reference's MeshInterleaved::writeOBJ of its current mesh (writes stem + ".obj")."""
+        return bool(self.L.ref_write_obj(self.h, stem.encode()))
 
     def state(self) -> dict:
         ints = np.zeros(16, np.int64)

@@ -111,6 +111,13 @@ int ref_write_ply(void *h, const char *stem, int binary) {
   return f->_meshCurrent->writePLY(std::string(stem), binary != 0) ? 1 : 0;
 }
 
+/* The reference's own OBJ writer (MeshInterleaved::writeOBJ); `stem` gets
+ * ".obj" appended by the writer. */
+int ref_write_obj(void *h, const char *stem) {
+  FusionMipMapCPU *f = (FusionMipMapCPU *)h;
+  return f->_meshCurrent->writeOBJ(std::string(stem)) ? 1 : 0;
+}
+
 void ref_mesh_copy(void *h, float *xyz, uint8_t *rgb, uint32_t *faces) {
   FusionMipMapCPU *f = (FusionMipMapCPU *)h;
   const MeshInterleaved &m = *f->_meshCurrent;

@@ -1,4 +1,4 @@
-"""PLY export: MeshInterleaved.writePLY must write the same bytes as the
+"""PLY and OBJ export: MeshInterleaved.writePLY must write the same bytes as the
 reference's MeshInterleaved::writePLY (mesh_interleaved.cpp:137-198), binary
 and ascii, for the same mesh (the compiled reference's own mesh here)."""
 
@@ -50,3 +50,26 @@ def test_ply_empty_mesh(tmp_path):
     want = (b"ply\nformat binary_little_endian 1.0\nelement vertex 0\n"
             b"property float32 x\nproperty float32 y\nproperty float32 z\nend_header\n")
     assert open(tmp_path / "empty.ply", "rb").read() == want
+
+
+def test_obj_bytes_equal_reference(tmp_path, ref_lib):
+    """OBJ export: MeshInterleaved.writeOBJ writes the same bytes as the
+    reference's MeshInterleaved::writeOBJ (mesh_interleaved.cpp:19-134)."""
+    from fastfusion_b200.fusion import MeshInterleaved
+    r = _ref_mesh(ref_lib, 4)
+    xyz, rgb, faces = r.mesh()
+    assert len(faces) > 0
+    assert r.write_obj(str(tmp_path / "ref"))
+    assert MeshInterleaved(xyz, rgb, faces).writeOBJ(str(tmp_path / "ours"))
+    a = open(tmp_path / "ref.obj", "rb").read()
+    b = open(tmp_path / "ours.obj", "rb").read()
+    assert a == b
+    assert not (tmp_path / "ours.mtl").exists()
+    r.close()
+
+
+def test_obj_empty_mesh(tmp_path):
+    from fastfusion_b200.fusion import MeshInterleaved
+    m = MeshInterleaved(np.zeros((0, 3), np.float32), np.zeros((0, 3), np.uint8), np.zeros((0, 3), np.uint32))
+    assert m.writeOBJ(str(tmp_path / "empty"))
+    assert open(tmp_path / "empty.obj", "rb").read() == b"\n#Written from Volume"
