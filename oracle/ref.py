@@ -39,6 +39,8 @@ def lib():
         L.ref_set_incremental_meshing.argtypes = [vp, i32]
         L.ref_add_map.restype = i32
         L.ref_add_map.argtypes = [vp, vp, vp, i32, i32, vp, vp, vp, ctypes.c_float, ctypes.c_float]
+        L.ref_add_map_f32.restype = i32
+        L.ref_add_map_f32.argtypes = [vp, vp, vp, vp, vp, i32, i32, vp, vp, vp]
         L.ref_update_meshes.restype = i32
         L.ref_update_meshes.argtypes = [vp]
         L.ref_mesh_counts.argtypes = [vp, ctypes.POINTER(ll), ctypes.POINTER(ll)]
@@ -117,6 +119,19 @@ class RefFusion:
     def write_obj(self, stem: str) -> bool:
         """The reference's MeshInterleaved::writeOBJ of its current mesh (writes stem + ".obj")."""
         return bool(self.L.ref_write_obj(self.h, stem.encode()))
+
+    def add_map_f32(self, depth, bgr, K, R, t) -> int:
+        """The reference's float-depth addMap: depth in metres (non-finite: hole),
+        colour passed as its three planes (split here from a BGR image)."""
+        depth = np.ascontiguousarray(depth, dtype=np.float32)
+        bgr = np.ascontiguousarray(bgr, dtype=np.uint8)
+        planes = [np.ascontiguousarray(bgr[..., c]) for c in range(3)]
+        K = np.ascontiguousarray(K, dtype=np.float64)
+        R = np.ascontiguousarray(R, dtype=np.float64)
+        t = np.ascontiguousarray(t, dtype=np.float64)
+        h, w = depth.shape
+        return self.L.ref_add_map_f32(self.h, _p(depth), _p(planes[0]), _p(planes[1]), _p(planes[2]), w, h,
+                                      _p(K), _p(R), _p(t))
 
     def state(self) -> dict:
         ints = np.zeros(16, np.int64)

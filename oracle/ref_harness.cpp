@@ -95,6 +95,34 @@ int ref_add_map(void *h, const uint16_t *depth, const uint8_t *bgr, int w, int h
   return f->addMap(d, cam, c, scaling, maxcam);
 }
 
+/* The reference's float-depth overload, addMap(cv::Mat &, CameraInfo,
+ * std::vector<cv::Mat>) (geometryfusion_mipmap_cpu.cpp:1308-1600): depth in
+ * metres (any non-finite value is a hole), colour as three planes in the
+ * order blue, green, red (cv::split of a BGR image). */
+int ref_add_map_f32(void *h, const float *depth, const uint8_t *blue, const uint8_t *green, const uint8_t *red,
+                    int w, int hgt, const double *K4, const double *R9, const double *t3) {
+  FusionMipMapCPU *f = (FusionMipMapCPU *)h;
+  cv::Mat d(hgt, w, CV_32FC1, (void *)depth);
+  std::vector<cv::Mat> planes;
+  planes.push_back(cv::Mat(hgt, w, CV_8UC1, (void *)blue));
+  planes.push_back(cv::Mat(hgt, w, CV_8UC1, (void *)green));
+  planes.push_back(cv::Mat(hgt, w, CV_8UC1, (void *)red));
+  CameraInfo cam;
+  cv::Mat K = cv::Mat::eye(3, 3, CV_64FC1);
+  K.at<double>(0, 0) = K4[0];
+  K.at<double>(1, 1) = K4[1];
+  K.at<double>(0, 2) = K4[2];
+  K.at<double>(1, 2) = K4[3];
+  cam.setIntrinsic(K);
+  cv::Mat E = cv::Mat::eye(4, 4, CV_64FC1);
+  for (int r = 0; r < 3; r++) {
+    for (int k = 0; k < 3; k++) E.at<double>(r, k) = R9[r * 3 + k];
+    E.at<double>(r, 3) = t3[r];
+  }
+  cam.setExtrinsic(E);
+  return f->addMap(d, cam, planes);
+}
+
 int ref_update_meshes(void *h) { return ((FusionMipMapCPU *)h)->updateMeshes() ? 1 : 0; }
 
 /* Mesh of the last finished update: counts, then copies. */

@@ -84,3 +84,30 @@ def test_meshing_cells_match_reference_live(port_lib):
                    and np.array_equal(rc, rgb[v0:v0 + nv]) and np.array_equal(rf, faces[f0:f0 + nf] - v0))
     assert n_common == len(refmap) == len(cells)
     assert n_same == n_common
+
+
+def test_reference_float_overload_behaviour():
+    """What the reference's float-depth addMap (geometryfusion_mipmap_cpu.cpp:1308-1600)
+    does, run live with incremental meshing off (with it on, the default, its
+    legacy mesh-cell bookkeeping in transformLoopSimPrecalculatedNeg_vis
+    crashes the process, so that case is not run): the same octree as the
+    16-bit overload for the same depths, but every brick updated twice per
+    frame (update8NaiveFloat, then update8AddLoopSSESingleFloat,
+    update_functions.cpp:1600-1623), so weights grow twice as fast, and no
+    mesh from updateMeshes.  The library therefore offers no float-depth
+    overload."""
+    K, frames = circle_frames(0, 3, 160, 120)
+    a, b = ref.RefFusion(), ref.RefFusion()
+    b.L.ref_set_incremental_meshing(b.h, 0)
+    for depth, bgr, R, t in frames:
+        z = depth.astype(np.float32) * np.float32(SCALING)
+        zf = np.where((z > 0) & (z < MAXCAM), z, np.nan).astype(np.float32)
+        assert a.add_map(depth, bgr, K, R, t, SCALING, MAXCAM) == b.add_map_f32(zf, bgr, K, R, t)
+    assert np.array_equal(a.tree(), b.tree())
+    (_, wa, _), (_, wb, _) = a.bricks(), b.bricks()
+    assert wa.max() <= 3.01 and wb.max() == 6.0
+    assert 1.9 < wb.sum() / wa.sum() < 2.0
+    b.update_meshes()
+    assert len(b.mesh()[2]) == 0
+    a.close()
+    b.close()
