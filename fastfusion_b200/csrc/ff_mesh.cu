@@ -901,7 +901,7 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
                                                                   const uint32_t *__restrict__ list, const uint32_t *list_n, CellOut *out,
                                                                   const uint64_t *vbase, const uint64_t *fbase,
                                                                   float *xyz, uint8_t *rgb, uint32_t *faces,
-                                                                  uint32_t *work) {
+                                                                  uint32_t *work, uint8_t *__restrict__ cases) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ McTab T;
   load_mc(T);
@@ -916,6 +916,8 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t ci = EMIT ? next_cell(work, lane) : gw; ci < n; ci = EMIT ? next_cell(work, lane) : ci + nw) {
     const uint32_t cid = list ? list[ci] : first + ci;
+    // emit: a cell that the count pass found without vertices writes nothing
+    if (EMIT && out[cid].nv == 0) continue;
     const Cell c = cells[cid];
     const CellGeom G = cell_geom(m, c);
     if (G.empty) {
@@ -924,48 +926,98 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
     }
     const int n3[3] = {G.cnt[0], G.cnt[1], G.cnt[2]};
     const int nsamp = n3[0] * n3[1] * n3[2];
-    bool fit = true;
-    for (int k = lane; k < nsamp; k += 32) {
-      const int bx = k % n3[0], by = (k / n3[0]) % n3[1], bz = k / (n3[0] * n3[1]);
-      Sample s;
-      fit &= lattice_sample(m, c, G, bx, by, bz, s);
-      const int si = (bz * 8 + by) * 8 + bx;
-      W.sd[si] = s.d;
-      W.sc[3 * si] = s.c[0];
-      W.sc[3 * si + 1] = s.c[1];
-      W.sc[3 * si + 2] = s.c[2];
-      W.wzero[si] = s.w == 0.0f;
-    }
-    for (int k = lane; k < 384; k += 32) reinterpret_cast<uint32_t *>(W.edge_set)[k] = 0;
-    fit = __all_sync(0xffffffffu, fit);
-    __syncwarp();
-    if (!EMIT && lane == 0) atomicAdd(m.samples, (unsigned long long)nsamp);
-    if (!fit) {
-      if (!EMIT && lane == 0) out[cid] = CellOut{0u, 0u};
-      continue;
-    }
     const int nc3[3] = {n3[0] - 1, n3[1] - 1, n3[2] - 1};
     const int ncube = nc3[0] * nc3[1] * nc3[2];
-    for (int k = lane; k < ncube; k += 32) {
-      const int bx = k % nc3[0], by = (k / nc3[0]) % nc3[1], bz = k / (nc3[0] * nc3[1]);
-      const int idx = (bz * 8 + by) * 8 + bx;
-      const int off[8] = {0, 1, 9, 8, 64, 65, 73, 72};
-      bool zero = false;
-      int ci8 = 0;
+    // the count pass's marching-cubes case of every cube of this cell
+    uint4 *const cell_cases = reinterpret_cast<uint4 *>(cases + (size_t)ci * 512);
+    if (EMIT) {
+      // Only the samples at the ends of lattice edges that carry a vertex
+      // are read: the edge slots follow from the stored cube cases, and the
+      // samples are the same function of the volume as in the count pass
+      // (which found every sample of this cell inside its leaves).
+      reinterpret_cast<uint4 *>(W.cube_case)[lane] = cell_cases[lane];
+      for (int k = lane; k < 384; k += 32) reinterpret_cast<uint32_t *>(W.edge_set)[k] = 0;
+      for (int k = lane; k < 128; k += 32) reinterpret_cast<uint32_t *>(W.wzero)[k] = 0;  // "needed" flags
+      __syncwarp();
+      for (int k = lane; k < ncube; k += 32) {
+        const int bx = k % nc3[0], by = (k / nc3[0]) % nc3[1], bz = k / (nc3[0] * nc3[1]);
+        const int idx = (bz * 8 + by) * 8 + bx;
+        const int ci8 = W.cube_case[idx];
+        const int nt = mc_ntri(T, ci8);
+        for (int q = 0; q < 3 * nt; q++) {
+          const int slot = 3 * idx + mc_slot(T, mc_edge(T, ci8, q));
+          const int si = slot / 3, a = slot - 3 * si;
+          W.edge_set[slot] = 1;
+          W.wzero[si] = 1;
+          W.wzero[si + (a == 0 ? 1 : (a == 1 ? 8 : 64))] = 1;
+        }
+      }
+      __syncwarp();
+      // compact list of the needed sample indices (in vidx, free until the
+      // vertex loop below)
+      uint16_t *need = W.vidx;
+      int nneed = 0;
+      for (int k0 = 0; k0 < 512; k0 += 32) {
+        const bool nd = W.wzero[k0 + lane] != 0;
+        const unsigned b = __ballot_sync(0xffffffffu, nd);
+        if (nd) need[nneed + __popc(b & ((1u << lane) - 1u))] = (uint16_t)(k0 + lane);
+        nneed += __popc(b);
+      }
+      __syncwarp();
+      for (int k = lane; k < nneed; k += 32) {
+        const int si = need[k];
+        Sample s;
+        lattice_sample(m, c, G, si & 7, (si >> 3) & 7, si >> 6, s);
+        W.sd[si] = s.d;
+        W.sc[3 * si] = s.c[0];
+        W.sc[3 * si + 1] = s.c[1];
+        W.sc[3 * si + 2] = s.c[2];
+      }
+      __syncwarp();
+    } else {
+      bool fit = true;
+      for (int k = lane; k < nsamp; k += 32) {
+        const int bx = k % n3[0], by = (k / n3[0]) % n3[1], bz = k / (n3[0] * n3[1]);
+        Sample s;
+        fit &= lattice_sample(m, c, G, bx, by, bz, s);
+        const int si = (bz * 8 + by) * 8 + bx;
+        W.sd[si] = s.d;
+        W.sc[3 * si] = s.c[0];
+        W.sc[3 * si + 1] = s.c[1];
+        W.sc[3 * si + 2] = s.c[2];
+        W.wzero[si] = s.w == 0.0f;
+      }
+      for (int k = lane; k < 384; k += 32) reinterpret_cast<uint32_t *>(W.edge_set)[k] = 0;
+      fit = __all_sync(0xffffffffu, fit);
+      __syncwarp();
+      if (lane == 0) atomicAdd(m.samples, (unsigned long long)nsamp);
+      if (!fit) {
+        if (lane == 0) out[cid] = CellOut{0u, 0u};
+        continue;
+      }
+      for (int k = lane; k < ncube; k += 32) {
+        const int bx = k % nc3[0], by = (k / nc3[0]) % nc3[1], bz = k / (nc3[0] * nc3[1]);
+        const int idx = (bz * 8 + by) * 8 + bx;
+        const int off[8] = {0, 1, 9, 8, 64, 65, 73, 72};
+        bool zero = false;
+        int ci8 = 0;
 #pragma unroll
-      for (int q = 0; q < 8; q++) {
-        zero |= W.wzero[idx + off[q]] != 0;
-        if (W.sd[idx + off[q]] < 0.0f) ci8 |= 1 << q;
+        for (int q = 0; q < 8; q++) {
+          zero |= W.wzero[idx + off[q]] != 0;
+          if (W.sd[idx + off[q]] < 0.0f) ci8 |= 1 << q;
+        }
+        if (zero) ci8 = 0;
+        W.cube_case[idx] = (uint8_t)ci8;
+        const int nt = mc_ntri(T, ci8);
+        for (int q = 0; q < 3 * nt; q++) {
+          const int slot = 3 * idx + mc_slot(T, mc_edge(T, ci8, q));
+          W.edge_set[slot] = 1;  // lanes that set the same slot store the same byte
+        }
       }
-      if (zero) ci8 = 0;
-      W.cube_case[idx] = (uint8_t)ci8;
-      const int nt = mc_ntri(T, ci8);
-      for (int q = 0; q < 3 * nt; q++) {
-        const int slot = 3 * idx + mc_slot(T, mc_edge(T, ci8, q));
-        W.edge_set[slot] = 1;  // lanes that set the same slot store the same byte
-      }
+      __syncwarp();
+      // kept for the emit pass (entries of cubes outside the lattice unused)
+      cell_cases[lane] = reinterpret_cast<const uint4 *>(W.cube_case)[lane];
     }
-    __syncwarp();
     // vertices, in the reference's loop order of this cell type
     uint32_t vrun = 0;
     const uint64_t vb = EMIT ? vbase[cid] : 0;
@@ -1310,6 +1362,8 @@ struct MeshImpl {
   size_t cap_oi = 0;
   uint32_t *dlist = nullptr;  // dirty cell ids: lattice cells, then (from first_corner) corner cells
   size_t cap_dlist = 0;
+  uint8_t *cases = nullptr;  // count pass -> emit pass: 512 cube cases per dirty lattice cell
+  size_t cap_cases = 0;
   void *scan_tmp = nullptr;
   size_t scan_tmp_bytes = 0;
   // previous mesh (the current output moves here before the next update)
@@ -1533,6 +1587,7 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
     MCK(cudaFuncSetAttribute(k_mesh_lattice<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_emit));
     attr_devices.fetch_or(dbit);
   }
+  MCK(grow_buf(I.cases, I.cap_cases, (size_t)first_corner * 512, s));
   const uint32_t *lat_list = incremental ? I.dlist : nullptr;
   const uint32_t *cor_list = incremental ? I.dlist + first_corner : nullptr;
   pi = P.begin(ST_MESH_COUNT, s);
@@ -1541,7 +1596,7 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   if (first_corner)
     k_mesh_lattice<false><<<lat_blocks, 32 * MESH_WARPS, smem_count, s>>>(vs, I.cells, 0, first_corner, lat_list,
                                                                     I.d_count + 14, I.out, nullptr, nullptr, nullptr,
-                                                                    nullptr, nullptr, I.d_count + 16);
+                                                                    nullptr, nullptr, I.d_count + 16, I.cases);
   if (ncells > first_corner)
     k_mesh_corner<false><<<(ncells - first_corner + 127) / 128, 128, 0, s>>>(
         vs, I.cells, first_corner, ncells - first_corner, cor_list, I.d_count + 15, I.out, nullptr, nullptr, nullptr,
@@ -1599,7 +1654,7 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   if (first_corner)
     k_mesh_lattice<true><<<lat_blocks, 32 * MESH_WARPS, smem_emit, s>>>(vs, I.cells, 0, first_corner, lat_list,
                                                                    I.d_count + 14, I.out, I.vbase, I.fbase, M.d_xyz,
-                                                                   M.d_rgb, M.d_faces, I.d_count + 17);
+                                                                   M.d_rgb, M.d_faces, I.d_count + 17, I.cases);
   if (ncells > first_corner)
     k_mesh_corner<true><<<(ncells - first_corner + 127) / 128, 128, 0, s>>>(
         vs, I.cells, first_corner, ncells - first_corner, cor_list, I.d_count + 15, I.out, I.vbase, I.fbase, M.d_xyz,
@@ -1753,7 +1808,7 @@ void mesh_free(MeshState &M) {
                     I.vertq[1], I.d_count, I.raw, I.cells, I.old_cells, I.keys, I.keys_sorted, I.old_keys,
                     I.vals, I.vals_sorted, I.sort_tmp, I.out, I.old_out, I.nv, I.nf, I.vbase, I.fbase,
                     I.old_vbase, I.old_fbase, I.dirty, I.old_index, I.scan_tmp, I.old_xyz, I.old_rgb,
-                    I.old_faces, I.dlist};
+                    I.old_faces, I.dlist, I.cases};
     for (void *p : ptrs)
       if (p) cudaFreeAsync(p, 0);
     if (I.h_count) cudaFreeHost(I.h_count);
