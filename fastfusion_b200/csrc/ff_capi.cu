@@ -586,6 +586,9 @@ struct FramePlan {
   float scaling, maxcam;
   uint32_t frame, leaves_before;
   bool one_sync;
+  // the counters reach the host before the leaf finalisation: their queued
+  // count does not yet hold the frame's new leaves
+  bool counters_early = false;
 };
 
 static uint32_t pad32(uint32_t v) { return (v + 31u) & ~31u; }
@@ -813,20 +816,22 @@ static ff_status frame_launch(ff_handle *lead, int n) {
   return st != FF_OK ? st : frame_issue(lead, n, lp);
 }
 
-// counters: a single map's counters are copied to the host between the
-// finalisation and the update, and this event recorded after the copy.
+// counters: a single map's counters are copied to the host before the
+// finalisation (which only places the new leaves and queues them: the host
+// adds their number itself), and this event recorded after the copy, so the
+// finalisation and the update overlap the host's return and its next frame.
 static ff_status frame_launch_update(ff_handle *lead, int n, uint32_t max_npix, int &pi_fin, int &pi_fuse,
                                      cudaEvent_t counters = nullptr, bool side = false) {
   ff_handle *h = lead;  // (error reporting)
   cudaStream_t s = lead->stream;
-  pi_fin = lead->prof.begin(ST_FINALIZE, s);
-  if (!launch_finalize_small(lead->d_batch, n, max_npix, lead->cfg.device, s))
-    return set_err(lead, FF_ERR_CUDA, "leaf finalisation could not be launched");
-  lead->prof.end(pi_fin, 0.0, s);
   if (counters) {
     CK(cudaMemcpyAsync(lead->h_cnt, lead->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
     CK(cudaEventRecord(counters, s));
   }
+  pi_fin = lead->prof.begin(ST_FINALIZE, s);
+  if (!launch_finalize_small(lead->d_batch, n, max_npix, lead->cfg.device, s))
+    return set_err(lead, FF_ERR_CUDA, "leaf finalisation could not be launched");
+  lead->prof.end(pi_fin, 0.0, s);
   // side: the update runs on fuse_stream once this frame's leaves are final
   cudaStream_t fs = s;
   if (side) {
@@ -867,8 +872,8 @@ static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf,
   const uint32_t npend = hc.pending;
   uint32_t new_queued = 0;
   if (leaves_before < h->cfg.leaves_max) new_queued = std::min(npend, h->cfg.leaves_max - leaves_before);
-  // with one synchronisation the counters already include the new leaves
-  const uint32_t nq = plan.one_sync ? hc.queued : hc.queued + new_queued;
+  // counters read after the finalisation already include the new leaves
+  const uint32_t nq = plan.one_sync && !plan.counters_early ? hc.queued : hc.queued + new_queued;
   if (!plan.one_sync && npend) {
     pi_fin = h->prof.begin(ST_FINALIZE, s);
     uint32_t *k_in = h->d_keys, *v_in = h->d_keys + h->cap_pix, *k_out = h->d_keys + 2 * h->cap_pix,
@@ -946,6 +951,7 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
     // the frame returns once its counters are on the host; its voxel update
     // (gated on the device) keeps running, ordered before anything that
     // follows on the stream
+    plan.counters_early = true;
     st = frame_launch_update(h, 1, (uint32_t)(W * H), pi_fin, pi_fuse, h->ev_counters, true);
     if (st != FF_OK) return st;
     CK(cudaEventSynchronize(h->ev_counters));
