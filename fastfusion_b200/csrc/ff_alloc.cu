@@ -171,6 +171,18 @@ __global__ void __launch_bounds__(32 * DD_WARPS) k_dedupe(const BatchDesc *__res
   uint32_t *pB = pR + 2 * (size_t)ntiles;
   const int tx = active ? tile % tilesX : 0, ty = active ? tile / tilesX : 0;
   const int x = tx * 32 + lane;
+  // each map's counters for this frame (read from the first barrier on)
+  if (blockIdx.x == 0 && (int)threadIdx.x < m1 - m0) {
+    const MapFrame &G = bd->f[m0 + threadIdx.x];
+    Counters *c = G.cnt;
+    uint32_t *w = reinterpret_cast<uint32_t *>(c);
+    for (int k = 0; k < (int)(sizeof(Counters) / 4); k++) w[k] = 0;
+    c->branches_used = G.branches_init;
+    for (int r = 0; r < 3; r++) {
+      c->box_min[r] = 0;
+      c->box_max[r] = (int)G.n - 1;
+    }
+  }
   const int rows = active ? min(DD_ROWS, H - ty * DD_ROWS) : 0;
   // project the tile (voxel keys for the insert that follows) and make the
   // key comparisons; the tile's depth and row factors are fetched first so
@@ -275,6 +287,12 @@ __global__ void __launch_bounds__(32 * DD_WARPS) k_dedupe(const BatchDesc *__res
     }
     if (*(volatile uint32_t *)&bd->f[m0].cnt->error & ERR_SPIN_TIMEOUT) break;
   }
+  // leave the barrier words as the next launch needs them: the arrival count
+  // is zero after every completed barrier, counter (round + 1) % 3 was zeroed
+  // in this round and counter round % 3 read as zero, and counter
+  // (round + 2) % 3 was last read before this round's barrier (after a
+  // barrier that gave up or no convergence, the host clears the words)
+  if (converged && blockIdx.x == 0 && threadIdx.x == 0) chg[(round + 2) % 3] = 0;
   if (active && x < W) {
     for (int r = 0; r < rows; r++) processed[(size_t)(ty * DD_ROWS + r) * W + x] = (uint8_t)((bits >> r) & 1u);
   }

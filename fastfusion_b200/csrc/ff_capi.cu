@@ -74,6 +74,9 @@ struct ff_handle {
   Counters *d_cnt = nullptr;
   Counters *h_cnt = nullptr;  // pinned
   uint32_t *d_barrier = nullptr;
+  // the de-duplication barrier words need clearing before the next launch
+  // (fresh memory, or a launch that ended without convergence)
+  bool barrier_dirty = true;
   uint32_t *d_rcp_tab = nullptr;  // FF_RCP_HOST: the host CPU's RCPPS per mantissa >> rcp_shift
   int rcp_shift = 0;
 
@@ -639,13 +642,6 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
   plan.frame = h->frames + 1;
   plan.leaves_before = h->leaves_used;
   plan.one_sync = finalize_small_fits((uint32_t)(W * H));
-  memset(&hc, 0, sizeof(Counters));
-  hc.branches_used = h->branches_used;
-  for (int r = 0; r < 3; r++) {
-    hc.box_min[r] = 0;
-    hc.box_max[r] = (int)h->n - 1;
-  }
-  CK(cudaMemcpyAsync(h->d_cnt, &hc, sizeof(Counters), cudaMemcpyHostToDevice, s));
   memset(&mf, 0, sizeof(MapFrame));
   mf.depth = d_depth;
   mf.bgr = d_bgr;
@@ -687,6 +683,7 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
   mf.proc = h->d_proc;
   mf.bnd = h->d_bnd;
   mf.cnt = h->d_cnt;
+  mf.branches_init = h->branches_used;  // (the counters are set up on the device)
   mf.rcp_tab = h->d_rcp_tab;
   mf.rcp_shift = h->rcp_shift;
   mf.conf = nullptr;
@@ -797,7 +794,13 @@ static ff_status frame_issue(ff_handle *lead, int n, const LaunchPlan &lp) {
   ff_handle *h = lead;  // (error reporting)
   cudaStream_t s = lead->stream;
   CK(cudaMemcpyAsync(lead->d_batch, lead->h_batch, batch_desc_bytes(n), cudaMemcpyHostToDevice, s));
-  CK(cudaMemsetAsync(lead->d_barrier, 0, BARRIER_WORDS * sizeof(uint32_t), s));
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(s, &cap));
+  // (a recorded graph always clears them: its replays cannot look)
+  if (lead->barrier_dirty || cap != cudaStreamCaptureStatusNone) {
+    CK(cudaMemsetAsync(lead->d_barrier, 0, BARRIER_WORDS * sizeof(uint32_t), s));
+    lead->barrier_dirty = false;
+  }
   int pi = lead->prof.begin(ST_DEDUPE, s);
   for (size_t g = 0; g < lp.groups.size(); g++)
     CK(launch_dedupe(lead->d_batch, (int)lp.groups[g][0], (int)lp.groups[g][1], lp.groups[g][2], lp.rows,
@@ -860,8 +863,10 @@ static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf,
                               int32_t *queued) {
   cudaStream_t s = h->stream;
   const Counters &hc = *h->h_cnt;
-  if (hc.error & (ERR_SPIN_TIMEOUT | ERR_DEDUPE_NOT_CONVERGED))
+  if (hc.error & (ERR_SPIN_TIMEOUT | ERR_DEDUPE_NOT_CONVERGED)) {
+    h->barrier_dirty = true;
     return set_err(h, FF_ERR_TIMEOUT, "a bounded device-side wait gave up during allocation");
+  }
   if (hc.error & ERR_PENDING_OVERFLOW) return set_err(h, FF_ERR_STATE, "pending-leaf buffer overflow");
   if (hc.error & ERR_BRANCH_OVERFLOW) h->meshing_ok = false;
   const uint32_t leaves_before = plan.leaves_before;
@@ -1137,7 +1142,10 @@ ff_status ff_add_maps_u16_device(ff_handle *const *maps, int n, const uint16_t *
   for (int i = 0; i < n; i++) {
     st = frame_finish(maps[i], plan[i], mf[i], i == 0 ? pi_fin : -1, i == 0 ? pi_fuse : -1,
                       queued ? queued + i : nullptr);
-    if (st != FF_OK) return st;
+    if (st != FF_OK) {
+      lead->barrier_dirty = true;  // (the batch ran on the lead's barrier words)
+      return st;
+    }
     bricks += maps[i]->queued;
     pending += maps[i]->new_leaves;
   }

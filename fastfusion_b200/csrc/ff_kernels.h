@@ -47,6 +47,9 @@ struct MapFrame {
   // grow() has moved the grid by, so that keys do not change with growth
   uint32_t shard, shards;
   int32_t shift[3];
+  // the frame's counters are set up by the de-duplication launch: zero, the
+  // octree's branch count, and the in-volume box [0, n - 1]
+  uint32_t branches_init;
 };
 
 constexpr int BATCH_MAX = 32;
