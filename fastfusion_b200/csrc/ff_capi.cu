@@ -47,8 +47,13 @@ struct ff_handle {
   // update reads (descriptor, counters, queue, host-input images, confidence
   // map) come in two sets used by alternate frames; a set is reused only
   // after the update that read it (ev_fuse[set]) has finished.
+  // The leaf finalisation runs there too, ahead of the update, so that the
+  // next frame's de-duplication (which reads no octree) overlaps it; the
+  // next frame's insert waits for it (ev_fin, fin_pending).
   cudaStream_t fuse_stream = nullptr;
-  cudaEvent_t ev_fin = nullptr;
+  cudaEvent_t ev_alloc = nullptr;  // the frame's insert done (map stream)
+  cudaEvent_t ev_fin = nullptr;    // the frame's finalisation done (fuse_stream)
+  bool fin_pending = false;
   cudaEvent_t ev_fuse[2] = {nullptr, nullptr};
   int last_fuse = -1;  // set of the last update launched on fuse_stream
   int set = 0;
@@ -444,6 +449,7 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
     }
     if (cudaStreamCreateWithFlags(&h->fuse_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_fin, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_alloc, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_fuse[0], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_fuse[1], cudaEventDisableTiming) != cudaSuccess) {
       fail(FF_ERR_CUDA, "update stream");
@@ -511,6 +517,7 @@ ff_status ff_destroy(ff_handle *h) {
     if (h->ev_fuse[k]) cudaEventDestroy(h->ev_fuse[k]);
   }
   if (h->ev_fin) cudaEventDestroy(h->ev_fin);
+  if (h->ev_alloc) cudaEventDestroy(h->ev_alloc);
   if (h->fuse_stream) cudaStreamDestroy(h->fuse_stream);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   if (h->copy_stream) {
@@ -806,6 +813,11 @@ static ff_status frame_issue(ff_handle *lead, int n, const LaunchPlan &lp) {
     CK(launch_dedupe(lead->d_batch, (int)lp.groups[g][0], (int)lp.groups[g][1], lp.groups[g][2], lp.rows,
                      lead->d_barrier + 8 * g, lead->cfg.device, s));
   lead->prof.end(pi, lp.npix * (2 + 16 + 1), s);  // depth in; voxel keys and processed flags out
+  if (lead->fin_pending) {
+    // the previous frame's finalisation (on fuse_stream) completes the octree
+    CK(cudaStreamWaitEvent(s, lead->ev_fin, 0));
+    lead->fin_pending = false;
+  }
   pi = lead->prof.begin(ST_INSERT, s);
   launch_insert(lead->d_batch, lp.pix, s, lead->tune.insert_block > 0 ? lead->tune.insert_block : 256);
   lead->prof.end(pi, lp.npix * (16 + 1), s);  // keys and flags in (tree walks counted below)
@@ -831,16 +843,20 @@ static ff_status frame_launch_update(ff_handle *lead, int n, uint32_t max_npix, 
     CK(cudaMemcpyAsync(lead->h_cnt, lead->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
     CK(cudaEventRecord(counters, s));
   }
-  pi_fin = lead->prof.begin(ST_FINALIZE, s);
-  if (!launch_finalize_small(lead->d_batch, n, max_npix, lead->cfg.device, s))
-    return set_err(lead, FF_ERR_CUDA, "leaf finalisation could not be launched");
-  lead->prof.end(pi_fin, 0.0, s);
-  // side: the update runs on fuse_stream once this frame's leaves are final
+  // side: the finalisation and the update run on fuse_stream after the insert
   cudaStream_t fs = s;
   if (side) {
     fs = lead->fuse_stream;
-    CK(cudaEventRecord(lead->ev_fin, s));
-    CK(cudaStreamWaitEvent(fs, lead->ev_fin, 0));
+    CK(cudaEventRecord(lead->ev_alloc, s));
+    CK(cudaStreamWaitEvent(fs, lead->ev_alloc, 0));
+  }
+  pi_fin = lead->prof.begin(ST_FINALIZE, fs);
+  if (!launch_finalize_small(lead->d_batch, n, max_npix, lead->cfg.device, fs))
+    return set_err(lead, FF_ERR_CUDA, "leaf finalisation could not be launched");
+  lead->prof.end(pi_fin, 0.0, fs);
+  if (side) {
+    CK(cudaEventRecord(lead->ev_fin, fs));
+    lead->fin_pending = true;
   }
   pi_fuse = lead->prof.begin(ST_FUSE, fs);
   // enough blocks for a frame's bricks in one pass; blocks loop over larger batches

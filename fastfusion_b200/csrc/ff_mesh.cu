@@ -1390,11 +1390,13 @@ static MeshImpl &impl(MeshState &m) {
   } while (0)
 
 // Generate, sort and store the mesh cells of the current octree.
-// Bits per origin coordinate in the cell keys of a volume of side n.
+// Bits per origin coordinate in the cell keys of a volume of side n (a
+// power of two): a cell's origin is the low corner of a slot inside the
+// volume, so below n (k_cell_keys reports one that is not).
 static int key_bits_for(uint32_t n) {
   int b = 1;
   while ((1u << b) < n) b++;
-  return std::min(b + 1, 16);
+  return std::min(b, 16);
 }
 
 static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uint32_t &ncells, std::string &err) {
