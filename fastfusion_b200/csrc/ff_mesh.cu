@@ -126,8 +126,10 @@ struct GenQueues {
 // counter words of the generation (see MeshImpl::d_count)
 constexpr int LEVEL_COUNTS = 32;
 constexpr int MAX_GEN_LEVELS = 48;
-constexpr int COUNT_WORDS = LEVEL_COUNTS + 4 * (MAX_GEN_LEVELS + 1) + 28;
-constexpr int HOST_TOTALS = COUNT_WORDS - 8;  // host mirror only: 3 uint64 + 2 uint32 read back per update
+constexpr int COUNT_WORDS = LEVEL_COUNTS + 4 * (MAX_GEN_LEVELS + 1) + 30;
+// host mirror only: 3 uint64 + 2 uint32 read back per update, then the emit
+// pass's sample count (uint64)
+constexpr int HOST_TOTALS = COUNT_WORDS - 10;
 
 struct GenCtx {
   const uint32_t *tree;
@@ -964,6 +966,7 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
         nneed += __popc(b);
       }
       __syncwarp();
+      if (lane == 0) atomicAdd(m.samples, (unsigned long long)nneed);
       for (int k = lane; k < nneed; k += 32) {
         const int si = need[k];
         Sample s;
@@ -1110,7 +1113,7 @@ __global__ void k_mesh_corner(VoxSrc m, const Cell *__restrict__ cells, uint32_t
     if (!EMIT) out[cid] = CellOut{0u, 0u};
     return;
   }
-  if (!EMIT) atomicAdd(m.samples, 8ull);
+  atomicAdd(m.samples, 8ull);
   float d[8], w[8];
   uint16_t col[8][3];
   for (int k = 0; k < 8; k++) {
@@ -1651,6 +1654,8 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   MCK(grow_buf(M.d_xyz, I.cap_xyz, 3 * tot[0] + 3, s));
   MCK(grow_buf(M.d_rgb, I.cap_rgb, 3 * tot[0] + 3, s));
   MCK(grow_buf(M.d_faces, I.cap_faces, 3 * tot[1] + 3, s));
+  // the emit pass counts the samples it reads in d_count words 18-19
+  vs.samples = reinterpret_cast<unsigned long long *>(I.d_count + 18);
   pi = P.begin(ST_MESH_EMIT, s);
   note_launch((first_corner ? 1 : 0) + (ncells > first_corner ? 1 : 0) + (incremental && ncells ? 1 : 0));
   if (first_corner)
@@ -1665,10 +1670,14 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
     k_copy_clean<<<148 * 8, 256, 0, s>>>(I.dirty, I.old_index, ncells, I.out, I.vbase, I.fbase, I.old_vbase,
                                          I.old_fbase, I.old_xyz, I.old_rgb, I.old_faces, M.d_xyz, M.d_rgb,
                                          M.d_faces);
-  // emit pass: the samples again and the whole mesh written (xyz 12 B + rgb
-  // 3 B per vertex, 12 B per face)
-  P.end(pi, (double)nsamples * sample_bytes + (double)tot[0] * 15 + (double)tot[1] * 12, s);
+  // emit pass: the samples it reads (the ends of vertex-carrying lattice
+  // edges, corner cells' 8) and the whole mesh written (xyz 12 B + rgb 3 B
+  // per vertex, 12 B per face); the sample count arrives with the final sync
+  const int pi_emit = pi;
+  P.end(pi_emit, 0.0, s);
   MCK(cudaGetLastError());
+  uint64_t *h_emit = reinterpret_cast<uint64_t *>(I.h_count + HOST_TOTALS + 8);
+  MCK(cudaMemcpyAsync(h_emit, I.d_count + 18, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
   // keep this update's cells, counts and bases for the next one
   std::swap(I.cells, I.old_cells);
   std::swap(I.cap_cells, I.cap_old);
@@ -1684,6 +1693,7 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   I.key_bits = kb;
   I.since = in.frame;
   MCK(cudaStreamSynchronize(s));
+  P.set_bytes(pi_emit, (double)*h_emit * sample_bytes + (double)tot[0] * 15 + (double)tot[1] * 12);
   M.n_vertices = tot[0];
   M.n_faces = tot[1];
   M.n_cells = ncells;
