@@ -92,8 +92,8 @@ ff_status ff_destroy(ff_handle *h);
  * library's own stream). */
 ff_status ff_set_stream(ff_handle *h, void *cuda_stream);
 
-/* Wait for this map's outstanding device work (the last frame's voxel
- * update, which an add-map call does not wait for). */
+/* Wait for this map's outstanding device work (the last frame's placement
+ * of new bricks and voxel update, which an add-map call does not wait for). */
 ff_status ff_sync(ff_handle *h);
 
 /* Fuse one frame.  Replaces FusionMipMapCPU::addMap(const cv::Mat &depth
@@ -109,9 +109,10 @@ ff_status ff_add_map_u16(ff_handle *h, const uint16_t *depth, int width, int hei
 
 /* Same as ff_add_map_u16 with depth/bgr already in device memory (tightly
  * packed).  No host<->device copy of the images.  The call returns once the
- * frame's bricks are allocated and counted; its voxel update may still be
- * running on the map's stream, so the device images must stay unchanged
- * until the next call on this handle returns or ff_sync(h). */
+ * frame's bricks are counted; the placement of its new bricks and its voxel
+ * update may still be running on a second stream of the map (every later call
+ * on this handle is ordered after them), so the device images must stay
+ * unchanged until the next call on this handle returns or ff_sync(h). */
 ff_status ff_add_map_u16_device(ff_handle *h, const uint16_t *d_depth, const uint8_t *d_bgr, int width, int height,
                                 const double K[4], const double R[9], const double t[3], float scaling,
                                 float maxcam, int32_t *queued);
