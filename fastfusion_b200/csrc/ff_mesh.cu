@@ -1677,7 +1677,7 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   P.end(pi_emit, 0.0, s);
   MCK(cudaGetLastError());
   uint64_t *h_emit = reinterpret_cast<uint64_t *>(I.h_count + HOST_TOTALS + 8);
-  MCK(cudaMemcpyAsync(h_emit, I.d_count + 18, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  if (P.on) MCK(cudaMemcpyAsync(h_emit, I.d_count + 18, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
   // keep this update's cells, counts and bases for the next one
   std::swap(I.cells, I.old_cells);
   std::swap(I.cap_cells, I.cap_old);
@@ -1692,8 +1692,13 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   I.n_old = ncells;
   I.key_bits = kb;
   I.since = in.frame;
-  MCK(cudaStreamSynchronize(s));
-  P.set_bytes(pi_emit, (double)*h_emit * sample_bytes + (double)tot[0] * 15 + (double)tot[1] * 12);
+  // The emit pass may still run when this returns: everything that reads the
+  // mesh or the volume later is ordered after it on this stream.  With the
+  // stage profile on, wait for its sample count (the stage's bytes).
+  if (P.on) {
+    MCK(cudaStreamSynchronize(s));
+    P.set_bytes(pi_emit, (double)*h_emit * sample_bytes + (double)tot[0] * 15 + (double)tot[1] * 12);
+  }
   M.n_vertices = tot[0];
   M.n_faces = tot[1];
   M.n_cells = ncells;
