@@ -265,11 +265,22 @@ __device__ __forceinline__ void put_edge(const GenQueues &Q, const Out &O, uint3
 
 // The item functions are templated on their axis and fully unrolled, so every
 // slot array index is a compile-time constant and the slots stay in registers.
+//
+// A slot that is not subdivided and has no leaf at or above it is empty
+// space: it stays itself in every descendant of an item that holds it, and a
+// cell with a side without a leaf is never meshed, so such an item is
+// dropped without expanding it (the meshed cells are the same).
+__device__ __forceinline__ bool dead_slot(const Slot &s, bool sub) { return !sub && s.la >= BRANCHINIT; }
 
 __device__ __forceinline__ void vert_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot (&S8)[8]) {
-  bool any = false;
+  bool any = false, dead = false;
 #pragma unroll
-  for (int j = 0; j < 8; j++) any |= is_sub(g, S8[j]);
+  for (int j = 0; j < 8; j++) {
+    const bool sub = is_sub(g, S8[j]);
+    any |= sub;
+    dead |= dead_slot(S8[j], sub);
+  }
+  if (dead) return;
   if (any) {
     Slot C[8];
 #pragma unroll
@@ -298,9 +309,14 @@ __device__ __forceinline__ void vert_item(const GenCtx &g, const GenQueues &Q, c
 template <int E>
 __device__ __forceinline__ void edge_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot (&S4)[4]) {
   constexpr int P = E == 0 ? 1 : 0, Qx = E == 2 ? 1 : 2;  // the two axes across the edge line
-  bool any = false;
+  bool any = false, dead = false;
 #pragma unroll
-  for (int j = 0; j < 4; j++) any |= is_sub(g, S4[j]);
+  for (int j = 0; j < 4; j++) {
+    const bool sub = is_sub(g, S4[j]);
+    any |= sub;
+    dead |= dead_slot(S4[j], sub);
+  }
+  if (dead) return;
   if (!any) {
     // the edge line runs along a side of the smallest slot
     int size = S4[0].size, small = 0;
@@ -345,7 +361,9 @@ __device__ __forceinline__ void edge_item(const GenCtx &g, const GenQueues &Q, c
 template <int AX>
 __device__ __forceinline__ void face_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot &A,
                                           const Slot &B) {
-  if (!is_sub(g, A) && !is_sub(g, B)) {
+  const bool sa = is_sub(g, A), sb = is_sub(g, B);
+  if (dead_slot(A, sa) || dead_slot(B, sb)) return;
+  if (!sa && !sb) {
     const int size = min((int)A.size, (int)B.size);
     const bool a_small = A.size <= B.size;
     int o[3] = {a_small ? A.o[0] : B.o[0], a_small ? A.o[1] : B.o[1], a_small ? A.o[2] : B.o[2]};
