@@ -145,8 +145,7 @@ __device__ __forceinline__ bool same3(int a0, int a1, int a2, int b0, int b1, in
 // have settled recomputes the same bits until every map has).
 // Maps [m0, m1) of the batch (their tiles must all be resident at once).
 template <int DD_ROWS>
-__global__ void __launch_bounds__(32 * DD_WARPS) k_dedupe(const BatchDesc *__restrict__ bd, int m0, int m1,
-                                                          uint32_t *bar) {
+__device__ __forceinline__ void dedupe_body(const BatchDesc *__restrict__ bd, int m0, int m1, uint32_t *bar) {
   const int lane = threadIdx.x & 31;
   const uint32_t base = m0 ? bd->tile_end[m0 - 1] : 0u;
   const uint32_t gtile = base + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -304,6 +303,25 @@ __global__ void __launch_bounds__(32 * DD_WARPS) k_dedupe(const BatchDesc *__res
   }
 }
 
+template <int DD_ROWS>
+__global__ void __launch_bounds__(32 * DD_WARPS) k_dedupe(const BatchDesc *__restrict__ bd, int m0, int m1,
+                                                          uint32_t *bar) {
+  dedupe_body<DD_ROWS>(bd, m0, m1, bar);
+}
+
+// One map's frame, its descriptor a launch parameter: block 0 also stores it
+// to `out`, where the frame's later kernels read it.
+template <int DD_ROWS>
+__global__ void __launch_bounds__(32 * DD_WARPS) k_dedupe_one(const __grid_constant__ BatchDesc1 desc,
+                                                              BatchDesc *out, uint32_t *bar) {
+  if (blockIdx.x == 0) {
+    const uint2 *src = reinterpret_cast<const uint2 *>(&desc);
+    uint2 *dst = reinterpret_cast<uint2 *>(out);
+    for (int k = threadIdx.x; k < (int)(sizeof(BatchDesc1) / 8); k += blockDim.x) dst[k] = src[k];
+  }
+  dedupe_body<DD_ROWS>(reinterpret_cast<const BatchDesc *>(&desc), 0, 1, bar);
+}
+
 int dedupe_tiles(int W, int H, int *tilesX, int *tilesY, int rows) {
   const int tx = (W + 31) / 32, ty = (H + rows - 1) / rows;
   if (tilesX) *tilesX = tx;
@@ -322,9 +340,12 @@ static cudaError_t resident_dedupe_warps(int device, int &warps) {
   static int resident[64] = {};
   const int dslot = device & 63;
   if (!resident[dslot]) {
-    int per_sm = 0, sms = 0;
+    int per_sm = 0, per_sm_one = 0, sms = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dedupe<ROWS>, 32 * DD_WARPS, 0);
     if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_one, k_dedupe_one<ROWS>, 32 * DD_WARPS, 0);
+    if (e != cudaSuccess) return e;
+    per_sm = std::min(per_sm, per_sm_one);  // (both launch forms use one capacity)
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
     resident[dslot] = per_sm * sms;
@@ -355,6 +376,23 @@ cudaError_t launch_dedupe(const BatchDesc *d_batch, int m0, int m1, uint32_t til
   const void *fn = rows == DD_ROWS_SHORT  ? (const void *)k_dedupe<DD_ROWS_SHORT>
                    : rows == DD_ROWS_LOW ? (const void *)k_dedupe<DD_ROWS_LOW>
                                          : (const void *)k_dedupe<DD_ROWS_TALL>;
+  return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(32 * DD_WARPS), args, 0, s);
+}
+
+cudaError_t launch_dedupe_one(const BatchDesc *h_desc, BatchDesc *d_batch, uint32_t tiles, int rows,
+                              uint32_t *barrier, int device, cudaStream_t s) {
+  uint32_t cap = 0;
+  cudaError_t e = dedupe_capacity(device, rows, cap);
+  if (e != cudaSuccess) return e;
+  const int blocks = (int)((tiles + DD_WARPS - 1) / DD_WARPS);
+  if ((uint32_t)blocks * DD_WARPS > cap || blocks < 1 || h_desc->n != 1) return cudaErrorInvalidConfiguration;
+  BatchDesc1 d1;
+  memcpy(&d1, h_desc, sizeof(BatchDesc1));
+  void *args[] = {(void *)&d1, (void *)&d_batch, (void *)&barrier};
+  note_launch();
+  const void *fn = rows == DD_ROWS_SHORT  ? (const void *)k_dedupe_one<DD_ROWS_SHORT>
+                   : rows == DD_ROWS_LOW ? (const void *)k_dedupe_one<DD_ROWS_LOW>
+                                         : (const void *)k_dedupe_one<DD_ROWS_TALL>;
   return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(32 * DD_WARPS), args, 0, s);
 }
 
@@ -753,6 +791,8 @@ void launch_fill(uint32_t *p, size_t n, uint32_t v, cudaStream_t s) {
 // would otherwise land inside the first frame that needs a kernel).
 cudaError_t prewarm_alloc_kernels() {
   const void *fns[] = {(const void *)k_first_bbox, (const void *)k_dedupe<DD_ROWS_SHORT>,
+                       (const void *)k_dedupe_one<DD_ROWS_SHORT>, (const void *)k_dedupe_one<DD_ROWS_LOW>,
+                       (const void *)k_dedupe_one<DD_ROWS_TALL>,
                        (const void *)k_dedupe<DD_ROWS_LOW>,
                        (const void *)k_dedupe<DD_ROWS_TALL>, (const void *)k_insert,
                        (const void *)k_pending_keys, (const void *)k_finalize, (const void *)k_parents,

@@ -800,18 +800,27 @@ static ff_status frame_plan(ff_handle *lead, int n, LaunchPlan &lp) {
 static ff_status frame_issue(ff_handle *lead, int n, const LaunchPlan &lp) {
   ff_handle *h = lead;  // (error reporting)
   cudaStream_t s = lead->stream;
-  CK(cudaMemcpyAsync(lead->d_batch, lead->h_batch, batch_desc_bytes(n), cudaMemcpyHostToDevice, s));
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   CK(cudaStreamIsCapturing(s, &cap));
+  // one map: the descriptor travels as the de-duplication launch's parameter,
+  // which stores it for the later kernels; otherwise it is uploaded (a
+  // recorded graph re-reads it from pinned memory at each replay)
+  const bool by_param = n == 1 && lp.groups.size() == 1 && cap == cudaStreamCaptureStatusNone;
+  if (!by_param)
+    CK(cudaMemcpyAsync(lead->d_batch, lead->h_batch, batch_desc_bytes(n), cudaMemcpyHostToDevice, s));
   // (a recorded graph always clears them: its replays cannot look)
   if (lead->barrier_dirty || cap != cudaStreamCaptureStatusNone) {
     CK(cudaMemsetAsync(lead->d_barrier, 0, BARRIER_WORDS * sizeof(uint32_t), s));
     lead->barrier_dirty = false;
   }
   int pi = lead->prof.begin(ST_DEDUPE, s);
-  for (size_t g = 0; g < lp.groups.size(); g++)
-    CK(launch_dedupe(lead->d_batch, (int)lp.groups[g][0], (int)lp.groups[g][1], lp.groups[g][2], lp.rows,
-                     lead->d_barrier + 8 * g, lead->cfg.device, s));
+  if (by_param)
+    CK(launch_dedupe_one(lead->h_batch, lead->d_batch, lp.groups[0][2], lp.rows, lead->d_barrier, lead->cfg.device,
+                         s));
+  else
+    for (size_t g = 0; g < lp.groups.size(); g++)
+      CK(launch_dedupe(lead->d_batch, (int)lp.groups[g][0], (int)lp.groups[g][1], lp.groups[g][2], lp.rows,
+                       lead->d_barrier + 8 * g, lead->cfg.device, s));
   lead->prof.end(pi, lp.npix * (2 + 16 + 1), s);  // depth in; voxel keys and processed flags out
   if (lead->fin_pending) {
     // the previous frame's finalisation (on fuse_stream) completes the octree

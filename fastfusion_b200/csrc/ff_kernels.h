@@ -65,6 +65,21 @@ struct BatchDesc {
 // Bytes of a BatchDesc holding n maps (the tail past f[n-1] is not uploaded).
 inline size_t batch_desc_bytes(int n) { return offsetof(BatchDesc, f) + sizeof(MapFrame) * (size_t)n; }
 
+// The descriptor of one map's frame, passed by value to its de-duplication
+// launch (which stores it for the frame's later kernels): the first
+// batch_desc_bytes(1) bytes of a BatchDesc.
+struct BatchDesc1 {
+  int n;
+  int max_rounds;
+  uint32_t tile_end[BATCH_MAX];
+  uint32_t pix_end[BATCH_MAX];
+  MapFrame f[1];
+};
+static_assert(offsetof(BatchDesc1, f) == offsetof(BatchDesc, f) && sizeof(BatchDesc1) == offsetof(BatchDesc, f) +
+                                                                                          sizeof(MapFrame),
+              "one-map descriptor layout");
+static_assert(sizeof(BatchDesc1) % 8 == 0 && alignof(BatchDesc1) >= 8, "copied in 8-byte words");
+
 // A leaf claimed during the frame's traversal, before its index is assigned.
 struct PendingLeaf {
   uint32_t slot;         // tree entry that will hold the leaf index
@@ -91,6 +106,11 @@ size_t dedupe_boundary_elems(int W, int H);
 // fit the launch.  barrier: 8 zeroed uint32 words per launch.
 cudaError_t launch_dedupe(const BatchDesc *d_batch, int m0, int m1, uint32_t tiles, int rows, uint32_t *barrier,
                           int device, cudaStream_t s);
+// The same for a one-map descriptor h_desc in host memory: passed as the
+// launch's parameter (no upload of its own) and stored to d_batch by the
+// launch for the frame's later kernels.
+cudaError_t launch_dedupe_one(const BatchDesc *h_desc, BatchDesc *d_batch, uint32_t tiles, int rows,
+                              uint32_t *barrier, int device, cudaStream_t s);
 
 // Octree descent / allocation of every processed pixel of the batch.
 void launch_insert(const BatchDesc *d_batch, uint32_t total_pix, cudaStream_t s, int block = 256);
