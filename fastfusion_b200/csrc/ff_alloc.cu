@@ -174,8 +174,12 @@ __device__ __forceinline__ void dedupe_body(const BatchDesc *__restrict__ bd, in
   if (blockIdx.x == 0 && (int)threadIdx.x < m1 - m0) {
     const MapFrame &G = bd->f[m0 + threadIdx.x];
     Counters *c = G.cnt;
+    // (not the confidence network's error word, which that network may be
+    // setting meanwhile on another stream)
+    constexpr int keep = (int)(offsetof(Counters, cnn_error) / 4);
     uint32_t *w = reinterpret_cast<uint32_t *>(c);
-    for (int k = 0; k < (int)(sizeof(Counters) / 4); k++) w[k] = 0;
+    for (int k = 0; k < (int)(sizeof(Counters) / 4); k++)
+      if (k != keep) w[k] = 0;
     c->branches_used = G.branches_init;
     for (int r = 0; r < 3; r++) {
       c->box_min[r] = 0;

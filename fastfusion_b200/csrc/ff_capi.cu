@@ -52,6 +52,8 @@ struct ff_handle {
   // next frame's insert waits for it (ev_fin, fin_pending).
   cudaStream_t fuse_stream = nullptr;
   cudaEvent_t ev_alloc = nullptr;  // the frame's insert done (map stream)
+  cudaEvent_t ev_cnn_in = nullptr, ev_cnn_done = nullptr;  // the confidence network on fuse_stream
+  bool cnn_pending = false;
   cudaEvent_t ev_fin = nullptr;    // the frame's finalisation done (fuse_stream)
   bool fin_pending = false;
   cudaEvent_t ev_fuse[2] = {nullptr, nullptr};
@@ -438,6 +440,9 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
     if (alloc(&h->d_col, L * 1536) != cudaSuccess) { fail(FF_ERR_OOM_POOL, "colour pool"); break; }
     if (alloc(&h->d_cnt_set[0], 1) != cudaSuccess || alloc(&h->d_cnt_set[1], 1) != cudaSuccess ||
         alloc(&h->d_barrier, BARRIER_WORDS) != cudaSuccess) { fail(FF_ERR_CUDA, "counters"); break; }
+    // (frames set their counters up on the device; the network's error word is kept)
+    if (cudaMemset(h->d_cnt_set[0], 0, sizeof(Counters)) != cudaSuccess ||
+        cudaMemset(h->d_cnt_set[1], 0, sizeof(Counters)) != cudaSuccess) { fail(FF_ERR_CUDA, "counters"); break; }
     if (cudaMallocHost((void **)&h->h_cnt_set[0], sizeof(Counters)) != cudaSuccess ||
         cudaMallocHost((void **)&h->h_cnt_set[1], sizeof(Counters)) != cudaSuccess) { fail(FF_ERR_CUDA, "pinned"); break; }
     if (cudaMalloc((void **)&h->d_batch_set[0], sizeof(BatchDesc)) != cudaSuccess ||
@@ -450,6 +455,8 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
     if (cudaStreamCreateWithFlags(&h->fuse_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_fin, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_alloc, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_cnn_in, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_cnn_done, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_fuse[0], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_fuse[1], cudaEventDisableTiming) != cudaSuccess) {
       fail(FF_ERR_CUDA, "update stream");
@@ -518,6 +525,8 @@ ff_status ff_destroy(ff_handle *h) {
   }
   if (h->ev_fin) cudaEventDestroy(h->ev_fin);
   if (h->ev_alloc) cudaEventDestroy(h->ev_alloc);
+  if (h->ev_cnn_in) cudaEventDestroy(h->ev_cnn_in);
+  if (h->ev_cnn_done) cudaEventDestroy(h->ev_cnn_done);
   if (h->fuse_stream) cudaStreamDestroy(h->fuse_stream);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   if (h->copy_stream) {
@@ -604,9 +613,12 @@ struct FramePlan {
 static uint32_t pad32(uint32_t v) { return (v + 31u) & ~31u; }
 
 // Host part before the launches; fills the frame's descriptor.
+// side: a single-map frame whose update runs on fuse_stream; its confidence
+// network (learned weight) runs there too, overlapping the de-duplication and
+// the insert, and the counter copy waits for it (it reports into them).
 static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint8_t *d_bgr, int W, int H,
                                const double *K, const double *R, const double *t, float scaling, float maxcam,
-                               MapFrame &mf, FramePlan &plan) {
+                               MapFrame &mf, FramePlan &plan, bool side = false) {
   cudaStream_t s = h->stream;
   CamF p = cam_world_to_grid(h, K, R, t);
   Counters &hc = *h->h_cnt;
@@ -719,13 +731,24 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
       h->conf_cap = npx;
     }
     const float kf[4] = {(float)K[0], (float)K[1], (float)K[2], (float)K[3]};
-    const int pc = h->prof.begin(ST_CONFIDENCE, s);
-    CK(cnn_features(d_depth, 1, W, H, scaling, kf, h->d_feat, s));
+    cudaStream_t cs = s;
+    if (side && plan.one_sync) {
+      // after the depth image is ready on the map's stream
+      cs = h->fuse_stream;
+      CK(cudaEventRecord(h->ev_cnn_in, s));
+      CK(cudaStreamWaitEvent(cs, h->ev_cnn_in, 0));
+    }
+    const int pc = h->prof.begin(ST_CONFIDENCE, cs);
+    CK(cnn_features(d_depth, 1, W, H, scaling, kf, h->d_feat, cs));
     CK(cnn_forward(h->d_cnn_params, h->d_cnn_packed, h->cnn_packed_ready, h->d_feat, 1, W, H, h->d_a1, h->d_a2,
-                   h->d_conf, h->conf_tau_cm, &h->d_cnt->error, s));
+                   h->d_conf, h->conf_tau_cm, &h->d_cnt->cnn_error, cs));
     h->cnn_packed_ready = true;
     // depth -> features -> a1 -> a2 -> confidence, each written once and read once
-    h->prof.end(pc, (double)npx * ((2 + 16) + (16 + 32) + (32 + 32) + (32 + 4)), s);
+    h->prof.end(pc, (double)npx * ((2 + 16) + (16 + 32) + (32 + 32) + (32 + 4)), cs);
+    if (cs != s) {
+      CK(cudaEventRecord(h->ev_cnn_done, cs));
+      h->cnn_pending = true;
+    }
     h->conf_w = W;
     h->conf_h = H;
     mf.conf = h->d_conf;
@@ -849,6 +872,11 @@ static ff_status frame_launch_update(ff_handle *lead, int n, uint32_t max_npix, 
   ff_handle *h = lead;  // (error reporting)
   cudaStream_t s = lead->stream;
   if (counters) {
+    if (lead->cnn_pending) {
+      // the frame's confidence network reports into these counters
+      CK(cudaStreamWaitEvent(s, lead->ev_cnn_done, 0));
+      lead->cnn_pending = false;
+    }
     CK(cudaMemcpyAsync(lead->h_cnt, lead->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
     CK(cudaEventRecord(counters, s));
   }
@@ -888,6 +916,11 @@ static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf,
                               int32_t *queued) {
   cudaStream_t s = h->stream;
   const Counters &hc = *h->h_cnt;
+  if (hc.cnn_error) {
+    // (the word is kept across frames until cleared here)
+    CK(cudaMemsetAsync(&h->d_cnt->cnn_error, 0, sizeof(uint32_t), h->stream));
+    return set_err(h, FF_ERR_TIMEOUT, "a bounded device-side wait gave up in the confidence network");
+  }
   if (hc.error & (ERR_SPIN_TIMEOUT | ERR_DEDUPE_NOT_CONVERGED)) {
     h->barrier_dirty = true;
     return set_err(h, FF_ERR_TIMEOUT, "a bounded device-side wait gave up during allocation");
@@ -970,7 +1003,7 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
   cudaStream_t s = h->stream;
   FramePlan plan;
   MapFrame mf;
-  ff_status st = frame_prepare(h, d_depth, d_bgr, W, H, K, R, t, scaling, maxcam, mf, plan);
+  ff_status st = frame_prepare(h, d_depth, d_bgr, W, H, K, R, t, scaling, maxcam, mf, plan, true);
   if (st != FF_OK) return st;
   h->h_batch->f[0] = mf;
   st = frame_launch(h, 1);

@@ -60,7 +60,8 @@ struct Counters {
   uint32_t n_work_next;
   uint64_t mesh_v;
   uint64_t mesh_f;
-  uint32_t pad[4];
+  uint32_t cnn_error;  // the confidence network's bounded waits (kept by the frame's counter set-up)
+  uint32_t pad[3];
 };
 
 // Float camera parameters (the reference's camPamsFloat, definitions.h:71-88).
