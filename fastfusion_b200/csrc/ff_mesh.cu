@@ -561,6 +561,13 @@ __device__ __forceinline__ uint16_t vc(const VoxSrc &m, size_t i, int c) {
   return m.col[(i >> 9) * 1536 + c * 512 + (i & 511)];
 }
 
+// A sample's colour channel, or 0 without a read when the pass needs no
+// colour (the count pass: only SDF and weight decide the cube cases).
+template <bool COLOR>
+__device__ __forceinline__ uint16_t vcs(const VoxSrc &m, size_t i, int c) {
+  return COLOR ? vc(m, i, c) : (uint16_t)0;
+}
+
 // MarchingCubes::VertexInterp(Vertex3f, Vertex3f, double, double), mesh.cpp:1266-1315
 __device__ void vinterp(const float *p1, const float *p2, double v1, double v2, float *out) {
   if (fabs(__dsub_rn(0.0, v1)) < 1e-40) {
@@ -663,6 +670,7 @@ __device__ __forceinline__ int sample_pos(const CellGeom &G, int r, int b) {
 // One lattice sample of an interior/wall/edge cell; returns false when the
 // interior cell does not fit in a leaf of its chain (the reference then
 // leaves the cell's mesh empty).
+template <bool COLOR>
 __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G, int bx, int by, int bz, Sample &s) {
   const int t = G.type;
   const int bb[3] = {bx, by, bz};
@@ -729,7 +737,7 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
         s.w = __fadd_rn(s.w, vw(m, v0));
         s.d = d0;
 #pragma unroll
-        for (int r = 0; r < 3; r++) s.c[r] = vc(m, v0, r);
+        for (int r = 0; r < 3; r++) s.c[r] = vcs<COLOR>(m, v0, r);
         continue;
       }
     }
@@ -751,16 +759,16 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
       float cf3[3][8];
       if (on_lattice) {
         const float d0 = vd(m, vi[0]);
-        const float c0 = (float)vc(m, vi[0], 0), c1 = (float)vc(m, vi[0], 1), c2 = (float)vc(m, vi[0], 2);
+        const float c0 = (float)vcs<COLOR>(m, vi[0], 0), c1 = (float)vcs<COLOR>(m, vi[0], 1), c2 = (float)vcs<COLOR>(m, vi[0], 2);
 #pragma unroll
         for (int k = 0; k < 8; k++) df[k] = d0, cf3[0][k] = c0, cf3[1][k] = c1, cf3[2][k] = c2;
       } else {
 #pragma unroll
         for (int k = 0; k < 8; k++) {
           df[k] = vd(m, vi[k]);
-          cf3[0][k] = (float)vc(m, vi[k], 0);
-          cf3[1][k] = (float)vc(m, vi[k], 1);
-          cf3[2][k] = (float)vc(m, vi[k], 2);
+          cf3[0][k] = (float)vcs<COLOR>(m, vi[k], 0);
+          cf3[1][k] = (float)vcs<COLOR>(m, vi[k], 1);
+          cf3[2][k] = (float)vcs<COLOR>(m, vi[k], 2);
         }
       }
       s.w = __fadd_rn(s.w, vw(m, vi[0]));
@@ -789,7 +797,7 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
           s.w = __fadd_rn(s.w, w0);
           s.d = d0;
 #pragma unroll
-          for (int r = 0; r < 3; r++) s.c[r] = vc(m, v0, r);
+          for (int r = 0; r < 3; r++) s.c[r] = vcs<COLOR>(m, v0, r);
           continue;
         }
       }
@@ -806,7 +814,7 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
       if (lh[a] == ll[a] && lh[b] == ll[b]) {
         // on the leaf's own lattice: one voxel
         const float w0 = vw(m, vi[0]), d0 = vd(m, vi[0]);
-        const float c0 = (float)vc(m, vi[0], 0), c1 = (float)vc(m, vi[0], 1), c2 = (float)vc(m, vi[0], 2);
+        const float c0 = (float)vcs<COLOR>(m, vi[0], 0), c1 = (float)vcs<COLOR>(m, vi[0], 1), c2 = (float)vcs<COLOR>(m, vi[0], 2);
 #pragma unroll
         for (int k = 0; k < 4; k++) wf[k] = w0, df[k] = d0, cf3[0][k] = c0, cf3[1][k] = c1, cf3[2][k] = c2;
       } else {
@@ -814,9 +822,9 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
         for (int k = 0; k < 4; k++) {
           wf[k] = vw(m, vi[k]);
           df[k] = vd(m, vi[k]);
-          cf3[0][k] = (float)vc(m, vi[k], 0);
-          cf3[1][k] = (float)vc(m, vi[k], 1);
-          cf3[2][k] = (float)vc(m, vi[k], 2);
+          cf3[0][k] = (float)vcs<COLOR>(m, vi[k], 0);
+          cf3[1][k] = (float)vcs<COLOR>(m, vi[k], 1);
+          cf3[2][k] = (float)vcs<COLOR>(m, vi[k], 2);
         }
       }
       const float wsum = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(f[0], wf[0]), __fmul_rn(f[1], wf[1])),
@@ -846,7 +854,7 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
       s.d = __fadd_rn(__fmul_rn(ran, vd(m, v0)), __fmul_rn(ra, vd(m, v1)));
 #pragma unroll
       for (int r = 0; r < 3; r++) {
-        const float v = __fadd_rn(__fmul_rn(ran, (float)vc(m, v0, r)), __fmul_rn(ra, (float)vc(m, v1, r)));
+        const float v = __fadd_rn(__fmul_rn(ran, (float)vcs<COLOR>(m, v0, r)), __fmul_rn(ra, (float)vcs<COLOR>(m, v1, r)));
         s.c[r] = (uint16_t)__float2int_rz(v);
       }
     }
@@ -855,18 +863,19 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
 }
 
 // Per-warp shared scratch of one lattice cell.  Only the zero test of a
-// sample's weight is needed after sampling; vidx is used by the emit pass
-// alone, so the count pass's scratch stops before it (more warps per SM).
+// sample's weight is needed after sampling; colours and vertex numbers are
+// used by the emit pass alone, so the count pass's scratch stops before them
+// (more warps per SM).
 // Edge flags are bytes: plain stores, where bits would need atomics.
 struct WarpScratch {
   float sd[512];           // SDF of each lattice sample
-  uint16_t sc[512 * 3];    // colour (R, G, B) of each sample
   uint8_t wzero[512];      // the sample's weight is zero
   uint8_t cube_case[512];  // marching-cubes case of each cube
   uint8_t edge_set[512 * 3];  // lattice-edge slots (3 per voxel) that carry a vertex
+  uint16_t sc[512 * 3];    // emit pass: colour (R, G, B) of each sample
   uint16_t vidx[512 * 3];  // emit pass: the vertex number of each such slot
 };
-constexpr size_t SCRATCH_COUNT_BYTES = offsetof(WarpScratch, vidx);
+constexpr size_t SCRATCH_COUNT_BYTES = offsetof(WarpScratch, sc);
 constexpr size_t SCRATCH_EMIT_BYTES = sizeof(WarpScratch);
 static_assert(SCRATCH_COUNT_BYTES % 16 == 0 && SCRATCH_EMIT_BYTES % 16 == 0, "scratch alignment");
 
@@ -988,7 +997,7 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
       for (int k = lane; k < nneed; k += 32) {
         const int si = need[k];
         Sample s;
-        lattice_sample(m, c, G, si & 7, (si >> 3) & 7, si >> 6, s);
+        lattice_sample<true>(m, c, G, si & 7, (si >> 3) & 7, si >> 6, s);
         W.sd[si] = s.d;
         W.sc[3 * si] = s.c[0];
         W.sc[3 * si + 1] = s.c[1];
@@ -1000,12 +1009,9 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
       for (int k = lane; k < nsamp; k += 32) {
         const int bx = k % n3[0], by = (k / n3[0]) % n3[1], bz = k / (n3[0] * n3[1]);
         Sample s;
-        fit &= lattice_sample(m, c, G, bx, by, bz, s);
+        fit &= lattice_sample<false>(m, c, G, bx, by, bz, s);  // (no colour: the count pass needs none)
         const int si = (bz * 8 + by) * 8 + bx;
         W.sd[si] = s.d;
-        W.sc[3 * si] = s.c[0];
-        W.sc[3 * si + 1] = s.c[1];
-        W.sc[3 * si + 2] = s.c[2];
         W.wzero[si] = s.w == 0.0f;
       }
       for (int k = lane; k < 384; k += 32) reinterpret_cast<uint32_t *>(W.edge_set)[k] = 0;
@@ -1659,9 +1665,10 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   const uint64_t tot[2] = {h_tot[0], h_tot[1]};
   const unsigned long long nsamples = h_tot[2];
   const uint32_t ndirty = incremental ? I.h_count[HOST_TOTALS + 6] : ncells;
-  // count pass: SDF, weight and colour of every sample of the dirty cells
+  // count pass: SDF and weight of every sample of the dirty cells (the emit
+  // pass reads colour as well: sample_bytes)
   const double sample_bytes = vs.fp16 ? 10.0 : 14.0;
-  P.set_bytes(pi_count, (double)nsamples * sample_bytes);
+  P.set_bytes(pi_count, (double)nsamples * (vs.fp16 ? 4.0 : 8.0));
   // the previous output becomes the copy source; the new output is written fresh
   std::swap(I.old_xyz, M.d_xyz);
   std::swap(I.cap_oxyz, I.cap_xyz);
