@@ -1157,7 +1157,7 @@ __global__ void k_mesh_corner(VoxSrc m, const Cell *__restrict__ cells, uint32_t
       const size_t vi = vox_index(m, leaf, lx, ly, lz);
       w[k] = __fadd_rn(w[k], vw(m, vi));
       d[k] = vd(m, vi);
-      for (int r = 0; r < 3; r++) col[k][r] = vc(m, vi, r);
+      for (int r = 0; r < 3; r++) col[k][r] = vcs<EMIT>(m, vi, r);  // (the count pass needs no colour)
     }
   }
   const int mcv[8] = {0, 1, 3, 2, 4, 5, 7, 6};
@@ -1186,7 +1186,7 @@ __global__ void k_mesh_corner(VoxSrc m, const Cell *__restrict__ cells, uint32_t
     const int a = c_edge_a[e], b = c_edge_b[e];
     if (((ci8 >> a) & 1) != ((ci8 >> b) & 1)) {
       vinterp(P[a], P[b], (double)val[a], (double)val[b], vl[e]);
-      cinterp(col[mcv[a]], col[mcv[b]], val[a], val[b], cl[e]);
+      if (EMIT) cinterp(col[mcv[a]], col[mcv[b]], val[a], val[b], cl[e]);
     }
   }
   const int nt = mc_ntri(T, ci8);
