@@ -168,6 +168,16 @@ static void select_set(ff_handle *h, int k) {
   h->d_conf = h->d_conf_set[k];
 }
 
+// Wait for an event the next few microseconds will bring (a frame's counter
+// copy): poll it first, which wakes sooner than a blocking wait, then block.
+static cudaError_t wait_event_polling(cudaEvent_t ev) {
+  for (int k = 0; k < 20000; k++) {
+    const cudaError_t e = cudaEventQuery(ev);
+    if (e != cudaErrorNotReady) return e;
+  }
+  return cudaEventSynchronize(ev);
+}
+
 // Order the map's stream after every voxel update launched on fuse_stream.
 static cudaError_t join_fuse(ff_handle *h) {
   return h->last_fuse >= 0 ? cudaStreamWaitEvent(h->stream, h->ev_fuse[h->last_fuse], 0) : cudaSuccess;
@@ -1017,7 +1027,7 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
     plan.counters_early = true;
     st = frame_launch_update(h, 1, (uint32_t)(W * H), pi_fin, pi_fuse, h->ev_counters, true);
     if (st != FF_OK) return st;
-    CK(cudaEventSynchronize(h->ev_counters));
+    CK(wait_event_polling(h->ev_counters));
   } else {
     CK(cudaMemcpyAsync(h->h_cnt, h->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
