@@ -1474,7 +1474,15 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
     while (leftover && lv < MAX_GEN_LEVELS) {
       const int end = std::min(lv + batch, MAX_GEN_LEVELS);
       note_launch((unsigned)(end - lv));
-      for (; lv < end; lv++) k_gen_level<<<148 * 8, 128, 0, s>>>(g, Q, lv, in.n);
+      for (; lv < end; lv++) {
+        // an item expands into at most 27 (8 cells, 12 faces, 6 edges, 1
+        // vertex), so level l holds at most 27^l items: the first levels
+        // need few blocks (the loop inside strides over any grid)
+        uint64_t bound = 1;
+        for (int k = 0; k < lv && bound < (uint64_t)148 * 8 * 128; k++) bound *= 27;
+        const int blocks = (int)std::min<uint64_t>(148 * 8, (bound + 127) / 128);
+        k_gen_level<<<blocks, 128, 0, s>>>(g, Q, lv, in.n);
+      }
       MCK(cudaGetLastError());
       MCK(cudaMemcpyAsync(I.h_count, I.d_count, COUNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
       MCK(cudaStreamSynchronize(s));
