@@ -1,26 +1,32 @@
 """Throughput of the fusion + incremental-meshing path on B200.
 
-Workload (one map per GPU): 640x480 uint16 depth + BGR8 frames of a seeded
-8x8x3 m room with 80 boxes/spheres, rendered along a seeded random walk
-(2 cm steps, 2 degree yaw jitter, 1.2 m height; fx=fy=525).  Fusion at 5 mm
-voxels, 10 mm truncation, 4 m maximum camera distance, 8^3 bricks, FP32
-storage; incremental meshing every 10 frames.  One step = 10 addMap calls
-plus one updateMeshes.  The default run (3 warm-up + 97 timed steps) covers
-the 1000-frame walk.
+Workload (one map per GPU): the whole 1000-frame random walk of the larger
+synthetic room -- 640x480 uint16 depth + BGR8 frames of a seeded 8x8x3 m
+room with 80 boxes/spheres, rendered along a seeded random walk (2 cm steps,
+2 degree yaw jitter, 1.2 m height; fx=fy=525).  Fusion at 5 mm voxels, 10 mm
+truncation, 4 m maximum camera distance, 8^3 bricks, FP32 storage;
+incremental meshing every 10 frames.  One step = 10 addMap calls plus one
+updateMeshes.  Every run fuses the whole walk (100 steps); `--steps K` of
+them, spread evenly over the walk after the `--warmup W` first ones, are
+timed, so the timed steps sample the map from small to full size whatever K
+is.
 
 Reported (one JSON line from rank 0):
   value      frames/s over all ranks, depth/BGR already in HBM (ff_add_map_u16_device)
-  e2e        the same through the host API (ff_add_map_u16 from pinned host
-             memory, ff_update_meshes, and the whole mesh copied back to the host
-             every step)
+  e2e        the same through the host API (ff_add_map_u16 from page-locked
+             host frames, ff_update_meshes, and the whole mesh copied back to the
+             host every step); e2e_pageable: the same from pageable host frames
   roofline   the dominant stage's algorithmic bytes / CUDA-event time vs the
-             measured HBM copy bandwidth
-  cpu_baseline  the reference's FusionMipMapCPU (compiled from its sources) on
-             one host core over a bounded prefix of the same frames
+             measured HBM copy bandwidth; roofline_fuse: the same for the
+             voxel-update kernel
+  cpu_baseline  the reference's FusionMipMapCPU (compiled from its sources)
+             pinned to one host core over the same walk and the same timed
+             steps, median of 3 runs, plus a row with its threaded meshing
 
 `--impl reference` times the reference's CPU implementation instead: one map
 per host core (all cores the box gives this process, bounded by host memory),
-each running the same frames, aggregated frames/s.
+each pinned to its core and running the same walk, aggregated frames/s over
+the same timed steps.
 
 Multi-GPU (`torchrun --nproc-per-node N bench.py --gpus N`): every rank fuses
 its own independent map (walk seed = rank); no data-path collective; weak
@@ -52,7 +58,8 @@ METRIC = "depth frames/s fused+meshed (640x480, 5 mm)"
 UNIT = "frames/s"
 FALLBACK_HBM_GBS = 6650.0
 L2_FLUSH_BYTES = 256 << 20
-CPU_SAMPLE_SECONDS = 20.0
+WALK_FRAMES = 1000  # the random walk's length: every run fuses all of it
+CPU_RUNS = 3        # the CPU baseline: median of this many pinned runs
 
 # stage -> kernels it times (for the roofline record)
 # the reference's brick pool: its 2 GB cap in bricks (treeandbrick.cpp:169-229)
@@ -68,6 +75,21 @@ STAGE_KERNELS = {
     "mesh_count": "k_mesh_lattice<count>+k_mesh_corner<count>",
     "mesh_emit": "k_mesh_lattice<emit>+k_mesh_corner<emit>+k_copy_clean",
     "confidence": "k_cnn_features+k_conv x3 (learned weight)",
+}
+
+
+# stage -> the algorithmic bytes its roofline counts (per launch)
+STAGE_BYTES = {
+    "grow": "octree and leaf positions read and written",
+    "dedupe": "W*H*2 B: the depth image read (voxel keys and flags it writes stay in L2)",
+    "insert": "16 B per octree level probed per processed pixel (counted on the device)",
+    "finalize": "8 B per new brick",
+    "fuse": "14,336 B per queued brick per frame (512 voxels x (4 SDF + 4 weight + 6 colour) B, read and written; "
+            "10,240 B with FP16 storage)",
+    "mesh_cells": "3 x 48 B per mesh cell (written, then read and written by the key sort)",
+    "mesh_count": "SDF and weight (8 B, 4 B FP16) of every sample of the re-meshed cells",
+    "mesh_emit": "14 B (10 B FP16) per sample read + 15 B per vertex + 12 B per face written",
+    "confidence": "per pixel: depth in, features, two activations and the confidence written and read once",
 }
 
 
@@ -106,8 +128,17 @@ def parse_args(argv=None):
     return a
 
 
+def step_plan(a, frames: int = WALK_FRAMES):
+    """(steps run, indices of the timed steps): every step of the walk runs;
+    K timed steps are spread evenly over the steps after the W warm-up ones
+    (a walk longer than 1000 frames only when W + K steps need it)."""
+    total = max(frames // FRAMES_PER_STEP, a.warmup + a.steps)
+    span = total - a.warmup
+    return total, [a.warmup + (i * span) // a.steps for i in range(a.steps)]
+
+
 def n_frames_needed(a) -> int:
-    return (a.warmup + a.steps) * FRAMES_PER_STEP
+    return step_plan(a)[0] * FRAMES_PER_STEP
 
 
 def make_sequence(seed: int, n_frames: int):
@@ -132,11 +163,14 @@ def render_frames(seq, n_frames: int, device):
 
 
 def workload_config(a, n_frames: int) -> dict:
+    total, timed = step_plan(a)
     return {
-        "workload": f"walk{n_frames}: 8x8x3 m room, 80 primitives, {n_frames} frames 640x480 along a seeded "
-                    f"random walk, voxel 5 mm, threshold 10 mm, maxcam 4 m, 8^3 bricks, updateMeshes every "
-                    f"{FRAMES_PER_STEP} frames",
+        "workload": f"walk{n_frames}: the whole {n_frames}-frame seeded random walk (640x480) in the 8x8x3 m room "
+                    f"with 80 primitives (the larger synthetic configuration), voxel 5 mm, threshold 10 mm, maxcam "
+                    f"4 m, 8^3 bricks, multi-resolution levels, updateMeshes every {FRAMES_PER_STEP} frames; "
+                    f"{len(timed)} of its {total} steps timed, spread over the walk after {a.warmup} warm-up steps",
         "frames": n_frames,
+        "timed_steps": timed,
         "frames_per_step": FRAMES_PER_STEP,
         "width": WIDTH,
         "height": HEIGHT,
@@ -277,7 +311,9 @@ def run_b200(a):
     if a.weight == "learned":
         from fastfusion_b200.confidence import load_weights
         learned = load_weights()
-    nf = n_frames_needed(a)
+    total, timed_idx = step_plan(a)
+    timed_set = set(timed_idx)
+    nf = total * FRAMES_PER_STEP
     seq = make_sequence(a.seed + rank, nf)
     depth, bgr = render_frames(seq, nf, dev)
     cams = [ff.CameraInfo(seq.K, *seq.poses[k]) for k in range(nf)]
@@ -297,23 +333,38 @@ def run_b200(a):
             m.addMapDevice(depth[k].data_ptr(), bgr[k].data_ptr(), WIDTH, HEIGHT, cams[k], SCALING, MAXCAM)
         m.updateMeshes()
 
+    launches = [0, 0]
+
     def timed(step_fn, m, on_timed_start=None):
-        """W untimed steps, then K steps timed one by one with CUDA events
-        (L2 flushed before each); returns (device ms summed, wall s)."""
+        """The whole walk: W untimed warm-up steps, then every further step,
+        of which the K timed ones are bracketed by CUDA events (L2 flushed
+        before each); returns (device ms summed over the timed steps, wall s
+        of the walk after the warm-up).  Own kernel launches of the timed
+        steps are counted in `launches`."""
         for s in range(a.warmup):
             step_fn(m, s)
         if on_timed_start:
             on_timed_start(m)
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+        ev = []
+        launches[0] = launches[1] = 0
         torch.cuda.synchronize(dev)
         barrier()
         torch.cuda.synchronize(dev)
         w0 = time.perf_counter()
-        for i in range(a.steps):
-            flush.fill_(i)
-            ev[i][0].record(stream)
-            step_fn(m, a.warmup + i)
-            ev[i][1].record(stream)
+        for s in range(a.warmup, total):
+            if s not in timed_set:
+                step_fn(m, s)
+                continue
+            flush.fill_(s)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            own0, lib0 = ff.kernel_launches()
+            e0.record(stream)
+            step_fn(m, s)
+            e1.record(stream)
+            own1, lib1 = ff.kernel_launches()
+            launches[0] += own1 - own0
+            launches[1] += lib1 - lib0
+            ev.append((e0, e1))
         torch.cuda.synchronize(dev)
         barrier()
         torch.cuda.synchronize(dev)
@@ -326,11 +377,14 @@ def run_b200(a):
 
     # 1. device-resident throughput
     m = new_map()
-    launches = {}
+    dev_ms, dev_wall = timed(device_step, m)
+    gpu_launches, lib_calls = launches
+    st = m.stats()
+    m.close()
+    del m
 
-    def mark(mm):
-        launches["own0"], launches["lib0"] = ff.kernel_launches()
-
+    # 2. per-stage profile of the walk after the warm-up (separate map; events per stage)
+    m = new_map()
     dirty, rounds = [], []
 
     def device_step_stats(mm, s):
@@ -340,75 +394,87 @@ def run_b200(a):
         mm.updateMeshes()
         dirty.append(mm.stats()["mesh_cells_dirty"])
 
-    dev_ms, dev_wall = timed(device_step, m, mark)
-    own1, lib1 = ff.kernel_launches()
-    gpu_launches, lib_calls = own1 - launches["own0"], lib1 - launches["lib0"]
-    st = m.stats()
-    m.close()
-    del m
-
-    # 2. per-stage profile of the same steps (separate map; events per stage)
-    m = new_map()
-    prof_ms, _ = timed(device_step_stats, m, lambda mm: mm.profile(True))
+    for s_ in range(a.warmup):
+        device_step(m, s_)
+    m.profile(True)
+    torch.cuda.synchronize(dev)
+    p0 = time.perf_counter()
+    for s_ in range(a.warmup, total):
+        device_step_stats(m, s_)
     stages = m.profile_read()
+    prof_wall_ms = 1e3 * (time.perf_counter() - p0)
     m.close()
     del m
 
-    # 3. end to end through the host API
-    e2e = None
+    # 3. end to end through the host API: host frames in, whole mesh out, every step
+    e2e = e2e_pageable = None
     rms = None
     if not a.no_e2e:
-        h_depth = depth.cpu().pin_memory()
-        h_bgr = bgr.cpu().pin_memory()
-        hd = h_depth.numpy().view(np.uint16)
-        hb = h_bgr.numpy()
-        d2h = []
         last_mesh = {}
         # page-locked mesh buffer reserved before the timed region, like a
         # viewer would size it for its scene (it grows if the mesh outgrows it)
         mesh_buf = ff.MeshBuffer(4 << 20, 6 << 20)
 
-        def host_step(mm, s):
-            for k in range(s * FRAMES_PER_STEP, (s + 1) * FRAMES_PER_STEP):
-                mm.addMap(hd[k], cams[k], hb[k], SCALING, MAXCAM)
-            mm.updateMeshes()
-            mesh = mm.getMeshInterleavedMarchingCubes(out=mesh_buf)
-            d2h.append(mesh.vertices.nbytes + mesh.colors.nbytes + mesh.faces.nbytes)
-            last_mesh["m"] = mesh
+        def host_run(hd, hb):
+            d2h = []
 
-        m = new_map()
-        e2e_ms, _ = timed(host_step, m, lambda mm: d2h.clear())
-        m.close()
-        del m
-        e2e_value, e2e_ms = whole_job_rate(a.steps * FRAMES_PER_STEP, e2e_ms, dev)
-        e2e = {"value": e2e_value, "unit": UNIT,
-               "h2d_bytes_per_step": FRAMES_PER_STEP * (WIDTH * HEIGHT * 2 + WIDTH * HEIGHT * 3),
-               "d2h_bytes_per_step": int(np.mean(d2h)) if d2h else 0,
-               "ms_per_step": e2e_ms / a.steps}
+            def host_step(mm, s):
+                for k in range(s * FRAMES_PER_STEP, (s + 1) * FRAMES_PER_STEP):
+                    mm.addMap(hd[k], cams[k], hb[k], SCALING, MAXCAM)
+                mm.updateMeshes()
+                mesh = mm.getMeshInterleavedMarchingCubes(out=mesh_buf)
+                if s in timed_set:
+                    d2h.append(mesh.vertices.nbytes + mesh.colors.nbytes + mesh.faces.nbytes)
+                last_mesh["m"] = mesh
+
+            mm = new_map()
+            ms, _ = timed(host_step, mm)
+            mm.close()
+            rate, ms = whole_job_rate(a.steps * FRAMES_PER_STEP, ms, dev)
+            return {"value": rate, "unit": UNIT,
+                    "h2d_bytes_per_step": FRAMES_PER_STEP * (WIDTH * HEIGHT * 2 + WIDTH * HEIGHT * 3),
+                    "d2h_bytes_per_step": int(np.mean(d2h)) if d2h else 0, "ms_per_step": ms / a.steps}
+
+        # page-locked host frames (ff_alloc_host-style pinned memory)
+        h_depth = depth.cpu().pin_memory()
+        h_bgr = bgr.cpu().pin_memory()
+        e2e = host_run(h_depth.numpy().view(np.uint16), h_bgr.numpy())
+        e2e["host_frames"] = "page-locked"
         if rank == 0 and "m" in last_mesh and len(last_mesh["m"].vertices):
             v = last_mesh["m"].vertices
             rng = np.random.default_rng(0)
             sel = rng.choice(len(v), size=min(len(v), 300000), replace=False)
             rms = float(np.sqrt(np.mean(seq.scene.sdf(v[sel].astype(np.float64)) ** 2)))
+        del h_depth, h_bgr
+        # pageable host frames, as a caller's cv::Mat images are
+        p_depth = depth.cpu().numpy().view(np.uint16).copy()
+        p_bgr = bgr.cpu().numpy().copy()
+        e2e_pageable = host_run(p_depth, p_bgr)
+        e2e_pageable["host_frames"] = "pageable"
+        del p_depth, p_bgr
         mesh_buf.close()
     clocks = clk.stop() if clk else None
 
     value, dev_ms_max = whole_job_rate(a.steps * FRAMES_PER_STEP, dev_ms, dev)
 
-    # roofline of the dominant stage
     peak, peak_kind = measured_hbm_peak()
-    dom = max(stages, key=lambda k: stages[k][0])
-    ms_d, bytes_d, n_d = stages[dom]
-    achieved = bytes_d / (ms_d / 1e3) / 1e9 if ms_d > 0 else 0.0
-    traffic = None
     tt = read_traffic_table()
-    if dom in tt and n_d:
-        traffic = round(tt[dom] * bytes_d / n_d)
-    roofline = {"bound": "hbm", "kernel": STAGE_KERNELS[dom], "stage": dom, "achieved": round(achieved, 1),
+
+    def roofline_of(stage):
+        ms_d, bytes_d, n_d = stages[stage]
+        achieved = bytes_d / (ms_d / 1e3) / 1e9 if ms_d > 0 else 0.0
+        traffic = round(tt[stage] * bytes_d / n_d) if (stage in tt and n_d) else None
+        return {"bound": "hbm", "kernel": STAGE_KERNELS[stage], "stage": stage, "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "peak_source": f"{peak_kind} (copy bandwidth)",
-                "algorithmic_bytes_per_launch": bytes_d / n_d if n_d else 0, "launches": n_d,
-                "avg_launch_us": 1e3 * ms_d / n_d if n_d else 0, "traffic": traffic}
+                "algorithmic_bytes_per_launch": round(bytes_d / n_d) if n_d else 0, "launches": n_d,
+                "avg_launch_us": round(1e3 * ms_d / n_d, 3) if n_d else 0, "traffic": traffic,
+                "bytes_rule": STAGE_BYTES[stage]}
+
+    dom = max(stages, key=lambda k: stages[k][0])
+    roofline = roofline_of(dom)
+    roofline_fuse = roofline_of("fuse")
+    prof_ms = sum(v[0] for v in stages.values())
     stage_rec = {k: {"ms": round(v[0], 3), "share": round(v[0] / prof_ms, 4) if prof_ms else 0,
                      "GB/s": round(v[1] / (v[0] / 1e3) / 1e9, 1) if v[0] > 0 else 0, "launches": v[2],
                      "bytes_per_launch": round(v[1] / v[2]) if v[2] else 0,
@@ -426,10 +492,13 @@ def run_b200(a):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if a.storage == "fp32" else "f16-storage/f32",
             "data": "synthetic: seeded room scene rendered to depth+BGR on the GPU (the TUM RGB-D sequences "
                     "the reference documents are not available offline)",
-            "config": dict(workload_config(a, n_frames_needed(a)), parallelism=f"independent maps x{world}"),
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": gpu_launches,
+            "config": dict(workload_config(a, nf), parallelism=f"independent maps x{world}"),
+            "e2e": e2e, "e2e_pageable": e2e_pageable, "roofline": roofline, "roofline_fuse": roofline_fuse,
+            "cpu_baseline": cpu, "gpu_launches": gpu_launches,
             "library_calls": lib_calls, "clocks": clocks, "stages": stage_rec,
-            "wall_s_timed": round(dev_wall, 3), "surface_rms_m": rms,
+            "stage_profile": f"CUDA events per stage over steps {a.warmup}-{total - 1} of a separate run "
+                             f"({round(prof_wall_ms)} ms wall)",
+            "wall_s_walk": round(dev_wall, 3), "surface_rms_m": rms,
             "map": {"leaves": st["leaves_used"], "leaves_max": st["leaves_max"], "n": st["n"],
                     "mesh_vertices": st["mesh_vertices"], "mesh_faces": st["mesh_faces"],
                     "mesh_cells": st["mesh_cells"], "grows": st["grows"], "meshing_ok": st["meshing_ok"],
@@ -450,106 +519,154 @@ def _cpu_impl():
     return "port", None
 
 
-def cpu_baseline(depth, bgr, seq, a) -> dict:
-    """The reference on one core over a bounded prefix of the same steps."""
-    kind, ref = _cpu_impl()
-    steps_max = a.warmup + a.steps
-    hd = depth.cpu().numpy().view(np.uint16)
-    hb = bgr.cpu().numpy()
-    if kind == "reference":
-        m = ref.RefFusion(VOXEL, THRESHOLD, True)
-        add = lambda k: m.add_map(hd[k], hb[k], seq.K, *seq.poses[k], SCALING, MAXCAM)
-        upd = m.update_meshes
-    else:
-        from oracle.port import PortFusion
-        m = PortFusion(update_mode=2)
-        add = lambda k: m.add_map(hd[k], hb[k], seq.K, *seq.poses[k], SCALING, MAXCAM)
-        upd = m.update_meshes
-    t0 = time.perf_counter()
-    steps = 0
-    while steps < steps_max and time.perf_counter() - t0 < CPU_SAMPLE_SECONDS:
-        for k in range(steps * FRAMES_PER_STEP, (steps + 1) * FRAMES_PER_STEP):
-            add(k)
-        upd()
-        m.mesh()
-        steps += 1
-    el = time.perf_counter() - t0
-    if kind == "reference":
-        m.close()
-    return {"value": round(steps * FRAMES_PER_STEP / el, 3), "unit": UNIT, "cores": 1, "kind": kind,
-            "sample": f"first {steps} steps ({steps * FRAMES_PER_STEP} frames, {steps} updateMeshes and mesh copies) of the "
-                      f"same walk on one host core, {el:.1f} s"}
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
-# -- the reference arm ------------------------------------------------------------
+def _save_frames(depth, bgr):
+    tmp = tempfile.mkdtemp(prefix="ffref_")
+    dpath, bpath = os.path.join(tmp, "depth.npy"), os.path.join(tmp, "bgr.npy")
+    np.save(dpath, depth.cpu().numpy().view(np.uint16))
+    np.save(bpath, bgr.cpu().numpy())
+    return tmp, dpath, bpath
+
+
+def _drop_frames(tmp, dpath, bpath):
+    for f in (dpath, bpath):
+        os.unlink(f)
+    os.rmdir(tmp)
+
+
 def _ref_worker(args):
-    (idx, dpath, bpath, K, poses, warmup, steps, barrier, q) = args
+    """One map of the reference (or the restatement where the reference is
+    not built) pinned to `cores`, running the whole walk: W warm-up steps,
+    then every step, the timed ones measured with the wall clock.  Puts
+    (index, seconds of the timed steps) on the queue."""
+    (idx, cores, dpath, bpath, K, poses, warmup, total, timed, thread_meshing, barrier, q) = args
     import numpy as np  # noqa: F811
+    if cores:
+        os.sched_setaffinity(0, cores)
     from oracle import ref as refmod
     hd = np.load(dpath, mmap_mode="r")
     hb = np.load(bpath, mmap_mode="r")
     if refmod.available():
         m = refmod.RefFusion(VOXEL, THRESHOLD, True)
+        if thread_meshing:
+            m.set_thread_meshing(True)
         add = lambda k: m.add_map(np.asarray(hd[k]), np.asarray(hb[k]), K, *poses[k], SCALING, MAXCAM)
     else:
         from oracle.port import PortFusion
         m = PortFusion(update_mode=2)
         add = lambda k: m.add_map(np.asarray(hd[k]), np.asarray(hb[k]), K, *poses[k], SCALING, MAXCAM)
+
     # a step: 10 addMap, updateMeshes, and the mesh copied out
     # (getMeshInterleavedMarchingCubes returns the reference's mesh by value)
+    def step(s):
+        for k in range(s * FRAMES_PER_STEP, (s + 1) * FRAMES_PER_STEP):
+            add(k)
+        m.update_meshes()
+        m.mesh()
+
     for s in range(warmup):
-        for k in range(s * FRAMES_PER_STEP, (s + 1) * FRAMES_PER_STEP):
-            add(k)
-        m.update_meshes()
-        m.mesh()
-    barrier.wait()
-    t0 = time.perf_counter()
-    for s in range(warmup, warmup + steps):
-        for k in range(s * FRAMES_PER_STEP, (s + 1) * FRAMES_PER_STEP):
-            add(k)
-        m.update_meshes()
-        m.mesh()
-    q.put((idx, time.perf_counter() - t0))
+        step(s)
+    timed = set(timed)
+    if barrier is not None:
+        barrier.wait()
+    secs = 0.0
+    for s in range(warmup, total):
+        if s in timed:
+            t0 = time.perf_counter()
+            step(s)
+            secs += time.perf_counter() - t0
+        else:
+            step(s)
+    q.put((idx, secs))
+    if thread_meshing:
+        # the reference's destructor frees its mesh cells' meshes before it
+        # joins a mesher thread that may still run (geometryfusion_mipmap_cpu.cpp
+        # :754 before :966): leave the object to the process exit
+        os._exit(0)
 
 
+def _run_workers(jobs, with_barrier: bool):
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(len(jobs)) if with_barrier else None
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_ref_worker, args=(j[:10] + (barrier, q),)) for j in jobs]
+    for pr in procs:
+        pr.start()
+    out = [q.get() for _ in procs]
+    for pr in procs:
+        pr.join()
+    return [t for _, t in sorted(out)]
+
+
+def cpu_baseline(depth, bgr, seq, a) -> dict:
+    """The reference on one pinned host core over the same walk and the same
+    timed steps: CPU_RUNS runs at once, each on its own core, the median
+    reported; plus one run with the reference's threaded meshing on two
+    cores."""
+    kind, _ = _cpu_impl()
+    total, timed = step_plan(a)
+    nf = total * FRAMES_PER_STEP
+    tmp, dpath, bpath = _save_frames(depth, bgr)
+    avail = sorted(os.sched_getaffinity(0))
+    runs = min(CPU_RUNS, len(avail))
+    jobs = [(i, {avail[i]}, dpath, bpath, seq.K, seq.poses[:nf], a.warmup, total, timed, False)
+            for i in range(runs)]
+    secs = _run_workers(jobs, with_barrier=False)
+    threaded = None
+    if kind == "reference" and len(avail) >= 2:
+        tsecs = _run_workers([(0, set(avail[:2]), dpath, bpath, seq.K, seq.poses[:nf], a.warmup, total, timed,
+                               True)], with_barrier=False)
+        threaded = {"value": round(a.steps * FRAMES_PER_STEP / tsecs[0], 3), "unit": UNIT, "cores": 2,
+                    "note": "setThreadMeshing(true): meshing on a second thread, updateMeshes returning false "
+                            "while it runs (the mesh copied each step is the last finished one)"}
+    _drop_frames(tmp, dpath, bpath)
+    med = float(np.median(secs))
+    return {"value": round(a.steps * FRAMES_PER_STEP / med, 3), "unit": UNIT, "cores": 1, "kind": kind,
+            "runs": [round(a.steps * FRAMES_PER_STEP / t, 3) for t in secs], "statistic": f"median of {runs}",
+            "cpu_model": cpu_model(), "host_cores": os.cpu_count(), "pinned": "one core per run (sched_setaffinity)",
+            "sample": f"the whole walk ({nf} frames) on one core per run, {a.warmup} warm-up steps, the same "
+                      f"{a.steps} timed steps (10 addMap + updateMeshes + mesh copy each); setThreadMeshing(false)",
+            "threaded_meshing": threaded}
+
+
+# -- the reference arm ------------------------------------------------------------
 def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    import multiprocessing as mp
     import torch
     kind, _ = _cpu_impl()
-    nf = n_frames_needed(a)
+    total, timed = step_plan(a)
+    nf = total * FRAMES_PER_STEP
     seq = make_sequence(a.seed, nf)
     device = "cuda" if torch.cuda.is_available() else "cpu"
     depth, bgr = render_frames(seq, nf, device)
-    tmp = tempfile.mkdtemp(prefix="ffref_")
-    dpath, bpath = os.path.join(tmp, "depth.npy"), os.path.join(tmp, "bgr.npy")
-    np.save(dpath, depth.cpu().numpy().view(np.uint16))
-    np.save(bpath, bgr.cpu().numpy())
+    tmp, dpath, bpath = _save_frames(depth, bgr)
     del depth, bgr
-    cores = len(os.sched_getaffinity(0))
+    avail = sorted(os.sched_getaffinity(0))
     try:
         import psutil
         mem_maps = int(psutil.virtual_memory().available // (3 << 30))
     except ImportError:
-        mem_maps = cores
-    workers = a.workers or max(1, min(cores, mem_maps))
-    ctx = mp.get_context("spawn")
-    barrier = ctx.Barrier(workers)
-    q = ctx.Queue()
-    procs = [ctx.Process(target=_ref_worker, args=((i, dpath, bpath, seq.K, seq.poses[:nf], a.warmup, a.steps,
-                                                    barrier, q),)) for i in range(workers)]
-    for p in procs:
-        p.start()
-    times = [q.get() for _ in procs]
-    for p in procs:
-        p.join()
-    for f in (dpath, bpath):
-        os.unlink(f)
-    os.rmdir(tmp)
-    wall = max(t for _, t in times)
+        mem_maps = len(avail)
+    workers = a.workers or max(1, min(len(avail), mem_maps))
+    jobs = [(i, {avail[i % len(avail)]}, dpath, bpath, seq.K, seq.poses[:nf], a.warmup, total, timed, False)
+            for i in range(workers)]
+    secs = _run_workers(jobs, with_barrier=True)
+    _drop_frames(tmp, dpath, bpath)
+    wall = max(secs)
     value = workers * a.steps * FRAMES_PER_STEP / wall
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
@@ -558,8 +675,9 @@ def run_reference(a):
         "data": "synthetic: same frames as the B200 arm",
         "config": dict(workload_config(a, nf), parallelism=f"{workers} independent maps on {workers} host cores"),
         "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": workers, "kind": kind,
-                         "sample": f"{workers} maps in parallel, each {a.steps} timed steps after {a.warmup} "
-                                   f"warm-up steps of the walk"},
+                         "cpu_model": cpu_model(),
+                         "sample": f"{workers} maps in parallel, each pinned to its own core and running the whole "
+                                   f"walk; the same {a.steps} timed steps after {a.warmup} warm-up steps"},
         "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -576,7 +694,7 @@ def run_batch(a):
     from fastfusion_b200.scene import batch_sequences, render_torch
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    nf = n_frames_needed(a)
+    nf = (a.warmup + a.steps) * FRAMES_PER_STEP
     seqs = batch_sequences(a.maps, n_frames=nf)
     frames = []
     for seq, _ in seqs:
@@ -671,7 +789,7 @@ def run_corridor(a):
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
-    nf = n_frames_needed(a)
+    nf = (a.warmup + a.steps) * FRAMES_PER_STEP
     W, H = 1280, 960
     stride = a.stride if a.stride > 0 else max(1, 10000 // nf)
     seq = corridor_sequence(a.seed, n_frames=10000, width=W, height=H)

@@ -29,7 +29,7 @@ class FusionMipMapCPU {
    * (geometryfusion_mipmap_cpu.cpp:420-640; the reference ignores the
    * offsets and n as well). */
   FusionMipMapCPU(float offsetX, float offsetY, float offsetZ, float scale, float distanceThreshold,
-                  unsigned int n = 0, bool color = true)
+                  sidetype n = 0, bool color = true)
       : h_(0) {
     (void)offsetX;
     (void)offsetY;

@@ -121,8 +121,8 @@ __device__ __forceinline__ int4 project_point(float d, float px, float py, const
 // boundary bits and repeat until no boundary changes; a chain of dependencies
 // crosses at most tilesX+tilesY tiles, which bounds the number of rounds.
 
-__device__ __forceinline__ void grid_barrier(uint32_t *bar, uint32_t nblocks, Counters *cnt) {
-  grid_barrier_bounded(bar, nblocks, &cnt->error, ERR_SPIN_TIMEOUT);
+__device__ __forceinline__ void grid_barrier(uint32_t *bar, uint32_t nblocks, Counters *cnt, uint32_t limit) {
+  grid_barrier_bounded(bar, nblocks, &cnt->error, ERR_DEDUPE_TIMEOUT, limit);
 }
 
 constexpr int DD_WARPS = 4;  // tiles (warps) per block
@@ -282,13 +282,13 @@ __device__ __forceinline__ void dedupe_body(const BatchDesc *__restrict__ bd, in
     // counter (round + 1) % 3 was last read before the previous barrier
     if (blockIdx.x == 0 && threadIdx.x == 0) chg[(round + 1) % 3] = 0;
     // a barrier that gives up marks the first map; every map's frame reports it
-    grid_barrier(bar, gridDim.x, bd->f[m0].cnt);
+    grid_barrier(bar, gridDim.x, bd->f[m0].cnt, bd->f[m0].spin_limit);
     const uint32_t any = chg[round % 3];
     if (!any) {
       converged = true;
       break;
     }
-    if (*(volatile uint32_t *)&bd->f[m0].cnt->error & ERR_SPIN_TIMEOUT) break;
+    if (*(volatile uint32_t *)&bd->f[m0].cnt->error & ERR_DEDUPE_TIMEOUT) break;
   }
   // leave the barrier words as the next launch needs them: the arrival count
   // is zero after every completed barrier, counter (round + 1) % 3 was zeroed
@@ -303,7 +303,7 @@ __device__ __forceinline__ void dedupe_body(const BatchDesc *__restrict__ bd, in
     Counters *c = bd->f[m0 + threadIdx.x].cnt;
     c->dedupe_iters = round + 1;
     if (!converged) atomicOr(&c->error, ERR_DEDUPE_NOT_CONVERGED);
-    if (*(volatile uint32_t *)&bd->f[m0].cnt->error & ERR_SPIN_TIMEOUT) atomicOr(&c->error, ERR_SPIN_TIMEOUT);
+    if (*(volatile uint32_t *)&bd->f[m0].cnt->error & ERR_DEDUPE_TIMEOUT) atomicOr(&c->error, ERR_DEDUPE_TIMEOUT);
   }
 }
 
@@ -415,10 +415,10 @@ __device__ __forceinline__ void queue_leaf(uint32_t leaf, uint32_t frame, uint32
 
 // Wait until another thread finished allocating tree[ptr]; bounded.
 __device__ __forceinline__ uint32_t wait_unlocked(uint32_t *tree, uint32_t ptr, uint32_t cur, Counters *cnt,
-                                                  bool *ok) {
-  int spins = 0;
+                                                  bool *ok, uint32_t limit) {
+  uint32_t spins = 0;
   while (cur == LOCKED) {
-    if (++spins > SPIN_LIMIT) {
+    if (spins++ >= limit) {
       atomicOr(&cnt->error, ERR_SPIN_TIMEOUT);
       *ok = false;
       return cur;
@@ -445,22 +445,11 @@ __device__ __forceinline__ bool owns_brick(const MapFrame &F, uint32_t ox, uint3
   return hsh % F.shards == F.shard;
 }
 
-// One processed pixel: bounding-box growth, then (inside the volume) the
-// descent of queryPointDepthSingle_func_subtree: queue the existing coarser
-// leaves on the path, allocate missing branches, claim the final leaf.
-// One thread per pixel of every frame of the batch (each map's pixels padded
-// to whole warps, so a warp never spans two maps).
-__global__ void k_insert(const BatchDesc *__restrict__ bd) {
-  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nmaps = bd->n;
-  if (g >= bd->pix_end[nmaps - 1]) return;
-  int mi = 0;
-  while (mi < nmaps - 1 && g >= bd->pix_end[mi]) mi++;
-  const MapFrame &F = bd->f[mi];
-  const int i = (int)(g - (mi ? bd->pix_end[mi - 1] : 0u));
-  const int npix = (int)F.npix;
-  const int4 *__restrict__ vox = F.vox;
-  const uint8_t *__restrict__ processed = F.proc;
+// One processed pixel of the frame F (voxel key v): bounding-box growth,
+// then (inside the volume) the descent of queryPointDepthSingle_func_subtree:
+// queue the existing coarser leaves on the path, allocate missing branches,
+// claim the final leaf.  Returns the number of octree levels probed.
+__device__ __forceinline__ uint32_t insert_pixel(const MapFrame &F, int i, int4 v, Counters *cnt) {
   const uint32_t n = F.n;
   const int bw = (int)F.bw;
   uint32_t *tree = F.tree;
@@ -468,12 +457,7 @@ __global__ void k_insert(const BatchDesc *__restrict__ bd) {
   uint32_t *stamp = F.stamp, *queue = F.queue;
   PendingLeaf *pend = F.pend;
   const uint32_t pend_cap = F.pend_cap;
-  Counters *cnt = F.cnt;
-  bool act = i < npix && processed[i];
-  unsigned m = __ballot_sync(0xffffffffu, act);
-  if (!act) return;
-  if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&cnt->processed, __popc(m));
-  int4 v = vox[i];
+  uint32_t probed = 0;
   int vv[3] = {v.x, v.y, v.z};
 #pragma unroll
   for (int r = 0; r < 3; r++) {
@@ -481,7 +465,7 @@ __global__ void k_insert(const BatchDesc *__restrict__ bd) {
     if (lo < 0) atomicMin(&cnt->box_min[r], lo);
     if (hi >= (int)n) atomicMax(&cnt->box_max[r], hi);
   }
-  if (!(v.x >= 0 && (uint16_t)v.x < n && v.y >= 0 && (uint16_t)v.y < n && v.z >= 0 && (uint16_t)v.z < n)) return;
+  if (!(v.x >= 0 && (uint16_t)v.x < n && v.y >= 0 && (uint16_t)v.y < n && v.z >= 0 && (uint16_t)v.z < n)) return 0;
   const uint32_t x = (uint16_t)v.x, y = (uint16_t)v.y, z = (uint16_t)v.z;
   const uint32_t target = (uint32_t)v.w;
   // sharded map: the pixel's own brick (the level the descent stops at) is
@@ -498,20 +482,21 @@ __global__ void k_insert(const BatchDesc *__restrict__ bd) {
   uint32_t branch = 0;
   bool ok = true;
   while ((half >> 1) >= target) {
+    probed++;
     uint32_t co = (x >= ox + half) * 1u + (y >= oy + half) * 2u + (z >= oz + half) * 4u;
     uint32_t ptr = branch + co + 8;
     uint32_t leaf = ld_tree(tree + ptr - 8);
     if (leaf < leaves_max) queue_leaf(leaf, frame, stamp, queue, cnt);
     uint32_t child = ld_tree(tree + ptr);
     if (child == BRANCHINIT) {
-      if (!owned) return;
+      if (!owned) return probed;
       uint32_t old = atomicCAS(tree + ptr, BRANCHINIT, LOCKED);
       if (old == BRANCHINIT) {
         uint32_t nb = atomicAdd(&cnt->branches_used, 16u);
         if (nb + 16 > branches_max) {
           atomicOr(&cnt->error, ERR_BRANCH_OVERFLOW);
           atomicExch(tree + ptr, BRANCHINIT);
-          return;
+          return probed;
         }
         __threadfence();
         atomicExch(tree + ptr, nb);
@@ -520,8 +505,8 @@ __global__ void k_insert(const BatchDesc *__restrict__ bd) {
         child = old;
       }
     }
-    child = wait_unlocked(tree, ptr, child, cnt, &ok);
-    if (!ok || child == BRANCHINIT) return;
+    child = wait_unlocked(tree, ptr, child, cnt, &ok, F.spin_limit);
+    if (!ok || child == BRANCHINIT) return probed;
     ox += half * ((co & 1) != 0);
     oy += half * ((co & 2) != 0);
     oz += half * ((co & 4) != 0);
@@ -530,16 +515,17 @@ __global__ void k_insert(const BatchDesc *__restrict__ bd) {
   }
   uint32_t co = (x >= ox + half) * 1u + (y >= oy + half) * 2u + (z >= oz + half) * 4u;
   uint32_t ptr = branch + co;
+  probed++;
   uint32_t cur = ld_tree(tree + ptr);
   if (cur == BRANCHINIT) {
-    if (!owned) return;
+    if (!owned) return probed;
     uint32_t old = atomicCAS(tree + ptr, BRANCHINIT, LOCKED);
     if (old == BRANCHINIT) {
       uint32_t rec = atomicAdd(&cnt->pending, 1u);
       if (rec >= pend_cap) {
         atomicOr(&cnt->error, ERR_PENDING_OVERFLOW);
         atomicExch(tree + ptr, BRANCHINIT);
-        return;
+        return probed;
       }
       PendingLeaf pl;
       pl.slot = ptr;
@@ -549,17 +535,46 @@ __global__ void k_insert(const BatchDesc *__restrict__ bd) {
       pend[rec] = pl;
       __threadfence();
       atomicExch(tree + ptr, PENDING + rec);
-      return;
+      return probed;
     }
     cur = old;
   }
-  cur = wait_unlocked(tree, ptr, cur, cnt, &ok);
-  if (!ok) return;
+  cur = wait_unlocked(tree, ptr, cur, cnt, &ok, F.spin_limit);
+  if (!ok) return probed;
   if (cur >= PENDING && cur < PENDING + pend_cap) {
     atomicMin(&pend[cur - PENDING].first_pixel, (uint32_t)i);
   } else if (cur < leaves_max) {
     queue_leaf(cur, frame, stamp, queue, cnt);
   }
+  return probed;
+}
+
+// One thread per pixel of every frame of the batch (each map's pixels padded
+// to whole warps, so a warp never spans two maps).
+__global__ void k_insert(const BatchDesc *__restrict__ bd) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nmaps = bd->n;
+  if (g >= bd->pix_end[nmaps - 1]) return;
+  int mi = 0;
+  while (mi < nmaps - 1 && g >= bd->pix_end[mi]) mi++;
+  const MapFrame &F = bd->f[mi];
+  const int i = (int)(g - (mi ? bd->pix_end[mi - 1] : 0u));
+  const int npix = (int)F.npix;
+  const int4 *__restrict__ vox = F.vox;
+  const uint8_t *__restrict__ processed = F.proc;
+  Counters *cnt = F.cnt;
+  // a de-duplication that did not complete leaves the frame out: the octree
+  // is not touched, so the map stays as it was
+  if (ld_volatile(&cnt->error) & ERR_DEDUPE_FAILED) return;
+  bool act = i < npix && processed[i];
+  unsigned m = __ballot_sync(0xffffffffu, act);
+  if (!act) return;
+  if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&cnt->processed, __popc(m));
+  // octree entries this pixel reads on its descent (the algorithmic bytes of
+  // the insert: 16 B per level probed), summed per warp
+  const uint32_t levels = insert_pixel(F, i, vox[i], cnt);
+  const uint32_t sum = __reduce_add_sync(m, levels);
+  if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&cnt->levels, sum);
 }
 
 void launch_insert(const BatchDesc *d_batch, uint32_t total_pix, cudaStream_t s, int block) {
@@ -670,7 +685,11 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc
   extern __shared__ uint32_t fin_smem[];
   const MapFrame &F = bd->f[blockIdx.x];
   Counters *cnt = F.cnt;
-  if (cnt->error & (ERR_SPIN_TIMEOUT | ERR_DEDUPE_NOT_CONVERGED | ERR_PENDING_OVERFLOW)) return;
+  // After a de-duplication error nothing was inserted.  After an insert whose
+  // wait gave up (ERR_SPIN_TIMEOUT) the pending leaves recorded before it are
+  // complete records and are placed, so that no octree slot keeps a pending
+  // mark; the frame's update is skipped (ERR_FRAME_FAILED).
+  if (cnt->error & (ERR_DEDUPE_FAILED | ERR_PENDING_OVERFLOW)) return;
   const int npend = (int)cnt->pending;
   const PendingLeaf *pend = F.pend;
   const uint32_t npix = F.npix, leaves_before = F.leaves_before, leaves_max = F.leaves_max, frame = F.frame;

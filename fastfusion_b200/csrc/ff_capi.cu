@@ -120,6 +120,13 @@ struct ff_handle {
   size_t conf_cap = 0;  // pixels the buffers hold
   int conf_w = 0, conf_h = 0;  // size of the last confidence map
 
+  // iterations after which a device-side wait gives up (ff_set_spin_limit),
+  // and a failure the next frame reports as if a device wait had given up
+  // (ff_inject_error)
+  uint32_t spin_limit = SPIN_LIMIT;
+  int inject = 0;
+  int pi_insert = -1;  // profile record of the last insert launch this map led
+
   // brick ownership (ff_set_shard) and the voxels grow() has moved the grid by
   uint32_t shard = 0, shards = 1;
   int32_t shift[3] = {0, 0, 0};
@@ -561,6 +568,20 @@ ff_status ff_set_shard(ff_handle *h, int shard, int shards) {
   return FF_OK;
 }
 
+ff_status ff_set_spin_limit(ff_handle *h, uint32_t iterations) {
+  if (!h) return FF_ERR_BAD_ARG;
+  h->spin_limit = iterations;
+  return FF_OK;
+}
+
+ff_status ff_inject_error(ff_handle *h, int what) {
+  if (!h) return FF_ERR_BAD_ARG;
+  if (what != 0 && what != FF_INJECT_CONFIDENCE_TIMEOUT)
+    return set_err(h, FF_ERR_BAD_ARG, "ff_inject_error: unknown failure");
+  h->inject = what;
+  return FF_OK;
+}
+
 ff_status ff_set_tuning(ff_handle *h, const ff_tuning *t) {
   if (!h || !t) return FF_ERR_BAD_ARG;
   if ((t->dedupe_rows && t->dedupe_rows != 8 && t->dedupe_rows != 16 && t->dedupe_rows != 32) || t->fuse_shape < 0 ||
@@ -718,6 +739,7 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
   mf.conf = nullptr;
   mf.shard = h->shard;
   mf.shards = h->shards;
+  mf.spin_limit = h->spin_limit;
   for (int r = 0; r < 3; r++) mf.shift[r] = h->shift[r];
   if (h->conf_tau_cm > 0.0f) {
     // the frame's confidence map, ahead of the launches that read it on this stream
@@ -753,6 +775,11 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
     CK(cnn_forward(h->d_cnn_params, h->d_cnn_packed, h->cnn_packed_ready, h->d_feat, 1, W, H, h->d_a1, h->d_a2,
                    h->d_conf, h->conf_tau_cm, &h->d_cnt->cnn_error, cs));
     h->cnn_packed_ready = true;
+    if (h->inject == FF_INJECT_CONFIDENCE_TIMEOUT) {
+      // the word the network sets when one of its waits gives up
+      CK(cudaMemsetAsync(&h->d_cnt->cnn_error, 0xFF, sizeof(uint32_t), cs));
+      h->inject = 0;
+    }
     // depth -> features -> a1 -> a2 -> confidence, each written once and read once
     h->prof.end(pc, (double)npx * ((2 + 16) + (16 + 32) + (32 + 32) + (32 + 4)), cs);
     if (cs != s) {
@@ -762,6 +789,12 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
     h->conf_w = W;
     h->conf_h = H;
     mf.conf = h->d_conf;
+  }
+  if (h->inject == FF_INJECT_CONFIDENCE_TIMEOUT) {
+    // no network this frame: the word is set all the same (the frame's
+    // counter set-up keeps it; the update and the host read it)
+    CK(cudaMemsetAsync(&h->d_cnt->cnn_error, 0xFF, sizeof(uint32_t), s));
+    h->inject = 0;
   }
   return FF_OK;
 }
@@ -854,7 +887,7 @@ static ff_status frame_issue(ff_handle *lead, int n, const LaunchPlan &lp) {
     for (size_t g = 0; g < lp.groups.size(); g++)
       CK(launch_dedupe(lead->d_batch, (int)lp.groups[g][0], (int)lp.groups[g][1], lp.groups[g][2], lp.rows,
                        lead->d_barrier + 8 * g, lead->cfg.device, s));
-  lead->prof.end(pi, lp.npix * (2 + 16 + 1), s);  // depth in; voxel keys and processed flags out
+  lead->prof.end(pi, lp.npix * 2, s);  // the depth image read (the keys and flags it writes stay in L2)
   if (lead->fin_pending) {
     // the previous frame's finalisation (on fuse_stream) completes the octree
     CK(cudaStreamWaitEvent(s, lead->ev_fin, 0));
@@ -862,7 +895,9 @@ static ff_status frame_issue(ff_handle *lead, int n, const LaunchPlan &lp) {
   }
   pi = lead->prof.begin(ST_INSERT, s);
   launch_insert(lead->d_batch, lp.pix, s, lead->tune.insert_block > 0 ? lead->tune.insert_block : 256);
-  lead->prof.end(pi, lp.npix * (16 + 1), s);  // keys and flags in (tree walks counted below)
+  // 16 B per octree level probed, counted on the device (set after the frame)
+  lead->prof.end(pi, 0.0, s);
+  lead->pi_insert = pi;
   CK(cudaGetLastError());
   return FF_OK;
 }
@@ -926,17 +961,30 @@ static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf,
                               int32_t *queued) {
   cudaStream_t s = h->stream;
   const Counters &hc = *h->h_cnt;
-  if (hc.cnn_error) {
-    // (the word is kept across frames until cleared here)
-    CK(cudaMemsetAsync(&h->d_cnt->cnn_error, 0, sizeof(uint32_t), h->stream));
-    return set_err(h, FF_ERR_TIMEOUT, "a bounded device-side wait gave up in the confidence network");
-  }
-  if (hc.error & (ERR_SPIN_TIMEOUT | ERR_DEDUPE_NOT_CONVERGED)) {
+  if (hc.error & ERR_DEDUPE_FAILED) {
+    // the insert, the finalisation and the update left the frame out: the
+    // map is as it was before the call
     h->barrier_dirty = true;
-    return set_err(h, FF_ERR_TIMEOUT, "a bounded device-side wait gave up during allocation");
+    if (hc.cnn_error) {
+      CK(join_fuse(h));
+      CK(cudaStreamSynchronize(s));
+      CK(cudaMemsetAsync(&h->d_cnt->cnn_error, 0, sizeof(uint32_t), s));
+      CK(cudaStreamSynchronize(s));
+    }
+    return set_err(h, FF_ERR_TIMEOUT,
+                   (hc.error & ERR_DEDUPE_TIMEOUT)
+                       ? "a bounded device-side wait gave up in the de-duplication; the frame was not fused"
+                       : "the de-duplication did not settle within its round limit; the frame was not fused");
   }
   if (hc.error & ERR_PENDING_OVERFLOW) return set_err(h, FF_ERR_STATE, "pending-leaf buffer overflow");
   if (hc.error & ERR_BRANCH_OVERFLOW) h->meshing_ok = false;
+  // A wait of the octree insert or of the confidence network that gave up:
+  // the frame's new bricks are placed (the octree stays consistent) and the
+  // bookkeeping below is done, but its voxel update is skipped (on the device
+  // as well); the call then reports FF_ERR_TIMEOUT.
+  const bool insert_timeout = (hc.error & ERR_SPIN_TIMEOUT) != 0;
+  const bool cnn_failed = hc.cnn_error != 0;
+  const bool skip_update = insert_timeout || cnn_failed;
   const uint32_t leaves_before = plan.leaves_before;
   const int W = plan.W, H = plan.H;
   h->branches_used = std::min(hc.branches_used, h->cfg.branches_max);
@@ -959,10 +1007,11 @@ static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf,
     launch_parents((int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->n, h->d_leaf, h->d_parent, s);
     h->prof.end(pi_fin, 0.0, s);
   }
-  h->prof.set_bytes(pi_fin, (double)npend * (sizeof(PendingLeaf) + 8 + 4));
+  h->prof.set_bytes(pi_fin, (double)npend * 8);  // 8 B per new brick
+  if (h->pi_insert >= 0) h->prof.set_bytes(h->pi_insert, 16.0 * hc.levels);
   h->leaves_used += npend;
   h->new_leaves = npend;
-  bool fuse_now = !plan.one_sync;
+  bool fuse_now = !plan.one_sync && !skip_update;
   if (h->leaves_used < h->cfg.leaves_max && h->branches_used < h->cfg.branches_max &&
       (hc.box_min[0] < 0 || hc.box_min[1] < 0 || hc.box_min[2] < 0 || hc.box_max[0] >= (int)h->n ||
        hc.box_max[1] >= (int)h->n || hc.box_max[2] >= (int)h->n)) {
@@ -974,7 +1023,7 @@ static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf,
     ff_status st = grow(h, hc.box_min, hc.box_max);
     h->prof.end(pi, tree_bytes, s);  // octree and leaf positions read and written
     if (st != FF_OK) return st;
-    fuse_now = true;
+    fuse_now = !skip_update;
   }
   // fuse: every voxel of every queued brick read and written: SDF, weight
   // (4+4 B, or 2+2 B in FP16) and three 16-bit colour channels
@@ -1003,6 +1052,21 @@ static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf,
   h->frames++;
   mesh_note_frame(h->mesh);
   if (queued) *queued = (int32_t)nq;
+  if (cnn_failed) {
+    // the word is kept across frames: clear it once every kernel of the
+    // frame that reads it has run
+    CK(join_fuse(h));
+    CK(cudaStreamSynchronize(s));
+    CK(cudaMemsetAsync(&h->d_cnt->cnn_error, 0, sizeof(uint32_t), s));
+    CK(cudaStreamSynchronize(s));
+    return set_err(h, FF_ERR_TIMEOUT,
+                   "a bounded device-side wait gave up in the confidence network; the frame's bricks were "
+                   "allocated but not updated");
+  }
+  if (insert_timeout)
+    return set_err(h, FF_ERR_TIMEOUT,
+                   "a bounded device-side wait gave up in the octree insert; the frame's bricks found so far "
+                   "were allocated but not updated");
   return FF_OK;
 }
 
@@ -1207,12 +1271,17 @@ ff_status ff_add_maps_u16_device(ff_handle *const *maps, int n, const uint16_t *
   }
   CK(cudaStreamSynchronize(lead->stream));
   double bricks = 0, pending = 0;
+  // every map's frame is finished, also after another map's failure (each
+  // map's own state must match what ran on the device); the first failure is
+  // reported
+  ff_status first = FF_OK;
+  std::string first_err;
   for (int i = 0; i < n; i++) {
     st = frame_finish(maps[i], plan[i], mf[i], i == 0 ? pi_fin : -1, i == 0 ? pi_fuse : -1,
                       queued ? queued + i : nullptr);
-    if (st != FF_OK) {
-      lead->barrier_dirty = true;  // (the batch ran on the lead's barrier words)
-      return st;
+    if (st != FF_OK && first == FF_OK) {
+      first = st;
+      first_err = "map " + std::to_string(i) + ": " + maps[i]->err;
     }
     bricks += maps[i]->queued;
     pending += maps[i]->new_leaves;
@@ -1220,7 +1289,14 @@ ff_status ff_add_maps_u16_device(ff_handle *const *maps, int n, const uint16_t *
   // the lead's profile holds the batch's launches: count every map's work
   const double brick_bytes = 512.0 * 2 * ((lead->cfg.storage == FF_STORAGE_FP16 ? 4 : 8) + 6);
   lead->prof.set_bytes(pi_fuse, bricks * brick_bytes);
-  lead->prof.set_bytes(pi_fin, pending * (sizeof(PendingLeaf) + 8 + 4));
+  lead->prof.set_bytes(pi_fin, pending * 8);
+  double levels = 0;
+  for (int i = 0; i < n; i++) levels += maps[i]->h_cnt->levels;
+  if (lead->pi_insert >= 0) lead->prof.set_bytes(lead->pi_insert, 16.0 * levels);
+  if (first != FF_OK) {
+    lead->barrier_dirty = true;  // (the batch ran on the lead's barrier words)
+    return set_err(lead, first, first_err);
+  }
   return FF_OK;
 }
 

@@ -499,8 +499,20 @@ __global__ void __launch_bounds__(128) k_conv_tc(const __grid_constant__ CUtenso
       }
     }
   };
-  epilogue(0, TC_ROWS / 2, wait_bar(mbar));
-  epilogue(TC_ROWS / 2, TC_ROWS, wait_bar(mbar + 1));
+  const uint32_t done0 = wait_bar(mbar);
+  epilogue(0, TC_ROWS / 2, done0);
+  const uint32_t done1 = wait_bar(mbar + 1);
+  epilogue(TC_ROWS / 2, TC_ROWS, done1);
+  // A wait that gave up may leave the tile copies or the MMAs in flight,
+  // writing this block's shared and tensor memory: wait for them once more
+  // (bounded again) before both are given back.  If that wait gives up too,
+  // the frame is already reported failed and its confidence map is not used.
+  if (!loaded) {
+    mbar_wait(ld_bar, 0);
+  } else {
+    if (!done0) mbar_wait(smem_addr(mbar), 0);
+    if (!done1) mbar_wait(smem_addr(mbar + 1), 0);
+  }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)

@@ -31,7 +31,9 @@ constexpr int BL = 8;                         // BRICKLENGTH
 constexpr float DIST_W_EPS = 0.005f;          // DISTANCEWEIGHTEPSILON
 constexpr float WEIGHT_FACTOR = 3.0f;
 constexpr float COLOR_MUL = 256.0f;
-constexpr int SPIN_LIMIT = 1 << 22;           // bound of every device-side wait
+// default bound of every device-side wait (iterations); a map can set its
+// own (ff_set_spin_limit), down to 0: a wait then gives up at once
+constexpr uint32_t SPIN_LIMIT = 1u << 22;
 
 // error bits written by kernels into Counters::error
 enum : uint32_t {
@@ -42,7 +44,16 @@ enum : uint32_t {
   ERR_MESH_OVERFLOW = 16u,
   ERR_DEDUPE_NOT_CONVERGED = 32u,
   ERR_CELL_KEY = 64u,  // a mesh cell's origin does not fit its sort key
+  ERR_DEDUPE_TIMEOUT = 128u,  // a grid barrier of the de-duplication gave up (nothing was inserted)
 };
+
+// Error bits after which a frame's voxel update is skipped: its allocation
+// did not complete as the reference's would have.
+constexpr uint32_t ERR_FRAME_FAILED = ERR_SPIN_TIMEOUT | ERR_DEDUPE_NOT_CONVERGED | ERR_DEDUPE_TIMEOUT |
+                                      ERR_PENDING_OVERFLOW;
+// Error bits of the de-duplication: the insert, the leaf finalisation and the
+// update leave such a frame out entirely, so the map stays as it was.
+constexpr uint32_t ERR_DEDUPE_FAILED = ERR_DEDUPE_NOT_CONVERGED | ERR_DEDUPE_TIMEOUT;
 
 // Per-map counters kept in device memory; read back once per frame.
 struct Counters {
@@ -61,7 +72,8 @@ struct Counters {
   uint64_t mesh_v;
   uint64_t mesh_f;
   uint32_t cnn_error;  // the confidence network's bounded waits (kept by the frame's counter set-up)
-  uint32_t pad[3];
+  uint32_t levels;     // octree levels the insert probed, summed over the processed pixels
+  uint32_t pad[2];
 };
 
 // Float camera parameters (the reference's camPamsFloat, definitions.h:71-88).
@@ -73,8 +85,10 @@ struct CamF {
 
 // Barrier over all blocks of a cooperative launch (every block resident).
 // bar[0] counts arrivals, bar[1] is the generation; both start at zero.
-// A wait that exceeds SPIN_LIMIT sets err_bit in *err and stops waiting.
-__device__ __forceinline__ void grid_barrier_bounded(uint32_t *bar, uint32_t nblocks, uint32_t *err, uint32_t err_bit) {
+// A wait that exceeds `limit` iterations sets err_bit in *err and stops
+// waiting.
+__device__ __forceinline__ void grid_barrier_bounded(uint32_t *bar, uint32_t nblocks, uint32_t *err, uint32_t err_bit,
+                                                     uint32_t limit) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile uint32_t *gen = bar + 1;
@@ -85,9 +99,9 @@ __device__ __forceinline__ void grid_barrier_bounded(uint32_t *bar, uint32_t nbl
       __threadfence();
       atomicAdd(bar + 1, 1u);
     } else {
-      int spins = 0;
+      uint32_t spins = 0;
       while (*gen == g) {
-        if (++spins > SPIN_LIMIT) {
+        if (spins++ >= limit) {
           atomicOr(err, err_bit);
           break;
         }

@@ -163,7 +163,9 @@ __device__ __forceinline__ void fuse_brick(const uint32_t brick, const ushort4 *
 // again).  Mirrors the host's test after the traversal.
 __device__ __forceinline__ bool fuse_deferred(const MapFrame &F) {
   const Counters *c = F.cnt;
-  if (c->error & (ERR_SPIN_TIMEOUT | ERR_DEDUPE_NOT_CONVERGED | ERR_PENDING_OVERFLOW)) return true;
+  // a failed allocation, or a confidence network whose wait gave up (its
+  // confidence map is not valid): the frame is not fused
+  if ((c->error & ERR_FRAME_FAILED) || c->cnn_error) return true;
   const uint32_t leaves = F.leaves_before + c->pending;
   const uint32_t branches = min(c->branches_used, F.branches_max);
   const int n = (int)F.n;

@@ -50,6 +50,8 @@ struct MapFrame {
   // the frame's counters are set up by the de-duplication launch: zero, the
   // octree's branch count, and the in-volume box [0, n - 1]
   uint32_t branches_init;
+  // iterations after which a device-side wait of this frame gives up
+  uint32_t spin_limit;
 };
 
 constexpr int BATCH_MAX = 32;

@@ -1804,25 +1804,16 @@ constexpr size_t NOALLOC_RANGES_BYTES = sizeof(int64_t) * 4 * NOALLOC_MAX_CELLS;
 constexpr size_t NOALLOC_ROWS_BYTES = sizeof(int32_t) * 14 * NOALLOC_MAX_CELLS;
 static __device__ __align__(256) unsigned char g_export_scratch[NOALLOC_RANGES_BYTES + NOALLOC_ROWS_BYTES];
 
-// The array's device address, looked up once per device with that device
-// current (in host code the symbol names a host-side stand-in, never the
-// device memory itself).
-static std::mutex g_export_scratch_mu;
-static unsigned char *g_export_scratch_dev[64] = {};
-
+// The array's device address on the current device, looked up at every call
+// with the map's device current (in host code the symbol names a host-side
+// stand-in, never the device memory itself).  The lookup is cheap, and a
+// cached address would go stale with a new primary context (after
+// cudaDeviceReset, say).
 static cudaError_t export_scratch_address(unsigned char **out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_export_scratch);
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_export_scratch_mu);
-  if (!g_export_scratch_dev[dev]) {
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_export_scratch);
-    if (e != cudaSuccess) return e;
-    g_export_scratch_dev[dev] = static_cast<unsigned char *>(p);
-  }
-  *out = g_export_scratch_dev[dev];
+  *out = static_cast<unsigned char *>(p);
   return cudaSuccess;
 }
 

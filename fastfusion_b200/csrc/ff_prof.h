@@ -58,7 +58,7 @@ struct Prof {
     cudaEventRecord(recs[idx].b, s);
   }
   void set_bytes(int idx, double nbytes) {
-    if (idx >= 0) recs[idx].bytes = nbytes;
+    if (idx >= 0 && idx < (int)recs.size()) recs[idx].bytes = nbytes;
   }
   void flush() {
     for (auto &r : recs) {

@@ -25,6 +25,8 @@ FF_OK = 0
 _STATUS = {0: "FF_OK", 1: "FF_ERR_BAD_ARG", 2: "FF_ERR_CUDA", 3: "FF_ERR_OOM_POOL", 4: "FF_ERR_OOM_MESH",
            5: "FF_ERR_TIMEOUT", 6: "FF_ERR_STATE", 7: "FF_ERR_NO_DEVICE"}
 NOALLOC_MAX_CELLS = 65536  # FF_NOALLOC_MAX_CELLS
+SPIN_LIMIT_DEFAULT = 1 << 22  # FF_SPIN_LIMIT_DEFAULT
+INJECT_CONFIDENCE_TIMEOUT = 1  # FF_INJECT_CONFIDENCE_TIMEOUT
 
 STORAGE = {"fp32": 0, "fp16": 1}
 RCP = {"host": 0, "exact": 1}
@@ -70,6 +72,8 @@ SIGNATURES = {
     "ff_sync": (_i32, [_vp]),
     "ff_set_tuning": (_i32, [_vp, ctypes.POINTER(ff_tuning)]),
     "ff_set_shard": (_i32, [_vp, _i32, _i32]),
+    "ff_set_spin_limit": (_i32, [_vp, _u32]),
+    "ff_inject_error": (_i32, [_vp, _i32]),
     "ff_add_map_u16": (_i32, [_vp, _vp, _i32, _i32, _sz, _vp, _sz, _vp, _vp, _vp, _f32, _f32, _vp]),
     "ff_add_map_u16_device": (_i32, [_vp, _vp, _vp, _i32, _i32, _vp, _vp, _vp, _f32, _f32, _vp]),
     "ff_add_maps_u16_device": (_i32, [_vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
@@ -420,6 +424,17 @@ class FusionMipMapCPU:
         """Make this map part `shard` of `shards` of a larger map (brick
         ownership by a hash of each brick's key); before the first frame."""
         self._check(self._L.ff_set_shard(self._h, int(shard), int(shards)))
+
+    def set_spin_limit(self, iterations: int = SPIN_LIMIT_DEFAULT):
+        """Bound of the device-side waits of this map's frames (polling
+        iterations; 0: a wait gives up at once and the frame reports
+        FF_ERR_TIMEOUT)."""
+        self._check(self._L.ff_set_spin_limit(self._h, int(iterations)))
+
+    def inject_error(self, what: int = INJECT_CONFIDENCE_TIMEOUT):
+        """Make the next frame report a failure as the device would (tests of
+        the error paths; 0 cancels)."""
+        self._check(self._L.ff_inject_error(self._h, int(what)))
 
     def sync(self):
         """Wait for the map's outstanding device work (the last voxel update)."""

@@ -169,6 +169,27 @@ ff_status ff_set_shard(ff_handle *h, int shard, int shards);
  * or a batch whose maps[0] it is). */
 ff_status ff_set_tuning(ff_handle *h, const ff_tuning *t);
 
+/* Bound of every device-side wait of this map's frames (the grid barriers of
+ * the de-duplication, the lock wait of the octree insert), in polling
+ * iterations; default FF_SPIN_LIMIT_DEFAULT.  A wait that runs out sets an
+ * error flag and returns instead of waiting on; the call then returns
+ * FF_ERR_TIMEOUT: after a de-duplication wait the frame is left out and the
+ * map is as it was before the call; after an insert wait the bricks found so
+ * far are allocated but the frame's voxel update is skipped.  The handle
+ * stays usable either way.  No counterpart in the reference (its traversal
+ * is sequential and has no waits). */
+#define FF_SPIN_LIMIT_DEFAULT (1u << 22)
+ff_status ff_set_spin_limit(ff_handle *h, uint32_t iterations);
+
+/* Failure injection for tests of the error paths (no counterpart in the
+ * reference).  FF_INJECT_CONFIDENCE_TIMEOUT: the next frame reports that a
+ * bounded wait of the confidence network gave up, exactly as the network
+ * reports it on the device (its error word is set); the frame's bricks are
+ * allocated, its voxel update is skipped and the call returns
+ * FF_ERR_TIMEOUT.  0 cancels a pending injection. */
+enum { FF_INJECT_CONFIDENCE_TIMEOUT = 1 };
+ff_status ff_inject_error(ff_handle *h, int what);
+
 /* Re-mesh the cells touched since the last update and rebuild the
  * interleaved mesh.  Replaces FusionMipMapCPU::updateMeshes()
  * (geometryfusion_mipmap_cpu.cpp:2884-2954) with threaded meshing off;

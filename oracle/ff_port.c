@@ -48,6 +48,7 @@ struct ffp_map {
   int grows;
   int branch_overflow;
   int rz_exact;
+  int fp16; /* SDF and weight stored rounded to half precision (ffp_set_storage_fp16) */
   const float *conf; /* per-pixel confidence of the next frames (learned weight), or NULL */
   /* mesh of the last ffp_update_meshes */
   ffp_cell *cells;
@@ -138,6 +139,50 @@ void ffp_set_update_mode(ffp_map *m, int mode) {
     m->wgt64 = (double *)calloc((size_t)m->leaves_total * 512, sizeof(double));
   }
 }
+
+/* FP16 storage of SDF and weight (no counterpart in the reference, whose
+ * pool is float): after each update the stored value is the nearest binary16
+ * value (ties to even, overflow to infinity, subnormals kept), held here as
+ * the float it converts back to.  Done with integer operations, so the
+ * rounding does not depend on the floating-point rounding mode the update
+ * runs in (round-toward-zero). */
+void ffp_set_storage_fp16(ffp_map *m, int on) { m->fp16 = on != 0; }
+
+static float round_to_half(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  const uint32_t sign = u & 0x80000000u, a = u & 0x7fffffffu;
+  uint32_t r;
+  if (a >= 0x7f800000u) {
+    r = u; /* infinity or NaN */
+  } else if (a >= 0x477ff000u) {
+    r = sign | 0x7f800000u; /* at or above 65520: infinity */
+  } else if (a <= 0x33000000u) {
+    r = sign; /* at or below 2^-25: zero (2^-25 ties to the even zero) */
+  } else {
+    const int e = (int)(a >> 23) - 127;
+    if (e >= -14) {
+      /* normal binary16: keep 10 mantissa bits, round to nearest even */
+      const uint32_t lsb = (a >> 13) & 1u;
+      r = sign | ((a + 0xfffu + lsb) & ~0x1fffu);
+    } else {
+      /* subnormal binary16: a multiple of 2^-24 */
+      const uint32_t mant = (a & 0x7fffffu) | 0x800000u;
+      const int sh = -(e + 1);
+      uint32_t q = mant >> sh;
+      const uint32_t rem = mant & ((1u << sh) - 1u), half = 1u << (sh - 1);
+      if (rem > half || (rem == half && (q & 1u))) q++;
+      float v = (float)q * 5.9604644775390625e-08f; /* exact: q <= 1024 */
+      memcpy(&r, &v, 4);
+      r |= sign;
+    }
+  }
+  float out;
+  memcpy(&out, &r, 4);
+  return out;
+}
+
+float ffp_half_round(float f) { return round_to_half(f); }
 
 /* Float camera parameters, the reference's camPamsFloat (definitions.h:71-88),
  * built in double and rounded once to float. */
@@ -457,6 +502,10 @@ static void update_brick(ffp_map *m, const campams *q, const uint16_t *depth, co
         float add = mask ? tr * wInc : 0.0f;
         m->dist[idx] = (dAcc * wAcc + add) * factor;
         m->wgt[idx] = wNew;
+        if (m->fp16) {
+          m->dist[idx] = round_to_half(m->dist[idx]);
+          m->wgt[idx] = round_to_half(wNew);
+        }
         if (m->color) {
           const uint8_t *px8 = rgb + 3 * (size_t)ii;
           float inc[3] = {(float)px8[2] * COLOR_MUL, (float)px8[1] * COLOR_MUL, (float)px8[0] * COLOR_MUL};

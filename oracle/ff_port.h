@@ -46,6 +46,11 @@ void ffp_destroy(ffp_map *m);
 void ffp_set_update_mode(ffp_map *m, int mode);
 /* Per-pixel confidence multiplying the weight increment (borrowed; NULL: off). */
 void ffp_set_confidence(ffp_map *m, const float *conf);
+/* SDF and weight stored at half precision (round to nearest even after each
+ * update), as the GPU's FP16 storage keeps them. */
+void ffp_set_storage_fp16(ffp_map *m, int on);
+/* The value the FP16 storage keeps for f (for tests of the rounding). */
+float ffp_half_round(float f);
 
 /* One depth frame (uint16, depth*scaling = metres) with BGR colour.
  * K = {fx, fy, cx, cy}; R (row-major 3x3) and t map camera to world.

@@ -35,6 +35,9 @@ def lib():
         L.ffp_destroy.argtypes = [vp]
         L.ffp_set_update_mode.argtypes = [vp, i32]
         L.ffp_set_confidence.argtypes = [vp, vp]
+        L.ffp_set_storage_fp16.argtypes = [vp, i32]
+        L.ffp_half_round.restype = ctypes.c_float
+        L.ffp_half_round.argtypes = [ctypes.c_float]
         L.ffp_add_map.restype = i32
         L.ffp_add_map.argtypes = [vp, vp, vp, i32, i32, vp, vp, vp, ctypes.c_float, ctypes.c_float]
         L.ffp_state.argtypes = [vp, vp, vp]
@@ -62,11 +65,13 @@ class PortFusion:
     """The restated addMap path: bit-exact target of the GPU plain FP32 path."""
 
     def __init__(self, scale=0.005, threshold=0.01, color=True, leaves_total=271420, branches_total=None,
-                 update_mode=1):
+                 update_mode=1, fp16=False):
         if branches_total is None:
             branches_total = max(16 * 4096, leaves_total * 4)
         self.h = lib().ffp_create(scale, threshold, 1 if color else 0, leaves_total, branches_total)
         lib().ffp_set_update_mode(self.h, int(update_mode))
+        if fp16:
+            lib().ffp_set_storage_fp16(self.h, 1)
 
     def close(self):
         if self.h:

@@ -58,6 +58,7 @@ def lib():
         L.ref_cells.restype = ll
         L.ref_cells.argtypes = [vp, vp]
         L.ref_queue_all_cells.argtypes = [vp]
+        L.ref_set_thread_meshing.argtypes = [vp, ctypes.c_int]
         L.ref_cell_mesh.restype = ll
         L.ref_cell_mesh.argtypes = [vp, ll, vp, vp, vp, ctypes.POINTER(ll)]
         L.ref_mc_offset_table.argtypes = [vp]
@@ -102,6 +103,11 @@ class RefFusion:
 
     def update_meshes(self) -> bool:
         return bool(self.L.ref_update_meshes(self.h))
+
+    def set_thread_meshing(self, on: bool):
+        """The reference's setThreadMeshing: meshing on a second thread,
+        updateMeshes returning False while it is busy."""
+        self.L.ref_set_thread_meshing(self.h, 1 if on else 0)
 
     def mesh(self):
         nv, nf = ctypes.c_longlong(), ctypes.c_longlong()

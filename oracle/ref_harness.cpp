@@ -74,6 +74,10 @@ void ref_destroy(void *h) { delete (FusionMipMapCPU *)h; }
 
 void ref_set_incremental_meshing(void *h, int on) { ((FusionMipMapCPU *)h)->setIncrementalMeshing(on != 0); }
 
+/* The reference's threaded meshing (setThreadMeshing(true)): updateMeshes
+ * starts a mesher thread and returns false while one is still running. */
+void ref_set_thread_meshing(void *h, int on) { ((FusionMipMapCPU *)h)->setThreadMeshing(on != 0); }
+
 int ref_add_map(void *h, const uint16_t *depth, const uint8_t *bgr, int w, int hgt, const double *K4,
                 const double *R9, const double *t3, float scaling, float maxcam) {
   FusionMipMapCPU *f = (FusionMipMapCPU *)h;

@@ -11,7 +11,17 @@ import subprocess
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_SRC = os.environ.get("FF_REFERENCE_SRC", "/root/reference/src")
+
+
+def _reference_src():
+    """The reference's src/ directory, as the oracle's build recipe finds it
+    (FF_REFERENCE_DIR or its default checkout); '' where it is absent."""
+    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "refdir"], capture_output=True, text=True)
+    d = r.stdout.strip()
+    return os.path.join(d, "src") if d else ""
+
+
+REF_SRC = _reference_src()
 
 VIEWER_LIKE = r'''
 #include <camerautils.hpp>
@@ -33,7 +43,8 @@ FusionMipMapCPU *make_fusion() { return new FusionMipMapCPU(0, 0, 0, 0.005, 0.01
 '''
 
 
-@pytest.mark.skipif(not os.path.isdir(os.path.join(REF_SRC, "fusion")), reason="reference headers not present")
+@pytest.mark.skipif(not REF_SRC or not os.path.isdir(os.path.join(REF_SRC, "fusion")),
+                    reason="reference headers not present")
 def test_facade_compiles_against_reference_types(tmp_path):
     gxx = shutil.which("g++")
     if not gxx:

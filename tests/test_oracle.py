@@ -111,3 +111,22 @@ def test_reference_float_overload_behaviour():
     assert len(b.mesh()[2]) == 0
     a.close()
     b.close()
+
+
+def test_fp16_storage_rounding_matches_ieee_half(port_lib):
+    """The restatement's FP16 storage keeps the nearest binary16 value (ties
+    to even, overflow to infinity, subnormals): checked against numpy's
+    float16 conversion on edge cases and a million random floats."""
+    L = port_lib.lib()
+    rng = np.random.default_rng(7)
+    bits = rng.integers(0, 2**32, size=1_000_000, dtype=np.uint64).astype(np.uint32)
+    vals = bits.view(np.float32)
+    vals = vals[np.isfinite(vals)]
+    edge = np.array([0.0, -0.0, 1.0, 65504.0, 65519.99, 65520.0, 70000.0, -65520.0, 2.0**-24, 2.0**-25,
+                     1.5 * 2.0**-25, 2.0**-14, 2.0**-14 * (1 - 2.0**-11), 1e-9, 0.1, 0.3333333, 1 + 2.0**-11,
+                     1 + 3 * 2.0**-11], np.float32)
+    xs = np.concatenate([edge, -edge, vals[:200_000], (vals[:200_000] * 1e-30).astype(np.float32),
+                         rng.normal(0, 0.02, 200_000).astype(np.float32)])
+    want = xs.astype(np.float16).astype(np.float32)
+    got = np.array([L.ffp_half_round(float(x)) for x in xs], np.float32)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))

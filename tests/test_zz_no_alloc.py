@@ -47,3 +47,24 @@ def test_noalloc_cells_equal_allocating_export(lib_built):
     # the second call exported a different (larger) mesh through the same buffer
     assert seen[1] > seen[0]
     m.close()
+
+
+def test_noalloc_rejects_more_cells_than_its_buffer(lib_built):
+    """A mesh of more than FF_NOALLOC_MAX_CELLS cells is refused with
+    FF_ERR_BAD_ARG and a message, and nothing is written to the caller's
+    buffers; the allocating export still returns it."""
+    from fastfusion_b200 import fusion as ff
+    K, frames = circle_frames(0, 4, 1280, 960)
+    m = ff.FusionMipMapCPU(0, 0, 0, 0.002, 0.004, 0, True, leaves_max=400000, branches_max=8000000, rcp="exact")
+    for depth, bgr, R, t in frames:
+        m.addMap(depth, ff.CameraInfo(K, R, t), bgr, SCALING, MAXCAM)
+    m.updateMeshes()
+    n = m.stats()["mesh_cells"]
+    assert n > ff.NOALLOC_MAX_CELLS, n
+    st, cells, ranges = _noalloc(m)
+    assert st == 1  # FF_ERR_BAD_ARG
+    assert b"cells" in m._L.ff_last_error(m._h)
+    assert (cells == -7).all() and (ranges == -7).all()
+    want_cells, _ = m.mesh_cells()
+    assert len(want_cells) == n
+    m.close()
