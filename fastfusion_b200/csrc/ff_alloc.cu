@@ -732,6 +732,19 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc
     const uint32_t idx = leaves_before + rank[j];
     if (idx < leaves_max) parent[idx] = parent_of(idx, leaves_max, tree, n, leaf[idx]);
   }
+  // Deferred update: the frame's queue is complete (the new leaves were
+  // queued above); mark each queued brick with the frame's bit and list the
+  // bricks no earlier frame of the pass has marked.  A frame the update must
+  // not take (failed, or the volume must grow first) is left to the host.
+  if (F.upd_mask && !fuse_deferred(F)) {
+    const uint32_t nq = ld_volatile(&cnt->queued);
+    const uint32_t bit = 1u << F.upd_slot;
+    for (uint32_t j = t; j < nq; j += FIN_THREADS) {
+      const uint32_t b = queue[j];
+      // (the queue holds each brick once, so the old mask lacks this bit)
+      if (atomicOr(&F.upd_mask[b], bit) == 0u) F.upd_list[atomicAdd(F.upd_count, 1u)] = b;
+    }
+  }
 }
 
 bool finalize_small_fits(uint32_t npix) {

@@ -125,6 +125,30 @@ struct ff_handle {
   // (ff_inject_error)
   uint32_t spin_limit = SPIN_LIMIT;
   int inject = 0;
+
+  // Deferred voxel update: a single-map frame's update waits for one pass
+  // (k_fuse_multi) over the union of the bricks of up to upd_batch frames,
+  // run when the batch is full, before a growth of the volume, and before
+  // anything reads or replaces voxel state (updateMeshes, accessors, ff_sync).
+  // The waiting frames' images and confidence maps are kept in a ring of
+  // slots; a slot is written again only after the pass that read it.
+  int upd_batch = FUSE_SLOTS_DEFAULT;  // frames a pass takes (ff_set_update_batch)
+  int upd_pending = 0;                 // frames waiting for the pass
+  int cur_slot = -1;                   // the slot of the frame being added (-1: not deferred)
+  FuseSlot upd_slot[FUSE_SLOTS_MAX];
+  double pass_frame_bricks = 0;        // queued bricks of the waiting frames
+  uint32_t *d_upd_mask = nullptr, *d_upd_list = nullptr, *d_upd_count = nullptr;
+  unsigned long long *d_upd_total = nullptr, *h_upd_total = nullptr;  // bricks of all passes
+  uint64_t fused_frame_bricks = 0, direct_bricks = 0;
+  uint16_t *d_ring_depth = nullptr;
+  uint8_t *d_ring_bgr = nullptr;
+  float *d_ring_conf = nullptr;
+  size_t ring_pix = 0, ring_conf_pix = 0;
+  int ring_slots = 0;
+  cudaEvent_t ev_ring_free = nullptr;  // the last pass has read the ring
+  bool ring_read = false;              // a pass was launched since the ring was allocated
+  cudaEvent_t ev_copy = nullptr;       // a device frame's images copied into its slot
+  bool copy_pending = false;
   int pi_insert = -1;  // profile record of the last insert launch this map led
 
   // brick ownership (ff_set_shard) and the voxels grow() has moved the grid by
@@ -155,6 +179,13 @@ static thread_local std::string g_create_error;
       h->err = std::string(#call) + ": " + cudaGetErrorString(e_);                    \
       return FF_ERR_CUDA;                                                             \
     }                                                                                 \
+  } while (0)
+
+// Return a failed ff_status (its message already set).
+#define FCK(call)                  \
+  do {                             \
+    const ff_status s_ = (call);   \
+    if (s_ != FF_OK) return s_;    \
   } while (0)
 
 static ff_status set_err(ff_handle *h, ff_status s, const std::string &m) {
@@ -188,6 +219,58 @@ static cudaError_t wait_event_polling(cudaEvent_t ev) {
 // Order the map's stream after every voxel update launched on fuse_stream.
 static cudaError_t join_fuse(ff_handle *h) {
   return h->last_fuse >= 0 ? cudaStreamWaitEvent(h->stream, h->ev_fuse[h->last_fuse], 0) : cudaSuccess;
+}
+
+// Run the deferred update of the waiting frames: one pass over the union of
+// their bricks on fuse_stream (ordered after their finalisations there);
+// the map's later work and every accessor order after it through ev_fuse.
+static ff_status flush_updates(ff_handle *h) {
+  if (!h->upd_pending) return FF_OK;
+  FuseBatch fb;
+  memset(&fb, 0, sizeof(fb));
+  fb.leaf = h->d_leaf;
+  fb.sdf = h->d_sdf;
+  fb.wgt = h->d_wgt;
+  fb.sdf16 = h->d_sdf16;
+  fb.wgt16 = h->d_wgt16;
+  fb.col = h->d_col;
+  fb.mask = h->d_upd_mask;
+  fb.list = h->d_upd_list;
+  fb.count = h->d_upd_count;
+  fb.total = h->d_upd_total;
+  fb.rcp_tab = h->d_rcp_tab;
+  fb.rcp_shift = h->rcp_shift;
+  fb.scale = h->cfg.scale;
+  fb.thr = h->cfg.threshold;
+  fb.nslots = h->upd_pending;
+  for (int j = 0; j < h->upd_pending; j++) fb.s[j] = h->upd_slot[j];
+  cudaStream_t fs = h->fuse_stream;
+  const int pi = h->prof.begin(ST_FUSE, fs);
+  launch_fuse_multi(fb, h->cfg.storage, h->d_rcp_tab != nullptr, h->sm_count * 2, fs);
+  // every queued brick of every frame read and written once per frame in
+  // the reference: the pass's algorithmic bytes
+  const double brick_bytes = 512.0 * 2 * ((h->cfg.storage == FF_STORAGE_FP16 ? 4 : 8) + 6);
+  h->prof.end(pi, h->pass_frame_bricks * brick_bytes, fs);
+  CK(cudaGetLastError());
+  CK(cudaMemsetAsync(h->d_upd_count, 0, sizeof(uint32_t), fs));
+  CK(cudaMemcpyAsync(h->h_upd_total, h->d_upd_total, sizeof(unsigned long long), cudaMemcpyDeviceToHost, fs));
+  CK(cudaEventRecord(h->ev_ring_free, fs));
+  const int k = h->last_fuse >= 0 ? h->last_fuse : h->set;
+  CK(cudaEventRecord(h->ev_fuse[k], fs));
+  h->last_fuse = k;
+  h->upd_pending = 0;
+  h->pass_frame_bricks = 0;
+  h->ring_read = true;
+  return FF_OK;
+}
+
+// The waiting frames updated, and the map's stream ordered after every
+// update: before anything reads or replaces voxel state.
+static ff_status settle(ff_handle *h) {
+  ff_status st = flush_updates(h);
+  if (st != FF_OK) return st;
+  CK(join_fuse(h));
+  return FF_OK;
 }
 
 // ----------------------------------------------------------- camera math --
@@ -364,6 +447,47 @@ static ff_status ensure_image(ff_handle *h, int W, int H) {
   return FF_OK;
 }
 
+// The ring of image slots for `slots` waiting frames of W x H pixels (and
+// their confidence maps when the learned weight is on); a reallocation first
+// runs the waiting frames' pass.
+static ff_status ensure_ring(ff_handle *h, int W, int H) {
+  const size_t npix = (size_t)W * H;
+  const bool need_conf = h->conf_tau_cm > 0.0f;
+  if (npix <= h->ring_pix && h->ring_slots >= h->upd_batch && (!need_conf || npix <= h->ring_conf_pix))
+    return FF_OK;
+  ff_status st = settle(h);
+  if (st != FF_OK) return st;
+  CK(cudaStreamSynchronize(h->fuse_stream));
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaStreamSynchronize(h->copy_stream));
+  const int slots = std::max(h->upd_batch, h->ring_slots);
+  const size_t pix = std::max(npix, h->ring_pix);
+  if (pix > h->ring_pix || slots > h->ring_slots) {
+    cudaFree(h->d_ring_depth);
+    cudaFree(h->d_ring_bgr);
+    h->d_ring_depth = nullptr;
+    h->d_ring_bgr = nullptr;
+    h->ring_pix = 0;
+    CK(alloc(&h->d_ring_depth, pix * slots));
+    CK(alloc(&h->d_ring_bgr, pix * 3 * slots));
+    if (h->d_ring_conf) {
+      cudaFree(h->d_ring_conf);
+      h->d_ring_conf = nullptr;
+      h->ring_conf_pix = 0;
+    }
+    h->ring_pix = pix;
+    h->ring_slots = slots;
+  }
+  if (need_conf && h->ring_conf_pix < h->ring_pix) {
+    cudaFree(h->d_ring_conf);
+    h->d_ring_conf = nullptr;
+    CK(alloc(&h->d_ring_conf, h->ring_pix * h->ring_slots));
+    h->ring_conf_pix = h->ring_pix;
+  }
+  h->ring_read = false;
+  return FF_OK;
+}
+
 // ------------------------------------------------------------------ API ---
 
 extern "C" {
@@ -479,6 +603,15 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
       fail(FF_ERR_CUDA, "update stream");
       break;
     }
+    if (alloc(&h->d_upd_mask, L) != cudaSuccess || alloc(&h->d_upd_list, L) != cudaSuccess ||
+        alloc(&h->d_upd_count, 1) != cudaSuccess || alloc(&h->d_upd_total, 1) != cudaSuccess ||
+        cudaMallocHost((void **)&h->h_upd_total, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_ring_free, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_copy, cudaEventDisableTiming) != cudaSuccess) {
+      fail(FF_ERR_OOM_POOL, "deferred update");
+      break;
+    }
+    *h->h_upd_total = 0;
     select_set(h, 0);
     if (cfg->rcp_mode == FF_RCP_HOST) {
       std::vector<uint32_t> tab;
@@ -510,6 +643,9 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
       cudaMemsetAsync(h->d_wgt16, 0, sizeof(__half) * L * 512, h->stream);
     }
     cudaMemsetAsync(h->d_col, 0, sizeof(uint16_t) * L * 1536, h->stream);
+    cudaMemsetAsync(h->d_upd_mask, 0, sizeof(uint32_t) * L, h->stream);
+    cudaMemsetAsync(h->d_upd_count, 0, sizeof(uint32_t), h->stream);
+    cudaMemsetAsync(h->d_upd_total, 0, sizeof(unsigned long long), h->stream);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) { fail(FF_ERR_CUDA, "init"); break; }
   } while (0);
   if (st != FF_OK) {
@@ -532,7 +668,8 @@ ff_status ff_destroy(ff_handle *h) {
                   h->d_barrier, h->d_depth_set[0], h->d_depth_set[1], h->d_bgr_set[0], h->d_bgr_set[1], h->d_pxp,
                   h->d_pyp, h->d_vox, h->d_proc, h->d_bnd, h->d_pend, h->d_keys, h->d_sort_tmp, h->d_rcp_tab,
                   h->d_cnn_params, h->d_cnn_packed, h->d_feat, h->d_a1, h->d_a2, h->d_conf_set[0], h->d_conf_set[1],
-                  h->d_batch_set[0], h->d_batch_set[1]};
+                  h->d_batch_set[0], h->d_batch_set[1], h->d_upd_mask, h->d_upd_list, h->d_upd_count,
+                  h->d_upd_total, h->d_ring_depth, h->d_ring_bgr, h->d_ring_conf};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 2; k++) {
@@ -540,6 +677,9 @@ ff_status ff_destroy(ff_handle *h) {
     if (h->h_batch_set[k]) cudaFreeHost(h->h_batch_set[k]);
     if (h->ev_fuse[k]) cudaEventDestroy(h->ev_fuse[k]);
   }
+  if (h->h_upd_total) cudaFreeHost(h->h_upd_total);
+  if (h->ev_ring_free) cudaEventDestroy(h->ev_ring_free);
+  if (h->ev_copy) cudaEventDestroy(h->ev_copy);
   if (h->ev_fin) cudaEventDestroy(h->ev_fin);
   if (h->ev_alloc) cudaEventDestroy(h->ev_alloc);
   if (h->ev_cnn_in) cudaEventDestroy(h->ev_cnn_in);
@@ -565,6 +705,16 @@ ff_status ff_set_shard(ff_handle *h, int shard, int shards) {
   if (h->frames || h->n) return set_err(h, FF_ERR_BAD_ARG, "ff_set_shard: set before the first frame");
   h->shard = (uint32_t)shard;
   h->shards = (uint32_t)shards;
+  return FF_OK;
+}
+
+ff_status ff_set_update_batch(ff_handle *h, int frames) {
+  if (!h) return FF_ERR_BAD_ARG;
+  if (frames < 1 || frames > FUSE_SLOTS_MAX)
+    return set_err(h, FF_ERR_BAD_ARG, "ff_set_update_batch: frames must be 1.." + std::to_string(FUSE_SLOTS_MAX));
+  CK(cudaSetDevice(h->cfg.device));
+  FCK(settle(h));
+  h->upd_batch = frames;
   return FF_OK;
 }
 
@@ -597,15 +747,16 @@ ff_status ff_set_tuning(ff_handle *h, const ff_tuning *t) {
 ff_status ff_sync(ff_handle *h) {
   if (!h) return FF_ERR_BAD_ARG;
   CK(cudaSetDevice(h->cfg.device));
-  CK(join_fuse(h));
+  FCK(settle(h));
   CK(cudaStreamSynchronize(h->stream));
+  CK(cudaStreamSynchronize(h->fuse_stream));
   return FF_OK;
 }
 
 ff_status ff_set_stream(ff_handle *h, void *cuda_stream) {
   if (!h) return FF_ERR_BAD_ARG;
   cudaSetDevice(h->cfg.device);
-  join_fuse(h);
+  settle(h);
   cudaStreamSynchronize(h->stream);
   if (h->own_stream) cudaStreamDestroy(h->stream);
   if (cuda_stream) {
@@ -741,6 +892,12 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
   mf.shards = h->shards;
   mf.spin_limit = h->spin_limit;
   for (int r = 0; r < 3; r++) mf.shift[r] = h->shift[r];
+  if (h->cur_slot >= 0) {
+    mf.upd_mask = h->d_upd_mask;
+    mf.upd_list = h->d_upd_list;
+    mf.upd_count = h->d_upd_count;
+    mf.upd_slot = h->cur_slot;
+  }
   if (h->conf_tau_cm > 0.0f) {
     // the frame's confidence map, ahead of the launches that read it on this stream
     const size_t npx = (size_t)W * H;
@@ -762,6 +919,8 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
       h->d_conf = h->d_conf_set[h->set];
       h->conf_cap = npx;
     }
+    // a waiting frame's confidence map lives in its ring slot until the pass
+    if (h->cur_slot >= 0) h->d_conf = h->d_ring_conf + (size_t)h->cur_slot * h->ring_pix;
     const float kf[4] = {(float)K[0], (float)K[1], (float)K[2], (float)K[3]};
     cudaStream_t cs = s;
     if (side && plan.one_sync) {
@@ -913,7 +1072,7 @@ static ff_status frame_launch(ff_handle *lead, int n) {
 // adds their number itself), and this event recorded after the copy, so the
 // finalisation and the update overlap the host's return and its next frame.
 static ff_status frame_launch_update(ff_handle *lead, int n, uint32_t max_npix, int &pi_fin, int &pi_fuse,
-                                     cudaEvent_t counters = nullptr, bool side = false) {
+                                     cudaEvent_t counters = nullptr, bool side = false, bool deferred = false) {
   ff_handle *h = lead;  // (error reporting)
   cudaStream_t s = lead->stream;
   if (counters) {
@@ -921,6 +1080,11 @@ static ff_status frame_launch_update(ff_handle *lead, int n, uint32_t max_npix, 
       // the frame's confidence network reports into these counters
       CK(cudaStreamWaitEvent(s, lead->ev_cnn_done, 0));
       lead->cnn_pending = false;
+    }
+    if (lead->copy_pending) {
+      // a device frame's images are in its ring slot before the call returns
+      CK(cudaStreamWaitEvent(s, lead->ev_copy, 0));
+      lead->copy_pending = false;
     }
     CK(cudaMemcpyAsync(lead->h_cnt, lead->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, s));
     CK(cudaEventRecord(counters, s));
@@ -940,13 +1104,16 @@ static ff_status frame_launch_update(ff_handle *lead, int n, uint32_t max_npix, 
     CK(cudaEventRecord(lead->ev_fin, fs));
     lead->fin_pending = true;
   }
-  pi_fuse = lead->prof.begin(ST_FUSE, fs);
-  // enough blocks for a frame's bricks in one pass; blocks loop over larger batches
-  const int shape = lead->tune.fuse_shape;
-  const int per_sm = lead->tune.fuse_blocks_per_sm > 0 ? lead->tune.fuse_blocks_per_sm : 8 / fuse_shape_bricks(shape);
-  launch_fuse(lead->d_batch, n, true, lead->cfg.storage, lead->d_rcp_tab != nullptr, lead->sm_count * per_sm, fs,
-              shape);
-  lead->prof.end(pi_fuse, 0.0, fs);
+  if (!deferred) {
+    pi_fuse = lead->prof.begin(ST_FUSE, fs);
+    // enough blocks for a frame's bricks in one pass; blocks loop over larger batches
+    const int shape = lead->tune.fuse_shape;
+    const int per_sm =
+        lead->tune.fuse_blocks_per_sm > 0 ? lead->tune.fuse_blocks_per_sm : 8 / fuse_shape_bricks(shape);
+    launch_fuse(lead->d_batch, n, true, lead->cfg.storage, lead->d_rcp_tab != nullptr, lead->sm_count * per_sm, fs,
+                shape);
+    lead->prof.end(pi_fuse, 0.0, fs);
+  }
   if (side) {
     CK(cudaEventRecord(lead->ev_fuse[lead->set], fs));
     lead->last_fuse = lead->set;
@@ -1016,7 +1183,9 @@ static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf,
       (hc.box_min[0] < 0 || hc.box_min[1] < 0 || hc.box_min[2] < 0 || hc.box_max[0] >= (int)h->n ||
        hc.box_max[1] >= (int)h->n || hc.box_max[2] >= (int)h->n)) {
     // (with one synchronisation the update stood aside for this); the growth
-    // moves leaf positions that updates still in flight read
+    // moves leaf positions that the waiting frames' update and updates still
+    // in flight read: those run first
+    FCK(flush_updates(h));
     CK(join_fuse(h));
     int pi = h->prof.begin(ST_GROW, s);
     const double tree_bytes = (double)h->branches_used * 4 * 2 + (double)h->leaves_used * 8 * 2;
@@ -1029,6 +1198,7 @@ static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf,
   // (4+4 B, or 2+2 B in FP16) and three 16-bit colour channels
   const double brick_bytes = 512.0 * 2 * ((h->cfg.storage == FF_STORAGE_FP16 ? 4 : 8) + 6);
   if (fuse_now && nq) {
+    FCK(flush_updates(h));
     CK(join_fuse(h));  // after the previous frames' updates
     // this map's own descriptor, with the host's count (leaf positions may
     // have moved with the growth; the camera parameters are the frame's)
@@ -1052,6 +1222,27 @@ static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf,
   h->frames++;
   mesh_note_frame(h->mesh);
   if (queued) *queued = (int32_t)nq;
+  if (h->cur_slot >= 0 && plan.one_sync && !skip_update && !fuse_now) {
+    // the finalisation marked the frame's bricks: the frame waits for the
+    // pass, which reads its slot's images
+    FuseSlot &fs_ = h->upd_slot[h->cur_slot];
+    fs_.q = mf.q;
+    fs_.depth = h->d_ring_depth + (size_t)h->cur_slot * h->ring_pix;
+    fs_.bgr = h->d_ring_bgr + (size_t)h->cur_slot * h->ring_pix * 3;
+    fs_.conf = mf.conf;
+    fs_.W = plan.W;
+    fs_.H = plan.H;
+    fs_.scaling = plan.scaling;
+    fs_.maxcam = plan.maxcam;
+    h->upd_pending = h->cur_slot + 1;
+    h->pass_frame_bricks += nq;
+    h->fused_frame_bricks += nq;
+    if (h->upd_pending >= h->upd_batch) FCK(flush_updates(h));
+  } else if (!skip_update) {
+    // updated by itself (on the device, gated, or just now after a growth)
+    h->fused_frame_bricks += nq;
+    h->direct_bricks += nq;
+  }
   if (cnn_failed) {
     // the word is kept across frames: clear it once every kernel of the
     // frame that reads it has run
@@ -1085,11 +1276,12 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
   if (bgr_pending) CK(cudaStreamWaitEvent(s, h->ev_bgr_ready, 0));
   int pi_fin = -1, pi_fuse = -1;
   if (plan.one_sync) {
-    // the frame returns once its counters are on the host; its voxel update
-    // (gated on the device) keeps running, ordered before anything that
-    // follows on the stream
+    // the frame returns once its counters are on the host; its leaf
+    // finalisation (and, for a deferred frame, the marking of its bricks for
+    // the next pass; else its voxel update, gated on the device) keeps
+    // running, ordered before anything that follows on the stream
     plan.counters_early = true;
-    st = frame_launch_update(h, 1, (uint32_t)(W * H), pi_fin, pi_fuse, h->ev_counters, true);
+    st = frame_launch_update(h, 1, (uint32_t)(W * H), pi_fin, pi_fuse, h->ev_counters, true, h->cur_slot >= 0);
     if (st != FF_OK) return st;
     CK(wait_event_polling(h->ev_counters));
   } else {
@@ -1097,9 +1289,17 @@ static ff_status add_map_device(ff_handle *h, const uint16_t *d_depth, const uin
     CK(cudaStreamSynchronize(s));
   }
   st = frame_finish(h, plan, mf, pi_fin, pi_fuse, queued);
-  // the previous frame's update has finished reading its images
-  if (st == FF_OK && h->last_fuse >= 0) CK(cudaEventSynchronize(h->ev_fuse[h->set ^ 1]));
+  // the previous frame's update has finished reading its images (a deferred
+  // frame's images are the ring's copies instead)
+  if (st == FF_OK && h->cur_slot < 0 && h->last_fuse >= 0) CK(cudaEventSynchronize(h->ev_fuse[h->set ^ 1]));
   return st;
+}
+
+// Whether a single-map frame of W x H pixels waits for a deferred update
+// pass: every frame the one-block leaf finalisation takes (it marks the
+// frame's bricks), when passes take more than one frame.
+static bool deferrable(const ff_handle *h, int W, int H) {
+  return h->upd_batch > 1 && finalize_small_fits((uint32_t)W * (uint32_t)H);
 }
 
 // Before a single-map frame: its buffer set, free once the update two frames
@@ -1117,24 +1317,41 @@ ff_status ff_add_map_u16(ff_handle *h, const uint16_t *depth, int width, int hei
   if (!h) return FF_ERR_BAD_ARG;
   if (!depth || !bgr || !K || !R || !t || width <= 0 || height <= 0)
     return set_err(h, FF_ERR_BAD_ARG, "ff_add_map_u16: NULL pointer or empty image");
+  h->cur_slot = -1;
   CK(cudaSetDevice(h->cfg.device));
   ff_status st = ensure_image(h, width, height);
   if (st != FF_OK) return st;
+  const bool defer = deferrable(h, width, height);
+  if (defer && (st = ensure_ring(h, width, height)) != FF_OK) return st;
   st = begin_frame(h);
   if (st != FF_OK) return st;
   if (!depth_pitch) depth_pitch = sizeof(uint16_t) * width;
   if (!bgr_pitch) bgr_pitch = 3 * (size_t)width;
-  CK(cudaMemcpy2DAsync(h->d_depth, sizeof(uint16_t) * width, depth, depth_pitch, sizeof(uint16_t) * width, height,
+  // a deferred frame's images go to its ring slot (free once the last pass
+  // that read the ring has run)
+  uint16_t *dd = h->d_depth;
+  uint8_t *db = h->d_bgr;
+  if (defer) {
+    h->cur_slot = h->upd_pending;
+    dd = h->d_ring_depth + (size_t)h->cur_slot * h->ring_pix;
+    db = h->d_ring_bgr + (size_t)h->cur_slot * h->ring_pix * 3;
+    if (h->ring_read) {
+      CK(cudaStreamWaitEvent(h->stream, h->ev_ring_free, 0));
+      CK(cudaStreamWaitEvent(h->copy_stream, h->ev_ring_free, 0));
+    }
+  }
+  CK(cudaMemcpy2DAsync(dd, sizeof(uint16_t) * width, depth, depth_pitch, sizeof(uint16_t) * width, height,
                        cudaMemcpyHostToDevice, h->stream));
   // the colour copy waits for the previous frame's update (the last reader of
   // d_bgr) and overlaps this frame's allocation kernels
   CK(cudaEventRecord(h->ev_bgr_free, h->stream));
   CK(cudaStreamWaitEvent(h->copy_stream, h->ev_bgr_free, 0));
   CK(cudaStreamWaitEvent(h->copy_stream, h->ev_fuse[h->set], 0));  // this set's last reader
-  CK(cudaMemcpy2DAsync(h->d_bgr, 3 * (size_t)width, bgr, bgr_pitch, 3 * (size_t)width, height,
-                       cudaMemcpyHostToDevice, h->copy_stream));
+  CK(cudaMemcpy2DAsync(db, 3 * (size_t)width, bgr, bgr_pitch, 3 * (size_t)width, height, cudaMemcpyHostToDevice,
+                       h->copy_stream));
   CK(cudaEventRecord(h->ev_bgr_ready, h->copy_stream));
-  st = add_map_device(h, h->d_depth, h->d_bgr, true, width, height, K, R, t, scaling, maxcam, queued);
+  st = add_map_device(h, dd, db, true, width, height, K, R, t, scaling, maxcam, queued);
+  h->cur_slot = -1;
   // the caller's image must not be read after return, error paths included
   cudaStreamSynchronize(h->copy_stream);
   return st;
@@ -1146,12 +1363,39 @@ ff_status ff_add_map_u16_device(ff_handle *h, const uint16_t *d_depth, const uin
   if (!h) return FF_ERR_BAD_ARG;
   if (!d_depth || !d_bgr || !K || !R || !t || width <= 0 || height <= 0)
     return set_err(h, FF_ERR_BAD_ARG, "ff_add_map_u16_device: NULL pointer or empty image");
+  h->cur_slot = -1;
+  h->copy_pending = false;
   CK(cudaSetDevice(h->cfg.device));
   ff_status st = ensure_image(h, width, height);
   if (st != FF_OK) return st;
+  const bool defer = deferrable(h, width, height);
+  if (defer && (st = ensure_ring(h, width, height)) != FF_OK) return st;
   st = begin_frame(h);
   if (st != FF_OK) return st;
-  return add_map_device(h, d_depth, d_bgr, false, width, height, K, R, t, scaling, maxcam, queued);
+  if (defer) {
+    // the images are copied into the frame's ring slot (after the work the
+    // caller ordered on the map's stream, and after the last pass that read
+    // the ring); the call returns once the copies are done
+    h->cur_slot = h->upd_pending;
+    const size_t npix = (size_t)width * height;
+    CK(cudaEventRecord(h->ev_bgr_free, h->stream));
+    CK(cudaStreamWaitEvent(h->copy_stream, h->ev_bgr_free, 0));
+    if (h->ring_read) CK(cudaStreamWaitEvent(h->copy_stream, h->ev_ring_free, 0));
+    CK(cudaMemcpyAsync(h->d_ring_depth + (size_t)h->cur_slot * h->ring_pix, d_depth, 2 * npix,
+                       cudaMemcpyDeviceToDevice, h->copy_stream));
+    CK(cudaMemcpyAsync(h->d_ring_bgr + (size_t)h->cur_slot * h->ring_pix * 3, d_bgr, 3 * npix,
+                       cudaMemcpyDeviceToDevice, h->copy_stream));
+    CK(cudaEventRecord(h->ev_copy, h->copy_stream));
+    h->copy_pending = true;
+  }
+  st = add_map_device(h, d_depth, d_bgr, false, width, height, K, R, t, scaling, maxcam, queued);
+  if (h->copy_pending) {
+    // (an error returned before the counter copy waited for it)
+    cudaEventSynchronize(h->ev_copy);
+    h->copy_pending = false;
+  }
+  h->cur_slot = -1;
+  return st;
 }
 
 ff_status ff_add_maps_u16_device(ff_handle *const *maps, int n, const uint16_t *const *d_depth,
@@ -1196,7 +1440,12 @@ ff_status ff_add_maps_u16_device(ff_handle *const *maps, int n, const uint16_t *
   std::vector<MapFrame> mf(n);
   for (int i = 0; i < n; i++) {
     ff_handle *m = maps[i];
-    CK(join_fuse(m));  // single-map frames' updates still in flight
+    // single-map frames waiting for their update, or still in flight
+    {
+      const ff_status st_ = settle(m);
+      if (st_ != FF_OK) return set_err(lead, st_, m->err);
+    }
+    m->cur_slot = -1;
     CK(cudaStreamSynchronize(m->stream));
     ff_status st = ensure_image(m, width[i], height[i]);
     if (st != FF_OK) return st;
@@ -1321,6 +1570,9 @@ ff_status ff_get_stats(ff_handle *h, ff_stats *o) {
   o->new_leaves = h->new_leaves;
   o->dedupe_rounds = h->dedupe_rounds;
   o->graph_replays = h->graph_replays;
+  o->update_batch = (uint32_t)h->upd_batch;
+  o->fused_bricks = *h->h_upd_total + h->direct_bricks;
+  o->fused_frame_bricks = h->fused_frame_bricks;
   return FF_OK;
 }
 
@@ -1366,7 +1618,7 @@ ff_status ff_get_bricks(ff_handle *h, uint32_t first, uint32_t count, float *sdf
   if (!h || !sdf || !weight || !rgb) return FF_ERR_BAD_ARG;
   if ((uint64_t)first + count > h->cfg.leaves_max) return set_err(h, FF_ERR_BAD_ARG, "ff_get_bricks: range");
   CK(cudaSetDevice(h->cfg.device));
-  CK(join_fuse(h));
+  FCK(settle(h));
   size_t nv = (size_t)count * 512;
   if (h->cfg.storage == FF_STORAGE_FP16) {
     std::vector<__half> a(nv), b(nv);
@@ -1395,7 +1647,7 @@ ff_status ff_set_bricks(ff_handle *h, uint32_t first, uint32_t count, const floa
   if (!h || !sdf || !weight || !rgb) return FF_ERR_BAD_ARG;
   if ((uint64_t)first + count > h->cfg.leaves_max) return set_err(h, FF_ERR_BAD_ARG, "ff_set_bricks: range");
   CK(cudaSetDevice(h->cfg.device));
-  CK(join_fuse(h));
+  FCK(settle(h));
   size_t nv = (size_t)count * 512;
   if (h->cfg.storage == FF_STORAGE_FP16) {
     std::vector<__half> a(nv), b(nv);
@@ -1427,7 +1679,7 @@ ff_status ff_set_state(ff_handle *h, uint32_t n, const float offset[3], const ui
   if (branches_used > h->cfg.branches_max || leaves_used > h->cfg.leaves_max || (branches_used & 15))
     return set_err(h, FF_ERR_BAD_ARG, "ff_set_state: state larger than this map's capacity");
   CK(cudaSetDevice(h->cfg.device));
-  CK(join_fuse(h));
+  FCK(settle(h));
   launch_fill(h->d_tree, h->cfg.branches_max, BRANCHINIT, h->stream);
   CK(cudaMemcpyAsync(h->d_tree, tree, sizeof(uint32_t) * branches_used, cudaMemcpyHostToDevice, h->stream));
   std::vector<ushort4> lp(leaves_used);
@@ -1454,7 +1706,7 @@ ff_status ff_set_state(ff_handle *h, uint32_t n, const float offset[3], const ui
 ff_status ff_update_meshes(ff_handle *h, int *updated) {
   if (!h) return FF_ERR_BAD_ARG;
   CK(cudaSetDevice(h->cfg.device));
-  CK(join_fuse(h));
+  FCK(settle(h));
   if (!h->meshing_ok || !h->n) {
     if (updated) *updated = 1;
     return FF_OK;
@@ -1505,7 +1757,7 @@ ff_status ff_profile(ff_handle *h, int enable) {
 ff_status ff_profile_read(ff_handle *h, double *ms, double *bytes, uint64_t *launches) {
   if (!h || !ms || !bytes || !launches) return FF_ERR_BAD_ARG;
   CK(cudaSetDevice(h->cfg.device));
-  CK(join_fuse(h));
+  FCK(settle(h));
   CK(cudaStreamSynchronize(h->fuse_stream));
   h->prof.flush();
   for (int i = 0; i < FF_PROFILE_STAGES; i++) {
@@ -1641,7 +1893,7 @@ ff_status ff_raycast_depth(ff_handle *h, const double K[4], const double R[9], c
     return set_err(h, FF_ERR_BAD_ARG, "ff_raycast_depth: window must be in (0, 4] m and step in [1e-4, window]");
   if (!h->n) return set_err(h, FF_ERR_BAD_ARG, "ff_raycast_depth: the map holds no frame");
   CK(cudaSetDevice(h->cfg.device));
-  CK(join_fuse(h));
+  FCK(settle(h));
   RaycastMap m;
   m.tree = h->d_tree;
   m.leaf = h->d_leaf;

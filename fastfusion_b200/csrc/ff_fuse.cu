@@ -158,22 +158,6 @@ __device__ __forceinline__ void fuse_brick(const uint32_t brick, const ushort4 *
   }
 }
 
-// Whether a frame's update must wait for the host: an allocation error, or
-// the volume must grow first (the host then grows and launches the update
-// again).  Mirrors the host's test after the traversal.
-__device__ __forceinline__ bool fuse_deferred(const MapFrame &F) {
-  const Counters *c = F.cnt;
-  // a failed allocation, or a confidence network whose wait gave up (its
-  // confidence map is not valid): the frame is not fused
-  if ((c->error & ERR_FRAME_FAILED) || c->cnn_error) return true;
-  const uint32_t leaves = F.leaves_before + c->pending;
-  const uint32_t branches = min(c->branches_used, F.branches_max);
-  const int n = (int)F.n;
-  const bool outside = c->box_min[0] < 0 || c->box_min[1] < 0 || c->box_min[2] < 0 || c->box_max[0] >= n ||
-                       c->box_max[1] >= n || c->box_max[2] >= n;
-  return leaves < F.leaves_max && branches < F.branches_max && outside;
-}
-
 // BPC bricks per block of 512 BPC threads, one thread per voxel, blocks
 // looping over the bricks of every map of the batch in order.  Gated: each
 // map's count is read on the device; otherwise the host's count (nq_host)
@@ -204,6 +188,182 @@ __global__ void __launch_bounds__(512 * BPC, MINB) k_fuse(const BatchDesc *__res
     const uint32_t local = b - (m ? end[m - 1] : 0u);
     fuse_brick<FP16, RCP_HOST>(F.queue[local], F.leaf, F.sdf, F.wgt, F.sdf16, F.wgt16, F.col, F.depth, F.bgr, F.W,
                                F.H, sq[m], F.scale, F.thr, F.scaling, F.maxcam, F.rcp_tab, F.rcp_shift, F.conf, v);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Deferred update: one pass over the bricks of several frames.
+//
+// The reference updates every queued brick once per frame.  A voxel's update
+// depends only on its own stored state and on the frame (camera parameters,
+// depth, colour, confidence), so the frames of a batch can be applied to a
+// voxel one after another in a single pass: load the state once, apply each
+// frame that queued the brick, in frame order, with the same round-toward-zero
+// operations, and store once.  Between two frames the state is rounded exactly
+// as a store and a load would round it (colour truncated to uint16; SDF and
+// weight to half with FP16 storage), so every bit equals the frame-by-frame
+// update.  The brick's state is read and written once per pass instead of
+// once per frame.
+//
+// One block of 512 threads per brick (one thread per voxel), blocks striding
+// over the pass's brick list.  Per brick and frame, the start positions of
+// the 64 voxel rows -- the reference's loop accumulation, z steps then y
+// steps -- are made once, by 64 threads, into shared memory.
+// ---------------------------------------------------------------------------
+
+constexpr int FUSE_MULTI_BLOCKS_PER_SM = 2;
+
+template <bool FP16, bool RCP_HOST>
+__global__ void __launch_bounds__(512, FUSE_MULTI_BLOCKS_PER_SM) k_fuse_multi(const __grid_constant__ FuseBatch fb) {
+  __shared__ float3 rows[FUSE_SLOTS_MAX][64];  // per frame: (z, y) row start in camera coordinates
+  __shared__ float3 xstep[FUSE_SLOTS_MAX];     // per frame: d11, d21, d31 (one voxel along x)
+  __shared__ int order[FUSE_SLOTS_MAX];        // the brick's frames, in frame order
+  __shared__ uint32_t s_mask;
+  __shared__ ushort4 s_leaf;
+  const int v = threadIdx.x;
+  const int x = v & 7, y = (v >> 3) & 7, z = v >> 6;
+  const uint32_t total = *fb.count;
+  const float scale = fb.scale, thr = fb.thr;
+  const uint32_t *__restrict__ rtab = fb.rcp_tab;
+  const int rshift = fb.rcp_shift;
+  for (uint32_t bi = blockIdx.x; bi < total; bi += gridDim.x) {
+    const uint32_t brick = fb.list[bi];
+    if (v == 0) {
+      s_mask = fb.mask[brick];
+      s_leaf = fb.leaf[brick];
+    }
+    __syncthreads();
+    const uint32_t mask = s_mask;
+    const ushort4 o = s_leaf;
+    const int nk = __popc(mask);
+    if (v < 32 && ((mask >> v) & 1u)) order[__popc(mask & ((1u << v) - 1u))] = v;
+    // the voxel's stored state, loaded while the row starts are made
+    const size_t vi = (size_t)brick * 512 + v;
+    float wAcc, dAcc;
+    if (FP16) {
+      wAcc = __half2float(fb.wgt16[vi]);
+      dAcc = __half2float(fb.sdf16[vi]);
+    } else {
+      wAcc = fb.wgt[vi];
+      dAcc = fb.sdf[vi];
+    }
+    uint16_t *cb = fb.col + (size_t)brick * 1536 + v;
+    uint16_t acc[3] = {cb[0], cb[512], cb[1024]};
+    __syncthreads();
+    const float ls = (float)o.w;
+    const float fls = __fmul_rz(ls, scale);
+    const float fo0 = (float)o.x, fo1 = (float)o.y, fo2 = (float)o.z;
+    for (int k0 = 0; k0 < nk; k0 += 8) {
+      const int k = k0 + (v >> 6);
+      if (k < nk) {
+        const int j = order[k];
+        const CamF &q = fb.s[j].q;
+        const float *M = q.r;
+        // brick origin in camera coordinates, then z steps and y steps as
+        // the reference's loops add them
+        float pzx = __fadd_rz(__fmul_rz(__fadd_rz(__fadd_rz(__fmul_rz(M[0], fo0), __fmul_rz(M[1], fo1)), __fmul_rz(M[2], fo2)), scale), q.t[0]);
+        float pzy = __fadd_rz(__fmul_rz(__fadd_rz(__fadd_rz(__fmul_rz(M[3], fo0), __fmul_rz(M[4], fo1)), __fmul_rz(M[5], fo2)), scale), q.t[1]);
+        float pzz = __fadd_rz(__fmul_rz(__fadd_rz(__fadd_rz(__fmul_rz(M[6], fo0), __fmul_rz(M[7], fo1)), __fmul_rz(M[8], fo2)), scale), q.t[2]);
+        const float d12 = __fmul_rz(M[1], fls), d22 = __fmul_rz(M[4], fls), d32 = __fmul_rz(M[7], fls);
+        const float d13 = __fmul_rz(M[2], fls), d23 = __fmul_rz(M[5], fls), d33 = __fmul_rz(M[8], fls);
+        const int r = v & 63, rz = r >> 3, ry = r & 7;
+        for (int i = 0; i < rz; i++) {
+          pzx = __fadd_rz(pzx, d13);
+          pzy = __fadd_rz(pzy, d23);
+          pzz = __fadd_rz(pzz, d33);
+        }
+        for (int i = 0; i < ry; i++) {
+          pzx = __fadd_rz(pzx, d12);
+          pzy = __fadd_rz(pzy, d22);
+          pzz = __fadd_rz(pzz, d32);
+        }
+        rows[j][r] = make_float3(pzx, pzy, pzz);
+        if (r == 0) xstep[j] = make_float3(__fmul_rz(M[0], fls), __fmul_rz(M[3], fls), __fmul_rz(M[6], fls));
+      }
+    }
+    __syncthreads();
+    const float thrD = __fmul_rz(thr, ls);
+    const float thrW = __fmul_rz(__fmul_rz(WEIGHT_FACTOR, thr), ls);
+    const float fx_ = (float)x;
+    for (int k = 0; k < nk; k++) {
+      const int j = order[k];
+      const FuseSlot &S = fb.s[j];
+      const float3 rb = rows[j][z * 8 + y];
+      const float3 d1 = xstep[j];
+      // lane offsets 0, d, 2d, ..., 7d of the 8-wide rows
+      const float kx = x == 0 ? 0.0f : (x == 1 ? d1.x : __fmul_rz(fx_, d1.x));
+      const float ky = x == 0 ? 0.0f : (x == 1 ? d1.y : __fmul_rz(fx_, d1.y));
+      const float kz = x == 0 ? 0.0f : (x == 1 ? d1.z : __fmul_rz(fx_, d1.z));
+      const float px = __fadd_rz(rb.x, kx), py = __fadd_rz(rb.y, ky), pz = __fadd_rz(rb.z, kz);
+      const int W = S.W, H = S.H;
+      const float len = __fsqrt_rz(__fadd_rz(__fadd_rz(__fmul_rz(px, px), __fmul_rz(py, py)), __fmul_rz(pz, pz)));
+      const float rc = rcp_upd<RCP_HOST>(pz, rtab, rshift);
+      const int imx = cvt_x86_rz(__fadd_rz(S.q.cx, __fmul_rz(S.q.fx, __fmul_rz(px, rc))));
+      const int imy = cvt_x86_rz(__fadd_rz(S.q.cy, __fmul_rz(S.q.fy, __fmul_rz(py, rc))));
+      const int cyi = max(min(imy, H - 1), 0);
+      const int cxi = max(min(imx, W - 1), 0);
+      const int ii = W * cyi + cxi;
+      const uint16_t draw = __ldg(S.depth + ii);
+      const uint8_t *p8 = S.bgr + 3 * (size_t)ii;
+      const uint8_t cr = __ldg(p8 + 2), cg = __ldg(p8 + 1), cbl = __ldg(p8 + 0);
+      const float cw = S.conf ? __ldg(S.conf + ii) : 1.0f;
+      const float h = __fmul_rz(S.scaling, (float)draw);
+      const float dInc = __fsub_rz(len, __fmul_rz(__fmul_rz(len, rc), h));
+      const bool msk = pz > 0.0f && imy < H && imy > -1 && imx < W && imx > -1 && h < S.maxcam;
+      const float front = dInc < DIST_W_EPS ? 1.0f : 0.0f;
+      const float back = (dInc >= DIST_W_EPS && dInc < thrW) ? 1.0f : 0.0f;
+      const float fall = __fmul_rz(__fsub_rz(thrW, dInc), rcp_upd<RCP_HOST>(__fsub_rz(thrW, DIST_W_EPS), rtab, rshift));
+      float wInc = msk ? __fadd_rz(front, __fmul_rz(fall, back)) : 0.0f;
+      if (S.conf) wInc = __fmul_rz(wInc, cw);
+      const float wNew = __fadd_rz(wAcc, wInc);
+      const float factor = rcp_upd<RCP_HOST>(__fadd_rz(wNew, wNew <= 0.0f ? 1.0f : 0.0f), rtab, rshift);
+      float tr = dInc < thrD ? dInc : thrD;
+      const float lo = -thrD;
+      tr = tr > lo ? tr : lo;
+      const float add = msk ? __fmul_rz(tr, wInc) : 0.0f;
+      const float dNew = __fmul_rz(__fadd_rz(__fmul_rz(dAcc, wAcc), add), factor);
+      const float inc[3] = {__fmul_rz((float)cr, COLOR_MUL), __fmul_rz((float)cg, COLOR_MUL),
+                            __fmul_rz((float)cbl, COLOR_MUL)};
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        float val = __fmul_rz(__fadd_rz(__fmul_rz((float)acc[c], wAcc), __fmul_rz(inc[c], wInc)), factor);
+        val = val < 65280.0f ? val : 65280.0f;
+        acc[c] = (uint16_t)__float2int_rz(val);
+      }
+      // the state as the next frame would load it
+      if (FP16) {
+        dAcc = __half2float(__float2half_rn(dNew));
+        wAcc = __half2float(__float2half_rn(wNew));
+      } else {
+        dAcc = dNew;
+        wAcc = wNew;
+      }
+    }
+    if (FP16) {
+      fb.sdf16[vi] = __float2half_rn(dAcc);
+      fb.wgt16[vi] = __float2half_rn(wAcc);
+    } else {
+      fb.sdf[vi] = dAcc;
+      fb.wgt[vi] = wAcc;
+    }
+    cb[0] = acc[0];
+    cb[512] = acc[1];
+    cb[1024] = acc[2];
+    if (v == 0) fb.mask[brick] = 0u;  // the next pass starts from an empty mask
+    __syncthreads();                   // (shared state of this brick reused by the next)
+  }
+  if (blockIdx.x == 0 && v == 0) atomicAdd(fb.total, (unsigned long long)total);
+}
+
+void launch_fuse_multi(const FuseBatch &fb, int storage, bool rcp_host, int grid, cudaStream_t s) {
+  if (grid <= 0) return;
+  note_launch();
+  if (storage == 1) {
+    if (rcp_host) k_fuse_multi<true, true><<<grid, 512, 0, s>>>(fb);
+    else k_fuse_multi<true, false><<<grid, 512, 0, s>>>(fb);
+  } else {
+    if (rcp_host) k_fuse_multi<false, true><<<grid, 512, 0, s>>>(fb);
+    else k_fuse_multi<false, false><<<grid, 512, 0, s>>>(fb);
   }
 }
 
@@ -294,7 +454,9 @@ bool build_rcp_table(std::vector<uint32_t> &tab, int &shift) {
 
 cudaError_t prewarm_fuse_kernels() {
   const void *fns[] = {(const void *)k_fuse<false, false, 1, 4>, (const void *)k_fuse<false, true, 1, 4>,
-                       (const void *)k_fuse<true, false, 1, 4>,  (const void *)k_fuse<true, true, 1, 4>};
+                       (const void *)k_fuse<true, false, 1, 4>,  (const void *)k_fuse<true, true, 1, 4>,
+                       (const void *)k_fuse_multi<false, false>, (const void *)k_fuse_multi<false, true>,
+                       (const void *)k_fuse_multi<true, false>,  (const void *)k_fuse_multi<true, true>};
   for (const void *f : fns) {
     cudaFuncAttributes a;
     cudaError_t e = cudaFuncGetAttributes(&a, f);

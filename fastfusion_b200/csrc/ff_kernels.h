@@ -52,7 +52,61 @@ struct MapFrame {
   uint32_t branches_init;
   // iterations after which a device-side wait of this frame gives up
   uint32_t spin_limit;
+  // Deferred voxel update (upd_mask non-null): the leaf finalisation marks the
+  // frame's queued bricks with bit upd_slot in upd_mask and appends bricks
+  // not yet marked to upd_list (count in *upd_count); one k_fuse_multi pass
+  // later updates every listed brick with all its marked frames in order.
+  uint32_t *upd_mask, *upd_list, *upd_count;
+  int32_t upd_slot;
 };
+
+// Whether a frame's voxel update must not run with the others: an allocation
+// error or a failed confidence network (the frame is not fused), or the
+// volume must grow first (the host grows it and updates the frame itself).
+// Mirrors the host's test after the traversal.
+__device__ __forceinline__ bool fuse_deferred(const MapFrame &F) {
+  const Counters *c = F.cnt;
+  if ((c->error & ERR_FRAME_FAILED) || c->cnn_error) return true;
+  const uint32_t leaves = F.leaves_before + c->pending;
+  const uint32_t branches = min(c->branches_used, F.branches_max);
+  const int n = (int)F.n;
+  const bool outside = c->box_min[0] < 0 || c->box_min[1] < 0 || c->box_min[2] < 0 || c->box_max[0] >= n ||
+                       c->box_max[1] >= n || c->box_max[2] >= n;
+  return leaves < F.leaves_max && branches < F.branches_max && outside;
+}
+
+// One frame of a deferred update: what the voxel update of that frame reads.
+struct FuseSlot {
+  CamF q;                // voxel grid -> camera, as of the frame
+  const uint16_t *depth;
+  const uint8_t *bgr;
+  const float *conf;     // learned confidence, or null
+  int W, H;
+  float scaling, maxcam;
+};
+
+constexpr int FUSE_SLOTS_MAX = 32;      // frames one deferred pass takes (bits of upd_mask)
+constexpr int FUSE_SLOTS_DEFAULT = 16;
+
+// A deferred update pass over one map: every brick of list[0, *count) with
+// the frames of its mask bits, in order (a kernel parameter).
+struct FuseBatch {
+  const ushort4 *leaf;
+  float *sdf, *wgt;
+  __half *sdf16, *wgt16;
+  uint16_t *col;
+  uint32_t *mask;
+  const uint32_t *list, *count;
+  unsigned long long *total;  // bricks of all passes so far (device counter)
+  const uint32_t *rcp_tab;
+  int rcp_shift;
+  float scale, thr;
+  int nslots;
+  FuseSlot s[FUSE_SLOTS_MAX];
+};
+
+// Launch the deferred update pass (grid: blocks of 512 threads).
+void launch_fuse_multi(const FuseBatch &fb, int storage, bool rcp_host, int grid, cudaStream_t s);
 
 constexpr int BATCH_MAX = 32;
 

@@ -54,7 +54,8 @@ class ff_stats(ctypes.Structure):
                 ("mesh_faces", ctypes.c_uint64), ("mesh_cells", ctypes.c_uint64),
                 ("mesh_cells_dirty", ctypes.c_uint64), ("processed_pixels", ctypes.c_uint32),
                 ("new_leaves", ctypes.c_uint32), ("dedupe_rounds", ctypes.c_uint32),
-                ("graph_replays", ctypes.c_uint32)]
+                ("graph_replays", ctypes.c_uint32), ("update_batch", ctypes.c_uint32),
+                ("fused_bricks", ctypes.c_uint64), ("fused_frame_bricks", ctypes.c_uint64)]
 
 
 class ff_tuning(ctypes.Structure):
@@ -73,6 +74,7 @@ SIGNATURES = {
     "ff_set_tuning": (_i32, [_vp, ctypes.POINTER(ff_tuning)]),
     "ff_set_shard": (_i32, [_vp, _i32, _i32]),
     "ff_set_spin_limit": (_i32, [_vp, _u32]),
+    "ff_set_update_batch": (_i32, [_vp, _i32]),
     "ff_inject_error": (_i32, [_vp, _i32]),
     "ff_add_map_u16": (_i32, [_vp, _vp, _i32, _i32, _sz, _vp, _sz, _vp, _vp, _vp, _f32, _f32, _vp]),
     "ff_add_map_u16_device": (_i32, [_vp, _vp, _vp, _i32, _i32, _vp, _vp, _vp, _f32, _f32, _vp]),
@@ -424,6 +426,11 @@ class FusionMipMapCPU:
         """Make this map part `shard` of `shards` of a larger map (brick
         ownership by a hash of each brick's key); before the first frame."""
         self._check(self._L.ff_set_shard(self._h, int(shard), int(shards)))
+
+    def set_update_batch(self, frames: int = 16):
+        """Frames whose voxel update waits for one pass over their bricks
+        (1 = every frame updated by itself); results are the same either way."""
+        self._check(self._L.ff_set_update_batch(self._h, int(frames)))
 
     def set_spin_limit(self, iterations: int = SPIN_LIMIT_DEFAULT):
         """Bound of the device-side waits of this map's frames (polling

@@ -79,6 +79,11 @@ typedef struct ff_stats {
   uint32_t new_leaves;         /* leaves allocated by the last frame */
   uint32_t dedupe_rounds;      /* rounds the last frame's de-duplication took to settle */
   uint32_t graph_replays;      /* batched calls led by this map that replayed a recorded CUDA graph */
+  uint32_t update_batch;       /* frames one deferred voxel-update pass takes (ff_set_update_batch) */
+  uint64_t fused_bricks;       /* bricks read and written by the voxel updates so far (a pass counts a brick once,
+                                  whatever the number of its frames; as of the last finished pass) */
+  uint64_t fused_frame_bricks; /* queued bricks summed over the frames updated so far (the reference reads and
+                                  writes each of them once per frame) */
 } ff_stats;
 
 /* Create a map.  Replaces `new FusionMipMapCPU(0,0,0,scale,threshold,0,color)`
@@ -109,10 +114,15 @@ ff_status ff_add_map_u16(ff_handle *h, const uint16_t *depth, int width, int hei
 
 /* Same as ff_add_map_u16 with depth/bgr already in device memory (tightly
  * packed).  No host<->device copy of the images.  The call returns once the
- * frame's bricks are counted; the placement of its new bricks and its voxel
- * update may still be running on a second stream of the map (every later call
- * on this handle is ordered after them), so the device images must stay
- * unchanged until the next call on this handle returns or ff_sync(h). */
+ * frame's bricks are counted; the placement of its new bricks may still be
+ * running on a second stream of the map (every later call on this handle is
+ * ordered after it), and its voxel update is deferred (ff_set_update_batch).
+ * The images are read by the call itself (and copied for the deferred
+ * update), so they are free when it returns; they must be ready in the order
+ * of the map's stream (ff_set_stream).  With deferral off
+ * (ff_set_update_batch(h, 1)) the update runs on the second stream and reads
+ * the images: they must then stay unchanged until the next call on this
+ * handle returns or ff_sync(h). */
 ff_status ff_add_map_u16_device(ff_handle *h, const uint16_t *d_depth, const uint8_t *d_bgr, int width, int height,
                                 const double K[4], const double R[9], const double t[3], float scaling,
                                 float maxcam, int32_t *queued);
@@ -169,6 +179,23 @@ ff_status ff_set_shard(ff_handle *h, int shard, int shards);
  * or a batch whose maps[0] it is). */
 ff_status ff_set_tuning(ff_handle *h, const ff_tuning *t);
 
+/* Frames whose voxel update is deferred to one pass (at most
+ * FF_UPDATE_BATCH_MAX, default 16; 1 = every frame updated by itself).  The
+ * reference updates each queued brick once per frame
+ * (update_functions.cpp:1633-1732); here a single-map frame only marks its
+ * bricks, and one pass later reads and writes each marked brick once,
+ * applying its frames in order with the same operations -- the voxel values
+ * are bit-identical to frame-by-frame updates.  The pass runs when the batch
+ * is full, before the volume grows, and before anything reads or replaces
+ * voxel state (ff_update_meshes, ff_get_bricks, ff_set_bricks, ff_set_state,
+ * ff_raycast_depth, ff_sync, ff_set_stream, a batched call).  The waiting
+ * frames' images are copies the map keeps (a ring of frames x W x H x 5
+ * bytes, x 9 with the learned weight), so device images given to
+ * ff_add_map_u16_device are free when the call returns.  No counterpart in
+ * the reference. */
+#define FF_UPDATE_BATCH_MAX 32
+ff_status ff_set_update_batch(ff_handle *h, int frames);
+
 /* Bound of every device-side wait of this map's frames (the grid barriers of
  * the de-duplication, the lock wait of the octree insert), in polling
  * iterations; default FF_SPIN_LIMIT_DEFAULT.  A wait that runs out sets an
@@ -224,9 +251,10 @@ ff_status ff_get_mesh_cells(ff_handle *h, int32_t *cells, int64_t *ranges);
  * cells are staged in a fixed device buffer that is part of the library
  * (FF_NOALLOC_MAX_CELLS cells, 5.8 MB, held on every GPU that loads the
  * library until the process exits); the call allocates nothing.  A mesh with
- * more cells is rejected with FF_ERR_BAD_ARG and a message.  The first call
- * on a device looks up the buffer's device address; make that first call
- * before any stream capture.  Every call on one device uses the same buffer,
+ * more cells is rejected with FF_ERR_BAD_ARG and a message, and nothing is
+ * written.  Every call looks up the buffer's device address on the current
+ * device (the first call on a device may load the library's device code:
+ * make that first call before any stream capture).  Every call on one device uses the same buffer,
  * so calls whose GPU work overlaps (maps on different streams) race: order
  * them on the host or on one stream. */
 #define FF_NOALLOC_MAX_CELLS 65536

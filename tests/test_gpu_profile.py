@@ -8,10 +8,14 @@ from tests.helpers import MAXCAM, SCALING, circle_frames
 pytestmark = pytest.mark.gpu
 
 
-def test_profile_counts_match_the_work(lib_built):
+@pytest.mark.parametrize("batch", [16, 1])
+def test_profile_counts_match_the_work(lib_built, batch):
+    """batch 16: the frames' voxel updates wait for one pass at updateMeshes;
+    batch 1: every frame is updated by itself."""
     from fastfusion_b200 import fusion as ff
     K, frames = circle_frames(0, 6, 160, 120)
     m = ff.FusionMipMapCPU(0, 0, 0, 0.005, 0.01, 0, True, leaves_max=271420, branches_max=4793488, rcp="exact")
+    m.set_update_batch(batch)
     m.profile(True)
     own0, lib0 = ff.kernel_launches()
     queued = 0
@@ -21,12 +25,19 @@ def test_profile_counts_match_the_work(lib_built):
     own1, lib1 = ff.kernel_launches()
     prof = m.profile_read()
     assert set(prof) == set(ff.FusionMipMapCPU.PROFILE_STAGES)
-    # one launch of each per-frame stage per frame; the fuse bytes are the
-    # 14,336 B of every queued FP32 brick
-    for stage in ("dedupe", "insert", "fuse"):
+    # one launch of each per-frame stage per frame, one update pass per batch;
+    # the fuse bytes are the 14,336 B of every queued FP32 brick of every frame
+    for stage in ("dedupe", "insert", "finalize"):
         assert prof[stage][2] == len(frames), (stage, prof[stage])
         assert prof[stage][0] > 0.0
+    assert prof["fuse"][2] == (1 if batch > 1 else len(frames))
+    assert prof["fuse"][0] > 0.0
     assert prof["fuse"][1] == pytest.approx(14336.0 * queued)
+    st = m.stats()
+    assert st["fused_frame_bricks"] == queued
+    if batch > 1:
+        # the pass reads and writes each brick once: fewer than the frame-bricks
+        assert 0 < st["fused_bricks"] < queued
     for stage in ("mesh_cells", "mesh_count", "mesh_emit"):
         assert prof[stage][2] == 1
     assert prof["mesh_count"][1] > 0
