@@ -817,9 +817,11 @@ def run_corridor(a):
     m = ff.FusionMipMapCPU(0, 0, 0, VOXEL, THRESHOLD, 0, True, storage=a.storage, rcp=a.rcp,
                            pool_bytes=int(a.pool_gb * 1e9), device=local)
     if world > 1:
-        # one map over all GPUs: rank r holds the bricks whose key hashes to r
-        # (every rank is given every frame; no data-path collective)
+        # one map over all GPUs: every rank is given every frame and holds the
+        # whole octree; rank r updates the bricks and meshes the cells whose
+        # keys hash to r, after a halo all-gather of the changed bricks
         m.set_shard(rank, world)
+    halo_bytes = [0]
     free1, _ = torch.cuda.mem_get_info(dev)
     m.set_stream(stream.cuda_stream)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
@@ -832,6 +834,9 @@ def run_corridor(a):
         base = (s_ // CHUNK) * CHUNK * FRAMES_PER_STEP
         for i in range(s_ * FRAMES_PER_STEP, (s_ + 1) * FRAMES_PER_STEP):
             m.addMapDevice(depth[i - base].data_ptr(), bgr[i - base].data_ptr(), W, H, cams[i], SCALING, MAXCAM)
+        if world > 1:
+            from fastfusion_b200.shard import halo_exchange
+            halo_bytes[0] += halo_exchange(m, dev)["bytes_sent"]
         m.updateMeshes()
 
     for s_ in range(a.warmup):
@@ -855,7 +860,7 @@ def run_corridor(a):
     ms = [e0.elapsed_time(e1) for e0, e1 in ev]
     # the whole map's frames over the slowest part's device time
     ms_total = reduce_over_ranks(float(sum(ms)), "max", dev)
-    leaves_all = int(reduce_over_ranks(float(m.stats()["leaves_used"]), "sum", dev))
+    leaves_all = int(m.stats()["leaves_used"])  # every part holds the whole leaf table
     stages = m.profile_read()
     st = m.stats()
     peak, peak_kind = measured_hbm_peak()
@@ -892,6 +897,7 @@ def run_corridor(a):
                  "peak_source": peak_kind, "avg_launch_us": round(1e3 * fms / fl, 2) if fl else 0},
         "stages": {k: {"ms": round(v[0], 3), "launches": v[2]} for k, v in stages.items()},
         "render_s": round(render_s[0], 1),
+        "halo_bytes_sent_rank0": halo_bytes[0],
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -429,22 +429,6 @@ __device__ __forceinline__ uint32_t wait_unlocked(uint32_t *tree, uint32_t ptr, 
   return cur;
 }
 
-// Whether this part of a sharded map keeps the brick of edge `half` voxels
-// at grid origin (ox, oy, oz): a hash of its origin in units of its edge (in
-// coordinates grow() does not move) and of its edge.
-__device__ __forceinline__ bool owns_brick(const MapFrame &F, uint32_t ox, uint32_t oy, uint32_t oz, uint32_t half) {
-  if (F.shards <= 1) return true;
-  const int lg = 31 - __clz(half);
-  const uint32_t kx = (uint32_t)(((int32_t)ox - F.shift[0]) >> lg);
-  const uint32_t ky = (uint32_t)(((int32_t)oy - F.shift[1]) >> lg);
-  const uint32_t kz = (uint32_t)(((int32_t)oz - F.shift[2]) >> lg);
-  uint32_t hsh = kx * 73856093u ^ ky * 19349663u ^ kz * 83492791u ^ (uint32_t)lg * 2654435761u;
-  hsh ^= hsh >> 16;
-  hsh *= 0x45d9f3bu;
-  hsh ^= hsh >> 16;
-  return hsh % F.shards == F.shard;
-}
-
 // One processed pixel of the frame F (voxel key v): bounding-box growth,
 // then (inside the volume) the descent of queryPointDepthSingle_func_subtree:
 // queue the existing coarser leaves on the path, allocate missing branches,
@@ -468,15 +452,6 @@ __device__ __forceinline__ uint32_t insert_pixel(const MapFrame &F, int i, int4 
   if (!(v.x >= 0 && (uint16_t)v.x < n && v.y >= 0 && (uint16_t)v.y < n && v.z >= 0 && (uint16_t)v.z < n)) return 0;
   const uint32_t x = (uint16_t)v.x, y = (uint16_t)v.y, z = (uint16_t)v.z;
   const uint32_t target = (uint32_t)v.w;
-  // sharded map: the pixel's own brick (the level the descent stops at) is
-  // created only by its owner; other parts only queue the coarser bricks
-  // they hold on its path and create no branch for it
-  bool owned = true;
-  if (F.shards > 1) {
-    uint32_t lh = (uint16_t)(n >> 1);
-    while ((lh >> 1) >= target) lh >>= 1;
-    owned = owns_brick(F, x & ~(lh - 1u), y & ~(lh - 1u), z & ~(lh - 1u), lh);
-  }
   uint32_t ox = 0, oy = 0, oz = 0;
   uint32_t half = (uint16_t)(n >> 1);
   uint32_t branch = 0;
@@ -489,7 +464,6 @@ __device__ __forceinline__ uint32_t insert_pixel(const MapFrame &F, int i, int4 
     if (leaf < leaves_max) queue_leaf(leaf, frame, stamp, queue, cnt);
     uint32_t child = ld_tree(tree + ptr);
     if (child == BRANCHINIT) {
-      if (!owned) return probed;
       uint32_t old = atomicCAS(tree + ptr, BRANCHINIT, LOCKED);
       if (old == BRANCHINIT) {
         uint32_t nb = atomicAdd(&cnt->branches_used, 16u);
@@ -518,7 +492,6 @@ __device__ __forceinline__ uint32_t insert_pixel(const MapFrame &F, int i, int4 
   probed++;
   uint32_t cur = ld_tree(tree + ptr);
   if (cur == BRANCHINIT) {
-    if (!owned) return probed;
     uint32_t old = atomicCAS(tree + ptr, BRANCHINIT, LOCKED);
     if (old == BRANCHINIT) {
       uint32_t rec = atomicAdd(&cnt->pending, 1u);
@@ -741,6 +714,8 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc
     const uint32_t bit = 1u << F.upd_slot;
     for (uint32_t j = t; j < nq; j += FIN_THREADS) {
       const uint32_t b = queue[j];
+      // a part of a sharded map updates the bricks it owns
+      if (F.shards > 1 && !owns_brick(F, leaf[b])) continue;
       // (the queue holds each brick once, so the old mask lacks this bit)
       if (atomicOr(&F.upd_mask[b], bit) == 0u) F.upd_list[atomicAdd(F.upd_count, 1u)] = b;
     }

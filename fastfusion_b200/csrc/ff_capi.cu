@@ -125,6 +125,8 @@ struct ff_handle {
   // (ff_inject_error)
   uint32_t spin_limit = SPIN_LIMIT;
   int inject = 0;
+  uint32_t halo_since = 0;           // frames whose changes the last halo export covered
+  uint32_t *h_halo_count = nullptr;  // pinned: the export's record count
 
   // Deferred voxel update: a single-map frame's update waits for one pass
   // (k_fuse_multi) over the union of the bricks of up to upd_batch frames,
@@ -606,6 +608,7 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
     if (alloc(&h->d_upd_mask, L) != cudaSuccess || alloc(&h->d_upd_list, L) != cudaSuccess ||
         alloc(&h->d_upd_count, 1) != cudaSuccess || alloc(&h->d_upd_total, 1) != cudaSuccess ||
         cudaMallocHost((void **)&h->h_upd_total, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMallocHost((void **)&h->h_halo_count, sizeof(uint32_t)) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_ring_free, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_copy, cudaEventDisableTiming) != cudaSuccess) {
       fail(FF_ERR_OOM_POOL, "deferred update");
@@ -678,6 +681,7 @@ ff_status ff_destroy(ff_handle *h) {
     if (h->ev_fuse[k]) cudaEventDestroy(h->ev_fuse[k]);
   }
   if (h->h_upd_total) cudaFreeHost(h->h_upd_total);
+  if (h->h_halo_count) cudaFreeHost(h->h_halo_count);
   if (h->ev_ring_free) cudaEventDestroy(h->ev_ring_free);
   if (h->ev_copy) cudaEventDestroy(h->ev_copy);
   if (h->ev_fin) cudaEventDestroy(h->ev_fin);
@@ -705,6 +709,53 @@ ff_status ff_set_shard(ff_handle *h, int shard, int shards) {
   if (h->frames || h->n) return set_err(h, FF_ERR_BAD_ARG, "ff_set_shard: set before the first frame");
   h->shard = (uint32_t)shard;
   h->shards = (uint32_t)shards;
+  return FF_OK;
+}
+
+ff_status ff_halo_export(ff_handle *h, void *d_records, uint64_t capacity, uint64_t *n_records,
+                         uint64_t *record_bytes) {
+  if (!h || !n_records) return FF_ERR_BAD_ARG;
+  CK(cudaSetDevice(h->cfg.device));
+  const bool fp16 = h->cfg.storage == FF_STORAGE_FP16;
+  if (record_bytes) *record_bytes = halo_record_bytes(fp16);
+  // the changes include the waiting frames' updates; the pass's brick list is
+  // free once it has run
+  FCK(settle(h));
+  cudaStream_t s = h->stream;
+  const uint32_t nl = std::min(h->leaves_used, h->cfg.leaves_max);
+  CK(cudaMemsetAsync(h->d_upd_count, 0, sizeof(uint32_t), s));
+  launch_halo_select(h->d_leaf, h->d_stamp, nl, h->halo_since, h->shard, h->shards, h->shift, h->d_upd_list,
+                     h->d_upd_count, s);
+  CK(cudaMemcpyAsync(h->h_halo_count, h->d_upd_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  const uint32_t n = *h->h_halo_count;
+  *n_records = n;
+  if (d_records) {
+    if (n > capacity) {
+      CK(cudaMemsetAsync(h->d_upd_count, 0, sizeof(uint32_t), s));
+      CK(cudaStreamSynchronize(s));
+      return set_err(h, FF_ERR_BAD_ARG, "ff_halo_export: " + std::to_string(n) + " records, room for " +
+                                            std::to_string(capacity));
+    }
+    launch_halo_pack(h->d_upd_list, n, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col, d_records, fp16,
+                     h->sm_count * 4, s);
+    CK(cudaGetLastError());
+    h->halo_since = h->frames;
+  }
+  // the list belongs to the deferred update again
+  CK(cudaMemsetAsync(h->d_upd_count, 0, sizeof(uint32_t), s));
+  CK(cudaStreamSynchronize(s));
+  return FF_OK;
+}
+
+ff_status ff_halo_import(ff_handle *h, const void *d_records, uint64_t n_records) {
+  if (!h || (n_records && !d_records)) return FF_ERR_BAD_ARG;
+  CK(cudaSetDevice(h->cfg.device));
+  FCK(settle(h));
+  launch_halo_unpack(d_records, n_records, h->cfg.leaves_max, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
+                     h->cfg.storage == FF_STORAGE_FP16, h->sm_count * 4, h->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->stream));
   return FF_OK;
 }
 
@@ -1732,6 +1783,9 @@ ff_status ff_update_meshes(ff_handle *h, int *updated) {
   in.cnt = h->d_cnt;
   in.h_cnt = h->h_cnt;
   in.prof = &h->prof;
+  in.shard = h->shard;
+  in.shards = h->shards;
+  for (int r = 0; r < 3; r++) in.shift[r] = h->shift[r];
   std::string err;
   int rc = mesh_update(h->mesh, in, h->stream, err);
   if (rc != 0) return set_err(h, (ff_status)rc, err);

@@ -83,6 +83,25 @@ struct CamF {
   float fx, fy, cx, cy;
 };
 
+// Ownership in a sharded map (ff_set_shard): every part holds the whole
+// octree and leaf table (all parts run the same allocation), updates the
+// voxels of the bricks it owns and meshes the cells it owns.  Both are a hash
+// of the object's origin in units of its edge, in coordinates that grow()
+// does not move (shift: the voxels the grid has been moved by), and of its
+// edge (and, for a cell, its type).
+__device__ __forceinline__ uint32_t shard_hash(int32_t ox, int32_t oy, int32_t oz, uint32_t edge, uint32_t kind,
+                                               const int32_t *shift) {
+  const int lg = 31 - __clz(edge);
+  const uint32_t kx = (uint32_t)((ox - shift[0]) >> lg);
+  const uint32_t ky = (uint32_t)((oy - shift[1]) >> lg);
+  const uint32_t kz = (uint32_t)((oz - shift[2]) >> lg);
+  uint32_t hsh = kx * 73856093u ^ ky * 19349663u ^ kz * 83492791u ^ (uint32_t)lg * 2654435761u ^ kind * 40503u;
+  hsh ^= hsh >> 16;
+  hsh *= 0x45d9f3bu;
+  hsh ^= hsh >> 16;
+  return hsh;
+}
+
 // Barrier over all blocks of a cooperative launch (every block resident).
 // bar[0] counts arrivals, bar[1] is the generation; both start at zero.
 // A wait that exceeds `limit` iterations sets err_bit in *err and stops

@@ -186,8 +186,11 @@ __global__ void __launch_bounds__(512 * BPC, MINB) k_fuse(const BatchDesc *__res
     while (b >= end[m]) m++;
     const MapFrame &F = bd->f[m];
     const uint32_t local = b - (m ? end[m - 1] : 0u);
-    fuse_brick<FP16, RCP_HOST>(F.queue[local], F.leaf, F.sdf, F.wgt, F.sdf16, F.wgt16, F.col, F.depth, F.bgr, F.W,
-                               F.H, sq[m], F.scale, F.thr, F.scaling, F.maxcam, F.rcp_tab, F.rcp_shift, F.conf, v);
+    const uint32_t brick = F.queue[local];
+    // a part of a sharded map updates the bricks it owns
+    if (F.shards > 1 && !owns_brick(F, F.leaf[brick])) continue;
+    fuse_brick<FP16, RCP_HOST>(brick, F.leaf, F.sdf, F.wgt, F.sdf16, F.wgt16, F.col, F.depth, F.bgr, F.W, F.H, sq[m],
+                               F.scale, F.thr, F.scaling, F.maxcam, F.rcp_tab, F.rcp_shift, F.conf, v);
   }
 }
 
@@ -365,6 +368,124 @@ void launch_fuse_multi(const FuseBatch &fb, int storage, bool rcp_host, int grid
     if (rcp_host) k_fuse_multi<false, true><<<grid, 512, 0, s>>>(fb);
     else k_fuse_multi<false, false><<<grid, 512, 0, s>>>(fb);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Halo exchange of a sharded map: the bricks a part owns whose voxels changed
+// since its last export, as records (uint32 leaf index, 12 bytes of padding,
+// then SDF, weight and colour planes as the pool stores them), and their
+// import into another part's pool.
+// ---------------------------------------------------------------------------
+
+size_t halo_record_bytes(bool fp16) { return 16 + 512 * (fp16 ? 4 : 8) + 512 * 6; }
+
+__global__ void k_halo_select(const ushort4 *__restrict__ leaf, const uint32_t *__restrict__ stamp, uint32_t nleaves,
+                              uint32_t since, uint32_t shard, uint32_t shards, int3 shift, uint32_t *list,
+                              uint32_t *count) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool take = false;
+  if (i < nleaves && stamp[i] > since) {
+    const ushort4 p = leaf[i];
+    const int32_t sh[3] = {shift.x, shift.y, shift.z};
+    take = shards <= 1 || shard_hash(p.x, p.y, p.z, (uint32_t)p.w * 8u, 0u, sh) % shards == shard;
+  }
+  // one claim per warp
+  const unsigned b = __ballot_sync(0xffffffffu, take);
+  if (!b) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(b) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(count, (uint32_t)__popc(b));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (take) list[base + __popc(b & ((1u << lane) - 1u))] = i;
+}
+
+template <bool FP16>
+__global__ void __launch_bounds__(512) k_halo_pack(const uint32_t *__restrict__ list, uint32_t n,
+                                                   const float *__restrict__ sdf, const float *__restrict__ wgt,
+                                                   const __half *__restrict__ sdf16,
+                                                   const __half *__restrict__ wgt16,
+                                                   const uint16_t *__restrict__ col, uint8_t *out, size_t rec) {
+  const int t = threadIdx.x;
+  for (uint32_t r = blockIdx.x; r < n; r += gridDim.x) {
+    const uint32_t b = list[r];
+    uint8_t *p = out + (size_t)r * rec;
+    if (t < 4) reinterpret_cast<uint32_t *>(p)[t] = t == 0 ? b : 0u;
+    const size_t vi = (size_t)b * 512 + t;
+    uint8_t *q = p + 16;
+    if (FP16) {
+      reinterpret_cast<__half *>(q)[t] = sdf16[vi];
+      reinterpret_cast<__half *>(q + 1024)[t] = wgt16[vi];
+      q += 2048;
+    } else {
+      reinterpret_cast<float *>(q)[t] = sdf[vi];
+      reinterpret_cast<float *>(q + 2048)[t] = wgt[vi];
+      q += 4096;
+    }
+    const uint16_t *cb = col + (size_t)b * 1536;
+    uint16_t *cq = reinterpret_cast<uint16_t *>(q);
+    cq[t] = cb[t];
+    cq[512 + t] = cb[512 + t];
+    cq[1024 + t] = cb[1024 + t];
+  }
+}
+
+template <bool FP16>
+__global__ void __launch_bounds__(512) k_halo_unpack(const uint8_t *in, uint64_t n, uint32_t leaves_max, float *sdf,
+                                                     float *wgt, __half *sdf16, __half *wgt16, uint16_t *col,
+                                                     size_t rec) {
+  const int t = threadIdx.x;
+  for (uint64_t r = blockIdx.x; r < n; r += gridDim.x) {
+    const uint8_t *p = in + (size_t)r * rec;
+    const uint32_t b = reinterpret_cast<const uint32_t *>(p)[0];
+    if (b >= leaves_max) continue;  // not a brick of this map's pool
+    const size_t vi = (size_t)b * 512 + t;
+    const uint8_t *q = p + 16;
+    if (FP16) {
+      sdf16[vi] = reinterpret_cast<const __half *>(q)[t];
+      wgt16[vi] = reinterpret_cast<const __half *>(q + 1024)[t];
+      q += 2048;
+    } else {
+      sdf[vi] = reinterpret_cast<const float *>(q)[t];
+      wgt[vi] = reinterpret_cast<const float *>(q + 2048)[t];
+      q += 4096;
+    }
+    const uint16_t *cq = reinterpret_cast<const uint16_t *>(q);
+    uint16_t *cb = col + (size_t)b * 1536;
+    cb[t] = cq[t];
+    cb[512 + t] = cq[512 + t];
+    cb[1024 + t] = cq[1024 + t];
+  }
+}
+
+void launch_halo_select(const ushort4 *leaf, const uint32_t *stamp, uint32_t nleaves, uint32_t since,
+                        uint32_t shard, uint32_t shards, const int32_t shift[3], uint32_t *list, uint32_t *count,
+                        cudaStream_t s) {
+  if (!nleaves) return;
+  note_launch();
+  k_halo_select<<<(nleaves + 255) / 256, 256, 0, s>>>(leaf, stamp, nleaves, since, shard, shards,
+                                                      make_int3(shift[0], shift[1], shift[2]), list, count);
+}
+
+void launch_halo_pack(const uint32_t *list, uint32_t n, const float *sdf, const float *wgt, const __half *sdf16,
+                      const __half *wgt16, const uint16_t *col, void *out, bool fp16, int grid, cudaStream_t s) {
+  if (!n) return;
+  note_launch();
+  const size_t rec = halo_record_bytes(fp16);
+  if (fp16)
+    k_halo_pack<true><<<grid, 512, 0, s>>>(list, n, sdf, wgt, sdf16, wgt16, col, (uint8_t *)out, rec);
+  else
+    k_halo_pack<false><<<grid, 512, 0, s>>>(list, n, sdf, wgt, sdf16, wgt16, col, (uint8_t *)out, rec);
+}
+
+void launch_halo_unpack(const void *in, uint64_t n, uint32_t leaves_max, float *sdf, float *wgt, __half *sdf16,
+                        __half *wgt16, uint16_t *col, bool fp16, int grid, cudaStream_t s) {
+  if (!n) return;
+  note_launch();
+  const size_t rec = halo_record_bytes(fp16);
+  if (fp16)
+    k_halo_unpack<true><<<grid, 512, 0, s>>>((const uint8_t *)in, n, leaves_max, sdf, wgt, sdf16, wgt16, col, rec);
+  else
+    k_halo_unpack<false><<<grid, 512, 0, s>>>((const uint8_t *)in, n, leaves_max, sdf, wgt, sdf16, wgt16, col, rec);
 }
 
 // Block shapes of the voxel update: (bricks per block, blocks per SM the

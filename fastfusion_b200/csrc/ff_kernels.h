@@ -75,6 +75,12 @@ __device__ __forceinline__ bool fuse_deferred(const MapFrame &F) {
   return leaves < F.leaves_max && branches < F.branches_max && outside;
 }
 
+// Whether this part updates the brick at leaf position p (x, y, z, scale).
+__device__ __forceinline__ bool owns_brick(const MapFrame &F, ushort4 p) {
+  if (F.shards <= 1) return true;
+  return shard_hash(p.x, p.y, p.z, (uint32_t)p.w * 8u, 0u, F.shift) % F.shards == F.shard;
+}
+
 // One frame of a deferred update: what the voxel update of that frame reads.
 struct FuseSlot {
   CamF q;                // voxel grid -> camera, as of the frame
@@ -107,6 +113,19 @@ struct FuseBatch {
 
 // Launch the deferred update pass (grid: blocks of 512 threads).
 void launch_fuse_multi(const FuseBatch &fb, int storage, bool rcp_host, int grid, cudaStream_t s);
+
+// Halo exchange of a sharded map (records: uint32 leaf index, 12 bytes of
+// padding, SDF, weight and colour planes as the pool stores them).
+size_t halo_record_bytes(bool fp16);
+// list[0, *count) += the leaves [0, nleaves) whose stamp is after `since` and
+// that this part owns (every leaf when shards <= 1)
+void launch_halo_select(const ushort4 *leaf, const uint32_t *stamp, uint32_t nleaves, uint32_t since,
+                        uint32_t shard, uint32_t shards, const int32_t shift[3], uint32_t *list, uint32_t *count,
+                        cudaStream_t s);
+void launch_halo_pack(const uint32_t *list, uint32_t n, const float *sdf, const float *wgt, const __half *sdf16,
+                      const __half *wgt16, const uint16_t *col, void *out, bool fp16, int grid, cudaStream_t s);
+void launch_halo_unpack(const void *in, uint64_t n, uint32_t leaves_max, float *sdf, float *wgt, __half *sdf16,
+                        __half *wgt16, uint16_t *col, bool fp16, int grid, cudaStream_t s);
 
 constexpr int BATCH_MAX = 32;
 

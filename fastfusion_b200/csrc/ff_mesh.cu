@@ -546,7 +546,18 @@ struct VoxSrc {
   float offset[3];
   float scale;
   unsigned long long *samples;  // count pass: voxel samples read (profiling)
+  // a part of a sharded map meshes the cells it owns (ff_set_shard)
+  uint32_t shard, shards;
+  int32_t shift[3];
 };
+
+// Whether this part meshes cell c: a hash of its origin, size and type in
+// coordinates that grow() does not move (every part has every cell; each
+// cell is meshed by exactly one part).
+__device__ __forceinline__ bool owns_cell(const VoxSrc &m, const Cell &c) {
+  if (m.shards <= 1) return true;
+  return shard_hash(c.o[0], c.o[1], c.o[2], c.size, 1u + c.type, m.shift) % m.shards == m.shard;
+}
 
 __device__ __forceinline__ size_t vox_index(const VoxSrc &m, uint32_t leaf, uint16_t lx, uint16_t ly, uint16_t lz) {
   // the reference computes the index in uint16 voxel coordinates and may
@@ -948,6 +959,11 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
     // emit: a cell that the count pass found without vertices writes nothing
     if (EMIT && out[cid].nv == 0) continue;
     const Cell c = cells[cid];
+    if (!owns_cell(m, c)) {
+      // another part meshes it
+      if (!EMIT && lane == 0) out[cid] = CellOut{0u, 0u};
+      continue;
+    }
     const CellGeom G = cell_geom(m, c);
     if (G.empty) {
       if (!EMIT && lane == 0) out[cid] = CellOut{0u, 0u};
@@ -1131,6 +1147,10 @@ __global__ void k_mesh_corner(VoxSrc m, const Cell *__restrict__ cells, uint32_t
   if (i >= (list ? *list_n : ncell)) return;
   const uint32_t cid = list ? list[i] : first + i;
   const Cell c = cells[cid];
+  if (!owns_cell(m, c)) {
+    if (!EMIT) out[cid] = CellOut{0u, 0u};
+    return;
+  }
   int stretch = m.leaf[c.L[0]].w;
   for (int k = 1; k < 7; k++) stretch = max(stretch, (int)m.leaf[c.L[k]].w);
   if (stretch > c.size) {
@@ -1581,6 +1601,9 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   vs.leaves_used = in.leaves_used;
   for (int r = 0; r < 3; r++) vs.offset[r] = in.offset[r];
   vs.scale = in.scale;
+  vs.shard = in.shard;
+  vs.shards = in.shards;
+  for (int r = 0; r < 3; r++) vs.shift[r] = in.shift[r];
   // d_count words 12-13 hold the sample counter (8-byte aligned)
   vs.samples = reinterpret_cast<unsigned long long *>(I.d_count + 12);
   MCK(cudaMemsetAsync(I.d_count + 12, 0, 2 * sizeof(uint32_t), s));

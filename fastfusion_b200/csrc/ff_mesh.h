@@ -30,6 +30,9 @@ struct MeshInputs {
   Counters *cnt;
   Counters *h_cnt;
   Prof *prof;
+  // a part of a sharded map: the cells it meshes (ff_set_shard)
+  uint32_t shard = 0, shards = 1;
+  int32_t shift[3] = {0, 0, 0};
 };
 
 struct MeshState {

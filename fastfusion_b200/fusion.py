@@ -75,6 +75,8 @@ SIGNATURES = {
     "ff_set_shard": (_i32, [_vp, _i32, _i32]),
     "ff_set_spin_limit": (_i32, [_vp, _u32]),
     "ff_set_update_batch": (_i32, [_vp, _i32]),
+    "ff_halo_export": (_i32, [_vp, _vp, _u64, ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
+    "ff_halo_import": (_i32, [_vp, _vp, _u64]),
     "ff_inject_error": (_i32, [_vp, _i32]),
     "ff_add_map_u16": (_i32, [_vp, _vp, _i32, _i32, _sz, _vp, _sz, _vp, _vp, _vp, _f32, _f32, _vp]),
     "ff_add_map_u16_device": (_i32, [_vp, _vp, _vp, _i32, _i32, _vp, _vp, _vp, _f32, _f32, _vp]),
@@ -442,6 +444,24 @@ class FusionMipMapCPU:
         """Make the next frame report a failure as the device would (tests of
         the error paths; 0 cancels)."""
         self._check(self._L.ff_inject_error(self._h, int(what)))
+
+    def halo_count(self) -> tuple[int, int]:
+        """(records, bytes per record) the next halo export would write."""
+        n, rb = ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(self._L.ff_halo_export(self._h, None, 0, ctypes.byref(n), ctypes.byref(rb)))
+        return n.value, rb.value
+
+    def halo_export(self, d_records: int, capacity: int) -> int:
+        """Write this part's changed bricks as records to device memory
+        d_records (room for `capacity`); returns the number written."""
+        n, rb = ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(self._L.ff_halo_export(self._h, ctypes.c_void_p(int(d_records)), int(capacity),
+                                           ctypes.byref(n), ctypes.byref(rb)))
+        return n.value
+
+    def halo_import(self, d_records: int, n_records: int):
+        """Write another part's records (device memory) into this part's pool."""
+        self._check(self._L.ff_halo_import(self._h, ctypes.c_void_p(int(d_records)), int(n_records)))
 
     def sync(self):
         """Wait for the map's outstanding device work (the last voxel update)."""

@@ -162,18 +162,40 @@ typedef struct {
   int graph;
 } ff_tuning;
 
-/* Make this map one of `shards` parts of a larger map (call before its first
- * frame; no counterpart in the reference, which fuses one map on one
- * machine).  Every part is given every frame; a part creates and updates only
- * the bricks whose key -- the brick's origin in units of its own edge,
- * independent of volume growth, and its size -- hashes to `shard`, and
- * queues the coarser bricks it holds on a pixel's path exactly as the whole
- * map would.  The parts' bricks are disjoint and together are the whole
- * map's, each with the whole map's voxel values; the queued counts add up to
- * the whole map's.  Leaf indices and parent links are per part.  Meshing a
- * part covers its own bricks; the cells between bricks of different parts
- * need the other parts' bricks, which this library does not exchange. */
+/* Make this map one of `shards` parts of a larger map, one part per GPU
+ * (call before its first frame; no counterpart in the reference, which fuses
+ * one map on one machine).  Every part is given every frame and holds the
+ * whole map's octree and leaf table (the same allocation as the whole map:
+ * identical leaf indices, queues and counts).  The voxel updates and the
+ * meshing are divided: a part updates the bricks it owns and meshes the mesh
+ * cells it owns, each owner a hash of the object's origin in units of its
+ * edge (in coordinates that volume growth does not move) and of its edge.
+ * Before a part meshes, the bricks the other parts changed must reach it:
+ * each part exports the bricks it owns that changed since its last export
+ * (ff_halo_export), the caller moves the records between the GPUs (an NCCL
+ * all-gather, say: records land in each GPU's own memory) and each part
+ * imports the others' (ff_halo_import).  Each part's mesh then holds the
+ * meshes of its cells, exactly as the whole map meshes them; together the
+ * parts' meshes are the whole map's mesh. */
 ff_status ff_set_shard(ff_handle *h, int shard, int shards);
+
+/* Halo export of a part of a sharded map: the bricks this part owns whose
+ * voxels changed since its last export (with a buffer), as records of
+ * *record_bytes bytes each -- uint32 leaf index, 12 bytes of padding, then
+ * the brick's SDF and weight (float, or half with FP16 storage) and its three
+ * uint16 colour planes, 512 voxels each -- written to device memory d_records
+ * with room for `capacity` records.  With d_records NULL only *n_records is
+ * set (call again with a buffer that large); more records than capacity is
+ * FF_ERR_BAD_ARG and nothing is written.  The waiting voxel updates run first.
+ * On an unsharded map every changed brick is exported. */
+ff_status ff_halo_export(ff_handle *h, void *d_records, uint64_t capacity, uint64_t *n_records,
+                         uint64_t *record_bytes);
+
+/* Halo import: write the bricks of n_records records (as ff_halo_export
+ * writes them, from another part of the same map; device memory) into this
+ * part's pool.  Records whose leaf index lies past this map's pool are
+ * skipped. */
+ff_status ff_halo_import(ff_handle *h, const void *d_records, uint64_t n_records);
 
 /* Set the launch shapes used by calls that this map leads (the map itself,
  * or a batch whose maps[0] it is). */
