@@ -524,11 +524,11 @@ __device__ __forceinline__ uint32_t insert_pixel(const MapFrame &F, int i, int4 
 
 // One thread per pixel of every frame of the batch (each map's pixels padded
 // to whole warps, so a warp never spans two maps).
-__global__ void k_insert(const BatchDesc *__restrict__ bd) {
-  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nmaps = bd->n;
+__global__ void k_insert(const BatchDesc *__restrict__ bd, int m0, int m1) {
+  const int nmaps = min(bd->n, m1);
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x + (m0 ? bd->pix_end[m0 - 1] : 0u);
   if (g >= bd->pix_end[nmaps - 1]) return;
-  int mi = 0;
+  int mi = m0;
   while (mi < nmaps - 1 && g >= bd->pix_end[mi]) mi++;
   const MapFrame &F = bd->f[mi];
   const int i = (int)(g - (mi ? bd->pix_end[mi - 1] : 0u));
@@ -536,9 +536,9 @@ __global__ void k_insert(const BatchDesc *__restrict__ bd) {
   const int4 *__restrict__ vox = F.vox;
   const uint8_t *__restrict__ processed = F.proc;
   Counters *cnt = F.cnt;
-  // a de-duplication that did not complete leaves the frame out: the octree
-  // is not touched, so the map stays as it was
-  if (ld_volatile(&cnt->error) & ERR_DEDUPE_FAILED) return;
+  // a de-duplication that did not complete leaves the frame out, and so does
+  // a sequence halted by an earlier frame: the octree is not touched
+  if (ld_volatile(&cnt->error) & (ERR_DEDUPE_FAILED | ERR_SEQ_HALT)) return;
   bool act = i < npix && processed[i];
   unsigned m = __ballot_sync(0xffffffffu, act);
   if (!act) return;
@@ -550,11 +550,11 @@ __global__ void k_insert(const BatchDesc *__restrict__ bd) {
   if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&cnt->levels, sum);
 }
 
-void launch_insert(const BatchDesc *d_batch, uint32_t total_pix, cudaStream_t s, int block) {
-  if (!total_pix) return;
+void launch_insert(const BatchDesc *d_batch, uint32_t pix, cudaStream_t s, int block, int m0, int m1) {
+  if (!pix) return;
   if (block < 64 || block > 1024 || block % 32) block = 256;
   note_launch();
-  k_insert<<<(total_pix + block - 1) / block, block, 0, s>>>(d_batch);
+  k_insert<<<(pix + block - 1) / block, block, 0, s>>>(d_batch, m0, m1);
 }
 
 // ------------------------------------------------- pending leaf order -----
@@ -654,10 +654,30 @@ constexpr size_t FIN_SMEM_MAX = 200 * 1024;
 
 // One block per map of the batch; the pending count is read on the device
 // (nothing is done after an allocation error, which the host reports).
-__global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc *__restrict__ bd) {
+// A frame of a sequence hands the next frame its branch count and leaf base,
+// or halts it (and so every later frame) when this frame must grow the
+// volume, failed or was halted itself: the host runs those frames again after
+// the growth, or reports the failure.
+__device__ __forceinline__ void chain_next(const MapFrame &F, Counters *cnt, uint32_t leaves_before, bool halt) {
+  Counters *nx = F.next_cnt;
+  if (!nx) return;
+  nx->branches_used = ld_volatile(&cnt->branches_used);
+  nx->leaves_base = leaves_before + ld_volatile(&cnt->pending);
+  if (halt) atomicOr(&nx->error, ERR_SEQ_HALT);
+}
+
+__global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc *__restrict__ bd, int m0) {
   extern __shared__ uint32_t fin_smem[];
-  const MapFrame &F = bd->f[blockIdx.x];
+  const MapFrame &F = bd->f[m0 + blockIdx.x];
   Counters *cnt = F.cnt;
+  if (F.chain || F.next_cnt) {
+    // a sequence's frame: everything it reads of the counters was written by
+    // earlier kernels (its own insert, the previous finalisation)
+    if (ld_volatile(&cnt->error) & (ERR_SEQ_HALT | ERR_DEDUPE_FAILED | ERR_PENDING_OVERFLOW)) {
+      if (threadIdx.x == 0) chain_next(F, cnt, F.chain ? ld_volatile(&cnt->leaves_base) : F.leaves_before, true);
+      return;
+    }
+  }
   // After a de-duplication error nothing was inserted.  After an insert whose
   // wait gave up (ERR_SPIN_TIMEOUT) the pending leaves recorded before it are
   // complete records and are placed, so that no octree slot keeps a pending
@@ -665,7 +685,8 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc
   if (cnt->error & (ERR_DEDUPE_FAILED | ERR_PENDING_OVERFLOW)) return;
   const int npend = (int)cnt->pending;
   const PendingLeaf *pend = F.pend;
-  const uint32_t npix = F.npix, leaves_before = F.leaves_before, leaves_max = F.leaves_max, frame = F.frame;
+  const uint32_t leaves_before = F.chain ? ld_volatile(&cnt->leaves_base) : F.leaves_before;
+  const uint32_t npix = F.npix, leaves_max = F.leaves_max, frame = F.frame;
   const uint32_t n = F.n;
   uint32_t *rank = F.rank, *tree = F.tree, *stamp = F.stamp, *queue = F.queue, *parent = F.parent;
   ushort4 *leaf = F.leaf;
@@ -709,7 +730,8 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc
   // queued above); mark each queued brick with the frame's bit and list the
   // bricks no earlier frame of the pass has marked.  A frame the update must
   // not take (failed, or the volume must grow first) is left to the host.
-  if (F.upd_mask && !fuse_deferred(F)) {
+  const bool stand_aside = fuse_deferred(F);  // failed, or the volume must grow first
+  if (F.upd_mask && !stand_aside) {
     const uint32_t nq = ld_volatile(&cnt->queued);
     const uint32_t bit = 1u << F.upd_slot;
     for (uint32_t j = t; j < nq; j += FIN_THREADS) {
@@ -720,6 +742,7 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc
       if (atomicOr(&F.upd_mask[b], bit) == 0u) F.upd_list[atomicAdd(F.upd_count, 1u)] = b;
     }
   }
+  if (t == 0) chain_next(F, cnt, leaves_before, stand_aside);
 }
 
 bool finalize_small_fits(uint32_t npix) {
@@ -738,12 +761,13 @@ bool finalize_small_prepare(int device) {
   return true;
 }
 
-bool launch_finalize_small(const BatchDesc *d_batch, int nmaps, uint32_t max_npix, int device, cudaStream_t s) {
+bool launch_finalize_small(const BatchDesc *d_batch, int nmaps, uint32_t max_npix, int device, cudaStream_t s,
+                           int m0) {
   const size_t smem = sizeof(uint32_t) * (((size_t)max_npix + 31) / 32 + FIN_THREADS);
   if (smem > FIN_SMEM_MAX || nmaps < 1) return false;
   if (!finalize_small_prepare(device)) return false;
   note_launch();
-  k_finalize_bitmap<<<nmaps, FIN_THREADS, smem, s>>>(d_batch);
+  k_finalize_bitmap<<<nmaps, FIN_THREADS, smem, s>>>(d_batch, m0);
   return true;
 }
 

@@ -151,6 +151,17 @@ struct ff_handle {
   bool ring_read = false;              // a pass was launched since the ring was allocated
   cudaEvent_t ev_copy = nullptr;       // a device frame's images copied into its slot
   bool copy_pending = false;
+  bool seq_images = false;             // the frames being finished are a sequence's (caller images)
+
+  // a sequence of one map's frames (ff_add_map_sequence_u16_device): per
+  // frame its voxel keys, processed flags, de-duplication boundaries and
+  // counters (device, and a pinned mirror)
+  int seq_frames = 0;
+  size_t seq_pix = 0, seq_bnd = 0;
+  int4 *d_seq_vox = nullptr;
+  uint8_t *d_seq_proc = nullptr;
+  int4 *d_seq_bnd = nullptr;
+  Counters *d_seq_cnt = nullptr, *h_seq_cnt = nullptr;
   int pi_insert = -1;  // profile record of the last insert launch this map led
 
   // brick ownership (ff_set_shard) and the voxels grow() has moved the grid by
@@ -672,7 +683,8 @@ ff_status ff_destroy(ff_handle *h) {
                   h->d_pyp, h->d_vox, h->d_proc, h->d_bnd, h->d_pend, h->d_keys, h->d_sort_tmp, h->d_rcp_tab,
                   h->d_cnn_params, h->d_cnn_packed, h->d_feat, h->d_a1, h->d_a2, h->d_conf_set[0], h->d_conf_set[1],
                   h->d_batch_set[0], h->d_batch_set[1], h->d_upd_mask, h->d_upd_list, h->d_upd_count,
-                  h->d_upd_total, h->d_ring_depth, h->d_ring_bgr, h->d_ring_conf};
+                  h->d_upd_total, h->d_ring_depth, h->d_ring_bgr, h->d_ring_conf, h->d_seq_vox, h->d_seq_proc,
+                  h->d_seq_bnd, h->d_seq_cnt};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 2; k++) {
@@ -682,6 +694,7 @@ ff_status ff_destroy(ff_handle *h) {
   }
   if (h->h_upd_total) cudaFreeHost(h->h_upd_total);
   if (h->h_halo_count) cudaFreeHost(h->h_halo_count);
+  if (h->h_seq_cnt) cudaFreeHost(h->h_seq_cnt);
   if (h->ev_ring_free) cudaEventDestroy(h->ev_ring_free);
   if (h->ev_copy) cudaEventDestroy(h->ev_copy);
   if (h->ev_fin) cudaEventDestroy(h->ev_fin);
@@ -1071,9 +1084,9 @@ static ff_status frame_plan(ff_handle *lead, int n, LaunchPlan &lp) {
   return FF_OK;
 }
 
-// Device part: upload the descriptor and launch the de-duplication and the
-// insert on the lead's stream.
-static ff_status frame_issue(ff_handle *lead, int n, const LaunchPlan &lp) {
+// Device part: upload the descriptor and launch the de-duplication and (with
+// insert) the insert on the lead's stream.
+static ff_status frame_issue(ff_handle *lead, int n, const LaunchPlan &lp, bool insert = true) {
   ff_handle *h = lead;  // (error reporting)
   cudaStream_t s = lead->stream;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
@@ -1098,6 +1111,10 @@ static ff_status frame_issue(ff_handle *lead, int n, const LaunchPlan &lp) {
       CK(launch_dedupe(lead->d_batch, (int)lp.groups[g][0], (int)lp.groups[g][1], lp.groups[g][2], lp.rows,
                        lead->d_barrier + 8 * g, lead->cfg.device, s));
   lead->prof.end(pi, lp.npix * 2, s);  // the depth image read (the keys and flags it writes stay in L2)
+  if (!insert) {
+    CK(cudaGetLastError());
+    return FF_OK;
+  }
   if (lead->fin_pending) {
     // the previous frame's finalisation (on fuse_stream) completes the octree
     CK(cudaStreamWaitEvent(s, lead->ev_fin, 0));
@@ -1278,8 +1295,10 @@ static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf,
     // pass, which reads its slot's images
     FuseSlot &fs_ = h->upd_slot[h->cur_slot];
     fs_.q = mf.q;
-    fs_.depth = h->d_ring_depth + (size_t)h->cur_slot * h->ring_pix;
-    fs_.bgr = h->d_ring_bgr + (size_t)h->cur_slot * h->ring_pix * 3;
+    // a sequence's frames are read where the caller keeps them (the call
+    // waits for their update); other frames from their ring slot
+    fs_.depth = h->seq_images ? mf.depth : h->d_ring_depth + (size_t)h->cur_slot * h->ring_pix;
+    fs_.bgr = h->seq_images ? mf.bgr : h->d_ring_bgr + (size_t)h->cur_slot * h->ring_pix * 3;
     fs_.conf = mf.conf;
     fs_.W = plan.W;
     fs_.H = plan.H;
@@ -1445,6 +1464,157 @@ ff_status ff_add_map_u16_device(ff_handle *h, const uint16_t *d_depth, const uin
     cudaEventSynchronize(h->ev_copy);
     h->copy_pending = false;
   }
+  h->cur_slot = -1;
+  return st;
+}
+
+// Per-frame buffers of a sequence of up to `frames` frames of W x H pixels.
+static ff_status ensure_seq(ff_handle *h, int W, int H, int frames) {
+  const size_t pix = (size_t)W * H, bnd = dedupe_boundary_elems(W, H);
+  if (frames <= h->seq_frames && pix <= h->seq_pix && bnd <= h->seq_bnd) return FF_OK;
+  const int nf = std::max(frames, h->seq_frames);
+  const size_t np = std::max(pix, h->seq_pix), nb = std::max(bnd, h->seq_bnd);
+  cudaFree(h->d_seq_vox);
+  cudaFree(h->d_seq_proc);
+  cudaFree(h->d_seq_bnd);
+  h->d_seq_vox = nullptr;
+  h->d_seq_proc = nullptr;
+  h->d_seq_bnd = nullptr;
+  h->seq_frames = 0;
+  CK(alloc(&h->d_seq_vox, np * nf));
+  CK(alloc(&h->d_seq_proc, np * nf));
+  CK(alloc(&h->d_seq_bnd, nb * nf));
+  if (!h->d_seq_cnt) {
+    CK(alloc(&h->d_seq_cnt, (size_t)BATCH_MAX));
+    CK(cudaMemset(h->d_seq_cnt, 0, sizeof(Counters) * BATCH_MAX));
+    CK(cudaMallocHost((void **)&h->h_seq_cnt, sizeof(Counters) * BATCH_MAX));
+  }
+  h->seq_frames = nf;
+  h->seq_pix = np;
+  h->seq_bnd = nb;
+  return FF_OK;
+}
+
+// One chunk of a sequence: frames [0, c) of the arrays, all de-duplicated in
+// one set of cooperative launches, then inserted and finalised frame after
+// frame on the device (each finalisation hands the next frame its branch count
+// and leaf base, or halts it), one read-back of every frame's counters, and
+// the host's bookkeeping frame by frame.  done: frames finished (a frame
+// halted by an earlier one that grew the volume is not; the caller runs it
+// again).
+static ff_status sequence_chunk(ff_handle *h, int c, const uint16_t *const *d_depth, const uint8_t *const *d_bgr,
+                                int W, int H, const double *K, const double *R, const double *t, float scaling,
+                                float maxcam, int32_t *queued, int &done) {
+  done = 0;
+  cudaStream_t s = h->stream;
+  FCK(ensure_seq(h, W, H, c));
+  const size_t pix = (size_t)W * H;
+  std::vector<FramePlan> plan(c);
+  std::vector<MapFrame> mf(c);
+  const uint32_t frame0 = h->frames;
+  for (int k = 0; k < c; k++) {
+    h->cur_slot = h->upd_pending + k;
+    h->d_cnt = h->d_seq_cnt + k;
+    h->h_cnt = h->h_seq_cnt + k;
+    FCK(frame_prepare(h, d_depth[k], d_bgr[k], W, H, K + 4 * k, R + 9 * k, t + 3 * k, scaling, maxcam, mf[k],
+                      plan[k]));
+    MapFrame &F = mf[k];
+    F.vox = h->d_seq_vox + (size_t)k * h->seq_pix;
+    F.proc = h->d_seq_proc + (size_t)k * h->seq_pix;
+    F.bnd = h->d_seq_bnd + (size_t)k * h->seq_bnd;
+    F.cnt = h->d_seq_cnt + k;
+    F.frame = frame0 + 1 + (uint32_t)k;
+    F.chain = k > 0 ? 1u : 0u;
+    F.next_cnt = k + 1 < c ? h->d_seq_cnt + k + 1 : nullptr;
+    h->h_batch->f[k] = F;
+  }
+  LaunchPlan lp;
+  FCK(frame_plan(h, c, lp));
+  FCK(frame_issue(h, c, lp, false));
+  const int block = h->tune.insert_block > 0 ? h->tune.insert_block : 256;
+  std::vector<int> pi_ins(c, -1);
+  for (int k = 0; k < c; k++) {
+    int pi = h->prof.begin(ST_INSERT, s);
+    pi_ins[k] = pi;
+    launch_insert(h->d_batch, (uint32_t)(h->h_batch->pix_end[k] - (k ? h->h_batch->pix_end[k - 1] : 0u)), s, block,
+                  k, k + 1);
+    h->prof.end(pi, 0.0, s);
+    pi = h->prof.begin(ST_FINALIZE, s);
+    if (!launch_finalize_small(h->d_batch, 1, (uint32_t)pix, h->cfg.device, s, k))
+      return set_err(h, FF_ERR_CUDA, "leaf finalisation could not be launched");
+    h->prof.end(pi, 0.0, s);
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h->h_seq_cnt, h->d_seq_cnt, sizeof(Counters) * c, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  h->seq_images = true;
+  ff_status st = FF_OK;
+  for (int k = 0; k < c; k++) {
+    if (h->h_seq_cnt[k].error & ERR_SEQ_HALT) break;
+    h->cur_slot = h->upd_pending;
+    h->d_cnt = h->d_seq_cnt + k;
+    h->h_cnt = h->h_seq_cnt + k;
+    plan[k].leaves_before = h->leaves_used;
+    plan[k].frame = h->frames + 1;
+    plan[k].counters_early = false;  // read after the finalisation: the new leaves are counted
+    h->pi_insert = pi_ins[k];        // (its bytes follow from the frame's counters)
+    st = frame_finish(h, plan[k], mf[k], -1, -1, queued ? queued + k : nullptr);
+    if (st != FF_OK) break;
+    done++;
+  }
+  h->seq_images = false;
+  h->pi_insert = -1;
+  // the next chunk's counters start clean of this one's halts
+  CK(cudaMemsetAsync(h->d_seq_cnt, 0, sizeof(Counters) * c, s));
+  return st;
+}
+
+ff_status ff_add_map_sequence_u16_device(ff_handle *h, int n, const uint16_t *const *d_depth,
+                                         const uint8_t *const *d_bgr, int width, int height, const double *K,
+                                         const double *R, const double *t, float scaling, float maxcam,
+                                         int32_t *queued) {
+  if (!h) return FF_ERR_BAD_ARG;
+  if (n < 1 || !d_depth || !d_bgr || !K || !R || !t || width <= 0 || height <= 0)
+    return set_err(h, FF_ERR_BAD_ARG, "ff_add_map_sequence_u16_device: bad argument");
+  for (int k = 0; k < n; k++)
+    if (!d_depth[k] || !d_bgr[k]) return set_err(h, FF_ERR_BAD_ARG, "ff_add_map_sequence_u16_device: NULL image");
+  h->cur_slot = -1;
+  CK(cudaSetDevice(h->cfg.device));
+  if (!deferrable(h, width, height) || n == 1) {
+    // frames the one-block finalisation does not take (or deferral is off):
+    // one by one
+    for (int k = 0; k < n; k++)
+      FCK(ff_add_map_u16_device(h, d_depth[k], d_bgr[k], width, height, K + 4 * k, R + 9 * k, t + 3 * k, scaling,
+                                maxcam, queued ? queued + k : nullptr));
+    return FF_OK;
+  }
+  FCK(ensure_image(h, width, height));
+  FCK(ensure_ring(h, width, height));
+  // the single-map frames before: their placement and marking done, their
+  // buffers free
+  CK(join_fuse(h));
+  CK(cudaStreamSynchronize(h->stream));
+  h->fin_pending = false;
+  select_set(h, 0);
+  ff_status st = FF_OK;
+  for (int i = 0; i < n && st == FF_OK;) {
+    const int c = std::min(n - i, std::min(BATCH_MAX, h->upd_batch));
+    if (h->upd_pending + c > h->upd_batch) {
+      st = flush_updates(h);
+      if (st != FF_OK) break;
+    }
+    int done = 0;
+    st = sequence_chunk(h, c, d_depth + i, d_bgr + i, width, height, K + 4 * i, R + 9 * i, t + 3 * i, scaling,
+                        maxcam, queued ? queued + i : nullptr, done);
+    i += done;
+  }
+  // the sequence's frames are read where the caller keeps them: their update
+  // runs before the call returns
+  const ff_status st2 = flush_updates(h);
+  if (st == FF_OK) st = st2;
+  if (cudaEventSynchronize(h->ev_ring_free) != cudaSuccess && st == FF_OK)
+    st = set_err(h, FF_ERR_CUDA, "the sequence's voxel update failed");
+  select_set(h, (int)(h->frames & 1u));
   h->cur_slot = -1;
   return st;
 }

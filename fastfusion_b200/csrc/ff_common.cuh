@@ -45,12 +45,13 @@ enum : uint32_t {
   ERR_DEDUPE_NOT_CONVERGED = 32u,
   ERR_CELL_KEY = 64u,  // a mesh cell's origin does not fit its sort key
   ERR_DEDUPE_TIMEOUT = 128u,  // a grid barrier of the de-duplication gave up (nothing was inserted)
+  ERR_SEQ_HALT = 256u,        // an earlier frame of a sequence must grow the volume or failed: not run
 };
 
 // Error bits after which a frame's voxel update is skipped: its allocation
 // did not complete as the reference's would have.
 constexpr uint32_t ERR_FRAME_FAILED = ERR_SPIN_TIMEOUT | ERR_DEDUPE_NOT_CONVERGED | ERR_DEDUPE_TIMEOUT |
-                                      ERR_PENDING_OVERFLOW;
+                                      ERR_PENDING_OVERFLOW | ERR_SEQ_HALT;
 // Error bits of the de-duplication: the insert, the leaf finalisation and the
 // update leave such a frame out entirely, so the map stays as it was.
 constexpr uint32_t ERR_DEDUPE_FAILED = ERR_DEDUPE_NOT_CONVERGED | ERR_DEDUPE_TIMEOUT;
@@ -73,7 +74,8 @@ struct Counters {
   uint64_t mesh_f;
   uint32_t cnn_error;  // the confidence network's bounded waits (kept by the frame's counter set-up)
   uint32_t levels;     // octree levels the insert probed, summed over the processed pixels
-  uint32_t pad[2];
+  uint32_t leaves_base;  // a sequence's later frame: leaves before it (set by the previous frame's finalisation)
+  uint32_t pad;
 };
 
 // Float camera parameters (the reference's camPamsFloat, definitions.h:71-88).

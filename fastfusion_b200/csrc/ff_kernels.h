@@ -58,6 +58,14 @@ struct MapFrame {
   // later updates every listed brick with all its marked frames in order.
   uint32_t *upd_mask, *upd_list, *upd_count;
   int32_t upd_slot;
+  // A frame of a sequence of one map (ff_add_map_sequence_u16_device): all
+  // its frames are de-duplicated in one launch, then inserted and finalised
+  // frame after frame on the device.  chain: the frame's branch count and
+  // leaf base come from the previous frame's finalisation (cnt->branches_used,
+  // cnt->leaves_base) rather than from the host; next_cnt: the next frame's
+  // counters, which this frame's finalisation sets up (or halts).
+  uint32_t chain;
+  Counters *next_cnt;
 };
 
 // Whether a frame's voxel update must not run with the others: an allocation
@@ -67,7 +75,7 @@ struct MapFrame {
 __device__ __forceinline__ bool fuse_deferred(const MapFrame &F) {
   const Counters *c = F.cnt;
   if ((c->error & ERR_FRAME_FAILED) || c->cnn_error) return true;
-  const uint32_t leaves = F.leaves_before + c->pending;
+  const uint32_t leaves = (F.chain ? c->leaves_base : F.leaves_before) + c->pending;
   const uint32_t branches = min(c->branches_used, F.branches_max);
   const int n = (int)F.n;
   const bool outside = c->box_min[0] < 0 || c->box_min[1] < 0 || c->box_min[2] < 0 || c->box_max[0] >= n ||
@@ -187,8 +195,10 @@ cudaError_t launch_dedupe(const BatchDesc *d_batch, int m0, int m1, uint32_t til
 cudaError_t launch_dedupe_one(const BatchDesc *h_desc, BatchDesc *d_batch, uint32_t tiles, int rows,
                               uint32_t *barrier, int device, cudaStream_t s);
 
-// Octree descent / allocation of every processed pixel of the batch.
-void launch_insert(const BatchDesc *d_batch, uint32_t total_pix, cudaStream_t s, int block = 256);
+// Octree descent / allocation of every processed pixel of the batch's maps
+// [m0, m1) (pixels [pix_end[m0 - 1], pix_end[m1 - 1]), pix = their count).
+void launch_insert(const BatchDesc *d_batch, uint32_t pix, cudaStream_t s, int block = 256, int m0 = 0,
+                   int m1 = BATCH_MAX);
 
 // Sort scratch size for `n` pending leaves.
 size_t pending_sort_bytes(int n);
@@ -210,7 +220,8 @@ bool finalize_small_fits(uint32_t npix);
 // Ranks (creation order), leaf table and parents of each map's pending
 // leaves, one block per map, counts read on the device; for images of up to
 // about 1.6 million pixels (false, nothing launched, for larger ones).
-bool launch_finalize_small(const BatchDesc *d_batch, int nmaps, uint32_t max_npix, int device, cudaStream_t s);
+bool launch_finalize_small(const BatchDesc *d_batch, int nmaps, uint32_t max_npix, int device, cudaStream_t s,
+                           int m0 = 0);
 // Set the finalisation kernel's shared-memory limit on this device (once).
 bool finalize_small_prepare(int device);
 

@@ -81,6 +81,7 @@ SIGNATURES = {
     "ff_add_map_u16": (_i32, [_vp, _vp, _i32, _i32, _sz, _vp, _sz, _vp, _vp, _vp, _f32, _f32, _vp]),
     "ff_add_map_u16_device": (_i32, [_vp, _vp, _vp, _i32, _i32, _vp, _vp, _vp, _f32, _f32, _vp]),
     "ff_add_maps_u16_device": (_i32, [_vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "ff_add_map_sequence_u16_device": (_i32, [_vp, _i32, _vp, _vp, _i32, _i32, _vp, _vp, _vp, _f32, _f32, _vp]),
     "ff_update_meshes": (_i32, [_vp, _vp]),
     "ff_get_mesh_counts": (_i32, [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
     "ff_get_mesh": (_i32, [_vp, _vp, _vp, _vp]),
@@ -367,6 +368,25 @@ class FusionMipMapCPU:
         if st != FF_OK:
             self._check(st)
         return self._q.value
+
+    def addMapSequenceDevice(self, d_depth, d_bgr, width: int, height: int, cams, scaling: float = 1.0 / 5000.0,
+                             maxcamdistance: float = 10.0) -> list:
+        """Several frames of this map in one call (ff_add_map_sequence_u16_device):
+        d_depth/d_bgr are sequences of device pointers, cams CameraInfo
+        objects; returns each frame's queued count.  Same results as
+        addMapDevice frame by frame; the images are free when it returns."""
+        n = len(cams)
+        dd = (ctypes.c_void_p * n)(*[int(p) for p in d_depth])
+        db = (ctypes.c_void_p * n)(*[int(p) for p in d_bgr])
+        K = np.ascontiguousarray(np.stack([c.K for c in cams]), np.float64)
+        R = np.ascontiguousarray(np.stack([c.R.reshape(9) for c in cams]), np.float64)
+        t = np.ascontiguousarray(np.stack([c.t for c in cams]), np.float64)
+        q = np.zeros(n, np.int32)
+        st = self._L.ff_add_map_sequence_u16_device(self._h, n, dd, db, width, height, _p(K), _p(R), _p(t),
+                                                    scaling, maxcamdistance, _p(q))
+        if st != FF_OK:
+            self._check(st)
+        return [int(x) for x in q]
 
     def updateMeshes(self) -> bool:
         st = self._L.ff_update_meshes(self._h, self._uref)

@@ -127,6 +127,25 @@ ff_status ff_add_map_u16_device(ff_handle *h, const uint16_t *d_depth, const uin
                                 const double K[4], const double R[9], const double t[3], float scaling,
                                 float maxcam, int32_t *queued);
 
+/* A sequence of n frames of one map, all W x H, in device memory; the same
+ * results as n calls of ff_add_map_u16_device (queued[k] = frame k's count).
+ * The frames' de-duplication (which reads no octree) runs for all of them in
+ * one set of cooperative launches; their inserts and leaf finalisations run
+ * frame after frame on the device without returning to the host (each
+ * finalisation hands the next frame its branch count and leaf base); one
+ * read-back of all frames' counters follows.  When a frame must grow the
+ * volume, the frames after it were de-duplicated in the old volume: they are
+ * halted on the device and run again after the growth.  Their voxel update
+ * runs as one deferred pass before the call returns, so the images are free
+ * then.  K + 4k, R + 9k, t + 3k: frame k's camera, as in ff_add_map_u16.
+ * On an error the frames before the failing one are fused and queued[] of
+ * the later ones is left unset.  The reference fuses one frame per call
+ * (geometryfusion_mipmap_cpu.cpp:1603-2034); this is the frame-batched form. */
+ff_status ff_add_map_sequence_u16_device(ff_handle *h, int n, const uint16_t *const *d_depth,
+                                         const uint8_t *const *d_bgr, int width, int height, const double *K,
+                                         const double *R, const double *t, float scaling, float maxcam,
+                                         int32_t *queued);
+
 /* Several independent maps fuse one frame each, in one set of launches (the
  * de-duplication of all frames in one cooperative launch, their inserts,
  * leaf finalisations and voxel updates in one launch each) -- for many maps
