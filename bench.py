@@ -115,6 +115,10 @@ def parse_args(argv=None):
                     help="corridor: use every stride-th frame of the path (0: spread the frames over all of it)")
     ap.add_argument("--no-tuning", action="store_true",
                     help="batched workload: default launch shapes instead of the autotuner's table")
+    ap.add_argument("--walk-frames", type=int, default=WALK_FRAMES,
+                    help="frames of the walk to fuse (default: all 1000; a shorter prefix for profiling captures)")
+    ap.add_argument("--batch-frames", type=int, default=0,
+                    help="batched workload: frames per map (0: each map its own length, 200-2000)")
     ap.add_argument("--maps", type=int, default=0,
                     help="batched workload instead: this many independent maps of uneven size fused together "
                          "(ff_add_maps_u16_device), one frame of each per launch set")
@@ -128,10 +132,13 @@ def parse_args(argv=None):
     return a
 
 
-def step_plan(a, frames: int = WALK_FRAMES):
+def step_plan(a, frames: int | None = None):
     """(steps run, indices of the timed steps): every step of the walk runs;
     K timed steps are spread evenly over the steps after the W warm-up ones
-    (a walk longer than 1000 frames only when W + K steps need it)."""
+    (a walk longer than 1000 frames only when W + K steps need it).  A
+    profiling capture may run a prefix of the walk (--walk-frames)."""
+    if frames is None:
+        frames = getattr(a, "walk_frames", WALK_FRAMES) or WALK_FRAMES
     total = max(frames // FRAMES_PER_STEP, a.warmup + a.steps)
     span = total - a.warmup
     return total, [a.warmup + (i * span) // a.steps for i in range(a.steps)]
@@ -165,7 +172,8 @@ def render_frames(seq, n_frames: int, device):
 def workload_config(a, n_frames: int) -> dict:
     total, timed = step_plan(a)
     return {
-        "workload": f"walk{n_frames}: the whole {n_frames}-frame seeded random walk (640x480) in the 8x8x3 m room "
+        "workload": f"walk{n_frames}: {'the whole' if n_frames >= WALK_FRAMES else 'the first'} {n_frames} "
+                    f"frames of the 1000-frame seeded random walk (640x480) in the 8x8x3 m room "
                     f"with 80 primitives (the larger synthetic configuration), voxel 5 mm, threshold 10 mm, maxcam "
                     f"4 m, 8^3 bricks, multi-resolution levels, updateMeshes every {FRAMES_PER_STEP} frames; "
                     f"{len(timed)} of its {total} steps timed, spread over the walk after {a.warmup} warm-up steps",
@@ -329,6 +337,14 @@ def run_b200(a):
         return m
 
     def device_step(m, s):
+        # the step's frames in one call (ff_add_map_sequence_u16_device)
+        ks = range(s * FRAMES_PER_STEP, (s + 1) * FRAMES_PER_STEP)
+        m.addMapSequenceDevice([depth[k].data_ptr() for k in ks], [bgr[k].data_ptr() for k in ks], WIDTH, HEIGHT,
+                               [cams[k] for k in ks], SCALING, MAXCAM)
+        m.updateMeshes()
+
+    def device_step_single(m, s):
+        # one call per frame (ff_add_map_u16_device)
         for k in range(s * FRAMES_PER_STEP, (s + 1) * FRAMES_PER_STEP):
             m.addMapDevice(depth[k].data_ptr(), bgr[k].data_ptr(), WIDTH, HEIGHT, cams[k], SCALING, MAXCAM)
         m.updateMeshes()
@@ -382,17 +398,21 @@ def run_b200(a):
     st = m.stats()
     m.close()
     del m
+    # the same with one call per frame
+    m = new_map()
+    single_ms, _ = timed(device_step_single, m)
+    m.close()
+    del m
 
     # 2. per-stage profile of the walk after the warm-up (separate map; events per stage)
     m = new_map()
     dirty, rounds = [], []
 
     def device_step_stats(mm, s):
-        for k in range(s * FRAMES_PER_STEP, (s + 1) * FRAMES_PER_STEP):
-            mm.addMapDevice(depth[k].data_ptr(), bgr[k].data_ptr(), WIDTH, HEIGHT, cams[k], SCALING, MAXCAM)
-            rounds.append(mm.stats()["dedupe_rounds"])
-        mm.updateMeshes()
-        dirty.append(mm.stats()["mesh_cells_dirty"])
+        device_step(mm, s)
+        st_ = mm.stats()
+        rounds.append(st_["dedupe_rounds"])
+        dirty.append(st_["mesh_cells_dirty"])
 
     for s_ in range(a.warmup):
         device_step(m, s_)
@@ -456,6 +476,7 @@ def run_b200(a):
     clocks = clk.stop() if clk else None
 
     value, dev_ms_max = whole_job_rate(a.steps * FRAMES_PER_STEP, dev_ms, dev)
+    value_single, _ = whole_job_rate(a.steps * FRAMES_PER_STEP, single_ms, dev)
 
     peak, peak_kind = measured_hbm_peak()
     tt = read_traffic_table()
@@ -493,12 +514,18 @@ def run_b200(a):
             "data": "synthetic: seeded room scene rendered to depth+BGR on the GPU (the TUM RGB-D sequences "
                     "the reference documents are not available offline)",
             "config": dict(workload_config(a, nf), parallelism=f"independent maps x{world}"),
+            "api": "value: ff_add_map_sequence_u16_device (a step's 10 frames per call); "
+                   "value_single_frame_calls: ff_add_map_u16_device per frame; e2e: ff_add_map_u16 per frame",
+            "value_single_frame_calls": round(value_single, 2),
             "e2e": e2e, "e2e_pageable": e2e_pageable, "roofline": roofline, "roofline_fuse": roofline_fuse,
             "cpu_baseline": cpu, "gpu_launches": gpu_launches,
             "library_calls": lib_calls, "clocks": clocks, "stages": stage_rec,
             "stage_profile": f"CUDA events per stage over steps {a.warmup}-{total - 1} of a separate run "
                              f"({round(prof_wall_ms)} ms wall)",
             "wall_s_walk": round(dev_wall, 3), "surface_rms_m": rms,
+            "fused_bricks": {"frame_bricks": st["fused_frame_bricks"], "bricks_read_and_written": st["fused_bricks"],
+                             "note": "the deferred update pass reads and writes each brick once per pass, "
+                                     "whatever the number of its frames"},
             "map": {"leaves": st["leaves_used"], "leaves_max": st["leaves_max"], "n": st["n"],
                     "mesh_vertices": st["mesh_vertices"], "mesh_faces": st["mesh_faces"],
                     "mesh_cells": st["mesh_cells"], "grows": st["grows"], "meshing_ok": st["meshing_ok"],
@@ -686,86 +713,151 @@ def run_reference(a):
 # -- the batched workload -------------------------------------------------------
 def run_batch(a):
     """Independent maps of uneven size (rooms 2-12 m, 10-150 primitives,
-    320x240 / 640x480 / 1280x960, voxels 4-10 mm), one frame of every map per
-    ff_add_maps_u16_device call, updateMeshes per map every 10 frames; frames/s
-    over all maps, device-resident inputs, CUDA events per step."""
+    320x240 / 640x480 / 1280x960, voxels 4-10 mm, 200-2000 frames each):
+    maps placed over the ranks by longest processing time first (frames x
+    pixels); on each rank one frame of every map that still has frames per
+    ff_add_maps_u16_device call, updateMeshes per map every 10 frames.  Every
+    map fuses its whole sequence; K steps spread over the run are timed (CUDA
+    events; the frames of a step are rendered on the GPU before its timer
+    starts).  frames/s over all ranks' maps over the slowest rank's time."""
     import torch
+    import torch.distributed as dist
     from fastfusion_b200 import fusion as ff
     from fastfusion_b200.scene import batch_sequences, render_torch
-    dev = torch.device("cuda", 0)
+    from fastfusion_b200.shard import lpt_placement
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != a.gpus:
+        raise SystemExit(f"--gpus {a.gpus} but WORLD_SIZE={world}")
+    dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    nf = (a.warmup + a.steps) * FRAMES_PER_STEP
-    seqs = batch_sequences(a.maps, n_frames=nf)
-    frames = []
-    for seq, _ in seqs:
-        d = torch.empty((nf, seq.height, seq.width), dtype=torch.int16, device=dev)
-        c = torch.empty((nf, seq.height, seq.width, 3), dtype=torch.uint8, device=dev)
-        for k in range(nf):
-            dk, ck = render_torch(seq.scene, *seq.poses[k], seq.width, seq.height, seq.K, seq.seed, k, device=dev)
-            d[k].copy_(dk)
-            c[k].copy_(ck)
-        frames.append((d, c))
-    cams = [[ff.CameraInfo(seq.K, *seq.poses[k]) for k in range(nf)] for seq, _ in seqs]
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    fixed = a.batch_frames if a.batch_frames > 0 else None
+    seqs_all = batch_sequences(a.maps, n_frames=fixed)
+    lengths_all = [len(sq.poses) for sq, _ in seqs_all]
+    costs = [n * sq.width * sq.height for n, (sq, _) in zip(lengths_all, seqs_all)]
+    placement = lpt_placement(costs, world)
+    mine = placement[rank]
+    seqs = [seqs_all[i] for i in mine]
+    lengths = [lengths_all[i] for i in mine]
+    # one step plan for every rank: the longest map of the whole job
+    total = max(-(-max(lengths_all) // FRAMES_PER_STEP), a.warmup + a.steps)
+    span = total - a.warmup
+    timed = set(a.warmup + (i * span) // a.steps for i in range(a.steps))
     stream = torch.cuda.current_stream(dev)
     maps = []
     for seq, voxel in seqs:
         m = ff.FusionMipMapCPU(0, 0, 0, voxel, 2 * voxel, 0, True, leaves_max=400000, branches_max=8000000,
-                               storage=a.storage, rcp=a.rcp)
+                               storage=a.storage, rcp=a.rcp, device=local)
         m.set_stream(stream.cuda_stream)
         maps.append(m)
-    widths = [seq.width for seq, _ in seqs]
-    heights = [seq.height for seq, _ in seqs]
-    # launch shapes chosen by the autotuner for this GPU (python -m fastfusion_b200.autotune), if any
     from fastfusion_b200.autotune import DEFAULT, load_tuning
     tuning = {} if a.no_tuning else load_tuning()
-    if tuning:
+    if tuning and maps:
         maps[0].set_tuning(**{**DEFAULT, **tuning})
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    # frames of one step, rendered before it (outside its timer)
+    buf = [(torch.empty((FRAMES_PER_STEP, sq.height, sq.width), dtype=torch.int16, device=dev),
+            torch.empty((FRAMES_PER_STEP, sq.height, sq.width, 3), dtype=torch.uint8, device=dev)) for sq, _ in seqs]
+    render_s = [0.0]
+
+    def render_step(s_):
+        t0 = time.perf_counter()
+        for (sq, _), (d, c), n in zip(seqs, buf, lengths):
+            for j in range(FRAMES_PER_STEP):
+                k = s_ * FRAMES_PER_STEP + j
+                if k < n:
+                    dk, ck = render_torch(sq.scene, *sq.poses[k], sq.width, sq.height, sq.K, sq.seed, k, device=dev)
+                    d[j].copy_(dk)
+                    c[j].copy_(ck)
+        torch.cuda.synchronize(dev)
+        render_s[0] += time.perf_counter() - t0
+
+    frames_done = [0]
 
     def step(s_):
-        for k in range(s_ * FRAMES_PER_STEP, (s_ + 1) * FRAMES_PER_STEP):
-            ff.add_maps_device(maps, [f[0][k].data_ptr() for f in frames], [f[1][k].data_ptr() for f in frames],
-                               widths, heights, [c[k] for c in cams], SCALING, MAXCAM)
-        for m in maps:
-            m.updateMeshes()
+        for j in range(FRAMES_PER_STEP):
+            k = s_ * FRAMES_PER_STEP + j
+            act = [i for i, n in enumerate(lengths) if k < n]
+            if not act:
+                continue
+            ff.add_maps_device([maps[i] for i in act], [buf[i][0][j].data_ptr() for i in act],
+                               [buf[i][1][j].data_ptr() for i in act], [seqs[i][0].width for i in act],
+                               [seqs[i][0].height for i in act],
+                               [ff.CameraInfo(seqs[i][0].K, *seqs[i][0].poses[k]) for i in act], SCALING, MAXCAM)
+            frames_done[0] += len(act)
+        for i, m in enumerate(maps):
+            if s_ * FRAMES_PER_STEP < lengths[i]:
+                m.updateMeshes()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
 
     for s_ in range(a.warmup):
+        render_step(s_)
         step(s_)
-    maps[0].profile(True)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    if maps:
+        maps[0].profile(True)
+    ev = []
+    timed_frames = 0
     torch.cuda.synchronize(dev)
-    for i in range(a.steps):
-        flush.fill_(i)
-        ev[i][0].record(stream)
-        step(a.warmup + i)
-        ev[i][1].record(stream)
+    barrier()
+    for s_ in range(a.warmup, total):
+        render_step(s_)
+        if s_ not in timed:
+            step(s_)
+            continue
+        flush.fill_(s_)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0 = frames_done[0]
+        e0.record(stream)
+        step(s_)
+        e1.record(stream)
+        timed_frames += frames_done[0] - f0
+        ev.append((e0, e1))
     torch.cuda.synchronize(dev)
+    barrier()
     ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
-    stages = maps[0].profile_read()
-    frames_total = a.steps * FRAMES_PER_STEP * len(maps)
+    value, ms_max = whole_job_rate(timed_frames, ms, dev)
+    stages = maps[0].profile_read() if maps else {}
     peak, peak_kind = measured_hbm_peak()
-    fms, fbytes, fl = stages["fuse"]
+    fms, fbytes, fl = stages.get("fuse", (0.0, 0.0, 0))
     fuse_gbs = fbytes / (fms / 1e3) / 1e9 if fms > 0 else 0.0
-    line = {
-        "metric": METRIC.replace("(640x480, 5 mm)", "(batched maps)"), "value": round(frames_total / (ms / 1e3), 2),
-        "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32" if a.storage == "fp32" else "f16-storage/f32",
-        "data": "synthetic: seeded rooms of uneven size rendered on the GPU",
-        "config": {"workload": f"batch{len(maps)}: independent maps, rooms 2-12 m, 10-150 primitives, "
-                               f"320x240/640x480/1280x960, voxels 4-10 mm, {nf} frames each, one frame of "
-                               f"every map per launch set, updateMeshes every {FRAMES_PER_STEP} frames",
-                   "maps": len(maps), "widths": widths, "voxels_mm": [round(v * 1e3, 2) for _, v in seqs],
-                   "tuning": tuning or "defaults",
-                   "l2": "flushed between timed steps (256 MB write)"},
-        "fuse": {"GB/s": round(fuse_gbs, 1), "frac_of_hbm": round(fuse_gbs / peak, 4), "peak": peak,
-                 "peak_source": peak_kind, "launches": fl, "avg_launch_us": round(1e3 * fms / fl, 2) if fl else 0,
-                 "bytes_per_launch": round(fbytes / fl) if fl else 0},
-        "stages_lead_map": {k: {"ms": round(v[0], 3), "launches": v[2]} for k, v in stages.items()},
-    }
-    print(json.dumps(line), flush=True)
+    if rank == 0:
+        line = {
+            "metric": METRIC.replace("(640x480, 5 mm)", "(batched maps)"), "value": round(value, 2),
+            "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": round(ms_max / a.steps, 4), "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32" if a.storage == "fp32" else "f16-storage/f32",
+            "data": "synthetic: seeded rooms of uneven size rendered on the GPU",
+            "config": {"workload": f"batch{len(seqs_all)}: independent maps, rooms 2-12 m, 10-150 primitives, "
+                                   f"320x240/640x480/1280x960, voxels 4-10 mm, "
+                                   f"{'%d frames each' % fixed if fixed else '200-2000 frames each'}, one frame "
+                                   f"of every map per launch set, updateMeshes every {FRAMES_PER_STEP} frames; "
+                                   f"{a.steps} of {total} steps timed",
+                       "maps": len(seqs_all), "frames": lengths_all,
+                       "widths": [sq.width for sq, _ in seqs_all],
+                       "voxels_mm": [round(v * 1e3, 2) for _, v in seqs_all],
+                       "placement": placement, "tuning": tuning or "defaults",
+                       "l2": "flushed between timed steps (256 MB write)",
+                       "parallelism": f"maps over {world} GPUs by longest processing time first"},
+            "timed_frames_rank0": timed_frames, "render_s_rank0": round(render_s[0], 1),
+            "fuse": {"GB/s": round(fuse_gbs, 1), "frac_of_hbm": round(fuse_gbs / peak, 4), "peak": peak,
+                     "peak_source": peak_kind, "launches": fl,
+                     "avg_launch_us": round(1e3 * fms / fl, 2) if fl else 0,
+                     "bytes_per_launch": round(fbytes / fl) if fl else 0},
+            "stages_lead_map": {k: {"ms": round(v[0], 3), "launches": v[2]} for k, v in stages.items()},
+        }
+        print(json.dumps(line), flush=True)
     for m in maps:
         m.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_corridor(a):

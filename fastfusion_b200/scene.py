@@ -450,11 +450,13 @@ def render_torch(scene: Scene, R, t, width: int, height: int, K, seed: int, fram
     return depth, bgr
 
 
-def batch_sequences(n_maps: int = 16, n_frames: int = 200, seed0: int = 100):
+def batch_sequences(n_maps: int = 16, n_frames: int | None = 200, seed0: int = 100):
     """Independent maps of uneven size (the batched workload): per map i, seed
     seed0 + i draws room sides U(2, 12) m (3 m high), U{10..150} primitives,
-    an image size from 320x240 / 640x480 / 1280x960 and a voxel size U(4, 10)
-    mm; each map walks its own room.  Returns [(Sequence, voxel metres)]."""
+    an image size from 320x240 / 640x480 / 1280x960, a voxel size U(4, 10) mm
+    and a length U{200..2000} frames (used when n_frames is None; otherwise
+    every map has n_frames); each map walks its own room.  Returns
+    [(Sequence, voxel metres)]; len(Sequence.poses) is the map's length."""
     out = []
     sizes = [(320, 240), (640, 480), (1280, 960)]
     for i in range(n_maps):
@@ -463,10 +465,13 @@ def batch_sequences(n_maps: int = 16, n_frames: int = 200, seed0: int = 100):
         prims = int(rng.integers(10, 151))
         w, h = sizes[int(rng.integers(0, 3))]
         voxel = float(rng.uniform(0.004, 0.010))
+        length = int(rng.integers(200, 2001))
+        if n_frames is not None:
+            length = n_frames
         margin = min(0.8, 0.3 * min(room[0], room[1]))
         s = w / 640.0
         K = np.array([525.0 * s, 525.0 * s, (w - 1) / 2.0, (h - 1) / 2.0])
-        poses = random_walk_trajectory(n_frames, seed0 + i, room=room, margin=margin)
+        poses = random_walk_trajectory(length, seed0 + i, room=room, margin=margin)
         cams = np.array([p[1] for p in poses])
 
         def clear(c, rad, cams=cams):

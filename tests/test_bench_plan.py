@@ -29,5 +29,12 @@ def test_longer_runs_extend_the_walk():
 def test_workload_names_the_whole_walk():
     a = bench.parse_args(["--steps", "20", "--warmup", "5"])
     cfg = bench.workload_config(a, bench.n_frames_needed(a))
-    assert cfg["workload"].startswith("walk1000: the whole 1000-frame")
+    assert cfg["workload"].startswith("walk1000: the whole 1000 frames of the 1000-frame")
     assert cfg["timed_steps"] == bench.step_plan(a)[1]
+
+
+def test_profiling_prefix():
+    a = bench.parse_args(["--steps", "5", "--warmup", "3", "--walk-frames", "80"])
+    total, timed = bench.step_plan(a)
+    assert total == 8 and timed == [3, 4, 5, 6, 7]
+    assert bench.workload_config(a, 80)["workload"].startswith("walk80: the first 80 frames")
