@@ -125,6 +125,13 @@ struct ff_handle {
   // (ff_inject_error)
   uint32_t spin_limit = SPIN_LIMIT;
   int inject = 0;
+  // loop closure (ff_loop_begin): the loop arrays, each leaf's slot in them,
+  // per queue entry its slot, [slots in use, entries taken]
+  uint32_t loop_cap = 0;
+  uint32_t *d_loop_map = nullptr, *d_loop_slots = nullptr, *d_loop_st = nullptr, *h_loop_st = nullptr;
+  size_t loop_slots_cap = 0;
+  float *d_loop_sdf = nullptr, *d_loop_wgt = nullptr;
+  uint16_t *d_loop_col = nullptr;
   uint32_t halo_since = 0;           // frames whose changes the last halo export covered
   uint32_t *h_halo_count = nullptr;  // pinned: the export's record count
 
@@ -684,7 +691,8 @@ ff_status ff_destroy(ff_handle *h) {
                   h->d_cnn_params, h->d_cnn_packed, h->d_feat, h->d_a1, h->d_a2, h->d_conf_set[0], h->d_conf_set[1],
                   h->d_batch_set[0], h->d_batch_set[1], h->d_upd_mask, h->d_upd_list, h->d_upd_count,
                   h->d_upd_total, h->d_ring_depth, h->d_ring_bgr, h->d_ring_conf, h->d_seq_vox, h->d_seq_proc,
-                  h->d_seq_bnd, h->d_seq_cnt};
+                  h->d_seq_bnd, h->d_seq_cnt, h->d_loop_map, h->d_loop_slots, h->d_loop_st, h->d_loop_sdf,
+                  h->d_loop_wgt, h->d_loop_col};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 2; k++) {
@@ -695,6 +703,7 @@ ff_status ff_destroy(ff_handle *h) {
   if (h->h_upd_total) cudaFreeHost(h->h_upd_total);
   if (h->h_halo_count) cudaFreeHost(h->h_halo_count);
   if (h->h_seq_cnt) cudaFreeHost(h->h_seq_cnt);
+  if (h->h_loop_st) cudaFreeHost(h->h_loop_st);
   if (h->ev_ring_free) cudaEventDestroy(h->ev_ring_free);
   if (h->ev_copy) cudaEventDestroy(h->ev_copy);
   if (h->ev_fin) cudaEventDestroy(h->ev_fin);
@@ -769,6 +778,114 @@ ff_status ff_halo_import(ff_handle *h, const void *d_records, uint64_t n_records
                      h->cfg.storage == FF_STORAGE_FP16, h->sm_count * 4, h->stream);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(h->stream));
+  return FF_OK;
+}
+
+ff_status ff_loop_begin(ff_handle *h, uint32_t capacity) {
+  if (!h) return FF_ERR_BAD_ARG;
+  if (capacity < 1 || capacity > h->cfg.leaves_max)
+    return set_err(h, FF_ERR_BAD_ARG, "ff_loop_begin: capacity must be 1..leaves_max");
+  CK(cudaSetDevice(h->cfg.device));
+  FCK(settle(h));
+  cudaStream_t s = h->stream;
+  CK(cudaStreamSynchronize(s));
+  if (capacity != h->loop_cap) {
+    cudaFree(h->d_loop_sdf);
+    cudaFree(h->d_loop_wgt);
+    cudaFree(h->d_loop_col);
+    h->d_loop_sdf = h->d_loop_wgt = nullptr;
+    h->d_loop_col = nullptr;
+    h->loop_cap = 0;
+    CK(alloc(&h->d_loop_sdf, (size_t)capacity * 512));
+    CK(alloc(&h->d_loop_wgt, (size_t)capacity * 512));
+    CK(alloc(&h->d_loop_col, (size_t)capacity * 1536));
+    h->loop_cap = capacity;
+  }
+  if (!h->d_loop_map) {
+    CK(alloc(&h->d_loop_map, (size_t)h->cfg.leaves_max));
+    CK(alloc(&h->d_loop_st, (size_t)4));
+    CK(cudaMallocHost((void **)&h->h_loop_st, 4 * sizeof(uint32_t)));
+  }
+  launch_fill(h->d_loop_map, h->cfg.leaves_max, BRANCHINIT, s);
+  CK(cudaMemsetAsync(h->d_loop_st, 0, 4 * sizeof(uint32_t), s));
+  CK(cudaMemsetAsync(h->d_loop_sdf, 0, sizeof(float) * capacity * 512, s));
+  CK(cudaMemsetAsync(h->d_loop_wgt, 0, sizeof(float) * capacity * 512, s));
+  CK(cudaMemsetAsync(h->d_loop_col, 0, sizeof(uint16_t) * capacity * 1536, s));
+  CK(cudaStreamSynchronize(s));
+  return FF_OK;
+}
+
+ff_status ff_loop_delete_frame(ff_handle *h, const float *d_depth, const uint8_t *d_red, const uint8_t *d_green,
+                               const uint8_t *d_blue, int width, int height, const double K[4], const double R[9],
+                               const double t[3], const uint32_t *d_queue, uint32_t n_queue, int *complete) {
+  if (!h) return FF_ERR_BAD_ARG;
+  if (!h->loop_cap) return set_err(h, FF_ERR_STATE, "ff_loop_delete_frame: call ff_loop_begin first");
+  if (!d_depth || !d_red || !d_green || !d_blue || !K || !R || !t || width <= 0 || height <= 0 ||
+      (n_queue && !d_queue))
+    return set_err(h, FF_ERR_BAD_ARG, "ff_loop_delete_frame: NULL pointer or empty image");
+  CK(cudaSetDevice(h->cfg.device));
+  FCK(settle(h));
+  cudaStream_t s = h->stream;
+  if (n_queue > h->loop_slots_cap) {
+    cudaFree(h->d_loop_slots);
+    h->d_loop_slots = nullptr;
+    h->loop_slots_cap = 0;
+    CK(alloc(&h->d_loop_slots, (size_t)n_queue));
+    h->loop_slots_cap = n_queue;
+  }
+  if (n_queue) {
+    launch_loop_slots(d_queue, n_queue, h->d_loop_map, h->loop_cap, h->d_loop_slots, h->d_loop_st, s);
+    LoopFrame L;
+    L.q = cam_grid_to_camera(h, K, R, t);  // as deleteOldLoopPoses builds pInv (geometryfusion_mipmap_cpu.cpp:3990-4005)
+    L.depth = d_depth;
+    L.red = d_red;
+    L.green = d_green;
+    L.blue = d_blue;
+    L.W = width;
+    L.H = height;
+    L.queue = d_queue;
+    L.slots = h->d_loop_slots;
+    L.taken = h->d_loop_st + 1;
+    L.leaf = h->d_leaf;
+    L.sdf = h->d_loop_sdf;
+    L.wgt = h->d_loop_wgt;
+    L.col = h->d_loop_col;
+    L.rcp_tab = h->d_rcp_tab;
+    L.rcp_shift = h->rcp_shift;
+    L.scale = h->cfg.scale;
+    L.thr = h->cfg.threshold;
+    launch_loop_delete(L, h->d_rcp_tab != nullptr, h->sm_count * 4, s);
+    CK(cudaGetLastError());
+  }
+  CK(cudaMemcpyAsync(h->h_loop_st, h->d_loop_st, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (complete) *complete = (!n_queue || h->h_loop_st[1] >= n_queue) ? 1 : 0;
+  return FF_OK;
+}
+
+ff_status ff_loop_get(ff_handle *h, uint32_t *n_mapped, uint32_t *leaf_slot, float *sdf, float *weight,
+                      uint16_t *rgb) {
+  if (!h || !n_mapped) return FF_ERR_BAD_ARG;
+  if (!h->loop_cap) return set_err(h, FF_ERR_STATE, "ff_loop_get: call ff_loop_begin first");
+  CK(cudaSetDevice(h->cfg.device));
+  cudaStream_t s = h->stream;
+  CK(cudaMemcpyAsync(h->h_loop_st, h->d_loop_st, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  const uint32_t n = h->h_loop_st[0];
+  *n_mapped = n;
+  const uint32_t nl = std::min(h->leaves_used, h->cfg.leaves_max);
+  if (leaf_slot && nl) CK(cudaMemcpyAsync(leaf_slot, h->d_loop_map, sizeof(uint32_t) * nl, cudaMemcpyDeviceToHost, s));
+  if (sdf && n) CK(cudaMemcpyAsync(sdf, h->d_loop_sdf, sizeof(float) * n * 512, cudaMemcpyDeviceToHost, s));
+  if (weight && n) CK(cudaMemcpyAsync(weight, h->d_loop_wgt, sizeof(float) * n * 512, cudaMemcpyDeviceToHost, s));
+  if (rgb && n) {
+    std::vector<uint16_t> planes((size_t)n * 1536);
+    CK(cudaMemcpyAsync(planes.data(), h->d_loop_col, sizeof(uint16_t) * n * 1536, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (size_t b = 0; b < n; b++)
+      for (int c = 0; c < 3; c++)
+        for (int v = 0; v < 512; v++) rgb[(b * 512 + v) * 3 + c] = planes[b * 1536 + c * 512 + v];
+  }
+  CK(cudaStreamSynchronize(s));
   return FF_OK;
 }
 

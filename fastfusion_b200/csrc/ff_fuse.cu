@@ -488,6 +488,178 @@ void launch_halo_unpack(const void *in, uint64_t n, uint32_t leaves_max, float *
     k_halo_unpack<false><<<grid, 512, 0, s>>>((const uint8_t *)in, n, leaves_max, sdf, wgt, sdf16, wgt16, col, rec);
 }
 
+// ---------------------------------------------------------------------------
+// Loop closure: removing a fused frame's contribution into separate loop
+// arrays (the reference's deleteOldLoopPoses, geometryfusion_mipmap_cpu.cpp:
+// 3933-4025, with updateWrapper_deleteloop / update8AddLoopSSESingleDeleteloop,
+// loopclosure.cpp:15-309).
+// ---------------------------------------------------------------------------
+
+// Slots of the frame's queued bricks in the loop arrays, in queue order: a
+// brick without a slot gets the next one (updateWrapper_deleteloop,
+// loopclosure.cpp:281-289).  When the slots run out, that entry and every
+// later one are left out (the reference returns there).  One block;
+// st[0] = slots in use (in and out), st[1] = entries taken.
+__global__ void __launch_bounds__(1024) k_loop_slots(const uint32_t *__restrict__ queue, uint32_t nq, uint32_t *map,
+                                                     uint32_t capacity, uint32_t *slots, uint32_t *st) {
+  __shared__ uint32_t warp_sum[32];
+  __shared__ uint32_t s_base, s_stop;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  if (t == 0) {
+    s_base = st[0];
+    s_stop = nq;
+  }
+  __syncthreads();
+  for (uint32_t c0 = 0; c0 < nq; c0 += 1024) {
+    const uint32_t i = c0 + t;
+    uint32_t b = 0, cur = 0;
+    bool fresh = false;
+    if (i < nq) {
+      b = queue[i];
+      cur = map[b];
+      fresh = cur >= s_base;  // no slot yet (slots below the count in use are taken)
+    }
+    // exclusive prefix of the fresh entries of this chunk
+    const unsigned bal = __ballot_sync(0xffffffffu, fresh);
+    if (lane == 0) warp_sum[w] = __popc(bal);
+    __syncthreads();
+    if (w == 0) {
+      uint32_t v = warp_sum[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+      }
+      warp_sum[lane] = v;  // inclusive
+    }
+    __syncthreads();
+    const uint32_t before = (w ? warp_sum[w - 1] : 0u) + __popc(bal & ((1u << lane) - 1u));
+    const uint32_t chunk_fresh = warp_sum[31];
+    if (i < nq) {
+      const uint32_t base = s_base;
+      if (fresh) {
+        const uint32_t slot = base + before;
+        if (slot >= capacity) {
+          atomicMin(&s_stop, i);
+        } else {
+          map[b] = slot;
+          slots[i] = slot;
+        }
+      } else {
+        slots[i] = cur;
+      }
+    }
+    __syncthreads();
+    // slots are handed out consecutively, so the ones given are exactly those
+    // below the capacity; entries past the first one that found none are left
+    // out (fresh ones there received no slot)
+    if (t == 0) s_base = min(s_base + chunk_fresh, capacity);
+    __syncthreads();
+    if (s_stop < nq) break;
+  }
+  if (t == 0) {
+    st[0] = s_base;
+    st[1] = s_stop;
+  }
+}
+
+template <bool RCP_HOST>
+__global__ void __launch_bounds__(512) k_loop_delete(LoopFrame L) {
+  const int v = threadIdx.x;
+  const int x = v & 7, y = (v >> 3) & 7, z = v >> 6;
+  const uint32_t n = *L.taken;
+  const CamF &q = L.q;
+  const float *M = q.r;
+  for (uint32_t e = blockIdx.x; e < n; e += gridDim.x) {
+    const uint32_t brick = L.queue[e];
+    const uint32_t slot = L.slots[e];
+    const ushort4 o = L.leaf[brick];
+    const float ls = (float)o.w;
+    const float fls = __fmul_rz(ls, L.scale);
+    const float fo0 = (float)o.x, fo1 = (float)o.y, fo2 = (float)o.z;
+    float pzx = __fadd_rz(__fmul_rz(__fadd_rz(__fadd_rz(__fmul_rz(M[0], fo0), __fmul_rz(M[1], fo1)), __fmul_rz(M[2], fo2)), L.scale), q.t[0]);
+    float pzy = __fadd_rz(__fmul_rz(__fadd_rz(__fadd_rz(__fmul_rz(M[3], fo0), __fmul_rz(M[4], fo1)), __fmul_rz(M[5], fo2)), L.scale), q.t[1]);
+    float pzz = __fadd_rz(__fmul_rz(__fadd_rz(__fadd_rz(__fmul_rz(M[6], fo0), __fmul_rz(M[7], fo1)), __fmul_rz(M[8], fo2)), L.scale), q.t[2]);
+    const float d11 = __fmul_rz(M[0], fls), d21 = __fmul_rz(M[3], fls), d31 = __fmul_rz(M[6], fls);
+    const float d12 = __fmul_rz(M[1], fls), d22 = __fmul_rz(M[4], fls), d32 = __fmul_rz(M[7], fls);
+    const float d13 = __fmul_rz(M[2], fls), d23 = __fmul_rz(M[5], fls), d33 = __fmul_rz(M[8], fls);
+    for (int i = 0; i < z; i++) {
+      pzx = __fadd_rz(pzx, d13);
+      pzy = __fadd_rz(pzy, d23);
+      pzz = __fadd_rz(pzz, d33);
+    }
+    for (int i = 0; i < y; i++) {
+      pzx = __fadd_rz(pzx, d12);
+      pzy = __fadd_rz(pzy, d22);
+      pzz = __fadd_rz(pzz, d32);
+    }
+    // 4-wide rows: lanes 0, d, 2d, 3d from the row start, the second half
+    // from the start advanced by 4d (loopclosure.cpp:40-60)
+    if (x >= 4) {
+      pzx = __fadd_rz(pzx, __fmul_rz(d11, 4.0f));
+      pzy = __fadd_rz(pzy, __fmul_rz(d21, 4.0f));
+      pzz = __fadd_rz(pzz, __fmul_rz(d31, 4.0f));
+    }
+    const int l = x & 3;
+    const float kx = l == 0 ? 0.0f : (l == 1 ? d11 : __fmul_rz((float)l, d11));
+    const float ky = l == 0 ? 0.0f : (l == 1 ? d21 : __fmul_rz((float)l, d21));
+    const float kz = l == 0 ? 0.0f : (l == 1 ? d31 : __fmul_rz((float)l, d31));
+    const float px = __fadd_rz(pzx, kx), py = __fadd_rz(pzy, ky), pz = __fadd_rz(pzz, kz);
+    const int W = L.W, H = L.H;
+    const float len = __fsqrt_rz(__fadd_rz(__fadd_rz(__fmul_rz(px, px), __fmul_rz(py, py)), __fmul_rz(pz, pz)));
+    const float rc = rcp_upd<RCP_HOST>(pz, L.rcp_tab, L.rcp_shift);
+    const int imx = cvt_x86_rz(__fadd_rz(q.cx, __fmul_rz(q.fx, __fmul_rz(px, rc))));
+    const int imy = cvt_x86_rz(__fadd_rz(q.cy, __fmul_rz(q.fy, __fmul_rz(py, rc))));
+    const int ii = W * max(min(imy, H - 1), 0) + max(min(imx, W - 1), 0);
+    const float h = __ldg(L.depth + ii);
+    const float rI = __fmul_rz((float)__ldg(L.red + ii), COLOR_MUL);
+    const float gI = __fmul_rz((float)__ldg(L.green + ii), COLOR_MUL);
+    const float bI = __fmul_rz((float)__ldg(L.blue + ii), COLOR_MUL);
+    const float dInc = __fsub_rz(len, __fmul_rz(__fmul_rz(len, rc), h));
+    // no maximum distance here; a hole (NaN depth) fails the ordered test
+    const bool msk = pz > 0.0f && imy < H && imy > -1 && imx < W && imx > -1 && !isnan(dInc);
+    const float thrD = __fmul_rz(L.thr, ls);
+    const float thrW = __fmul_rz(__fmul_rz(WEIGHT_FACTOR, L.thr), ls);
+    const float front = dInc < DIST_W_EPS ? 1.0f : 0.0f;
+    const float back = (dInc >= DIST_W_EPS && dInc < thrW) ? 1.0f : 0.0f;
+    // the fall-off with its sign turned (loopclosure.cpp:166-172)
+    const float fall =
+        __fmul_rz(__fsub_rz(dInc, thrW), rcp_upd<RCP_HOST>(__fsub_rz(thrW, DIST_W_EPS), L.rcp_tab, L.rcp_shift));
+    const float wInc = msk ? __fadd_rz(front, __fmul_rz(fall, back)) : 0.0f;
+    const size_t vi = (size_t)slot * 512 + v;
+    const float wAcc = L.wgt[vi], dAcc = L.sdf[vi];
+    const float wNew = __fadd_rz(wAcc, wInc);
+    const float factor = rcp_upd<RCP_HOST>(__fadd_rz(wNew, wNew <= 0.0f ? 1.0f : 0.0f), L.rcp_tab, L.rcp_shift);
+    const float mn = thrD < dInc ? thrD : dInc;                    // _mm_min_ps(thrD, dInc)
+    const float lo = __fmul_rz(-1.0f, thrD);
+    const float tr = lo > mn ? lo : mn;                            // _mm_max_ps(-thrD, min)
+    const float add = msk ? __fmul_rz(tr, wInc) : 0.0f;
+    L.sdf[vi] = __fmul_rz(__fadd_rz(__fmul_rz(dAcc, wAcc), add), factor);
+    L.wgt[vi] = wNew;
+    uint16_t *cb = L.col + (size_t)slot * 1536 + v;
+    const float inc[3] = {rI, gI, bI};
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float acc = (float)cb[c * 512];
+      const float val = __fmul_rz(__fadd_rz(__fmul_rz(acc, wAcc), __fmul_rz(inc[c], wInc)), factor);
+      // the float -> unsigned short store of the reference (no clamp): a
+      // truncating conversion to int, of which the low 16 bits are kept
+      cb[c * 512] = (uint16_t)cvt_x86_rz(val);
+    }
+  }
+}
+
+void launch_loop_slots(const uint32_t *queue, uint32_t nq, uint32_t *map, uint32_t capacity, uint32_t *slots,
+                       uint32_t *st, cudaStream_t s) {
+  note_launch();
+  k_loop_slots<<<1, 1024, 0, s>>>(queue, nq, map, capacity, slots, st);
+}
+
+void launch_loop_delete(const LoopFrame &L, bool rcp_host, int grid, cudaStream_t s) {
+  note_launch();
+  if (rcp_host) k_loop_delete<true><<<grid, 512, 0, s>>>(L);
+  else k_loop_delete<false><<<grid, 512, 0, s>>>(L);
+}
+
 // Block shapes of the voxel update: (bricks per block, blocks per SM the
 // register budget is cut for).  Shape 0 is the default.
 static const int FUSE_SHAPES[FUSE_SHAPE_COUNT][2] = {{1, 4}, {1, 3}, {2, 2}, {2, 1}};

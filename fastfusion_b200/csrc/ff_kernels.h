@@ -122,6 +122,28 @@ struct FuseBatch {
 // Launch the deferred update pass (grid: blocks of 512 threads).
 void launch_fuse_multi(const FuseBatch &fb, int storage, bool rcp_host, int grid, cudaStream_t s);
 
+// Loop closure: one fused frame removed into the loop arrays
+// (update8AddLoopSSESingleDeleteloop, loopclosure.cpp:15-228).
+struct LoopFrame {
+  CamF q;                      // voxel grid -> camera of the frame
+  const float *depth;          // metres, NaN = no depth
+  const uint8_t *red, *green, *blue;
+  int W, H;
+  const uint32_t *queue;       // the frame's queued leaves
+  const uint32_t *slots;       // their loop slots
+  const uint32_t *taken;       // entries of the queue that have a slot
+  const ushort4 *leaf;
+  float *sdf, *wgt;            // loop arrays [slot][512]
+  uint16_t *col;               // [slot][3][512]
+  const uint32_t *rcp_tab;
+  int rcp_shift;
+  float scale, thr;
+};
+// st[0]: slots in use; st[1] (out): queue entries that got a slot.
+void launch_loop_slots(const uint32_t *queue, uint32_t nq, uint32_t *map, uint32_t capacity, uint32_t *slots,
+                       uint32_t *st, cudaStream_t s);
+void launch_loop_delete(const LoopFrame &L, bool rcp_host, int grid, cudaStream_t s);
+
 // Halo exchange of a sharded map (records: uint32 leaf index, 12 bytes of
 // padding, SDF, weight and colour planes as the pool stores them).
 size_t halo_record_bytes(bool fp16);

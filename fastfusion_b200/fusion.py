@@ -77,6 +77,10 @@ SIGNATURES = {
     "ff_set_update_batch": (_i32, [_vp, _i32]),
     "ff_halo_export": (_i32, [_vp, _vp, _u64, ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
     "ff_halo_import": (_i32, [_vp, _vp, _u64]),
+    "ff_loop_begin": (_i32, [_vp, _u32]),
+    "ff_loop_delete_frame": (_i32, [_vp, _vp, _vp, _vp, _vp, _i32, _i32, _vp, _vp, _vp, _vp, _u32,
+                                    ctypes.POINTER(_i32)]),
+    "ff_loop_get": (_i32, [_vp, ctypes.POINTER(_u32), _vp, _vp, _vp, _vp]),
     "ff_inject_error": (_i32, [_vp, _i32]),
     "ff_add_map_u16": (_i32, [_vp, _vp, _i32, _i32, _sz, _vp, _sz, _vp, _vp, _vp, _f32, _f32, _vp]),
     "ff_add_map_u16_device": (_i32, [_vp, _vp, _vp, _i32, _i32, _vp, _vp, _vp, _f32, _f32, _vp]),
@@ -464,6 +468,36 @@ class FusionMipMapCPU:
         """Make the next frame report a failure as the device would (tests of
         the error paths; 0 cancels)."""
         self._check(self._L.ff_inject_error(self._h, int(what)))
+
+    # -- loop closure: removing fused frames (deleteOldLoopPoses) ------------
+    def loop_begin(self, capacity: int = 100000):
+        """Zeroed loop arrays for `capacity` bricks, no brick mapped."""
+        self._check(self._L.ff_loop_begin(self._h, int(capacity)))
+
+    def loop_delete_frame(self, d_depth: int, d_red: int, d_green: int, d_blue: int, width: int, height: int,
+                          caminfo: CameraInfo, d_queue: int, n_queue: int) -> bool:
+        """One fused frame's removal into the loop arrays (device pointers:
+        depth float metres with NaN holes, colour planes, the frame's queued
+        leaves); False when the slots ran out."""
+        pK, pR, pt = caminfo._ptrs
+        done = ctypes.c_int()
+        self._check(self._L.ff_loop_delete_frame(self._h, int(d_depth), int(d_red), int(d_green), int(d_blue),
+                                                 int(width), int(height), pK, pR, pt, int(d_queue), int(n_queue),
+                                                 ctypes.byref(done)))
+        return bool(done.value)
+
+    def loop_arrays(self):
+        """(leaf -> slot uint32[leaves], sdf float[n,512], weight float[n,512],
+        colour uint16[n,512,3]) of the slots in use."""
+        n = ctypes.c_uint32()
+        self._check(self._L.ff_loop_get(self._h, ctypes.byref(n), None, None, None, None))
+        nl = min(self.stats()["leaves_used"], self.stats()["leaves_max"])
+        m = np.zeros(nl, np.uint32)
+        d = np.zeros((n.value, 512), np.float32)
+        w = np.zeros((n.value, 512), np.float32)
+        c = np.zeros((n.value, 512, 3), np.uint16)
+        self._check(self._L.ff_loop_get(self._h, ctypes.byref(n), _p(m), _p(d), _p(w), _p(c)))
+        return m, d, w, c
 
     def halo_count(self) -> tuple[int, int]:
         """(records, bytes per record) the next halo export would write."""

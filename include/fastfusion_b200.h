@@ -198,6 +198,36 @@ typedef struct {
  * parts' meshes are the whole map's mesh. */
 ff_status ff_set_shard(ff_handle *h, int shard, int shards);
 
+/* ---- Loop closure: removing fused frames (the reference's deleteOldLoopPoses) ----
+ *
+ * When a trajectory is corrected, the reference's loop closure removes the
+ * contribution of already fused frames: a second set of voxel arrays ("loop
+ * arrays") for at most `capacity` bricks (MAX_LOOP_CLOSURE_LEAVES = 100,000
+ * there, definitions.h:124) receives, per frame, the update of
+ * update8AddLoopSSESingleDeleteloop (loopclosure.cpp:15-228) -- the frame's
+ * depth (float metres, NaN where there is none) and colour planes, projected
+ * with the frame's corrected pose, with the weight fall-off's sign turned --
+ * over the bricks the frame queued when it was fused; each brick gets the
+ * next free slot in queue order the first time (updateWrapper_deleteloop,
+ * loopclosure.cpp:232-309).  The voxel values equal the reference's bit for
+ * bit with FF_RCP_HOST.
+ *
+ * ff_loop_begin: (re)start with zeroed loop arrays for `capacity` bricks and
+ * no brick mapped (updateArraysForLoopClosure,
+ * geometryfusion_mipmap_cpu.cpp:3910-3931).  ff_loop_delete_frame: one frame
+ * (device memory: depth float[h][w], red/green/blue uint8[h][w], the queue of
+ * the frame's leaves -- ff_get_queue after its addMap); *complete = 0 when the
+ * slots ran out (the entry that found none and every later one are left out,
+ * as the reference returns there).  ff_loop_get: slots in use; per leaf its
+ * slot (0xFFFFFFFE: none; leaf_slot[leaves_used]); and the loop arrays of the
+ * slots in use as ff_get_bricks lays out bricks (any pointer may be NULL). */
+ff_status ff_loop_begin(ff_handle *h, uint32_t capacity);
+ff_status ff_loop_delete_frame(ff_handle *h, const float *d_depth, const uint8_t *d_red, const uint8_t *d_green,
+                               const uint8_t *d_blue, int width, int height, const double K[4], const double R[9],
+                               const double t[3], const uint32_t *d_queue, uint32_t n_queue, int *complete);
+ff_status ff_loop_get(ff_handle *h, uint32_t *n_mapped, uint32_t *leaf_slot, float *sdf, float *weight,
+                      uint16_t *rgb);
+
 /* Halo export of a part of a sharded map: the bricks this part owns whose
  * voxels changed since its last export (with a buffer), as records of
  * *record_bytes bytes each -- uint32 leaf index, 12 bytes of padding, then

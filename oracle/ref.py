@@ -59,6 +59,9 @@ def lib():
         L.ref_cells.argtypes = [vp, vp]
         L.ref_queue_all_cells.argtypes = [vp]
         L.ref_set_thread_meshing.argtypes = [vp, ctypes.c_int]
+        L.ref_loop_delete.restype = ctypes.c_int
+        L.ref_loop_delete.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, ll, vp, vp,
+                                      ctypes.c_uint32, vp, vp, vp]
         L.ref_cell_mesh.restype = ll
         L.ref_cell_mesh.argtypes = [vp, ll, vp, vp, vp, ctypes.POINTER(ll)]
         L.ref_mc_offset_table.argtypes = [vp]
@@ -103,6 +106,25 @@ class RefFusion:
 
     def update_meshes(self) -> bool:
         return bool(self.L.ref_update_meshes(self.h))
+
+    def loop_delete(self, depth_m, red, green, blue, K, R, t, queue, leaf_map, n_mapped, capacity, dist, wgt,
+                    col) -> tuple[bool, int]:
+        """The reference's removal of one fused frame into caller loop arrays
+        (deleteOldLoopPoses' camera set-up, then updateWrapper_deleteloop):
+        leaf_map (uint32, one per leaf) and the arrays are updated in place;
+        returns (completed, slots in use)."""
+        depth_m = np.ascontiguousarray(depth_m, np.float32)
+        h, w = depth_m.shape
+        planes = [np.ascontiguousarray(a, np.uint8) for a in (red, green, blue)]
+        K = np.ascontiguousarray(K, np.float64)
+        R = np.ascontiguousarray(R, np.float64)
+        t = np.ascontiguousarray(t, np.float64)
+        q = np.ascontiguousarray(queue, np.uint32)
+        nm = np.array([n_mapped], np.uint32)
+        ok = self.L.ref_loop_delete(self.h, _p(depth_m), _p(planes[0]), _p(planes[1]), _p(planes[2]), w, h, _p(K),
+                                    _p(R), _p(t), _p(q), len(q), _p(leaf_map), _p(nm), int(capacity), _p(dist),
+                                    _p(wgt), _p(col))
+        return bool(ok), int(nm[0])
 
     def set_thread_meshing(self, on: bool):
         """The reference's setThreadMeshing: meshing on a second thread,

@@ -23,6 +23,7 @@
 #define protected public
 #include <fusion/geometryfusion_mipmap_cpu.hpp>
 #undef protected
+#include <fusion/loopclosure.hpp>
 
 #include <auxiliary/memory.hpp>
 #include <fcntl.h>
@@ -128,6 +129,55 @@ int ref_add_map_f32(void *h, const float *depth, const uint8_t *blue, const uint
 }
 
 int ref_update_meshes(void *h) { return ((FusionMipMapCPU *)h)->updateMeshes() ? 1 : 0; }
+
+/* Loop closure's removal of one fused frame (deleteOldLoopPoses,
+ * geometryfusion_mipmap_cpu.cpp:3933-4025): the frame's camera parameters
+ * built as that function builds them (extrinsic inverse of the pose, the
+ * map's offset folded in, rounded once to float), then the reference's
+ * updateWrapper_deleteloop (loopclosure.cpp:232-309) over the frame's leaf
+ * queue, with this object's leaf table and the caller's loop arrays: depth in
+ * metres (NaN = no depth), colour planes, leaf_map (leaves -> loop slot,
+ * 0xFFFFFFFE = none yet), *n_mapped slots in use of `capacity`; dist/wgt
+ * float[capacity * 512], col uint16[capacity * 512][3].  Returns the
+ * wrapper's result (0: the slots ran out). */
+int ref_loop_delete(void *h, const float *depth, const uint8_t *red, const uint8_t *green, const uint8_t *blue, int w,
+                    int hgt, const double *K4, const double *R9, const double *t3, uint32_t *queue, long long nq,
+                    uint32_t *leaf_map, uint32_t *n_mapped, uint32_t capacity, float *dist, float *wgt,
+                    uint16_t *col) {
+  FusionMipMapCPU *f = (FusionMipMapCPU *)h;
+  CameraInfo cam;
+  cv::Mat K = cv::Mat::eye(3, 3, CV_64FC1);
+  K.at<double>(0, 0) = K4[0];
+  K.at<double>(1, 1) = K4[1];
+  K.at<double>(0, 2) = K4[2];
+  K.at<double>(1, 2) = K4[3];
+  cam.setIntrinsic(K);
+  cv::Mat E = cv::Mat::eye(4, 4, CV_64FC1);
+  for (int r = 0; r < 3; r++) {
+    for (int k = 0; k < 3; k++) E.at<double>(r, k) = R9[r * 3 + k];
+    E.at<double>(r, 3) = t3[r];
+  }
+  cam.setExtrinsic(E);
+  cam.setExtrinsic(cam.getExtrinsicInverse());
+  cv::Mat rot = cam.getRotation(), tr = cam.getTranslation(), in = cam.getIntrinsic();
+  const double ox = f->_offset.x, oy = f->_offset.y, oz = f->_offset.z;
+  camPamsFloat p(rot.at<double>(0, 0), rot.at<double>(0, 1), rot.at<double>(0, 2), rot.at<double>(1, 0),
+                 rot.at<double>(1, 1), rot.at<double>(1, 2), rot.at<double>(2, 0), rot.at<double>(2, 1),
+                 rot.at<double>(2, 2),
+                 rot.at<double>(0, 0) * ox + rot.at<double>(0, 1) * oy + rot.at<double>(0, 2) * oz + tr.at<double>(0, 0),
+                 rot.at<double>(1, 0) * ox + rot.at<double>(1, 1) * oy + rot.at<double>(1, 2) * oz + tr.at<double>(1, 0),
+                 rot.at<double>(2, 0) * ox + rot.at<double>(2, 1) * oy + rot.at<double>(2, 2) * oz + tr.at<double>(2, 0),
+                 in.at<double>(0, 0), in.at<double>(1, 1), in.at<double>(0, 2), in.at<double>(1, 2));
+  volumetype mapped = *n_mapped;
+  const bool ok = updateWrapper_deleteloop(
+      threadparameterLoop(depth, red, green, blue, w, hgt, p.r11, p.r12, p.r13, p.t1, p.r21, p.r22, p.r23, p.t2,
+                          p.r31, p.r32, p.r33, p.t3, p.fx, p.fy, p.cx, p.cy, f->_scale, f->_distanceThreshold,
+                          (volumetype *)queue, f->_leafPos, f->_leafScale, dist, wgt, (colortype3 *)col,
+                          f->_brickLength),
+      (size_t)nq, (volumetype *)leaf_map, (volumetype)capacity, &mapped);
+  *n_mapped = mapped;
+  return ok ? 1 : 0;
+}
 
 /* Mesh of the last finished update: counts, then copies. */
 void ref_mesh_counts(void *h, long long *nv, long long *nf) {
