@@ -1283,11 +1283,111 @@ __global__ void k_mark_dirty(const Cell *cells, uint32_t n, const Cell *old_cell
   }
 }
 
-__global__ void k_counts_to_arrays(const CellOut *out, uint32_t n, uint64_t *nv, uint64_t *nf) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  nv[i] = out[i].nv;
-  nf[i] = out[i].nf;
+// ---------------------------------------------------------------------------
+// Exclusive scans of the cells' vertex and face counts (both at once): the
+// mesh offsets of every cell, and the totals at index n.  Three launches: the
+// sums of tiles of 4096 cells, a scan of the tile sums in one block, then
+// each tile's scan from its offset.
+// ---------------------------------------------------------------------------
+constexpr int SCAN_THREADS = 1024, SCAN_PER_THREAD = 4, SCAN_TILE = SCAN_THREADS * SCAN_PER_THREAD;
+
+// Exclusive prefix over the block of each thread's pair (a, b); the block's
+// totals in *ta, *tb.  Every thread of the 1024-thread block calls it.
+__device__ __forceinline__ void block_scan2(uint64_t a, uint64_t b, uint64_t &pa, uint64_t &pb, uint64_t *ta,
+                                            uint64_t *tb) {
+  __shared__ uint64_t wa[32], wb[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint64_t ia = a, ib = b;  // inclusive within the warp
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t ua = __shfl_up_sync(0xffffffffu, ia, o), ub = __shfl_up_sync(0xffffffffu, ib, o);
+    if (lane >= o) ia += ua, ib += ub;
+  }
+  if (lane == 31) wa[w] = ia, wb[w] = ib;
+  __syncthreads();
+  if (w == 0) {
+    uint64_t xa = wa[lane], xb = wb[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t ua = __shfl_up_sync(0xffffffffu, xa, o), ub = __shfl_up_sync(0xffffffffu, xb, o);
+      if (lane >= o) xa += ua, xb += ub;
+    }
+    wa[lane] = xa;  // inclusive over warps
+    wb[lane] = xb;
+  }
+  __syncthreads();
+  pa = (w ? wa[w - 1] : 0ull) + ia - a;
+  pb = (w ? wb[w - 1] : 0ull) + ib - b;
+  if (ta) *ta = wa[31];
+  if (tb) *tb = wb[31];
+  __syncthreads();  // (wa/wb reused by the next call)
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_count_tile_sums(const CellOut *__restrict__ out, uint32_t n,
+                                                                  uint64_t *tile_v, uint64_t *tile_f) {
+  const uint32_t i0 = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_PER_THREAD;
+  uint64_t a = 0, b = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_PER_THREAD; k++)
+    if (i0 + k < n) a += out[i0 + k].nv, b += out[i0 + k].nf;
+  uint64_t pa, pb, ta, tb;
+  block_scan2(a, b, pa, pb, &ta, &tb);
+  if (threadIdx.x == 0) {
+    tile_v[blockIdx.x] = ta;
+    tile_f[blockIdx.x] = tb;
+  }
+}
+
+// One block: tile sums -> exclusive tile offsets (in place), totals to
+// vbase[n] and fbase[n].
+__global__ void __launch_bounds__(SCAN_THREADS) k_count_tile_scan(uint64_t *tile_v, uint64_t *tile_f, uint32_t ntiles,
+                                                                  uint64_t *vbase, uint64_t *fbase, uint32_t n) {
+  __shared__ uint64_t carry_v, carry_f;
+  if (threadIdx.x == 0) carry_v = carry_f = 0;
+  __syncthreads();
+  for (uint32_t c0 = 0; c0 < ntiles; c0 += SCAN_THREADS) {
+    const uint32_t i = c0 + threadIdx.x;
+    const uint64_t a = i < ntiles ? tile_v[i] : 0ull, b = i < ntiles ? tile_f[i] : 0ull;
+    uint64_t pa, pb, ta, tb;
+    block_scan2(a, b, pa, pb, &ta, &tb);
+    if (i < ntiles) {
+      tile_v[i] = carry_v + pa;
+      tile_f[i] = carry_f + pb;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) carry_v += ta, carry_f += tb;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    vbase[n] = carry_v;
+    fbase[n] = carry_f;
+  }
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_count_tile_apply(const CellOut *__restrict__ out, uint32_t n,
+                                                                   const uint64_t *tile_v, const uint64_t *tile_f,
+                                                                   uint64_t *vbase, uint64_t *fbase) {
+  const uint32_t i0 = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_PER_THREAD;
+  uint32_t cv[SCAN_PER_THREAD], cf[SCAN_PER_THREAD];
+  uint64_t a = 0, b = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_PER_THREAD; k++) {
+    const bool in = i0 + k < n;
+    cv[k] = in ? out[i0 + k].nv : 0u;
+    cf[k] = in ? out[i0 + k].nf : 0u;
+    a += cv[k];
+    b += cf[k];
+  }
+  uint64_t pa, pb;
+  block_scan2(a, b, pa, pb, nullptr, nullptr);
+  uint64_t ov = tile_v[blockIdx.x] + pa, of = tile_f[blockIdx.x] + pb;
+#pragma unroll
+  for (int k = 0; k < SCAN_PER_THREAD; k++) {
+    if (i0 + k < n) {
+      vbase[i0 + k] = ov;
+      fbase[i0 + k] = of;
+    }
+    ov += cv[k];
+    of += cf[k];
+  }
 }
 
 // clean cells copy their previous vertices and faces (faces re-based)
@@ -1400,6 +1500,7 @@ struct MeshImpl {
   // per-cell counts and offsets: current and previous
   CellOut *out = nullptr, *old_out = nullptr;
   size_t cap_out = 0, cap_oldout = 0;
+  // nv/nf: the count scan's tile sums (vertices, faces) of 4096-cell tiles
   uint64_t *nv = nullptr, *nf = nullptr, *vbase = nullptr, *fbase = nullptr, *old_vbase = nullptr,
            *old_fbase = nullptr;
   size_t cap_nv = 0, cap_nf = 0, cap_vb = 0, cap_fb = 0, cap_ovb = 0, cap_ofb = 0;
@@ -1611,8 +1712,6 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   MCK(grow_buf(I.out, I.cap_out, ncells, s));
   MCK(grow_buf(I.dirty, I.cap_dirty, ncells, s));
   MCK(grow_buf(I.old_index, I.cap_oi, ncells, s));
-  MCK(grow_buf(I.nv, I.cap_nv, ncells + 1, s));
-  MCK(grow_buf(I.nf, I.cap_nf, ncells + 1, s));
   MCK(grow_buf(I.vbase, I.cap_vb, ncells + 1, s));
   MCK(grow_buf(I.fbase, I.cap_fb, ncells + 1, s));
   MCK(grow_buf(I.dlist, I.cap_dlist, ncells, s));
@@ -1664,22 +1763,16 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   const int pi_count = pi;
   P.end(pi_count, 0.0, s);
   MCK(cudaGetLastError());
-  // exclusive scans of vertex and face counts -> per-cell bases
-  if (ncells) k_counts_to_arrays<<<(ncells + 255) / 256, 256, 0, s>>>(I.out, ncells, I.nv, I.nf);
-  MCK(cudaMemsetAsync(I.nv + ncells, 0, sizeof(uint64_t), s));
-  MCK(cudaMemsetAsync(I.nf + ncells, 0, sizeof(uint64_t), s));
-  size_t bytes = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, bytes, I.nv, I.vbase, (int)ncells + 1, s);
-  if (bytes > I.scan_tmp_bytes) {
-    if (I.scan_tmp) MCK(cudaFreeAsync(I.scan_tmp, s));
-    I.scan_tmp = nullptr;
-    MCK(pool_alloc(&I.scan_tmp, bytes, s));
-    I.scan_tmp_bytes = bytes;
+  // exclusive scans of vertex and face counts -> per-cell bases (totals at ncells)
+  {
+    const uint32_t ntiles = (ncells + SCAN_TILE - 1) / SCAN_TILE;
+    MCK(grow_buf(I.nv, I.cap_nv, std::max<uint32_t>(ntiles, 1), s));  // tile sums of the vertex counts
+    MCK(grow_buf(I.nf, I.cap_nf, std::max<uint32_t>(ntiles, 1), s));  // and of the face counts
+    note_launch(ntiles ? 3 : 1);
+    if (ntiles) k_count_tile_sums<<<ntiles, SCAN_THREADS, 0, s>>>(I.out, ncells, I.nv, I.nf);
+    k_count_tile_scan<<<1, SCAN_THREADS, 0, s>>>(I.nv, I.nf, ntiles, I.vbase, I.fbase, ncells);
+    if (ntiles) k_count_tile_apply<<<ntiles, SCAN_THREADS, 0, s>>>(I.out, ncells, I.nv, I.nf, I.vbase, I.fbase);
   }
-  note_lib_call();
-  note_lib_call();
-  MCK(cub::DeviceScan::ExclusiveSum(I.scan_tmp, I.scan_tmp_bytes, I.nv, I.vbase, (int)ncells + 1, s));
-  MCK(cub::DeviceScan::ExclusiveSum(I.scan_tmp, I.scan_tmp_bytes, I.nf, I.fbase, (int)ncells + 1, s));
   // totals, dirty count and samples through the pinned counter mirror
   uint64_t *h_tot = reinterpret_cast<uint64_t *>(I.h_count + HOST_TOTALS);
   MCK(cudaMemcpyAsync(h_tot + 0, I.vbase + ncells, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
@@ -1900,7 +1993,8 @@ cudaError_t prewarm_mesh_kernels() {
                        (const void *)k_gather_cells,       (const void *)k_mesh_lattice<false>,
                        (const void *)k_mesh_lattice<true>, (const void *)k_mesh_corner<false>,
                        (const void *)k_mesh_corner<true>,  (const void *)k_mark_dirty,
-                       (const void *)k_counts_to_arrays,   (const void *)k_copy_clean,
+                       (const void *)k_count_tile_sums,    (const void *)k_copy_clean,
+                       (const void *)k_count_tile_scan,    (const void *)k_count_tile_apply,
                        (const void *)k_fill_counts_from_old, (const void *)k_export_cells};
   for (const void *f : fns) {
     cudaFuncAttributes a;
