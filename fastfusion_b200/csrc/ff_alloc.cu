@@ -543,8 +543,9 @@ __global__ void k_insert(const BatchDesc *__restrict__ bd, int m0, int m1) {
   unsigned m = __ballot_sync(0xffffffffu, act);
   if (!act) return;
   if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&cnt->processed, __popc(m));
-  // octree entries this pixel reads on its descent (the algorithmic bytes of
-  // the insert: 16 B per level probed), summed per warp
+  // octree levels this pixel probes on its descent, summed per warp (the
+  // algorithmic bytes of the insert: 16 B per level -- the node's leaf and
+  // child slots, the leaf's frame stamp and its queue entry, 4 B each)
   const uint32_t levels = insert_pixel(F, i, vox[i], cnt);
   const uint32_t sum = __reduce_add_sync(m, levels);
   if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&cnt->levels, sum);
