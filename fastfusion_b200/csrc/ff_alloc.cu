@@ -432,8 +432,9 @@ __device__ __forceinline__ uint32_t wait_unlocked(uint32_t *tree, uint32_t ptr, 
 // One processed pixel of the frame F (voxel key v): bounding-box growth,
 // then (inside the volume) the descent of queryPointDepthSingle_func_subtree:
 // queue the existing coarser leaves on the path, allocate missing branches,
-// claim the final leaf.  Returns the number of octree levels probed.
-__device__ __forceinline__ uint32_t insert_pixel(const MapFrame &F, int i, int4 v, Counters *cnt) {
+// claim the final leaf.  Returns the number of octree levels probed; sets
+// *created when this pixel wrote a new branch or leaf slot into the octree.
+__device__ __forceinline__ uint32_t insert_descend(const MapFrame &F, int i, int4 v, Counters *cnt, bool *created) {
   const uint32_t n = F.n;
   const int bw = (int)F.bw;
   uint32_t *tree = F.tree;
@@ -475,6 +476,7 @@ __device__ __forceinline__ uint32_t insert_pixel(const MapFrame &F, int i, int4 
         __threadfence();
         atomicExch(tree + ptr, nb);
         child = nb;
+        *created = true;
       } else {
         child = old;
       }
@@ -508,6 +510,7 @@ __device__ __forceinline__ uint32_t insert_pixel(const MapFrame &F, int i, int4 
       pend[rec] = pl;
       __threadfence();
       atomicExch(tree + ptr, PENDING + rec);
+      *created = true;
       return probed;
     }
     cur = old;
@@ -519,6 +522,37 @@ __device__ __forceinline__ uint32_t insert_pixel(const MapFrame &F, int i, int4 
   } else if (cur < leaves_max) {
     queue_leaf(cur, frame, stamp, queue, cnt);
   }
+  return probed;
+}
+
+// Mark every branch on the path from the root to the branch that holds the
+// slot of voxel key v with the frame: the branches whose subtree gained a
+// branch or a leaf.  Only pixels that created something walk it again; the
+// path's child slots are all set by now, and are read past L1, which may
+// still hold a slot as it was before another thread set it.
+__device__ __forceinline__ void stamp_path(const MapFrame &F, int4 v) {
+  const uint32_t x = (uint16_t)v.x, y = (uint16_t)v.y, z = (uint16_t)v.z, target = (uint32_t)v.w;
+  uint32_t ox = 0, oy = 0, oz = 0, branch = 0;
+  uint32_t half = (uint16_t)(F.n >> 1);
+  for (int lvl = 0; lvl < 32; lvl++) {
+    uint32_t *b = F.bstamp + (branch >> 4);
+    if (*b != F.frame) *b = F.frame;
+    if ((half >> 1) < target) break;
+    const uint32_t co = (x >= ox + half) * 1u + (y >= oy + half) * 2u + (z >= oz + half) * 4u;
+    const uint32_t child = ld_volatile(F.tree + branch + co + 8);
+    if (child >= PENDING) break;  // a branch whose allocation failed: nothing below
+    ox += half * ((co & 1) != 0);
+    oy += half * ((co & 2) != 0);
+    oz += half * ((co & 4) != 0);
+    branch = child;
+    half >>= 1;
+  }
+}
+
+__device__ __forceinline__ uint32_t insert_pixel(const MapFrame &F, int i, int4 v, Counters *cnt) {
+  bool created = false;
+  const uint32_t probed = insert_descend(F, i, v, cnt, &created);
+  if (created) stamp_path(F, v);
   return probed;
 }
 

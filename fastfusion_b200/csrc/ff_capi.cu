@@ -77,6 +77,7 @@ struct ff_handle {
   __half *d_sdf16 = nullptr, *d_wgt16 = nullptr;
   uint16_t *d_col = nullptr;
   uint32_t *d_stamp = nullptr;
+  uint32_t *d_bstamp = nullptr;  // per branch: last frame that created something at or below it
   uint32_t *d_queue = nullptr;
   Counters *d_cnt = nullptr;
   Counters *h_cnt = nullptr;  // pinned
@@ -124,6 +125,7 @@ struct ff_handle {
   // and a failure the next frame reports as if a device wait had given up
   // (ff_inject_error)
   uint32_t spin_limit = SPIN_LIMIT;
+  int full_cells = 0;  // 1: regenerate every mesh cell at every update (ff_set_cell_generation)
   int inject = 0;
   // loop closure (ff_loop_begin): the loop arrays, each leaf's slot in them,
   // per queue entry its slot, [slots in use, entries taken]
@@ -583,7 +585,8 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
     if (alloc(&h->d_tree, h->cfg.branches_max) != cudaSuccess) { fail(FF_ERR_OOM_POOL, "tree"); break; }
     if (alloc(&h->d_leaf, L) != cudaSuccess || alloc(&h->d_parent, L) != cudaSuccess ||
         alloc(&h->d_stamp, L) != cudaSuccess || alloc(&h->d_queue_set[0], L) != cudaSuccess ||
-        alloc(&h->d_queue_set[1], L) != cudaSuccess) {
+        alloc(&h->d_queue_set[1], L) != cudaSuccess ||
+        alloc(&h->d_bstamp, (size_t)h->cfg.branches_max / 16 + 1) != cudaSuccess) {
       fail(FF_ERR_OOM_POOL, "leaf table");
       break;
     }
@@ -654,6 +657,7 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
     }
     launch_fill(h->d_tree, h->cfg.branches_max, BRANCHINIT, h->stream);
     cudaMemsetAsync(h->d_stamp, 0, sizeof(uint32_t) * L, h->stream);
+    cudaMemsetAsync(h->d_bstamp, 0, sizeof(uint32_t) * (h->cfg.branches_max / 16 + 1), h->stream);
     cudaMemsetAsync(h->d_parent, 0xFF, sizeof(uint32_t) * L, h->stream);
     cudaMemsetAsync(h->d_leaf, 0, sizeof(ushort4) * L, h->stream);
     if (h->d_sdf) {
@@ -685,7 +689,7 @@ ff_status ff_destroy(ff_handle *h) {
   mesh_free(h->mesh);
   h->prof.destroy();
   void *ptrs[] = {h->d_tree, h->d_leaf, h->d_parent, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
-                  h->d_stamp, h->d_queue_set[0], h->d_queue_set[1], h->d_cnt_set[0], h->d_cnt_set[1],
+                  h->d_stamp, h->d_bstamp, h->d_queue_set[0], h->d_queue_set[1], h->d_cnt_set[0], h->d_cnt_set[1],
                   h->d_barrier, h->d_depth_set[0], h->d_depth_set[1], h->d_bgr_set[0], h->d_bgr_set[1], h->d_pxp,
                   h->d_pyp, h->d_vox, h->d_proc, h->d_bnd, h->d_pend, h->d_keys, h->d_sort_tmp, h->d_rcp_tab,
                   h->d_cnn_params, h->d_cnn_packed, h->d_feat, h->d_a1, h->d_a2, h->d_conf_set[0], h->d_conf_set[1],
@@ -905,6 +909,14 @@ ff_status ff_set_spin_limit(ff_handle *h, uint32_t iterations) {
   return FF_OK;
 }
 
+ff_status ff_set_cell_generation(ff_handle *h, int mode) {
+  if (!h) return FF_ERR_BAD_ARG;
+  if (mode != FF_CELLS_INCREMENTAL && mode != FF_CELLS_FULL)
+    return set_err(h, FF_ERR_BAD_ARG, "ff_set_cell_generation: mode is FF_CELLS_INCREMENTAL or FF_CELLS_FULL");
+  h->full_cells = mode == FF_CELLS_FULL ? 1 : 0;
+  return FF_OK;
+}
+
 ff_status ff_inject_error(ff_handle *h, int what) {
   if (!h) return FF_ERR_BAD_ARG;
   if (what != 0 && what != FF_INJECT_CONFIDENCE_TIMEOUT)
@@ -1058,6 +1070,7 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
   mf.wgt16 = h->d_wgt16;
   mf.col = h->d_col;
   mf.stamp = h->d_stamp;
+  mf.bstamp = h->d_bstamp;
   mf.queue = h->d_queue;
   mf.rank = h->d_keys + 3 * h->cap_pix;
   mf.pend = h->d_pend;
@@ -1911,6 +1924,7 @@ ff_status ff_get_stats(ff_handle *h, ff_stats *o) {
   o->update_batch = (uint32_t)h->upd_batch;
   o->fused_bricks = *h->h_upd_total + h->direct_bricks;
   o->fused_frame_bricks = h->fused_frame_bricks;
+  o->mesh_cells_generated = h->mesh.n_generated;
   return FF_OK;
 }
 
@@ -2063,6 +2077,9 @@ ff_status ff_update_meshes(ff_handle *h, int *updated) {
   in.leaves_used = std::min(h->leaves_used, h->cfg.leaves_max);
   in.leaves_max = h->cfg.leaves_max;
   in.stamp = h->d_stamp;
+  in.bstamp = h->d_bstamp;
+  in.grows = h->grows;
+  in.full_cells = h->full_cells;
   in.frame = h->frames;
   in.n = h->n;
   for (int r = 0; r < 3; r++) in.offset[r] = h->offset[r];

@@ -46,6 +46,7 @@ enum : uint32_t {
   ERR_CELL_KEY = 64u,  // a mesh cell's origin does not fit its sort key
   ERR_DEDUPE_TIMEOUT = 128u,  // a grid barrier of the de-duplication gave up (nothing was inserted)
   ERR_SEQ_HALT = 256u,        // an earlier frame of a sequence must grow the volume or failed: not run
+  ERR_CELL_MERGE = 512u,      // the kept and the new mesh cells share a sort key (the update is redone in full)
 };
 
 // Error bits after which a frame's voxel update is skipped: its allocation

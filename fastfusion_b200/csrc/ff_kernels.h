@@ -34,6 +34,10 @@ struct MapFrame {
   __half *sdf16, *wgt16;
   uint16_t *col;
   uint32_t *stamp, *queue, *rank;
+  // per branch (index = branch base / 16): the last frame that created a
+  // branch or a leaf in the branch or below it (the mesher's test for
+  // octree subtrees unchanged since its previous update)
+  uint32_t *bstamp;
   PendingLeaf *pend;
   int4 *vox;
   uint8_t *proc;

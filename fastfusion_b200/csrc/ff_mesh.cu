@@ -134,6 +134,15 @@ constexpr int HOST_TOTALS = COUNT_WORDS - 10;
 struct GenCtx {
   const uint32_t *tree;
   uint32_t leaves_max;
+  // Incremental generation (incr != 0): only items with a slot that changed
+  // since the previous update are expanded or emit cells; the cells of the
+  // other items are kept from the previous list.  A slot changed if its
+  // finest leaf at or above is new (index >= prev_leaves), if it was
+  // subdivided since (child branch index >= prev_branches), or if a branch
+  // or leaf was created in its subtree since (branch stamp > since).
+  const uint32_t *bstamp;
+  uint32_t since, prev_leaves, prev_branches;
+  int incr;
 };
 
 // the octree is read-only while the mesh is built: reads go through the
@@ -157,6 +166,15 @@ __device__ __forceinline__ Slot child_of(const GenCtx &g, const Slot &s, int co)
 }
 
 __device__ __forceinline__ Slot ch(const GenCtx &g, const Slot &s, int co) { return is_sub(g, s) ? child_of(g, s, co) : s; }
+
+__device__ __forceinline__ bool slot_changed(const GenCtx &g, const Slot &s) {
+  if (!g.incr) return true;
+  if (s.la < g.leaves_max && s.la >= g.prev_leaves) return true;
+  const uint32_t c = tree_at(g, s.S + 8);
+  if (c >= PENDING) return false;
+  if (c >= g.prev_branches) return true;
+  return __ldg(g.bstamp + (c >> 4)) > g.since;
+}
 
 __device__ __forceinline__ void others(int e, int &p, int &q) {
   p = e == 0 ? 1 : 0;
@@ -424,7 +442,7 @@ __device__ __forceinline__ void cell_item(const GenCtx &g, const GenQueues &Q, c
   for (int j = 0; j < 8; j++) {
     if (is_sub(g, C[j])) {
       push_cell(Q, O, C[j]);
-    } else {
+    } else if (slot_changed(g, C[j])) {
       int o[3] = {C[j].o[0], C[j].o[1], C[j].o[2]};
       uint32_t L[1] = {C[j].la};
       emit_cell(Q, 0, 0, o, C[j].size, L, 1);
@@ -482,21 +500,31 @@ __device__ __forceinline__ void gen_level(const GenCtx &g, const GenQueues &Q, i
         }
       } else {
         const Slot s = Q.cellq[cur][i];
+        if (!slot_changed(g, s)) continue;
         for (int co = 0; co < 8; co++) C[co] = child_of(g, s, co);
       }
       cell_item(g, Q, O, C);
     } else if (i < nc + nf) {
       const FaceItem f = Q.faceq[cur][i - nc];
+      if (!slot_changed(g, f.a) && !slot_changed(g, f.b)) continue;
       if (f.axis == 0) face_item<0>(g, Q, O, f.a, f.b);
       else if (f.axis == 1) face_item<1>(g, Q, O, f.a, f.b);
       else face_item<2>(g, Q, O, f.a, f.b);
     } else if (i < nc + nf + ne) {
       const EdgeItem e = Q.edgeq[cur][i - nc - nf];
+      bool changed = false;
+#pragma unroll
+      for (int j = 0; j < 4; j++) changed |= slot_changed(g, e.s[j]);
+      if (!changed) continue;
       if (e.axis == 0) edge_item<0>(g, Q, O, e.s);
       else if (e.axis == 1) edge_item<1>(g, Q, O, e.s);
       else edge_item<2>(g, Q, O, e.s);
     } else {
       const VertItem v = Q.vertq[cur][i - nc - nf - ne];
+      bool changed = false;
+#pragma unroll
+      for (int j = 0; j < 8; j++) changed |= slot_changed(g, v.s[j]);
+      if (!changed) continue;
       vert_item(g, Q, O, v.s);
     }
   }
@@ -529,6 +557,201 @@ __global__ void k_cell_keys(const Cell *cells, uint32_t n, int B, uint64_t *keys
 __global__ void k_gather_cells(const Cell *in, const uint32_t *order, uint32_t n, Cell *out) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = in[order[i]];
+}
+
+// ---------------------------------------------------------------------------
+// Incremental cell list: the previous update's cells whose item did not
+// change are kept; the traversal (pruned to changed items) adds the rest.
+// ---------------------------------------------------------------------------
+
+// Did the slot that held point p in the previous update's octree change?  The
+// previous octree is this one without the branches allocated since
+// (index >= prev_branches; a child slot, once set, never changes), so the
+// descent stops where the previous one stopped: at the slot that was not
+// subdivided.  It changed if it is subdivided now or if its finest leaf at or
+// above is new.
+__device__ __forceinline__ bool side_changed(const GenCtx &g, uint32_t n, const int (&p)[3]) {
+  uint32_t branch = 0, la = BRANCHINIT, half = n >> 1;
+  uint32_t ox = 0, oy = 0, oz = 0;
+  for (int lvl = 0; lvl < 32 && half; lvl++) {
+    const uint32_t co = ((uint32_t)p[0] >= ox + half) * 1u + ((uint32_t)p[1] >= oy + half) * 2u +
+                        ((uint32_t)p[2] >= oz + half) * 4u;
+    const uint32_t S = branch + co;
+    const uint32_t lf = tree_at(g, S);
+    if (lf < g.leaves_max) la = lf;
+    const uint32_t c = tree_at(g, S + 8);
+    if (c >= PENDING) return la < g.leaves_max && la >= g.prev_leaves;
+    if (c >= g.prev_branches) return true;
+    ox += half * ((co & 1) != 0);
+    oy += half * ((co & 2) != 0);
+    oz += half * ((co & 4) != 0);
+    branch = c;
+    half >>= 1;
+  }
+  return true;  // deeper than any octree: treat as changed
+}
+
+// A point inside side k of a cell (the sides in the order of Cell::L):
+// interior cell: its slot; wall across axis a: the slot before and after the
+// plane o[a] + size; edge along axis e: the four slots around the line
+// (o[p] + size, o[q] + size), bit 0 of k the +p side, bit 1 the +q side;
+// corner: the eight slots around the vertex o + size, bit r of k the +r side.
+__device__ __forceinline__ void side_point(const Cell &c, int k, int (&p)[3]) {
+  const int sz = c.size;
+  for (int r = 0; r < 3; r++) p[r] = c.o[r];
+  if (c.type == 0) return;
+  if (c.type <= 3) {
+    const int a = c.type - 1;
+    p[a] = c.o[a] + sz - (k == 0 ? 1 : 0);
+    return;
+  }
+  if (c.type <= 6) {
+    const int e = c.type - 4;
+    const int pa = e == 0 ? 1 : 0, qa = e == 2 ? 1 : 2;
+    p[pa] = c.o[pa] + sz - ((k & 1) ? 0 : 1);
+    p[qa] = c.o[qa] + sz - ((k & 2) ? 0 : 1);
+    return;
+  }
+  for (int r = 0; r < 3; r++) p[r] = c.o[r] + sz - (((k >> r) & 1) ? 0 : 1);
+}
+
+constexpr int KEEP_THREADS = 256, KEEP_SCAN_THREADS = 1024;
+
+// Block-wide exclusive prefix of one value per thread (KEEP_THREADS threads);
+// the block's total in *total.
+__device__ __forceinline__ uint32_t block_scan_keep(uint32_t v, uint32_t *total) {
+  __shared__ uint32_t warp_sum[KEEP_THREADS / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t u = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += u;
+  }
+  if (lane == 31) warp_sum[w] = x;
+  __syncthreads();
+  uint32_t before = 0, all = 0;
+  for (int j = 0; j < KEEP_THREADS / 32; j++) {
+    const uint32_t t = warp_sum[j];
+    if (j < w) before += t;
+    all += t;
+  }
+  *total = all;
+  return before + x - v;
+}
+
+// keep[i] = 1 if previous cell i is kept; per tile of KEEP_THREADS cells, the
+// number kept (tile_sum).
+__global__ void __launch_bounds__(KEEP_THREADS) k_keep_cells(GenCtx g, uint32_t n, const Cell *__restrict__ old_cells,
+                                                            uint32_t n_old, uint32_t *keep, uint32_t *tile_sum) {
+  const uint32_t i = blockIdx.x * KEEP_THREADS + threadIdx.x;
+  uint32_t k = 0;
+  if (i < n_old) {
+    const Cell c = old_cells[i];
+    const int nl = c.type == 0 ? 1 : (c.type <= 3 ? 2 : (c.type <= 6 ? 4 : 8));
+    bool changed = false;
+    for (int s = 0; s < nl && !changed; s++) {
+      int p[3];
+      side_point(c, s, p);
+      changed = side_changed(g, n, p);
+    }
+    k = changed ? 0u : 1u;
+    keep[i] = k;
+  }
+  uint32_t total;
+  (void)block_scan_keep(k, &total);
+  if (threadIdx.x == 0) tile_sum[blockIdx.x] = total;
+}
+
+// Exclusive scan of the tile sums in one block (any number of tiles, in
+// chunks of the block size).
+__global__ void __launch_bounds__(KEEP_SCAN_THREADS) k_keep_tile_scan(uint32_t *tile_sum, uint32_t ntiles) {
+  __shared__ uint32_t warp_sum[KEEP_SCAN_THREADS / 32];
+  __shared__ uint32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (uint32_t base = 0; base < ntiles; base += KEEP_SCAN_THREADS) {
+    const uint32_t i = base + threadIdx.x;
+    const uint32_t v = i < ntiles ? tile_sum[i] : 0u;
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t u = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += u;
+    }
+    if (lane == 31) warp_sum[w] = x;
+    __syncthreads();
+    uint32_t before = 0, all = 0;
+    for (int j = 0; j < KEEP_SCAN_THREADS / 32; j++) {
+      const uint32_t t = warp_sum[j];
+      if (j < w) before += t;
+      all += t;
+    }
+    const uint32_t c0 = carry;
+    if (i < ntiles) tile_sum[i] = c0 + before + x - v;
+    __syncthreads();
+    if (threadIdx.x == 0) carry = c0 + all;
+    __syncthreads();
+  }
+}
+
+// keep[] becomes the exclusive prefix of the kept flags, with the total at
+// keep[n_old]; counts[0] = cells kept, counts[1] = cells kept before the
+// previous list's first corner cell.
+__global__ void __launch_bounds__(KEEP_THREADS) k_keep_apply(uint32_t *keep, uint32_t n_old, const uint32_t *tile_sum,
+                                                            uint32_t ntiles, uint32_t first_corner_old,
+                                                            uint32_t *counts) {
+  const uint32_t i = blockIdx.x * KEEP_THREADS + threadIdx.x;
+  const uint32_t k = i < n_old ? keep[i] : 0u;
+  uint32_t total;
+  const uint32_t ex = block_scan_keep(k, &total) + tile_sum[blockIdx.x];
+  if (i < n_old) keep[i] = ex;
+  if (i == first_corner_old) counts[1] = ex;
+  if (blockIdx.x == ntiles - 1 && threadIdx.x == 0) {
+    keep[n_old] = tile_sum[blockIdx.x] + total;
+    counts[0] = tile_sum[blockIdx.x] + total;
+    if (first_corner_old >= n_old) counts[1] = tile_sum[blockIdx.x] + total;
+  }
+}
+
+// first index in keys[0, n) whose key is >= key (strict: > key)
+__device__ __forceinline__ uint32_t key_bound(const uint64_t *keys, uint32_t n, uint64_t key, bool strict) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    const uint64_t k = keys[mid];
+    if (k < key || (strict && k == key)) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Merge the kept previous cells (sorted, keep_scan their exclusive prefix)
+// with the new cells (sorted keys, order into raw): a stable merge with the
+// kept cells first among equal keys, so every position of the output is
+// written exactly once.  Equal keys (which the cell geometry rules out) are
+// reported with ERR_CELL_MERGE.
+__global__ void k_merge_cells(const Cell *__restrict__ old_cells, const uint64_t *__restrict__ old_keys,
+                              const uint32_t *__restrict__ keep_scan, uint32_t n_old, const Cell *__restrict__ raw,
+                              const uint64_t *__restrict__ new_keys, const uint32_t *__restrict__ new_order,
+                              uint32_t n_new, Cell *out, uint64_t *out_keys, uint32_t *error) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n_old) {
+    const uint32_t ks = keep_scan[i];
+    if (keep_scan[i + 1] == ks) return;  // not kept
+    const uint64_t key = old_keys[i];
+    const uint32_t lb = key_bound(new_keys, n_new, key, false);
+    if (lb < n_new && new_keys[lb] == key) atomicOr(error, ERR_CELL_MERGE);
+    out[ks + lb] = old_cells[i];
+    out_keys[ks + lb] = key;
+  } else if (i < n_old + n_new) {
+    const uint32_t j = i - n_old;
+    const uint64_t key = new_keys[j];
+    if (j > 0 && new_keys[j - 1] == key) atomicOr(error, ERR_CELL_MERGE);
+    const uint32_t ub = key_bound(old_keys, n_old, key, true);
+    const uint32_t pos = j + keep_scan[ub];
+    out[pos] = raw[new_order[j]];
+    out_keys[pos] = key;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1521,6 +1744,16 @@ struct MeshImpl {
   size_t cap_oxyz = 0, cap_orgb = 0, cap_ofaces = 0;
   size_t cap_xyz = 0, cap_rgb = 0, cap_faces = 0;
   uint32_t since = 0;
+  // incremental cell list: the previous update's leaf and branch counts and
+  // growth count; per previous cell its kept flag, then their prefix; merged
+  // keys; the last update's generated and kept cell counts
+  uint32_t prev_leaves = 0, prev_branches = 0, grows = 0;
+  uint32_t *keep = nullptr, *keep_tiles = nullptr;
+  size_t cap_keep = 0, cap_keep_tiles = 0;
+  uint64_t *mkeys = nullptr;
+  size_t cap_mkeys = 0;
+  uint32_t n_new = 0, n_kept = 0;
+  bool redo_full = false;  // the last incremental list was inconsistent: regenerate every cell
 };
 
 static MeshImpl &impl(MeshState &m) {
@@ -1547,8 +1780,20 @@ static int key_bits_for(uint32_t n) {
   return std::min(b, 16);
 }
 
-static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uint32_t &ncells, std::string &err) {
+// Cell words of the counter array (d_count) used by the incremental list:
+// cells kept, and kept before the previous list's first corner cell.
+constexpr int KEPT_WORD = 20;
+
+static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStream_t s, uint32_t &ncells,
+                          std::string &err) {
   const int key_bits = key_bits_for(in.n);
+  const uint32_t n_old = incr ? I.n_old : 0u;
+  const uint32_t first_corner_old = n_old - std::min(I.n_corners, n_old);
+  const uint32_t keep_tiles = (n_old + KEEP_THREADS - 1) / KEEP_THREADS;
+  if (incr) {
+    MCK(grow_buf(I.keep, I.cap_keep, (size_t)n_old + 1, s));
+    MCK(grow_buf(I.keep_tiles, I.cap_keep_tiles, std::max<size_t>(keep_tiles, 1), s));
+  }
   // queue sizes: a first guess from the octree size, then the previous
   // update's peaks with headroom (the map grows slowly between updates)
   const uint32_t slots = std::max<uint32_t>(in.branches_used / 2, 64);
@@ -1585,7 +1830,24 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
     Q.cap_cells = (uint32_t)I.cap_raw;
     Q.error = I.d_count + 9;
     Q.n_corners = I.d_count + 11;
-    GenCtx g{in.tree, in.leaves_max};
+    GenCtx g;
+    g.tree = in.tree;
+    g.leaves_max = in.leaves_max;
+    g.bstamp = in.bstamp;
+    g.since = I.since;
+    g.prev_leaves = I.prev_leaves;
+    g.prev_branches = I.prev_branches;
+    g.incr = incr ? 1 : 0;
+    if (incr) {
+      // the previous cells whose sides did not change, and their positions
+      // among the kept (words KEPT_WORD, KEPT_WORD + 1: kept, kept before the
+      // first corner cell)
+      note_launch(3);
+      k_keep_cells<<<keep_tiles, KEEP_THREADS, 0, s>>>(g, in.n, I.old_cells, n_old, I.keep, I.keep_tiles);
+      k_keep_tile_scan<<<1, KEEP_SCAN_THREADS, 0, s>>>(I.keep_tiles, keep_tiles);
+      k_keep_apply<<<keep_tiles, KEEP_THREADS, 0, s>>>(I.keep, n_old, I.keep_tiles, keep_tiles, first_corner_old,
+                                                       I.d_count + KEPT_WORD);
+    }
     // a chain cell -> face -> edge -> vertex adds up to three levels below
     // the octree's depth; more levels run if items are left
     int depth = 1;
@@ -1626,26 +1888,33 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
       err = "meshing: cell generation did not finish within the level limit";
       return 6;
     }
-    ncells = hc[8];
-    I.n_corners = hc[11];
+    const uint32_t n_kept = incr ? hc[KEPT_WORD] : 0u;
+    const uint32_t kept_corners = incr ? n_kept - hc[KEPT_WORD + 1] : 0u;
+    I.n_new = hc[8];
+    I.n_kept = n_kept;
+    ncells = n_kept + I.n_new;
+    I.n_corners = hc[11] + kept_corners;
     break;
   }
   if (I.h_count[9] & ERR_CELL_OVERFLOW) {
     err = "meshing: cell queues overflow";
     return 4;
   }
-  // sort by key: deterministic order and a stable identity across updates
-  MCK(grow_buf(I.keys, I.cap_keys, ncells, s));
-  MCK(grow_buf(I.keys_sorted, I.cap_keys2, ncells, s));
-  MCK(grow_buf(I.vals, I.cap_vals, ncells, s));
-  MCK(grow_buf(I.vals_sorted, I.cap_vals2, ncells, s));
+  // sort the generated cells by key: deterministic order and a stable
+  // identity across updates; with a kept list, merge the two
+  const uint32_t n_new = I.n_new;
+  MCK(grow_buf(I.keys, I.cap_keys, n_new, s));
+  MCK(grow_buf(I.keys_sorted, I.cap_keys2, std::max(n_new, ncells), s));
+  MCK(grow_buf(I.vals, I.cap_vals, n_new, s));
+  MCK(grow_buf(I.vals_sorted, I.cap_vals2, n_new, s));
   MCK(grow_buf(I.cells, I.cap_cells, ncells, s));
-  if (ncells) {
-    note_launch(2);
-    k_cell_keys<<<(ncells + 255) / 256, 256, 0, s>>>(I.raw, ncells, key_bits, I.keys, I.vals, I.d_count + 9);
+  if (incr) MCK(grow_buf(I.mkeys, I.cap_mkeys, ncells, s));
+  if (n_new) {
+    note_launch(1);
+    k_cell_keys<<<(n_new + 255) / 256, 256, 0, s>>>(I.raw, n_new, key_bits, I.keys, I.vals, I.d_count + 9);
     const int end_bit = 3 * key_bits + 7;
     size_t bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, bytes, I.keys, I.keys_sorted, I.vals, I.vals_sorted, (int)ncells, 0,
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, I.keys, I.keys_sorted, I.vals, I.vals_sorted, (int)n_new, 0,
                                     end_bit, s);
     if (bytes > I.sort_tmp_bytes) {
       if (I.sort_tmp) MCK(cudaFreeAsync(I.sort_tmp, s));
@@ -1655,8 +1924,22 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, cudaStream_t s, uin
     }
     note_lib_call();
     MCK(cub::DeviceRadixSort::SortPairs(I.sort_tmp, I.sort_tmp_bytes, I.keys, I.keys_sorted, I.vals, I.vals_sorted,
-                                        (int)ncells, 0, end_bit, s));
-    k_gather_cells<<<(ncells + 255) / 256, 256, 0, s>>>(I.raw, I.vals_sorted, ncells, I.cells);
+                                        (int)n_new, 0, end_bit, s));
+  }
+  if (!incr) {
+    if (n_new) {
+      note_launch(1);
+      k_gather_cells<<<(n_new + 255) / 256, 256, 0, s>>>(I.raw, I.vals_sorted, n_new, I.cells);
+    }
+  } else if (ncells) {
+    // kept and new cells merged in key order; the merged keys replace the
+    // sorted ones
+    note_launch(1);
+    k_merge_cells<<<(n_old + n_new + 255) / 256, 256, 0, s>>>(I.old_cells, I.old_keys, I.keep, n_old, I.raw,
+                                                               I.keys_sorted, I.vals_sorted, n_new, I.cells, I.mkeys,
+                                                               I.d_count + 9);
+    std::swap(I.mkeys, I.keys_sorted);
+    std::swap(I.cap_mkeys, I.cap_keys2);
   }
   return 0;
 }
@@ -1686,10 +1969,17 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   uint32_t ncells = 0;
   Prof &P = *in.prof;
   int pi = P.begin(ST_MESH_CELLS, s);
-  int rc = generate_cells(I, in, s, ncells, err);
+  // the previous list can be kept where the octree did not change: not after
+  // a growth (every cell moves) or a change of the key layout
+  const bool incr_cells = M.valid && I.n_old > 0 && I.key_bits == key_bits_for(in.n) && !in.full_cells &&
+                          I.grows == in.grows && !I.redo_full;
+  const uint32_t n_old_cells = incr_cells ? I.n_old : 0u;
+  int rc = generate_cells(I, in, incr_cells, s, ncells, err);
   if (rc) return rc;
-  // cells written by generation, then read and written by the key sort
-  P.end(pi, (double)ncells * sizeof(Cell) * 3, s);
+  // 48 B per cell read or written: the previous list read by the keep test,
+  // the new cells written by the traversal and read by the gather or merge,
+  // the kept cells read by the merge, the list written
+  P.end(pi, (double)sizeof(Cell) * ((double)n_old_cells + 2.0 * I.n_new + I.n_kept + ncells), s);
   VoxSrc vs;
   vs.leaf = in.leaf;
   vs.parent = in.parent;
@@ -1786,6 +2076,20 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
     err = "meshing: a mesh cell lies outside the volume";
     return 6;
   }
+  if (I.h_count[HOST_TOTALS + 7] & ERR_CELL_MERGE) {
+    // the kept and the new cells overlap: build this update from the whole
+    // octree instead (every cell generated and meshed again)
+    if (!incr_cells) {
+      mesh_invalidate(M);
+      err = "meshing: two mesh cells share a sort key";
+      return 6;
+    }
+    mesh_invalidate(M);
+    I.redo_full = true;
+    rc = mesh_update(M, in, s, err);
+    I.redo_full = false;
+    return rc;
+  }
   const uint64_t tot[2] = {h_tot[0], h_tot[1]};
   const unsigned long long nsamples = h_tot[2];
   const uint32_t ndirty = incremental ? I.h_count[HOST_TOTALS + 6] : ncells;
@@ -1841,6 +2145,9 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   I.n_old = ncells;
   I.key_bits = kb;
   I.since = in.frame;
+  I.prev_leaves = in.leaves_used;
+  I.prev_branches = in.branches_used;
+  I.grows = in.grows;
   // The emit pass may still run when this returns: everything that reads the
   // mesh or the volume later is ordered after it on this stream.  With the
   // stage profile on, wait for its sample count (the stage's bytes).
@@ -1852,6 +2159,7 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   M.n_faces = tot[1];
   M.n_cells = ncells;
   M.n_dirty = ndirty;
+  M.n_generated = I.n_new;
   M.valid = true;
   return 0;
 }
@@ -1965,7 +2273,7 @@ void mesh_free(MeshState &M) {
                     I.vertq[1], I.d_count, I.raw, I.cells, I.old_cells, I.keys, I.keys_sorted, I.old_keys,
                     I.vals, I.vals_sorted, I.sort_tmp, I.out, I.old_out, I.nv, I.nf, I.vbase, I.fbase,
                     I.old_vbase, I.old_fbase, I.dirty, I.old_index, I.scan_tmp, I.old_xyz, I.old_rgb,
-                    I.old_faces, I.dlist, I.cases};
+                    I.old_faces, I.dlist, I.cases, I.keep, I.keep_tiles, I.mkeys};
     for (void *p : ptrs)
       if (p) cudaFreeAsync(p, 0);
     if (I.h_count) cudaFreeHost(I.h_count);

@@ -23,6 +23,10 @@ struct MeshInputs {
   int storage;
   uint32_t leaves_used, leaves_max;
   const uint32_t *stamp;  // frame of the last update of each brick
+  // per branch: the last frame that created a branch or leaf at or below it
+  const uint32_t *bstamp;
+  uint32_t grows = 0;   // volume growths so far (a growth moves every cell)
+  int full_cells = 0;   // regenerate every cell instead of the changed ones
   uint32_t frame;
   uint32_t n;
   float offset[3];
@@ -42,7 +46,7 @@ struct MeshState {
   uint32_t *d_faces = nullptr;
   uint64_t n_vertices = 0, n_faces = 0;
   uint64_t cap_vertices = 0, cap_faces = 0;
-  uint64_t n_cells = 0, n_dirty = 0;
+  uint64_t n_cells = 0, n_dirty = 0, n_generated = 0;
   uint32_t last_frame = 0;
   bool valid = false;
   void *impl = nullptr;  // buffers private to ff_mesh.cu

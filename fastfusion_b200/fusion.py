@@ -26,6 +26,7 @@ _STATUS = {0: "FF_OK", 1: "FF_ERR_BAD_ARG", 2: "FF_ERR_CUDA", 3: "FF_ERR_OOM_POO
            5: "FF_ERR_TIMEOUT", 6: "FF_ERR_STATE", 7: "FF_ERR_NO_DEVICE"}
 NOALLOC_MAX_CELLS = 65536  # FF_NOALLOC_MAX_CELLS
 SPIN_LIMIT_DEFAULT = 1 << 22  # FF_SPIN_LIMIT_DEFAULT
+CELLS_INCREMENTAL, CELLS_FULL = 0, 1  # FF_CELLS_INCREMENTAL, FF_CELLS_FULL
 INJECT_CONFIDENCE_TIMEOUT = 1  # FF_INJECT_CONFIDENCE_TIMEOUT
 
 STORAGE = {"fp32": 0, "fp16": 1}
@@ -55,7 +56,8 @@ class ff_stats(ctypes.Structure):
                 ("mesh_cells_dirty", ctypes.c_uint64), ("processed_pixels", ctypes.c_uint32),
                 ("new_leaves", ctypes.c_uint32), ("dedupe_rounds", ctypes.c_uint32),
                 ("graph_replays", ctypes.c_uint32), ("update_batch", ctypes.c_uint32),
-                ("fused_bricks", ctypes.c_uint64), ("fused_frame_bricks", ctypes.c_uint64)]
+                ("fused_bricks", ctypes.c_uint64), ("fused_frame_bricks", ctypes.c_uint64),
+                ("mesh_cells_generated", ctypes.c_uint64)]
 
 
 class ff_tuning(ctypes.Structure):
@@ -74,6 +76,7 @@ SIGNATURES = {
     "ff_set_tuning": (_i32, [_vp, ctypes.POINTER(ff_tuning)]),
     "ff_set_shard": (_i32, [_vp, _i32, _i32]),
     "ff_set_spin_limit": (_i32, [_vp, _u32]),
+    "ff_set_cell_generation": (_i32, [_vp, _i32]),
     "ff_set_update_batch": (_i32, [_vp, _i32]),
     "ff_halo_export": (_i32, [_vp, _vp, _u64, ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
     "ff_halo_import": (_i32, [_vp, _vp, _u64]),
@@ -463,6 +466,13 @@ class FusionMipMapCPU:
         iterations; 0: a wait gives up at once and the frame reports
         FF_ERR_TIMEOUT)."""
         self._check(self._L.ff_set_spin_limit(self._h, int(iterations)))
+
+    def set_cell_generation(self, mode: int = CELLS_INCREMENTAL):
+        """How updateMeshes finds the mesh cells: CELLS_INCREMENTAL (only the
+        octree parts that changed since the previous update are traversed;
+        the other cells are kept) or CELLS_FULL (the whole octree every
+        update).  The cell list is the same either way."""
+        self._check(self._L.ff_set_cell_generation(self._h, int(mode)))
 
     def inject_error(self, what: int = INJECT_CONFIDENCE_TIMEOUT):
         """Make the next frame report a failure as the device would (tests of

@@ -84,6 +84,8 @@ typedef struct ff_stats {
                                   whatever the number of its frames; as of the last finished pass) */
   uint64_t fused_frame_bricks; /* queued bricks summed over the frames updated so far (the reference reads and
                                   writes each of them once per frame) */
+  uint64_t mesh_cells_generated; /* cells the last update's octree traversal produced (the rest were kept from
+                                    the update before; all of them after a full generation) */
 } ff_stats;
 
 /* Create a map.  Replaces `new FusionMipMapCPU(0,0,0,scale,threshold,0,color)`
@@ -278,6 +280,19 @@ ff_status ff_set_update_batch(ff_handle *h, int frames);
  * is sequential and has no waits). */
 #define FF_SPIN_LIMIT_DEFAULT (1u << 22)
 ff_status ff_set_spin_limit(ff_handle *h, uint32_t iterations);
+
+/* How ff_update_meshes finds the mesh cells.  FF_CELLS_INCREMENTAL (the
+ * default): only the parts of the octree that gained a branch or a leaf
+ * since the previous update are traversed again; the cells elsewhere are
+ * kept from the previous update's list (like the reference's
+ * updateMeshCellStructure, geometryfusion_mipmap_cpu.cpp:2488-2616, which
+ * adds cells only for new octree slots).  FF_CELLS_FULL: every cell is
+ * generated again from the whole octree at every update.  Both give the same
+ * cell list in the same order; the first update, a growth of the volume and
+ * ff_set_state always generate every cell. */
+#define FF_CELLS_INCREMENTAL 0
+#define FF_CELLS_FULL 1
+ff_status ff_set_cell_generation(ff_handle *h, int mode);
 
 /* Failure injection for tests of the error paths (no counterpart in the
  * reference).  FF_INJECT_CONFIDENCE_TIMEOUT: the next frame reports that a
