@@ -21,7 +21,9 @@ Reported (one JSON line from rank 0):
              voxel-update kernel
   cpu_baseline  the reference's FusionMipMapCPU (compiled from its sources)
              pinned to one host core over the same walk and the same timed
-             steps, median of 3 runs, plus a row with its threaded meshing
+             steps, median of 3 runs, plus a row with its threaded meshing;
+             sdf_err_vs_fp64: the walk's first 20 frames fused with FP32 and
+             FP16 storage against the FP64 restatement (the checker)
 
 `--impl reference` times the reference's CPU implementation instead: one map
 per host core (all cores the box gives this process, bounded by host memory),
@@ -505,6 +507,7 @@ def run_b200(a):
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(depth, bgr, seq, a)
+        cpu["sdf_err_vs_fp64"] = precision_vs_fp64(depth, bgr, seq, local)
 
     if rank == 0:
         line = {
@@ -665,6 +668,40 @@ def cpu_baseline(depth, bgr, seq, a) -> dict:
             "sample": f"the whole walk ({nf} frames) on one core per run, {a.warmup} warm-up steps, the same "
                       f"{a.steps} timed steps (10 addMap + updateMeshes + mesh copy each); setThreadMeshing(false)",
             "threaded_meshing": threaded}
+
+
+PRECISION_FRAMES = 20
+
+
+def precision_vs_fp64(depth, bgr, seq, device, frames=PRECISION_FRAMES) -> dict:
+    """Part of the host-side baseline leg: the walk's first frames fused by
+    the FP64 restatement on the host (the checker) and by this library with
+    FP32 and with FP16 storage (exact round-toward-zero reciprocals, so that
+    only the storage and float arithmetic differ); SDF error over every voxel
+    the FP64 fusion weighted, in metres."""
+    from fastfusion_b200 import fusion as ff
+    from oracle import port
+    p64 = port.PortFusion(leaves_total=271420, branches_total=4793488, update_mode=3)
+    maps = {s: ff.FusionMipMapCPU(0, 0, 0, VOXEL, THRESHOLD, 0, True, leaves_max=271420, branches_max=4793488,
+                                  device=device, storage=s, rcp="exact") for s in ("fp32", "fp16")}
+    for k in range(frames):
+        hd = depth[k].cpu().numpy().view(np.uint16)
+        hb = bgr[k].cpu().numpy()
+        R, t = seq.poses[k]
+        p64.add_map(hd, hb, seq.K, R, t, SCALING, MAXCAM)
+        for m in maps.values():
+            m.addMap(hd, ff.CameraInfo(seq.K, R, t), hb, SCALING, MAXCAM)
+    d64, w64 = p64.bricks64()
+    out = {"frames": frames, "reciprocal": "exact", "voxels": int((w64 > 0).sum())}
+    for s, m in maps.items():
+        d, _, _ = m.bricks()
+        sel = w64 > 0
+        err = np.abs(d.astype(np.float64)[sel] - d64[sel]) if d.shape == d64.shape else None
+        out[s] = None if err is None else {"rms_m": float(np.sqrt(np.mean(err ** 2))),
+                                           "p99_m": float(np.quantile(err, 0.99)), "max_m": float(err.max())}
+        m.close()
+    p64.close()
+    return out
 
 
 # -- the reference arm ------------------------------------------------------------
