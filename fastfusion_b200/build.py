@@ -17,7 +17,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libfastfusion_b200.so")
-SOURCES = ["ff_alloc.cu", "ff_fuse.cu", "ff_mesh.cu", "ff_cnn.cu", "ff_capi.cu"]
+SOURCES = ["ff_alloc.cu", "ff_fuse.cu", "ff_mesh.cu", "ff_sort.cu", "ff_cnn.cu", "ff_capi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -24,8 +24,6 @@
 // Incremental: a cell whose leaves (and their parent chains) were not updated
 // since the previous mesh, and whose leaves did not change, copies its old
 // vertices and faces instead of being re-meshed.
-#include <cub/cub.cuh>
-
 #include <algorithm>
 #include <cstddef>
 #include <mutex>
@@ -33,6 +31,7 @@
 #include <vector>
 
 #include "ff_mesh.h"
+#include "ff_sort.h"
 
 namespace ffb {
 
@@ -544,14 +543,13 @@ __device__ __forceinline__ uint64_t cell_key(const Cell &c, int B) {
          ((uint64_t)c.o[1] << B) | (uint64_t)c.o[2];
 }
 
-__global__ void k_cell_keys(const Cell *cells, uint32_t n, int B, uint64_t *keys, uint32_t *vals, uint32_t *error) {
+__global__ void k_cell_keys(const Cell *cells, uint32_t n, int B, uint64_t *keys, uint32_t *error) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Cell c = cells[i];
   const uint32_t lim = 1u << B;
   if (c.o[0] >= lim || c.o[1] >= lim || c.o[2] >= lim) atomicOr(error, ERR_CELL_KEY);
   keys[i] = cell_key(c, B);
-  vals[i] = i;
 }
 
 __global__ void k_gather_cells(const Cell *in, const uint32_t *order, uint32_t n, Cell *out) {
@@ -1905,26 +1903,24 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
   const uint32_t n_new = I.n_new;
   MCK(grow_buf(I.keys, I.cap_keys, n_new, s));
   MCK(grow_buf(I.keys_sorted, I.cap_keys2, std::max(n_new, ncells), s));
-  MCK(grow_buf(I.vals, I.cap_vals, n_new, s));
   MCK(grow_buf(I.vals_sorted, I.cap_vals2, n_new, s));
   MCK(grow_buf(I.cells, I.cap_cells, ncells, s));
   if (incr) MCK(grow_buf(I.mkeys, I.cap_mkeys, ncells, s));
   if (n_new) {
     note_launch(1);
-    k_cell_keys<<<(n_new + 255) / 256, 256, 0, s>>>(I.raw, n_new, key_bits, I.keys, I.vals, I.d_count + 9);
+    k_cell_keys<<<(n_new + 255) / 256, 256, 0, s>>>(I.raw, n_new, key_bits, I.keys, I.d_count + 9);
     const int end_bit = 3 * key_bits + 7;
-    size_t bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, bytes, I.keys, I.keys_sorted, I.vals, I.vals_sorted, (int)n_new, 0,
-                                    end_bit, s);
+    const size_t bytes = argsort_temp_bytes(n_new);
     if (bytes > I.sort_tmp_bytes) {
       if (I.sort_tmp) MCK(cudaFreeAsync(I.sort_tmp, s));
       I.sort_tmp = nullptr;
       MCK(pool_alloc(&I.sort_tmp, bytes, s));
       I.sort_tmp_bytes = bytes;
     }
-    note_lib_call();
-    MCK(cub::DeviceRadixSort::SortPairs(I.sort_tmp, I.sort_tmp_bytes, I.keys, I.keys_sorted, I.vals, I.vals_sorted,
-                                        (int)n_new, 0, end_bit, s));
+    unsigned sort_launches = 0;
+    MCK(argsort_u64(I.keys, n_new, end_bit, I.keys_sorted, I.vals_sorted, I.sort_tmp, I.sort_tmp_bytes, s,
+                    &sort_launches));
+    note_launch(sort_launches);
   }
   if (!incr) {
     if (n_new) {
@@ -2303,13 +2299,15 @@ cudaError_t prewarm_mesh_kernels() {
                        (const void *)k_mesh_corner<true>,  (const void *)k_mark_dirty,
                        (const void *)k_count_tile_sums,    (const void *)k_copy_clean,
                        (const void *)k_count_tile_scan,    (const void *)k_count_tile_apply,
-                       (const void *)k_fill_counts_from_old, (const void *)k_export_cells};
+                       (const void *)k_fill_counts_from_old, (const void *)k_export_cells,
+                       (const void *)k_keep_cells,         (const void *)k_keep_tile_scan,
+                       (const void *)k_keep_apply,         (const void *)k_merge_cells};
   for (const void *f : fns) {
     cudaFuncAttributes a;
     cudaError_t e = cudaFuncGetAttributes(&a, f);
     if (e != cudaSuccess) return e;
   }
-  return cudaSuccess;
+  return prewarm_sort_kernels();
 }
 
 }  // namespace ffb
