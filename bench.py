@@ -73,7 +73,7 @@ STAGE_KERNELS = {
     "insert": "k_insert",
     "finalize": "k_finalize_bitmap",
     "fuse": "k_fuse",
-    "mesh_cells": "k_gen_level+k_cell_keys+radix sort+k_gather_cells",
+    "mesh_cells": "k_keep_cells+k_gen_level+k_cell_keys+argsort (k_sort_small or k_rs_*)+k_merge_cells/k_gather_cells",
     "mesh_count": "k_mesh_lattice<count>+k_mesh_corner<count>",
     "mesh_emit": "k_mesh_lattice<emit>+k_mesh_corner<emit>+k_copy_clean",
     "confidence": "k_cnn_features+k_conv x3 (learned weight)",
@@ -88,7 +88,8 @@ STAGE_BYTES = {
     "finalize": "8 B per new brick",
     "fuse": "14,336 B per queued brick per frame (512 voxels x (4 SDF + 4 weight + 6 colour) B, read and written; "
             "10,240 B with FP16 storage)",
-    "mesh_cells": "3 x 48 B per mesh cell (written, then read and written by the key sort)",
+    "mesh_cells": "48 B per cell read or written: the previous list read by the keep test, each new cell written "
+                  "by the octree traversal and read by the merge, the kept cells read by the merge, the list written",
     "mesh_count": "SDF and weight (8 B, 4 B FP16) of every sample of the re-meshed cells",
     "mesh_emit": "14 B (10 B FP16) per sample read + 15 B per vertex + 12 B per face written",
     "confidence": "per pixel: depth in, features, two activations and the confidence written and read once",
@@ -408,13 +409,14 @@ def run_b200(a):
 
     # 2. per-stage profile of the walk after the warm-up (separate map; events per stage)
     m = new_map()
-    dirty, rounds = [], []
+    dirty, rounds, generated = [], [], []
 
     def device_step_stats(mm, s):
         device_step(mm, s)
         st_ = mm.stats()
         rounds.append(st_["dedupe_rounds"])
         dirty.append(st_["mesh_cells_dirty"])
+        generated.append(st_["mesh_cells_generated"] / max(st_["mesh_cells"], 1))
 
     for s_ in range(a.warmup):
         device_step(m, s_)
@@ -533,6 +535,7 @@ def run_b200(a):
                     "mesh_vertices": st["mesh_vertices"], "mesh_faces": st["mesh_faces"],
                     "mesh_cells": st["mesh_cells"], "grows": st["grows"], "meshing_ok": st["meshing_ok"],
                     "mesh_cells_dirty_mean": float(np.mean(dirty)) if dirty else None,
+                    "mesh_cells_generated_frac_mean": round(float(np.mean(generated)), 4) if generated else None,
                     "dedupe_rounds_mean": float(np.mean(rounds)) if rounds else None},
         }
         print(json.dumps(line), flush=True)
