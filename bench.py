@@ -59,6 +59,12 @@ THRESHOLD = 0.01
 METRIC = "depth frames/s fused+meshed (640x480, 5 mm)"
 UNIT = "frames/s"
 FALLBACK_HBM_GBS = 6650.0
+_T0 = time.monotonic()
+
+
+def log(msg: str) -> None:
+    """Progress on stderr (the JSON line stays alone on stdout)."""
+    print(f"[bench {time.monotonic() - _T0:7.1f} s] {msg}", file=sys.stderr, flush=True)
 L2_FLUSH_BYTES = 256 << 20
 WALK_FRAMES = 1000  # the random walk's length: every run fuses all of it
 CPU_RUNS = 3        # the CPU baseline: median of this many pinned runs
@@ -326,6 +332,7 @@ def run_b200(a):
     timed_set = set(timed_idx)
     nf = total * FRAMES_PER_STEP
     seq = make_sequence(a.seed + rank, nf)
+    log(f"rendering {nf} frames")
     depth, bgr = render_frames(seq, nf, dev)
     cams = [ff.CameraInfo(seq.K, *seq.poses[k]) for k in range(nf)]
     stream = torch.cuda.current_stream(dev)
@@ -395,6 +402,7 @@ def run_b200(a):
     clk = ClockSampler(gpu_index) if rank == 0 else None
 
     # 1. device-resident throughput
+    log("device-resident walk (sequence call)")
     m = new_map()
     dev_ms, dev_wall = timed(device_step, m)
     gpu_launches, lib_calls = launches
@@ -402,12 +410,14 @@ def run_b200(a):
     m.close()
     del m
     # the same with one call per frame
+    log("device-resident walk (one call per frame)")
     m = new_map()
     single_ms, _ = timed(device_step_single, m)
     m.close()
     del m
 
     # 2. per-stage profile of the walk after the warm-up (separate map; events per stage)
+    log("stage profile")
     m = new_map()
     dirty, rounds, generated = [], [], []
 
@@ -460,6 +470,7 @@ def run_b200(a):
                     "d2h_bytes_per_step": int(np.mean(d2h)) if d2h else 0, "ms_per_step": ms / a.steps}
 
         # page-locked host frames (ff_alloc_host-style pinned memory)
+        log("end to end, page-locked host frames")
         h_depth = depth.cpu().pin_memory()
         h_bgr = bgr.cpu().pin_memory()
         e2e = host_run(h_depth.numpy().view(np.uint16), h_bgr.numpy())
@@ -471,6 +482,7 @@ def run_b200(a):
             rms = float(np.sqrt(np.mean(seq.scene.sdf(v[sel].astype(np.float64)) ** 2)))
         del h_depth, h_bgr
         # pageable host frames, as a caller's cv::Mat images are
+        log("end to end, pageable host frames")
         p_depth = depth.cpu().numpy().view(np.uint16).copy()
         p_bgr = bgr.cpu().numpy().copy()
         e2e_pageable = host_run(p_depth, p_bgr)
@@ -509,7 +521,9 @@ def run_b200(a):
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(depth, bgr, seq, a)
+        log("FP32/FP16 storage against the FP64 restatement")
         cpu["sdf_err_vs_fp64"] = precision_vs_fp64(depth, bgr, seq, local)
+        log("done")
 
     if rank == 0:
         line = {
@@ -624,21 +638,48 @@ def _ref_worker(args):
     if thread_meshing:
         # the reference's destructor frees its mesh cells' meshes before it
         # joins a mesher thread that may still run (geometryfusion_mipmap_cpu.cpp
-        # :754 before :966): leave the object to the process exit
+        # :754 before :966): leave the object to the process exit, after the
+        # queue's feeder thread has handed the result over
+        q.close()
+        q.join_thread()
         os._exit(0)
 
 
-def _run_workers(jobs, with_barrier: bool):
+def _run_workers(jobs, with_barrier: bool, limit_s: float = 900.0):
+    """Run the reference workers; their timed seconds in job order, or None
+    if a worker died or the whole set did not finish within limit_s."""
     import multiprocessing as mp
+    import queue as queue_mod
     ctx = mp.get_context("spawn")
-    barrier = ctx.Barrier(len(jobs)) if with_barrier else None
+    barrier = ctx.Barrier(len(jobs), timeout=limit_s) if with_barrier else None
     q = ctx.Queue()
     procs = [ctx.Process(target=_ref_worker, args=(j[:10] + (barrier, q),)) for j in jobs]
     for pr in procs:
         pr.start()
-    out = [q.get() for _ in procs]
+    out = []
+    deadline = time.monotonic() + limit_s
+    try:
+        while len(out) < len(procs):
+            left = deadline - time.monotonic()
+            if left <= 0:
+                raise queue_mod.Empty
+            try:
+                out.append(q.get(timeout=min(left, 5.0)))
+            except queue_mod.Empty:
+                # a worker that exited without a result will never send one
+                if any(pr.exitcode not in (None, 0) for pr in procs):
+                    raise
+    except queue_mod.Empty:
+        for pr in procs:
+            if pr.is_alive():
+                pr.kill()
+        for pr in procs:
+            pr.join(10)
+        log(f"reference workers: {len(out)} of {len(procs)} finished "
+            f"(exit codes {[pr.exitcode for pr in procs]})")
+        return None
     for pr in procs:
-        pr.join()
+        pr.join(30)
     return [t for _, t in sorted(out)]
 
 
@@ -655,15 +696,21 @@ def cpu_baseline(depth, bgr, seq, a) -> dict:
     runs = min(CPU_RUNS, len(avail))
     jobs = [(i, {avail[i]}, dpath, bpath, seq.K, seq.poses[:nf], a.warmup, total, timed, False)
             for i in range(runs)]
+    log(f"cpu baseline: {runs} runs of the reference on one core each")
     secs = _run_workers(jobs, with_barrier=False)
     threaded = None
-    if kind == "reference" and len(avail) >= 2:
+    if secs and kind == "reference" and len(avail) >= 2:
+        log("cpu baseline: the reference with threaded meshing")
         tsecs = _run_workers([(0, set(avail[:2]), dpath, bpath, seq.K, seq.poses[:nf], a.warmup, total, timed,
                                True)], with_barrier=False)
-        threaded = {"value": round(a.steps * FRAMES_PER_STEP / tsecs[0], 3), "unit": UNIT, "cores": 2,
-                    "note": "setThreadMeshing(true): meshing on a second thread, updateMeshes returning false "
-                            "while it runs (the mesh copied each step is the last finished one)"}
+        threaded = None if not tsecs else {
+            "value": round(a.steps * FRAMES_PER_STEP / tsecs[0], 3), "unit": UNIT, "cores": 2,
+            "note": "setThreadMeshing(true): meshing on a second thread, updateMeshes returning false "
+                    "while it runs (the mesh copied each step is the last finished one)"}
     _drop_frames(tmp, dpath, bpath)
+    if not secs:
+        return {"value": None, "unit": UNIT, "cores": 1, "kind": kind,
+                "unavailable": "the reference runs did not finish within their time limit"}
     med = float(np.median(secs))
     return {"value": round(a.steps * FRAMES_PER_STEP / med, 3), "unit": UNIT, "cores": 1, "kind": kind,
             "runs": [round(a.steps * FRAMES_PER_STEP / t, 3) for t in secs], "statistic": f"median of {runs}",
@@ -733,6 +780,10 @@ def run_reference(a):
             for i in range(workers)]
     secs = _run_workers(jobs, with_barrier=True)
     _drop_frames(tmp, dpath, bpath)
+    if not secs:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "the reference's maps did not finish within their time limit"}), flush=True)
+        return
     wall = max(secs)
     value = workers * a.steps * FRAMES_PER_STEP / wall
     line = {

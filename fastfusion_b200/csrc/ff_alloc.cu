@@ -15,6 +15,7 @@
 #include <cub/cub.cuh>
 
 #include "ff_kernels.h"
+#include "ff_sort.h"
 
 namespace ffb {
 
@@ -594,28 +595,23 @@ void launch_insert(const BatchDesc *d_batch, uint32_t pix, cudaStream_t s, int b
 
 // ------------------------------------------------- pending leaf order -----
 
-__global__ void k_pending_keys(const PendingLeaf *pend, int npend, uint32_t *keys, uint32_t *vals) {
+__global__ void k_pending_keys(const PendingLeaf *pend, int npend, uint64_t *keys) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= npend) return;
   keys[i] = pend[i].first_pixel;
-  vals[i] = (uint32_t)i;
 }
 
-size_t pending_sort_bytes(int n) {
-  size_t bytes = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, bytes, (uint32_t *)nullptr, (uint32_t *)nullptr, (uint32_t *)nullptr,
-                                  (uint32_t *)nullptr, n);
-  return bytes;
-}
+size_t pending_sort_bytes(int n) { return argsort_temp_bytes((uint32_t)std::max(n, 0)); }
 
-cudaError_t sort_pending(const PendingLeaf *pend, int npend, uint32_t *keys_in, uint32_t *vals_in, uint32_t *keys_out,
-                         uint32_t *vals_out, void *tmp, size_t tmp_bytes, int end_bit, cudaStream_t s) {
+cudaError_t sort_pending(const PendingLeaf *pend, int npend, uint64_t *keys, uint64_t *keys_sorted, uint32_t *order,
+                         void *tmp, size_t tmp_bytes, int end_bit, cudaStream_t s) {
   if (npend <= 0) return cudaSuccess;
   note_launch();
-  k_pending_keys<<<(npend + 255) / 256, 256, 0, s>>>(pend, npend, keys_in, vals_in);
-  note_lib_call();
-  return cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys_in, keys_out, vals_in, vals_out, npend, 0, end_bit,
-                                         s);
+  k_pending_keys<<<(npend + 255) / 256, 256, 0, s>>>(pend, npend, keys);
+  unsigned launches = 0;
+  const cudaError_t e = argsort_u64(keys, (uint32_t)npend, end_bit, keys_sorted, order, tmp, tmp_bytes, s, &launches);
+  note_launch(launches);
+  return e;
 }
 
 // Leaf index = leaves_before + rank of first pixel; indices past the pool are

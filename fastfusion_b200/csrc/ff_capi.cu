@@ -98,7 +98,8 @@ struct ff_handle {
   int4 *d_bnd = nullptr;
   size_t bnd_elems = 0;
   PendingLeaf *d_pend = nullptr;
-  uint32_t *d_keys = nullptr;  // 4 x cap_pix
+  // 6 x cap_pix words: pending-leaf sort keys (u64), sorted keys (u64), order; finalisation ranks
+  uint32_t *d_keys = nullptr;
   void *d_sort_tmp = nullptr;
   size_t sort_tmp_bytes = 0;
 
@@ -455,7 +456,7 @@ static ff_status ensure_image(ff_handle *h, int W, int H) {
     CK(alloc(&h->d_vox, npix));
     CK(alloc(&h->d_proc, npix));
     CK(alloc(&h->d_pend, npix));
-    CK(alloc(&h->d_keys, (size_t)npix * 4));
+    CK(alloc(&h->d_keys, (size_t)npix * 6));
     h->sort_tmp_bytes = pending_sort_bytes(npix);
     CK(cudaMalloc(&h->d_sort_tmp, std::max<size_t>(h->sort_tmp_bytes, 16)));
     h->cap_pix = npix;
@@ -1072,7 +1073,7 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
   mf.stamp = h->d_stamp;
   mf.bstamp = h->d_bstamp;
   mf.queue = h->d_queue;
-  mf.rank = h->d_keys + 3 * h->cap_pix;
+  mf.rank = h->d_keys + 5 * h->cap_pix;
   mf.pend = h->d_pend;
   mf.vox = h->d_vox;
   mf.proc = h->d_proc;
@@ -1362,11 +1363,12 @@ static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf,
   const uint32_t nq = plan.one_sync && !plan.counters_early ? hc.queued : hc.queued + new_queued;
   if (!plan.one_sync && npend) {
     pi_fin = h->prof.begin(ST_FINALIZE, s);
-    uint32_t *k_in = h->d_keys, *v_in = h->d_keys + h->cap_pix, *k_out = h->d_keys + 2 * h->cap_pix,
-             *v_out = h->d_keys + 3 * h->cap_pix;
+    uint64_t *k_in = reinterpret_cast<uint64_t *>(h->d_keys),
+             *k_out = reinterpret_cast<uint64_t *>(h->d_keys + 2 * h->cap_pix);
+    uint32_t *v_out = h->d_keys + 4 * h->cap_pix;
     int end_bit = 1;
     while ((1u << end_bit) < (uint32_t)(W * H)) end_bit++;
-    CK(sort_pending(h->d_pend, (int)npend, k_in, v_in, k_out, v_out, h->d_sort_tmp, h->sort_tmp_bytes, end_bit, s));
+    CK(sort_pending(h->d_pend, (int)npend, k_in, k_out, v_out, h->d_sort_tmp, h->sort_tmp_bytes, end_bit, s));
     launch_finalize(h->d_pend, v_out, (int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->d_leaf,
                     plan.frame, h->d_stamp, h->d_queue, h->d_cnt, s);
     launch_parents((int)npend, leaves_before, h->cfg.leaves_max, h->d_tree, h->n, h->d_leaf, h->d_parent, s);

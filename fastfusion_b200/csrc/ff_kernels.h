@@ -228,9 +228,10 @@ void launch_insert(const BatchDesc *d_batch, uint32_t pix, cudaStream_t s, int b
 
 // Sort scratch size for `n` pending leaves.
 size_t pending_sort_bytes(int n);
-// Order pending leaves by first pixel; out_rec receives record ids.
-cudaError_t sort_pending(const PendingLeaf *pend, int npend, uint32_t *keys_in, uint32_t *vals_in, uint32_t *keys_out,
-                         uint32_t *vals_out, void *tmp, size_t tmp_bytes, int end_bit, cudaStream_t s);
+// Order pending leaves by first pixel: order[k] = record of the k-th (keys
+// and keys_sorted: npend 64-bit words each of scratch).
+cudaError_t sort_pending(const PendingLeaf *pend, int npend, uint64_t *keys, uint64_t *keys_sorted, uint32_t *order,
+                         void *tmp, size_t tmp_bytes, int end_bit, cudaStream_t s);
 
 // Assign leaf indices in creation order, fill the leaf table, queue new leaves.
 void launch_finalize(const PendingLeaf *pend, const uint32_t *order, int npend, uint32_t leaves_before,

@@ -20,3 +20,26 @@ def circle_frames(seed: int, n_frames: int, width: int, height: int, total: int 
 
 def queue_set(q) -> set:
     return set(int(x) for x in q)
+
+
+BRANCHINIT = 0xFFFFFFFE
+
+
+def tree_shape(tree) -> list:
+    """The octree with its branch numbering taken out: per branch, in a
+    depth-first walk from the root in octant order, its eight leaf entries
+    and which of its eight children exist.  Branch indices are handed out in
+    the order threads reach them on the GPU and in traversal order on the
+    CPU, so two octrees of the same map compare equal in this form."""
+    tree = np.asarray(tree, np.uint32)
+    out = []
+    stack = [0] if len(tree) >= 16 else []
+    while stack:
+        b = stack.pop()
+        row = tree[b:b + 16]
+        out.append((tuple(int(x) for x in row[:8]), tuple(bool(x != BRANCHINIT) for x in row[8:])))
+        for co in range(7, -1, -1):
+            c = int(row[8 + co])
+            if c != BRANCHINIT:
+                stack.append(c)
+    return out

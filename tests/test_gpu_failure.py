@@ -12,7 +12,7 @@ handle then fuses the following frames bit-exactly against the oracle.
 import numpy as np
 import pytest
 
-from tests.helpers import MAXCAM, SCALING, circle_frames, queue_set
+from tests.helpers import MAXCAM, SCALING, circle_frames, queue_set, tree_shape
 
 pytestmark = pytest.mark.gpu
 
@@ -34,7 +34,7 @@ def _same_map(g, p):
     assert (sg["n"], sg["leaves_used"]) == (sp["n"], sp["leaves_used"])
     for a, b in zip(g.leaves(), p.leaves()):
         assert np.array_equal(a, b)
-    assert np.array_equal(g.tree(), p.tree())
+    assert tree_shape(g.tree()) == tree_shape(p.tree())
     dg, wg, cg = g.bricks()
     dp, wp, cp = p.bricks()
     assert np.array_equal(dg.view(np.uint32), dp.view(np.uint32))

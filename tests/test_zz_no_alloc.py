@@ -54,7 +54,9 @@ def test_noalloc_rejects_more_cells_than_its_buffer(lib_built):
     FF_ERR_BAD_ARG and a message, and nothing is written to the caller's
     buffers; the allocating export still returns it."""
     from fastfusion_b200 import fusion as ff
-    K, frames = circle_frames(0, 4, 1280, 960)
+    # a quarter turn of 1280x960 frames at 2 mm voxels: well over 65,536
+    # cells (four nearly overlapping frames made 53,432)
+    K, frames = circle_frames(0, 10, 1280, 960, total=40)
     m = ff.FusionMipMapCPU(0, 0, 0, 0.002, 0.004, 0, True, leaves_max=400000, branches_max=8000000, rcp="exact")
     for depth, bgr, R, t in frames:
         m.addMap(depth, ff.CameraInfo(K, R, t), bgr, SCALING, MAXCAM)
