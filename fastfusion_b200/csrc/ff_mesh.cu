@@ -135,7 +135,8 @@ struct GenCtx {
   uint32_t leaves_max;
   // Incremental generation (incr != 0): only items with a slot that changed
   // since the previous update are expanded or emit cells; the cells of the
-  // other items are kept from the previous list.  A slot changed if its
+  // other items are kept from the previous list.  A slot changed if it lies
+  // in a branch allocated since (entry index >= prev_branches), if its
   // finest leaf at or above is new (index >= prev_leaves), if it was
   // subdivided since (child branch index >= prev_branches), or if a branch
   // or leaf was created in its subtree since (branch stamp > since).
@@ -168,6 +169,9 @@ __device__ __forceinline__ Slot ch(const GenCtx &g, const Slot &s, int co) { ret
 
 __device__ __forceinline__ bool slot_changed(const GenCtx &g, const Slot &s) {
   if (!g.incr) return true;
+  // a slot of a branch allocated since: it did not exist (its cells are new
+  // even where it inherits an old leaf)
+  if (s.S >= g.prev_branches) return true;
   if (s.la < g.leaves_max && s.la >= g.prev_leaves) return true;
   const uint32_t c = tree_at(g, s.S + 8);
   if (c >= PENDING) return false;

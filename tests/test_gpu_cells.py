@@ -82,6 +82,7 @@ def test_incremental_cells_on_the_walk(lib_built):
         d16 = torch.empty((480, 640), dtype=torch.int16, device="cuda")
         d16.copy_(d)
         c = c.contiguous()
+        torch.cuda.synchronize()  # the maps read the images on their own streams
         cam = CameraInfo(seq.K, R, t)
         qa = a.addMapDevice(d16.data_ptr(), c.data_ptr(), 640, 480, cam, SCALING, MAXCAM)
         qb = b.addMapDevice(d16.data_ptr(), c.data_ptr(), 640, 480, cam, SCALING, MAXCAM)
