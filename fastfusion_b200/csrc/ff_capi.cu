@@ -79,6 +79,7 @@ struct ff_handle {
   uint32_t *d_stamp = nullptr;
   uint32_t *d_bstamp = nullptr;  // per branch: last frame that created something at or below it
   uint32_t *d_queue = nullptr;
+  uint32_t *d_queue_last = nullptr;  // the queue the last finished frame wrote (ff_get_queue)
   Counters *d_cnt = nullptr;
   Counters *h_cnt = nullptr;  // pinned
   uint32_t *d_barrier = nullptr;
@@ -1392,6 +1393,8 @@ static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf,
     ff_status st = grow(h, hc.box_min, hc.box_max);
     h->prof.end(pi, tree_bytes, s);  // octree and leaf positions read and written
     if (st != FF_OK) return st;
+    // the brick ownership of a part follows the moved positions
+    for (int r = 0; r < 3; r++) mf.shift[r] = h->shift[r];
     fuse_now = !skip_update;
   }
   // fuse: every voxel of every queued brick read and written: SDF, weight
@@ -1419,6 +1422,7 @@ static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf,
   CK(cudaGetLastError());
   if (h->leaves_used > h->cfg.leaves_max) h->meshing_ok = false;
   h->queued = nq;
+  h->d_queue_last = mf.queue;
   h->frames++;
   mesh_note_frame(h->mesh);
   if (queued) *queued = (int32_t)nq;
@@ -1954,7 +1958,8 @@ ff_status ff_get_queue(ff_handle *h, uint32_t *leaves) {
   if (!h || !leaves) return FF_ERR_BAD_ARG;
   CK(cudaSetDevice(h->cfg.device));
   CK(join_fuse(h));
-  if (h->queued) CK(cudaMemcpyAsync(leaves, h->d_queue, sizeof(uint32_t) * h->queued, cudaMemcpyDeviceToHost, h->stream));
+  const uint32_t *q = h->d_queue_last ? h->d_queue_last : h->d_queue;
+  if (h->queued) CK(cudaMemcpyAsync(leaves, q, sizeof(uint32_t) * h->queued, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return FF_OK;
 }

@@ -20,6 +20,7 @@
 #include <iostream>
 #include <thread>
 #include <tuple>
+#include <xmmintrin.h>
 #define protected public
 #include <fusion/geometryfusion_mipmap_cpu.hpp>
 #undef protected
@@ -169,12 +170,18 @@ int ref_loop_delete(void *h, const float *depth, const uint8_t *red, const uint8
                  rot.at<double>(2, 0) * ox + rot.at<double>(2, 1) * oy + rot.at<double>(2, 2) * oz + tr.at<double>(2, 0),
                  in.at<double>(0, 0), in.at<double>(1, 1), in.at<double>(0, 2), in.at<double>(1, 2));
   volumetype mapped = *n_mapped;
+  // updateWrapper_deleteloop returns false when the slots run out
+  // (loopclosure.cpp:287) without restoring the rounding mode it switched to
+  // round-toward-zero (:276; restored only at :309): the caller's mode is
+  // put back here, so that the next frame's camera set-up rounds as usual
+  const unsigned int caller_mode = _MM_GET_ROUNDING_MODE();
   const bool ok = updateWrapper_deleteloop(
       threadparameterLoop(depth, red, green, blue, w, hgt, p.r11, p.r12, p.r13, p.t1, p.r21, p.r22, p.r23, p.t2,
                           p.r31, p.r32, p.r33, p.t3, p.fx, p.fy, p.cx, p.cy, f->_scale, f->_distanceThreshold,
                           (volumetype *)queue, f->_leafPos, f->_leafScale, dist, wgt, (colortype3 *)col,
                           f->_brickLength),
       (size_t)nq, (volumetype *)leaf_map, (volumetype)capacity, &mapped);
+  _MM_SET_ROUNDING_MODE(caller_mode);
   *n_mapped = mapped;
   return ok ? 1 : 0;
 }
