@@ -571,7 +571,9 @@ __global__ void k_gather_cells(const Cell *in, const uint32_t *order, uint32_t n
 // (index >= prev_branches; a child slot, once set, never changes), so the
 // descent stops where the previous one stopped: at the slot that was not
 // subdivided.  It changed if it is subdivided now or if its finest leaf at or
-// above is new.
+// above is new.  Most of the octree is unchanged: the descent ends early at
+// a branch whose subtree gained nothing (its stamp) while the leaves on the
+// path so far are old, since every leaf further down is old then too.
 __device__ __forceinline__ bool side_changed(const GenCtx &g, uint32_t n, const int (&p)[3]) {
   uint32_t branch = 0, la = BRANCHINIT, half = n >> 1;
   uint32_t ox = 0, oy = 0, oz = 0;
@@ -584,6 +586,9 @@ __device__ __forceinline__ bool side_changed(const GenCtx &g, uint32_t n, const 
     const uint32_t c = tree_at(g, S + 8);
     if (c >= PENDING) return la < g.leaves_max && la >= g.prev_leaves;
     if (c >= g.prev_branches) return true;
+    // nothing created below since, and no new leaf on the path so far: the
+    // slot and its finest leaf are as they were
+    if (__ldg(g.bstamp + (c >> 4)) <= g.since && !(la < g.leaves_max && la >= g.prev_leaves)) return false;
     ox += half * ((co & 1) != 0);
     oy += half * ((co & 2) != 0);
     oz += half * ((co & 4) != 0);
