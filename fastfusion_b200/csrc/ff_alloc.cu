@@ -675,6 +675,33 @@ __global__ void k_parents(int npend, uint32_t leaves_before, uint32_t leaves_max
   parent[idx] = parent_of(idx, leaves_max, tree, n, leaf[idx]);
 }
 
+// Parents of the leaves the finalisation of each frame of the descriptor
+// placed: blocks PARENT_BLOCKS per frame, striding over its new leaves.  A
+// parent is the finest ancestor with a smaller index, so it can be found any
+// time after the leaf is placed; off the chain of frames (the next frame's
+// insert does not wait for it).  Frames that placed nothing are skipped.
+constexpr int PARENT_BLOCKS = 4, PARENT_THREADS = 256;
+
+__global__ void __launch_bounds__(PARENT_THREADS) k_parents_frames(const BatchDesc *__restrict__ bd, int m0) {
+  const MapFrame &F = bd->f[m0 + blockIdx.x / PARENT_BLOCKS];
+  const Counters *cnt = F.cnt;
+  if (ld_volatile(&cnt->error) & (ERR_DEDUPE_FAILED | ERR_PENDING_OVERFLOW | ERR_SEQ_HALT)) return;
+  const uint32_t npend = ld_volatile(&cnt->pending);
+  const uint32_t leaves_before = F.chain ? ld_volatile(&cnt->leaves_base) : F.leaves_before;
+  const uint32_t stride = PARENT_BLOCKS * PARENT_THREADS;
+  for (uint32_t j = (blockIdx.x % PARENT_BLOCKS) * PARENT_THREADS + threadIdx.x; j < npend; j += stride) {
+    const uint32_t idx = leaves_before + j;
+    if (idx >= F.leaves_max) break;
+    F.parent[idx] = parent_of(idx, F.leaves_max, F.tree, F.n, F.leaf[idx]);
+  }
+}
+
+void launch_parents_frames(const BatchDesc *d_batch, int nframes, cudaStream_t s, int m0) {
+  if (nframes < 1) return;
+  note_launch();
+  k_parents_frames<<<nframes * PARENT_BLOCKS, PARENT_THREADS, 0, s>>>(d_batch, m0);
+}
+
 // The whole frame's pending leaves in one block.  A leaf's creation rank is
 // the number of pending leaves with a smaller first pixel; first pixels are
 // distinct (a pixel creates at most one leaf), so the rank is a prefix count
@@ -718,8 +745,7 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc
   const PendingLeaf *pend = F.pend;
   const uint32_t leaves_before = F.chain ? ld_volatile(&cnt->leaves_base) : F.leaves_before;
   const uint32_t npix = F.npix, leaves_max = F.leaves_max, frame = F.frame;
-  const uint32_t n = F.n;
-  uint32_t *rank = F.rank, *tree = F.tree, *stamp = F.stamp, *queue = F.queue, *parent = F.parent;
+  uint32_t *rank = F.rank, *tree = F.tree, *stamp = F.stamp, *queue = F.queue;
   ushort4 *leaf = F.leaf;
   const uint32_t nwords = (npix + 31) / 32;
   uint32_t *bitmap = fin_smem;
@@ -752,11 +778,8 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc
     rank[j] = r;
     finalize_one(p, leaves_before + r, leaves_max, tree, leaf, frame, stamp, queue, cnt);
   }
+  // (the new leaves' parents: k_parents_frames, after this kernel)
   __syncthreads();
-  for (int j = t; j < npend; j += FIN_THREADS) {
-    const uint32_t idx = leaves_before + rank[j];
-    if (idx < leaves_max) parent[idx] = parent_of(idx, leaves_max, tree, n, leaf[idx]);
-  }
   // Deferred update: the frame's queue is complete (the new leaves were
   // queued above); mark each queued brick with the frame's bit and list the
   // bricks no earlier frame of the pass has marked.  A frame the update must
@@ -861,7 +884,7 @@ cudaError_t prewarm_alloc_kernels() {
                        (const void *)k_dedupe_one<DD_ROWS_TALL>,
                        (const void *)k_dedupe<DD_ROWS_LOW>,
                        (const void *)k_dedupe<DD_ROWS_TALL>, (const void *)k_insert,
-                       (const void *)k_pending_keys, (const void *)k_finalize, (const void *)k_parents,
+                       (const void *)k_pending_keys, (const void *)k_finalize, (const void *)k_parents, (const void *)k_parents_frames,
                        (const void *)k_finalize_bitmap, (const void *)k_shift_branches,
                        (const void *)k_shift_leaves, (const void *)k_fill};
   for (const void *f : fns) {

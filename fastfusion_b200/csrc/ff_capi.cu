@@ -1299,11 +1299,13 @@ static ff_status frame_launch_update(ff_handle *lead, int n, uint32_t max_npix, 
   pi_fin = lead->prof.begin(ST_FINALIZE, fs);
   if (!launch_finalize_small(lead->d_batch, n, max_npix, lead->cfg.device, fs))
     return set_err(lead, FF_ERR_CUDA, "leaf finalisation could not be launched");
-  lead->prof.end(pi_fin, 0.0, fs);
   if (side) {
     CK(cudaEventRecord(lead->ev_fin, fs));
     lead->fin_pending = true;
   }
+  // the new leaves' parents: after the event the next frame's insert waits for
+  launch_parents_frames(lead->d_batch, n, fs);
+  lead->prof.end(pi_fin, 0.0, fs);
   if (!deferred) {
     pi_fuse = lead->prof.begin(ST_FUSE, fs);
     // enough blocks for a frame's bricks in one pass; blocks loop over larger batches
@@ -1680,6 +1682,8 @@ static ff_status sequence_chunk(ff_handle *h, int c, const uint16_t *const *d_de
       return set_err(h, FF_ERR_CUDA, "leaf finalisation could not be launched");
     h->prof.end(pi, 0.0, s);
   }
+  // the parents of every frame's new leaves, once the chain has run
+  launch_parents_frames(h->d_batch, c, s);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(h->h_seq_cnt, h->d_seq_cnt, sizeof(Counters) * c, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));

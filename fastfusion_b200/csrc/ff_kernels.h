@@ -237,6 +237,9 @@ cudaError_t sort_pending(const PendingLeaf *pend, int npend, uint64_t *keys, uin
 void launch_finalize(const PendingLeaf *pend, const uint32_t *order, int npend, uint32_t leaves_before,
                      uint32_t leaves_max, uint32_t *tree, ushort4 *leaf, uint32_t frame, uint32_t *stamp,
                      uint32_t *queue, Counters *cnt, cudaStream_t s);
+// Parents of the leaves placed by the one-block finalisation of frames
+// [m0, m0 + nframes) of the descriptor (after it on the stream).
+void launch_parents_frames(const BatchDesc *d_batch, int nframes, cudaStream_t s, int m0 = 0);
 // Parent leaf of each new leaf: finest ancestor leaf created before it.
 void launch_parents(int npend, uint32_t leaves_before, uint32_t leaves_max, const uint32_t *tree, uint32_t n,
                     const ushort4 *leaf, uint32_t *parent, cudaStream_t s);
