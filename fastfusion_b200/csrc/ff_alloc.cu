@@ -414,6 +414,19 @@ __device__ __forceinline__ void queue_leaf(uint32_t leaf, uint32_t frame, uint32
   }
 }
 
+// The second half of queue_leaf for a leaf whose stamp was read earlier (st):
+// the insert's descent reads a level's stamp, then issues the next level's
+// octree loads before it looks at the value, so that the two round trips
+// overlap.
+__device__ __forceinline__ void queue_leaf_after(uint32_t leaf, uint32_t st, uint32_t frame, uint32_t *stamp,
+                                                 uint32_t *queue, Counters *cnt) {
+  if (st == frame) return;
+  if (atomicExch(&stamp[leaf], frame) != frame) {
+    uint32_t q = atomicAdd(&cnt->queued, 1u);
+    queue[q] = leaf;
+  }
+}
+
 // Wait until another thread finished allocating tree[ptr]; bounded.
 __device__ __forceinline__ uint32_t wait_unlocked(uint32_t *tree, uint32_t ptr, uint32_t cur, Counters *cnt,
                                                   bool *ok, uint32_t limit) {
@@ -458,13 +471,17 @@ __device__ __forceinline__ uint32_t insert_descend(const MapFrame &F, int i, int
   uint32_t half = (uint16_t)(n >> 1);
   uint32_t branch = 0;
   bool ok = true;
+  // the previous level's leaf (if any) and its stamp, read but not yet looked at
+  uint32_t prev_leaf = BRANCHINIT, prev_st = frame;
   while ((half >> 1) >= target) {
     probed++;
     uint32_t co = (x >= ox + half) * 1u + (y >= oy + half) * 2u + (z >= oz + half) * 4u;
     uint32_t ptr = branch + co + 8;
     uint32_t leaf = ld_tree(tree + ptr - 8);
-    if (leaf < leaves_max) queue_leaf(leaf, frame, stamp, queue, cnt);
     uint32_t child = ld_tree(tree + ptr);
+    if (prev_leaf < leaves_max) queue_leaf_after(prev_leaf, prev_st, frame, stamp, queue, cnt);
+    prev_leaf = leaf;
+    prev_st = leaf < leaves_max ? ld_volatile(&stamp[leaf]) : frame;
     if (child == BRANCHINIT) {
       uint32_t old = atomicCAS(tree + ptr, BRANCHINIT, LOCKED);
       if (old == BRANCHINIT) {
@@ -472,6 +489,7 @@ __device__ __forceinline__ uint32_t insert_descend(const MapFrame &F, int i, int
         if (nb + 16 > branches_max) {
           atomicOr(&cnt->error, ERR_BRANCH_OVERFLOW);
           atomicExch(tree + ptr, BRANCHINIT);
+          if (prev_leaf < leaves_max) queue_leaf_after(prev_leaf, prev_st, frame, stamp, queue, cnt);
           return probed;
         }
         __threadfence();
@@ -483,7 +501,10 @@ __device__ __forceinline__ uint32_t insert_descend(const MapFrame &F, int i, int
       }
     }
     child = wait_unlocked(tree, ptr, child, cnt, &ok, F.spin_limit);
-    if (!ok || child == BRANCHINIT) return probed;
+    if (!ok || child == BRANCHINIT) {
+      if (prev_leaf < leaves_max) queue_leaf_after(prev_leaf, prev_st, frame, stamp, queue, cnt);
+      return probed;
+    }
     ox += half * ((co & 1) != 0);
     oy += half * ((co & 2) != 0);
     oz += half * ((co & 4) != 0);
@@ -494,6 +515,7 @@ __device__ __forceinline__ uint32_t insert_descend(const MapFrame &F, int i, int
   uint32_t ptr = branch + co;
   probed++;
   uint32_t cur = ld_tree(tree + ptr);
+  if (prev_leaf < leaves_max) queue_leaf_after(prev_leaf, prev_st, frame, stamp, queue, cnt);
   if (cur == BRANCHINIT) {
     uint32_t old = atomicCAS(tree + ptr, BRANCHINIT, LOCKED);
     if (old == BRANCHINIT) {
