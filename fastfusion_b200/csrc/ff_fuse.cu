@@ -288,7 +288,17 @@ __global__ void __launch_bounds__(512, FUSE_MULTI_BLOCKS_PER_SM) k_fuse_multi(co
     const float thrD = __fmul_rz(thr, ls);
     const float thrW = __fmul_rz(__fmul_rz(WEIGHT_FACTOR, thr), ls);
     const float fx_ = (float)x;
-    for (int k = 0; k < nk; k++) {
+    // Frame k's sample of this voxel: the projection and the image reads,
+    // issued one frame ahead so that they overlap the previous frame's
+    // update (which they do not depend on).
+    struct Sample {
+      float len, rc;
+      bool in;  // in front of the camera and inside the image
+      uint16_t draw;
+      uint8_t cr, cg, cb;
+      float cw;
+    };
+    auto fetch = [&](int k, Sample &sm) {
       const int j = order[k];
       const FuseSlot &S = fb.s[j];
       const float3 rb = rows[j][z * 8 + y];
@@ -299,25 +309,35 @@ __global__ void __launch_bounds__(512, FUSE_MULTI_BLOCKS_PER_SM) k_fuse_multi(co
       const float kz = x == 0 ? 0.0f : (x == 1 ? d1.z : __fmul_rz(fx_, d1.z));
       const float px = __fadd_rz(rb.x, kx), py = __fadd_rz(rb.y, ky), pz = __fadd_rz(rb.z, kz);
       const int W = S.W, H = S.H;
-      const float len = __fsqrt_rz(__fadd_rz(__fadd_rz(__fmul_rz(px, px), __fmul_rz(py, py)), __fmul_rz(pz, pz)));
-      const float rc = rcp_upd<RCP_HOST>(pz, rtab, rshift);
-      const int imx = cvt_x86_rz(__fadd_rz(S.q.cx, __fmul_rz(S.q.fx, __fmul_rz(px, rc))));
-      const int imy = cvt_x86_rz(__fadd_rz(S.q.cy, __fmul_rz(S.q.fy, __fmul_rz(py, rc))));
+      sm.len = __fsqrt_rz(__fadd_rz(__fadd_rz(__fmul_rz(px, px), __fmul_rz(py, py)), __fmul_rz(pz, pz)));
+      sm.rc = rcp_upd<RCP_HOST>(pz, rtab, rshift);
+      const int imx = cvt_x86_rz(__fadd_rz(S.q.cx, __fmul_rz(S.q.fx, __fmul_rz(px, sm.rc))));
+      const int imy = cvt_x86_rz(__fadd_rz(S.q.cy, __fmul_rz(S.q.fy, __fmul_rz(py, sm.rc))));
+      sm.in = pz > 0.0f && imy < H && imy > -1 && imx < W && imx > -1;
       const int cyi = max(min(imy, H - 1), 0);
       const int cxi = max(min(imx, W - 1), 0);
       const int ii = W * cyi + cxi;
-      const uint16_t draw = __ldg(S.depth + ii);
+      sm.draw = __ldg(S.depth + ii);
       const uint8_t *p8 = S.bgr + 3 * (size_t)ii;
-      const uint8_t cr = __ldg(p8 + 2), cg = __ldg(p8 + 1), cbl = __ldg(p8 + 0);
-      const float cw = S.conf ? __ldg(S.conf + ii) : 1.0f;
-      const float h = __fmul_rz(S.scaling, (float)draw);
+      sm.cr = __ldg(p8 + 2);
+      sm.cg = __ldg(p8 + 1);
+      sm.cb = __ldg(p8 + 0);
+      sm.cw = S.conf ? __ldg(S.conf + ii) : 1.0f;
+    };
+    Sample cur, nxt;
+    if (nk > 0) fetch(0, cur);
+    for (int k = 0; k < nk; k++) {
+      if (k + 1 < nk) fetch(k + 1, nxt);
+      const FuseSlot &S = fb.s[order[k]];
+      const float len = cur.len, rc = cur.rc;
+      const float h = __fmul_rz(S.scaling, (float)cur.draw);
       const float dInc = __fsub_rz(len, __fmul_rz(__fmul_rz(len, rc), h));
-      const bool msk = pz > 0.0f && imy < H && imy > -1 && imx < W && imx > -1 && h < S.maxcam;
+      const bool msk = cur.in && h < S.maxcam;
       const float front = dInc < DIST_W_EPS ? 1.0f : 0.0f;
       const float back = (dInc >= DIST_W_EPS && dInc < thrW) ? 1.0f : 0.0f;
       const float fall = __fmul_rz(__fsub_rz(thrW, dInc), rcp_upd<RCP_HOST>(__fsub_rz(thrW, DIST_W_EPS), rtab, rshift));
       float wInc = msk ? __fadd_rz(front, __fmul_rz(fall, back)) : 0.0f;
-      if (S.conf) wInc = __fmul_rz(wInc, cw);
+      if (S.conf) wInc = __fmul_rz(wInc, cur.cw);
       const float wNew = __fadd_rz(wAcc, wInc);
       const float factor = rcp_upd<RCP_HOST>(__fadd_rz(wNew, wNew <= 0.0f ? 1.0f : 0.0f), rtab, rshift);
       float tr = dInc < thrD ? dInc : thrD;
@@ -325,8 +345,8 @@ __global__ void __launch_bounds__(512, FUSE_MULTI_BLOCKS_PER_SM) k_fuse_multi(co
       tr = tr > lo ? tr : lo;
       const float add = msk ? __fmul_rz(tr, wInc) : 0.0f;
       const float dNew = __fmul_rz(__fadd_rz(__fmul_rz(dAcc, wAcc), add), factor);
-      const float inc[3] = {__fmul_rz((float)cr, COLOR_MUL), __fmul_rz((float)cg, COLOR_MUL),
-                            __fmul_rz((float)cbl, COLOR_MUL)};
+      const float inc[3] = {__fmul_rz((float)cur.cr, COLOR_MUL), __fmul_rz((float)cur.cg, COLOR_MUL),
+                            __fmul_rz((float)cur.cb, COLOR_MUL)};
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         float val = __fmul_rz(__fadd_rz(__fmul_rz((float)acc[c], wAcc), __fmul_rz(inc[c], wInc)), factor);
@@ -341,6 +361,7 @@ __global__ void __launch_bounds__(512, FUSE_MULTI_BLOCKS_PER_SM) k_fuse_multi(co
         dAcc = dNew;
         wAcc = wNew;
       }
+      cur = nxt;
     }
     if (FP16) {
       fb.sdf16[vi] = __float2half_rn(dAcc);
