@@ -38,6 +38,10 @@ struct ff_handle {
   // host-input frames: the colour image is copied on a second stream while
   // the allocation kernels run (it is first read by the voxel update)
   cudaStream_t copy_stream = nullptr;
+  // ff_get_mesh_async: the mesh's device-to-host copies, after ev_mesh_ready
+  cudaStream_t mesh_stream = nullptr;
+  cudaEvent_t ev_mesh_ready = nullptr, ev_mesh_copied = nullptr;
+  bool mesh_copy_pending = false;
   cudaEvent_t ev_bgr_free = nullptr, ev_bgr_ready = nullptr;
   // recorded once a frame's counters have reached the host: a single-map
   // frame returns then, while its voxel update still runs
@@ -579,7 +583,10 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
     if (cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_bgr_free, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_bgr_ready, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h->ev_counters, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&h->ev_counters, cudaEventDisableTiming) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->mesh_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_mesh_ready, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_mesh_copied, cudaEventDisableTiming) != cudaSuccess) {
       fail(FF_ERR_CUDA, "copy stream");
       break;
     }
@@ -688,6 +695,7 @@ ff_status ff_destroy(ff_handle *h) {
   cudaSetDevice(h->cfg.device);
   if (h->fuse_stream) cudaStreamSynchronize(h->fuse_stream);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->mesh_stream) cudaStreamSynchronize(h->mesh_stream);  // (copies out of the mesh buffers)
   mesh_free(h->mesh);
   h->prof.destroy();
   void *ptrs[] = {h->d_tree, h->d_leaf, h->d_parent, h->d_sdf, h->d_wgt, h->d_sdf16, h->d_wgt16, h->d_col,
@@ -725,6 +733,9 @@ ff_status ff_destroy(ff_handle *h) {
   if (h->ev_bgr_free) cudaEventDestroy(h->ev_bgr_free);
   if (h->ev_bgr_ready) cudaEventDestroy(h->ev_bgr_ready);
   if (h->ev_counters) cudaEventDestroy(h->ev_counters);
+  if (h->mesh_stream) cudaStreamDestroy(h->mesh_stream);
+  if (h->ev_mesh_ready) cudaEventDestroy(h->ev_mesh_ready);
+  if (h->ev_mesh_copied) cudaEventDestroy(h->ev_mesh_copied);
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   delete h;
   return FF_OK;
@@ -945,7 +956,7 @@ ff_status ff_sync(ff_handle *h) {
   FCK(settle(h));
   CK(cudaStreamSynchronize(h->stream));
   CK(cudaStreamSynchronize(h->fuse_stream));
-  return FF_OK;
+  return ff_mesh_wait(h);
 }
 
 ff_status ff_set_stream(ff_handle *h, void *cuda_stream) {
@@ -2074,6 +2085,9 @@ ff_status ff_update_meshes(ff_handle *h, int *updated) {
     if (updated) *updated = 1;
     return FF_OK;
   }
+  // the mesh buffers are rewritten (or freed as they grow) only after the
+  // copies of an earlier ff_get_mesh_async have read them
+  if (h->mesh_copy_pending) CK(cudaStreamWaitEvent(h->stream, h->ev_mesh_copied, 0));
   MeshInputs in;
   in.tree = h->d_tree;
   in.branches_used = h->branches_used;
@@ -2152,6 +2166,35 @@ ff_status ff_get_mesh(ff_handle *h, float *xyz, uint8_t *rgb, uint32_t *faces) {
   std::string err;
   int rc = mesh_copy_out(h->mesh, xyz, rgb, faces, h->stream, err);
   if (rc != 0) return set_err(h, (ff_status)rc, err);
+  return FF_OK;
+}
+
+ff_status ff_get_mesh_async(ff_handle *h, float *xyz, uint8_t *rgb, uint32_t *faces) {
+  if (!h) return FF_ERR_BAD_ARG;
+  const MeshState &M = h->mesh;
+  if ((M.n_vertices && (!xyz || !rgb)) || (M.n_faces && !faces))
+    return set_err(h, FF_ERR_BAD_ARG, "ff_get_mesh_async: NULL output buffer");
+  CK(cudaSetDevice(h->cfg.device));
+  // behind the update's device work (its emit pass may still run)
+  CK(cudaEventRecord(h->ev_mesh_ready, h->stream));
+  CK(cudaStreamWaitEvent(h->mesh_stream, h->ev_mesh_ready, 0));
+  if (M.n_vertices) {
+    CK(cudaMemcpyAsync(xyz, M.d_xyz, sizeof(float) * 3 * M.n_vertices, cudaMemcpyDeviceToHost, h->mesh_stream));
+    CK(cudaMemcpyAsync(rgb, M.d_rgb, 3 * M.n_vertices, cudaMemcpyDeviceToHost, h->mesh_stream));
+  }
+  if (M.n_faces)
+    CK(cudaMemcpyAsync(faces, M.d_faces, sizeof(uint32_t) * 3 * M.n_faces, cudaMemcpyDeviceToHost, h->mesh_stream));
+  CK(cudaEventRecord(h->ev_mesh_copied, h->mesh_stream));
+  h->mesh_copy_pending = true;
+  return FF_OK;
+}
+
+ff_status ff_mesh_wait(ff_handle *h) {
+  if (!h) return FF_ERR_BAD_ARG;
+  if (!h->mesh_copy_pending) return FF_OK;
+  CK(cudaSetDevice(h->cfg.device));
+  CK(cudaEventSynchronize(h->ev_mesh_copied));
+  h->mesh_copy_pending = false;
   return FF_OK;
 }
 

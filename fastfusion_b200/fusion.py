@@ -77,6 +77,8 @@ SIGNATURES = {
     "ff_set_shard": (_i32, [_vp, _i32, _i32]),
     "ff_set_spin_limit": (_i32, [_vp, _u32]),
     "ff_set_cell_generation": (_i32, [_vp, _i32]),
+    "ff_get_mesh_async": (_i32, [_vp, _vp, _vp, _vp]),
+    "ff_mesh_wait": (_i32, [_vp]),
     "ff_set_update_batch": (_i32, [_vp, _i32]),
     "ff_halo_export": (_i32, [_vp, _vp, _u64, ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
     "ff_halo_import": (_i32, [_vp, _vp, _u64]),
@@ -280,6 +282,11 @@ class MeshBuffer:
         self._ptr[key] = p.value
         self._cap[key] = nbytes
 
+    def needs(self, n_vertices: int, n_faces: int) -> bool:
+        """Whether a mesh of this size makes the buffer grow (and replace its memory)."""
+        return 12 * n_vertices > self._cap["xyz"] or 3 * n_vertices > self._cap["rgb"] or \
+            12 * n_faces > self._cap["faces"]
+
     def reserve(self, n_vertices: int, n_faces: int):
         self._grow("xyz", 12 * n_vertices)
         self._grow("rgb", 3 * n_vertices)
@@ -401,15 +408,25 @@ class FusionMipMapCPU:
             self._check(st)
         return bool(self._u.value)
 
-    def getMeshInterleavedMarchingCubes(self, out: MeshBuffer | None = None) -> MeshInterleaved:
+    def getMeshInterleavedMarchingCubes(self, out: MeshBuffer | None = None, wait: bool = True) -> MeshInterleaved:
         """The mesh of the last updateMeshes as a host copy (the reference
         returns its mesh by value).  With `out`, the copy lands in that
-        reusable page-locked buffer and the returned arrays are views of it."""
+        reusable page-locked buffer and the returned arrays are views of it;
+        with wait=False as well, the copy runs behind the map's device work
+        and the call returns at once: the arrays hold the mesh after
+        mesh_wait() (ff_get_mesh_async), and meanwhile the next frames can be
+        issued."""
         nv, nf = ctypes.c_uint64(), ctypes.c_uint64()
         self._check(self._L.ff_get_mesh_counts(self._h, ctypes.byref(nv), ctypes.byref(nf)))
         if out is not None:
+            if out.needs(nv.value, nf.value):
+                self.mesh_wait()  # (a copy into the buffer about to be replaced)
             out.reserve(nv.value, nf.value)
-            self._check(self._L.ff_get_mesh(self._h, *out.pointers()))
+            if wait:
+                self.mesh_wait()
+                self._check(self._L.ff_get_mesh(self._h, *out.pointers()))
+            else:
+                self._check(self._L.ff_get_mesh_async(self._h, *out.pointers()))
             return MeshInterleaved(out.view("xyz", np.float32, (nv.value, 3)), out.view("rgb", np.uint8, (nv.value, 3)),
                                    out.view("faces", np.uint32, (nf.value, 3)))
         xyz = np.zeros((nv.value, 3), np.float32)
@@ -417,6 +434,10 @@ class FusionMipMapCPU:
         faces = np.zeros((nf.value, 3), np.uint32)
         self._check(self._L.ff_get_mesh(self._h, _p(xyz), _p(rgb), _p(faces)))
         return MeshInterleaved(xyz, rgb, faces)
+
+    def mesh_wait(self):
+        """Wait for the copy of the last getMeshInterleavedMarchingCubes(wait=False)."""
+        self._check(self._L.ff_mesh_wait(self._h))
 
     def mesh_cells(self):
         """(cells int32[n,14], ranges int64[n,4]) of the last updateMeshes."""

@@ -317,6 +317,20 @@ ff_status ff_get_mesh_counts(ff_handle *h, uint64_t *n_vertices, uint64_t *n_fac
  * getMeshInterleavedMarchingCubes() (geometryfusion_mipmap_cpu.cpp:3359-3374). */
 ff_status ff_get_mesh(ff_handle *h, float *xyz, uint8_t *rgb, uint32_t *faces);
 
+/* ff_get_mesh without waiting: the copies are queued on a copy stream of the
+ * map behind the last update's device work and the call returns at once, so
+ * the copy overlaps what the caller issues next (the next frames).  The
+ * buffers (page-locked memory, ff_alloc_host, lets the copy run without the
+ * host) hold the mesh when ff_mesh_wait returns; they must stay allocated
+ * until then.  A later ff_update_meshes orders its writes after the copy on
+ * the device, without blocking the host.  No counterpart in the reference
+ * (its mesh is returned by value). */
+ff_status ff_get_mesh_async(ff_handle *h, float *xyz, uint8_t *rgb, uint32_t *faces);
+
+/* Wait for the copies of the last ff_get_mesh_async (returns at once if there
+ * are none). */
+ff_status ff_mesh_wait(ff_handle *h);
+
 /* Page-locked host memory for ff_get_mesh / ff_add_map_u16 buffers: copies
  * to and from it run at full PCIe/C2C speed.  Not a counterpart of a
  * reference call (the reference has no device). */
