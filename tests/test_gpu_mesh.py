@@ -136,3 +136,32 @@ def test_mesh_matches_reference_binary_cells(lib_built):
                  and np.array_equal(rc, mesh.colors[v0:v0 + nv]) and np.array_equal(rf, mesh.faces[f0:f0 + nf] - v0))
     assert common == len(refmap) == len(cells)
     assert same == common
+
+
+def test_async_mesh_export_overlaps_and_matches(lib_built):
+    """getMeshInterleavedMarchingCubes(wait=False) (ff_get_mesh_async): the
+    copy runs behind the map's work while the next frames -- and the next
+    updateMeshes, which rewrites the device mesh -- are issued; after
+    mesh_wait() the buffer holds exactly the mesh the blocking export gave."""
+    from fastfusion_b200 import fusion as ff
+    K, frames = circle_frames(3, 12, 320, 240)
+    m = ff.FusionMipMapCPU(0, 0, 0, 0.005, 0.01, 0, True, leaves_max=271420, branches_max=4793488, rcp="exact")
+    buf = ff.MeshBuffer()
+    for k0 in (0, 4):
+        for depth, bgr, R, t in frames[k0:k0 + 4]:
+            m.addMap(depth, ff.CameraInfo(K, R, t), bgr, SCALING, MAXCAM)
+        m.updateMeshes()
+        want = m.getMeshInterleavedMarchingCubes()
+        got = m.getMeshInterleavedMarchingCubes(out=buf, wait=False)
+        # more work behind the copy: frames and a mesh update that rewrites
+        # the device buffers the copy reads
+        for depth, bgr, R, t in frames[k0 + 4:k0 + 6]:
+            m.addMap(depth, ff.CameraInfo(K, R, t), bgr, SCALING, MAXCAM)
+        m.updateMeshes()
+        m.mesh_wait()
+        assert len(want.faces) > 0
+        assert np.array_equal(got.vertices.view(np.uint32), want.vertices.view(np.uint32))
+        assert np.array_equal(got.colors, want.colors)
+        assert np.array_equal(got.faces, want.faces)
+    m.close()
+    buf.close()
