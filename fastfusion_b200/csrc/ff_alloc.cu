@@ -731,6 +731,7 @@ void launch_parents_frames(const BatchDesc *d_batch, int nframes, cudaStream_t s
 // the leaf table and the parents.
 constexpr int FIN_THREADS = 1024;
 constexpr size_t FIN_SMEM_MAX = 200 * 1024;
+constexpr int FIN_FEW = 1024;  // new leaves ranked by direct count (the dynamic shared memory holds >= 1024 words)
 
 // One block per map of the batch; the pending count is read on the device
 // (nothing is done after an allocation error, which the host reports).
@@ -774,31 +775,47 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc
   uint32_t *chunk_base = fin_smem + nwords;  // [FIN_THREADS]
   const uint32_t chunk = (nwords + FIN_THREADS - 1) / FIN_THREADS;
   const int t = threadIdx.x;
-  for (uint32_t w = t; w < nwords; w += FIN_THREADS) bitmap[w] = 0;
-  __syncthreads();
-  for (int j = t; j < npend; j += FIN_THREADS) {
-    const uint32_t fp = pend[j].first_pixel;
-    atomicOr(&bitmap[fp >> 5], 1u << (fp & 31));
-  }
-  __syncthreads();
-  // exclusive prefix of the per-thread chunk counts
-  uint32_t mine = 0;
-  const uint32_t w0 = (uint32_t)t * chunk, w1 = min(nwords, w0 + chunk);
-  for (uint32_t w = w0; w < w1; w++) mine += __popc(bitmap[w]);
-  using Scan = cub::BlockScan<uint32_t, FIN_THREADS>;
-  __shared__ typename Scan::TempStorage scan_tmp;
-  uint32_t before = 0;
-  Scan(scan_tmp).ExclusiveSum(mine, before);
-  chunk_base[t] = before;
-  __syncthreads();
-  for (int j = t; j < npend; j += FIN_THREADS) {
-    const PendingLeaf p = pend[j];
-    const uint32_t w = p.first_pixel >> 5, c = w / chunk;
-    uint32_t r = chunk_base[c];
-    for (uint32_t k = c * chunk; k < w; k++) r += __popc(bitmap[k]);
-    r += __popc(bitmap[w] & ((1u << (p.first_pixel & 31)) - 1u));
-    rank[j] = r;
-    finalize_one(p, leaves_before + r, leaves_max, tree, leaf, frame, stamp, queue, cnt);
+  if (npend <= FIN_FEW) {
+    // few new leaves (the usual frame): a leaf's rank counted directly over
+    // the others' first pixels in shared memory, without the image bitmap
+    uint32_t *fp = fin_smem;
+    for (int j = t; j < npend; j += FIN_THREADS) fp[j] = pend[j].first_pixel;
+    __syncthreads();
+    for (int j = t; j < npend; j += FIN_THREADS) {
+      const uint32_t mine_fp = fp[j];
+      uint32_t r = 0;
+      for (int i = 0; i < npend; i++) r += fp[i] < mine_fp ? 1u : 0u;
+      rank[j] = r;
+      finalize_one(pend[j], leaves_before + r, leaves_max, tree, leaf, frame, stamp, queue, cnt);
+    }
+  } else {
+    for (uint32_t w = t; w < nwords; w += FIN_THREADS) bitmap[w] = 0;
+    __syncthreads();
+    for (int j = t; j < npend; j += FIN_THREADS) {
+      const uint32_t fp = pend[j].first_pixel;
+      atomicOr(&bitmap[fp >> 5], 1u << (fp & 31));
+    }
+    __syncthreads();
+    // the image bitmap of first pixels; exclusive prefix of the per-thread
+    // chunk counts
+    uint32_t mine = 0;
+    const uint32_t w0 = (uint32_t)t * chunk, w1 = min(nwords, w0 + chunk);
+    for (uint32_t w = w0; w < w1; w++) mine += __popc(bitmap[w]);
+    using Scan = cub::BlockScan<uint32_t, FIN_THREADS>;
+    __shared__ typename Scan::TempStorage scan_tmp;
+    uint32_t before = 0;
+    Scan(scan_tmp).ExclusiveSum(mine, before);
+    chunk_base[t] = before;
+    __syncthreads();
+    for (int j = t; j < npend; j += FIN_THREADS) {
+      const PendingLeaf p = pend[j];
+      const uint32_t w = p.first_pixel >> 5, c = w / chunk;
+      uint32_t r = chunk_base[c];
+      for (uint32_t k = c * chunk; k < w; k++) r += __popc(bitmap[k]);
+      r += __popc(bitmap[w] & ((1u << (p.first_pixel & 31)) - 1u));
+      rank[j] = r;
+      finalize_one(p, leaves_before + r, leaves_max, tree, leaf, frame, stamp, queue, cnt);
+    }
   }
   // (the new leaves' parents: k_parents_frames, after this kernel)
   __syncthreads();
