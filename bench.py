@@ -13,9 +13,11 @@ is.
 
 Reported (one JSON line from rank 0):
   value      frames/s over all ranks, depth/BGR already in HBM (ff_add_map_u16_device)
-  e2e        the same through the host API (ff_add_map_u16 from page-locked
-             host frames, ff_update_meshes, and the whole mesh copied back to the
-             host every step); e2e_pageable: the same from pageable host frames
+  e2e        the same through the host API: ff_add_map_sequence_u16 (the
+             reference's several-frames addMap) from page-locked host frames,
+             ff_update_meshes, and the whole mesh copied back to the host every
+             step; e2e_pageable: the same from pageable host frames;
+             e2e_single_frame_calls: one ff_add_map_u16 per frame
   roofline   the dominant stage's algorithmic bytes / CUDA-event time vs the
              measured HBM copy bandwidth; roofline_fuse: the same for the
              voxel-update kernel
@@ -441,7 +443,7 @@ def run_b200(a):
     del m
 
     # 3. end to end through the host API: host frames in, whole mesh out, every step
-    e2e = e2e_pageable = None
+    e2e = e2e_pageable = e2e_single = None
     rms = None
     if not a.no_e2e:
         last_mesh = {}
@@ -449,12 +451,18 @@ def run_b200(a):
         # viewer would size it for its scene (it grows if the mesh outgrows it)
         mesh_buf = ff.MeshBuffer(4 << 20, 6 << 20)
 
-        def host_run(hd, hb):
+        def host_run(hd, hb, per_frame=False):
             d2h = []
 
             def host_step(mm, s):
-                for k in range(s * FRAMES_PER_STEP, (s + 1) * FRAMES_PER_STEP):
-                    mm.addMap(hd[k], cams[k], hb[k], SCALING, MAXCAM)
+                ks = range(s * FRAMES_PER_STEP, (s + 1) * FRAMES_PER_STEP)
+                if per_frame:
+                    for k in ks:
+                        mm.addMap(hd[k], cams[k], hb[k], SCALING, MAXCAM)
+                else:
+                    # the reference's several-frames addMap (host images)
+                    mm.addMapSequence([hd[k] for k in ks], [cams[k] for k in ks], [hb[k] for k in ks], SCALING,
+                                      MAXCAM)
                 mm.updateMeshes()
                 # the whole mesh to the host, the copy overlapping the next
                 # step's frames (ff_get_mesh_async; every copy has finished
@@ -493,8 +501,10 @@ def run_b200(a):
                     "h2d_bytes_per_step": FRAMES_PER_STEP * (WIDTH * HEIGHT * 2 + WIDTH * HEIGHT * 3),
                     "d2h_bytes_per_step": int(np.mean(d2h)) if d2h else 0, "ms_per_step": ms / span_steps,
                     "steps": span_steps, "gpu_launches_per_step": round((own1 - own0) / span_steps, 1),
-                    "span": f"steps {a.warmup}..{total - 1} of the walk back to back (every step: 10 addMap from "
-                            "host frames, updateMeshes, the whole mesh copied to page-locked host memory on a "
+                    "api": "ff_add_map_u16 per frame" if per_frame else
+                           "ff_add_map_sequence_u16 (the step's 10 host frames per call)",
+                    "span": f"steps {a.warmup}..{total - 1} of the walk back to back (every step: 10 frames from "
+                            "host memory, updateMeshes, the whole mesh copied to page-locked host memory on a "
                             "second stream); CUDA events around the span, the closing one after the last copy"}
 
         # page-locked host frames (ff_alloc_host-style pinned memory)
@@ -503,6 +513,9 @@ def run_b200(a):
         h_bgr = bgr.cpu().pin_memory()
         e2e = host_run(h_depth.numpy().view(np.uint16), h_bgr.numpy())
         e2e["host_frames"] = "page-locked"
+        log("end to end, page-locked host frames, one call per frame")
+        e2e_single = host_run(h_depth.numpy().view(np.uint16), h_bgr.numpy(), per_frame=True)
+        e2e_single["host_frames"] = "page-locked"
         if rank == 0 and "m" in last_mesh and len(last_mesh["m"].vertices):
             v = last_mesh["m"].vertices
             rng = np.random.default_rng(0)
@@ -562,9 +575,12 @@ def run_b200(a):
                     "the reference documents are not available offline)",
             "config": dict(workload_config(a, nf), parallelism=f"independent maps x{world}"),
             "api": "value: ff_add_map_sequence_u16_device (a step's 10 frames per call); "
-                   "value_single_frame_calls: ff_add_map_u16_device per frame; e2e: ff_add_map_u16 per frame",
+                   "value_single_frame_calls: ff_add_map_u16_device per frame; e2e: ff_add_map_sequence_u16 (the "
+                   "reference's several-frames addMap, host images); e2e_single_frame_calls: ff_add_map_u16 per "
+                   "frame",
             "value_single_frame_calls": round(value_single, 2),
-            "e2e": e2e, "e2e_pageable": e2e_pageable, "roofline": roofline, "roofline_fuse": roofline_fuse,
+            "e2e": e2e, "e2e_pageable": e2e_pageable, "e2e_single_frame_calls": e2e_single,
+            "roofline": roofline, "roofline_fuse": roofline_fuse,
             "cpu_baseline": cpu, "gpu_launches": gpu_launches,
             "library_calls": lib_calls, "clocks": clocks, "stages": stage_rec,
             "stage_profile": f"CUDA events per stage over steps {a.warmup}-{total - 1} of a separate run "

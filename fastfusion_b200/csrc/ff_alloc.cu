@@ -496,6 +496,7 @@ __device__ __forceinline__ uint32_t insert_descend(const MapFrame &F, int i, int
         atomicExch(tree + ptr, nb);
         child = nb;
         *created = true;
+        if (probed <= (uint32_t)MESH_TOP_LEVELS) atomicOr(&cnt->top_created, 1u);
       } else {
         child = old;
       }
@@ -534,6 +535,7 @@ __device__ __forceinline__ uint32_t insert_descend(const MapFrame &F, int i, int
       __threadfence();
       atomicExch(tree + ptr, PENDING + rec);
       *created = true;
+      if (probed <= (uint32_t)MESH_TOP_LEVELS) atomicOr(&cnt->top_created, 1u);
       return probed;
     }
     cur = old;

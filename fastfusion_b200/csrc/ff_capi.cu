@@ -42,6 +42,13 @@ struct ff_handle {
   cudaStream_t mesh_stream = nullptr;
   cudaEvent_t ev_mesh_ready = nullptr, ev_mesh_copied = nullptr;
   bool mesh_copy_pending = false;
+  // ff_add_map_sequence_u16: the frames' images staged on the device (up to
+  // BATCH_MAX frames), and the colour copies the next update pass waits for
+  uint16_t *d_hseq_depth = nullptr;
+  uint8_t *d_hseq_bgr = nullptr;
+  size_t hseq_frames = 0, hseq_pix = 0;
+  cudaEvent_t ev_host_images = nullptr;
+  bool host_images_pending = false;
   cudaEvent_t ev_bgr_free = nullptr, ev_bgr_ready = nullptr;
   // recorded once a frame's counters have reached the host: a single-map
   // frame returns then, while its voxel update still runs
@@ -132,6 +139,7 @@ struct ff_handle {
   // (ff_inject_error)
   uint32_t spin_limit = SPIN_LIMIT;
   int full_cells = 0;  // 1: regenerate every mesh cell at every update (ff_set_cell_generation)
+  bool top_changed = true;  // a frame since the last mesh update created a branch or leaf near the root
   int inject = 0;
   // loop closure (ff_loop_begin): the loop arrays, each leaf's slot in them,
   // per queue entry its slot, [slots in use, entries taken]
@@ -273,6 +281,11 @@ static ff_status flush_updates(ff_handle *h) {
   fb.nslots = h->upd_pending;
   for (int j = 0; j < h->upd_pending; j++) fb.s[j] = h->upd_slot[j];
   cudaStream_t fs = h->fuse_stream;
+  if (h->host_images_pending) {
+    // the colour images of a host-image sequence, copied on the copy stream
+    CK(cudaStreamWaitEvent(fs, h->ev_host_images, 0));
+    h->host_images_pending = false;
+  }
   const int pi = h->prof.begin(ST_FUSE, fs);
   launch_fuse_multi(fb, h->cfg.storage, h->d_rcp_tab != nullptr, h->sm_count * 2, fs);
   // every queued brick of every frame read and written once per frame in
@@ -586,7 +599,8 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
         cudaEventCreateWithFlags(&h->ev_counters, cudaEventDisableTiming) != cudaSuccess ||
         cudaStreamCreateWithFlags(&h->mesh_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_mesh_ready, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h->ev_mesh_copied, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&h->ev_mesh_copied, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_host_images, cudaEventDisableTiming) != cudaSuccess) {
       fail(FF_ERR_CUDA, "copy stream");
       break;
     }
@@ -736,6 +750,9 @@ ff_status ff_destroy(ff_handle *h) {
   if (h->mesh_stream) cudaStreamDestroy(h->mesh_stream);
   if (h->ev_mesh_ready) cudaEventDestroy(h->ev_mesh_ready);
   if (h->ev_mesh_copied) cudaEventDestroy(h->ev_mesh_copied);
+  if (h->ev_host_images) cudaEventDestroy(h->ev_host_images);
+  if (h->d_hseq_depth) cudaFree(h->d_hseq_depth);
+  if (h->d_hseq_bgr) cudaFree(h->d_hseq_bgr);
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   delete h;
   return FF_OK;
@@ -1341,6 +1358,7 @@ static ff_status frame_finish(ff_handle *h, const FramePlan &plan, MapFrame &mf,
                               int32_t *queued) {
   cudaStream_t s = h->stream;
   const Counters &hc = *h->h_cnt;
+  if (hc.top_created) h->top_changed = true;
   if (hc.error & ERR_DEDUPE_FAILED) {
     // the insert, the finalisation and the update left the frame out: the
     // map is as it was before the call
@@ -1770,6 +1788,70 @@ ff_status ff_add_map_sequence_u16_device(ff_handle *h, int n, const uint16_t *co
   return st;
 }
 
+ff_status ff_add_map_sequence_u16(ff_handle *h, int n, const uint16_t *const *depth, const uint8_t *const *bgr,
+                                  int width, int height, size_t depth_pitch, size_t bgr_pitch, const double *K,
+                                  const double *R, const double *t, float scaling, float maxcam,
+                                  int32_t *queued) {
+  if (!h) return FF_ERR_BAD_ARG;
+  if (n < 1 || !depth || !bgr || !K || !R || !t || width <= 0 || height <= 0)
+    return set_err(h, FF_ERR_BAD_ARG, "ff_add_map_sequence_u16: bad argument");
+  for (int k = 0; k < n; k++)
+    if (!depth[k] || !bgr[k]) return set_err(h, FF_ERR_BAD_ARG, "ff_add_map_sequence_u16: NULL image");
+  CK(cudaSetDevice(h->cfg.device));
+  if (!deferrable(h, width, height) || n == 1) {
+    for (int k = 0; k < n; k++)
+      FCK(ff_add_map_u16(h, depth[k], width, height, depth_pitch, bgr[k], bgr_pitch, K + 4 * k, R + 9 * k,
+                         t + 3 * k, scaling, maxcam, queued ? queued + k : nullptr));
+    return FF_OK;
+  }
+  if (!depth_pitch) depth_pitch = sizeof(uint16_t) * width;
+  if (!bgr_pitch) bgr_pitch = 3 * (size_t)width;
+  const size_t npix = (size_t)width * height;
+  const size_t frames = (size_t)std::min(n, BATCH_MAX);
+  if (frames > h->hseq_frames || npix > h->hseq_pix) {
+    cudaFree(h->d_hseq_depth);
+    cudaFree(h->d_hseq_bgr);
+    h->d_hseq_depth = nullptr;
+    h->d_hseq_bgr = nullptr;
+    h->hseq_frames = h->hseq_pix = 0;
+    CK(alloc(&h->d_hseq_depth, frames * npix));
+    CK(alloc(&h->d_hseq_bgr, frames * npix * 3));
+    h->hseq_frames = frames;
+    h->hseq_pix = npix;
+  }
+  std::vector<const uint16_t *> dd(frames);
+  std::vector<const uint8_t *> db(frames);
+  ff_status st = FF_OK;
+  for (int i = 0; i < n && st == FF_OK;) {
+    const int c = std::min(n - i, (int)frames);
+    // depth first, on the map's stream (the de-duplication reads it); the
+    // colour on the copy stream, overlapping the allocation (the update pass
+    // waits for it).  The staging is free: the previous group's call returned
+    // after its update pass.
+    for (int k = 0; k < c; k++) {
+      uint16_t *d = h->d_hseq_depth + (size_t)k * npix;
+      CK(cudaMemcpy2DAsync(d, sizeof(uint16_t) * width, depth[i + k], depth_pitch, sizeof(uint16_t) * width, height,
+                           cudaMemcpyHostToDevice, h->stream));
+      dd[k] = d;
+    }
+    for (int k = 0; k < c; k++) {
+      uint8_t *b = h->d_hseq_bgr + (size_t)k * npix * 3;
+      CK(cudaMemcpy2DAsync(b, 3 * (size_t)width, bgr[i + k], bgr_pitch, 3 * (size_t)width, height,
+                           cudaMemcpyHostToDevice, h->copy_stream));
+      db[k] = b;
+    }
+    CK(cudaEventRecord(h->ev_host_images, h->copy_stream));
+    h->host_images_pending = true;
+    st = ff_add_map_sequence_u16_device(h, c, dd.data(), db.data(), width, height, K + 4 * i, R + 9 * i, t + 3 * i,
+                                        scaling, maxcam, queued ? queued + i : nullptr);
+    i += c;
+  }
+  // the caller's images are not read after the call returns, error paths included
+  cudaStreamSynchronize(h->copy_stream);
+  h->host_images_pending = false;
+  return st;
+}
+
 ff_status ff_add_maps_u16_device(ff_handle *const *maps, int n, const uint16_t *const *d_depth,
                                  const uint8_t *const *d_bgr, const int *width, const int *height, const double *K,
                                  const double *R, const double *t, const float *scaling, const float *maxcam,
@@ -2105,6 +2187,7 @@ ff_status ff_update_meshes(ff_handle *h, int *updated) {
   in.bstamp = h->d_bstamp;
   in.grows = h->grows;
   in.full_cells = h->full_cells;
+  in.top_changed = h->top_changed;
   in.frame = h->frames;
   in.n = h->n;
   for (int r = 0; r < 3; r++) in.offset[r] = h->offset[r];
@@ -2118,6 +2201,7 @@ ff_status ff_update_meshes(ff_handle *h, int *updated) {
   std::string err;
   int rc = mesh_update(h->mesh, in, h->stream, err);
   if (rc != 0) return set_err(h, (ff_status)rc, err);
+  h->top_changed = false;
   if (updated) *updated = 1;
   return FF_OK;
 }

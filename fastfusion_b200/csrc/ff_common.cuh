@@ -76,8 +76,14 @@ struct Counters {
   uint32_t cnn_error;  // the confidence network's bounded waits (kept by the frame's counter set-up)
   uint32_t levels;     // octree levels the insert probed, summed over the processed pixels
   uint32_t leaves_base;  // a sequence's later frame: leaves before it (set by the previous frame's finalisation)
-  uint32_t pad;
+  uint32_t top_created;  // a branch or leaf was created in a slot within MESH_TOP_LEVELS of the root
 };
+
+// The mesher keeps the items of its octree traversal's level MESH_TOP_LEVELS
+// from one update to the next; a frame that creates a branch or a leaf in a
+// slot that close to the root (depth <= MESH_TOP_LEVELS) makes it build them
+// again.
+constexpr int MESH_TOP_LEVELS = 4;
 
 // Float camera parameters (the reference's camPamsFloat, definitions.h:71-88).
 struct CamF {

@@ -143,6 +143,9 @@ struct GenCtx {
   const uint32_t *bstamp;
   uint32_t since, prev_leaves, prev_branches;
   int incr;
+  // incremental, while the top levels are traversed again to refill their
+  // cache: every item is expanded, but only changed items emit cells
+  int expand_all;
 };
 
 // the octree is read-only while the mesh is built: reads go through the
@@ -293,7 +296,8 @@ __device__ __forceinline__ void put_edge(const GenQueues &Q, const Out &O, uint3
 // dropped without expanding it (the meshed cells are the same).
 __device__ __forceinline__ bool dead_slot(const Slot &s, bool sub) { return !sub && s.la >= BRANCHINIT; }
 
-__device__ __forceinline__ void vert_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot (&S8)[8]) {
+__device__ __forceinline__ void vert_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot (&S8)[8],
+                                          bool emit) {
   bool any = false, dead = false;
 #pragma unroll
   for (int j = 0; j < 8; j++) {
@@ -309,6 +313,7 @@ __device__ __forceinline__ void vert_item(const GenCtx &g, const GenQueues &Q, c
     push_vert(Q, O, C);
     return;
   }
+  if (!emit) return;
   // the vertex is a corner of the smallest slot around it
   int size = S8[0].size, small = 0;
 #pragma unroll
@@ -328,7 +333,8 @@ __device__ __forceinline__ void vert_item(const GenCtx &g, const GenQueues &Q, c
 }
 
 template <int E>
-__device__ __forceinline__ void edge_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot (&S4)[4]) {
+__device__ __forceinline__ void edge_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot (&S4)[4],
+                                          bool emit) {
   constexpr int P = E == 0 ? 1 : 0, Qx = E == 2 ? 1 : 2;  // the two axes across the edge line
   bool any = false, dead = false;
 #pragma unroll
@@ -339,6 +345,7 @@ __device__ __forceinline__ void edge_item(const GenCtx &g, const GenQueues &Q, c
   }
   if (dead) return;
   if (!any) {
+    if (!emit) return;
     // the edge line runs along a side of the smallest slot
     int size = S4[0].size, small = 0;
 #pragma unroll
@@ -381,10 +388,11 @@ __device__ __forceinline__ void edge_item(const GenCtx &g, const GenQueues &Q, c
 
 template <int AX>
 __device__ __forceinline__ void face_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot &A,
-                                          const Slot &B) {
+                                          const Slot &B, bool emit) {
   const bool sa = is_sub(g, A), sb = is_sub(g, B);
   if (dead_slot(A, sa) || dead_slot(B, sb)) return;
   if (!sa && !sb) {
+    if (!emit) return;
     const int size = min((int)A.size, (int)B.size);
     const bool a_small = A.size <= B.size;
     int o[3] = {a_small ? A.o[0] : B.o[0], a_small ? A.o[1] : B.o[1], a_small ? A.o[2] : B.o[2]};
@@ -503,38 +511,90 @@ __device__ __forceinline__ void gen_level(const GenCtx &g, const GenQueues &Q, i
         }
       } else {
         const Slot s = Q.cellq[cur][i];
-        if (!slot_changed(g, s)) continue;
+        if (!g.expand_all && !slot_changed(g, s)) continue;
         for (int co = 0; co < 8; co++) C[co] = child_of(g, s, co);
       }
       cell_item(g, Q, O, C);
     } else if (i < nc + nf) {
       const FaceItem f = Q.faceq[cur][i - nc];
-      if (!slot_changed(g, f.a) && !slot_changed(g, f.b)) continue;
-      if (f.axis == 0) face_item<0>(g, Q, O, f.a, f.b);
-      else if (f.axis == 1) face_item<1>(g, Q, O, f.a, f.b);
-      else face_item<2>(g, Q, O, f.a, f.b);
+      const bool changed = slot_changed(g, f.a) || slot_changed(g, f.b);
+      if (!changed && !g.expand_all) continue;
+      if (f.axis == 0) face_item<0>(g, Q, O, f.a, f.b, changed);
+      else if (f.axis == 1) face_item<1>(g, Q, O, f.a, f.b, changed);
+      else face_item<2>(g, Q, O, f.a, f.b, changed);
     } else if (i < nc + nf + ne) {
       const EdgeItem e = Q.edgeq[cur][i - nc - nf];
       bool changed = false;
 #pragma unroll
       for (int j = 0; j < 4; j++) changed |= slot_changed(g, e.s[j]);
-      if (!changed) continue;
-      if (e.axis == 0) edge_item<0>(g, Q, O, e.s);
-      else if (e.axis == 1) edge_item<1>(g, Q, O, e.s);
-      else edge_item<2>(g, Q, O, e.s);
+      if (!changed && !g.expand_all) continue;
+      if (e.axis == 0) edge_item<0>(g, Q, O, e.s, changed);
+      else if (e.axis == 1) edge_item<1>(g, Q, O, e.s, changed);
+      else edge_item<2>(g, Q, O, e.s, changed);
     } else {
       const VertItem v = Q.vertq[cur][i - nc - nf - ne];
       bool changed = false;
 #pragma unroll
       for (int j = 0; j < 8; j++) changed |= slot_changed(g, v.s[j]);
-      if (!changed) continue;
-      vert_item(g, Q, O, v.s);
+      if (!changed && !g.expand_all) continue;
+      vert_item(g, Q, O, v.s, changed);
     }
   }
 }
 
 __global__ void __launch_bounds__(128, 6) k_gen_level(GenCtx g, GenQueues Q, int lv, uint32_t n) {
   gen_level(g, Q, lv, n);
+}
+
+// The items of traversal level MESH_TOP_LEVELS, kept from one update to the
+// next: the levels above it hold few items, each a long chain of dependent
+// queue claims, and they produce the same items until a frame creates a
+// branch or a leaf that close to the root.
+struct TopCache {
+  Slot *cellq;
+  FaceItem *faceq;
+  EdgeItem *edgeq;
+  VertItem *vertq;
+  uint32_t cap[4];
+  uint32_t *count;  // cell, face, edge, vertex items; [4]: 1 if they did not fit
+};
+
+__global__ void k_save_top(GenQueues Q, int lv, TopCache T) {
+  const uint32_t *c = Q.lvl + 4 * lv;
+  const int b = lv & 1;
+  const uint32_t n0 = c[0], n1 = c[1], n2 = c[2], n3 = c[3];
+  const bool fits = n0 <= T.cap[0] && n1 <= T.cap[1] && n2 <= T.cap[2] && n3 <= T.cap[3] && n0 <= Q.cap_cell &&
+                    n1 <= Q.cap_face && n2 <= Q.cap_edge && n3 <= Q.cap_vert;
+  const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  if (t0 == 0) {
+    T.count[0] = n0;
+    T.count[1] = n1;
+    T.count[2] = n2;
+    T.count[3] = n3;
+    T.count[4] = fits ? 0u : 1u;
+  }
+  if (!fits) return;
+  for (uint32_t i = t0; i < n0; i += stride) T.cellq[i] = Q.cellq[b][i];
+  for (uint32_t i = t0; i < n1; i += stride) T.faceq[i] = Q.faceq[b][i];
+  for (uint32_t i = t0; i < n2; i += stride) T.edgeq[i] = Q.edgeq[b][i];
+  for (uint32_t i = t0; i < n3; i += stride) T.vertq[i] = Q.vertq[b][i];
+}
+
+__global__ void k_load_top(GenQueues Q, int lv, TopCache T) {
+  const int b = lv & 1;
+  const uint32_t n0 = T.count[0], n1 = T.count[1], n2 = T.count[2], n3 = T.count[3];
+  const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  if (t0 == 0) {
+    uint32_t *c = Q.lvl + 4 * lv;
+    c[0] = n0;
+    c[1] = n1;
+    c[2] = n2;
+    c[3] = n3;
+  }
+  for (uint32_t i = t0; i < n0; i += stride) Q.cellq[b][i] = T.cellq[i];
+  for (uint32_t i = t0; i < n1; i += stride) Q.faceq[b][i] = T.faceq[i];
+  for (uint32_t i = t0; i < n2; i += stride) Q.edgeq[b][i] = T.edgeq[i];
+  for (uint32_t i = t0; i < n3; i += stride) Q.vertq[b][i] = T.vertq[i];
 }
 
 // Sort key of a cell: (type, log2 size, origin x, y, z), the order of the
@@ -1761,6 +1821,16 @@ struct MeshImpl {
   size_t cap_mkeys = 0;
   uint32_t n_new = 0, n_kept = 0;
   bool redo_full = false;  // the last incremental list was inconsistent: regenerate every cell
+  // the traversal's level-MESH_TOP_LEVELS items (TopCache), their count and
+  // fit flag (device, pinned mirror), and whether they are current
+  Slot *top_cellq = nullptr;
+  FaceItem *top_faceq = nullptr;
+  EdgeItem *top_edgeq = nullptr;
+  VertItem *top_vertq = nullptr;
+  size_t cap_top[4] = {0, 0, 0, 0};
+  uint32_t *d_top_count = nullptr, *h_top_count = nullptr;
+  bool top_valid = false;
+  uint32_t gen_start_level = 0;  // the last update's first traversed level (statistics)
 };
 
 static MeshImpl &impl(MeshState &m) {
@@ -1845,6 +1915,7 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
     g.prev_leaves = I.prev_leaves;
     g.prev_branches = I.prev_branches;
     g.incr = incr ? 1 : 0;
+    g.expand_all = 0;
     if (incr) {
       // the previous cells whose sides did not change, and their positions
       // among the kept (words KEPT_WORD, KEPT_WORD + 1: kept, kept before the
@@ -1855,11 +1926,36 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
       k_keep_apply<<<keep_tiles, KEEP_THREADS, 0, s>>>(I.keep, n_old, I.keep_tiles, keep_tiles, first_corner_old,
                                                        I.d_count + KEPT_WORD);
     }
+    // The top levels: an incremental update whose frames created nothing
+    // near the root starts from the kept level-MESH_TOP_LEVELS items;
+    // otherwise the top levels run (in an incremental update expanding every
+    // item, so that the whole level is there to keep, but emitting only the
+    // changed items' cells) and their output is kept for the next updates.
+    constexpr int LC = MESH_TOP_LEVELS;
+    if (!I.d_top_count) {
+      MCK(pool_alloc((void **)&I.d_top_count, 5 * sizeof(uint32_t), s));
+      MCK(cudaMallocHost((void **)&I.h_top_count, 5 * sizeof(uint32_t)));
+      I.h_top_count[4] = 1;
+    }
+    TopCache T;
+    T.cellq = I.top_cellq;
+    T.faceq = I.top_faceq;
+    T.edgeq = I.top_edgeq;
+    T.vertq = I.top_vertq;
+    for (int k = 0; k < 4; k++) T.cap[k] = (uint32_t)I.cap_top[k];
+    T.count = I.d_top_count;
+    const bool use_top = incr && I.top_valid && !in.top_changed;
+    const int lv0 = use_top ? LC : 0;
+    I.gen_start_level = (uint32_t)lv0;
+    if (use_top) {
+      note_launch(1);
+      k_load_top<<<148 * 2, 256, 0, s>>>(Q, LC, T);
+    }
     // a chain cell -> face -> edge -> vertex adds up to three levels below
     // the octree's depth; more levels run if items are left
     int depth = 1;
     for (uint32_t h = in.n; h > 8; h >>= 1) depth++;
-    int lv = 0, batch = depth + 4;
+    int lv = lv0, batch = std::max(depth + 4 - lv0, 4);
     bool leftover = true;
     while (leftover && lv < MAX_GEN_LEVELS) {
       const int end = std::min(lv + batch, MAX_GEN_LEVELS);
@@ -1871,10 +1967,18 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
         uint64_t bound = 1;
         for (int k = 0; k < lv && bound < (uint64_t)148 * 8 * 128; k++) bound *= 27;
         const int blocks = (int)std::min<uint64_t>(148 * 8, (bound + 127) / 128);
+        g.expand_all = (incr && lv < LC) ? 1 : 0;
         k_gen_level<<<blocks, 128, 0, s>>>(g, Q, lv, in.n);
+        if (!use_top && lv == LC - 1) {
+          // level LC's items are complete now: keep them
+          note_launch(1);
+          k_save_top<<<148 * 2, 256, 0, s>>>(Q, LC, T);
+        }
       }
       MCK(cudaGetLastError());
       MCK(cudaMemcpyAsync(I.h_count, I.d_count, COUNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      if (!use_top)
+        MCK(cudaMemcpyAsync(I.h_top_count, I.d_top_count, 5 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
       MCK(cudaStreamSynchronize(s));
       const uint32_t *cl = I.h_count + LEVEL_COUNTS + 4 * lv;
       leftover = cl[0] || cl[1] || cl[2] || cl[3];
@@ -1883,6 +1987,18 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
     }
     const bool overflow = (I.h_count[9] & ERR_CELL_OVERFLOW) != 0;
     const uint32_t *hc = I.h_count;
+    if (!use_top) {
+      // kept if it fitted; else the cache grows to the level's size and is
+      // filled by the next update that traverses the top levels
+      I.top_valid = !overflow && I.h_top_count[4] == 0 && lv > LC;
+      if (!I.top_valid && !overflow) {
+        const uint32_t *cl = hc + LEVEL_COUNTS + 4 * LC;
+        MCK(grow_buf(I.top_cellq, I.cap_top[0], (size_t)cl[0] + cl[0] / 4 + 256, s));
+        MCK(grow_buf(I.top_faceq, I.cap_top[1], (size_t)cl[1] + cl[1] / 4 + 256, s));
+        MCK(grow_buf(I.top_edgeq, I.cap_top[2], (size_t)cl[2] + cl[2] / 4 + 256, s));
+        MCK(grow_buf(I.top_vertq, I.cap_top[3], (size_t)cl[3] + cl[3] / 4 + 256, s));
+      }
+    }
     if (overflow) {
       for (int k = 0; k < 5; k++) want[k] *= 2;
       continue;
@@ -2278,10 +2394,12 @@ void mesh_free(MeshState &M) {
                     I.vertq[1], I.d_count, I.raw, I.cells, I.old_cells, I.keys, I.keys_sorted, I.old_keys,
                     I.vals, I.vals_sorted, I.sort_tmp, I.out, I.old_out, I.nv, I.nf, I.vbase, I.fbase,
                     I.old_vbase, I.old_fbase, I.dirty, I.old_index, I.scan_tmp, I.old_xyz, I.old_rgb,
-                    I.old_faces, I.dlist, I.cases, I.keep, I.keep_tiles, I.mkeys};
+                    I.old_faces, I.dlist, I.cases, I.keep, I.keep_tiles, I.mkeys, I.top_cellq, I.top_faceq,
+                    I.top_edgeq, I.top_vertq, I.d_top_count};
     for (void *p : ptrs)
       if (p) cudaFreeAsync(p, 0);
     if (I.h_count) cudaFreeHost(I.h_count);
+    if (I.h_top_count) cudaFreeHost(I.h_top_count);
     delete &I;
     M.impl = nullptr;
   }
@@ -2296,7 +2414,10 @@ void mesh_free(MeshState &M) {
 
 void mesh_invalidate(MeshState &M) {
   M.valid = false;
-  if (M.impl) impl(M).n_old = 0;
+  if (M.impl) {
+    impl(M).n_old = 0;
+    impl(M).top_valid = false;
+  }
 }
 
 void mesh_note_frame(MeshState &) {}

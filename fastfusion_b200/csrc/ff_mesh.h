@@ -27,6 +27,7 @@ struct MeshInputs {
   const uint32_t *bstamp;
   uint32_t grows = 0;   // volume growths so far (a growth moves every cell)
   int full_cells = 0;   // regenerate every cell instead of the changed ones
+  bool top_changed = true;  // a frame since the last update created something near the root
   uint32_t frame;
   uint32_t n;
   float offset[3];

@@ -91,6 +91,7 @@ SIGNATURES = {
     "ff_add_map_u16_device": (_i32, [_vp, _vp, _vp, _i32, _i32, _vp, _vp, _vp, _f32, _f32, _vp]),
     "ff_add_maps_u16_device": (_i32, [_vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ff_add_map_sequence_u16_device": (_i32, [_vp, _i32, _vp, _vp, _i32, _i32, _vp, _vp, _vp, _f32, _f32, _vp]),
+    "ff_add_map_sequence_u16": (_i32, [_vp, _i32, _vp, _vp, _i32, _i32, _sz, _sz, _vp, _vp, _vp, _f32, _f32, _vp]),
     "ff_update_meshes": (_i32, [_vp, _vp]),
     "ff_get_mesh_counts": (_i32, [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
     "ff_get_mesh": (_i32, [_vp, _vp, _vp, _vp]),
@@ -382,6 +383,33 @@ class FusionMipMapCPU:
         if st != FF_OK:
             self._check(st)
         return self._q.value
+
+    def addMapSequence(self, depths, cams, rgbs, scaling: float = 1.0 / 5000.0,
+                       maxcamdistance: float = 10.0) -> list:
+        """Several host frames in one call (ff_add_map_sequence_u16): the
+        reference's addMap(std::vector<cv::Mat> depthImages,
+        std::vector<CameraInfo>, std::vector<cv::Mat> rgbImages), which adds
+        them one after another.  depths: HxW uint16 arrays, rgbs: HxWx3 uint8
+        BGR arrays, cams: CameraInfo objects; returns each frame's queued
+        count.  The same results as addMap frame by frame."""
+        n = len(cams)
+        if n == 0 or len(depths) != n or len(rgbs) != n:
+            raise FFError(1, "addMapSequence: as many depth and colour images as cameras")
+        depths = [np.ascontiguousarray(d, dtype=np.uint16) for d in depths]
+        rgbs = [np.ascontiguousarray(c, dtype=np.uint8) for c in rgbs]
+        h, w = depths[0].shape
+        if any(d.shape != (h, w) for d in depths) or any(c.shape != (h, w, 3) for c in rgbs):
+            raise FFError(1, "addMapSequence: every depth HxW uint16 and every rgb HxWx3 uint8, one size")
+        dp = (ctypes.c_void_p * n)(*[d.ctypes.data for d in depths])
+        bp = (ctypes.c_void_p * n)(*[c.ctypes.data for c in rgbs])
+        K = np.ascontiguousarray(np.stack([c.K for c in cams]), np.float64)
+        R = np.ascontiguousarray(np.stack([c.R.reshape(9) for c in cams]), np.float64)
+        t = np.ascontiguousarray(np.stack([c.t for c in cams]), np.float64)
+        q = np.zeros(n, np.int32)
+        st = self._L.ff_add_map_sequence_u16(self._h, n, dp, bp, w, h, 0, 0, _p(K), _p(R), _p(t), scaling,
+                                             maxcamdistance, _p(q))
+        self._check(st)
+        return [int(x) for x in q]
 
     def addMapSequenceDevice(self, d_depth, d_bgr, width: int, height: int, cams, scaling: float = 1.0 / 5000.0,
                              maxcamdistance: float = 10.0) -> list:

@@ -148,6 +148,19 @@ ff_status ff_add_map_sequence_u16_device(ff_handle *h, int n, const uint16_t *co
                                          const double *R, const double *t, float scaling, float maxcam,
                                          int32_t *queued);
 
+/* The same with the n frames in HOST memory: the reference's several-frames
+ * addMap(std::vector<cv::Mat> depthImages, std::vector<CameraInfo>,
+ * std::vector<cv::Mat> rgbImages) (geometryfusion_mipmap_cpu.hpp:125-129,
+ * .cpp:2116-2240), which adds the frames one after another.  All frames'
+ * depth images are copied to the device first, their colour images on a
+ * second stream while the frames are allocated; frames are taken 32 at a
+ * time.  Pitches in bytes (0 = tightly packed).  The images are free when the
+ * call returns; page-locked memory (ff_alloc_host) lets the copies run
+ * without the host. */
+ff_status ff_add_map_sequence_u16(ff_handle *h, int n, const uint16_t *const *depth, const uint8_t *const *bgr,
+                                  int width, int height, size_t depth_pitch, size_t bgr_pitch, const double *K,
+                                  const double *R, const double *t, float scaling, float maxcam, int32_t *queued);
+
 /* Several independent maps fuse one frame each, in one set of launches (the
  * de-duplication of all frames in one cooperative launch, their inserts,
  * leaf finalisations and voxel updates in one launch each) -- for many maps

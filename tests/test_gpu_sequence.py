@@ -71,3 +71,31 @@ def test_sequence_equals_frame_by_frame(lib_built, port_lib, case):
     assert np.array_equal(dg.view(np.uint32), dp.view(np.uint32))
     g.close()
     p.close()
+
+
+def test_host_image_sequence_equals_frame_by_frame(lib_built, port_lib):
+    """ff_add_map_sequence_u16 (host images, the reference's several-frames
+    addMap): the same queued counts, leaf table, queue and voxels as the
+    restatement fed frame by frame -- over a call of more frames than one
+    group of 32 and a call that grows the volume."""
+    from fastfusion_b200.fusion import CameraInfo, FusionMipMapCPU
+    K, frames = circle_frames(0, 100, 160, 120)
+    g = FusionMipMapCPU(0, 0, 0, 0.005, 0.01, 0, True, leaves_max=271420, branches_max=4793488, rcp="exact")
+    p = port_lib.PortFusion(leaves_total=271420, branches_total=4793488, update_mode=1)
+    # frame 75 grows the volume set by frames 50 and 60; the first call takes
+    # 36 frames (two groups)
+    for chunk in ([50, 60, 75, 0, 10, 25] + list(range(30, 90, 2)), [3, 5, 7]):
+        qg = g.addMapSequence([frames[i][0] for i in chunk], [CameraInfo(K, frames[i][2], frames[i][3]) for i in chunk],
+                              [frames[i][1] for i in chunk], SCALING, MAXCAM)
+        qp = [p.add_map(frames[i][0], frames[i][1], K, frames[i][2], frames[i][3], SCALING, MAXCAM) for i in chunk]
+        assert qg == qp, chunk
+        assert queue_set(g.queue()) == queue_set(p.queue())
+    assert g.stats()["grows"] >= 1
+    for a, b in zip(g.leaves(), p.leaves()):
+        assert np.array_equal(a, b)
+    (dg, wg, cg), (dp, wp, cp) = g.bricks(), p.bricks()
+    assert np.array_equal(dg.view(np.uint32), dp.view(np.uint32))
+    assert np.array_equal(wg.view(np.uint32), wp.view(np.uint32))
+    assert np.array_equal(cg, cp)
+    g.close()
+    p.close()
