@@ -421,7 +421,7 @@ def run_b200(a):
     # 2. per-stage profile of the walk after the warm-up (separate map; events per stage)
     log("stage profile")
     m = new_map()
-    dirty, rounds, generated = [], [], []
+    dirty, rounds, generated, top_kept = [], [], [], []
 
     def device_step_stats(mm, s):
         device_step(mm, s)
@@ -429,6 +429,7 @@ def run_b200(a):
         rounds.append(st_["dedupe_rounds"])
         dirty.append(st_["mesh_cells_dirty"])
         generated.append(st_["mesh_cells_generated"] / max(st_["mesh_cells"], 1))
+        top_kept.append(st_["mesh_top_kept"])
 
     for s_ in range(a.warmup):
         device_step(m, s_)
@@ -594,6 +595,7 @@ def run_b200(a):
                     "mesh_cells": st["mesh_cells"], "grows": st["grows"], "meshing_ok": st["meshing_ok"],
                     "mesh_cells_dirty_mean": float(np.mean(dirty)) if dirty else None,
                     "mesh_cells_generated_frac_mean": round(float(np.mean(generated)), 4) if generated else None,
+                    "mesh_updates_from_kept_top_levels": round(float(np.mean(top_kept)), 4) if top_kept else None,
                     "dedupe_rounds_mean": float(np.mean(rounds)) if rounds else None},
         }
         print(json.dumps(line), flush=True)

@@ -2028,6 +2028,7 @@ ff_status ff_get_stats(ff_handle *h, ff_stats *o) {
   o->fused_bricks = *h->h_upd_total + h->direct_bricks;
   o->fused_frame_bricks = h->fused_frame_bricks;
   o->mesh_cells_generated = h->mesh.n_generated;
+  o->mesh_top_kept = h->mesh.top_kept ? 1u : 0u;
   return FF_OK;
 }
 

@@ -2281,6 +2281,7 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   M.n_cells = ncells;
   M.n_dirty = ndirty;
   M.n_generated = I.n_new;
+  M.top_kept = I.gen_start_level > 0;
   M.valid = true;
   return 0;
 }
@@ -2431,7 +2432,8 @@ cudaError_t prewarm_mesh_kernels() {
                        (const void *)k_count_tile_scan,    (const void *)k_count_tile_apply,
                        (const void *)k_fill_counts_from_old, (const void *)k_export_cells,
                        (const void *)k_keep_cells,         (const void *)k_keep_tile_scan,
-                       (const void *)k_keep_apply,         (const void *)k_merge_cells};
+                       (const void *)k_keep_apply,         (const void *)k_merge_cells,
+                       (const void *)k_save_top,           (const void *)k_load_top};
   for (const void *f : fns) {
     cudaFuncAttributes a;
     cudaError_t e = cudaFuncGetAttributes(&a, f);

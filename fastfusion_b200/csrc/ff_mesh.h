@@ -48,6 +48,7 @@ struct MeshState {
   uint64_t n_vertices = 0, n_faces = 0;
   uint64_t cap_vertices = 0, cap_faces = 0;
   uint64_t n_cells = 0, n_dirty = 0, n_generated = 0;
+  bool top_kept = false;  // the last update started from the kept top-level traversal items
   uint32_t last_frame = 0;
   bool valid = false;
   void *impl = nullptr;  // buffers private to ff_mesh.cu

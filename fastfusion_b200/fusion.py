@@ -57,7 +57,7 @@ class ff_stats(ctypes.Structure):
                 ("new_leaves", ctypes.c_uint32), ("dedupe_rounds", ctypes.c_uint32),
                 ("graph_replays", ctypes.c_uint32), ("update_batch", ctypes.c_uint32),
                 ("fused_bricks", ctypes.c_uint64), ("fused_frame_bricks", ctypes.c_uint64),
-                ("mesh_cells_generated", ctypes.c_uint64)]
+                ("mesh_cells_generated", ctypes.c_uint64), ("mesh_top_kept", ctypes.c_uint32)]
 
 
 class ff_tuning(ctypes.Structure):

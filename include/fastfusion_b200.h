@@ -86,6 +86,8 @@ typedef struct ff_stats {
                                   writes each of them once per frame) */
   uint64_t mesh_cells_generated; /* cells the last update's octree traversal produced (the rest were kept from
                                     the update before; all of them after a full generation) */
+  uint32_t mesh_top_kept;      /* 1: the last update's traversal started from the items of its first levels kept
+                                  from an earlier update (no frame since created anything near the root) */
 } ff_stats;
 
 /* Create a map.  Replaces `new FusionMipMapCPU(0,0,0,scale,threshold,0,color)`

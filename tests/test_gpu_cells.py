@@ -75,7 +75,7 @@ def test_incremental_cells_on_the_walk(lib_built):
     from fastfusion_b200.fusion import CameraInfo
     seq = scene.room_walk_sequence(0, 1000, 640, 480)
     a, b = _pair()
-    ratios = []
+    ratios, kept_top = [], []
     for k in range(120):
         R, t = seq.poses[k]
         d, c = scene.render_torch(seq.scene, R, t, 640, 480, seq.K, seq.seed, k, device="cuda")
@@ -92,7 +92,10 @@ def test_incremental_cells_on_the_walk(lib_built):
             b.updateMeshes()
             gen, total = _same_update(a, b, k)
             ratios.append(gen / max(total, 1))
+            kept_top.append(a.stats()["mesh_top_kept"])
     assert min(ratios[3:]) < 0.5, ratios
+    # later updates start from the kept top levels of the traversal
+    assert sum(kept_top) >= 1, kept_top
     a.close()
     b.close()
 
@@ -126,5 +129,29 @@ def test_state_restore_regenerates_every_cell(lib_built, tmp_path):
         a.updateMeshes()
         b.updateMeshes()
         _same_update(a, b, i)
+    a.close()
+    b.close()
+
+
+def test_kept_top_levels_when_nothing_is_created_near_the_root(lib_built):
+    """Frames that add no branch or leaf near the root (the same views again):
+    the update starts from the kept top-level items and still equals the
+    full generation; a frame of a new area brings the top levels back."""
+    from fastfusion_b200.fusion import CameraInfo
+    K, frames = circle_frames(4, 40, 320, 240)
+    a, b = _pair()
+    seen = []
+    for block in ([0, 1, 2], [0, 1, 2], [1, 2, 0], [30, 35], [0, 1]):
+        for i in block:
+            depth, bgr, R, t = frames[i]
+            cam = CameraInfo(K, R, t)
+            a.addMap(depth, cam, bgr, SCALING, MAXCAM)
+            b.addMap(depth, cam, bgr, SCALING, MAXCAM)
+        a.updateMeshes()
+        b.updateMeshes()
+        _same_update(a, b, block)
+        seen.append(a.stats()["mesh_top_kept"])
+    assert seen[0] == 0          # the first update generates everything
+    assert seen[1] == 1 and seen[2] == 1, seen
     a.close()
     b.close()
