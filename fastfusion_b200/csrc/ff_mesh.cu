@@ -1946,6 +1946,21 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
     T.count = I.d_top_count;
     const bool use_top = incr && I.top_valid && !in.top_changed;
     const int lv0 = use_top ? LC : 0;
+    if (!use_top) {
+      // room for the level's items: as much as the queues hold, at most the
+      // 8^LC cell items and 27^LC items of each other kind the level can have
+      size_t most = 1, cells_most = 1;
+      for (int k = 0; k < LC; k++) most *= 27, cells_most *= 8;
+      MCK(grow_buf(I.top_cellq, I.cap_top[0], std::min(want[0], cells_most), s));
+      MCK(grow_buf(I.top_faceq, I.cap_top[1], std::min(want[1], most), s));
+      MCK(grow_buf(I.top_edgeq, I.cap_top[2], std::min(want[2], most), s));
+      MCK(grow_buf(I.top_vertq, I.cap_top[3], std::min(want[3], most), s));
+      T.cellq = I.top_cellq;
+      T.faceq = I.top_faceq;
+      T.edgeq = I.top_edgeq;
+      T.vertq = I.top_vertq;
+      for (int k = 0; k < 4; k++) T.cap[k] = (uint32_t)I.cap_top[k];
+    }
     I.gen_start_level = (uint32_t)lv0;
     if (use_top) {
       note_launch(1);
