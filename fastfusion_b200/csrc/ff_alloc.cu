@@ -297,9 +297,15 @@ __device__ __forceinline__ void dedupe_body(const BatchDesc *__restrict__ bd, in
   // (round + 2) % 3 was last read before this round's barrier (after a
   // barrier that gave up or no convergence, the host clears the words)
   if (converged && blockIdx.x == 0 && threadIdx.x == 0) chg[(round + 2) % 3] = 0;
+  uint32_t nproc = 0;
   if (active && x < W) {
     for (int r = 0; r < rows; r++) processed[(size_t)(ty * DD_ROWS + r) * W + x] = (uint8_t)((bits >> r) & 1u);
+    nproc = (uint32_t)__popc(rows >= 32 ? bits : (bits & ((1u << rows) - 1u)));
   }
+  // the frame's processed pixels, counted once per tile (the insert that
+  // follows no longer adds them per warp on the counters' cache line)
+  nproc = __reduce_add_sync(0xffffffffu, nproc);
+  if (active && lane == 0 && nproc) atomicAdd(&F.cnt->processed, nproc);
   if (blockIdx.x == 0 && (int)threadIdx.x < m1 - m0) {
     Counters *c = bd->f[m0 + threadIdx.x].cnt;
     c->dedupe_iters = round + 1;
@@ -601,13 +607,15 @@ __global__ void k_insert(const BatchDesc *__restrict__ bd, int m0, int m1) {
   bool act = i < npix && processed[i];
   unsigned m = __ballot_sync(0xffffffffu, act);
   if (!act) return;
-  if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&cnt->processed, __popc(m));
-  // octree levels this pixel probes on its descent, summed per warp (the
-  // algorithmic bytes of the insert: 16 B per level -- the node's leaf and
-  // child slots, the leaf's frame stamp and its queue entry, 4 B each)
+  // octree levels this pixel probes on its descent, summed per warp when the
+  // stage profile is on (the algorithmic bytes of the insert: 16 B per level
+  // -- the node's leaf and child slots, the leaf's frame stamp and its queue
+  // entry, 4 B each)
   const uint32_t levels = insert_pixel(F, i, vox[i], cnt);
-  const uint32_t sum = __reduce_add_sync(m, levels);
-  if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&cnt->levels, sum);
+  if (F.count_levels) {
+    const uint32_t sum = __reduce_add_sync(m, levels);
+    if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&cnt->levels, sum);
+  }
 }
 
 void launch_insert(const BatchDesc *d_batch, uint32_t pix, cudaStream_t s, int block, int m0, int m1) {

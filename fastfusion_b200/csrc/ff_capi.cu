@@ -1115,6 +1115,7 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
   mf.shard = h->shard;
   mf.shards = h->shards;
   mf.spin_limit = h->spin_limit;
+  mf.count_levels = h->prof.on ? 1u : 0u;
   for (int r = 0; r < 3; r++) mf.shift[r] = h->shift[r];
   if (h->cur_slot >= 0) {
     mf.upd_mask = h->d_upd_mask;

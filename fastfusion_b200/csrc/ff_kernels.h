@@ -56,6 +56,8 @@ struct MapFrame {
   uint32_t branches_init;
   // iterations after which a device-side wait of this frame gives up
   uint32_t spin_limit;
+  // the insert sums the octree levels it probes (the stage profile's bytes)
+  uint32_t count_levels;
   // Deferred voxel update (upd_mask non-null): the leaf finalisation marks the
   // frame's queued bricks with bit upd_slot in upd_mask and appends bricks
   // not yet marked to upd_list (count in *upd_count); one k_fuse_multi pass
