@@ -287,6 +287,8 @@ __global__ void __launch_bounds__(512, FUSE_MULTI_BLOCKS_PER_SM) k_fuse_multi(co
     __syncthreads();
     const float thrD = __fmul_rz(thr, ls);
     const float thrW = __fmul_rz(__fmul_rz(WEIGHT_FACTOR, thr), ls);
+    // the fall-off's reciprocal depends on the brick only, not on the frame
+    const float rcp_fall = rcp_upd<RCP_HOST>(__fsub_rz(thrW, DIST_W_EPS), rtab, rshift);
     const float fx_ = (float)x;
     // Frame k's sample of this voxel: the projection and the image reads,
     // issued one frame ahead so that they overlap the previous frame's
@@ -335,7 +337,7 @@ __global__ void __launch_bounds__(512, FUSE_MULTI_BLOCKS_PER_SM) k_fuse_multi(co
       const bool msk = cur.in && h < S.maxcam;
       const float front = dInc < DIST_W_EPS ? 1.0f : 0.0f;
       const float back = (dInc >= DIST_W_EPS && dInc < thrW) ? 1.0f : 0.0f;
-      const float fall = __fmul_rz(__fsub_rz(thrW, dInc), rcp_upd<RCP_HOST>(__fsub_rz(thrW, DIST_W_EPS), rtab, rshift));
+      const float fall = __fmul_rz(__fsub_rz(thrW, dInc), rcp_fall);
       float wInc = msk ? __fadd_rz(front, __fmul_rz(fall, back)) : 0.0f;
       if (S.conf) wInc = __fmul_rz(wInc, cur.cw);
       const float wNew = __fadd_rz(wAcc, wInc);
