@@ -38,10 +38,18 @@ struct ff_handle {
   // host-input frames: the colour image is copied on a second stream while
   // the allocation kernels run (it is first read by the voxel update)
   cudaStream_t copy_stream = nullptr;
-  // ff_get_mesh_async: the mesh's device-to-host copies, after ev_mesh_ready
+  // ff_get_mesh_async: the mesh's device-to-host copies, after ev_mesh_ready;
+  // the last two copies and the device buffers they read (the mesher writes
+  // its two output buffers in turn, so an update waits only for the copy of
+  // the mesh two updates back)
   cudaStream_t mesh_stream = nullptr;
-  cudaEvent_t ev_mesh_ready = nullptr, ev_mesh_copied = nullptr;
-  bool mesh_copy_pending = false;
+  cudaEvent_t ev_mesh_ready = nullptr;
+  struct MeshCopy {
+    const void *src[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev = nullptr;
+    bool pending = false;
+  } mesh_copy[2];
+  int mesh_copy_next = 0;
   // ff_add_map_sequence_u16: the frames' images staged on the device (up to
   // BATCH_MAX frames), and the colour copies the next update pass waits for
   uint16_t *d_hseq_depth = nullptr;
@@ -599,7 +607,8 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
         cudaEventCreateWithFlags(&h->ev_counters, cudaEventDisableTiming) != cudaSuccess ||
         cudaStreamCreateWithFlags(&h->mesh_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_mesh_ready, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h->ev_mesh_copied, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->mesh_copy[0].ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->mesh_copy[1].ev, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_host_images, cudaEventDisableTiming) != cudaSuccess) {
       fail(FF_ERR_CUDA, "copy stream");
       break;
@@ -749,7 +758,8 @@ ff_status ff_destroy(ff_handle *h) {
   if (h->ev_counters) cudaEventDestroy(h->ev_counters);
   if (h->mesh_stream) cudaStreamDestroy(h->mesh_stream);
   if (h->ev_mesh_ready) cudaEventDestroy(h->ev_mesh_ready);
-  if (h->ev_mesh_copied) cudaEventDestroy(h->ev_mesh_copied);
+  for (auto &c : h->mesh_copy)
+    if (c.ev) cudaEventDestroy(c.ev);
   if (h->ev_host_images) cudaEventDestroy(h->ev_host_images);
   if (h->d_hseq_depth) cudaFree(h->d_hseq_depth);
   if (h->d_hseq_bgr) cudaFree(h->d_hseq_bgr);
@@ -2169,9 +2179,20 @@ ff_status ff_update_meshes(ff_handle *h, int *updated) {
     if (updated) *updated = 1;
     return FF_OK;
   }
-  // the mesh buffers are rewritten (or freed as they grow) only after the
-  // copies of an earlier ff_get_mesh_async have read them
-  if (h->mesh_copy_pending) CK(cudaStreamWaitEvent(h->stream, h->ev_mesh_copied, 0));
+  // the buffers this update writes (or frees as they grow) only after the
+  // asynchronous copies that read them; a copy of the last mesh, which this
+  // update only reads, goes on meanwhile
+  {
+    const void *next[3];
+    mesh_next_outputs(h->mesh, &next[0], &next[1], &next[2]);
+    for (auto &c : h->mesh_copy) {
+      if (!c.pending) continue;
+      bool hit = false;
+      for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) hit |= c.src[a] && c.src[a] == next[b];
+      if (hit) CK(cudaStreamWaitEvent(h->stream, c.ev, 0));
+    }
+  }
   MeshInputs in;
   in.tree = h->d_tree;
   in.branches_used = h->branches_used;
@@ -2270,17 +2291,24 @@ ff_status ff_get_mesh_async(ff_handle *h, float *xyz, uint8_t *rgb, uint32_t *fa
   }
   if (M.n_faces)
     CK(cudaMemcpyAsync(faces, M.d_faces, sizeof(uint32_t) * 3 * M.n_faces, cudaMemcpyDeviceToHost, h->mesh_stream));
-  CK(cudaEventRecord(h->ev_mesh_copied, h->mesh_stream));
-  h->mesh_copy_pending = true;
+  auto &c = h->mesh_copy[h->mesh_copy_next];
+  h->mesh_copy_next ^= 1;
+  CK(cudaEventRecord(c.ev, h->mesh_stream));
+  c.src[0] = M.d_xyz;
+  c.src[1] = M.d_rgb;
+  c.src[2] = M.d_faces;
+  c.pending = true;
   return FF_OK;
 }
 
 ff_status ff_mesh_wait(ff_handle *h) {
   if (!h) return FF_ERR_BAD_ARG;
-  if (!h->mesh_copy_pending) return FF_OK;
   CK(cudaSetDevice(h->cfg.device));
-  CK(cudaEventSynchronize(h->ev_mesh_copied));
-  h->mesh_copy_pending = false;
+  for (auto &c : h->mesh_copy)
+    if (c.pending) {
+      CK(cudaEventSynchronize(c.ev));
+      c.pending = false;
+    }
   return FF_OK;
 }
 

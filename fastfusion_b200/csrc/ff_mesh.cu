@@ -2428,6 +2428,17 @@ void mesh_free(MeshState &M) {
   M.d_faces = nullptr;
 }
 
+void mesh_next_outputs(MeshState &M, const void **xyz, const void **rgb, const void **faces) {
+  if (!M.impl) {
+    *xyz = *rgb = *faces = nullptr;
+    return;
+  }
+  MeshImpl &I = impl(M);
+  *xyz = I.old_xyz;
+  *rgb = I.old_rgb;
+  *faces = I.old_faces;
+}
+
 void mesh_invalidate(MeshState &M) {
   M.valid = false;
   if (M.impl) {

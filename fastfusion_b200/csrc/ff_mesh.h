@@ -64,6 +64,10 @@ int mesh_copy_cells(MeshState &m, int32_t *rows, int64_t *ranges, cudaStream_t s
 // most 65536 cells.
 int mesh_copy_cells_noalloc(MeshState &m, int32_t *rows, int64_t *ranges, cudaStream_t s, std::string &err);
 void mesh_free(MeshState &m);
+// The device buffers the next mesh_update writes its mesh into (the mesh of
+// the update before last; null before two updates): a copy out of them must
+// finish first.
+void mesh_next_outputs(MeshState &m, const void **xyz, const void **rgb, const void **faces);
 void mesh_invalidate(MeshState &m);
 void mesh_note_frame(MeshState &m);
 
