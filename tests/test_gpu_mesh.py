@@ -170,26 +170,32 @@ def test_async_mesh_export_overlaps_and_matches(lib_built):
 def test_async_mesh_exports_two_in_flight(lib_built):
     """Two asynchronous exports in flight with two updates between them and
     the wait: each buffer holds the mesh of its own update (the second update
-    rewrites the device buffers the first copy reads, so it must wait for
-    that copy on the device)."""
+    rewrites the device buffers the first copy reads, so it waits for that
+    copy on the device).  The expected meshes come from a second map fed the
+    same frames and read with the blocking export."""
     from fastfusion_b200 import fusion as ff
     K, frames = circle_frames(5, 12, 320, 240)
     m = ff.FusionMipMapCPU(0, 0, 0, 0.005, 0.01, 0, True, leaves_max=271420, branches_max=4793488, rcp="exact")
+    r = ff.FusionMipMapCPU(0, 0, 0, 0.005, 0.01, 0, True, leaves_max=271420, branches_max=4793488, rcp="exact")
     bufs = [ff.MeshBuffer(), ff.MeshBuffer()]
     want, got = [], []
     for u in range(4):
         for depth, bgr, R, t in frames[3 * u:3 * u + 3]:
             m.addMap(depth, ff.CameraInfo(K, R, t), bgr, SCALING, MAXCAM)
+            r.addMap(depth, ff.CameraInfo(K, R, t), bgr, SCALING, MAXCAM)
         m.updateMeshes()
-        w = m.getMeshInterleavedMarchingCubes()
-        want.append((w.vertices.copy(), w.colors.copy(), w.faces.copy()))
+        r.updateMeshes()
         got.append(m.getMeshInterleavedMarchingCubes(out=bufs[u % 2], wait=False))
+        w = r.getMeshInterleavedMarchingCubes()
+        want.append((w.vertices, w.colors, w.faces))
         if u % 2 == 1:
             m.mesh_wait()
             for k in (u - 1, u):
+                assert len(want[k][2]) > 0
                 assert np.array_equal(got[k].vertices.view(np.uint32), want[k][0].view(np.uint32)), k
                 assert np.array_equal(got[k].colors, want[k][1]), k
                 assert np.array_equal(got[k].faces, want[k][2]), k
     m.close()
+    r.close()
     for b in bufs:
         b.close()
