@@ -1831,6 +1831,10 @@ struct MeshImpl {
   uint32_t *d_top_count = nullptr, *h_top_count = nullptr;
   bool top_valid = false;
   uint32_t gen_start_level = 0;  // the last update's first traversed level (statistics)
+  // items per traversal level of the last update (sizes the next update's
+  // launches: an incremental update's deeper levels hold few items)
+  uint32_t level_items[MAX_GEN_LEVELS + 1] = {};
+  bool level_items_incr = false;
 };
 
 static MeshImpl &impl(MeshState &m) {
@@ -1981,6 +1985,9 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
         // need few blocks (the loop inside strides over any grid)
         uint64_t bound = 1;
         for (int k = 0; k < lv && bound < (uint64_t)148 * 8 * 128; k++) bound *= 27;
+        // an incremental update: about as many items as at this level last time
+        if (incr && I.level_items_incr)
+          bound = std::min<uint64_t>(bound, std::max<uint64_t>(2 * (uint64_t)I.level_items[lv], 8 * 128));
         const int blocks = (int)std::min<uint64_t>(148 * 8, (bound + 127) / 128);
         g.expand_all = (incr && lv < LC) ? 1 : 0;
         k_gen_level<<<blocks, 128, 0, s>>>(g, Q, lv, in.n);
@@ -2021,6 +2028,11 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
     for (int k = 0; k < 5; k++) I.peak[k] = 0;
     for (int l = 0; l <= lv; l++)
       for (int k = 0; k < 4; k++) I.peak[k] = std::max<size_t>(I.peak[k], hc[LEVEL_COUNTS + 4 * l + k]);
+    for (int l = 0; l <= MAX_GEN_LEVELS; l++) {
+      const uint32_t *c = hc + LEVEL_COUNTS + 4 * l;
+      I.level_items[l] = l <= lv ? c[0] + c[1] + c[2] + c[3] : 0u;
+    }
+    I.level_items_incr = incr;
     I.peak[4] = hc[8];
     if (leftover) {
       err = "meshing: cell generation did not finish within the level limit";

@@ -3,7 +3,7 @@
 // new leaves (first pixel).  Ascending; equal keys keep their input order.
 //
 //  * up to SORT_SMALL keys whose bits and position fit one 64-bit word: one
-//    block sorts the packed words (key << 13 | position) in shared memory by
+//    block sorts the packed words (key << 14 | position) in shared memory by
 //    a bitonic network (one launch);
 //  * otherwise a least-significant-digit radix sort, 8 bits per pass: per
 //    tile of 2048 keys a digit histogram, an exclusive scan of the histograms
@@ -18,11 +18,11 @@
 namespace ffb {
 
 constexpr int SORT_SMALL_THREADS = 1024;
-constexpr int SORT_SMALL_POS_BITS = 13;  // positions < SORT_SMALL = 2^13
+constexpr int SORT_SMALL_POS_BITS = 14;  // positions < SORT_SMALL = 2^14
 constexpr int RS_THREADS = 256, RS_ITEMS = 8, RS_TILE = RS_THREADS * RS_ITEMS, RS_BINS = 256;
 constexpr int SCAN_BLOCK = 1024;
 
-static_assert(SORT_SMALL == (1u << SORT_SMALL_POS_BITS), "positions of the small sort fill 13 bits");
+static_assert(SORT_SMALL == (1u << SORT_SMALL_POS_BITS), "positions of the small sort fill its position bits");
 static_assert(RS_BINS == RS_THREADS, "one digit per thread in the scatter's digit loops");
 
 // ----------------------------------------------------------- small sort ----
@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(SORT_SMALL_THREADS) k_sort_small(const uint64_
   for (uint32_t i = threadIdx.x; i < n; i += SORT_SMALL_THREADS) {
     const uint64_t v = w[i];
     keys_out[i] = v >> SORT_SMALL_POS_BITS;
-    pos_out[i] = (uint32_t)(v & (SORT_SMALL - 1));
+    pos_out[i] = (uint32_t)(v & (SORT_SMALL - 1u));
   }
 }
 
@@ -179,7 +179,7 @@ static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 static uint32_t tiles_of(uint32_t n) { return (n + RS_TILE - 1) / RS_TILE; }
 
-// packed words below the all-ones padding: end_bit + 13 < 64
+// packed words below the all-ones padding: end_bit + 14 < 64
 static bool small_path(uint32_t n, int end_bit) { return n <= SORT_SMALL && end_bit + SORT_SMALL_POS_BITS < 64; }
 
 size_t argsort_temp_bytes(uint32_t n) {

@@ -8,8 +8,9 @@
 
 namespace ffb {
 
-// up to this many keys (with end_bit + 13 < 64) are sorted by one block
-constexpr uint32_t SORT_SMALL = 8192;
+// up to this many keys (with end_bit + 14 < 64) are sorted by one block
+// (128 KB of shared memory)
+constexpr uint32_t SORT_SMALL = 16384;
 
 // Temporary device bytes argsort_u64 needs for n keys (none on the one-block
 // path, which the caller need not know: the figure covers both).
