@@ -295,6 +295,27 @@ def reduce_over_ranks(x: float, op: str, device=None) -> float:
     return float(t.item())
 
 
+def copy_bandwidth(dev, nbytes: int = 64 << 20, reps: int = 5) -> dict:
+    """Page-locked host <-> device copy bandwidth (GB/s): the best of a few
+    64 MB copies each way, timed with CUDA events."""
+    import torch
+    host = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    devbuf = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    out = {}
+    for name, dst, src in (("h2d_gbs", devbuf, host), ("d2h_gbs", host, devbuf)):
+        best = None
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            dst.copy_(src, non_blocking=True)
+            e1.record()
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        out[name] = round(nbytes / (best / 1e3) / 1e9, 1)
+    return out
+
+
 def whole_job_rate(frames_this_rank: float, ms_this_rank: float, device=None):
     """(frames/s of the whole job, slowest rank's ms): every rank's frames
     over the max-over-ranks device time."""
@@ -531,6 +552,13 @@ def run_b200(a):
         e2e_pageable["host_frames"] = "pageable"
         del p_depth, p_bgr
         mesh_buf.close()
+        # the copy bandwidth between page-locked host memory and the device on
+        # this box: what the e2e step's copies cost at best
+        pcie = copy_bandwidth(dev)
+        for e in (e2e, e2e_single, e2e_pageable):
+            e["copy_bound_ms_per_step"] = round(max(e["h2d_bytes_per_step"] / pcie["h2d_gbs"],
+                                                    e["d2h_bytes_per_step"] / pcie["d2h_gbs"]) / 1e6, 3)
+        e2e["pcie"] = pcie
     clocks = clk.stop() if clk else None
 
     value, dev_ms_max = whole_job_rate(a.steps * FRAMES_PER_STEP, dev_ms, dev)
