@@ -315,7 +315,9 @@ __device__ __forceinline__ void dedupe_body(const BatchDesc *__restrict__ bd, in
 }
 
 template <int DD_ROWS>
-__global__ void __launch_bounds__(32 * DD_WARPS) k_dedupe(const BatchDesc *__restrict__ bd, int m0, int m1,
+// (register budget for 6 blocks per SM: a 10-frame sequence of 640x480
+// frames fits one cooperative launch)
+__global__ void __launch_bounds__(32 * DD_WARPS, 6) k_dedupe(const BatchDesc *__restrict__ bd, int m0, int m1,
                                                           uint32_t *bar) {
   dedupe_body<DD_ROWS>(bd, m0, m1, bar);
 }
