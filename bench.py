@@ -1083,6 +1083,7 @@ def run_corridor(a):
     m.set_stream(stream.cuda_stream)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
     leaves, ref_cap_step = [], None
+    cells, mc_cum = [], []
 
     def step(s_, render=True):
         if render and s_ % CHUNK == 0:
@@ -1111,6 +1112,9 @@ def run_corridor(a):
         ev[i][1].record(stream)
         st = m.stats()
         leaves.append(st["leaves_used"])
+        cells.append(st["mesh_cells"])
+        # the cell list's device time per update (the stage profile is cumulative)
+        mc_cum.append(m.profile_read()["mesh_cells"][0])
         if ref_cap_step is None and st["leaves_used"] > REFERENCE_POOL_BRICKS:
             ref_cap_step = a.warmup + i
     torch.cuda.synchronize(dev)
@@ -1131,6 +1135,9 @@ def run_corridor(a):
         "ms_per_step_median": round(float(np.median(ms)), 3), "ms_per_step_max": round(float(np.max(ms)), 3),
         "ms_per_step_first_quarter": round(float(np.mean(ms[:q])), 3),
         "ms_per_step_last_quarter": round(float(np.mean(ms[-q:])), 3),
+        "mesh_cells_ms_per_update_first_quarter": round(float(np.mean(np.diff([0.0] + mc_cum)[:q])), 4),
+        "mesh_cells_ms_per_update_last_quarter": round(float(np.mean(np.diff([0.0] + mc_cum)[-q:])), 4),
+        "mesh_cells_first_quarter": int(np.mean(cells[:q])), "mesh_cells_last_quarter": int(np.mean(cells[-q:])),
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32" if a.storage == "fp32" else "f16-storage/f32",
         "data": "synthetic: seeded corridor/office floor rendered on the GPU (primitives beyond maxcam + 1 m "
