@@ -55,7 +55,7 @@ struct ff_handle {
   uint16_t *d_hseq_depth = nullptr;
   uint8_t *d_hseq_bgr = nullptr;
   size_t hseq_frames = 0, hseq_pix = 0;
-  cudaEvent_t ev_host_images = nullptr;
+  cudaEvent_t ev_host_depth = nullptr, ev_host_images = nullptr;
   bool host_images_pending = false;
   cudaEvent_t ev_bgr_free = nullptr, ev_bgr_ready = nullptr;
   // recorded once a frame's counters have reached the host: a single-map
@@ -609,7 +609,8 @@ ff_status ff_create(const ff_config *cfg, ff_handle **out) {
         cudaEventCreateWithFlags(&h->ev_mesh_ready, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->mesh_copy[0].ev, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->mesh_copy[1].ev, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h->ev_host_images, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&h->ev_host_images, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_host_depth, cudaEventDisableTiming) != cudaSuccess) {
       fail(FF_ERR_CUDA, "copy stream");
       break;
     }
@@ -761,6 +762,7 @@ ff_status ff_destroy(ff_handle *h) {
   for (auto &c : h->mesh_copy)
     if (c.ev) cudaEventDestroy(c.ev);
   if (h->ev_host_images) cudaEventDestroy(h->ev_host_images);
+  if (h->ev_host_depth) cudaEventDestroy(h->ev_host_depth);
   if (h->d_hseq_depth) cudaFree(h->d_hseq_depth);
   if (h->d_hseq_bgr) cudaFree(h->d_hseq_bgr);
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
@@ -1835,16 +1837,20 @@ ff_status ff_add_map_sequence_u16(ff_handle *h, int n, const uint16_t *const *de
   ff_status st = FF_OK;
   for (int i = 0; i < n && st == FF_OK;) {
     const int c = std::min(n - i, (int)frames);
-    // depth first, on the map's stream (the de-duplication reads it); the
-    // colour on the copy stream, overlapping the allocation (the update pass
-    // waits for it).  The staging is free: the previous group's call returned
-    // after its update pass.
+    // On the copy stream: the depth images first (the de-duplication reads
+    // them: the map's stream waits for these copies only, which meanwhile
+    // overlap the map's earlier work, the last mesh update say), then the
+    // colour images, overlapping the allocation (the update pass waits for
+    // them).  The staging is free: the previous group's call returned after
+    // its update pass.
     for (int k = 0; k < c; k++) {
       uint16_t *d = h->d_hseq_depth + (size_t)k * npix;
       CK(cudaMemcpy2DAsync(d, sizeof(uint16_t) * width, depth[i + k], depth_pitch, sizeof(uint16_t) * width, height,
-                           cudaMemcpyHostToDevice, h->stream));
+                           cudaMemcpyHostToDevice, h->copy_stream));
       dd[k] = d;
     }
+    CK(cudaEventRecord(h->ev_host_depth, h->copy_stream));
+    CK(cudaStreamWaitEvent(h->stream, h->ev_host_depth, 0));
     for (int k = 0; k < c; k++) {
       uint8_t *b = h->d_hseq_bgr + (size_t)k * npix * 3;
       CK(cudaMemcpy2DAsync(b, 3 * (size_t)width, bgr[i + k], bgr_pitch, 3 * (size_t)width, height,
