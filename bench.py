@@ -1135,8 +1135,12 @@ def run_corridor(a):
         "ms_per_step_median": round(float(np.median(ms)), 3), "ms_per_step_max": round(float(np.max(ms)), 3),
         "ms_per_step_first_quarter": round(float(np.mean(ms[:q])), 3),
         "ms_per_step_last_quarter": round(float(np.mean(ms[-q:])), 3),
-        "mesh_cells_ms_per_update_first_quarter": round(float(np.mean(np.diff([0.0] + mc_cum)[:q])), 4),
-        "mesh_cells_ms_per_update_last_quarter": round(float(np.mean(np.diff([0.0] + mc_cum)[-q:])), 4),
+        # the cell list per update: the median of each quarter (a growth of the
+        # volume moves every cell and regenerates the whole list: those few
+        # updates are reported apart, with the maximum)
+        "mesh_cells_ms_per_update_first_quarter": round(float(np.median(np.diff([0.0] + mc_cum)[:q])), 4),
+        "mesh_cells_ms_per_update_last_quarter": round(float(np.median(np.diff([0.0] + mc_cum)[-q:])), 4),
+        "mesh_cells_ms_per_update_max": round(float(np.max(np.diff([0.0] + mc_cum))), 3),
         "mesh_cells_first_quarter": int(np.mean(cells[:q])), "mesh_cells_last_quarter": int(np.mean(cells[-q:])),
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32" if a.storage == "fp32" else "f16-storage/f32",
