@@ -1083,7 +1083,6 @@ def run_corridor(a):
     m.set_stream(stream.cuda_stream)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
     leaves, ref_cap_step = [], None
-    cells, mc_cum = [], []
 
     def step(s_, render=True):
         if render and s_ % CHUNK == 0:
@@ -1099,22 +1098,39 @@ def run_corridor(a):
 
     for s_ in range(a.warmup):
         step(s_)
-    m.profile(True)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    # Every PROFILE_EVERY-th step runs with the per-stage CUDA-event profile
+    # on (its events and synchronisations would slow the step) and is not
+    # timed; the others are timed with the profile off.
+    PROFILE_EVERY = 10
+    stage_sum = {}
+    mc_steps = []  # (step, cell-list ms, cells) of the profiled steps
+    ev, timed_i = [], []
     torch.cuda.synchronize(dev)
     for i in range(a.steps):
         if (a.warmup + i) % CHUNK == 0:
             m.sync()
             render_chunk(a.warmup + i)
-        flush.fill_(i)
-        ev[i][0].record(stream)
-        step(a.warmup + i, render=False)
-        ev[i][1].record(stream)
+        if i % PROFILE_EVERY == PROFILE_EVERY - 1:
+            m.profile(True)
+            step(a.warmup + i, render=False)
+            p_ = m.profile_read()
+            m.profile(False)
+            for k_, v_ in p_.items():
+                acc = stage_sum.setdefault(k_, [0.0, 0.0, 0])
+                acc[0] += v_[0]
+                acc[1] += v_[1]
+                acc[2] += v_[2]
+            mc_steps.append((i, p_["mesh_cells"][0], m.stats()["mesh_cells"]))
+        else:
+            flush.fill_(i)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step(a.warmup + i, render=False)
+            e1.record(stream)
+            ev.append((e0, e1))
+            timed_i.append(i)
         st = m.stats()
         leaves.append(st["leaves_used"])
-        cells.append(st["mesh_cells"])
-        # the cell list's device time per update (the stage profile is cumulative)
-        mc_cum.append(m.profile_read()["mesh_cells"][0])
         if ref_cap_step is None and st["leaves_used"] > REFERENCE_POOL_BRICKS:
             ref_cap_step = a.warmup + i
     torch.cuda.synchronize(dev)
@@ -1122,26 +1138,31 @@ def run_corridor(a):
     # the whole map's frames over the slowest part's device time
     ms_total = reduce_over_ranks(float(sum(ms)), "max", dev)
     leaves_all = int(m.stats()["leaves_used"])  # every part holds the whole leaf table
-    stages = m.profile_read()
+    stages = {k_: tuple(v_) for k_, v_ in stage_sum.items()}
     st = m.stats()
     peak, peak_kind = measured_hbm_peak()
-    fms, fbytes, fl = stages["fuse"]
+    fms, fbytes, fl = stages.get("fuse", (0.0, 0.0, 0))
     fuse_gbs = fbytes / (fms / 1e3) / 1e9 if fms > 0 else 0.0
     q = max(1, len(ms) // 4)
+    mq = max(1, len(mc_steps) // 4)
+    mc_ms = [x[1] for x in mc_steps]
     line = {
         "metric": METRIC.replace("(640x480, 5 mm)", "(large map, 1280x960, 5 mm)"),
-        "value": round(a.steps * FRAMES_PER_STEP / (ms_total / 1e3), 2), "unit": UNIT, "n_gpus": world,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_total / a.steps, 4),
+        "value": round(len(ms) * FRAMES_PER_STEP / (ms_total / 1e3), 2), "unit": UNIT, "n_gpus": world,
+        "steps": a.steps, "timed_steps": len(ms),
+        "profiled_steps": f"every {PROFILE_EVERY}th step ran with the stage profile on and is not timed",
+        "warmup": a.warmup, "ms_per_step": round(ms_total / len(ms), 4),
         "ms_per_step_median": round(float(np.median(ms)), 3), "ms_per_step_max": round(float(np.max(ms)), 3),
         "ms_per_step_first_quarter": round(float(np.mean(ms[:q])), 3),
         "ms_per_step_last_quarter": round(float(np.mean(ms[-q:])), 3),
-        # the cell list per update: the median of each quarter (a growth of the
-        # volume moves every cell and regenerates the whole list: those few
-        # updates are reported apart, with the maximum)
-        "mesh_cells_ms_per_update_first_quarter": round(float(np.median(np.diff([0.0] + mc_cum)[:q])), 4),
-        "mesh_cells_ms_per_update_last_quarter": round(float(np.median(np.diff([0.0] + mc_cum)[-q:])), 4),
-        "mesh_cells_ms_per_update_max": round(float(np.max(np.diff([0.0] + mc_cum))), 3),
-        "mesh_cells_first_quarter": int(np.mean(cells[:q])), "mesh_cells_last_quarter": int(np.mean(cells[-q:])),
+        # the cell list per update over the profiled steps: the median of each
+        # quarter (a growth of the volume moves every cell and regenerates the
+        # whole list: those few updates show in the maximum)
+        "mesh_cells_ms_per_update_first_quarter": round(float(np.median(mc_ms[:mq])), 4) if mc_ms else None,
+        "mesh_cells_ms_per_update_last_quarter": round(float(np.median(mc_ms[-mq:])), 4) if mc_ms else None,
+        "mesh_cells_ms_per_update_max": round(float(np.max(mc_ms)), 3) if mc_ms else None,
+        "mesh_cells_first_quarter": int(np.mean([x[2] for x in mc_steps[:mq]])) if mc_steps else None,
+        "mesh_cells_last_quarter": int(np.mean([x[2] for x in mc_steps[-mq:]])) if mc_steps else None,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32" if a.storage == "fp32" else "f16-storage/f32",
         "data": "synthetic: seeded corridor/office floor rendered on the GPU (primitives beyond maxcam + 1 m "
