@@ -72,6 +72,7 @@ struct ff_handle {
   cudaStream_t fuse_stream = nullptr;
   cudaEvent_t ev_alloc = nullptr;  // the frame's insert done (map stream)
   cudaEvent_t ev_cnn_in = nullptr, ev_cnn_done = nullptr;  // the confidence network on fuse_stream
+  bool cnn_on_side = false;  // a sequence's frames: their networks on fuse_stream, beside the allocation chain
   bool cnn_pending = false;
   cudaEvent_t ev_fin = nullptr;    // the frame's finalisation done (fuse_stream)
   bool fin_pending = false;
@@ -1160,8 +1161,9 @@ static ff_status frame_prepare(ff_handle *h, const uint16_t *d_depth, const uint
     if (h->cur_slot >= 0) h->d_conf = h->d_ring_conf + (size_t)h->cur_slot * h->ring_pix;
     const float kf[4] = {(float)K[0], (float)K[1], (float)K[2], (float)K[3]};
     cudaStream_t cs = s;
-    if (side && plan.one_sync) {
-      // after the depth image is ready on the map's stream
+    if ((side && plan.one_sync) || h->cnn_on_side) {
+      // after the depth image is ready on the map's stream; the network
+      // feeds only the voxel update, so the frame's allocation need not wait
       cs = h->fuse_stream;
       CK(cudaEventRecord(h->ev_cnn_in, s));
       CK(cudaStreamWaitEvent(cs, h->ev_cnn_in, 0));
@@ -1696,8 +1698,11 @@ static ff_status sequence_chunk(ff_handle *h, int c, const uint16_t *const *d_de
     h->cur_slot = h->upd_pending + k;
     h->d_cnt = h->d_seq_cnt + k;
     h->h_cnt = h->h_seq_cnt + k;
-    FCK(frame_prepare(h, d_depth[k], d_bgr[k], W, H, K + 4 * k, R + 9 * k, t + 3 * k, scaling, maxcam, mf[k],
-                      plan[k]));
+    h->cnn_on_side = true;
+    const ff_status sp = frame_prepare(h, d_depth[k], d_bgr[k], W, H, K + 4 * k, R + 9 * k, t + 3 * k, scaling,
+                                       maxcam, mf[k], plan[k]);
+    h->cnn_on_side = false;
+    FCK(sp);
     MapFrame &F = mf[k];
     F.vox = h->d_seq_vox + (size_t)k * h->seq_pix;
     F.proc = h->d_seq_proc + (size_t)k * h->seq_pix;
@@ -1727,6 +1732,11 @@ static ff_status sequence_chunk(ff_handle *h, int c, const uint16_t *const *d_de
   // the parents of every frame's new leaves, once the chain has run
   launch_parents_frames(h->d_batch, c, s);
   CK(cudaGetLastError());
+  if (h->cnn_pending) {
+    // the frames' confidence networks report into their counters
+    CK(cudaStreamWaitEvent(s, h->ev_cnn_done, 0));
+    h->cnn_pending = false;
+  }
   CK(cudaMemcpyAsync(h->h_seq_cnt, h->d_seq_cnt, sizeof(Counters) * c, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   h->seq_images = true;
