@@ -81,7 +81,7 @@ __device__ __forceinline__ int mc_slot(const McTab &T, int e) {
 // Cell generation
 // ---------------------------------------------------------------------------
 
-struct Slot {
+struct __align__(16) Slot {
   uint32_t S;   // tree entry of the slot's leaf; child branch at S + 8
   uint32_t la;  // finest leaf at or above the slot (BRANCHINIT if none)
   uint16_t o[3];
@@ -96,24 +96,30 @@ struct Cell {
   uint32_t L[8];
 };
 
+// Work items of the traversal.  Faces and edges are queued per axis (the
+// queue gives the axis), so the lanes of a warp expand items of one kind and
+// axis: the item functions are specialised by axis, and a warp whose lanes
+// held several kinds would run them one after the other.
 struct FaceItem {
   Slot a, b;
-  int axis;
 };
 struct EdgeItem {
   Slot s[4];
-  int axis;
 };
 struct VertItem {
   Slot s[8];
 };
 
+// the queues of a level: cells, faces of axis 0-2, edges of axis 0-2, vertices
+constexpr int QK = 8;
+constexpr int QK_CELL = 0, QK_FACE = 1, QK_EDGE = 4, QK_VERT = 7;
+
 struct GenQueues {
   Slot *cellq[2];
-  FaceItem *faceq[2];
-  EdgeItem *edgeq[2];
+  FaceItem *faceq[2];  // three regions of cap_face items, one per axis
+  EdgeItem *edgeq[2];  // three regions of cap_edge items, one per axis
   VertItem *vertq[2];
-  uint32_t *lvl;  // [level][4]: cell, face, edge, vert item counts of each level
+  uint32_t *lvl;  // [level][QK]: item count of each queue of each level
   uint32_t cap_cell, cap_face, cap_edge, cap_vert;
   Cell *cells;
   uint32_t *n_cells;
@@ -125,10 +131,11 @@ struct GenQueues {
 // counter words of the generation (see MeshImpl::d_count)
 constexpr int LEVEL_COUNTS = 32;
 constexpr int MAX_GEN_LEVELS = 48;
-constexpr int COUNT_WORDS = LEVEL_COUNTS + 4 * (MAX_GEN_LEVELS + 1) + 30;
+constexpr int COUNT_WORDS = LEVEL_COUNTS + QK * (MAX_GEN_LEVELS + 1) + 30;
 // host mirror only: 3 uint64 + 2 uint32 read back per update, then the emit
 // pass's sample count (uint64)
 constexpr int HOST_TOTALS = COUNT_WORDS - 10;
+static_assert(HOST_TOTALS % 2 == 0, "the host totals are read as uint64");
 
 struct GenCtx {
   const uint32_t *tree;
@@ -187,8 +194,42 @@ __device__ __forceinline__ void others(int e, int &p, int &q) {
   q = e == 2 ? 1 : 2;
 }
 
-// Slot in a per-launch queue: one atomic per group of lanes that push to the
-// same counter at the same time (lanes that are active together share it).
+// Slots for every active lane of a warp: n[k] entries of counter ctr[k]
+// (0 <= n[k] < 16, per lane).  All lanes of a launch push into the same
+// counters (the next level's queues and the cell list), so each counter takes
+// one atomic per warp, and the K atomics are independent: their latencies
+// overlap instead of adding up.
+template <int K>
+__device__ __forceinline__ void claim_multi(uint32_t *const (&ctr)[K], const uint32_t (&n)[K], uint32_t (&base)[K]) {
+  const unsigned mask = __activemask();
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  const int leader = __ffs(mask) - 1;
+  uint32_t tot[K], got[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    uint32_t pre = 0, t = 0;
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const unsigned bal = __ballot_sync(mask, (n[k] >> b) & 1u);
+      pre += (uint32_t)__popc(bal & below) << b;
+      t += (uint32_t)__popc(bal) << b;
+    }
+    base[k] = pre;
+    tot[k] = t;
+    got[k] = 0;
+  }
+  if ((int)lane == leader) {
+#pragma unroll
+    for (int k = 0; k < K; k++)
+      if (tot[k]) got[k] = atomicAdd(ctr[k], tot[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < K; k++) base[k] += __shfl_sync(mask, got[k], leader);
+}
+
+// One slot of *ctr for the calling lane: one atomic per group of active lanes
+// that push to the same counter.
 __device__ __forceinline__ uint32_t claim(uint32_t *ctr) {
   const unsigned mask = __activemask();
   const unsigned peers = __match_any_sync(mask, (unsigned long long)(uintptr_t)ctr);
@@ -200,49 +241,35 @@ __device__ __forceinline__ uint32_t claim(uint32_t *ctr) {
   return base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
 }
 
-// n slots per lane; n must be the same for every lane that reaches the call
-// together (a constant at the call site).
-__device__ __forceinline__ uint32_t claim_n(uint32_t *ctr, uint32_t n) {
-  const unsigned mask = __activemask();
-  const unsigned peers = __match_any_sync(mask, (unsigned long long)(uintptr_t)ctr);
-  const int leader = __ffs(peers) - 1;
-  const unsigned lane = threadIdx.x & 31;
-  uint32_t base = 0;
-  if ((int)lane == leader) base = atomicAdd(ctr, (uint32_t)__popc(peers) * n);
-  base = __shfl_sync(peers, base, leader);
-  return base + (uint32_t)__popc(peers & ((1u << lane) - 1u)) * n;
+// a cell with a side without a leaf is never meshed
+template <int N>
+__device__ __forceinline__ bool all_leaves(const uint32_t (&L)[N]) {
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < N; k++) ok &= L[k] < BRANCHINIT;
+  return ok;
 }
 
-__device__ void emit_cell(const GenQueues &Q, int type, int quirk, const int *o, int size, const uint32_t *L, int nl) {
-  for (int k = 0; k < nl; k++)
-    if (L[k] >= BRANCHINIT) return;  // a side without a leaf is never meshed
-  const uint32_t i = claim(Q.n_cells);
+// Store a cell at a claimed position of the list.
+template <int N>
+__device__ __forceinline__ void store_cell(const GenQueues &Q, uint32_t i, int type, const int *o, int size,
+                                           const uint32_t (&L)[N]) {
   if (i >= Q.cap_cells) {
     atomicOr(Q.error, ERR_CELL_OVERFLOW);
     return;
   }
-  if (type == 7) claim(Q.n_corners);
   Cell c;
   c.type = (uint8_t)type;
-  c.quirk = (uint8_t)quirk;
+  c.quirk = 0;
   c.size = (uint16_t)size;
   for (int r = 0; r < 3; r++) c.o[r] = (uint16_t)o[r];
   c.pad = 0;
-  for (int k = 0; k < 8; k++) c.L[k] = k < nl ? L[k] : BRANCHINIT;
+#pragma unroll
+  for (int k = 0; k < 8; k++) c.L[k] = k < N ? L[k] : BRANCHINIT;
   Q.cells[i] = c;
 }
 
-template <typename T>
-__device__ __forceinline__ void push(T *q, uint32_t *count, uint32_t cap, const T &v, uint32_t *error) {
-  const uint32_t i = claim(count);
-  if (i >= cap) {
-    atomicOr(error, ERR_CELL_OVERFLOW);
-    return;
-  }
-  q[i] = v;
-}
-
-// Store at a slot claimed before (claim_n), unless past the queue's end.
+// Store an item at a claimed position of a queue, unless past its end.
 template <typename T>
 __device__ __forceinline__ void put(T *q, uint32_t i, uint32_t cap, const T &v, uint32_t *error) {
   if (i >= cap) {
@@ -255,36 +282,39 @@ __device__ __forceinline__ void put(T *q, uint32_t i, uint32_t cap, const T &v, 
 // Every item is a pure function of its slots, so an item found while
 // expanding another is queued for the next launch rather than expanded by the
 // same thread: each thread does a bounded amount of work (a few independent
-// tree reads, a few pushes) and the levels run wide.
+// tree reads, one set of queue claims) and the levels run wide.
 struct Out {
   Slot *cellq;
-  FaceItem *faceq;
-  EdgeItem *edgeq;
+  FaceItem *faceq;  // axis regions of Q.cap_face items
+  EdgeItem *edgeq;  // axis regions of Q.cap_edge items
   VertItem *vertq;
-  uint32_t *count;  // the next level's 4 counters
+  uint32_t *count;  // the next level's QK counters
 };
 
-__device__ __forceinline__ void push_cell(const GenQueues &Q, const Out &O, const Slot &s) {
-  push(O.cellq, O.count + 0, Q.cap_cell, s, Q.error);
-}
-__device__ __forceinline__ void push_vert(const GenQueues &Q, const Out &O, const Slot *S8) {
-  VertItem v;
-  for (int j = 0; j < 8; j++) v.s[j] = S8[j];
-  push(O.vertq, O.count + 3, Q.cap_vert, v, Q.error);
-}
-__device__ __forceinline__ void put_face(const GenQueues &Q, const Out &O, uint32_t i, const Slot &a, const Slot &b,
-                                         int ax) {
+__device__ __forceinline__ void put_face(const GenQueues &Q, const Out &O, int ax, uint32_t i, const Slot &a,
+                                         const Slot &b) {
   FaceItem f;
   f.a = a;
   f.b = b;
-  f.axis = ax;
-  put(O.faceq, i, Q.cap_face, f, Q.error);
+  if (i >= Q.cap_face) {
+    atomicOr(Q.error, ERR_CELL_OVERFLOW);
+    return;
+  }
+  O.faceq[(size_t)ax * Q.cap_face + i] = f;
 }
-__device__ __forceinline__ void put_edge(const GenQueues &Q, const Out &O, uint32_t i, const Slot *S4, int e) {
+__device__ __forceinline__ void put_edge(const GenQueues &Q, const Out &O, int ax, uint32_t i, const Slot *S4) {
   EdgeItem it;
-  it.axis = e;
   for (int j = 0; j < 4; j++) it.s[j] = S4[j];
-  put(O.edgeq, i, Q.cap_edge, it, Q.error);
+  if (i >= Q.cap_edge) {
+    atomicOr(Q.error, ERR_CELL_OVERFLOW);
+    return;
+  }
+  O.edgeq[(size_t)ax * Q.cap_edge + i] = it;
+}
+__device__ __forceinline__ void put_vert(const GenQueues &Q, const Out &O, uint32_t i, const Slot *S8) {
+  VertItem v;
+  for (int j = 0; j < 8; j++) v.s[j] = S8[j];
+  put(O.vertq, i, Q.cap_vert, v, Q.error);
 }
 
 // The item functions are templated on their axis and fully unrolled, so every
@@ -306,14 +336,24 @@ __device__ __forceinline__ void vert_item(const GenCtx &g, const GenQueues &Q, c
     dead |= dead_slot(S8[j], sub);
   }
   if (dead) return;
+  uint32_t L[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) L[j] = S8[j].la;
+  const bool em = !any && emit && all_leaves(L);
+  Slot C[8];
   if (any) {
-    Slot C[8];
 #pragma unroll
     for (int j = 0; j < 8; j++) C[j] = ch(g, S8[j], 7 - j);
-    push_vert(Q, O, C);
+  }
+  uint32_t *const ctr[3] = {O.count + QK_VERT, Q.n_cells, Q.n_corners};
+  const uint32_t n[3] = {any ? 1u : 0u, em ? 1u : 0u, em ? 1u : 0u};
+  uint32_t at[3];
+  claim_multi(ctr, n, at);
+  if (any) {
+    put_vert(Q, O, at[0], C);
     return;
   }
-  if (!emit) return;
+  if (!em) return;
   // the vertex is a corner of the smallest slot around it
   int size = S8[0].size, small = 0;
 #pragma unroll
@@ -326,10 +366,7 @@ __device__ __forceinline__ void vert_item(const GenCtx &g, const GenQueues &Q, c
 #pragma unroll
       for (int r = 0; r < 3; r++) o[r] = (int)S8[j].o[r] + (((j >> r) & 1) ? 0 : size) - size;
     }
-  uint32_t L[8];
-#pragma unroll
-  for (int j = 0; j < 8; j++) L[j] = S8[j].la;
-  emit_cell(Q, 7, 0, o, size, L, 8);
+  store_cell(Q, at[1], 7, o, size, L);
 }
 
 template <int E>
@@ -344,8 +381,14 @@ __device__ __forceinline__ void edge_item(const GenCtx &g, const GenQueues &Q, c
     dead |= dead_slot(S4[j], sub);
   }
   if (dead) return;
+  const uint32_t L[4] = {S4[0].la, S4[1].la, S4[2].la, S4[3].la};
+  const bool em = !any && emit && all_leaves(L);
+  uint32_t *const ctr[3] = {O.count + QK_EDGE + E, O.count + QK_VERT, Q.n_cells};
+  const uint32_t n[3] = {any ? 2u : 0u, any ? 1u : 0u, em ? 1u : 0u};
+  uint32_t at[3];
+  claim_multi(ctr, n, at);
   if (!any) {
-    if (!emit) return;
+    if (!em) return;
     // the edge line runs along a side of the smallest slot
     int size = S4[0].size, small = 0;
 #pragma unroll
@@ -359,11 +402,9 @@ __device__ __forceinline__ void edge_item(const GenCtx &g, const GenQueues &Q, c
         o[P] = (int)S4[j].o[P] + ((j & 1) ? 0 : size) - size;
         o[Qx] = (int)S4[j].o[Qx] + ((j & 2) ? 0 : size) - size;
       }
-    uint32_t L[4] = {S4[0].la, S4[1].la, S4[2].la, S4[3].la};
-    emit_cell(Q, 4 + E, 0, o, size, L, 4);
+    store_cell(Q, at[2], 4 + E, o, size, L);
     return;
   }
-  const uint32_t eb = claim_n(O.count + 2, 2);
 #pragma unroll
   for (int half = 0; half < 2; half++) {
     Slot H[4];
@@ -372,7 +413,7 @@ __device__ __forceinline__ void edge_item(const GenCtx &g, const GenQueues &Q, c
       const int k = ((j & 1) ? 0 : (1 << P)) | (((j >> 1) & 1) ? 0 : (1 << Qx)) | (half ? (1 << E) : 0);
       H[j] = ch(g, S4[j], k);
     }
-    put_edge(Q, O, eb + half, H, E);
+    put_edge(Q, O, E, at[0] + half, H);
   }
   Slot S8[8];
 #pragma unroll
@@ -383,7 +424,7 @@ __device__ __forceinline__ void edge_item(const GenCtx &g, const GenQueues &Q, c
     const int k = (pj ? 0 : (1 << P)) | (qj ? 0 : (1 << Qx)) | (ej ? (1 << E) : 0);
     S8[j] = ch(g, S4[pj | (qj << 1)], k);
   }
-  push_vert(Q, O, S8);
+  put_vert(Q, O, at[1], S8);
 }
 
 template <int AX>
@@ -391,18 +432,25 @@ __device__ __forceinline__ void face_item(const GenCtx &g, const GenQueues &Q, c
                                           const Slot &B, bool emit) {
   const bool sa = is_sub(g, A), sb = is_sub(g, B);
   if (dead_slot(A, sa) || dead_slot(B, sb)) return;
-  if (!sa && !sb) {
-    if (!emit) return;
+  constexpr int U = AX == 0 ? 1 : 0, V = AX == 2 ? 1 : 2;
+  const bool leafy = !sa && !sb;
+  const uint32_t L[2] = {A.la, B.la};
+  const bool em = leafy && emit && all_leaves(L);
+  uint32_t *const ctr[5] = {O.count + QK_FACE + AX, O.count + QK_EDGE + U, O.count + QK_EDGE + V, O.count + QK_VERT,
+                            Q.n_cells};
+  const uint32_t n[5] = {leafy ? 0u : 4u, leafy ? 0u : 2u, leafy ? 0u : 2u, leafy ? 0u : 1u, em ? 1u : 0u};
+  uint32_t at[5];
+  claim_multi(ctr, n, at);
+  if (leafy) {
+    if (!em) return;
     const int size = min((int)A.size, (int)B.size);
     const bool a_small = A.size <= B.size;
     int o[3] = {a_small ? A.o[0] : B.o[0], a_small ? A.o[1] : B.o[1], a_small ? A.o[2] : B.o[2]};
     o[AX] = (int)B.o[AX] - size;
-    uint32_t L[2] = {A.la, B.la};
-    emit_cell(Q, 1 + AX, 0, o, size, L, 2);
+    store_cell(Q, at[4], 1 + AX, o, size, L);
     return;
   }
   constexpr int bit = 1 << AX;
-  constexpr int U = AX == 0 ? 1 : 0, V = AX == 2 ? 1 : 2;
   // the two sides' halves next to the face: A's children on its +ax side, B's
   // on its -ax side (a slot that is not subdivided stands for all of them)
   Slot a[8], b[8];
@@ -412,13 +460,11 @@ __device__ __forceinline__ void face_item(const GenCtx &g, const GenQueues &Q, c
     a[k] = ch(g, A, k | bit);
     b[k] = ch(g, B, k);
   }
-  const uint32_t fb = claim_n(O.count + 1, 4);
 #pragma unroll
   for (int qd = 0; qd < 4; qd++) {
     const int k = ((qd & 1) ? (1 << U) : 0) | ((qd & 2) ? (1 << V) : 0);
-    put_face(Q, O, fb + qd, a[k], b[k], AX);
+    put_face(Q, O, AX, at[0] + qd, a[k], b[k]);
   }
-  const uint32_t eb = claim_n(O.count + 2, 4);
 #pragma unroll
   for (int t = 0; t < 2; t++) {
     const int e = t == 0 ? U : V;
@@ -435,7 +481,7 @@ __device__ __forceinline__ void face_item(const GenCtx &g, const GenQueues &Q, c
         const int k = (half ? (1 << e) : 0) | (side[other] ? (1 << other) : 0);
         S4[j] = side[AX] ? b[k] : a[k];
       }
-      put_edge(Q, O, eb + 2 * t + half, S4, e);
+      put_edge(Q, O, e, at[1 + t] + half, S4);
     }
   }
   Slot S8[8];
@@ -444,59 +490,97 @@ __device__ __forceinline__ void face_item(const GenCtx &g, const GenQueues &Q, c
     const int k = j & ~bit;
     S8[j] = ((j >> AX) & 1) ? b[k] : a[k];
   }
-  push_vert(Q, O, S8);
+  put_vert(Q, O, at[3], S8);
 }
 
 // one subdivided slot: its children, their 12 faces, 6 edges and centre
 __device__ __forceinline__ void cell_item(const GenCtx &g, const GenQueues &Q, const Out &O, const Slot (&C)[8]) {
+  uint32_t sub = 0, em = 0;
 #pragma unroll
   for (int j = 0; j < 8; j++) {
-    if (is_sub(g, C[j])) {
-      push_cell(Q, O, C[j]);
-    } else if (slot_changed(g, C[j])) {
-      int o[3] = {C[j].o[0], C[j].o[1], C[j].o[2]};
-      uint32_t L[1] = {C[j].la};
-      emit_cell(Q, 0, 0, o, C[j].size, L, 1);
+    if (is_sub(g, C[j])) sub |= 1u << j;
+    else if (C[j].la < BRANCHINIT && slot_changed(g, C[j])) em |= 1u << j;
+  }
+  uint32_t *const ctr[9] = {O.count + QK_CELL,     Q.n_cells,             O.count + QK_FACE, O.count + QK_FACE + 1,
+                            O.count + QK_FACE + 2, O.count + QK_EDGE,     O.count + QK_EDGE + 1,
+                            O.count + QK_EDGE + 2, O.count + QK_VERT};
+  const uint32_t n[9] = {(uint32_t)__popc(sub), (uint32_t)__popc(em), 4, 4, 4, 2, 2, 2, 1};
+  uint32_t at[9];
+  claim_multi(ctr, n, at);
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const uint32_t below = (1u << j) - 1u;
+    if (sub >> j & 1u) {
+      put(O.cellq, at[0] + (uint32_t)__popc(sub & below), Q.cap_cell, C[j], Q.error);
+    } else if (em >> j & 1u) {
+      const int o[3] = {C[j].o[0], C[j].o[1], C[j].o[2]};
+      const uint32_t L[1] = {C[j].la};
+      store_cell(Q, at[1] + (uint32_t)__popc(em & below), 0, o, C[j].size, L);
     }
   }
   constexpr int F[3][4][2] = {{{0, 1}, {2, 3}, {4, 5}, {6, 7}}, {{0, 2}, {1, 3}, {4, 6}, {5, 7}},
                               {{0, 4}, {1, 5}, {2, 6}, {3, 7}}};
-  const uint32_t fb = claim_n(O.count + 1, 12);
 #pragma unroll
   for (int ax = 0; ax < 3; ax++)
 #pragma unroll
-    for (int i = 0; i < 4; i++) put_face(Q, O, fb + 4 * ax + i, C[F[ax][i][0]], C[F[ax][i][1]], ax);
-  const uint32_t eb = claim_n(O.count + 2, 6);
+    for (int i = 0; i < 4; i++) put_face(Q, O, ax, at[2 + ax] + i, C[F[ax][i][0]], C[F[ax][i][1]]);
 #pragma unroll
   for (int x = 0; x < 2; x++) {
     Slot S4[4] = {C[x], C[x | 2], C[x | 4], C[x | 6]};
-    put_edge(Q, O, eb + x, S4, 0);
+    put_edge(Q, O, 0, at[5] + x, S4);
   }
 #pragma unroll
   for (int y = 0; y < 4; y += 2) {
     Slot S4[4] = {C[y], C[y | 1], C[y | 4], C[y | 5]};
-    put_edge(Q, O, eb + 2 + y / 2, S4, 1);
+    put_edge(Q, O, 1, at[6] + y / 2, S4);
   }
 #pragma unroll
   for (int z = 0; z < 8; z += 4) {
     Slot S4[4] = {C[z], C[z | 1], C[z | 2], C[z | 3]};
-    put_edge(Q, O, eb + 4 + z / 4, S4, 2);
+    put_edge(Q, O, 2, at[7] + z / 4, S4);
   }
-  push_vert(Q, O, C);
+  put_vert(Q, O, at[8], C);
 }
 
-// Items of level `lv` (queue buffer lv & 1, counters lvl + 4 lv) expand into
+template <int AX>
+__device__ __forceinline__ void face_at(const GenCtx &g, const GenQueues &Q, const Out &O, int cur, uint32_t j) {
+  const FaceItem f = Q.faceq[cur][(size_t)AX * Q.cap_face + j];
+  const bool changed = slot_changed(g, f.a) || slot_changed(g, f.b);
+  if (!changed && !g.expand_all) return;
+  face_item<AX>(g, Q, O, f.a, f.b, changed);
+}
+
+template <int E>
+__device__ __forceinline__ void edge_at(const GenCtx &g, const GenQueues &Q, const Out &O, int cur, uint32_t j) {
+  const EdgeItem e = Q.edgeq[cur][(size_t)E * Q.cap_edge + j];
+  bool changed = false;
+#pragma unroll
+  for (int k = 0; k < 4; k++) changed |= slot_changed(g, e.s[k]);
+  if (!changed && !g.expand_all) return;
+  edge_item<E>(g, Q, O, e.s, changed);
+}
+
+// Items of level `lv` (queue buffer lv & 1, counters lvl + QK lv) expand into
 // level lv + 1 or emit cells.  Level 0 is the root: the volume's 8 octants.
+// The queues' threads are laid out one after the other, each queue's padded
+// to whole warps, so that the lanes of a warp run the same item function.
 __device__ __forceinline__ void gen_level(const GenCtx &g, const GenQueues &Q, int lv, uint32_t n) {
   const int cur = lv & 1, nb = cur ^ 1;
   const bool root = lv == 0;
-  const uint32_t *cnt = Q.lvl + 4 * lv;
-  Out O{Q.cellq[nb], Q.faceq[nb], Q.edgeq[nb], Q.vertq[nb], Q.lvl + 4 * (lv + 1)};
-  const uint32_t nc = root ? 1u : min(cnt[0], Q.cap_cell), nf = root ? 0u : min(cnt[1], Q.cap_face);
-  const uint32_t ne = root ? 0u : min(cnt[2], Q.cap_edge), nv = root ? 0u : min(cnt[3], Q.cap_vert);
-  const uint32_t total = nc + nf + ne + nv;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-    if (i < nc) {
+  const uint32_t *cnt = Q.lvl + QK * lv;
+  Out O{Q.cellq[nb], Q.faceq[nb], Q.edgeq[nb], Q.vertq[nb], Q.lvl + QK * (lv + 1)};
+  uint32_t c[QK], e[QK];
+  uint32_t acc = 0;
+#pragma unroll
+  for (int k = 0; k < QK; k++) {
+    const uint32_t cap = k == QK_CELL ? Q.cap_cell : (k < QK_EDGE ? Q.cap_face : (k < QK_VERT ? Q.cap_edge : Q.cap_vert));
+    c[k] = root ? (k == QK_CELL ? 1u : 0u) : min(cnt[k], cap);
+    acc += (c[k] + 31u) & ~31u;
+    e[k] = acc;
+  }
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < e[QK - 1]; i += gridDim.x * blockDim.x) {
+    if (i < e[0]) {
+      if (i >= c[0]) continue;
       Slot C[8];
       if (root) {
         const uint16_t h = (uint16_t)(n >> 1);
@@ -515,24 +599,20 @@ __device__ __forceinline__ void gen_level(const GenCtx &g, const GenQueues &Q, i
         for (int co = 0; co < 8; co++) C[co] = child_of(g, s, co);
       }
       cell_item(g, Q, O, C);
-    } else if (i < nc + nf) {
-      const FaceItem f = Q.faceq[cur][i - nc];
-      const bool changed = slot_changed(g, f.a) || slot_changed(g, f.b);
-      if (!changed && !g.expand_all) continue;
-      if (f.axis == 0) face_item<0>(g, Q, O, f.a, f.b, changed);
-      else if (f.axis == 1) face_item<1>(g, Q, O, f.a, f.b, changed);
-      else face_item<2>(g, Q, O, f.a, f.b, changed);
-    } else if (i < nc + nf + ne) {
-      const EdgeItem e = Q.edgeq[cur][i - nc - nf];
-      bool changed = false;
-#pragma unroll
-      for (int j = 0; j < 4; j++) changed |= slot_changed(g, e.s[j]);
-      if (!changed && !g.expand_all) continue;
-      if (e.axis == 0) edge_item<0>(g, Q, O, e.s, changed);
-      else if (e.axis == 1) edge_item<1>(g, Q, O, e.s, changed);
-      else edge_item<2>(g, Q, O, e.s, changed);
-    } else {
-      const VertItem v = Q.vertq[cur][i - nc - nf - ne];
+    } else if (i < e[1]) {
+      if (i - e[0] < c[1]) face_at<0>(g, Q, O, cur, i - e[0]);
+    } else if (i < e[2]) {
+      if (i - e[1] < c[2]) face_at<1>(g, Q, O, cur, i - e[1]);
+    } else if (i < e[3]) {
+      if (i - e[2] < c[3]) face_at<2>(g, Q, O, cur, i - e[2]);
+    } else if (i < e[4]) {
+      if (i - e[3] < c[4]) edge_at<0>(g, Q, O, cur, i - e[3]);
+    } else if (i < e[5]) {
+      if (i - e[4] < c[5]) edge_at<1>(g, Q, O, cur, i - e[4]);
+    } else if (i < e[6]) {
+      if (i - e[5] < c[6]) edge_at<2>(g, Q, O, cur, i - e[5]);
+    } else if (i - e[6] < c[7]) {
+      const VertItem v = Q.vertq[cur][i - e[6]];
       bool changed = false;
 #pragma unroll
       for (int j = 0; j < 8; j++) changed |= slot_changed(g, v.s[j]);
@@ -542,59 +622,63 @@ __device__ __forceinline__ void gen_level(const GenCtx &g, const GenQueues &Q, i
   }
 }
 
-__global__ void __launch_bounds__(128, 6) k_gen_level(GenCtx g, GenQueues Q, int lv, uint32_t n) {
+__global__ void __launch_bounds__(128, 4) k_gen_level(GenCtx g, GenQueues Q, int lv, uint32_t n) {
   gen_level(g, Q, lv, n);
 }
 
 // The items of traversal level MESH_TOP_LEVELS, kept from one update to the
 // next: the levels above it hold few items, each a long chain of dependent
-// queue claims, and they produce the same items until a frame creates a
-// branch or a leaf that close to the root.
+// tree reads, and they produce the same items until a frame creates a branch
+// or a leaf that close to the root.
 struct TopCache {
   Slot *cellq;
-  FaceItem *faceq;
-  EdgeItem *edgeq;
+  FaceItem *faceq;  // axis regions of cap[1] items
+  EdgeItem *edgeq;  // axis regions of cap[2] items
   VertItem *vertq;
-  uint32_t cap[4];
-  uint32_t *count;  // cell, face, edge, vertex items; [4]: 1 if they did not fit
+  uint32_t cap[4];  // cells, faces and edges per axis, vertices
+  uint32_t *count;  // the QK queues' items; [QK]: 1 if they did not fit
 };
 
 __global__ void k_save_top(GenQueues Q, int lv, TopCache T) {
-  const uint32_t *c = Q.lvl + 4 * lv;
+  const uint32_t *c = Q.lvl + QK * lv;
   const int b = lv & 1;
-  const uint32_t n0 = c[0], n1 = c[1], n2 = c[2], n3 = c[3];
-  const bool fits = n0 <= T.cap[0] && n1 <= T.cap[1] && n2 <= T.cap[2] && n3 <= T.cap[3] && n0 <= Q.cap_cell &&
-                    n1 <= Q.cap_face && n2 <= Q.cap_edge && n3 <= Q.cap_vert;
+  bool fits = c[0] <= T.cap[0] && c[0] <= Q.cap_cell && c[7] <= T.cap[3] && c[7] <= Q.cap_vert;
+  for (int k = 0; k < 3; k++) {
+    fits &= c[QK_FACE + k] <= T.cap[1] && c[QK_FACE + k] <= Q.cap_face;
+    fits &= c[QK_EDGE + k] <= T.cap[2] && c[QK_EDGE + k] <= Q.cap_edge;
+  }
   const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   if (t0 == 0) {
-    T.count[0] = n0;
-    T.count[1] = n1;
-    T.count[2] = n2;
-    T.count[3] = n3;
-    T.count[4] = fits ? 0u : 1u;
+    for (int k = 0; k < QK; k++) T.count[k] = c[k];
+    T.count[QK] = fits ? 0u : 1u;
   }
   if (!fits) return;
-  for (uint32_t i = t0; i < n0; i += stride) T.cellq[i] = Q.cellq[b][i];
-  for (uint32_t i = t0; i < n1; i += stride) T.faceq[i] = Q.faceq[b][i];
-  for (uint32_t i = t0; i < n2; i += stride) T.edgeq[i] = Q.edgeq[b][i];
-  for (uint32_t i = t0; i < n3; i += stride) T.vertq[i] = Q.vertq[b][i];
+  for (uint32_t i = t0; i < c[0]; i += stride) T.cellq[i] = Q.cellq[b][i];
+  for (int k = 0; k < 3; k++) {
+    for (uint32_t i = t0; i < c[QK_FACE + k]; i += stride)
+      T.faceq[(size_t)k * T.cap[1] + i] = Q.faceq[b][(size_t)k * Q.cap_face + i];
+    for (uint32_t i = t0; i < c[QK_EDGE + k]; i += stride)
+      T.edgeq[(size_t)k * T.cap[2] + i] = Q.edgeq[b][(size_t)k * Q.cap_edge + i];
+  }
+  for (uint32_t i = t0; i < c[7]; i += stride) T.vertq[i] = Q.vertq[b][i];
 }
 
+// (the cache's counts fit the queues: the queues only grow while it is valid)
 __global__ void k_load_top(GenQueues Q, int lv, TopCache T) {
   const int b = lv & 1;
-  const uint32_t n0 = T.count[0], n1 = T.count[1], n2 = T.count[2], n3 = T.count[3];
   const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   if (t0 == 0) {
-    uint32_t *c = Q.lvl + 4 * lv;
-    c[0] = n0;
-    c[1] = n1;
-    c[2] = n2;
-    c[3] = n3;
+    uint32_t *c = Q.lvl + QK * lv;
+    for (int k = 0; k < QK; k++) c[k] = T.count[k];
   }
-  for (uint32_t i = t0; i < n0; i += stride) Q.cellq[b][i] = T.cellq[i];
-  for (uint32_t i = t0; i < n1; i += stride) Q.faceq[b][i] = T.faceq[i];
-  for (uint32_t i = t0; i < n2; i += stride) Q.edgeq[b][i] = T.edgeq[i];
-  for (uint32_t i = t0; i < n3; i += stride) Q.vertq[b][i] = T.vertq[i];
+  for (uint32_t i = t0; i < T.count[0]; i += stride) Q.cellq[b][i] = T.cellq[i];
+  for (int k = 0; k < 3; k++) {
+    for (uint32_t i = t0; i < T.count[QK_FACE + k]; i += stride)
+      Q.faceq[b][(size_t)k * Q.cap_face + i] = T.faceq[(size_t)k * T.cap[1] + i];
+    for (uint32_t i = t0; i < T.count[QK_EDGE + k]; i += stride)
+      Q.edgeq[b][(size_t)k * Q.cap_edge + i] = T.edgeq[(size_t)k * T.cap[2] + i];
+  }
+  for (uint32_t i = t0; i < T.count[7]; i += stride) Q.vertq[b][i] = T.vertq[i];
 }
 
 // Sort key of a cell: (type, log2 size, origin x, y, z), the order of the
@@ -1771,10 +1855,12 @@ struct MeshImpl {
   VertItem *vertq[2] = {nullptr, nullptr};
   size_t cap_cellq[2] = {0, 0}, cap_faceq[2] = {0, 0}, cap_edgeq[2] = {0, 0}, cap_vertq[2] = {0, 0};
   uint32_t n_corners = 0;
-  size_t peak[5] = {0, 0, 0, 0, 0};  // last update's largest level of each queue, and its cell count
+  // last update's largest level of each kind of queue (faces and edges: of
+  // one axis), and its cell count
+  size_t peak[5] = {0, 0, 0, 0, 0};
   int key_bits = 0;                   // bits per origin coordinate of old_keys / keys
   // words 8 n_cells, 9 error, 10 n_dirty, 11 n_corners, 12-13 samples;
-  // from LEVEL_COUNTS: 4 item counters per generation level
+  // from LEVEL_COUNTS: QK item counters per generation level
   uint32_t *d_count = nullptr;
   uint32_t *h_count = nullptr;
   // cells: unsorted, sorted (current), previous
@@ -1875,17 +1961,18 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
     MCK(grow_buf(I.keep, I.cap_keep, (size_t)n_old + 1, s));
     MCK(grow_buf(I.keep_tiles, I.cap_keep_tiles, std::max<size_t>(keep_tiles, 1), s));
   }
-  // queue sizes: a first guess from the octree size, then the previous
-  // update's peaks with headroom (the map grows slowly between updates)
+  // queue sizes (faces and edges: per axis): a first guess from the octree
+  // size, then the previous update's peaks with headroom (the map grows
+  // slowly between updates)
   const uint32_t slots = std::max<uint32_t>(in.branches_used / 2, 64);
-  size_t want[5] = {(size_t)slots * 2 + 4096, (size_t)slots * 4 + 4096, (size_t)slots * 4 + 4096,
+  size_t want[5] = {(size_t)slots * 2 + 4096, (size_t)slots * 2 + 4096, (size_t)slots * 2 + 4096,
                     (size_t)slots * 2 + 4096, (size_t)slots * 16 + 4096};
   for (int k = 0; k < 5; k++) want[k] = std::max<size_t>(want[k], I.peak[k] + I.peak[k] / 4 + 1024);
   for (int attempt = 0; attempt < 6; attempt++) {
     for (int b = 0; b < 2; b++) {
       MCK(grow_buf(I.cellq[b], I.cap_cellq[b], want[0], s));
-      MCK(grow_buf(I.faceq[b], I.cap_faceq[b], want[1], s));
-      MCK(grow_buf(I.edgeq[b], I.cap_edgeq[b], want[2], s));
+      MCK(grow_buf(I.faceq[b], I.cap_faceq[b], 3 * want[1], s));
+      MCK(grow_buf(I.edgeq[b], I.cap_edgeq[b], 3 * want[2], s));
       MCK(grow_buf(I.vertq[b], I.cap_vertq[b], want[3], s));
     }
     MCK(grow_buf(I.raw, I.cap_raw, want[4], s));
@@ -1903,8 +1990,8 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
     }
     Q.lvl = I.d_count + LEVEL_COUNTS;
     Q.cap_cell = (uint32_t)std::min(I.cap_cellq[0], I.cap_cellq[1]);
-    Q.cap_face = (uint32_t)std::min(I.cap_faceq[0], I.cap_faceq[1]);
-    Q.cap_edge = (uint32_t)std::min(I.cap_edgeq[0], I.cap_edgeq[1]);
+    Q.cap_face = (uint32_t)(std::min(I.cap_faceq[0], I.cap_faceq[1]) / 3);
+    Q.cap_edge = (uint32_t)(std::min(I.cap_edgeq[0], I.cap_edgeq[1]) / 3);
     Q.cap_vert = (uint32_t)std::min(I.cap_vertq[0], I.cap_vertq[1]);
     Q.cells = I.raw;
     Q.n_cells = I.d_count + 8;
@@ -1937,16 +2024,16 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
     // changed items' cells) and their output is kept for the next updates.
     constexpr int LC = MESH_TOP_LEVELS;
     if (!I.d_top_count) {
-      MCK(pool_alloc((void **)&I.d_top_count, 5 * sizeof(uint32_t), s));
-      MCK(cudaMallocHost((void **)&I.h_top_count, 5 * sizeof(uint32_t)));
-      I.h_top_count[4] = 1;
+      MCK(pool_alloc((void **)&I.d_top_count, (QK + 1) * sizeof(uint32_t), s));
+      MCK(cudaMallocHost((void **)&I.h_top_count, (QK + 1) * sizeof(uint32_t)));
+      I.h_top_count[QK] = 1;
     }
     TopCache T;
     T.cellq = I.top_cellq;
     T.faceq = I.top_faceq;
     T.edgeq = I.top_edgeq;
     T.vertq = I.top_vertq;
-    for (int k = 0; k < 4; k++) T.cap[k] = (uint32_t)I.cap_top[k];
+    for (int k = 0; k < 4; k++) T.cap[k] = (uint32_t)(k == 1 || k == 2 ? I.cap_top[k] / 3 : I.cap_top[k]);
     T.count = I.d_top_count;
     const bool use_top = incr && I.top_valid && !in.top_changed;
     const int lv0 = use_top ? LC : 0;
@@ -1956,25 +2043,28 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
       size_t most = 1, cells_most = 1;
       for (int k = 0; k < LC; k++) most *= 27, cells_most *= 8;
       MCK(grow_buf(I.top_cellq, I.cap_top[0], std::min(want[0], cells_most), s));
-      MCK(grow_buf(I.top_faceq, I.cap_top[1], std::min(want[1], most), s));
-      MCK(grow_buf(I.top_edgeq, I.cap_top[2], std::min(want[2], most), s));
+      MCK(grow_buf(I.top_faceq, I.cap_top[1], 3 * std::min(want[1], most), s));
+      MCK(grow_buf(I.top_edgeq, I.cap_top[2], 3 * std::min(want[2], most), s));
       MCK(grow_buf(I.top_vertq, I.cap_top[3], std::min(want[3], most), s));
       T.cellq = I.top_cellq;
       T.faceq = I.top_faceq;
       T.edgeq = I.top_edgeq;
       T.vertq = I.top_vertq;
-      for (int k = 0; k < 4; k++) T.cap[k] = (uint32_t)I.cap_top[k];
+      for (int k = 0; k < 4; k++) T.cap[k] = (uint32_t)(k == 1 || k == 2 ? I.cap_top[k] / 3 : I.cap_top[k]);
     }
     I.gen_start_level = (uint32_t)lv0;
     if (use_top) {
       note_launch(1);
       k_load_top<<<148 * 2, 256, 0, s>>>(Q, LC, T);
     }
-    // a chain cell -> face -> edge -> vertex adds up to three levels below
-    // the octree's depth; more levels run if items are left
+    // An item of level l holds slots of depth l at most, and it expands only
+    // if one of them is subdivided, so the last level with items is the
+    // depth of the finest slots (size 8, the finest leaf's brick): the first
+    // batch runs the levels down to it, and further ones only run if items
+    // are left all the same.
     int depth = 1;
     for (uint32_t h = in.n; h > 8; h >>= 1) depth++;
-    int lv = lv0, batch = std::max(depth + 4 - lv0, 4);
+    int lv = lv0, batch = std::max(depth - lv0, 1);
     bool leftover = true;
     while (leftover && lv < MAX_GEN_LEVELS) {
       const int end = std::min(lv + batch, MAX_GEN_LEVELS);
@@ -1988,7 +2078,8 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
         // an incremental update: about as many items as at this level last time
         if (incr && I.level_items_incr)
           bound = std::min<uint64_t>(bound, std::max<uint64_t>(2 * (uint64_t)I.level_items[lv], 8 * 128));
-        const int blocks = (int)std::min<uint64_t>(148 * 8, (bound + 127) / 128);
+        // (each of the QK queues' threads padded to whole warps)
+        const int blocks = (int)std::min<uint64_t>(148 * 8, (bound + 31 * QK + 127) / 128);
         g.expand_all = (incr && lv < LC) ? 1 : 0;
         k_gen_level<<<blocks, 128, 0, s>>>(g, Q, lv, in.n);
         if (!use_top && lv == LC - 1) {
@@ -2000,25 +2091,28 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
       MCK(cudaGetLastError());
       MCK(cudaMemcpyAsync(I.h_count, I.d_count, COUNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
       if (!use_top)
-        MCK(cudaMemcpyAsync(I.h_top_count, I.d_top_count, 5 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        MCK(cudaMemcpyAsync(I.h_top_count, I.d_top_count, (QK + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
       MCK(cudaStreamSynchronize(s));
-      const uint32_t *cl = I.h_count + LEVEL_COUNTS + 4 * lv;
-      leftover = cl[0] || cl[1] || cl[2] || cl[3];
+      const uint32_t *cl = I.h_count + LEVEL_COUNTS + QK * lv;
+      leftover = false;
+      for (int k = 0; k < QK; k++) leftover |= cl[k] != 0;
       if (I.h_count[9] & ERR_CELL_OVERFLOW) break;
-      batch = 4;
+      batch = 2;
     }
     const bool overflow = (I.h_count[9] & ERR_CELL_OVERFLOW) != 0;
     const uint32_t *hc = I.h_count;
     if (!use_top) {
       // kept if it fitted; else the cache grows to the level's size and is
       // filled by the next update that traverses the top levels
-      I.top_valid = !overflow && I.h_top_count[4] == 0 && lv > LC;
+      I.top_valid = !overflow && I.h_top_count[QK] == 0 && lv > LC;
       if (!I.top_valid && !overflow) {
-        const uint32_t *cl = hc + LEVEL_COUNTS + 4 * LC;
-        MCK(grow_buf(I.top_cellq, I.cap_top[0], (size_t)cl[0] + cl[0] / 4 + 256, s));
-        MCK(grow_buf(I.top_faceq, I.cap_top[1], (size_t)cl[1] + cl[1] / 4 + 256, s));
-        MCK(grow_buf(I.top_edgeq, I.cap_top[2], (size_t)cl[2] + cl[2] / 4 + 256, s));
-        MCK(grow_buf(I.top_vertq, I.cap_top[3], (size_t)cl[3] + cl[3] / 4 + 256, s));
+        const uint32_t *cl = hc + LEVEL_COUNTS + QK * LC;
+        const size_t nf = std::max({cl[QK_FACE], cl[QK_FACE + 1], cl[QK_FACE + 2]});
+        const size_t ne = std::max({cl[QK_EDGE], cl[QK_EDGE + 1], cl[QK_EDGE + 2]});
+        MCK(grow_buf(I.top_cellq, I.cap_top[0], (size_t)cl[QK_CELL] + cl[QK_CELL] / 4 + 256, s));
+        MCK(grow_buf(I.top_faceq, I.cap_top[1], 3 * (nf + nf / 4 + 256), s));
+        MCK(grow_buf(I.top_edgeq, I.cap_top[2], 3 * (ne + ne / 4 + 256), s));
+        MCK(grow_buf(I.top_vertq, I.cap_top[3], (size_t)cl[QK_VERT] + cl[QK_VERT] / 4 + 256, s));
       }
     }
     if (overflow) {
@@ -2026,11 +2120,17 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
       continue;
     }
     for (int k = 0; k < 5; k++) I.peak[k] = 0;
+    // (queue k's kind: cells, faces, edges, vertices)
     for (int l = 0; l <= lv; l++)
-      for (int k = 0; k < 4; k++) I.peak[k] = std::max<size_t>(I.peak[k], hc[LEVEL_COUNTS + 4 * l + k]);
+      for (int k = 0; k < QK; k++) {
+        const int kind = k == QK_CELL ? 0 : (k < QK_EDGE ? 1 : (k < QK_VERT ? 2 : 3));
+        I.peak[kind] = std::max<size_t>(I.peak[kind], hc[LEVEL_COUNTS + QK * l + k]);
+      }
     for (int l = 0; l <= MAX_GEN_LEVELS; l++) {
-      const uint32_t *c = hc + LEVEL_COUNTS + 4 * l;
-      I.level_items[l] = l <= lv ? c[0] + c[1] + c[2] + c[3] : 0u;
+      const uint32_t *c = hc + LEVEL_COUNTS + QK * l;
+      uint32_t items = 0;
+      for (int k = 0; k < QK; k++) items += c[k];
+      I.level_items[l] = l <= lv ? items : 0u;
     }
     I.level_items_incr = incr;
     I.peak[4] = hc[8];
