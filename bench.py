@@ -81,7 +81,7 @@ STAGE_KERNELS = {
     "insert": "k_insert",
     "finalize": "k_finalize_bitmap",
     "fuse": "k_fuse",
-    "mesh_cells": "k_keep_cells+k_gen_level+k_cell_keys+argsort (k_sort_small or k_rs_*)+k_merge_cells/k_gather_cells",
+    "mesh_cells": "k_keep_cells+k_gen_levels+k_cell_keys+argsort (k_sort_small or k_rs_*)+k_merge_cells/k_gather_cells",
     "mesh_count": "k_mesh_lattice<count>+k_mesh_corner<count>",
     "mesh_emit": "k_mesh_lattice<emit>+k_mesh_corner<emit>+k_copy_clean",
     "confidence": "k_cnn_features+k_conv x3 (learned weight)",
@@ -96,7 +96,7 @@ STAGE_BYTES = {
     "finalize": "8 B per new brick",
     "fuse": "14,336 B per queued brick per frame (512 voxels x (4 SDF + 4 weight + 6 colour) B, read and written; "
             "10,240 B with FP16 storage)",
-    "mesh_cells": "48 B per cell read or written: the previous list read by the keep test, each new cell written "
+    "mesh_cells": "44 B per cell read or written: the previous list read by the keep test, each new cell written "
                   "by the octree traversal and read by the merge, the kept cells read by the merge, the list written",
     "mesh_count": "SDF and weight (8 B, 4 B FP16) of every sample of the re-meshed cells",
     "mesh_emit": "14 B (10 B FP16) per sample read + 15 B per vertex + 12 B per face written",

@@ -2227,6 +2227,7 @@ ff_status ff_update_meshes(ff_handle *h, int *updated) {
   in.grows = h->grows;
   in.full_cells = h->full_cells;
   in.top_changed = h->top_changed;
+  in.spin_limit = h->spin_limit;
   in.frame = h->frames;
   in.n = h->n;
   for (int r = 0; r < 3; r++) in.offset[r] = h->offset[r];

@@ -47,6 +47,7 @@ enum : uint32_t {
   ERR_DEDUPE_TIMEOUT = 128u,  // a grid barrier of the de-duplication gave up (nothing was inserted)
   ERR_SEQ_HALT = 256u,        // an earlier frame of a sequence must grow the volume or failed: not run
   ERR_CELL_MERGE = 512u,      // the kept and the new mesh cells share a sort key (the update is redone in full)
+  ERR_CELL_TIMEOUT = 1024u,   // a grid barrier of the mesh-cell traversal gave up
 };
 
 // Error bits after which a frame's voxel update is skipped: its allocation

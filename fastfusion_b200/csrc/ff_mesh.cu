@@ -95,6 +95,8 @@ struct Cell {
   uint16_t pad;
   uint32_t L[8];
 };
+static_assert(sizeof(Cell) == 44, "mesh cell layout");
+static_assert(sizeof(Slot) == 16, "traversal slot layout");
 
 // Work items of the traversal.  Faces and edges are queued per axis (the
 // queue gives the axis), so the lanes of a warp expand items of one kind and
@@ -154,6 +156,21 @@ struct GenCtx {
   // cache: every item is expanded, but only changed items emit cells
   int expand_all;
 };
+
+// Queue reads bypass L1: in the one-launch traversal a block reads the items
+// that other blocks wrote during the previous level, into a buffer whose
+// lines its SM may still hold from two levels before.
+__device__ __forceinline__ Slot ld_slot(const Slot *p) {
+  const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(p));
+  Slot s;
+  s.S = v.x;
+  s.la = v.y;
+  s.o[0] = (uint16_t)(v.z & 0xffffu);
+  s.o[1] = (uint16_t)(v.z >> 16);
+  s.o[2] = (uint16_t)(v.w & 0xffffu);
+  s.size = (uint16_t)(v.w >> 16);
+  return s;
+}
 
 // the octree is read-only while the mesh is built: reads go through the
 // read-only data cache
@@ -544,20 +561,25 @@ __device__ __forceinline__ void cell_item(const GenCtx &g, const GenQueues &Q, c
 
 template <int AX>
 __device__ __forceinline__ void face_at(const GenCtx &g, const GenQueues &Q, const Out &O, int cur, uint32_t j) {
-  const FaceItem f = Q.faceq[cur][(size_t)AX * Q.cap_face + j];
-  const bool changed = slot_changed(g, f.a) || slot_changed(g, f.b);
+  const FaceItem *f = Q.faceq[cur] + (size_t)AX * Q.cap_face + j;
+  const Slot a = ld_slot(&f->a), b = ld_slot(&f->b);
+  const bool changed = slot_changed(g, a) || slot_changed(g, b);
   if (!changed && !g.expand_all) return;
-  face_item<AX>(g, Q, O, f.a, f.b, changed);
+  face_item<AX>(g, Q, O, a, b, changed);
 }
 
 template <int E>
 __device__ __forceinline__ void edge_at(const GenCtx &g, const GenQueues &Q, const Out &O, int cur, uint32_t j) {
-  const EdgeItem e = Q.edgeq[cur][(size_t)E * Q.cap_edge + j];
+  const EdgeItem *e = Q.edgeq[cur] + (size_t)E * Q.cap_edge + j;
+  Slot S4[4];
   bool changed = false;
 #pragma unroll
-  for (int k = 0; k < 4; k++) changed |= slot_changed(g, e.s[k]);
+  for (int k = 0; k < 4; k++) {
+    S4[k] = ld_slot(&e->s[k]);
+    changed |= slot_changed(g, S4[k]);
+  }
   if (!changed && !g.expand_all) return;
-  edge_item<E>(g, Q, O, e.s, changed);
+  edge_item<E>(g, Q, O, S4, changed);
 }
 
 // Items of level `lv` (queue buffer lv & 1, counters lvl + QK lv) expand into
@@ -574,7 +596,7 @@ __device__ __forceinline__ void gen_level(const GenCtx &g, const GenQueues &Q, i
 #pragma unroll
   for (int k = 0; k < QK; k++) {
     const uint32_t cap = k == QK_CELL ? Q.cap_cell : (k < QK_EDGE ? Q.cap_face : (k < QK_VERT ? Q.cap_edge : Q.cap_vert));
-    c[k] = root ? (k == QK_CELL ? 1u : 0u) : min(cnt[k], cap);
+    c[k] = root ? (k == QK_CELL ? 1u : 0u) : min(__ldcg(cnt + k), cap);
     acc += (c[k] + 31u) & ~31u;
     e[k] = acc;
   }
@@ -594,7 +616,7 @@ __device__ __forceinline__ void gen_level(const GenCtx &g, const GenQueues &Q, i
           C[co].la = lf < g.leaves_max ? lf : BRANCHINIT;
         }
       } else {
-        const Slot s = Q.cellq[cur][i];
+        const Slot s = ld_slot(Q.cellq[cur] + i);
         if (!g.expand_all && !slot_changed(g, s)) continue;
         for (int co = 0; co < 8; co++) C[co] = child_of(g, s, co);
       }
@@ -612,18 +634,18 @@ __device__ __forceinline__ void gen_level(const GenCtx &g, const GenQueues &Q, i
     } else if (i < e[6]) {
       if (i - e[5] < c[6]) edge_at<2>(g, Q, O, cur, i - e[5]);
     } else if (i - e[6] < c[7]) {
-      const VertItem v = Q.vertq[cur][i - e[6]];
+      const VertItem *v = Q.vertq[cur] + (i - e[6]);
+      Slot S8[8];
       bool changed = false;
 #pragma unroll
-      for (int j = 0; j < 8; j++) changed |= slot_changed(g, v.s[j]);
+      for (int j = 0; j < 8; j++) {
+        S8[j] = ld_slot(&v->s[j]);
+        changed |= slot_changed(g, S8[j]);
+      }
       if (!changed && !g.expand_all) continue;
-      vert_item(g, Q, O, v.s, changed);
+      vert_item(g, Q, O, S8, changed);
     }
   }
-}
-
-__global__ void __launch_bounds__(128, 4) k_gen_level(GenCtx g, GenQueues Q, int lv, uint32_t n) {
-  gen_level(g, Q, lv, n);
 }
 
 // The items of traversal level MESH_TOP_LEVELS, kept from one update to the
@@ -639,8 +661,21 @@ struct TopCache {
   uint32_t *count;  // the QK queues' items; [QK]: 1 if they did not fit
 };
 
-__global__ void k_save_top(GenQueues Q, int lv, TopCache T) {
-  const uint32_t *c = Q.lvl + QK * lv;
+// n items of `words` 16-byte words each, read past L1 (see ld_slot)
+__device__ __forceinline__ void copy_items(void *dst, const void *src, uint32_t n, int words, uint32_t t0,
+                                           uint32_t stride) {
+  uint4 *d = reinterpret_cast<uint4 *>(dst);
+  const uint4 *q = reinterpret_cast<const uint4 *>(src);
+  const size_t total = (size_t)n * (size_t)words;
+  for (size_t i = t0; i < total; i += stride) d[i] = __ldcg(q + i);
+}
+
+// Keep level lv's items (complete once level lv - 1 has run), every thread of
+// the grid taking part.
+__device__ void save_top(const GenQueues &Q, int lv, const TopCache &T) {
+  const uint32_t *cp = Q.lvl + QK * lv;
+  uint32_t c[QK];
+  for (int k = 0; k < QK; k++) c[k] = __ldcg(cp + k);
   const int b = lv & 1;
   bool fits = c[0] <= T.cap[0] && c[0] <= Q.cap_cell && c[7] <= T.cap[3] && c[7] <= Q.cap_vert;
   for (int k = 0; k < 3; k++) {
@@ -653,14 +688,12 @@ __global__ void k_save_top(GenQueues Q, int lv, TopCache T) {
     T.count[QK] = fits ? 0u : 1u;
   }
   if (!fits) return;
-  for (uint32_t i = t0; i < c[0]; i += stride) T.cellq[i] = Q.cellq[b][i];
+  copy_items(T.cellq, Q.cellq[b], c[0], 1, t0, stride);
   for (int k = 0; k < 3; k++) {
-    for (uint32_t i = t0; i < c[QK_FACE + k]; i += stride)
-      T.faceq[(size_t)k * T.cap[1] + i] = Q.faceq[b][(size_t)k * Q.cap_face + i];
-    for (uint32_t i = t0; i < c[QK_EDGE + k]; i += stride)
-      T.edgeq[(size_t)k * T.cap[2] + i] = Q.edgeq[b][(size_t)k * Q.cap_edge + i];
+    copy_items(T.faceq + (size_t)k * T.cap[1], Q.faceq[b] + (size_t)k * Q.cap_face, c[QK_FACE + k], 2, t0, stride);
+    copy_items(T.edgeq + (size_t)k * T.cap[2], Q.edgeq[b] + (size_t)k * Q.cap_edge, c[QK_EDGE + k], 4, t0, stride);
   }
-  for (uint32_t i = t0; i < c[7]; i += stride) T.vertq[i] = Q.vertq[b][i];
+  copy_items(T.vertq, Q.vertq[b], c[7], 8, t0, stride);
 }
 
 // (the cache's counts fit the queues: the queues only grow while it is valid)
@@ -679,6 +712,62 @@ __global__ void k_load_top(GenQueues Q, int lv, TopCache T) {
       Q.edgeq[b][(size_t)k * Q.cap_edge + i] = T.edgeq[(size_t)k * T.cap[2] + i];
   }
   for (uint32_t i = t0; i < T.count[7]; i += stride) Q.vertq[b][i] = T.vertq[i];
+}
+
+// One launch runs the traversal levels [lv0, lv_end): a grid barrier between
+// two levels (bounded: it gives up after spin_limit polls and sets
+// ERR_CELL_TIMEOUT), the top levels' items kept when level save_level is
+// complete, and an early end at the first level without items.  Each level
+// is a handful of microseconds of dependent tree reads and queue claims, so
+// one launch per level would cost as much again in launch gaps.
+struct GenRun {
+  int lv0, lv_end;
+  int incr;
+  int save_level;  // level whose items are kept (TopCache), -1: none
+  uint32_t *bar;   // grid barrier: arrivals, generation (zero at the first launch)
+  uint32_t spin_limit;
+};
+
+constexpr int GEN_THREADS = 128;
+
+__global__ void __launch_bounds__(GEN_THREADS, 4) k_gen_levels(GenCtx g, GenQueues Q, GenRun R, uint32_t n,
+                                                               TopCache T) {
+  for (int lv = R.lv0; lv < R.lv_end; lv++) {
+    g.expand_all = (R.incr && lv < MESH_TOP_LEVELS) ? 1 : 0;
+    gen_level(g, Q, lv, n);
+    grid_barrier_bounded(R.bar, gridDim.x, Q.error, ERR_CELL_TIMEOUT, R.spin_limit);
+    if (__ldcg(Q.error) & ERR_CELL_TIMEOUT) return;
+    if (lv + 1 == R.save_level) save_top(Q, lv + 1, T);
+    // every block reads the same counts after the barrier
+    const uint32_t *c = Q.lvl + QK * (lv + 1);
+    uint32_t any = 0;
+    for (int k = 0; k < QK; k++) any |= __ldcg(c + k);
+    if (!any) {
+      // the levels below are empty too: so is the one to keep
+      if (R.save_level > lv + 1) save_top(Q, R.save_level, T);
+      return;
+    }
+  }
+}
+
+// Blocks of the one-launch traversal for levels of about `items` items:
+// one block per SM at least (the barrier's cost grows with the blocks), as
+// many as are resident at once at most (the grid must be co-resident);
+// 0 if the device cannot be queried.
+static int gen_blocks(size_t items) {
+  static int sms = 0, most = 0;
+  if (!most) {
+    int per_sm = 0, n = 0, dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gen_levels, GEN_THREADS, 0) != cudaSuccess ||
+        per_sm < 1 || n < 1)
+      return 0;
+    sms = n;
+    most = std::min(per_sm, 4) * n;
+  }
+  const size_t want = (items + GEN_THREADS - 1) / GEN_THREADS;
+  return (int)std::max<size_t>(sms, std::min<size_t>(want, most));
 }
 
 // Sort key of a cell: (type, log2 size, origin x, y, z), the order of the
@@ -1273,12 +1362,37 @@ struct CellOut {
   uint32_t nv, nf;
 };
 
+// A position k < 512 of a lattice of extents n0 (fastest) x n1 x n2 split
+// into its three coordinates.  The quotients are products with ceil(2^16 / d)
+// shifted right by 16, exact while k (d - 1) < 2^16 (k < 512, d <= 64 here):
+// the extents vary per cell, and a division by a value known only at run
+// time costs a long instruction sequence per lattice position.
+struct Lat3 {
+  uint32_t n0, n1, m0, m01;  // extents, multipliers for n0 and n0 n1
+};
+__device__ __forceinline__ uint32_t quot_mul(uint32_t d) { return d ? (65536u + d - 1u) / d : 0u; }
+__device__ __forceinline__ Lat3 lat3(int n0, int n1) {
+  Lat3 L;
+  L.n0 = (uint32_t)n0;
+  L.n1 = (uint32_t)n1;
+  L.m0 = quot_mul(L.n0);
+  L.m01 = quot_mul(L.n0 * L.n1);
+  return L;
+}
+__device__ __forceinline__ void split3(const Lat3 &L, int k, int &c0, int &c1, int &c2) {
+  const uint32_t q0 = ((uint32_t)k * L.m0) >> 16;   // k / n0
+  const uint32_t q01 = ((uint32_t)k * L.m01) >> 16;  // k / (n0 n1) = (k / n0) / n1
+  c0 = k - (int)(q0 * L.n0);
+  c1 = (int)(q0 - q01 * L.n1);
+  c2 = (int)q01;
+}
+
 // lattice-order position k -> lattice index, for the cell type's loop nesting
-__device__ __forceinline__ int lattice_idx(const CellGeom &G, int k, const int *n3, int &b0, int &b1, int &b2) {
+// (L: the extents in that nesting, fastest first)
+__device__ __forceinline__ int lattice_idx(const CellGeom &G, int k, const Lat3 &L, int &b0, int &b1, int &b2) {
   const uint8_t *ord = c_order[G.type];
-  const int i2 = k % n3[ord[2]];
-  const int i1 = (k / n3[ord[2]]) % n3[ord[1]];
-  const int i0 = k / (n3[ord[2]] * n3[ord[1]]);
+  int i0, i1, i2;
+  split3(L, k, i2, i1, i0);
   int bb[3];
   bb[ord[0]] = i0;
   bb[ord[1]] = i1;
@@ -1309,8 +1423,10 @@ __device__ __forceinline__ uint32_t next_cell(uint32_t *work, int lane) {
   return __shfl_sync(0xffffffffu, v, 0);
 }
 
+// (register caps: the count pass's 4.6 KB of scratch per warp leaves room
+// for 8 blocks per SM at 64 registers; the emit pass's 10.5 KB for 5)
 template <bool EMIT>
-__global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, const Cell *__restrict__ cells,
+__global__ void __launch_bounds__(32 * MESH_WARPS, EMIT ? 5 : 8) k_mesh_lattice(VoxSrc m, const Cell *__restrict__ cells,
                                                                   uint32_t first, uint32_t ncell,
                                                                   const uint32_t *__restrict__ list, const uint32_t *list_n, CellOut *out,
                                                                   const uint64_t *vbase, const uint64_t *fbase,
@@ -1347,6 +1463,9 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
     const int nsamp = n3[0] * n3[1] * n3[2];
     const int nc3[3] = {n3[0] - 1, n3[1] - 1, n3[2] - 1};
     const int ncube = nc3[0] * nc3[1] * nc3[2];
+    // (the lattices of samples and cubes are split by Lat3s made just
+    // before each loop: in memory order, or in the cell type's loop nesting)
+    const uint8_t *ord = c_order[G.type];
     // the count pass's marching-cubes case of every cube of this cell
     uint4 *const cell_cases = reinterpret_cast<uint4 *>(cases + (size_t)ci * 512);
     if (EMIT) {
@@ -1358,8 +1477,10 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
       for (int k = lane; k < 384; k += 32) reinterpret_cast<uint32_t *>(W.edge_set)[k] = 0;
       for (int k = lane; k < 128; k += 32) reinterpret_cast<uint32_t *>(W.wzero)[k] = 0;  // "needed" flags
       __syncwarp();
+      const Lat3 Lc = lat3(nc3[0], nc3[1]);
       for (int k = lane; k < ncube; k += 32) {
-        const int bx = k % nc3[0], by = (k / nc3[0]) % nc3[1], bz = k / (nc3[0] * nc3[1]);
+        int bx, by, bz;
+        split3(Lc, k, bx, by, bz);
         const int idx = (bz * 8 + by) * 8 + bx;
         const int ci8 = W.cube_case[idx];
         const int nt = mc_ntri(T, ci8);
@@ -1396,8 +1517,10 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
       __syncwarp();
     } else {
       bool fit = true;
+      const Lat3 Ls = lat3(n3[0], n3[1]);
       for (int k = lane; k < nsamp; k += 32) {
-        const int bx = k % n3[0], by = (k / n3[0]) % n3[1], bz = k / (n3[0] * n3[1]);
+        int bx, by, bz;
+        split3(Ls, k, bx, by, bz);
         Sample s;
         fit &= lattice_sample<false>(m, c, G, bx, by, bz, s);  // (no colour: the count pass needs none)
         const int si = (bz * 8 + by) * 8 + bx;
@@ -1412,8 +1535,11 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
         if (lane == 0) out[cid] = CellOut{0u, 0u};
         continue;
       }
+      uint32_t tri = 0;  // this lane's cubes' triangles
+      const Lat3 Lc = lat3(nc3[0], nc3[1]);
       for (int k = lane; k < ncube; k += 32) {
-        const int bx = k % nc3[0], by = (k / nc3[0]) % nc3[1], bz = k / (nc3[0] * nc3[1]);
+        int bx, by, bz;
+        split3(Lc, k, bx, by, bz);
         const int idx = (bz * 8 + by) * 8 + bx;
         const int off[8] = {0, 1, 9, 8, 64, 65, 73, 72};
         bool zero = false;
@@ -1426,6 +1552,7 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
         if (zero) ci8 = 0;
         W.cube_case[idx] = (uint8_t)ci8;
         const int nt = mc_ntri(T, ci8);
+        tri += (uint32_t)nt;
         for (int q = 0; q < 3 * nt; q++) {
           const int slot = 3 * idx + mc_slot(T, mc_edge(T, ci8, q));
           W.edge_set[slot] = 1;  // lanes that set the same slot store the same byte
@@ -1434,15 +1561,27 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
       __syncwarp();
       // kept for the emit pass (entries of cubes outside the lattice unused)
       cell_cases[lane] = reinterpret_cast<const uint4 *>(W.cube_case)[lane];
+      // The counts need no order: a vertex per edge slot that carries one
+      // (every such slot lies at a lattice sample, and the flags outside the
+      // lattice are clear), a face per triangle of the lattice's cubes.
+      uint32_t verts = 0;
+      for (int k = lane; k < 384; k += 32) verts += (uint32_t)__popc(reinterpret_cast<const uint32_t *>(W.edge_set)[k]);
+      verts = __reduce_add_sync(0xffffffffu, verts);
+      tri = __reduce_add_sync(0xffffffffu, tri);
+      if (lane == 0) out[cid] = CellOut{verts, tri};
+      __syncwarp();
+      continue;
     }
-    // vertices, in the reference's loop order of this cell type
+    // (the emit pass from here) vertices, in the reference's loop order of
+    // this cell type
     uint32_t vrun = 0;
     const uint64_t vb = EMIT ? vbase[cid] : 0;
+    const Lat3 Lso = lat3(n3[ord[2]], n3[ord[1]]);
     for (int k0 = 0; k0 < nsamp; k0 += 32) {
       const int k = k0 + lane;
       int b0 = 0, b1 = 0, b2 = 0, idx = 0, cntv = 0;
       if (k < nsamp) {
-        idx = lattice_idx(G, k, n3, b0, b1, b2);
+        idx = lattice_idx(G, k, Lso, b0, b1, b2);
         cntv = edge_bit(W, 3 * idx) + edge_bit(W, 3 * idx + 1) + edge_bit(W, 3 * idx + 2);
       }
       int tot;
@@ -1482,13 +1621,13 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
     // faces, cube by cube in the same nesting
     uint32_t frun = 0;
     const uint64_t fb = EMIT ? fbase[cid] : 0;
-    const int nc3o[3] = {nc3[0], nc3[1], nc3[2]};
+    const Lat3 Lco = lat3(nc3[ord[2]], nc3[ord[1]]);
     for (int k0 = 0; k0 < ncube; k0 += 32) {
       const int k = k0 + lane;
       int idx = 0, nt = 0, ci8 = 0;
       if (k < ncube) {
         int b0, b1, b2;
-        idx = lattice_idx(G, k, nc3o, b0, b1, b2);
+        idx = lattice_idx(G, k, Lco, b0, b1, b2);
         ci8 = W.cube_case[idx];
         nt = mc_ntri(T, ci8);
       }
@@ -1504,12 +1643,16 @@ __global__ void __launch_bounds__(32 * MESH_WARPS) k_mesh_lattice(VoxSrc m, cons
       }
       frun += (uint32_t)tot;
     }
-    if (!EMIT && lane == 0) out[cid] = CellOut{vrun, frun};
     __syncwarp();
   }
 }
 
-// addBrickMiddle_indexed_incremental: one thread per corner cell
+// addBrickMiddle_indexed_incremental: eight lanes per corner cell, one per
+// sample (the samples' parent-leaf walks are chains of dependent loads: in
+// one thread they would run one after the other), then the cell's first lane
+// runs the single-cube marching cubes on the gathered samples.
+constexpr int CORNER_LANES = 8;
+
 template <bool EMIT>
 __global__ void k_mesh_corner(VoxSrc m, const Cell *__restrict__ cells, uint32_t first, uint32_t ncell,
                               const uint32_t *__restrict__ list, const uint32_t *list_n, CellOut *out,
@@ -1517,31 +1660,36 @@ __global__ void k_mesh_corner(VoxSrc m, const Cell *__restrict__ cells, uint32_t
                               uint32_t *faces) {
   __shared__ McTab T;
   load_mc(T);
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t i = t / CORNER_LANES;
+  const int k = (int)(t % CORNER_LANES);  // this lane's sample
+  const unsigned gmask = 0xffu << (threadIdx.x & 24u);
   if (i >= (list ? *list_n : ncell)) return;
   const uint32_t cid = list ? list[i] : first + i;
   const Cell c = cells[cid];
   if (!owns_cell(m, c)) {
-    if (!EMIT) out[cid] = CellOut{0u, 0u};
+    if (!EMIT && k == 0) out[cid] = CellOut{0u, 0u};
     return;
   }
-  int stretch = m.leaf[c.L[0]].w;
-  for (int k = 1; k < 7; k++) stretch = max(stretch, (int)m.leaf[c.L[k]].w);
+  // the largest leaf scale of sides 0-6
+  int stretch = k < 7 ? (int)m.leaf[c.L[k]].w : 0;
+#pragma unroll
+  for (int o = 1; o < CORNER_LANES; o <<= 1) stretch = max(stretch, __shfl_xor_sync(gmask, stretch, o, CORNER_LANES));
   if (stretch > c.size) {
-    if (!EMIT) out[cid] = CellOut{0u, 0u};
+    if (!EMIT && k == 0) out[cid] = CellOut{0u, 0u};
     return;
   }
-  atomicAdd(m.samples, 8ull);
-  float d[8], w[8];
-  uint16_t col[8][3];
-  for (int k = 0; k < 8; k++) {
+  {
+    const unsigned act = __activemask();
+    if ((threadIdx.x & 31u) == (unsigned)(__ffs(act) - 1)) atomicAdd(m.samples, (unsigned long long)__popc(act));
+  }
+  float dk = 0.0f, wk = 0.0f;
+  uint16_t ck[3] = {0, 0, 0};
+  {
     int p[3];
     for (int r = 0; r < 3; r++) p[r] = ((k >> r) & 1) ? c.o[r] + c.size : c.o[r] + c.size - stretch;
-    w[k] = 0.0f;
-    d[k] = 0.0f;
-    col[k][0] = col[k][1] = col[k][2] = 0;
     int guard = 0;
-    for (uint32_t leaf = c.L[k]; leaf < BRANCHINIT && w[k] <= 0.0f && guard < 64; leaf = m.parent[leaf], guard++) {
+    for (uint32_t leaf = c.L[k]; leaf < BRANCHINIT && wk <= 0.0f && guard < 64; leaf = m.parent[leaf], guard++) {
       if (leaf >= m.leaves_used) break;
       const ushort4 lo = m.leaf[leaf];
       const int ls = lo.w;
@@ -1549,11 +1697,26 @@ __global__ void k_mesh_corner(VoxSrc m, const Cell *__restrict__ cells, uint32_t
       const uint16_t ly = (uint16_t)(((int)(uint16_t)p[1] - (int)lo.y) / ls);
       const uint16_t lz = (uint16_t)(((int)(uint16_t)p[2] - (int)lo.z) / ls);
       const size_t vi = vox_index(m, leaf, lx, ly, lz);
-      w[k] = __fadd_rn(w[k], vw(m, vi));
-      d[k] = vd(m, vi);
-      for (int r = 0; r < 3; r++) col[k][r] = vcs<EMIT>(m, vi, r);  // (the count pass needs no colour)
+      wk = __fadd_rn(wk, vw(m, vi));
+      dk = vd(m, vi);
+      for (int r = 0; r < 3; r++) ck[r] = vcs<EMIT>(m, vi, r);  // (the count pass needs no colour)
     }
   }
+  // every lane of the cell gets all eight samples
+  float d[8], w[8];
+  uint16_t col[8][3];
+  const uint32_t ck01 = (uint32_t)ck[0] | ((uint32_t)ck[1] << 16);
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    d[j] = __shfl_sync(gmask, dk, j, CORNER_LANES);
+    w[j] = __shfl_sync(gmask, wk, j, CORNER_LANES);
+    const uint32_t a01 = __shfl_sync(gmask, ck01, j, CORNER_LANES);
+    const uint32_t a2 = __shfl_sync(gmask, (uint32_t)ck[2], j, CORNER_LANES);
+    col[j][0] = (uint16_t)(a01 & 0xffffu);
+    col[j][1] = (uint16_t)(a01 >> 16);
+    col[j][2] = (uint16_t)a2;
+  }
+  if (k != 0) return;
   const int mcv[8] = {0, 1, 3, 2, 4, 5, 7, 6};
   float val[8];
   bool zero = false;
@@ -1917,10 +2080,6 @@ struct MeshImpl {
   uint32_t *d_top_count = nullptr, *h_top_count = nullptr;
   bool top_valid = false;
   uint32_t gen_start_level = 0;  // the last update's first traversed level (statistics)
-  // items per traversal level of the last update (sizes the next update's
-  // launches: an incremental update's deeper levels hold few items)
-  uint32_t level_items[MAX_GEN_LEVELS + 1] = {};
-  bool level_items_incr = false;
 };
 
 static MeshImpl &impl(MeshState &m) {
@@ -1950,6 +2109,8 @@ static int key_bits_for(uint32_t n) {
 // Cell words of the counter array (d_count) used by the incremental list:
 // cells kept, and kept before the previous list's first corner cell.
 constexpr int KEPT_WORD = 20;
+// d_count words 24, 25: the grid barrier of the one-launch traversal
+constexpr int GEN_BARRIER_WORD = 24;
 
 static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStream_t s, uint32_t &ncells,
                           std::string &err) {
@@ -2006,7 +2167,7 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
     g.prev_leaves = I.prev_leaves;
     g.prev_branches = I.prev_branches;
     g.incr = incr ? 1 : 0;
-    g.expand_all = 0;
+    g.expand_all = 0;  // (set per level by the traversal)
     if (incr) {
       // the previous cells whose sides did not change, and their positions
       // among the kept (words KEPT_WORD, KEPT_WORD + 1: kept, kept before the
@@ -2068,26 +2229,26 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
     bool leftover = true;
     while (leftover && lv < MAX_GEN_LEVELS) {
       const int end = std::min(lv + batch, MAX_GEN_LEVELS);
-      note_launch((unsigned)(end - lv));
-      for (; lv < end; lv++) {
-        // an item expands into at most 27 (8 cells, 12 faces, 6 edges, 1
-        // vertex), so level l holds at most 27^l items: the first levels
-        // need few blocks (the loop inside strides over any grid)
-        uint64_t bound = 1;
-        for (int k = 0; k < lv && bound < (uint64_t)148 * 8 * 128; k++) bound *= 27;
-        // an incremental update: about as many items as at this level last time
-        if (incr && I.level_items_incr)
-          bound = std::min<uint64_t>(bound, std::max<uint64_t>(2 * (uint64_t)I.level_items[lv], 8 * 128));
-        // (each of the QK queues' threads padded to whole warps)
-        const int blocks = (int)std::min<uint64_t>(148 * 8, (bound + 31 * QK + 127) / 128);
-        g.expand_all = (incr && lv < LC) ? 1 : 0;
-        k_gen_level<<<blocks, 128, 0, s>>>(g, Q, lv, in.n);
-        if (!use_top && lv == LC - 1) {
-          // level LC's items are complete now: keep them
-          note_launch(1);
-          k_save_top<<<148 * 2, 256, 0, s>>>(Q, LC, T);
-        }
+      // the widest level of the last update (an incremental update's levels
+      // hold few items), or as many blocks as fit for a full generation
+      const size_t widest = incr ? I.peak[0] + 3 * I.peak[1] + 3 * I.peak[2] + I.peak[3] : SIZE_MAX / 2;
+      const int blocks = gen_blocks(widest);
+      if (!blocks) {
+        err = "meshing: no resident blocks for the cell generation";
+        return 2;
       }
+      GenRun R;
+      R.lv0 = lv;
+      R.lv_end = end;
+      R.incr = incr ? 1 : 0;
+      // level LC's items are complete once level LC - 1 has run: keep them
+      R.save_level = (!use_top && lv < LC && LC <= end) ? LC : -1;
+      R.bar = I.d_count + GEN_BARRIER_WORD;
+      R.spin_limit = in.spin_limit;
+      void *args[] = {&g, &Q, &R, (void *)&in.n, &T};
+      note_launch(1);
+      MCK(cudaLaunchCooperativeKernel((const void *)k_gen_levels, dim3(blocks), dim3(GEN_THREADS), args, 0, s));
+      lv = end;
       MCK(cudaGetLastError());
       MCK(cudaMemcpyAsync(I.h_count, I.d_count, COUNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
       if (!use_top)
@@ -2096,8 +2257,16 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
       const uint32_t *cl = I.h_count + LEVEL_COUNTS + QK * lv;
       leftover = false;
       for (int k = 0; k < QK; k++) leftover |= cl[k] != 0;
-      if (I.h_count[9] & ERR_CELL_OVERFLOW) break;
+      if (I.h_count[9] & (ERR_CELL_OVERFLOW | ERR_CELL_TIMEOUT)) break;
       batch = 2;
+    }
+    if (I.h_count[9] & ERR_CELL_TIMEOUT) {
+      // the traversal stopped part way: nothing of this update is used (the
+      // previous list and state stay as they were); the top-level items are
+      // traversed again next time
+      I.top_valid = false;
+      err = "meshing: a grid barrier of the cell generation gave up (spin limit)";
+      return 5;
     }
     const bool overflow = (I.h_count[9] & ERR_CELL_OVERFLOW) != 0;
     const uint32_t *hc = I.h_count;
@@ -2126,13 +2295,6 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
         const int kind = k == QK_CELL ? 0 : (k < QK_EDGE ? 1 : (k < QK_VERT ? 2 : 3));
         I.peak[kind] = std::max<size_t>(I.peak[kind], hc[LEVEL_COUNTS + QK * l + k]);
       }
-    for (int l = 0; l <= MAX_GEN_LEVELS; l++) {
-      const uint32_t *c = hc + LEVEL_COUNTS + QK * l;
-      uint32_t items = 0;
-      for (int k = 0; k < QK; k++) items += c[k];
-      I.level_items[l] = l <= lv ? items : 0u;
-    }
-    I.level_items_incr = incr;
     I.peak[4] = hc[8];
     if (leftover) {
       err = "meshing: cell generation did not finish within the level limit";
@@ -2224,7 +2386,7 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   const uint32_t n_old_cells = incr_cells ? I.n_old : 0u;
   int rc = generate_cells(I, in, incr_cells, s, ncells, err);
   if (rc) return rc;
-  // 48 B per cell read or written: the previous list read by the keep test,
+  // sizeof(Cell) = 44 B per cell read or written: the previous list read by the keep test,
   // the new cells written by the traversal and read by the gather or merge,
   // the kept cells read by the merge, the list written
   P.end(pi, (double)sizeof(Cell) * ((double)n_old_cells + 2.0 * I.n_new + I.n_kept + ncells), s);
@@ -2295,7 +2457,7 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
                                                                     I.d_count + 14, I.out, nullptr, nullptr, nullptr,
                                                                     nullptr, nullptr, I.d_count + 16, I.cases);
   if (ncells > first_corner)
-    k_mesh_corner<false><<<(ncells - first_corner + 127) / 128, 128, 0, s>>>(
+    k_mesh_corner<false><<<((ncells - first_corner) * CORNER_LANES + 127) / 128, 128, 0, s>>>(
         vs, I.cells, first_corner, ncells - first_corner, cor_list, I.d_count + 15, I.out, nullptr, nullptr, nullptr,
         nullptr, nullptr);
   const int pi_count = pi;
@@ -2364,7 +2526,7 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
                                                                    I.d_count + 14, I.out, I.vbase, I.fbase, M.d_xyz,
                                                                    M.d_rgb, M.d_faces, I.d_count + 17, I.cases);
   if (ncells > first_corner)
-    k_mesh_corner<true><<<(ncells - first_corner + 127) / 128, 128, 0, s>>>(
+    k_mesh_corner<true><<<((ncells - first_corner) * CORNER_LANES + 127) / 128, 128, 0, s>>>(
         vs, I.cells, first_corner, ncells - first_corner, cor_list, I.d_count + 15, I.out, I.vbase, I.fbase, M.d_xyz,
         M.d_rgb, M.d_faces);
   if (incremental && ncells)
@@ -2562,7 +2724,7 @@ void mesh_invalidate(MeshState &M) {
 void mesh_note_frame(MeshState &) {}
 
 cudaError_t prewarm_mesh_kernels() {
-  const void *fns[] = {(const void *)k_gen_level,          (const void *)k_cell_keys,
+  const void *fns[] = {(const void *)k_gen_levels,         (const void *)k_cell_keys,
                        (const void *)k_gather_cells,       (const void *)k_mesh_lattice<false>,
                        (const void *)k_mesh_lattice<true>, (const void *)k_mesh_corner<false>,
                        (const void *)k_mesh_corner<true>,  (const void *)k_mark_dirty,
@@ -2571,7 +2733,7 @@ cudaError_t prewarm_mesh_kernels() {
                        (const void *)k_fill_counts_from_old, (const void *)k_export_cells,
                        (const void *)k_keep_cells,         (const void *)k_keep_tile_scan,
                        (const void *)k_keep_apply,         (const void *)k_merge_cells,
-                       (const void *)k_save_top,           (const void *)k_load_top};
+                       (const void *)k_load_top};
   for (const void *f : fns) {
     cudaFuncAttributes a;
     cudaError_t e = cudaFuncGetAttributes(&a, f);

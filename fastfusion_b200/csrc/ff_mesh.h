@@ -28,6 +28,7 @@ struct MeshInputs {
   uint32_t grows = 0;   // volume growths so far (a growth moves every cell)
   int full_cells = 0;   // regenerate every cell instead of the changed ones
   bool top_changed = true;  // a frame since the last update created something near the root
+  uint32_t spin_limit = SPIN_LIMIT;  // bound of the traversal's grid barriers (polls)
   uint32_t frame;
   uint32_t n;
   float offset[3];

@@ -511,9 +511,9 @@ class FusionMipMapCPU:
         self._check(self._L.ff_set_update_batch(self._h, int(frames)))
 
     def set_spin_limit(self, iterations: int = SPIN_LIMIT_DEFAULT):
-        """Bound of the device-side waits of this map's frames (polling
-        iterations; 0: a wait gives up at once and the frame reports
-        FF_ERR_TIMEOUT)."""
+        """Bound of the device-side waits of this map's frames and mesh
+        updates (polling iterations; 0: a wait gives up at once and the call
+        reports FF_ERR_TIMEOUT)."""
         self._check(self._L.ff_set_spin_limit(self._h, int(iterations)))
 
     def set_cell_generation(self, mode: int = CELLS_INCREMENTAL):

@@ -284,14 +284,16 @@ ff_status ff_set_tuning(ff_handle *h, const ff_tuning *t);
 #define FF_UPDATE_BATCH_MAX 32
 ff_status ff_set_update_batch(ff_handle *h, int frames);
 
-/* Bound of every device-side wait of this map's frames (the grid barriers of
- * the de-duplication, the lock wait of the octree insert), in polling
- * iterations; default FF_SPIN_LIMIT_DEFAULT.  A wait that runs out sets an
- * error flag and returns instead of waiting on; the call then returns
- * FF_ERR_TIMEOUT: after a de-duplication wait the frame is left out and the
- * map is as it was before the call; after an insert wait the bricks found so
- * far are allocated but the frame's voxel update is skipped.  The handle
- * stays usable either way.  No counterpart in the reference (its traversal
+/* Bound of every device-side wait of this map (the grid barriers of the
+ * de-duplication and of the mesh-cell traversal, the lock wait of the octree
+ * insert), in polling iterations; default FF_SPIN_LIMIT_DEFAULT.  A wait
+ * that runs out sets an error flag and returns instead of waiting on; the
+ * call then returns FF_ERR_TIMEOUT: after a de-duplication wait the frame is
+ * left out and the map is as it was before the call; after an insert wait
+ * the bricks found so far are allocated but the frame's voxel update is
+ * skipped; after a traversal wait ff_update_meshes leaves the mesh of the
+ * previous update, and the next update meshes every change since then.  The
+ * handle stays usable either way.  No counterpart in the reference (its traversal
  * is sequential and has no waits). */
 #define FF_SPIN_LIMIT_DEFAULT (1u << 22)
 ff_status ff_set_spin_limit(ff_handle *h, uint32_t iterations);

@@ -2,7 +2,8 @@
 
 Every device-side wait of the fusion path is bounded.  These tests make a
 wait run out on purpose -- a spin limit of zero, so a grid barrier of the
-de-duplication gives up at its first poll -- or inject, from the host, the
+de-duplication or of the mesh-cell traversal gives up at its first poll --
+or inject, from the host, the
 error word the confidence network sets when one of its waits gives up.  No
 kernel faults, traps or hangs: a wait that runs out sets a flag and returns.
 Each test checks that the call reports FF_ERR_TIMEOUT with a message, that
@@ -40,6 +41,49 @@ def _same_map(g, p):
     assert np.array_equal(dg.view(np.uint32), dp.view(np.uint32))
     assert np.array_equal(wg.view(np.uint32), wp.view(np.uint32))
     assert np.array_equal(cg, cp)
+
+
+def test_mesh_traversal_wait_runs_out_and_next_update_recovers(lib_built):
+    """Spin limit 0 during updateMeshes: a grid barrier of the mesh-cell
+    traversal gives up, the call returns FF_ERR_TIMEOUT and nothing of that
+    update is used; at the default limit the same handle's next updates give
+    the cells and mesh of a map that never failed."""
+    from fastfusion_b200.fusion import FFError, FusionMipMapCPU, SPIN_LIMIT_DEFAULT
+    K, frames = circle_frames(1, 12, 320, 240)
+    a = FusionMipMapCPU(0, 0, 0, 0.005, 0.01, 0, True, leaves_max=271420, branches_max=4793488, rcp="exact")
+    b = FusionMipMapCPU(0, 0, 0, 0.005, 0.01, 0, True, leaves_max=271420, branches_max=4793488, rcp="exact")
+
+    def fuse(ks):
+        for k in ks:
+            depth, bgr, R, t = frames[k]
+            assert a.addMap(depth, _cam(K, R, t), bgr, SCALING, MAXCAM) == b.addMap(depth, _cam(K, R, t), bgr,
+                                                                                     SCALING, MAXCAM)
+
+    def same():
+        ca, ra = a.mesh_cells()
+        cb, rb = b.mesh_cells()
+        assert np.array_equal(ca, cb) and np.array_equal(ra, rb)
+        ma, mb = a.getMeshInterleavedMarchingCubes(), b.getMeshInterleavedMarchingCubes()
+        assert len(ma.faces) > 0
+        assert np.array_equal(ma.vertices.view(np.uint32), mb.vertices.view(np.uint32))
+        assert np.array_equal(ma.colors, mb.colors) and np.array_equal(ma.faces, mb.faces)
+
+    fuse(range(0, 4))
+    assert a.updateMeshes() and b.updateMeshes()
+    same()
+    fuse(range(4, 8))
+    a.set_spin_limit(0)
+    with pytest.raises(FFError) as e:
+        a.updateMeshes()
+    assert e.value.status == 5 and "gave up" in str(e.value)
+    a.set_spin_limit(SPIN_LIMIT_DEFAULT)
+    assert a.updateMeshes() and b.updateMeshes()
+    same()
+    fuse(range(8, 12))
+    assert a.updateMeshes() and b.updateMeshes()
+    same()
+    a.close()
+    b.close()
 
 
 def test_dedupe_wait_runs_out_and_map_recovers(lib_built, port_lib):
