@@ -830,21 +830,38 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc
     }
   }
   // (the new leaves' parents: k_parents_frames, after this kernel)
-  __syncthreads();
   // Deferred update: the frame's queue is complete (the new leaves were
   // queued above); mark each queued brick with the frame's bit and list the
   // bricks no earlier frame of the pass has marked.  A frame the update must
   // not take (failed, or the volume must grow first) is left to the host.
-  const bool stand_aside = fuse_deferred(F);  // failed, or the volume must grow first
+  // One thread decides for the block: the confidence network, on another
+  // stream, may set its error word meanwhile, and the loop below claims list
+  // slots with warp-wide votes.
+  __shared__ int aside_flag;
+  if (t == 0) aside_flag = fuse_deferred(F) ? 1 : 0;
+  __syncthreads();
+  const bool stand_aside = aside_flag != 0;  // failed, or the volume must grow first
   if (F.upd_mask && !stand_aside) {
     const uint32_t nq = ld_volatile(&cnt->queued);
     const uint32_t bit = 1u << F.upd_slot;
-    for (uint32_t j = t; j < nq; j += FIN_THREADS) {
-      const uint32_t b = queue[j];
-      // a part of a sharded map updates the bricks it owns
-      if (F.shards > 1 && !owns_brick(F, leaf[b])) continue;
-      // (the queue holds each brick once, so the old mask lacks this bit)
-      if (atomicOr(&F.upd_mask[b], bit) == 0u) F.upd_list[atomicAdd(F.upd_count, 1u)] = b;
+    // (every thread of the block runs the same number of iterations, so the
+    // list slots are claimed with one atomic per warp)
+    const uint32_t rounds = (nq + FIN_THREADS - 1) / FIN_THREADS;
+    for (uint32_t it = 0; it < rounds; it++) {
+      const uint32_t j = it * FIN_THREADS + (uint32_t)t;
+      bool add = false;
+      uint32_t b = 0;
+      if (j < nq) {
+        b = queue[j];
+        // a part of a sharded map updates the bricks it owns; the queue holds
+        // each brick once, so the old mask lacks this bit
+        if (F.shards <= 1 || owns_brick(F, leaf[b])) add = atomicOr(&F.upd_mask[b], bit) == 0u;
+      }
+      const unsigned ball = __ballot_sync(0xffffffffu, add);
+      uint32_t at = 0;
+      if ((t & 31) == 0 && ball) at = atomicAdd(F.upd_count, (uint32_t)__popc(ball));
+      at = __shfl_sync(0xffffffffu, at, 0);
+      if (add) F.upd_list[at + __popc(ball & ((1u << (t & 31)) - 1u))] = b;
     }
   }
   if (t == 0) chain_next(F, cnt, leaves_before, stand_aside);

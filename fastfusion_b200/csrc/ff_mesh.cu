@@ -1162,7 +1162,10 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
   s.d = 0.0f;
   s.c[0] = s.c[1] = s.c[2] = 0;
   int guard = 0;
-  for (uint32_t leaf = first; leaf < BRANCHINIT && s.w <= 0.0f && guard < 64; leaf = m.parent[leaf], guard++) {
+  // (the parent is read only when the walk goes on: most samples settle at
+  // their first leaf)
+  for (uint32_t leaf = first; leaf < BRANCHINIT && s.w <= 0.0f && guard < 64;
+       leaf = s.w <= 0.0f ? m.parent[leaf] : BRANCHINIT, guard++) {
     if (leaf >= m.leaves_used) break;
     const ushort4 lo4 = m.leaf[leaf];
     const int lo[3] = {lo4.x, lo4.y, lo4.z};
@@ -1199,7 +1202,7 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
       } else {
         const uint16_t rem = (uint16_t)rm;
         rr[r] = pow2 ? __fmul_rn((float)rem, inv_ls) : __fdiv_rn((float)rem, (float)ls);
-        lh[r] = (uint16_t)(ll[r] + ((double)rr[r] > 0.0 && ll[r] < 7));
+        lh[r] = (uint16_t)(ll[r] + (rr[r] > 0.0f && ll[r] < 7));
       }
     }
     if (t == 0 && rr[0] == 0.0f && rr[1] == 0.0f && rr[2] == 0.0f) {
@@ -1689,7 +1692,8 @@ __global__ void k_mesh_corner(VoxSrc m, const Cell *__restrict__ cells, uint32_t
     int p[3];
     for (int r = 0; r < 3; r++) p[r] = ((k >> r) & 1) ? c.o[r] + c.size : c.o[r] + c.size - stretch;
     int guard = 0;
-    for (uint32_t leaf = c.L[k]; leaf < BRANCHINIT && wk <= 0.0f && guard < 64; leaf = m.parent[leaf], guard++) {
+    for (uint32_t leaf = c.L[k]; leaf < BRANCHINIT && wk <= 0.0f && guard < 64;
+         leaf = wk <= 0.0f ? m.parent[leaf] : BRANCHINIT, guard++) {
       if (leaf >= m.leaves_used) break;
       const ushort4 lo = m.leaf[leaf];
       const int ls = lo.w;
