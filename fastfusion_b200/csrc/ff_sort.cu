@@ -57,6 +57,91 @@ __global__ void __launch_bounds__(SORT_SMALL_THREADS) k_sort_small(const uint64_
   }
 }
 
+// The same network with E packed words per thread in registers, thread t
+// holding words [E t, E t + E) of P = 1024 E: compare-exchanges of words
+// less than E apart are within a thread, less than 32 E apart between the
+// lanes of a warp (shuffles), the rest through shared memory -- 15 block
+// barriers for P = 16384 instead of 105.
+__device__ __forceinline__ void cx(uint64_t &lo, uint64_t &hi, bool up) {
+  const uint64_t a = lo, b = hi;
+  const bool sw = (a > b) == up;
+  lo = sw ? b : a;
+  hi = sw ? a : b;
+}
+
+// compare-exchanges J apart within a thread's E words (J < E)
+template <int E, int J>
+__device__ __forceinline__ void stage_in(uint64_t (&v)[E], uint32_t base, uint32_t k) {
+#pragma unroll
+  for (int e = 0; e < E; e++)
+    if ((e ^ J) > e) cx(v[e], v[e ^ J], ((base + (uint32_t)e) & k) == 0);
+}
+
+template <int E>
+__global__ void __launch_bounds__(SORT_SMALL_THREADS) k_sort_small_reg(const uint64_t *__restrict__ keys, uint32_t n,
+                                                                      uint64_t *keys_out, uint32_t *pos_out) {
+  extern __shared__ uint64_t w[];
+  constexpr uint32_t P = SORT_SMALL_THREADS * E;
+  const uint32_t t = threadIdx.x, base = t * E;
+  uint64_t v[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const uint32_t i = base + e;
+    v[e] = i < n ? (keys[i] << SORT_SMALL_POS_BITS) | i : ~0ull;
+  }
+  for (uint32_t k = 2; k <= P; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      if (j < (uint32_t)E) {
+        // within the thread
+        if (j == 1) stage_in<E, (E > 1 ? 1 : 0)>(v, base, k);
+        if constexpr (E > 2) {
+          if (j == 2) stage_in<E, 2>(v, base, k);
+        }
+        if constexpr (E > 4) {
+          if (j == 4) stage_in<E, 4>(v, base, k);
+        }
+        if constexpr (E > 8) {
+          if (j == 8) stage_in<E, 8>(v, base, k);
+        }
+      } else {
+        // the partner word is word e of thread t ^ (j / E); this thread keeps
+        // the smaller of the two where its index is the lower one of an
+        // ascending pair (or the upper one of a descending pair)
+        const uint32_t tj = j / E;
+        const bool up = (base & k) == 0;  // (k > j >= E: the same for all E words)
+        const bool lower = (t & tj) == 0;
+        const bool keep_min = lower == up;
+        if (tj < 32) {
+#pragma unroll
+          for (int e = 0; e < E; e++) {
+            const uint64_t o = __shfl_xor_sync(0xffffffffu, v[e], (int)tj);
+            v[e] = keep_min ? (o < v[e] ? o : v[e]) : (o > v[e] ? o : v[e]);
+          }
+        } else {
+          __syncthreads();  // (the previous exchange's reads are done)
+#pragma unroll
+          for (int e = 0; e < E; e++) w[base + e] = v[e];
+          __syncthreads();
+          const uint32_t ob = (t ^ tj) * E;
+#pragma unroll
+          for (int e = 0; e < E; e++) {
+            const uint64_t o = w[ob + e];
+            v[e] = keep_min ? (o < v[e] ? o : v[e]) : (o > v[e] ? o : v[e]);
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const uint32_t i = base + e;
+    if (i < n) {
+      keys_out[i] = v[e] >> SORT_SMALL_POS_BITS;
+      pos_out[i] = (uint32_t)(v[e] & (SORT_SMALL - 1u));
+    }
+  }
+}
+
 // ----------------------------------------------------------- radix sort ----
 
 // digit histogram of each tile, digit-major: hist[d * ntiles + tile]
@@ -192,20 +277,31 @@ cudaError_t argsort_u64(const uint64_t *keys, uint32_t n, int end_bit, uint64_t 
   if (!n) return cudaSuccess;
   if (end_bit < 1 || end_bit > 64) return cudaErrorInvalidValue;
   if (small_path(n, end_bit)) {
-    uint32_t p2 = 2;
-    while (p2 < n) p2 <<= 1;
-    const size_t smem = (size_t)p2 * sizeof(uint64_t);
     static bool attr_set[64] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (!attr_set[dev & 63]) {
-      e = cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)(SORT_SMALL * sizeof(uint64_t)));
-      if (e != cudaSuccess) return e;
+      const int most = (int)(SORT_SMALL * sizeof(uint64_t));
+      if ((e = cudaFuncSetAttribute(k_sort_small_reg<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, most)) !=
+              cudaSuccess ||
+          (e = cudaFuncSetAttribute(k_sort_small_reg<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, most)) !=
+              cudaSuccess)
+        return e;
       attr_set[dev & 63] = true;
     }
-    k_sort_small<<<1, SORT_SMALL_THREADS, smem, s>>>(keys, n, p2, keys_out, pos_out);
+    // words per thread: the smallest power of two with 1024 E >= n
+    const size_t per = sizeof(uint64_t) * SORT_SMALL_THREADS;
+    if (n <= 1024u)
+      k_sort_small_reg<1><<<1, SORT_SMALL_THREADS, per, s>>>(keys, n, keys_out, pos_out);
+    else if (n <= 2048u)
+      k_sort_small_reg<2><<<1, SORT_SMALL_THREADS, 2 * per, s>>>(keys, n, keys_out, pos_out);
+    else if (n <= 4096u)
+      k_sort_small_reg<4><<<1, SORT_SMALL_THREADS, 4 * per, s>>>(keys, n, keys_out, pos_out);
+    else if (n <= 8192u)
+      k_sort_small_reg<8><<<1, SORT_SMALL_THREADS, 8 * per, s>>>(keys, n, keys_out, pos_out);
+    else
+      k_sort_small_reg<16><<<1, SORT_SMALL_THREADS, 16 * per, s>>>(keys, n, keys_out, pos_out);
     if (launches) *launches += 1;
     return cudaGetLastError();
   }
