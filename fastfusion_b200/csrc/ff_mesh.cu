@@ -1339,6 +1339,20 @@ __device__ bool lattice_sample(const VoxSrc &m, const Cell &c, const CellGeom &G
   return true;
 }
 
+// An interior cell that is its leaf's whole brick: sample k (< 512) is
+// voxel k of the brick (lattice_sample's first step reads that one voxel).
+__device__ __forceinline__ bool brick_cell(const VoxSrc &m, const Cell &c, const CellGeom &G, uint32_t &leaf) {
+  if (G.type != 0) return false;
+  const uint32_t l0 = c.L[0];
+  if (l0 >= BRANCHINIT || l0 >= m.leaves_used) return false;
+  const ushort4 a = m.leaf[l0];
+  const int ls = a.w;
+  if (ls <= 0 || (ls & (ls - 1)) != 0 || G.sizeMin != ls || G.size != 8 * ls) return false;
+  if (G.o[0] != a.x || G.o[1] != a.y || G.o[2] != a.z) return false;
+  leaf = l0;
+  return true;
+}
+
 // Per-warp shared scratch of one lattice cell.  Only the zero test of a
 // sample's weight is needed after sampling; colours and vertex numbers are
 // used by the emit pass alone, so the count pass's scratch stops before them
@@ -1521,6 +1535,27 @@ __global__ void __launch_bounds__(32 * MESH_WARPS, EMIT ? 5 : 8) k_mesh_lattice(
     } else {
       bool fit = true;
       const Lat3 Ls = lat3(n3[0], n3[1]);
+      uint32_t bl;
+      if (brick_cell(m, c, G, bl)) {
+        // the brick's voxels in order; a sample that its voxel does not
+        // settle (no weight, or not finite) takes the general path
+        const size_t vb0 = (size_t)bl * 512;
+        for (int k = lane; k < 512; k += 32) {
+          const float d0 = vd(m, vb0 + k), w0 = vw(m, vb0 + k);
+          if (isfinite(d0)) {
+            const float w = __fadd_rn(0.0f, w0);
+            if (!(w <= 0.0f)) {
+              W.sd[k] = d0;
+              W.wzero[k] = 0;
+              continue;
+            }
+          }
+          Sample s;
+          fit &= lattice_sample<false>(m, c, G, k & 7, (k >> 3) & 7, k >> 6, s);
+          W.sd[k] = s.d;
+          W.wzero[k] = s.w == 0.0f;
+        }
+      } else
       for (int k = lane; k < nsamp; k += 32) {
         int bx, by, bz;
         split3(Ls, k, bx, by, bz);
