@@ -1365,6 +1365,7 @@ struct WarpScratch {
   uint8_t edge_set[512 * 3];  // lattice-edge slots (3 per voxel) that carry a vertex
   uint16_t sc[512 * 3];    // emit pass: colour (R, G, B) of each sample
   uint16_t vidx[512 * 3];  // emit pass: the vertex number of each such slot
+  uint16_t vlist[512 * 3];  // emit pass: the vertex-carrying slots in vertex order
 };
 constexpr size_t SCRATCH_COUNT_BYTES = offsetof(WarpScratch, sc);
 constexpr size_t SCRATCH_EMIT_BYTES = sizeof(WarpScratch);
@@ -1441,9 +1442,9 @@ __device__ __forceinline__ uint32_t next_cell(uint32_t *work, int lane) {
 }
 
 // (register caps: the count pass's 4.6 KB of scratch per warp leaves room
-// for 8 blocks per SM at 64 registers; the emit pass's 10.5 KB for 5)
+// for 8 blocks per SM at 64 registers; the emit pass's 13.5 KB for 4)
 template <bool EMIT>
-__global__ void __launch_bounds__(32 * MESH_WARPS, EMIT ? 5 : 8) k_mesh_lattice(VoxSrc m, const Cell *__restrict__ cells,
+__global__ void __launch_bounds__(32 * MESH_WARPS, EMIT ? 4 : 8) k_mesh_lattice(VoxSrc m, const Cell *__restrict__ cells,
                                                                   uint32_t first, uint32_t ncell,
                                                                   const uint32_t *__restrict__ list, const uint32_t *list_n, CellOut *out,
                                                                   const uint64_t *vbase, const uint64_t *fbase,
@@ -1611,7 +1612,8 @@ __global__ void __launch_bounds__(32 * MESH_WARPS, EMIT ? 5 : 8) k_mesh_lattice(
       continue;
     }
     // (the emit pass from here) vertices, in the reference's loop order of
-    // this cell type
+    // this cell type: the slots that carry one listed in that order first
+    // (a warp scan per 32 samples), then one lane per vertex
     uint32_t vrun = 0;
     const uint64_t vb = EMIT ? vbase[cid] : 0;
     const Lat3 Lso = lat3(n3[ord[2]], n3[ord[1]]);
@@ -1623,37 +1625,37 @@ __global__ void __launch_bounds__(32 * MESH_WARPS, EMIT ? 5 : 8) k_mesh_lattice(
         cntv = edge_bit(W, 3 * idx) + edge_bit(W, 3 * idx + 1) + edge_bit(W, 3 * idx + 2);
       }
       int tot;
-      int ex = warp_excl_scan(cntv, lane, tot);
-      if (EMIT && cntv) {
-        const int bb[3] = {b0, b1, b2};
-        float P0[3];
-#pragma unroll
-        for (int r = 0; r < 3; r++)
-          P0[r] = __fadd_rn(m.offset[r], __fmul_rn((float)sample_pos(G, r, bb[r]), m.scale));
-        uint32_t local = vrun + (uint32_t)ex;
-        for (int a = 0; a < 3; a++) {
-          if (!edge_bit(W, 3 * idx + a)) continue;
-          const int step = a == 0 ? 1 : (a == 1 ? 8 : 64);
-          float P1[3] = {P0[0], P0[1], P0[2]};
-          const int q2 = sample_pos(G, a, bb[a]) + (c_role[G.type][a] ? G.stretch : G.sizeMin);
-          P1[a] = __fadd_rn(m.offset[a], __fmul_rn((float)q2, m.scale));
-          float v[3];
-          uint16_t col[3];
-          const float d0 = W.sd[idx], d1 = W.sd[idx + step];
-          vinterp(P0, P1, (double)d0, (double)d1, v);
-          cinterp(&W.sc[3 * idx], &W.sc[3 * (idx + step)], d0, d1, col);
-          const uint64_t gi = vb + local;
-          xyz[3 * gi] = v[0];
-          xyz[3 * gi + 1] = v[1];
-          xyz[3 * gi + 2] = v[2];
-          rgb[3 * gi] = (uint8_t)(col[0] / 256);
-          rgb[3 * gi + 1] = (uint8_t)(col[1] / 256);
-          rgb[3 * gi + 2] = (uint8_t)(col[2] / 256);
-          W.vidx[3 * idx + a] = (uint16_t)local;
-          local++;
-        }
-      }
+      const int ex = warp_excl_scan(cntv, lane, tot);
+      uint32_t at = vrun + (uint32_t)ex;
+      for (int a = 0; a < 3 && cntv; a++)
+        if (edge_bit(W, 3 * idx + a)) W.vlist[at++] = (uint16_t)(3 * idx + a);
       vrun += (uint32_t)tot;
+    }
+    __syncwarp();
+    for (uint32_t q = lane; q < vrun; q += 32) {
+      const int slot = W.vlist[q];
+      const int idx = slot / 3, a = slot - 3 * idx;
+      const int bb[3] = {idx & 7, (idx >> 3) & 7, idx >> 6};
+      float P0[3];
+#pragma unroll
+      for (int r = 0; r < 3; r++) P0[r] = __fadd_rn(m.offset[r], __fmul_rn((float)sample_pos(G, r, bb[r]), m.scale));
+      const int step = a == 0 ? 1 : (a == 1 ? 8 : 64);
+      float P1[3] = {P0[0], P0[1], P0[2]};
+      const int q2 = sample_pos(G, a, bb[a]) + (c_role[G.type][a] ? G.stretch : G.sizeMin);
+      P1[a] = __fadd_rn(m.offset[a], __fmul_rn((float)q2, m.scale));
+      float v[3];
+      uint16_t col[3];
+      const float d0 = W.sd[idx], d1 = W.sd[idx + step];
+      vinterp(P0, P1, (double)d0, (double)d1, v);
+      cinterp(&W.sc[3 * idx], &W.sc[3 * (idx + step)], d0, d1, col);
+      const uint64_t gi = vb + q;
+      xyz[3 * gi] = v[0];
+      xyz[3 * gi + 1] = v[1];
+      xyz[3 * gi + 2] = v[2];
+      rgb[3 * gi] = (uint8_t)(col[0] / 256);
+      rgb[3 * gi + 1] = (uint8_t)(col[1] / 256);
+      rgb[3 * gi + 2] = (uint8_t)(col[2] / 256);
+      W.vidx[slot] = (uint16_t)q;
     }
     __syncwarp();
     // faces, cube by cube in the same nesting
