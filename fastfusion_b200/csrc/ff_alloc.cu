@@ -451,12 +451,18 @@ __device__ __forceinline__ uint32_t wait_unlocked(uint32_t *tree, uint32_t ptr, 
   return cur;
 }
 
+// Branches on one descent's path: at most one per halving of the volume's
+// side (16 bits of voxel coordinates) plus the root.
+constexpr int DESCENT_MAX = 18;
+
 // One processed pixel of the frame F (voxel key v): bounding-box growth,
 // then (inside the volume) the descent of queryPointDepthSingle_func_subtree:
 // queue the existing coarser leaves on the path, allocate missing branches,
 // claim the final leaf.  Returns the number of octree levels probed; sets
-// *created when this pixel wrote a new branch or leaf slot into the octree.
-__device__ __forceinline__ uint32_t insert_descend(const MapFrame &F, int i, int4 v, Counters *cnt, bool *created) {
+// *created when this pixel wrote a new branch or leaf slot into the octree,
+// and records the branches it passed (root first) in path[0, *npath).
+__device__ __forceinline__ uint32_t insert_descend(const MapFrame &F, int i, int4 v, Counters *cnt, bool *created,
+                                                   uint32_t *path, int *npath) {
   const uint32_t n = F.n;
   const int bw = (int)F.bw;
   uint32_t *tree = F.tree;
@@ -481,8 +487,11 @@ __device__ __forceinline__ uint32_t insert_descend(const MapFrame &F, int i, int
   bool ok = true;
   // the previous level's leaf (if any) and its stamp, read but not yet looked at
   uint32_t prev_leaf = BRANCHINIT, prev_st = frame;
+  int np = 0;
   while ((half >> 1) >= target) {
     probed++;
+    if (np < DESCENT_MAX) path[np++] = branch;
+    *npath = np;
     uint32_t co = (x >= ox + half) * 1u + (y >= oy + half) * 2u + (z >= oz + half) * 4u;
     uint32_t ptr = branch + co + 8;
     uint32_t leaf = ld_tree(tree + ptr - 8);
@@ -500,7 +509,8 @@ __device__ __forceinline__ uint32_t insert_descend(const MapFrame &F, int i, int
           if (prev_leaf < leaves_max) queue_leaf_after(prev_leaf, prev_st, frame, stamp, queue, cnt);
           return probed;
         }
-        __threadfence();
+        // (no fence: a new branch's slots hold BRANCHINIT since an earlier
+        // launch, and nothing else this thread wrote is read through it)
         atomicExch(tree + ptr, nb);
         child = nb;
         *created = true;
@@ -523,6 +533,8 @@ __device__ __forceinline__ uint32_t insert_descend(const MapFrame &F, int i, int
   uint32_t co = (x >= ox + half) * 1u + (y >= oy + half) * 2u + (z >= oz + half) * 4u;
   uint32_t ptr = branch + co;
   probed++;
+  if (np < DESCENT_MAX) path[np++] = branch;
+  *npath = np;
   uint32_t cur = ld_tree(tree + ptr);
   if (prev_leaf < leaves_max) queue_leaf_after(prev_leaf, prev_st, frame, stamp, queue, cnt);
   if (cur == BRANCHINIT) {
@@ -558,40 +570,31 @@ __device__ __forceinline__ uint32_t insert_descend(const MapFrame &F, int i, int
   return probed;
 }
 
-// Mark every branch on the path from the root to the branch that holds the
-// slot of voxel key v with the frame: the branches whose subtree gained a
-// branch or a leaf.  Only pixels that created something walk it again; the
-// path's child slots are all set by now, and are read past L1, which may
-// still hold a slot as it was before another thread set it.
-__device__ __forceinline__ void stamp_path(const MapFrame &F, int4 v) {
-  const uint32_t x = (uint16_t)v.x, y = (uint16_t)v.y, z = (uint16_t)v.z, target = (uint32_t)v.w;
-  uint32_t ox = 0, oy = 0, oz = 0, branch = 0;
-  uint32_t half = (uint16_t)(F.n >> 1);
-  for (int lvl = 0; lvl < 32; lvl++) {
-    uint32_t *b = F.bstamp + (branch >> 4);
+// Mark every branch on the descent's path (root first, down to the branch
+// that holds the pixel's slot, or to the last one reached when the descent
+// stopped early) with the frame: the branches whose subtree gained a branch
+// or a leaf.  Only pixels that created something do it; the loads of the
+// stamps are independent, so they overlap.
+__device__ __forceinline__ void stamp_path(const MapFrame &F, const uint32_t *path, int np) {
+  for (int k = 0; k < np; k++) {
+    uint32_t *b = F.bstamp + (path[k] >> 4);
     if (*b != F.frame) *b = F.frame;
-    if ((half >> 1) < target) break;
-    const uint32_t co = (x >= ox + half) * 1u + (y >= oy + half) * 2u + (z >= oz + half) * 4u;
-    const uint32_t child = ld_volatile(F.tree + branch + co + 8);
-    if (child >= PENDING) break;  // a branch whose allocation failed: nothing below
-    ox += half * ((co & 1) != 0);
-    oy += half * ((co & 2) != 0);
-    oz += half * ((co & 4) != 0);
-    branch = child;
-    half >>= 1;
   }
 }
 
 __device__ __forceinline__ uint32_t insert_pixel(const MapFrame &F, int i, int4 v, Counters *cnt) {
   bool created = false;
-  const uint32_t probed = insert_descend(F, i, v, cnt, &created);
-  if (created) stamp_path(F, v);
+  uint32_t path[DESCENT_MAX];
+  int np = 0;
+  const uint32_t probed = insert_descend(F, i, v, cnt, &created, path, &np);
+  if (created) stamp_path(F, path, np);
   return probed;
 }
 
 // One thread per pixel of every frame of the batch (each map's pixels padded
 // to whole warps, so a warp never spans two maps).
 __global__ void k_insert(const BatchDesc *__restrict__ bd, int m0, int m1) {
+  pdl_enter();
   const int nmaps = min(bd->n, m1);
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x + (m0 ? bd->pix_end[m0 - 1] : 0u);
   if (g >= bd->pix_end[nmaps - 1]) return;
@@ -620,11 +623,11 @@ __global__ void k_insert(const BatchDesc *__restrict__ bd, int m0, int m1) {
   }
 }
 
-void launch_insert(const BatchDesc *d_batch, uint32_t pix, cudaStream_t s, int block, int m0, int m1) {
+void launch_insert(const BatchDesc *d_batch, uint32_t pix, cudaStream_t s, int block, int m0, int m1, bool pdl) {
   if (!pix) return;
   if (block < 64 || block > 1024 || block % 32) block = 256;
   note_launch();
-  k_insert<<<(pix + block - 1) / block, block, 0, s>>>(d_batch, m0, m1);
+  launch_pdl(pdl, k_insert, dim3((pix + block - 1) / block), dim3(block), 0, s, d_batch, m0, m1);
 }
 
 // ------------------------------------------------- pending leaf order -----
@@ -658,6 +661,21 @@ __device__ __forceinline__ void finalize_one(const PendingLeaf &p, uint32_t idx,
   if (idx < leaves_max) {
     leaf[idx] = p.pos;
     queue_leaf(idx, frame, stamp, queue, cnt);
+  }
+}
+
+// A new leaf of rank r in its frame: index leaves_before + r, queued at
+// position q0 + r after the q0 bricks the insert queued (a pending leaf is
+// never on the insert's queue), so no atomics; the frame's queue length
+// becomes q0 + the number of leaves placed.
+__device__ __forceinline__ void finalize_new(const PendingLeaf &p, uint32_t idx, uint32_t qpos, uint32_t leaves_max,
+                                             uint32_t *tree, ushort4 *leaf, uint32_t frame, uint32_t *stamp,
+                                             uint32_t *queue) {
+  tree[p.slot] = idx;
+  if (idx < leaves_max) {
+    leaf[idx] = p.pos;
+    stamp[idx] = frame;
+    queue[qpos] = idx;
   }
 }
 
@@ -717,6 +735,7 @@ __global__ void k_parents(int npend, uint32_t leaves_before, uint32_t leaves_max
 constexpr int PARENT_BLOCKS = 4, PARENT_THREADS = 256;
 
 __global__ void __launch_bounds__(PARENT_THREADS) k_parents_frames(const BatchDesc *__restrict__ bd, int m0) {
+  pdl_enter();
   const MapFrame &F = bd->f[m0 + blockIdx.x / PARENT_BLOCKS];
   const Counters *cnt = F.cnt;
   if (ld_volatile(&cnt->error) & (ERR_DEDUPE_FAILED | ERR_PENDING_OVERFLOW | ERR_SEQ_HALT)) return;
@@ -730,10 +749,10 @@ __global__ void __launch_bounds__(PARENT_THREADS) k_parents_frames(const BatchDe
   }
 }
 
-void launch_parents_frames(const BatchDesc *d_batch, int nframes, cudaStream_t s, int m0) {
+void launch_parents_frames(const BatchDesc *d_batch, int nframes, cudaStream_t s, int m0, bool pdl) {
   if (nframes < 1) return;
   note_launch();
-  k_parents_frames<<<nframes * PARENT_BLOCKS, PARENT_THREADS, 0, s>>>(d_batch, m0);
+  launch_pdl(pdl, k_parents_frames, dim3(nframes * PARENT_BLOCKS), dim3(PARENT_THREADS), 0, s, d_batch, m0);
 }
 
 // The whole frame's pending leaves in one block.  A leaf's creation rank is
@@ -761,6 +780,10 @@ __device__ __forceinline__ void chain_next(const MapFrame &F, Counters *cnt, uin
 
 __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc *__restrict__ bd, int m0) {
   extern __shared__ uint32_t fin_smem[];
+  // (the next frame's insert is scheduled once this has started: it overlaps
+  // this kernel, not the insert before it)
+  pdl_wait();
+  pdl_trigger();
   const MapFrame &F = bd->f[m0 + blockIdx.x];
   Counters *cnt = F.cnt;
   if (F.chain || F.next_cnt) {
@@ -777,9 +800,12 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc
   // mark; the frame's update is skipped (ERR_FRAME_FAILED).
   if (cnt->error & (ERR_DEDUPE_FAILED | ERR_PENDING_OVERFLOW)) return;
   const int npend = (int)cnt->pending;
+  const uint32_t q0 = cnt->queued;  // the insert's queue
   const PendingLeaf *pend = F.pend;
   const uint32_t leaves_before = F.chain ? ld_volatile(&cnt->leaves_base) : F.leaves_before;
   const uint32_t npix = F.npix, leaves_max = F.leaves_max, frame = F.frame;
+  // the new leaves that fit the pool (indices below leaves_max) are queued
+  const uint32_t nplaced = leaves_before < leaves_max ? min((uint32_t)npend, leaves_max - leaves_before) : 0u;
   uint32_t *rank = F.rank, *tree = F.tree, *stamp = F.stamp, *queue = F.queue;
   ushort4 *leaf = F.leaf;
   const uint32_t nwords = (npix + 31) / 32;
@@ -798,7 +824,7 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc
       uint32_t r = 0;
       for (int i = 0; i < npend; i++) r += fp[i] < mine_fp ? 1u : 0u;
       rank[j] = r;
-      finalize_one(pend[j], leaves_before + r, leaves_max, tree, leaf, frame, stamp, queue, cnt);
+      finalize_new(pend[j], leaves_before + r, q0 + r, leaves_max, tree, leaf, frame, stamp, queue);
     }
   } else {
     for (uint32_t w = t; w < nwords; w += FIN_THREADS) bitmap[w] = 0;
@@ -826,7 +852,7 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc
       for (uint32_t k = c * chunk; k < w; k++) r += __popc(bitmap[k]);
       r += __popc(bitmap[w] & ((1u << (p.first_pixel & 31)) - 1u));
       rank[j] = r;
-      finalize_one(p, leaves_before + r, leaves_max, tree, leaf, frame, stamp, queue, cnt);
+      finalize_new(p, leaves_before + r, q0 + r, leaves_max, tree, leaf, frame, stamp, queue);
     }
   }
   // (the new leaves' parents: k_parents_frames, after this kernel)
@@ -838,11 +864,14 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc
   // stream, may set its error word meanwhile, and the loop below claims list
   // slots with warp-wide votes.
   __shared__ int aside_flag;
-  if (t == 0) aside_flag = fuse_deferred(F) ? 1 : 0;
+  if (t == 0) {
+    cnt->queued = q0 + nplaced;
+    aside_flag = fuse_deferred(F) ? 1 : 0;
+  }
   __syncthreads();
   const bool stand_aside = aside_flag != 0;  // failed, or the volume must grow first
   if (F.upd_mask && !stand_aside) {
-    const uint32_t nq = ld_volatile(&cnt->queued);
+    const uint32_t nq = q0 + nplaced;
     const uint32_t bit = 1u << F.upd_slot;
     // (every thread of the block runs the same number of iterations, so the
     // list slots are claimed with one atomic per warp)
@@ -884,13 +913,12 @@ bool finalize_small_prepare(int device) {
 }
 
 bool launch_finalize_small(const BatchDesc *d_batch, int nmaps, uint32_t max_npix, int device, cudaStream_t s,
-                           int m0) {
+                           int m0, bool pdl) {
   const size_t smem = sizeof(uint32_t) * (((size_t)max_npix + 31) / 32 + FIN_THREADS);
   if (smem > FIN_SMEM_MAX || nmaps < 1) return false;
   if (!finalize_small_prepare(device)) return false;
   note_launch();
-  k_finalize_bitmap<<<nmaps, FIN_THREADS, smem, s>>>(d_batch, m0);
-  return true;
+  return launch_pdl(pdl, k_finalize_bitmap, dim3(nmaps), dim3(FIN_THREADS), smem, s, d_batch, m0) == cudaSuccess;
 }
 
 void launch_parents(int npend, uint32_t leaves_before, uint32_t leaves_max, const uint32_t *tree, uint32_t n,

@@ -1718,19 +1718,24 @@ static ff_status sequence_chunk(ff_handle *h, int c, const uint16_t *const *d_de
   FCK(frame_issue(h, c, lp, false));
   const int block = h->tune.insert_block > 0 ? h->tune.insert_block : 256;
   std::vector<int> pi_ins(c, -1);
+  // The chain's kernels follow one another directly on the stream: each is
+  // launched as a programmatic dependent of the one before, so that its
+  // launch overlaps that kernel (not with the stage profile's events between
+  // them, nor for the first insert, which follows the de-duplication).
+  const bool pdl = !h->prof.on;
   for (int k = 0; k < c; k++) {
     int pi = h->prof.begin(ST_INSERT, s);
     pi_ins[k] = pi;
     launch_insert(h->d_batch, (uint32_t)(h->h_batch->pix_end[k] - (k ? h->h_batch->pix_end[k - 1] : 0u)), s, block,
-                  k, k + 1);
+                  k, k + 1, pdl && k > 0);
     h->prof.end(pi, 0.0, s);
     pi = h->prof.begin(ST_FINALIZE, s);
-    if (!launch_finalize_small(h->d_batch, 1, (uint32_t)pix, h->cfg.device, s, k))
+    if (!launch_finalize_small(h->d_batch, 1, (uint32_t)pix, h->cfg.device, s, k, pdl))
       return set_err(h, FF_ERR_CUDA, "leaf finalisation could not be launched");
     h->prof.end(pi, 0.0, s);
   }
   // the parents of every frame's new leaves, once the chain has run
-  launch_parents_frames(h->d_batch, c, s);
+  launch_parents_frames(h->d_batch, c, s, 0, pdl);
   CK(cudaGetLastError());
   if (h->cnn_pending) {
     // the frames' confidence networks report into their counters

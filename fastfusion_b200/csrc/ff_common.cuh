@@ -24,6 +24,38 @@ extern std::atomic<unsigned long long> g_own_launches, g_lib_calls;
 inline void note_launch(unsigned n = 1) { g_own_launches.fetch_add(n, std::memory_order_relaxed); }
 inline void note_lib_call() { g_lib_calls.fetch_add(1, std::memory_order_relaxed); }
 
+// Programmatic dependent launch.  A kernel launched by launch_pdl may be
+// scheduled while the kernel before it on the stream still runs, so that its
+// launch and ramp-up overlap that kernel's tail; it calls pdl_wait() before
+// anything else, which returns once the earlier kernel has completed and its
+// writes are visible (and at once in a launch without the attribute).
+// pdl_trigger() lets the next kernel of the stream be scheduled early.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_enter() {
+  pdl_trigger();
+  pdl_wait();
+}
+
+// Launch kern on s; with pdl, as a programmatic dependent of the stream's
+// previous kernel (which must then be a kernel: the kernel launched here
+// starts with pdl_enter()).
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(bool pdl, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 constexpr uint32_t BRANCHINIT = 0xFFFFFFFEu;  // reference definitions.h:128
 constexpr uint32_t LOCKED = 0xFFFFFFFDu;      // slot being allocated (device-internal)
 constexpr uint32_t PENDING = 0xC0000000u;     // slot holds a leaf created this frame: PENDING + record

@@ -225,8 +225,10 @@ cudaError_t launch_dedupe_one(const BatchDesc *h_desc, BatchDesc *d_batch, uint3
 
 // Octree descent / allocation of every processed pixel of the batch's maps
 // [m0, m1) (pixels [pix_end[m0 - 1], pix_end[m1 - 1]), pix = their count).
+// pdl: launched as a programmatic dependent of the stream's previous kernel
+// (which must be a kernel), as in the chained frames of a sequence.
 void launch_insert(const BatchDesc *d_batch, uint32_t pix, cudaStream_t s, int block = 256, int m0 = 0,
-                   int m1 = BATCH_MAX);
+                   int m1 = BATCH_MAX, bool pdl = false);
 
 // Sort scratch size for `n` pending leaves.
 size_t pending_sort_bytes(int n);
@@ -241,7 +243,7 @@ void launch_finalize(const PendingLeaf *pend, const uint32_t *order, int npend, 
                      uint32_t *queue, Counters *cnt, cudaStream_t s);
 // Parents of the leaves placed by the one-block finalisation of frames
 // [m0, m0 + nframes) of the descriptor (after it on the stream).
-void launch_parents_frames(const BatchDesc *d_batch, int nframes, cudaStream_t s, int m0 = 0);
+void launch_parents_frames(const BatchDesc *d_batch, int nframes, cudaStream_t s, int m0 = 0, bool pdl = false);
 // Parent leaf of each new leaf: finest ancestor leaf created before it.
 void launch_parents(int npend, uint32_t leaves_before, uint32_t leaves_max, const uint32_t *tree, uint32_t n,
                     const ushort4 *leaf, uint32_t *parent, cudaStream_t s);
@@ -253,7 +255,7 @@ bool finalize_small_fits(uint32_t npix);
 // leaves, one block per map, counts read on the device; for images of up to
 // about 1.6 million pixels (false, nothing launched, for larger ones).
 bool launch_finalize_small(const BatchDesc *d_batch, int nmaps, uint32_t max_npix, int device, cudaStream_t s,
-                           int m0 = 0);
+                           int m0 = 0, bool pdl = false);
 // Set the finalisation kernel's shared-memory limit on this device (once).
 bool finalize_small_prepare(int device);
 

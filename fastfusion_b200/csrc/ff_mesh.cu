@@ -1452,7 +1452,9 @@ __global__ void __launch_bounds__(32 * MESH_WARPS, EMIT ? 4 : 8) k_mesh_lattice(
                                                                   uint32_t *work, uint8_t *__restrict__ cases) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ McTab T;
-  load_mc(T);
+  pdl_trigger();
+  load_mc(T);  // (constant tables: before the wait for the kernel ahead)
+  pdl_wait();
   WarpScratch &W = *reinterpret_cast<WarpScratch *>(smem_raw + (size_t)(threadIdx.x >> 5) *
                                                                       (EMIT ? SCRATCH_EMIT_BYTES : SCRATCH_COUNT_BYTES));
   const int lane = threadIdx.x & 31;
@@ -1699,7 +1701,9 @@ __global__ void k_mesh_corner(VoxSrc m, const Cell *__restrict__ cells, uint32_t
                               const uint64_t *vbase, const uint64_t *fbase, float *xyz, uint8_t *rgb,
                               uint32_t *faces) {
   __shared__ McTab T;
-  load_mc(T);
+  pdl_trigger();
+  load_mc(T);  // (constant tables: before the wait for the kernel ahead)
+  pdl_wait();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t i = t / CORNER_LANES;
   const int k = (int)(t % CORNER_LANES);  // this lane's sample
@@ -1823,6 +1827,7 @@ __global__ void k_mark_dirty(const Cell *cells, uint32_t n, const Cell *old_cell
                              const uint64_t *old_keys, const uint32_t *stamp, const uint32_t *parent,
                              uint32_t leaves_used, uint32_t since, uint8_t *dirty, int32_t *old_index,
                              uint32_t *n_dirty, uint32_t first_corner, uint32_t *list, uint32_t *n_list, int B) {
+  pdl_enter();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Cell c = cells[i];
@@ -1901,6 +1906,7 @@ __device__ __forceinline__ void block_scan2(uint64_t a, uint64_t b, uint64_t &pa
 
 __global__ void __launch_bounds__(SCAN_THREADS) k_count_tile_sums(const CellOut *__restrict__ out, uint32_t n,
                                                                   uint64_t *tile_v, uint64_t *tile_f) {
+  pdl_enter();
   const uint32_t i0 = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_PER_THREAD;
   uint64_t a = 0, b = 0;
 #pragma unroll
@@ -1918,6 +1924,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_count_tile_sums(const CellOut 
 // vbase[n] and fbase[n].
 __global__ void __launch_bounds__(SCAN_THREADS) k_count_tile_scan(uint64_t *tile_v, uint64_t *tile_f, uint32_t ntiles,
                                                                   uint64_t *vbase, uint64_t *fbase, uint32_t n) {
+  pdl_enter();
   __shared__ uint64_t carry_v, carry_f;
   if (threadIdx.x == 0) carry_v = carry_f = 0;
   __syncthreads();
@@ -1943,6 +1950,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_count_tile_scan(uint64_t *tile
 __global__ void __launch_bounds__(SCAN_THREADS) k_count_tile_apply(const CellOut *__restrict__ out, uint32_t n,
                                                                    const uint64_t *tile_v, const uint64_t *tile_f,
                                                                    uint64_t *vbase, uint64_t *fbase) {
+  pdl_enter();
   const uint32_t i0 = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_PER_THREAD;
   uint32_t cv[SCAN_PER_THREAD], cf[SCAN_PER_THREAD];
   uint64_t a = 0, b = 0;
@@ -1973,6 +1981,7 @@ __global__ void k_copy_clean(const uint8_t *dirty, const int32_t *old_index, uin
                              const uint64_t *vbase, const uint64_t *fbase, const uint64_t *old_vbase,
                              const uint64_t *old_fbase, const float *old_xyz, const uint8_t *old_rgb,
                              const uint32_t *old_faces, float *xyz, uint8_t *rgb, uint32_t *faces) {
+  pdl_enter();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1991,6 +2000,7 @@ __global__ void k_copy_clean(const uint8_t *dirty, const int32_t *old_index, uin
 
 __global__ void k_fill_counts_from_old(const uint8_t *dirty, const int32_t *old_index, uint32_t n,
                                        const CellOut *old_out, CellOut *out) {
+  pdl_enter();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || dirty[i]) return;
   out[i] = old_out[old_index[i]];
@@ -2462,6 +2472,15 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   // the sorted cell list holds interiors, walls, edges, then corners (type is
   // the key's top field)
   const uint32_t first_corner = ncells - std::min(I.n_corners, ncells);
+  // buffers of the count pass and the scans, ahead of the kernels (nothing
+  // but kernels between them on the stream)
+  const uint32_t ntiles = (ncells + SCAN_TILE - 1) / SCAN_TILE;
+  MCK(grow_buf(I.cases, I.cap_cases, (size_t)first_corner * 512, s));
+  MCK(grow_buf(I.nv, I.cap_nv, std::max<uint32_t>(ntiles, 1), s));  // tile sums of the vertex counts
+  MCK(grow_buf(I.nf, I.cap_nf, std::max<uint32_t>(ntiles, 1), s));  // and of the face counts
+  // programmatic dependent launches, unless the stage profile's events lie
+  // between the kernels
+  const bool pdl = !P.on;
   // dirty cells: all on the first update, otherwise those whose inputs changed
   MCK(cudaMemsetAsync(I.d_count + 10, 0, sizeof(uint32_t), s));
   MCK(cudaMemsetAsync(I.d_count + 14, 0, 2 * sizeof(uint32_t), s));
@@ -2472,7 +2491,8 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
                                                         in.parent, in.leaves_used, I.since, I.dirty, I.old_index,
                                                         I.d_count + 10, first_corner, I.dlist, I.d_count + 14,
                                                         kb);
-      k_fill_counts_from_old<<<(ncells + 255) / 256, 256, 0, s>>>(I.dirty, I.old_index, ncells, I.old_out, I.out);
+      MCK(launch_pdl(pdl, k_fill_counts_from_old, dim3((ncells + 255) / 256), dim3(256), 0, s, I.dirty, I.old_index,
+                     ncells, I.old_out, I.out));
     } else {
       MCK(cudaMemsetAsync(I.dirty, 1, ncells, s));
     }
@@ -2487,32 +2507,45 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
     MCK(cudaFuncSetAttribute(k_mesh_lattice<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_emit));
     attr_devices.fetch_or(dbit);
   }
-  MCK(grow_buf(I.cases, I.cap_cases, (size_t)first_corner * 512, s));
   const uint32_t *lat_list = incremental ? I.dlist : nullptr;
   const uint32_t *cor_list = incremental ? I.dlist + first_corner : nullptr;
   pi = P.begin(ST_MESH_COUNT, s);
   const int lat_blocks = std::max(1, std::min<int>(148 * 8, (int)((first_corner + MESH_WARPS - 1) / MESH_WARPS)));
   note_launch((first_corner ? 1 : 0) + (ncells > first_corner ? 1 : 0) + (ncells ? 1 : 0));
-  if (first_corner)
-    k_mesh_lattice<false><<<lat_blocks, 32 * MESH_WARPS, smem_count, s>>>(vs, I.cells, 0, first_corner, lat_list,
-                                                                    I.d_count + 14, I.out, nullptr, nullptr, nullptr,
-                                                                    nullptr, nullptr, I.d_count + 16, I.cases);
-  if (ncells > first_corner)
-    k_mesh_corner<false><<<((ncells - first_corner) * CORNER_LANES + 127) / 128, 128, 0, s>>>(
-        vs, I.cells, first_corner, ncells - first_corner, cor_list, I.d_count + 15, I.out, nullptr, nullptr, nullptr,
-        nullptr, nullptr);
+  // (the kernels from here to the totals' copy follow one another on the
+  // stream: each after the first is a programmatic dependent of the one
+  // before; the dirty marking is one when the volume's cells were kept)
+  bool chained = pdl && incremental && ncells;
+  if (first_corner) {
+    MCK(launch_pdl(chained, k_mesh_lattice<false>, dim3(lat_blocks), dim3(32 * MESH_WARPS), smem_count, s, vs,
+                   (const Cell *)I.cells, 0u, first_corner, lat_list, (const uint32_t *)(I.d_count + 14), I.out,
+                   (const uint64_t *)nullptr, (const uint64_t *)nullptr, (float *)nullptr, (uint8_t *)nullptr,
+                   (uint32_t *)nullptr, I.d_count + 16, I.cases));
+    chained = pdl;
+  }
+  if (ncells > first_corner) {
+    MCK(launch_pdl(chained, k_mesh_corner<false>, dim3(((ncells - first_corner) * CORNER_LANES + 127) / 128),
+                   dim3(128), 0, s, vs, (const Cell *)I.cells, first_corner, ncells - first_corner, cor_list,
+                   (const uint32_t *)(I.d_count + 15), I.out, (const uint64_t *)nullptr, (const uint64_t *)nullptr,
+                   (float *)nullptr, (uint8_t *)nullptr, (uint32_t *)nullptr));
+    chained = pdl;
+  }
   const int pi_count = pi;
   P.end(pi_count, 0.0, s);
   MCK(cudaGetLastError());
   // exclusive scans of vertex and face counts -> per-cell bases (totals at ncells)
   {
-    const uint32_t ntiles = (ncells + SCAN_TILE - 1) / SCAN_TILE;
-    MCK(grow_buf(I.nv, I.cap_nv, std::max<uint32_t>(ntiles, 1), s));  // tile sums of the vertex counts
-    MCK(grow_buf(I.nf, I.cap_nf, std::max<uint32_t>(ntiles, 1), s));  // and of the face counts
     note_launch(ntiles ? 3 : 1);
-    if (ntiles) k_count_tile_sums<<<ntiles, SCAN_THREADS, 0, s>>>(I.out, ncells, I.nv, I.nf);
-    k_count_tile_scan<<<1, SCAN_THREADS, 0, s>>>(I.nv, I.nf, ntiles, I.vbase, I.fbase, ncells);
-    if (ntiles) k_count_tile_apply<<<ntiles, SCAN_THREADS, 0, s>>>(I.out, ncells, I.nv, I.nf, I.vbase, I.fbase);
+    if (ntiles) {
+      MCK(launch_pdl(chained, k_count_tile_sums, dim3(ntiles), dim3(SCAN_THREADS), 0, s, (const CellOut *)I.out,
+                     ncells, I.nv, I.nf));
+      chained = pdl;
+    }
+    MCK(launch_pdl(chained, k_count_tile_scan, dim3(1), dim3(SCAN_THREADS), 0, s, I.nv, I.nf, ntiles, I.vbase,
+                   I.fbase, ncells));
+    if (ntiles)
+      MCK(launch_pdl(pdl, k_count_tile_apply, dim3(ntiles), dim3(SCAN_THREADS), 0, s, (const CellOut *)I.out, ncells,
+                     (const uint64_t *)I.nv, (const uint64_t *)I.nf, I.vbase, I.fbase));
   }
   // totals, dirty count and samples through the pinned counter mirror
   uint64_t *h_tot = reinterpret_cast<uint64_t *>(I.h_count + HOST_TOTALS);
@@ -2562,18 +2595,28 @@ int mesh_update(MeshState &M, const MeshInputs &in, cudaStream_t s, std::string 
   vs.samples = reinterpret_cast<unsigned long long *>(I.d_count + 18);
   pi = P.begin(ST_MESH_EMIT, s);
   note_launch((first_corner ? 1 : 0) + (ncells > first_corner ? 1 : 0) + (incremental && ncells ? 1 : 0));
-  if (first_corner)
+  // (the emit kernels after the first: programmatic dependents of the one
+  // before)
+  chained = false;
+  if (first_corner) {
     k_mesh_lattice<true><<<lat_blocks, 32 * MESH_WARPS, smem_emit, s>>>(vs, I.cells, 0, first_corner, lat_list,
                                                                    I.d_count + 14, I.out, I.vbase, I.fbase, M.d_xyz,
                                                                    M.d_rgb, M.d_faces, I.d_count + 17, I.cases);
-  if (ncells > first_corner)
-    k_mesh_corner<true><<<((ncells - first_corner) * CORNER_LANES + 127) / 128, 128, 0, s>>>(
-        vs, I.cells, first_corner, ncells - first_corner, cor_list, I.d_count + 15, I.out, I.vbase, I.fbase, M.d_xyz,
-        M.d_rgb, M.d_faces);
+    chained = pdl;
+  }
+  if (ncells > first_corner) {
+    MCK(launch_pdl(chained, k_mesh_corner<true>, dim3(((ncells - first_corner) * CORNER_LANES + 127) / 128),
+                   dim3(128), 0, s, vs, (const Cell *)I.cells, first_corner, ncells - first_corner, cor_list,
+                   (const uint32_t *)(I.d_count + 15), I.out, (const uint64_t *)I.vbase, (const uint64_t *)I.fbase,
+                   M.d_xyz, M.d_rgb, M.d_faces));
+    chained = pdl;
+  }
   if (incremental && ncells)
-    k_copy_clean<<<148 * 8, 256, 0, s>>>(I.dirty, I.old_index, ncells, I.out, I.vbase, I.fbase, I.old_vbase,
-                                         I.old_fbase, I.old_xyz, I.old_rgb, I.old_faces, M.d_xyz, M.d_rgb,
-                                         M.d_faces);
+    MCK(launch_pdl(chained, k_copy_clean, dim3(148 * 8), dim3(256), 0, s, (const uint8_t *)I.dirty,
+                   (const int32_t *)I.old_index, ncells, (const CellOut *)I.out, (const uint64_t *)I.vbase,
+                   (const uint64_t *)I.fbase, (const uint64_t *)I.old_vbase, (const uint64_t *)I.old_fbase,
+                   (const float *)I.old_xyz, (const uint8_t *)I.old_rgb, (const uint32_t *)I.old_faces, M.d_xyz,
+                   M.d_rgb, M.d_faces));
   // emit pass: the samples it reads (the ends of vertex-carrying lattice
   // edges, corner cells' 8) and the whole mesh written (xyz 12 B + rgb 3 B
   // per vertex, 12 B per face); the sample count arrives with the final sync
