@@ -592,8 +592,10 @@ __device__ __forceinline__ uint32_t insert_pixel(const MapFrame &F, int i, int4 
 }
 
 // One thread per pixel of every frame of the batch (each map's pixels padded
-// to whole warps, so a warp never spans two maps).
-__global__ void k_insert(const BatchDesc *__restrict__ bd, int m0, int m1) {
+// to whole warps, so a warp never spans two maps).  At most 40 registers: six
+// 256-thread blocks per SM instead of five (a few bytes of spill), for any
+// block size the tuning picks.
+__global__ void __maxnreg__(40) k_insert(const BatchDesc *__restrict__ bd, int m0, int m1) {
   pdl_enter();
   const int nmaps = min(bd->n, m1);
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x + (m0 ? bd->pix_end[m0 - 1] : 0u);
@@ -778,6 +780,33 @@ __device__ __forceinline__ void chain_next(const MapFrame &F, Counters *cnt, uin
   if (halt) atomicOr(&nx->error, ERR_SEQ_HALT);
 }
 
+// Deferred update: mark each brick of the frame's queue (nq entries: the
+// q0 the insert queued, then the new leaves in rank order, indices from
+// leaves_before) with the frame's bit, and list the bricks no earlier frame
+// of the pass has marked.  Every thread of the block runs the same number of
+// iterations, so the list slots are claimed with one atomic per warp.
+__device__ __forceinline__ void finalize_mark(const MapFrame &F, uint32_t q0, uint32_t nq, uint32_t leaves_before,
+                                              int t) {
+  const uint32_t bit = 1u << F.upd_slot;
+  const uint32_t rounds = (nq + FIN_THREADS - 1) / FIN_THREADS;
+  for (uint32_t it = 0; it < rounds; it++) {
+    const uint32_t j = it * FIN_THREADS + (uint32_t)t;
+    bool add = false;
+    uint32_t b = 0;
+    if (j < nq) {
+      b = j < q0 ? F.queue[j] : leaves_before + (j - q0);
+      // a part of a sharded map updates the bricks it owns; the queue holds
+      // each brick once, so the old mask lacks this bit
+      if (F.shards <= 1 || owns_brick(F, F.leaf[b])) add = atomicOr(&F.upd_mask[b], bit) == 0u;
+    }
+    const unsigned ball = __ballot_sync(0xffffffffu, add);
+    uint32_t at = 0;
+    if ((t & 31) == 0 && ball) at = atomicAdd(F.upd_count, (uint32_t)__popc(ball));
+    at = __shfl_sync(0xffffffffu, at, 0);
+    if (add) F.upd_list[at + __popc(ball & ((1u << (t & 31)) - 1u))] = b;
+  }
+}
+
 __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc *__restrict__ bd, int m0) {
   extern __shared__ uint32_t fin_smem[];
   // (the next frame's insert is scheduled once this has started: it overlaps
@@ -801,18 +830,32 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc
   if (cnt->error & (ERR_DEDUPE_FAILED | ERR_PENDING_OVERFLOW)) return;
   const int npend = (int)cnt->pending;
   const uint32_t q0 = cnt->queued;  // the insert's queue
+  const uint32_t branches_used = cnt->branches_used;
   const PendingLeaf *pend = F.pend;
   const uint32_t leaves_before = F.chain ? ld_volatile(&cnt->leaves_base) : F.leaves_before;
   const uint32_t npix = F.npix, leaves_max = F.leaves_max, frame = F.frame;
   // the new leaves that fit the pool (indices below leaves_max) are queued
   const uint32_t nplaced = leaves_before < leaves_max ? min((uint32_t)npend, leaves_max - leaves_before) : 0u;
+  const int t = threadIdx.x;
+  // Whether the deferred update takes the frame (not when it failed or the
+  // volume must grow first: the host handles those), decided by one thread
+  // for the block (the confidence network, on another stream, may set its
+  // error word meanwhile).  A map in one part marks its queue at once: the
+  // marks need no leaf of this frame placed, so their atomics overlap the
+  // ranking below; a part of a sharded map needs the new leaves' positions
+  // and marks after it.
+  __shared__ int aside_flag;
+  if (t == 0) aside_flag = fuse_deferred(F) ? 1 : 0;
+  __syncthreads();
+  const bool stand_aside = aside_flag != 0;
+  const bool mark = F.upd_mask && !stand_aside;
+  if (mark && F.shards <= 1) finalize_mark(F, q0, q0 + nplaced, leaves_before, t);
   uint32_t *rank = F.rank, *tree = F.tree, *stamp = F.stamp, *queue = F.queue;
   ushort4 *leaf = F.leaf;
   const uint32_t nwords = (npix + 31) / 32;
   uint32_t *bitmap = fin_smem;
   uint32_t *chunk_base = fin_smem + nwords;  // [FIN_THREADS]
   const uint32_t chunk = (nwords + FIN_THREADS - 1) / FIN_THREADS;
-  const int t = threadIdx.x;
   if (npend <= FIN_FEW) {
     // few new leaves (the usual frame): a leaf's rank counted directly over
     // the others' first pixels in shared memory, without the image bitmap
@@ -856,44 +899,20 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize_bitmap(const BatchDesc
     }
   }
   // (the new leaves' parents: k_parents_frames, after this kernel)
-  // Deferred update: the frame's queue is complete (the new leaves were
-  // queued above); mark each queued brick with the frame's bit and list the
-  // bricks no earlier frame of the pass has marked.  A frame the update must
-  // not take (failed, or the volume must grow first) is left to the host.
-  // One thread decides for the block: the confidence network, on another
-  // stream, may set its error word meanwhile, and the loop below claims list
-  // slots with warp-wide votes.
-  __shared__ int aside_flag;
+  if (mark && F.shards > 1) {
+    __syncthreads();  // the new leaves' positions
+    finalize_mark(F, q0, q0 + nplaced, leaves_before, t);
+  }
   if (t == 0) {
     cnt->queued = q0 + nplaced;
-    aside_flag = fuse_deferred(F) ? 1 : 0;
-  }
-  __syncthreads();
-  const bool stand_aside = aside_flag != 0;  // failed, or the volume must grow first
-  if (F.upd_mask && !stand_aside) {
-    const uint32_t nq = q0 + nplaced;
-    const uint32_t bit = 1u << F.upd_slot;
-    // (every thread of the block runs the same number of iterations, so the
-    // list slots are claimed with one atomic per warp)
-    const uint32_t rounds = (nq + FIN_THREADS - 1) / FIN_THREADS;
-    for (uint32_t it = 0; it < rounds; it++) {
-      const uint32_t j = it * FIN_THREADS + (uint32_t)t;
-      bool add = false;
-      uint32_t b = 0;
-      if (j < nq) {
-        b = queue[j];
-        // a part of a sharded map updates the bricks it owns; the queue holds
-        // each brick once, so the old mask lacks this bit
-        if (F.shards <= 1 || owns_brick(F, leaf[b])) add = atomicOr(&F.upd_mask[b], bit) == 0u;
-      }
-      const unsigned ball = __ballot_sync(0xffffffffu, add);
-      uint32_t at = 0;
-      if ((t & 31) == 0 && ball) at = atomicAdd(F.upd_count, (uint32_t)__popc(ball));
-      at = __shfl_sync(0xffffffffu, at, 0);
-      if (add) F.upd_list[at + __popc(ball & ((1u << (t & 31)) - 1u))] = b;
+    Counters *nx = F.next_cnt;
+    if (nx) {
+      // the next frame of a sequence starts from this one's counts
+      nx->branches_used = branches_used;
+      nx->leaves_base = leaves_before + (uint32_t)npend;
+      if (stand_aside) atomicOr(&nx->error, ERR_SEQ_HALT);
     }
   }
-  if (t == 0) chain_next(F, cnt, leaves_before, stand_aside);
 }
 
 bool finalize_small_fits(uint32_t npix) {
