@@ -698,6 +698,7 @@ __device__ void save_top(const GenQueues &Q, int lv, const TopCache &T) {
 
 // (the cache's counts fit the queues: the queues only grow while it is valid)
 __global__ void k_load_top(GenQueues Q, int lv, TopCache T) {
+  pdl_enter();
   const int b = lv & 1;
   const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   if (t0 == 0) {
@@ -781,6 +782,7 @@ __device__ __forceinline__ uint64_t cell_key(const Cell &c, int B) {
 }
 
 __global__ void k_cell_keys(const Cell *cells, uint32_t n, int B, uint64_t *keys, uint32_t *error) {
+  pdl_enter();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Cell c = cells[i];
@@ -790,6 +792,7 @@ __global__ void k_cell_keys(const Cell *cells, uint32_t n, int B, uint64_t *keys
 }
 
 __global__ void k_gather_cells(const Cell *in, const uint32_t *order, uint32_t n, Cell *out) {
+  pdl_enter();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = in[order[i]];
 }
@@ -883,6 +886,7 @@ __device__ __forceinline__ uint32_t block_scan_keep(uint32_t v, uint32_t *total)
 // number kept (tile_sum).
 __global__ void __launch_bounds__(KEEP_THREADS) k_keep_cells(GenCtx g, uint32_t n, const Cell *__restrict__ old_cells,
                                                             uint32_t n_old, uint32_t *keep, uint32_t *tile_sum) {
+  pdl_enter();
   const uint32_t i = blockIdx.x * KEEP_THREADS + threadIdx.x;
   uint32_t k = 0;
   if (i < n_old) {
@@ -905,6 +909,7 @@ __global__ void __launch_bounds__(KEEP_THREADS) k_keep_cells(GenCtx g, uint32_t 
 // Exclusive scan of the tile sums in one block (any number of tiles, in
 // chunks of the block size).
 __global__ void __launch_bounds__(KEEP_SCAN_THREADS) k_keep_tile_scan(uint32_t *tile_sum, uint32_t ntiles) {
+  pdl_enter();
   __shared__ uint32_t warp_sum[KEEP_SCAN_THREADS / 32];
   __shared__ uint32_t carry;
   if (threadIdx.x == 0) carry = 0;
@@ -940,6 +945,7 @@ __global__ void __launch_bounds__(KEEP_SCAN_THREADS) k_keep_tile_scan(uint32_t *
 __global__ void __launch_bounds__(KEEP_THREADS) k_keep_apply(uint32_t *keep, uint32_t n_old, const uint32_t *tile_sum,
                                                             uint32_t ntiles, uint32_t first_corner_old,
                                                             uint32_t *counts) {
+  pdl_enter();
   const uint32_t i = blockIdx.x * KEEP_THREADS + threadIdx.x;
   const uint32_t k = i < n_old ? keep[i] : 0u;
   uint32_t total;
@@ -974,6 +980,7 @@ __global__ void k_merge_cells(const Cell *__restrict__ old_cells, const uint64_t
                               const uint32_t *__restrict__ keep_scan, uint32_t n_old, const Cell *__restrict__ raw,
                               const uint64_t *__restrict__ new_keys, const uint32_t *__restrict__ new_order,
                               uint32_t n_new, Cell *out, uint64_t *out_keys, uint32_t *error) {
+  pdl_enter();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n_old) {
     const uint32_t ks = keep_scan[i];
@@ -2167,6 +2174,8 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
                           std::string &err) {
   const int key_bits = key_bits_for(in.n);
   const uint32_t n_old = incr ? I.n_old : 0u;
+  // programmatic dependent launches, unless the stage profile is on
+  const bool pdl = !in.prof->on;
   const uint32_t first_corner_old = n_old - std::min(I.n_corners, n_old);
   const uint32_t keep_tiles = (n_old + KEEP_THREADS - 1) / KEEP_THREADS;
   if (incr) {
@@ -2223,11 +2232,12 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
       // the previous cells whose sides did not change, and their positions
       // among the kept (words KEPT_WORD, KEPT_WORD + 1: kept, kept before the
       // first corner cell)
+      // (the scan and the apply: programmatic dependents of the kernel before)
       note_launch(3);
       k_keep_cells<<<keep_tiles, KEEP_THREADS, 0, s>>>(g, in.n, I.old_cells, n_old, I.keep, I.keep_tiles);
-      k_keep_tile_scan<<<1, KEEP_SCAN_THREADS, 0, s>>>(I.keep_tiles, keep_tiles);
-      k_keep_apply<<<keep_tiles, KEEP_THREADS, 0, s>>>(I.keep, n_old, I.keep_tiles, keep_tiles, first_corner_old,
-                                                       I.d_count + KEPT_WORD);
+      MCK(launch_pdl(pdl, k_keep_tile_scan, dim3(1), dim3(KEEP_SCAN_THREADS), 0, s, I.keep_tiles, keep_tiles));
+      MCK(launch_pdl(pdl, k_keep_apply, dim3(keep_tiles), dim3(KEEP_THREADS), 0, s, I.keep, n_old,
+                     (const uint32_t *)I.keep_tiles, keep_tiles, first_corner_old, I.d_count + KEPT_WORD));
     }
     // The top levels: an incremental update whose frames created nothing
     // near the root starts from the kept level-MESH_TOP_LEVELS items;
@@ -2267,7 +2277,8 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
     I.gen_start_level = (uint32_t)lv0;
     if (use_top) {
       note_launch(1);
-      k_load_top<<<148 * 2, 256, 0, s>>>(Q, LC, T);
+      // (after the keep test's last kernel: a programmatic dependent)
+      MCK(launch_pdl(pdl, k_load_top, dim3(148 * 2), dim3(256), 0, s, Q, (int)LC, T));
     }
     // An item of level l holds slots of depth l at most, and it expands only
     // if one of them is subdivided, so the last level with items is the
@@ -2371,9 +2382,9 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
   MCK(grow_buf(I.vals_sorted, I.cap_vals2, n_new, s));
   MCK(grow_buf(I.cells, I.cap_cells, ncells, s));
   if (incr) MCK(grow_buf(I.mkeys, I.cap_mkeys, ncells, s));
+  // (keys, sort and merge follow one another on the stream: the sort and the
+  // merge or gather are programmatic dependents of the kernel before them)
   if (n_new) {
-    note_launch(1);
-    k_cell_keys<<<(n_new + 255) / 256, 256, 0, s>>>(I.raw, n_new, key_bits, I.keys, I.d_count + 9);
     const int end_bit = 3 * key_bits + 7;
     const size_t bytes = argsort_temp_bytes(n_new);
     if (bytes > I.sort_tmp_bytes) {
@@ -2382,23 +2393,27 @@ static int generate_cells(MeshImpl &I, const MeshInputs &in, bool incr, cudaStre
       MCK(pool_alloc(&I.sort_tmp, bytes, s));
       I.sort_tmp_bytes = bytes;
     }
+    note_launch(1);
+    k_cell_keys<<<(n_new + 255) / 256, 256, 0, s>>>(I.raw, n_new, key_bits, I.keys, I.d_count + 9);
     unsigned sort_launches = 0;
     MCK(argsort_u64(I.keys, n_new, end_bit, I.keys_sorted, I.vals_sorted, I.sort_tmp, I.sort_tmp_bytes, s,
-                    &sort_launches));
+                    &sort_launches, pdl));
     note_launch(sort_launches);
   }
   if (!incr) {
     if (n_new) {
       note_launch(1);
-      k_gather_cells<<<(n_new + 255) / 256, 256, 0, s>>>(I.raw, I.vals_sorted, n_new, I.cells);
+      MCK(launch_pdl(pdl, k_gather_cells, dim3((n_new + 255) / 256), dim3(256), 0, s, (const Cell *)I.raw,
+                     (const uint32_t *)I.vals_sorted, n_new, I.cells));
     }
   } else if (ncells) {
     // kept and new cells merged in key order; the merged keys replace the
     // sorted ones
     note_launch(1);
-    k_merge_cells<<<(n_old + n_new + 255) / 256, 256, 0, s>>>(I.old_cells, I.old_keys, I.keep, n_old, I.raw,
-                                                               I.keys_sorted, I.vals_sorted, n_new, I.cells, I.mkeys,
-                                                               I.d_count + 9);
+    MCK(launch_pdl(pdl && n_new > 0, k_merge_cells, dim3((n_old + n_new + 255) / 256), dim3(256), 0, s,
+                   (const Cell *)I.old_cells, (const uint64_t *)I.old_keys, (const uint32_t *)I.keep, n_old,
+                   (const Cell *)I.raw, (const uint64_t *)I.keys_sorted, (const uint32_t *)I.vals_sorted, n_new,
+                   I.cells, I.mkeys, I.d_count + 9));
     std::swap(I.mkeys, I.keys_sorted);
     std::swap(I.cap_mkeys, I.cap_keys2);
   }

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cstdint>
 
+#include "ff_common.cuh"
 #include "ff_sort.h"
 
 namespace ffb {
@@ -80,6 +81,7 @@ __device__ __forceinline__ void stage_in(uint64_t (&v)[E], uint32_t base, uint32
 template <int E>
 __global__ void __launch_bounds__(SORT_SMALL_THREADS) k_sort_small_reg(const uint64_t *__restrict__ keys, uint32_t n,
                                                                       uint64_t *keys_out, uint32_t *pos_out) {
+  pdl_enter();
   extern __shared__ uint64_t w[];
   constexpr uint32_t P = SORT_SMALL_THREADS * E;
   const uint32_t t = threadIdx.x, base = t * E;
@@ -273,7 +275,7 @@ size_t argsort_temp_bytes(uint32_t n) {
 }
 
 cudaError_t argsort_u64(const uint64_t *keys, uint32_t n, int end_bit, uint64_t *keys_out, uint32_t *pos_out,
-                        void *tmp, size_t tmp_bytes, cudaStream_t s, unsigned *launches) {
+                        void *tmp, size_t tmp_bytes, cudaStream_t s, unsigned *launches, bool pdl) {
   if (!n) return cudaSuccess;
   if (end_bit < 1 || end_bit > 64) return cudaErrorInvalidValue;
   if (small_path(n, end_bit)) {
@@ -292,16 +294,19 @@ cudaError_t argsort_u64(const uint64_t *keys, uint32_t n, int end_bit, uint64_t 
     }
     // words per thread: the smallest power of two with 1024 E >= n
     const size_t per = sizeof(uint64_t) * SORT_SMALL_THREADS;
+    const dim3 one(1), blk(SORT_SMALL_THREADS);
+    cudaError_t le;
     if (n <= 1024u)
-      k_sort_small_reg<1><<<1, SORT_SMALL_THREADS, per, s>>>(keys, n, keys_out, pos_out);
+      le = launch_pdl(pdl, k_sort_small_reg<1>, one, blk, per, s, keys, n, keys_out, pos_out);
     else if (n <= 2048u)
-      k_sort_small_reg<2><<<1, SORT_SMALL_THREADS, 2 * per, s>>>(keys, n, keys_out, pos_out);
+      le = launch_pdl(pdl, k_sort_small_reg<2>, one, blk, 2 * per, s, keys, n, keys_out, pos_out);
     else if (n <= 4096u)
-      k_sort_small_reg<4><<<1, SORT_SMALL_THREADS, 4 * per, s>>>(keys, n, keys_out, pos_out);
+      le = launch_pdl(pdl, k_sort_small_reg<4>, one, blk, 4 * per, s, keys, n, keys_out, pos_out);
     else if (n <= 8192u)
-      k_sort_small_reg<8><<<1, SORT_SMALL_THREADS, 8 * per, s>>>(keys, n, keys_out, pos_out);
+      le = launch_pdl(pdl, k_sort_small_reg<8>, one, blk, 8 * per, s, keys, n, keys_out, pos_out);
     else
-      k_sort_small_reg<16><<<1, SORT_SMALL_THREADS, 16 * per, s>>>(keys, n, keys_out, pos_out);
+      le = launch_pdl(pdl, k_sort_small_reg<16>, one, blk, 16 * per, s, keys, n, keys_out, pos_out);
+    if (le != cudaSuccess) return le;
     if (launches) *launches += 1;
     return cudaGetLastError();
   }
